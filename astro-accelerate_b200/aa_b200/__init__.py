@@ -1,0 +1,465 @@
+"""Python binding of the B200-native dedispersion library (libaa_b200.so).
+
+The classes mirror the reference's ctypes wrapper of its C ABI
+(AstroAccelerate v1.3.1, cmake/py_astro_accelerate.py.in:120-560):
+``aa_py_filterbank_metadata``, ``aa_py_dm``, ``aa_py_ddtr_plan``,
+``aa_py_pipeline_components``, ``aa_py_pipeline_component_options`` and
+``aa_py_pipeline`` keep their names, arguments and return values, so a script
+written against the reference runs against this library.  The functions below
+them expose the library's own seam (stateless device-pointer entry points)
+and extensions.
+
+There is no CPU fallback: every entry point runs the CUDA kernels of
+libaa_b200.so and fails loudly when the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libaa_b200.so")
+
+FLOAT = ctypes.c_float
+PFLOAT = ctypes.POINTER(FLOAT)
+PPFLOAT = ctypes.POINTER(PFLOAT)
+PPPFLOAT = ctypes.POINTER(PPFLOAT)
+
+KIND_SHARED8, KIND_SHARED16, KIND_SHARED4, KIND_CACHE = 0, 1, 2, 3
+KIND_NAMES = {0: "shared8", 1: "shared16", 2: "shared4", 3: "cache"}
+STRIDE_REFERENCE, STRIDE_TRUE = 0, 1
+STATUS_ERROR, STATUS_FINISHED, STATUS_HAS_MORE, STATUS_FINISHED_COMPONENT = -1, 0, 1, 2
+
+
+def build(jobs: int = 8) -> str:
+    """Compile libaa_b200.so for sm_100a with nvcc (no GPU needed)."""
+    subprocess.check_call(["make", "-C", PKG_ROOT, f"-j{jobs}"], stdout=subprocess.DEVNULL)
+    return LIB_PATH
+
+
+class filterbank_metadata_struct(ctypes.Structure):
+    """include/aa_py_filterbank_metadata.hpp:15-25."""
+
+    _fields_ = [("m_tstart", ctypes.c_double), ("m_tsamp", ctypes.c_double), ("m_fch1", ctypes.c_double),
+                ("m_foff", ctypes.c_double), ("m_nbits", ctypes.c_int), ("m_nsamples", ctypes.c_int),
+                ("m_nchans", ctypes.c_int), ("m_src_raj", ctypes.c_double)]
+
+
+class aa_py_pipeline_components(ctypes.Structure):
+    """include/aa_py_pipeline_api.hpp:20-25."""
+
+    _fields_ = [("dedispersion", ctypes.c_bool), ("analysis", ctypes.c_bool), ("periodicity", ctypes.c_bool),
+                ("fdas", ctypes.c_bool)]
+
+
+class aa_py_pipeline_component_options(ctypes.Structure):
+    """include/aa_py_pipeline_api.hpp:32-48."""
+
+    _fields_ = [(n, ctypes.c_bool) for n in (
+        "zero_dm", "zero_dm_with_outliers", "input_DDTR_normalization", "output_DDTR_normalization",
+        "set_bandpass_average", "old_rfi", "copy_ddtr_data_to_host", "msd_baseline_noise", "output_dmt",
+        "output_ffdot_plan", "output_fdas_list", "candidate_algorithm", "fdas_custom_fft", "fdas_inbin",
+        "fdas_norm")]
+
+
+class aa_b200_dm(ctypes.Structure):
+    """include/aa_ddtr_plan.hpp:28-34 struct dm."""
+
+    _fields_ = [("low", ctypes.c_float), ("high", ctypes.c_float), ("step", ctypes.c_float),
+                ("inBin", ctypes.c_int), ("outBin", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded libaa_b200.so with its prototypes (raises if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libaa_b200.so is not built ({LIB_PATH}); run aa_b200.build() or "
+                           "`make -C astro-accelerate_b200`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i, f, d, b, sz, ll = (ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double, ctypes.c_bool,
+                              ctypes.c_size_t, ctypes.c_longlong)
+    P = ctypes.POINTER
+    protos = {
+        "aa_py_filterbank_metadata": ([d, d, i, i, d, d, i, d], vp),
+        "aa_py_filterbank_metadata_delete": ([vp], None),
+        "aa_py_filterbank_metadata_tstart": ([vp], d),
+        "aa_py_ddtr_plan": ([], vp),
+        "aa_py_ddtr_plan_delete": ([vp], None),
+        "aa_py_ddtr_plan_add_dm": ([vp, f, f, f, i, i], b),
+        "aa_py_ddtr_plan_range": ([vp], sz),
+        "aa_py_ddtr_plan_set_power": ([vp, f], b),
+        "aa_py_ddtr_plan_power": ([vp], f),
+        "aa_py_ddtr_plan_set_enable_msd_baseline": ([vp, b], b),
+        "aa_py_ddtr_plan_enable_msd_baseline_noise": ([vp], b),
+        "aa_py_ddtr_plan_bind_bandpass_normalization": ([vp, PFLOAT, i], b),
+        "aa_py_pipeline_api": ([aa_py_pipeline_components, aa_py_pipeline_component_options,
+                                filterbank_metadata_struct, P(ctypes.c_ushort), i], vp),
+        "aa_py_pipeline_api_delete": ([vp], None),
+        "aa_py_pipeline_api_bind_ddtr_plan": ([vp, vp], b),
+        "aa_py_pipeline_api_ddtr_strategy": ([vp], vp),
+        "aa_py_ddtr_strategy_delete": ([vp], None),
+        "aa_py_get_ddtr_nRanges": ([vp], sz),
+        "aa_py_get_ndms_array": ([vp], P(i)),
+        "aa_py_get_t_proc": ([vp, i, i], i),
+        "aa_py_dm_low": ([vp, i], i),
+        "aa_py_total_computed_samples": ([vp], i),
+        "aa_py_pipeline_api_bind_analysis_plan": ([vp, vp], b),
+        "aa_py_pipeline_api_bind_periodicity_plan": ([vp, f, b, f, i, i], b),
+        "aa_py_pipeline_api_bind_fdas_plan": ([vp, f, f, b], b),
+        "aa_py_pipeline_api_run": ([vp, P(i)], b),
+        "aa_py_buffer": ([vp], PPPFLOAT),
+        "aa_py_current_range": ([vp], i),
+        "aa_py_current_time_chunk": ([vp], i),
+        "aa_py_current_inc": ([vp], ctypes.c_long),
+        "aa_py_cleanup": ([vp], b),
+        "aa_b200_strategy": ([P(aa_b200_dm), i, f, i, i, d, d, d, i, sz, i, i, P(f), P(i), P(aa_b200_dm),
+                              P(i), P(i), P(i), P(i)], i),
+        "aa_b200_select_kernel": ([i, f, f, f, i], i),
+        "aa_b200_corner_turn": ([vp, vp, i, i, ll, ll, vp], i),
+        "aa_b200_bin_gpu": ([vp, vp, i, i, ll, vp], i),
+        "aa_b200_dedisperse": ([i, i, P(i), P(f), vp, ll, sz, vp, ll, i, P(f), P(f), P(f), P(i), i, i, vp], i),
+        "aa_b200_last_error": ([], ctypes.c_char_p),
+        "aa_b200_kernel_launches": ([], ll),
+        "aa_b200_version": ([], ctypes.c_char_p),
+        "aa_b200_pipeline_set_options": ([vp, i, i, i, sz, i, i], b),
+        "aa_b200_pipeline_create": ([filterbank_metadata_struct, vp, i, i, i, vp, i], vp),
+        "aa_b200_pipeline_run_all": ([vp], b),
+        "aa_b200_pipeline_rewind": ([vp], b),
+        "aa_b200_pipeline_synchronize": ([vp], b),
+        "aa_b200_pipeline_device_output": ([vp, i], vp),
+        "aa_b200_pipeline_range_info": ([vp, i, P(i), P(i), P(i), P(i)], i),
+        "aa_b200_pipeline_kernel_launches": ([vp], ll),
+        "aa_b200_pipeline_last_error": ([vp], ctypes.c_char_p),
+        "aa_b200_pipeline_num_tchunks": ([vp], i),
+        "aa_b200_pipeline_maxshift": ([vp], i),
+        "aa_b200_pipeline_time_kernels": ([vp, i], b),
+        "aa_b200_pipeline_kernel_time": ([vp, i, P(d), P(ll)], i),
+        "aa_b200_pipeline_reset_kernel_times": ([vp], b),
+    }
+    for name, (args, res) in protos.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def declared_symbols() -> list:
+    """Every function name include/aa_b200.h declares."""
+    import re
+    hdr = os.path.join(os.path.dirname(PKG_ROOT), "include", "aa_b200.h")
+    text = open(hdr).read()
+    return sorted(set(re.findall(r"\b(aa_(?:py|b200)_\w+)\s*\(", text)))
+
+
+def last_error() -> str:
+    return lib().aa_b200_last_error().decode()
+
+
+# ---------------------------------------------------------------------------
+# Reference-facing classes (cmake/py_astro_accelerate.py.in)
+# ---------------------------------------------------------------------------
+class aa_py_filterbank_metadata:
+    def __init__(self, tstart: float, tsamp: float, nbits: int, nsamples: int, fch1: float, foff: float,
+                 nchans: int, src_raj: float = 0.0):
+        self.m_tstart, self.m_tsamp, self.m_nbits, self.m_nsamples = tstart, tsamp, nbits, nsamples
+        self.m_fch1, self.m_foff, self.m_nchans, self.m_src_raj = fch1, foff, nchans, src_raj
+        self.m_obj = lib().aa_py_filterbank_metadata(tstart, tsamp, nbits, nsamples, fch1, foff, nchans, src_raj)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, exc_type, exc_value, traceback):
+        lib().aa_py_filterbank_metadata_delete(self.m_obj)
+
+    def pointer(self):
+        return self.m_obj
+
+    def tstart(self):
+        return lib().aa_py_filterbank_metadata_tstart(self.m_obj)
+
+    def struct(self) -> filterbank_metadata_struct:
+        return filterbank_metadata_struct(self.m_tstart, self.m_tsamp, self.m_fch1, self.m_foff, self.m_nbits,
+                                          self.m_nsamples, self.m_nchans, self.m_src_raj)
+
+
+class aa_py_dm:
+    def __init__(self, low: float, high: float, step: float, inBin: int, outBin: int):
+        self.m_low, self.m_high, self.m_step, self.m_inBin, self.m_outBin = low, high, step, inBin, outBin
+
+    def low(self):
+        return self.m_low
+
+    def high(self):
+        return self.m_high
+
+    def step(self):
+        return self.m_step
+
+    def inBin(self):
+        return self.m_inBin
+
+    def outBin(self):
+        return self.m_outBin
+
+
+class aa_py_ddtr_plan:
+    def __init__(self, dm):
+        self.m_obj = lib().aa_py_ddtr_plan()
+        self.m_dm = list(dm)
+        for r in self.m_dm:
+            lib().aa_py_ddtr_plan_add_dm(self.m_obj, r.low(), r.high(), r.step(), r.inBin(), r.outBin())
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, exc_type, exc_value, traceback):
+        self.delete()
+
+    def delete(self):
+        if self.m_obj:
+            lib().aa_py_ddtr_plan_delete(self.m_obj)
+            self.m_obj = None
+
+    def pointer(self):
+        return self.m_obj
+
+    def set_power(self, power: float):
+        return lib().aa_py_ddtr_plan_set_power(self.m_obj, power)
+
+    def power(self):
+        return lib().aa_py_ddtr_plan_power(self.m_obj)
+
+    def set_enable_msd_baseline_noise(self, flag: bool):
+        return lib().aa_py_ddtr_plan_set_enable_msd_baseline(self.m_obj, flag)
+
+    def enable_msd_baseline_noise(self):
+        return lib().aa_py_ddtr_plan_enable_msd_baseline_noise(self.m_obj)
+
+    def bind_bandpass_normalization(self, data, data_size: int):
+        arr = np.ascontiguousarray(data, dtype=np.float32)
+        return lib().aa_py_ddtr_plan_bind_bandpass_normalization(self.m_obj, arr.ctypes.data_as(PFLOAT), data_size)
+
+    def range(self):
+        return lib().aa_py_ddtr_plan_range(self.m_obj)
+
+
+class aa_py_pipeline:
+    """aa_pipeline_api<unsigned short> through the C ABI."""
+
+    def __init__(self, pipeline: aa_py_pipeline_components, pipeline_options: aa_py_pipeline_component_options,
+                 metadata: filterbank_metadata_struct, input_data, card_number: int):
+        if isinstance(input_data, np.ndarray):
+            self._input_keepalive = input_data
+            input_data = input_data.ctypes.data_as(ctypes.POINTER(ctypes.c_ushort))
+        self.m_obj = lib().aa_py_pipeline_api(pipeline, pipeline_options, metadata, input_data, card_number)
+        self.m_status_code_c_int = ctypes.c_int(0)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, exc_type, exc_value, traceback):
+        self.delete()
+
+    def delete(self):
+        if self.m_obj:
+            lib().aa_py_pipeline_api_delete(self.m_obj)
+            self.m_obj = None
+
+    def bind_ddtr_plan(self, plan: aa_py_ddtr_plan):
+        return lib().aa_py_pipeline_api_bind_ddtr_plan(self.m_obj, plan.pointer())
+
+    def ddtr_strategy(self):
+        return lib().aa_py_pipeline_api_ddtr_strategy(self.m_obj)
+
+    def ddtr_range(self):
+        return lib().aa_py_get_ddtr_nRanges(self.m_obj)
+
+    def ddtr_ndms(self):
+        return lib().aa_py_get_ndms_array(self.m_obj)
+
+    def bind_analysis_plan(self, plan):
+        return lib().aa_py_pipeline_api_bind_analysis_plan(self.m_obj, None)
+
+    def bind_periodicity_plan(self, plan):
+        return lib().aa_py_pipeline_api_bind_periodicity_plan(self.m_obj, 0.0, False, 0.0, 0, 0)
+
+    def bind_fdas_plan(self, plan):
+        return lib().aa_py_pipeline_api_bind_fdas_plan(self.m_obj, 0.0, 0.0, False)
+
+    def run(self):
+        return bool(lib().aa_py_pipeline_api_run(self.m_obj, ctypes.byref(self.m_status_code_c_int)))
+
+    def status_code(self):
+        return self.m_status_code_c_int.value
+
+    def get_buffer(self):
+        return lib().aa_py_total_computed_samples(self.m_obj), lib().aa_py_buffer(self.m_obj)
+
+    def dm_low(self, pos: int):
+        return lib().aa_py_dm_low(self.m_obj, pos)
+
+    def t_processed(self, i: int, j: int):
+        return lib().aa_py_get_t_proc(self.m_obj, i, j)
+
+    def cleanUp(self):
+        return bool(lib().aa_py_cleanup(self.m_obj))
+
+    # ---- extensions of this library ----
+    def set_options(self, stride_mode=STRIDE_REFERENCE, fma_mode=7, failsafe=0, free_memory=0, tile_words=0,
+                    group_dms=0):
+        ok = lib().aa_b200_pipeline_set_options(self.m_obj, stride_mode, fma_mode, failsafe, free_memory,
+                                                 tile_words, group_dms)
+        if not ok:
+            raise ValueError(self.last_error())
+        return ok
+
+    def run_all(self):
+        return bool(lib().aa_b200_pipeline_run_all(self.m_obj))
+
+    def rewind(self):
+        return bool(lib().aa_b200_pipeline_rewind(self.m_obj))
+
+    def synchronize(self):
+        return bool(lib().aa_b200_pipeline_synchronize(self.m_obj))
+
+    def last_error(self) -> str:
+        return lib().aa_b200_pipeline_last_error(self.m_obj).decode()
+
+    def kernel_launches(self) -> int:
+        return lib().aa_b200_pipeline_kernel_launches(self.m_obj)
+
+    def num_tchunks(self) -> int:
+        return lib().aa_b200_pipeline_num_tchunks(self.m_obj)
+
+    def maxshift(self) -> int:
+        return lib().aa_b200_pipeline_maxshift(self.m_obj)
+
+    def range_info(self, r: int) -> dict:
+        k, g, s, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        if lib().aa_b200_pipeline_range_info(self.m_obj, r, ctypes.byref(k), ctypes.byref(g), ctypes.byref(s),
+                                              ctypes.byref(t)):
+            raise RuntimeError(self.last_error())
+        return {"kind": KIND_NAMES[k.value], "group_dms": g.value, "span": s.value, "tile_words": t.value}
+
+    def time_kernels(self, on: bool = True):
+        return bool(lib().aa_b200_pipeline_time_kernels(self.m_obj, int(on)))
+
+    def kernel_time(self, family: int = 0):
+        """(ms, launches) of a kernel family: 0 dedispersion, 1 corner turn, 2 binning."""
+        ms, n = ctypes.c_double(), ctypes.c_longlong()
+        if lib().aa_b200_pipeline_kernel_time(self.m_obj, family, ctypes.byref(ms), ctypes.byref(n)):
+            raise RuntimeError(self.last_error())
+        return ms.value, n.value
+
+    def reset_kernel_times(self):
+        return bool(lib().aa_b200_pipeline_reset_kernel_times(self.m_obj))
+
+    def device_output(self, r: int) -> int:
+        return lib().aa_b200_pipeline_device_output(self.m_obj, r) or 0
+
+    def output_arrays(self):
+        """The host output rows as numpy arrays [range] -> (ndms, total_samps).
+
+        Rows of one range are contiguous in this library's pinned output block,
+        so each range is one zero-copy view."""
+        nr = self.ddtr_range()
+        ndms = self.ddtr_ndms()
+        buf = lib().aa_py_buffer(self.m_obj)
+        nt = self.num_tchunks()
+        out = []
+        for r in range(nr):
+            tot = sum(self.t_processed(r, k) for k in range(nt))
+            n = ndms[r]
+            base = ctypes.cast(buf[r][0], ctypes.c_void_p).value
+            arr = np.ctypeslib.as_array((ctypes.c_float * (n * tot)).from_address(base)).reshape(n, tot)
+            out.append(arr)
+        return out
+
+
+def create_pipeline(metadata: filterbank_metadata_struct, input_ptr: int, device_input: bool,
+                    device_output: bool, copy_to_host: bool, stream: int = 0, card_number: int = 0):
+    """A pipeline over device-resident input and/or output (this library's extension)."""
+    p = aa_py_pipeline.__new__(aa_py_pipeline)
+    p.m_obj = lib().aa_b200_pipeline_create(metadata, ctypes.c_void_p(input_ptr), int(device_input),
+                                            int(device_output), int(copy_to_host), ctypes.c_void_p(stream),
+                                            card_number)
+    p.m_status_code_c_int = ctypes.c_int(0)
+    return p
+
+
+# ---------------------------------------------------------------------------
+# Seam (stateless)
+# ---------------------------------------------------------------------------
+def strategy(plan, nchans, nsamp, fch1, foff, tsamp, nbits, free_memory=180 * 2**30, power=2.0,
+             enable_analysis=False, max_chunks=4096):
+    """The reference strategy computed by this library's planner (host only)."""
+    L = lib()
+    nr = len(plan)
+    parr = (aa_b200_dm * nr)(*[aa_b200_dm(*p) for p in plan])
+    dmshifts = np.zeros(nchans, np.float32)
+    ndms = (ctypes.c_int * nr)()
+    sdm = (aa_b200_dm * nr)()
+    ms, mx, nt = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    tp = np.zeros(nr * max_chunks, np.int32)
+    rc = L.aa_b200_strategy(parr, nr, power, nchans, nsamp, fch1, foff, tsamp, nbits, free_memory,
+                            int(enable_analysis), max_chunks, dmshifts.ctypes.data_as(PFLOAT), ndms, sdm,
+                            ctypes.byref(ms), ctypes.byref(mx), ctypes.byref(nt),
+                            tp.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    if rc != 0:
+        raise ValueError(f"strategy refused the plan (code {rc})")
+    return {
+        "dmshifts": dmshifts,
+        "ndms": [int(ndms[r]) for r in range(nr)],
+        "dm": [(sdm[r].low, sdm[r].high, sdm[r].step, sdm[r].inBin, sdm[r].outBin) for r in range(nr)],
+        "maxshift": ms.value,
+        "max_ndms": mx.value,
+        "num_tchunks": nt.value,
+        "t_processed": [[int(tp[r * max_chunks + k]) for k in range(nt.value)] for r in range(nr)],
+    }
+
+
+def select_kernel(nbits, dm_step, tsamp, dmshift_last, failsafe=0) -> int:
+    return lib().aa_b200_select_kernel(nbits, dm_step, tsamp, dmshift_last, failsafe)
+
+
+def _ptr(x) -> int:
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    return int(x)
+
+
+def corner_turn(d_in_tc, d_out, nbits, nchans, nsamp, out_stride, stream=0):
+    if lib().aa_b200_corner_turn(_ptr(d_in_tc), _ptr(d_out), nbits, nchans, nsamp, out_stride, stream):
+        raise RuntimeError(last_error())
+
+
+def bin_gpu(d_src, d_dst, nbits, nchans, nsamp, stream=0):
+    if lib().aa_b200_bin_gpu(_ptr(d_src), _ptr(d_dst), nbits, nchans, nsamp, stream):
+        raise RuntimeError(last_error())
+
+
+def dedisperse(i, t_processed, inBin, dmshifts, d_input, i_nsamp, d_input_elems, d_output, out_pitch, nchans,
+               tsamp, dm_low, dm_step, ndms, nbits, failsafe=0, stream=0):
+    """dedisperse() of src/aa_dedisperse.cpp:5 with explicit stride, size and stream."""
+    nr = len(ndms)
+    inb = (ctypes.c_int * nr)(*inBin)
+    sh = np.ascontiguousarray(dmshifts, dtype=np.float32)
+    ts = ctypes.c_float(tsamp)
+    lo = (ctypes.c_float * nr)(*dm_low)
+    st = (ctypes.c_float * nr)(*dm_step)
+    nd = (ctypes.c_int * nr)(*ndms)
+    rc = lib().aa_b200_dedisperse(i, t_processed, inb, sh.ctypes.data_as(PFLOAT), _ptr(d_input), i_nsamp,
+                                  d_input_elems, _ptr(d_output), out_pitch, nchans, ctypes.byref(ts), lo, st, nd,
+                                  nbits, failsafe, stream)
+    if rc:
+        raise RuntimeError(last_error())

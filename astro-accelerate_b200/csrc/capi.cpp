@@ -1,0 +1,616 @@
+// capi.cpp -- extern "C" entry points declared in include/aa_b200.h.
+#include "aa_b200.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "ddtr_kernels.cuh"
+#include "pipeline.hpp"
+#include "planner.hpp"
+
+using namespace aab200;
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<long long> g_launches{0};
+
+void set_error(const std::string &m) { g_last_error = m; }
+
+// The object behind aa_py_pipeline_api (aa_pipeline_api<unsigned short>).
+struct Api {
+    pipeline_components_struct components;
+    pipeline_component_option_struct options;
+    FilterbankMetadata meta;
+    const unsigned short *input = nullptr;
+    int card = 0;
+    PipelineOptions popt;
+    std::unique_ptr<DdtrPipeline> pipe;
+    std::string error;
+    bool supported = true;
+};
+
+FilterbankMetadata to_meta(const aa_py_filterbank_metadata_struct &m)
+{
+    FilterbankMetadata f;
+    f.tstart = m.m_tstart;
+    f.tsamp = m.m_tsamp;
+    f.fch1 = m.m_fch1;
+    f.foff = m.m_foff;
+    f.nbits = m.m_nbits;
+    f.nsamples = m.m_nsamples;
+    f.nchans = m.m_nchans;
+    return f;
+}
+
+Api *as_api(void *p) { return static_cast<Api *>(p); }
+
+bool api_fail(Api *a, const std::string &m)
+{
+    if (a && a->error.empty())
+        a->error = m;
+    set_error(m);
+    return false;
+}
+
+int elem_bytes_for(int nbits) { return nbits <= 8 ? 1 : 2; }
+
+} // namespace
+
+extern "C" {
+
+// ---------------------------------------------------------------------------
+// metadata (src/aa_py_filterbank_metadata.cpp)
+// ---------------------------------------------------------------------------
+aa_py_filterbank_metadata_struct *aa_py_filterbank_metadata(double tstart, double tsamp, int nbits, int nsamples,
+                                                            double fch1, double foff, int nchans, double src_raj)
+{
+    auto *m = new aa_py_filterbank_metadata_struct;
+    m->m_tstart = tstart;
+    m->m_tsamp = tsamp;
+    m->m_fch1 = fch1;
+    m->m_foff = foff;
+    m->m_nbits = nbits;
+    m->m_nsamples = nsamples;
+    m->m_nchans = nchans;
+    m->m_src_raj = src_raj;
+    return m;
+}
+void aa_py_filterbank_metadata_delete(const aa_py_filterbank_metadata_struct *obj) { delete obj; }
+double aa_py_filterbank_metadata_tstart(const aa_py_filterbank_metadata_struct *obj) { return obj->m_tstart; }
+
+// ---------------------------------------------------------------------------
+// plan (src/aa_py_ddtr_plan.cpp)
+// ---------------------------------------------------------------------------
+void *aa_py_ddtr_plan(void) { return new DdtrPlan(); }
+void aa_py_ddtr_plan_delete(const void *obj) { delete static_cast<const DdtrPlan *>(obj); }
+bool aa_py_ddtr_plan_add_dm(void *obj, float low, float high, float step, int inBin, int outBin)
+{
+    return static_cast<DdtrPlan *>(obj)->add_dm(low, high, step, inBin, outBin);
+}
+size_t aa_py_ddtr_plan_range(const void *obj) { return static_cast<const DdtrPlan *>(obj)->range(); }
+bool aa_py_ddtr_plan_set_power(void *obj, float power) { return static_cast<DdtrPlan *>(obj)->set_power(power); }
+float aa_py_ddtr_plan_power(const void *obj) { return static_cast<const DdtrPlan *>(obj)->power(); }
+bool aa_py_ddtr_plan_set_enable_msd_baseline(void *obj, bool flag)
+{
+    return static_cast<DdtrPlan *>(obj)->set_enable_msd_baseline_noise(flag);
+}
+bool aa_py_ddtr_plan_enable_msd_baseline_noise(const void *obj)
+{
+    return static_cast<const DdtrPlan *>(obj)->enable_msd_baseline_noise();
+}
+bool aa_py_ddtr_plan_bind_bandpass_normalization(void *obj, const float *data, int data_size)
+{
+    return static_cast<DdtrPlan *>(obj)->bind_bandpass_normalization(data, data_size);
+}
+
+// ---------------------------------------------------------------------------
+// pipeline (src/aa_py_pipeline_api.cpp)
+// ---------------------------------------------------------------------------
+void *aa_py_pipeline_api(pipeline_components_struct pipeline, pipeline_component_option_struct options,
+                         aa_py_filterbank_metadata_struct metadata, const unsigned short *input_data,
+                         int card_number)
+{
+    Api *a = new Api();
+    a->components = pipeline;
+    a->options = options;
+    a->meta = to_meta(metadata);
+    a->input = input_data;
+    a->card = card_number;
+    a->popt.copy_to_host = options.copy_ddtr_data_to_host;
+    if (pipeline.analysis || pipeline.periodicity || pipeline.fdas || !pipeline.dedispersion) {
+        a->supported = false;
+        api_fail(a, "only the dedispersion component is implemented by this library");
+    }
+    if (options.zero_dm || options.zero_dm_with_outliers || options.input_DDTR_normalization ||
+        options.output_DDTR_normalization || options.set_bandpass_average || options.old_rfi || options.output_dmt) {
+        a->supported = false;
+        api_fail(a, "pre/post-processing options (zero DM, normalisation, RFI, output_dmt) are not implemented");
+    }
+    return a;
+}
+
+void aa_py_pipeline_api_delete(const void *obj) { delete static_cast<const Api *>(obj); }
+
+bool aa_py_pipeline_api_bind_ddtr_plan(void *obj, const void *plan)
+{
+    Api *a = as_api(obj);
+    if (!a->supported)
+        return false;
+    if (a->pipe)
+        return api_fail(a, "a DDTR plan is already bound");
+    if (cudaSetDevice(a->card) != cudaSuccess)
+        return api_fail(a, "cannot select CUDA device " + std::to_string(a->card));
+    a->pipe.reset(new DdtrPipeline(a->meta, a->input, a->popt));
+    if (!a->pipe->bind(*static_cast<const DdtrPlan *>(plan))) {
+        api_fail(a, a->pipe->last_error());
+        a->pipe.reset();
+        return false;
+    }
+    return true;
+}
+
+void *aa_py_pipeline_api_ddtr_strategy(void *obj)
+{
+    Api *a = as_api(obj);
+    if (!a->pipe)
+        return nullptr;
+    return new DdtrStrategy(a->pipe->strategy());
+}
+void aa_py_ddtr_strategy_delete(const void *obj) { delete static_cast<const DdtrStrategy *>(obj); }
+
+size_t aa_py_get_ddtr_nRanges(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? a->pipe->strategy().nranges() : 0;
+}
+const int *aa_py_get_ndms_array(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? a->pipe->strategy().ndms_data() : nullptr;
+}
+int aa_py_get_t_proc(void *obj, int i, int j)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? a->pipe->strategy().t_processed()[i][j] : 0;
+}
+int aa_py_dm_low(void *obj, int range)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? static_cast<int>(a->pipe->strategy().dm(range).low) : 0;
+}
+int aa_py_total_computed_samples(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? static_cast<int>(a->pipe->strategy().nProcessedTimesamples()) : 0;
+}
+
+bool aa_py_pipeline_api_bind_analysis_plan(void *obj, const void *)
+{
+    return api_fail(as_api(obj), "analysis (single-pulse search) is not implemented by this library");
+}
+bool aa_py_pipeline_api_bind_periodicity_plan(void *obj, float, bool, float, int, int)
+{
+    return api_fail(as_api(obj), "periodicity search is not implemented by this library");
+}
+bool aa_py_pipeline_api_bind_fdas_plan(void *obj, float, float, bool)
+{
+    return api_fail(as_api(obj), "FDAS is not implemented by this library");
+}
+
+bool aa_py_pipeline_api_run(void *obj, int *status_code)
+{
+    Api *a = as_api(obj);
+    if (!a->supported || !a->pipe || !a->pipe->ready()) {
+        *status_code = static_cast<int>(RunStatus::error);
+        if (!a->pipe)
+            api_fail(a, "no DDTR plan bound");
+        return false;
+    }
+    RunStatus st = RunStatus::finished;
+    const bool more = a->pipe->next(st);
+    *status_code = static_cast<int>(st);
+    if (st == RunStatus::error) {
+        api_fail(a, a->pipe->last_error());
+        return false;
+    }
+    return more;
+}
+
+float ***aa_py_buffer(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? a->pipe->output_buffer() : nullptr;
+}
+int aa_py_current_range(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? a->pipe->current_range() : 0;
+}
+int aa_py_current_time_chunk(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? a->pipe->current_tchunk() : 0;
+}
+long aa_py_current_inc(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? static_cast<long>(a->pipe->current_inc()) : 0;
+}
+bool aa_py_cleanup(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? a->pipe->cleanup() : true;
+}
+
+// ---------------------------------------------------------------------------
+// seam
+// ---------------------------------------------------------------------------
+int aa_b200_strategy(const aa_b200_dm *plan, int nranges, float power, int nchans, int nsamp, double fch1,
+                     double foff, double tsamp, int nbits, size_t free_memory, int enable_analysis, int max_chunks,
+                     float *dmshifts, int *ndms, aa_b200_dm *str_dm, int *maxshift, int *max_ndms, int *num_tchunks,
+                     int *t_processed)
+{
+    DdtrPlan p;
+    for (int i = 0; i < nranges; ++i)
+        p.add_dm(plan[i].low, plan[i].high, plan[i].step, plan[i].inBin, plan[i].outBin);
+    p.set_power(power);
+    FilterbankMetadata m;
+    m.tsamp = tsamp;
+    m.fch1 = fch1;
+    m.foff = foff;
+    m.nbits = nbits;
+    m.nsamples = nsamp;
+    m.nchans = nchans;
+    DdtrStrategy s;
+    const StrategyStatus rc = s.compute(p, m, free_memory, enable_analysis != 0);
+    if (rc != STRAT_OK) {
+        set_error("strategy refused the plan");
+        return static_cast<int>(rc);
+    }
+    if (s.num_tchunks() > max_chunks) {
+        set_error("more time chunks than max_chunks");
+        return -5;
+    }
+    std::copy(s.dmshifts().begin(), s.dmshifts().end(), dmshifts);
+    for (int i = 0; i < nranges; ++i) {
+        ndms[i] = s.ndms(i);
+        const DmRange &d = s.dm(i);
+        str_dm[i] = aa_b200_dm{d.low, d.high, d.step, d.inBin, d.outBin};
+        for (int k = 0; k < s.num_tchunks(); ++k)
+            t_processed[i * max_chunks + k] = s.t_processed()[i][k];
+    }
+    *maxshift = s.maxshift();
+    *max_ndms = s.max_ndms();
+    *num_tchunks = s.num_tchunks();
+    return 0;
+}
+
+int aa_b200_select_kernel(int nbits, float dm_step, float tsamp, float dmshift_last, int failsafe)
+{
+    return select_delay_kind(nbits, dm_step, tsamp, dmshift_last, failsafe);
+}
+
+int aa_b200_corner_turn(const unsigned short *d_in_tc, void *d_out, int nbits, int nchans, long long nsamp,
+                        long long out_stride, void *stream)
+{
+    int *d_err = nullptr;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMalloc(&d_err, sizeof(int)) != cudaSuccess) {
+        set_error("cudaMalloc failed");
+        return 1;
+    }
+    cudaMemsetAsync(d_err, 0, sizeof(int), st);
+    const int max_value = (nbits == 4) ? 15 : (nbits <= 8 ? 255 : 65535);
+    cudaError_t e = launch_corner_turn(d_in_tc, d_out, elem_bytes_for(nbits), nchans, nsamp, out_stride, max_value,
+                                       d_err, st);
+    ++g_launches;
+    int h = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    cudaFree(d_err);
+    if (e != cudaSuccess) {
+        set_error(cudaGetErrorString(e));
+        return 1;
+    }
+    if (h) {
+        set_error("input sample above the bit depth's range");
+        return 1;
+    }
+    return 0;
+}
+
+int aa_b200_bin_gpu(const void *d_src, void *d_dst, int nbits, int nchans, long long nsamp, void *stream)
+{
+    if (nsamp <= 0 || (nsamp & 1)) {
+        set_error("nsamp must be positive and even");
+        return 1;
+    }
+    cudaError_t e = launch_bin_flat(d_src, d_dst, elem_bytes_for(nbits), nchans, nsamp, static_cast<cudaStream_t>(stream));
+    ++g_launches;
+    if (e != cudaSuccess) {
+        set_error(cudaGetErrorString(e));
+        return 1;
+    }
+    return 0;
+}
+
+int aa_b200_dedisperse(int i, int t_processed, const int *inBin, const float *dmshifts, const void *d_input,
+                       long long i_nsamp, size_t d_input_elems, float *d_output, long long out_pitch, int nchans,
+                       const float *tsamp, const float *dm_low, const float *dm_step, const int *ndms, int nbits,
+                       int failsafe, void *stream)
+{
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int eb = elem_bytes_for(nbits);
+    const int nd = ndms[i];
+    if (nd <= 0 || (nd % 4) || t_processed <= 0 || (t_processed & 3) || nchans <= 0) {
+        set_error("ndms must be a positive multiple of 4 and t_processed a positive multiple of 4");
+        return 1;
+    }
+    const float mstartdm = dm_low[i] / *tsamp; // src/aa_dedisperse.cpp:28,37-40
+    const float mdmstep = dm_step[i] / *tsamp;
+    const int kind = select_delay_kind(nbits, dm_step[i], *tsamp, dmshifts[nchans - 1], failsafe);
+    const int nch_used = (kind == KIND_SHARED4 && nchans > 4096) ? 4096 * (nchans / 4096) : nchans;
+    const int nch_pad = (nchans + 3) & ~3;
+    const size_t nent = static_cast<size_t>(nchans) * nd;
+    float *d_shifts = nullptr;
+    int32_t *d_table = nullptr, *d_wmin = nullptr, *d_off = nullptr;
+    int *d_flags = nullptr; // [0] error flags, [1] span, [2] max delay
+    int h[3] = {0, 0, 0};
+    int rc = 1;
+    const int tile_words = 4;
+    int gd = 0;
+    cudaError_t e = cudaMalloc(&d_shifts, sizeof(float) * nchans);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&d_table, nent * sizeof(int32_t));
+    if (e == cudaSuccess)
+        e = cudaMalloc(&d_flags, 3 * sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_shifts, dmshifts, sizeof(float) * nchans, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(d_flags, 0, 3 * sizeof(int), st);
+    if (e == cudaSuccess) {
+        e = launch_delay_table(d_shifts, nchans, nd, kind, FMA_ALL, mstartdm, mdmstep, d_table, d_flags, st);
+        ++g_launches;
+    }
+    // DM group: the largest that fits shared memory
+    for (int cand : {64, 32, 16, 8, 4}) {
+        if (e != cudaSuccess)
+            break;
+        if (nd % cand)
+            continue;
+        cudaFree(d_wmin);
+        d_wmin = nullptr;
+        e = cudaMalloc(&d_wmin, static_cast<size_t>(nd / cand) * nch_pad * sizeof(int32_t));
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(d_flags + 1, 0, 2 * sizeof(int), st);
+        if (e == cudaSuccess) {
+            e = launch_group_windows(d_table, nchans, nd, cand, d_wmin, d_flags + 1, d_flags + 2, st);
+            ++g_launches;
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h, d_flags, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess)
+            break;
+        if (eb == 2 || ddtr_u8_smem_bytes(h[1], cand, tile_words, nchans) <= 227 * 1024) {
+            gd = cand;
+            break;
+        }
+    }
+    if (e == cudaSuccess && gd == 0)
+        set_error("no DM-group size fits the delay span");
+    else if (e == cudaSuccess && h[0] != 0)
+        set_error("delay outside [0, 2^24) or class step > 1");
+    else if (e == cudaSuccess) {
+        const long long tile = 128LL * tile_words;
+        long long need;
+        if (eb == 1)
+            need = static_cast<long long>(nch_used - 1) * i_nsamp + ((t_processed + tile - 1) / tile) * tile + h[2] +
+                   4LL * ddtr_u8_rw(h[1], tile_words) + 64;
+        else
+            need = static_cast<long long>(nch_used - 1) * i_nsamp + t_processed + h[2] + 2;
+        if (need > static_cast<long long>(d_input_elems)) {
+            set_error("d_input needs " + std::to_string(need) + " elements including window padding, has " +
+                      std::to_string(d_input_elems));
+        } else {
+            if (eb == 1) {
+                e = cudaMalloc(&d_off, nent * sizeof(int32_t));
+                if (e == cudaSuccess) {
+                    e = launch_offset_table(d_table, d_wmin, nchans, nd, gd, ddtr_u8_rw(h[1], tile_words), h[1],
+                                            d_off, st);
+                    ++g_launches;
+                }
+            }
+            DdtrLaunch p;
+            p.in = d_input;
+            p.stride = i_nsamp;
+            p.nchans = nchans;
+            p.nch_used = nch_used;
+            p.tp = t_processed;
+            p.ndms = nd;
+            p.table = d_table;
+            p.wmin = d_wmin;
+            p.group_dms = gd;
+            p.span = h[1];
+            p.kind = kind;
+            p.nchans_f = static_cast<float>(nchans);
+            p.bin_f = static_cast<float>(inBin[i]);
+            p.divide_by_bin = (kind == KIND_SHARED4) ? 0 : 1;
+            p.out = d_output;
+            p.out_pitch = out_pitch;
+            p.err = d_flags;
+            if (e == cudaSuccess) {
+                e = (eb == 1) ? launch_ddtr_u8(p, d_off, tile_words, st) : launch_ddtr_u16(p, st);
+                ++g_launches;
+            }
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(h, d_flags, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess)
+                e = cudaStreamSynchronize(st);
+            if (e == cudaSuccess && h[0] == 0)
+                rc = 0;
+            else if (e == cudaSuccess)
+                set_error("device reported an error flag " + std::to_string(h[0]));
+        }
+    }
+    if (e != cudaSuccess)
+        set_error(cudaGetErrorString(e));
+    cudaFree(d_shifts);
+    cudaFree(d_table);
+    cudaFree(d_wmin);
+    cudaFree(d_off);
+    cudaFree(d_flags);
+    return rc;
+}
+
+const char *aa_b200_last_error(void) { return g_last_error.c_str(); }
+
+long long aa_b200_kernel_launches(void) { return g_launches.load(); }
+
+const char *aa_b200_version(void) { return "aa_b200 0.1 (sm_100a)"; }
+
+// ---------------------------------------------------------------------------
+// pipeline extensions
+// ---------------------------------------------------------------------------
+bool aa_b200_pipeline_set_options(void *obj, int stride_mode, int fma_mode, int failsafe, size_t free_memory,
+                                  int tile_words, int group_dms)
+{
+    Api *a = as_api(obj);
+    if (a->pipe)
+        return api_fail(a, "options must be set before the plan is bound");
+    if (stride_mode != STRIDE_REFERENCE && stride_mode != STRIDE_TRUE)
+        return api_fail(a, "stride_mode must be 0 or 1");
+    if (tile_words != 0 && tile_words != 2 && tile_words != 4)
+        return api_fail(a, "tile_words must be 0, 2 or 4");
+    a->popt.stride_mode = stride_mode;
+    a->popt.fma_mode = fma_mode;
+    a->popt.failsafe = failsafe;
+    a->popt.free_memory = free_memory;
+    a->popt.tile_words = tile_words;
+    a->popt.group_dms = group_dms;
+    return true;
+}
+
+void *aa_b200_pipeline_create(aa_py_filterbank_metadata_struct metadata, const unsigned short *input, int device_input,
+                              int device_output, int copy_to_host, void *stream, int card_number)
+{
+    pipeline_components_struct comp{true, false, false, false};
+    pipeline_component_option_struct opt{};
+    opt.copy_ddtr_data_to_host = copy_to_host != 0;
+    Api *a = static_cast<Api *>(aa_py_pipeline_api(comp, opt, metadata, input, card_number));
+    a->popt.device_input = device_input != 0;
+    a->popt.device_output = device_output != 0;
+    a->popt.stream = static_cast<cudaStream_t>(stream);
+    return a;
+}
+
+bool aa_b200_pipeline_run_all(void *obj)
+{
+    Api *a = as_api(obj);
+    if (!a->pipe)
+        return api_fail(a, "no DDTR plan bound");
+    if (!a->pipe->run_all())
+        return api_fail(a, a->pipe->last_error());
+    return true;
+}
+
+bool aa_b200_pipeline_rewind(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? a->pipe->rewind() : api_fail(a, "no DDTR plan bound");
+}
+
+bool aa_b200_pipeline_synchronize(void *obj)
+{
+    Api *a = as_api(obj);
+    if (!a->pipe)
+        return api_fail(a, "no DDTR plan bound");
+    if (!a->pipe->synchronize())
+        return api_fail(a, a->pipe->last_error());
+    return true;
+}
+
+float *aa_b200_pipeline_device_output(void *obj, int range)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? a->pipe->device_output(range) : nullptr;
+}
+
+int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms, int *span, int *tile_words)
+{
+    Api *a = as_api(obj);
+    if (!a->pipe || !a->pipe->setup() || range < 0 || range >= static_cast<int>(a->pipe->strategy().nranges()))
+        return 1;
+    const RangeConfig &rc = a->pipe->range_config(range);
+    *kind = rc.kind;
+    *group_dms = rc.group_dms;
+    *span = rc.span;
+    *tile_words = rc.tile_words;
+    return 0;
+}
+
+long long aa_b200_pipeline_kernel_launches(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? a->pipe->kernel_launches() : 0;
+}
+
+const char *aa_b200_pipeline_last_error(void *obj)
+{
+    Api *a = as_api(obj);
+    if (a->pipe && !a->pipe->last_error().empty())
+        return a->pipe->last_error().c_str();
+    return a->error.c_str();
+}
+
+int aa_b200_pipeline_num_tchunks(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? a->pipe->strategy().num_tchunks() : 0;
+}
+
+bool aa_b200_pipeline_time_kernels(void *obj, int on)
+{
+    Api *a = as_api(obj);
+    if (a->pipe)
+        return a->pipe->set_time_kernels(on != 0);
+    a->popt.time_kernels = on != 0;
+    return true;
+}
+
+int aa_b200_pipeline_kernel_time(void *obj, int family, double *ms, long long *count)
+{
+    Api *a = as_api(obj);
+    if (!a->pipe || family < 0 || family >= KF_COUNT)
+        return 1;
+    *ms = a->pipe->kernel_ms(family);
+    *count = a->pipe->kernel_count(family);
+    return 0;
+}
+
+bool aa_b200_pipeline_reset_kernel_times(void *obj)
+{
+    Api *a = as_api(obj);
+    if (!a->pipe)
+        return false;
+    a->pipe->reset_kernel_times();
+    return true;
+}
+
+int aa_b200_pipeline_maxshift(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->pipe ? a->pipe->strategy().maxshift() : 0;
+}
+
+} // extern "C"

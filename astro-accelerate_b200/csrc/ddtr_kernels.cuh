@@ -1,0 +1,80 @@
+// ddtr_kernels.cuh -- launchers of the sm_100a DDTR kernels (ddtr_kernels.cu).
+//
+// Device data layout (row-major and flat, like the reference's device buffers,
+// so that the reference runner's flat-buffer behaviour replays exactly):
+//   raw chunk    : [t][c]  uint16  (host format, one value per sample)
+//   filterbank   : [c][stride] uint8 (nbits <= 8) or uint16 (nbits 16/32)
+//   delay table  : [c][ndms] int32 = smallest delay | (class mask << 24)
+//   window table : [group][c4] int32 = smallest delay of the DM group
+//   offset table : [c][ndms] int32 = word offset in the staged window or -1
+//   output       : [dm][pitch] float32
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace aab200 {
+
+// Delay semantics of the reference kernel a range is dispatched to
+// (src/aa_dedisperse.cpp:5-163).
+enum DelayKind : int {
+    KIND_SHARED8 = 0,  // shared_dedisperse_kernel: findex = 2tx+1, classes (t%16)/2
+    KIND_SHARED16 = 1, // shared_dedisperse_kernel_16: findex = 2tx, classes (t%16)/2
+    KIND_SHARED4 = 2,  // shared_dedisperse_kernel_4bit: findex = 4tx+3, classes (t%32)/4
+    KIND_CACHE = 3     // cache_dedisperse_kernel: one delay per (c, dm)
+};
+
+enum FmaBits : int { FMA_TWO = 1, FMA_ONE = 2, FMA_CACHE = 4, FMA_ALL = 7 };
+
+// Device error flags (bitwise OR into one int).
+enum DevErr : int {
+    DERR_DELAY_RANGE = 1, // a delay outside [0, 2^24) or a class step > 1
+    DERR_INPUT_RANGE = 2, // a sample above the bit depth's range
+    DERR_WINDOW = 4,      // a delay outside the staged window
+};
+
+struct DdtrLaunch {
+    const void *in;       // filterbank [c][stride]
+    long long stride;     // elements per channel row
+    int nchans;           // channels in the data
+    int nch_used;         // channels summed (4-bit wide-band truncation)
+    int tp;               // outputs per DM row (t_processed)
+    int ndms;             // DM trials in the range
+    const int32_t *table; // [c][ndms]
+    const int32_t *wmin;  // [group][c4]
+    int group_dms;        // DM trials per CTA
+    int span;             // max window span of any (group, channel)
+    int kind;             // DelayKind
+    float nchans_f;       // divisor (reference i_nchans)
+    float bin_f;          // divisor (reference bin)
+    int divide_by_bin;    // 0 for the 4-bit kernel
+    float *out;           // [dm][out_pitch]
+    long long out_pitch;
+    int *err;             // device error flags
+};
+
+cudaError_t launch_delay_table(const float *dmshifts, int nchans, int ndms, int kind, int fma_mode,
+                               float mstartdm, float mdmstep, int32_t *table, int *err, cudaStream_t st);
+cudaError_t launch_group_windows(const int32_t *table, int nchans, int ndms, int group_dms,
+                                 int32_t *wmin, int *span_max, int *delay_max, cudaStream_t st);
+cudaError_t launch_offset_table(const int32_t *table, const int32_t *wmin, int nchans, int ndms,
+                                int group_dms, int rw, int span, int32_t *offtab, cudaStream_t st);
+
+// [t][c] uint16 chunk -> [c][stride] storage type, rows of length nsamp.
+cudaError_t launch_corner_turn(const uint16_t *in_tc, void *out_ct, int elem_bytes, int nchans,
+                               long long nsamp, long long out_stride, int max_value, int *err,
+                               cudaStream_t st);
+
+// Reference x2 binning on the flat buffer (src/aa_bin_gpu.cpp:8-44):
+// dst[0, nchans*nsamp/2) = binned [c][nsamp/2], dst[.., nchans*nsamp) = 0.
+cudaError_t launch_bin_flat(const void *src, void *dst, int elem_bytes, int nchans, long long nsamp,
+                            cudaStream_t st);
+
+// Dedispersion of one (chunk, range).
+cudaError_t launch_ddtr_u8(const DdtrLaunch &p, const int32_t *offtab, int tile_words, cudaStream_t st);
+cudaError_t launch_ddtr_u16(const DdtrLaunch &p, cudaStream_t st);
+
+size_t ddtr_u8_smem_bytes(int span, int group_dms, int tile_words, int nchans);
+int ddtr_u8_rw(int span, int tile_words);
+
+} // namespace aab200

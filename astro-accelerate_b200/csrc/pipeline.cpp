@@ -1,0 +1,641 @@
+// pipeline.cpp -- DDTR runner (see pipeline.hpp).
+#include "pipeline.hpp"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+#include "ddtr_kernels.cuh"
+
+namespace aab200 {
+
+namespace {
+constexpr int kMaxSmemOptin = 227 * 1024;
+}
+
+DdtrPipeline::DdtrPipeline(const FilterbankMetadata &meta, const uint16_t *input, const PipelineOptions &opt)
+    : meta_(meta), input_(input), opt_(opt)
+{
+}
+
+DdtrPipeline::~DdtrPipeline() { cleanup(); }
+
+bool DdtrPipeline::fail(const std::string &msg)
+{
+    if (error_.empty())
+        error_ = msg;
+    return false;
+}
+
+bool DdtrPipeline::check_cuda(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess)
+        return true;
+    return fail(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+bool DdtrPipeline::bind(const DdtrPlan &plan)
+{
+    // include/aa_pipeline_api.hpp:130-174: the strategy is computed on bind
+    // with the device's free memory.
+    bound_ = false;
+    plan_ = plan;
+    size_t free_mem = opt_.free_memory;
+    if (free_mem == 0) {
+        size_t fr = 0, tot = 0;
+        if (!check_cuda(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo"))
+            return false;
+        free_mem = fr;
+    }
+    const StrategyStatus s = strategy_.compute(plan_, meta_, free_mem, false);
+    if (s != STRAT_OK) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "DDTR strategy refused the plan (code %d)", static_cast<int>(s));
+        return fail(buf);
+    }
+    bound_ = true;
+    return true;
+}
+
+bool DdtrPipeline::build_range(int r)
+{
+    RangeConfig &rc = ranges_[r];
+    const DmRange &d = strategy_.dm(r);
+    const int nchans = meta_.nchans;
+    const int ndms = strategy_.ndms(r);
+    const float tsamp_original = static_cast<float>(meta_.tsamp);
+    rc.tsamp = tsamp_original * static_cast<float>(d.inBin); // :778
+    rc.mstartdm = d.low / rc.tsamp;                           // src/aa_dedisperse.cpp:28,37-40
+    rc.mdmstep = d.step / rc.tsamp;
+    rc.kind = select_delay_kind(meta_.nbits, d.step, rc.tsamp, strategy_.dmshifts()[nchans - 1], opt_.failsafe);
+    rc.elem_bytes = elem_bytes_;
+    rc.nch_used = (rc.kind == KIND_SHARED4 && nchans > 4096) ? 4096 * (nchans / 4096) : nchans;
+
+    const size_t nent = static_cast<size_t>(nchans) * ndms;
+    if (!check_cuda(cudaMalloc(&rc.d_table, nent * sizeof(int32_t)), "cudaMalloc(delay table)"))
+        return false;
+    if (!check_cuda(launch_delay_table(d_dmshifts_, nchans, ndms, rc.kind, opt_.fma_mode, rc.mstartdm, rc.mdmstep,
+                                       rc.d_table, d_err_, st_),
+                    "delay table"))
+        return false;
+    ++launches_;
+
+    const int nch_pad = (nchans + 3) & ~3;
+    int *d_mx = nullptr;
+    if (!check_cuda(cudaMalloc(&d_mx, 2 * sizeof(int)), "cudaMalloc"))
+        return false;
+    rc.tile_words = opt_.tile_words > 0 ? opt_.tile_words : 4;
+    int cand[] = {64, 32, 16, 8, 4};
+    bool ok = false;
+    for (int gd : cand) {
+        if (opt_.group_dms > 0 && gd != opt_.group_dms)
+            continue;
+        if (ndms % gd)
+            continue;
+        if (rc.d_wmin) {
+            cudaFree(rc.d_wmin);
+            rc.d_wmin = nullptr;
+        }
+        if (!check_cuda(cudaMalloc(&rc.d_wmin, static_cast<size_t>(ndms / gd) * nch_pad * sizeof(int32_t)),
+                        "cudaMalloc(windows)"))
+            break;
+        int hm[2] = {0, 0};
+        cudaMemsetAsync(d_mx, 0, 2 * sizeof(int), st_);
+        if (!check_cuda(launch_group_windows(rc.d_table, nchans, ndms, gd, rc.d_wmin, d_mx, d_mx + 1, st_),
+                        "group windows"))
+            break;
+        ++launches_;
+        if (!check_cuda(cudaMemcpyAsync(hm, d_mx, 2 * sizeof(int), cudaMemcpyDeviceToHost, st_), "D2H") ||
+            !check_cuda(cudaStreamSynchronize(st_), "sync"))
+            break;
+        rc.span = hm[0];
+        rc.delay_max = hm[1];
+        rc.group_dms = gd;
+        if (elem_bytes_ == 2) {
+            ok = true;
+            break;
+        }
+        const size_t smem = ddtr_u8_smem_bytes(rc.span, gd, rc.tile_words, nchans);
+        if (smem <= static_cast<size_t>(kMaxSmemOptin) && nchans <= 16384) {
+            ok = true;
+            break;
+        }
+    }
+    cudaFree(d_mx);
+    if (!ok)
+        return fail(error_.empty() ? "no DM-group size fits the delay span of range " + std::to_string(r) : error_);
+    if (!check_device_flags())
+        return false;
+    if (elem_bytes_ == 1) {
+        if (!check_cuda(cudaMalloc(&rc.d_offtab, nent * sizeof(int32_t)), "cudaMalloc(offset table)"))
+            return false;
+        if (!check_cuda(launch_offset_table(rc.d_table, rc.d_wmin, nchans, ndms, rc.group_dms,
+                                            ddtr_u8_rw(rc.span, rc.tile_words), rc.span, rc.d_offtab, st_),
+                        "offset table"))
+            return false;
+        ++launches_;
+    }
+    return true;
+}
+
+bool DdtrPipeline::check_device_flags()
+{
+    if (!check_cuda(cudaMemcpyAsync(h_err_, d_err_, sizeof(int), cudaMemcpyDeviceToHost, st_), "D2H flags") ||
+        !check_cuda(cudaStreamSynchronize(st_), "sync"))
+        return false;
+    const int f = *h_err_;
+    if (f == 0)
+        return true;
+    std::string m = "device reported:";
+    if (f & DERR_DELAY_RANGE)
+        m += " delay outside [0, 2^24) or class step > 1;";
+    if (f & DERR_INPUT_RANGE)
+        m += " input sample above the bit depth's range;";
+    if (f & DERR_WINDOW)
+        m += " delay outside the staged window;";
+    return fail(m);
+}
+
+bool DdtrPipeline::timed_launch_begin(int family)
+{
+    if (!opt_.time_kernels)
+        return true;
+    if (kev_used_ == kev_.size()) {
+        // the pool only grows while a run is queued without a synchronize
+        if (kev_.size() >= 4096 && !collect_kernel_times())
+            return false;
+        if (kev_used_ == kev_.size()) {
+            TimedLaunch t;
+            if (!check_cuda(cudaEventCreate(&t.start), "event") || !check_cuda(cudaEventCreate(&t.stop), "event"))
+                return false;
+            kev_.push_back(t);
+        }
+    }
+    kev_[kev_used_].family = family;
+    return check_cuda(cudaEventRecord(kev_[kev_used_].start, st_), "event");
+}
+
+bool DdtrPipeline::timed_launch_end()
+{
+    if (!opt_.time_kernels)
+        return true;
+    const bool ok = check_cuda(cudaEventRecord(kev_[kev_used_].stop, st_), "event");
+    ++kev_used_;
+    return ok;
+}
+
+bool DdtrPipeline::collect_kernel_times()
+{
+    if (kev_used_ == 0)
+        return true;
+    if (!check_cuda(cudaEventSynchronize(kev_[kev_used_ - 1].stop), "event sync"))
+        return false;
+    for (size_t i = 0; i < kev_used_; ++i) {
+        float ms = 0.f;
+        if (!check_cuda(cudaEventElapsedTime(&ms, kev_[i].start, kev_[i].stop), "event time"))
+            return false;
+        kernel_ms_[kev_[i].family] += ms;
+        kernel_n_[kev_[i].family] += 1;
+    }
+    kev_used_ = 0;
+    return true;
+}
+
+void DdtrPipeline::reset_kernel_times()
+{
+    collect_kernel_times();
+    for (int f = 0; f < KF_COUNT; ++f) {
+        kernel_ms_[f] = 0.0;
+        kernel_n_[f] = 0;
+    }
+}
+
+bool DdtrPipeline::setup()
+{
+    if (setup_done_)
+        return true;
+    if (!bound_)
+        return fail("no DDTR plan bound");
+    const int nchans = meta_.nchans;
+    const int nr = static_cast<int>(strategy_.nranges());
+    if (meta_.nbits != 1 && meta_.nbits != 2 && meta_.nbits != 4 && meta_.nbits != 8 && meta_.nbits != 16 &&
+        meta_.nbits != 32)
+        return fail("unsupported nbits");
+    elem_bytes_ = (meta_.nbits <= 8) ? 1 : 2;
+    for (int r = 0; r < nr; ++r) {
+        const int b = strategy_.dm(r).inBin;
+        if (b < 1 || (b & (b - 1)))
+            return fail("inBin must be a power of two");
+    }
+    if (opt_.stride_mode == STRIDE_REFERENCE && strategy_.dm(0).inBin > 1)
+        return fail("the first DM range must have inBin 1 (the reference runner reads t_processed[-1] otherwise)");
+    for (float v : strategy_.dmshifts())
+        if (!(v >= 0.f))
+            return fail("negative dispersion delays (foff > 0) are not supported");
+
+    if (opt_.stream) {
+        st_ = opt_.stream;
+    } else {
+        if (!check_cuda(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "stream"))
+            return false;
+        own_stream_ = true;
+    }
+    if (!check_cuda(cudaStreamCreateWithFlags(&st_h2d_, cudaStreamNonBlocking), "stream") ||
+        !check_cuda(cudaStreamCreateWithFlags(&st_d2h_, cudaStreamNonBlocking), "stream"))
+        return false;
+    for (int i = 0; i < 2; ++i) {
+        if (!check_cuda(cudaEventCreateWithFlags(&ev_tile_free_[i], cudaEventDisableTiming), "event") ||
+            !check_cuda(cudaEventCreateWithFlags(&ev_tile_done_[i], cudaEventDisableTiming), "event") ||
+            !check_cuda(cudaEventCreateWithFlags(&ev_raw_ready_[i], cudaEventDisableTiming), "event") ||
+            !check_cuda(cudaEventCreateWithFlags(&ev_raw_free_[i], cudaEventDisableTiming), "event"))
+            return false;
+    }
+    if (!check_cuda(cudaMalloc(&d_err_, sizeof(int)), "cudaMalloc") ||
+        !check_cuda(cudaMemsetAsync(d_err_, 0, sizeof(int), st_), "memset") ||
+        !check_cuda(cudaMallocHost(&h_err_, sizeof(int)), "cudaMallocHost"))
+        return false;
+    if (!check_cuda(cudaMalloc(&d_dmshifts_, sizeof(float) * nchans), "cudaMalloc") ||
+        !check_cuda(cudaMemcpyAsync(d_dmshifts_, strategy_.dmshifts().data(), sizeof(float) * nchans,
+                                    cudaMemcpyHostToDevice, st_),
+                    "H2D dmshifts"))
+        return false;
+
+    ranges_.assign(nr, RangeConfig());
+    int span_max = 0, delay_max = 0, rawb_max = 0;
+    for (int r = 0; r < nr; ++r) {
+        if (!build_range(r))
+            return false;
+        span_max = std::max(span_max, ranges_[r].span);
+        delay_max = std::max(delay_max, ranges_[r].delay_max);
+        rawb_max = std::max(rawb_max, 4 * ddtr_u8_rw(ranges_[r].span, ranges_[r].tile_words) + 32);
+    }
+
+    const long long L0 = static_cast<long long>(strategy_.t_processed()[0][0]) + strategy_.maxshift();
+    const long long pad = 4LL * (512 + span_max + delay_max) + rawb_max + 65536;
+    flat_elems_ = static_cast<size_t>(nchans) * static_cast<size_t>(L0) + static_cast<size_t>(pad);
+    for (int i = 0; i < 2; ++i) {
+        if (!check_cuda(cudaMalloc(&d_flat_[i], flat_elems_ * elem_bytes_), "cudaMalloc(filterbank)") ||
+            !check_cuda(cudaMemsetAsync(d_flat_[i], 0, flat_elems_ * elem_bytes_, st_), "memset"))
+            return false;
+    }
+    if (!opt_.device_input) {
+        for (int i = 0; i < 2; ++i)
+            if (!check_cuda(cudaMalloc(&d_raw_[i], static_cast<size_t>(L0) * nchans * sizeof(uint16_t)),
+                            "cudaMalloc(raw chunk)"))
+                return false;
+    }
+
+    // outputs
+    if (opt_.device_output) {
+        d_out_full_.assign(nr, nullptr);
+        for (int r = 0; r < nr; ++r) {
+            const size_t n = static_cast<size_t>(strategy_.ndms(r)) * static_cast<size_t>(strategy_.total_samps(r));
+            if (!check_cuda(cudaMalloc(&d_out_full_[r], std::max<size_t>(n, 1) * sizeof(float)),
+                            "cudaMalloc(output)"))
+                return false;
+        }
+    } else {
+        tile_elems_ = 1;
+        for (int r = 0; r < nr; ++r)
+            for (int k = 0; k < strategy_.num_tchunks(); ++k)
+                tile_elems_ = std::max(tile_elems_, static_cast<size_t>(strategy_.ndms(r)) *
+                                                        static_cast<size_t>(strategy_.t_processed()[r][k]));
+        for (int i = 0; i < 2; ++i)
+            if (!check_cuda(cudaMalloc(&d_tile_[i], tile_elems_ * sizeof(float)), "cudaMalloc(output tile)"))
+                return false;
+    }
+    if (opt_.copy_to_host) {
+        // include/aa_permitted_pipelines_generic.hpp:418-445: float***
+        // [range][dm][sum_k t_processed]; here all rows live in one pinned block.
+        size_t total = 0;
+        for (int r = 0; r < nr; ++r)
+            total += static_cast<size_t>(strategy_.ndms(r)) * static_cast<size_t>(strategy_.total_samps(r));
+        if (!check_cuda(cudaMallocHost(&h_block_, std::max<size_t>(total, 1) * sizeof(float)),
+                        "cudaMallocHost(output)"))
+            return false;
+        host_row_ptrs_.assign(nr, std::vector<float *>());
+        host_rows_.assign(nr, nullptr);
+        size_t off = 0;
+        for (int r = 0; r < nr; ++r) {
+            const size_t tot = static_cast<size_t>(strategy_.total_samps(r));
+            host_row_ptrs_[r].resize(strategy_.ndms(r));
+            for (int dm = 0; dm < strategy_.ndms(r); ++dm)
+                host_row_ptrs_[r][dm] = h_block_ + off + static_cast<size_t>(dm) * tot;
+            host_rows_[r] = host_row_ptrs_[r].data();
+            off += tot * static_cast<size_t>(strategy_.ndms(r));
+        }
+    }
+    for (int i = 0; i < 2; ++i) {
+        cudaEventRecord(ev_tile_free_[i], st_d2h_);
+        cudaEventRecord(ev_raw_free_[i], st_);
+    }
+    if (!check_device_flags())
+        return false;
+    setup_done_ = true;
+    rewind();
+    return true;
+}
+
+bool DdtrPipeline::rewind()
+{
+    cur_chunk_ = 0;
+    cur_range_ = 0;
+    inc_ = 0;
+    old_bin_ = 1;
+    finished_component_sent_ = false;
+    return true;
+}
+
+bool DdtrPipeline::do_chunk_start()
+{
+    const int nchans = meta_.nchans;
+    const int k = cur_chunk_;
+    const long long L = static_cast<long long>(strategy_.t_processed()[0][k]) + strategy_.maxshift();
+    if (inc_ + L > meta_.nsamples)
+        return fail("chunk extends past the end of the input");
+    if (static_cast<size_t>(nchans) * static_cast<size_t>(L) > flat_elems_)
+        return fail("chunk larger than the filterbank buffer");
+    const uint16_t *src;
+    const int slot = k & 1;
+    if (opt_.device_input) {
+        src = input_ + static_cast<size_t>(inc_) * nchans;
+    } else {
+        // issue this chunk's copy if it was not prefetched, and prefetch the next
+        auto issue = [&](int kk, long long inc_kk) -> bool {
+            const long long Lk = static_cast<long long>(strategy_.t_processed()[0][kk]) + strategy_.maxshift();
+            const int s = kk & 1;
+            if (!check_cuda(cudaStreamWaitEvent(st_h2d_, ev_raw_free_[s], 0), "wait"))
+                return false;
+            if (!check_cuda(cudaMemcpyAsync(d_raw_[s], input_ + static_cast<size_t>(inc_kk) * nchans,
+                                            static_cast<size_t>(Lk) * nchans * sizeof(uint16_t),
+                                            cudaMemcpyHostToDevice, st_h2d_),
+                            "H2D chunk"))
+                return false;
+            return check_cuda(cudaEventRecord(ev_raw_ready_[s], st_h2d_), "event");
+        };
+        if (k == 0 && !issue(0, 0))
+            return false;
+        if (k + 1 < strategy_.num_tchunks()) {
+            const long long inc_next = inc_ + strategy_.t_processed()[0][k];
+            if (!issue(k + 1, inc_next))
+                return false;
+        }
+        if (!check_cuda(cudaStreamWaitEvent(st_, ev_raw_ready_[slot], 0), "wait"))
+            return false;
+        src = d_raw_[slot];
+    }
+    const int max_value = (meta_.nbits == 4) ? 15 : (meta_.nbits <= 8 ? 255 : 65535);
+    cur_flat_ = 0;
+    if (!timed_launch_begin(KF_CORNER_TURN) ||
+        !check_cuda(launch_corner_turn(src, d_flat_[0], elem_bytes_, nchans, L, L, max_value, d_err_, st_),
+                    "corner turn") ||
+        !timed_launch_end())
+        return false;
+    ++launches_;
+    if (!opt_.device_input && !check_cuda(cudaEventRecord(ev_raw_free_[slot], st_), "event"))
+        return false;
+    old_bin_ = 1;
+    cur_stride_ = L;
+    cur_bin_ = 1;
+    return true;
+}
+
+bool DdtrPipeline::do_range()
+{
+    const int nchans = meta_.nchans;
+    const int r = cur_range_, k = cur_chunk_;
+    const RangeConfig &rc = ranges_[r];
+    const DmRange &d = strategy_.dm(r);
+    const int tp = strategy_.t_processed()[r][k];
+    const int ms_r = strategy_.maxshift() / d.inBin; // :782
+    long long i_nsamp;
+
+    auto bin_once = [&](long long nsb) -> bool {
+        if (nsb <= 0 || (nsb & 1))
+            return fail("binning length must be positive and even");
+        if (static_cast<size_t>(nchans) * static_cast<size_t>(nsb) > flat_elems_)
+            return fail("binning length exceeds the filterbank buffer");
+        if (!timed_launch_begin(KF_BIN) ||
+            !check_cuda(launch_bin_flat(d_flat_[cur_flat_], d_flat_[cur_flat_ ^ 1], elem_bytes_, nchans, nsb, st_),
+                        "binning") ||
+            !timed_launch_end())
+            return false;
+        ++launches_;
+        cur_flat_ ^= 1;
+        return true;
+    };
+
+    if (opt_.stride_mode == STRIDE_REFERENCE) {
+        if (d.inBin > old_bin_) {
+            const long long nsb = static_cast<long long>(strategy_.t_processed()[r - 1][k]) +
+                                  static_cast<long long>(ms_r) * d.inBin; // :797-798
+            if (!bin_once(nsb))
+                return false;
+        }
+        i_nsamp = static_cast<long long>(tp) + ms_r; // :786
+    } else {
+        while (cur_bin_ < d.inBin) {
+            if (!bin_once(cur_stride_))
+                return false;
+            cur_stride_ /= 2;
+            cur_bin_ *= 2;
+        }
+        i_nsamp = cur_stride_;
+    }
+
+    const int tile = 128 * rc.tile_words;
+    long long need;
+    if (elem_bytes_ == 1)
+        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ((tp + tile - 1) / tile) * static_cast<long long>(tile) +
+               rc.delay_max + 4LL * ddtr_u8_rw(rc.span, rc.tile_words) + 64;
+    else
+        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + tp + rc.delay_max + 2;
+    if (need > static_cast<long long>(flat_elems_))
+        return fail("dedispersion window exceeds the filterbank buffer");
+
+    DdtrLaunch p;
+    p.in = d_flat_[cur_flat_];
+    p.stride = i_nsamp;
+    p.nchans = nchans;
+    p.nch_used = rc.nch_used;
+    p.tp = tp;
+    p.ndms = strategy_.ndms(r);
+    p.table = rc.d_table;
+    p.wmin = rc.d_wmin;
+    p.group_dms = rc.group_dms;
+    p.span = rc.span;
+    p.kind = rc.kind;
+    p.nchans_f = static_cast<float>(nchans);
+    p.bin_f = static_cast<float>(d.inBin);
+    p.divide_by_bin = (rc.kind == KIND_SHARED4) ? 0 : 1;
+    p.err = d_err_;
+    const long long host_off = inc_ / d.inBin; // src/aa_device_save_data.cu:41
+    const int slot = tile_slot_;
+    if (opt_.device_output) {
+        p.out = d_out_full_[r] + host_off;
+        p.out_pitch = strategy_.total_samps(r);
+    } else {
+        if (!check_cuda(cudaStreamWaitEvent(st_, ev_tile_free_[slot], 0), "wait"))
+            return false;
+        p.out = d_tile_[slot];
+        p.out_pitch = tp;
+    }
+    if ((reinterpret_cast<uintptr_t>(p.out) & 15) || (p.out_pitch & 3) || (tp & 3))
+        return fail("output rows are not 16-byte aligned");
+    if (!timed_launch_begin(KF_DDTR))
+        return false;
+    cudaError_t e = (elem_bytes_ == 1) ? launch_ddtr_u8(p, rc.d_offtab, rc.tile_words, st_) : launch_ddtr_u16(p, st_);
+    if (!check_cuda(e, "dedispersion") || !timed_launch_end())
+        return false;
+    ++launches_;
+
+    if (opt_.copy_to_host) {
+        // src/aa_device_save_data.cu:19-62: row dm of this chunk lands at
+        // output_buffer[r][dm] + inc/inBin.
+        if (!check_cuda(cudaEventRecord(ev_tile_done_[slot], st_), "event") ||
+            !check_cuda(cudaStreamWaitEvent(st_d2h_, ev_tile_done_[slot], 0), "wait"))
+            return false;
+        const size_t tot = static_cast<size_t>(strategy_.total_samps(r));
+        if (!check_cuda(cudaMemcpy2DAsync(host_rows_[r][0] + host_off, tot * sizeof(float), p.out,
+                                          static_cast<size_t>(p.out_pitch) * sizeof(float), static_cast<size_t>(tp) * sizeof(float),
+                                          static_cast<size_t>(p.ndms), cudaMemcpyDeviceToHost, st_d2h_),
+                        "D2H output"))
+            return false;
+        if (!opt_.device_output && !check_cuda(cudaEventRecord(ev_tile_free_[slot], st_d2h_), "event"))
+            return false;
+    }
+    if (!opt_.device_output)
+        tile_slot_ ^= 1;
+    old_bin_ = d.inBin;
+    return true;
+}
+
+bool DdtrPipeline::step(bool /*allow_sync*/)
+{
+    if (cur_range_ == 0 && !do_chunk_start())
+        return false;
+    if (!do_range())
+        return false;
+    ++cur_range_;
+    if (cur_range_ >= static_cast<int>(strategy_.nranges())) {
+        inc_ += strategy_.t_processed()[0][cur_chunk_]; // :898
+        ++cur_chunk_;
+        cur_range_ = 0;
+    }
+    return true;
+}
+
+bool DdtrPipeline::synchronize()
+{
+    if (!check_cuda(cudaStreamSynchronize(st_), "sync") || !check_cuda(cudaStreamSynchronize(st_d2h_), "sync") ||
+        !check_cuda(cudaStreamSynchronize(st_h2d_), "sync"))
+        return false;
+    if (!collect_kernel_times())
+        return false;
+    return check_device_flags();
+}
+
+bool DdtrPipeline::next(RunStatus &status)
+{
+    if (!error_.empty() || !setup()) {
+        status = RunStatus::error;
+        return false;
+    }
+    if (cur_chunk_ >= strategy_.num_tchunks()) {
+        if (!finished_component_sent_) {
+            finished_component_sent_ = true;
+            if (!synchronize()) {
+                status = RunStatus::error;
+                return false;
+            }
+            status = RunStatus::finished_component;
+            return true;
+        }
+        status = RunStatus::finished;
+        return false;
+    }
+    if (!step(false)) {
+        status = RunStatus::error;
+        return false;
+    }
+    status = RunStatus::has_more;
+    return true;
+}
+
+bool DdtrPipeline::run_all()
+{
+    if (!error_.empty() || !setup())
+        return false;
+    while (cur_chunk_ < strategy_.num_tchunks())
+        if (!step(false))
+            return false;
+    finished_component_sent_ = true;
+    return true;
+}
+
+bool DdtrPipeline::cleanup()
+{
+    if (st_)
+        cudaStreamSynchronize(st_);
+    if (st_d2h_)
+        cudaStreamSynchronize(st_d2h_);
+    if (st_h2d_)
+        cudaStreamSynchronize(st_h2d_);
+    for (RangeConfig &rc : ranges_) {
+        cudaFree(rc.d_table);
+        cudaFree(rc.d_wmin);
+        cudaFree(rc.d_offtab);
+        rc.d_table = rc.d_wmin = rc.d_offtab = nullptr;
+    }
+    ranges_.clear();
+    for (int i = 0; i < 2; ++i) {
+        cudaFree(d_flat_[i]);
+        cudaFree(d_raw_[i]);
+        cudaFree(d_tile_[i]);
+        d_flat_[i] = nullptr;
+        d_raw_[i] = nullptr;
+        d_tile_[i] = nullptr;
+        if (ev_tile_free_[i])
+            cudaEventDestroy(ev_tile_free_[i]);
+        if (ev_tile_done_[i])
+            cudaEventDestroy(ev_tile_done_[i]);
+        if (ev_raw_ready_[i])
+            cudaEventDestroy(ev_raw_ready_[i]);
+        if (ev_raw_free_[i])
+            cudaEventDestroy(ev_raw_free_[i]);
+        ev_tile_free_[i] = ev_tile_done_[i] = ev_raw_ready_[i] = ev_raw_free_[i] = nullptr;
+    }
+    for (TimedLaunch &t : kev_) {
+        cudaEventDestroy(t.start);
+        cudaEventDestroy(t.stop);
+    }
+    kev_.clear();
+    kev_used_ = 0;
+    for (float *p : d_out_full_)
+        cudaFree(p);
+    d_out_full_.clear();
+    cudaFree(d_dmshifts_);
+    d_dmshifts_ = nullptr;
+    cudaFree(d_err_);
+    d_err_ = nullptr;
+    if (h_err_)
+        cudaFreeHost(h_err_);
+    h_err_ = nullptr;
+    if (h_block_)
+        cudaFreeHost(h_block_);
+    h_block_ = nullptr;
+    host_rows_.clear();
+    host_row_ptrs_.clear();
+    if (st_h2d_)
+        cudaStreamDestroy(st_h2d_);
+    if (st_d2h_)
+        cudaStreamDestroy(st_d2h_);
+    if (own_stream_ && st_)
+        cudaStreamDestroy(st_);
+    st_ = st_h2d_ = st_d2h_ = nullptr;
+    own_stream_ = false;
+    setup_done_ = false;
+    return true;
+}
+
+} // namespace aab200

@@ -1,0 +1,178 @@
+// pipeline.hpp -- the DDTR runner behind the aa_pipeline_api surface.
+//
+// Mirrors the dedispersion part of the reference's generic runner
+// (include/aa_permitted_pipelines_generic.hpp:606-914): one call of next()
+// processes one (time chunk, DM range) step in the reference's order --
+// chunk load and corner turn on the first range of a chunk, a single x2
+// binning whenever inBin grows, dedispersion, copy into the host output
+// rows at inc/inBin -- and reports has_more / finished_component / finished
+// / error like aa_pipeline_runner::status (include/aa_pipeline_runner.hpp:25-30).
+//
+// B200 specifics: the input is corner-turned and narrowed to one byte per
+// sample for nbits <= 8, every delay of a range is evaluated once into a
+// device table when the pipeline is set up, host<->device copies run on their
+// own streams against double buffers, and run_all() issues the whole job
+// without host synchronisation between steps.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "planner.hpp"
+
+namespace aab200 {
+
+enum class RunStatus : int { error = -1, finished = 0, has_more = 1, finished_component = 2 };
+
+enum StrideMode : int {
+    STRIDE_REFERENCE = 0, // binning length exactly as the reference runner passes it (:797-798)
+    STRIDE_TRUE = 1       // binning on the true row stride, repeated to reach inBin
+};
+
+struct PipelineOptions {
+    bool copy_to_host = true;   // aa_pipeline::component_option::copy_ddtr_data_to_host
+    int stride_mode = STRIDE_REFERENCE;
+    int fma_mode = 7;           // which contractible delay expressions are fused
+    int failsafe = 0;           // force the cache-kernel delay semantics
+    size_t free_memory = 0;     // 0: query the device like aa_device_info::free_memory()
+    int tile_words = 0;         // 0: autotune
+    int group_dms = 0;          // 0: autotune
+    bool device_input = false;  // the input pointer is device memory ([t][c] uint16)
+    bool device_output = false; // keep the whole output on the device ([range][dm][t])
+    bool time_kernels = false;  // CUDA events around every kernel launch
+    cudaStream_t stream = nullptr;
+};
+
+// Kernel families timed when PipelineOptions::time_kernels is set.
+enum KernelFamily : int { KF_DDTR = 0, KF_CORNER_TURN = 1, KF_BIN = 2, KF_COUNT = 3 };
+
+struct RangeConfig {
+    int kind = 0;
+    int elem_bytes = 1;
+    int group_dms = 64;
+    int tile_words = 4;
+    int span = 0;
+    int delay_max = 0;
+    int nch_used = 0;
+    float mstartdm = 0.f;
+    float mdmstep = 0.f;
+    float tsamp = 0.f;
+    int32_t *d_table = nullptr;
+    int32_t *d_wmin = nullptr;
+    int32_t *d_offtab = nullptr;
+};
+
+class DdtrPipeline {
+public:
+    DdtrPipeline(const FilterbankMetadata &meta, const uint16_t *input, const PipelineOptions &opt);
+    ~DdtrPipeline();
+    DdtrPipeline(const DdtrPipeline &) = delete;
+    DdtrPipeline &operator=(const DdtrPipeline &) = delete;
+
+    bool bind(const DdtrPlan &plan);
+    bool ready() const { return bound_; }
+    bool setup();                       // allocates and builds the delay tables (idempotent)
+    bool next(RunStatus &status);       // one (chunk, range) step
+    bool run_all();                     // the whole job, no host sync between steps
+    bool rewind();                      // start again from the first chunk, same buffers
+    bool synchronize();
+
+    const DdtrStrategy &strategy() const { return strategy_; }
+    float ***output_buffer() { return host_rows_.empty() ? nullptr : host_rows_.data(); }
+    float *device_output(int range) const
+    {
+        return (range >= 0 && range < static_cast<int>(d_out_full_.size())) ? d_out_full_[range] : nullptr;
+    }
+    int current_range() const { return cur_range_; }
+    int current_tchunk() const { return cur_chunk_; }
+    long long current_inc() const { return inc_; }
+    const RangeConfig &range_config(int r) const { return ranges_[r]; }
+    const std::string &last_error() const { return error_; }
+    long long kernel_launches() const { return launches_; }
+    // Device time (ms) and launch count of one kernel family since the last
+    // reset, collected at synchronize().
+    double kernel_ms(int family) const { return (family >= 0 && family < KF_COUNT) ? kernel_ms_[family] : 0.0; }
+    long long kernel_count(int family) const { return (family >= 0 && family < KF_COUNT) ? kernel_n_[family] : 0; }
+    void reset_kernel_times();
+    bool set_time_kernels(bool on)
+    {
+        opt_.time_kernels = on;
+        return true;
+    }
+    bool cleanup();
+
+private:
+    bool fail(const std::string &msg);
+    bool check_cuda(cudaError_t e, const char *what);
+    bool check_device_flags();
+    bool build_range(int r);
+    bool step(bool allow_sync);
+    bool do_chunk_start();
+    bool do_range();
+    size_t buffer_elems() const { return flat_elems_; }
+    bool timed_launch_begin(int family);
+    bool timed_launch_end();
+    bool collect_kernel_times();
+
+    FilterbankMetadata meta_;
+    const uint16_t *input_;
+    PipelineOptions opt_;
+    DdtrPlan plan_;
+    DdtrStrategy strategy_;
+    bool bound_ = false;
+    bool setup_done_ = false;
+    bool finished_component_sent_ = false;
+    std::string error_;
+
+    // device state
+    int device_ = 0;
+    cudaStream_t st_ = nullptr;       // compute stream
+    cudaStream_t st_h2d_ = nullptr;
+    cudaStream_t st_d2h_ = nullptr;
+    bool own_stream_ = false;
+    int elem_bytes_ = 1;
+    size_t flat_elems_ = 0;           // elements per flat buffer incl. padding
+    void *d_flat_[2] = {nullptr, nullptr};
+    uint16_t *d_raw_[2] = {nullptr, nullptr};
+    float *d_dmshifts_ = nullptr;
+    int *d_err_ = nullptr;
+    int *h_err_ = nullptr;            // pinned
+    std::vector<RangeConfig> ranges_;
+    std::vector<float *> d_out_full_; // device_output mode: [range] -> [ndms][total]
+    float *d_tile_[2] = {nullptr, nullptr}; // copy_to_host mode: per-(chunk,range) output
+    size_t tile_elems_ = 0;
+    cudaEvent_t ev_tile_free_[2] = {nullptr, nullptr};
+    cudaEvent_t ev_tile_done_[2] = {nullptr, nullptr};
+    cudaEvent_t ev_raw_ready_[2] = {nullptr, nullptr};
+    cudaEvent_t ev_raw_free_[2] = {nullptr, nullptr};
+
+    // host output: rows of one pinned block, like float*** [range][dm][t]
+    float *h_block_ = nullptr;
+    std::vector<float **> host_rows_;
+    std::vector<std::vector<float *>> host_row_ptrs_;
+
+    // iteration state (reference :1053-1054 current_time_chunk/current_range)
+    int cur_chunk_ = 0;
+    int cur_range_ = 0;
+    long long inc_ = 0;
+    int old_bin_ = 1;
+    int cur_flat_ = 0;
+    long long cur_stride_ = 0;
+    int cur_bin_ = 1;
+    int tile_slot_ = 0;
+    long long launches_ = 0;
+
+    struct TimedLaunch {
+        cudaEvent_t start = nullptr, stop = nullptr;
+        int family = 0;
+    };
+    std::vector<TimedLaunch> kev_;
+    size_t kev_used_ = 0;
+    double kernel_ms_[KF_COUNT] = {0.0, 0.0, 0.0};
+    long long kernel_n_[KF_COUNT] = {0, 0, 0};
+};
+
+} // namespace aab200

@@ -1,0 +1,399 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 dedispersion (DDTR) path.
+
+One "step" is one full DDTR pass -- every time chunk and DM range of the
+strategy -- over one synthetic filterbank of the survey-scale configuration:
+4096 channels, 8-bit, fch1 1670 MHz, foff -0.0732421875 MHz, tsamp 64 us,
+2^21 samples, the 8-range plan 0-150/0.1/1 ... 2000-3000/2.0/8, seeded
+Gaussian noise N(127.5, 16) plus 8 dispersed boxcar pulses (DM U[50, 2900],
+width log-U[0.25, 8] ms, 3-10 sigma).
+
+  value  DM-trial.samples/s with the input resident in HBM ([t][c] uint16) and
+         the output kept in HBM; corner turn, binning and dedispersion of all
+         chunks and ranges are timed with CUDA events on the library's stream.
+  e2e    the same metric through the reference-facing C ABI
+         (aa_py_pipeline_api / run loop) from a pinned host input to the
+         pinned host float*** output, host<->device copies inside the timed
+         region (wall clock between device synchronisations).
+
+`--impl reference` times the reference path's CPU restatement (the oracle;
+the reference ships no CPU DDTR) on the box's host cores on a bounded sample
+of the same workload.  Under torchrun every rank runs its own beam (weak
+scaling, no collective on the data path); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "astro-accelerate_b200"))
+
+SURVEY = dict(nchans=4096, nbits=8, fch1=1670.0, foff=-0.0732421875, tsamp=64e-6, nsamp=1 << 21,
+              plan=[(0, 150, 0.1, 1, 1), (150, 300, 0.2, 1, 1), (300, 500, 0.25, 1, 1), (500, 900, 0.4, 2, 1),
+                    (900, 1200, 0.6, 4, 1), (1200, 1500, 0.8, 4, 1), (1500, 2000, 1.0, 4, 1),
+                    (2000, 3000, 2.0, 8, 1)],
+              npulses=8, seed=20)
+MID = dict(SURVEY, nsamp=1 << 18)
+SMALL = dict(nchans=1024, nbits=8, fch1=1550.0, foff=-0.390625, tsamp=64e-6, nsamp=1 << 18,
+             plan=[(0, 500, 0.5, 1, 1)], npulses=1, seed=1)
+METRIC = "DM-trial*samples/s (plain DDTR, 1 beam per GPU, bit-exact)"
+PUBLISHED_REALTIME = 6.28  # reference wiki, 8-range "b2" plan, unnamed GPU
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="survey", choices=["survey", "mid", "small"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--tile-words", type=int, default=0)
+    ap.add_argument("--group-dms", type=int, default=0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def synth_input_device(cfg, seed, device):
+    """[nsamp][nchans] uint16 (bit pattern in an int16 tensor) on the GPU."""
+    import numpy as np
+    import torch
+    nchans, nsamp = cfg["nchans"], cfg["nsamp"]
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    x = torch.empty((nsamp, nchans), dtype=torch.int16, device=device)
+    rows = 1 << 16
+    for t0 in range(0, nsamp, rows):
+        n = min(rows, nsamp - t0)
+        v = torch.randn((n, nchans), generator=g, device=device) * 16.0 + 127.5
+        x[t0:t0 + n] = v.round_().clamp_(0, 255).to(torch.int16)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    f = cfg["fch1"] + cfg["foff"] * np.arange(nchans, dtype=np.float64)
+    pulses = []
+    for _ in range(cfg["npulses"]):
+        dm = float(rng.uniform(50, 2900)) if len(cfg["plan"]) > 1 else 300.0
+        width = max(1, int(round(math.exp(rng.uniform(math.log(0.25), math.log(8.0))) * 1e-3 / cfg["tsamp"])))
+        amp = float(rng.uniform(3, 10)) * 16.0
+        start = int(rng.integers(0, nsamp // 2))
+        d = np.floor(4.148808e3 * dm * (f ** -2 - cfg["fch1"] ** -2) / cfg["tsamp"]).astype(np.int64)
+        tt = (start + d[None, :] + np.arange(width)[:, None])
+        cc = np.broadcast_to(np.arange(nchans)[None, :], tt.shape)
+        ok = tt < nsamp
+        ti = torch.as_tensor(tt[ok], device=device)
+        ci = torch.as_tensor(cc[ok], device=device)
+        vals = (x[ti, ci].to(torch.float32) + amp).clamp_(0, 255).to(torch.int16)
+        x[ti, ci] = vals
+        pulses.append(dict(dm=dm, width=width, amp_sigma=amp / 16.0, start=start))
+    torch.cuda.synchronize(device)
+    return x, pulses
+
+
+def metadata_struct(aa, cfg):
+    return aa.filterbank_metadata_struct(0.0, cfg["tsamp"], cfg["fch1"], cfg["foff"], cfg["nbits"], cfg["nsamp"],
+                                         cfg["nchans"], 0.0)
+
+
+def units_per_step(strat):
+    return sum(strat["ndms"][r] * sum(strat["t_processed"][r]) for r in range(len(strat["ndms"])))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[4 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(cfg, x_host_tc, strat, seconds):
+    """The oracle on a bounded sample: range 0, 64-trial DM blocks over a
+    131040-sample window of chunk 0, repeated over DM blocks until `seconds`
+    of CPU work.  Returns (DM-trial.samples/s, threads, description)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    nch = cfg["nchans"]
+    tp = min(131040, strat["t_processed"][0][0])
+    L = tp + strat["maxshift"]
+    flat = O.corner_turn(np.ascontiguousarray(x_host_tc[:L]), nch, L)
+    d = strat["dm"][0]
+    tsr = np.float32(cfg["tsamp"]) * np.float32(d[3])
+    kind = O.select_kernel(cfg["nbits"], d[2], tsr, strat["dmshifts"][-1])
+    m0 = np.float32(np.float32(d[0]) / tsr)
+    ms = np.float32(np.float32(d[2]) / tsr)
+    done, t_total, blocks = 0, 0.0, 0
+    while t_total < seconds and blocks * 64 < strat["ndms"][0]:
+        start = np.float32(m0 + np.float32(blocks * 64) * ms)
+        t0 = time.perf_counter()
+        O.dedisperse(kind, O.FMA_ALL, flat, L, nch, tp, 64, strat["dmshifts"], start, ms, d[3])
+        t_total += time.perf_counter() - t0
+        done += 64 * tp
+        blocks += 1
+    return done / t_total, O.num_threads(), (f"oracle on {blocks} x 64 DM trials of range 0 over {tp} samples of "
+                                             f"chunk 0 ({nch} channels), {t_total:.1f} s")
+
+
+# ---------------------------------------------------------------------------
+def run_reference_arm(args, cfg, rank, world):
+    import numpy as np
+    import aa_b200 as aa
+    strat = aa.strategy(cfg["plan"], cfg["nchans"], cfg["nsamp"], cfg["fch1"], cfg["foff"], cfg["tsamp"],
+                        cfg["nbits"])
+    if rank != 0:
+        return 0
+    rng = np.random.Generator(np.random.PCG64(cfg["seed"]))
+    L = min(131040, strat["t_processed"][0][0]) + strat["maxshift"]
+    x = np.clip(np.rint(rng.normal(127.5, 16.0, size=(L, cfg["nchans"]))), 0, 255).astype(np.uint16)
+    per_step = max(2.0, 30.0 / max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        cpu_baseline(cfg, x, strat, 0.5)
+    vals = []
+    desc, threads = "", 1
+    for _ in range(args.steps):
+        v, threads, desc = cpu_baseline(cfg, x, strat, per_step)
+        vals.append(v)
+    value = statistics.median(vals)
+    line = {"metric": METRIC, "value": value, "unit": "DM-trial*samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": units_per_step(strat) / value * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": workload_config(cfg), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "DM-trial*samples/s", "cores": threads, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": value, "unit": "DM-trial*samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(cfg):
+    name = "survey-scale plain DDTR" if cfg is SURVEY else "reduced plain DDTR"
+    return {"workload": f"{name}: {cfg['nchans']} ch x {cfg['nsamp']} samples, {cfg['nbits']}-bit, "
+                        f"{len(cfg['plan'])}-range plan to DM {cfg['plan'][-1][1]}",
+            "nchans": cfg["nchans"], "nsamp": cfg["nsamp"], "nbits": cfg["nbits"], "tsamp": cfg["tsamp"],
+            "plan": [list(p) for p in cfg["plan"]], "l2_policy": "inputs larger than L2 (17 GB per step)",
+            "parallelism": "one beam per GPU"}
+
+
+def main():
+    args = parse()
+    cfg = {"survey": SURVEY, "mid": MID, "small": SMALL}[args.config]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, cfg, rank, world)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import aa_b200 as aa
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    x, pulses = synth_input_device(cfg, cfg["seed"] + rank, device)
+    # a stream of its own: the library launches on it and the CUDA events below
+    # are recorded on it (the legacy default stream would not order them)
+    stream = torch.cuda.Stream(device)
+    stream.wait_stream(torch.cuda.current_stream(device))
+    md = metadata_struct(aa, cfg)
+
+    # ---------------- device-resident value ----------------
+    pipe = aa.create_pipeline(md, x.data_ptr(), device_input=True, device_output=True, copy_to_host=False,
+                              stream=stream.cuda_stream, card_number=local)
+    pipe.set_options(tile_words=args.tile_words, group_dms=args.group_dms)
+    plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in cfg["plan"]])
+    if not pipe.bind_ddtr_plan(plan):
+        raise RuntimeError(pipe.last_error())
+    strat = aa.strategy(cfg["plan"], cfg["nchans"], cfg["nsamp"], cfg["fch1"], cfg["foff"], cfg["tsamp"],
+                        cfg["nbits"])
+    units = units_per_step(strat)
+    for _ in range(args.warmup):
+        if not (pipe.run_all() and pipe.synchronize() and pipe.rewind()):
+            raise RuntimeError(pipe.last_error())
+    pipe.time_kernels(True)
+    pipe.reset_kernel_times()
+    launches0 = aa.lib().aa_b200_pipeline_kernel_launches(pipe.m_obj)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize(device)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            if not (pipe.run_all() and pipe.rewind()):
+                raise RuntimeError(pipe.last_error())
+        ev1.record(stream)
+        torch.cuda.synchronize(device)
+    if not pipe.synchronize():
+        raise RuntimeError(pipe.last_error())
+    barrier()
+    ms_total = ev0.elapsed_time(ev1)
+    launches = aa.lib().aa_b200_pipeline_kernel_launches(pipe.m_obj) - launches0
+    kern = {name: pipe.kernel_time(f) for f, name in enumerate(["dedisperse", "corner_turn", "bin"])}
+    ranges = [pipe.range_info(r) for r in range(len(cfg["plan"]))]
+    ms_step = ms_total / args.steps
+    if world > 1:
+        t = torch.tensor([ms_step], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = units * world / (ms_step / 1e3)
+    pipe.cleanUp()
+    pipe.delete()
+
+    # ---------------- e2e through the reference-facing C ABI ----------------
+    e2e = None
+    if not args.no_e2e:
+        xh = torch.empty(x.shape, dtype=torch.int16, pin_memory=True)
+        xh.copy_(x)
+        del x
+        torch.cuda.empty_cache()
+        comps = aa.aa_py_pipeline_components(True, False, False, False)
+        opts = aa.aa_py_pipeline_component_options()
+        opts.copy_ddtr_data_to_host = True
+        api = aa.aa_py_pipeline(comps, opts, md, ctypes_ushort_ptr(xh), local)
+        if not api.bind_ddtr_plan(plan):
+            raise RuntimeError(api.last_error())
+        walls = []
+        for step in range(1 + args.e2e_steps):
+            torch.cuda.synchronize(device)
+            barrier()
+            t0 = time.perf_counter()
+            api.rewind()
+            while api.run():
+                pass
+            if api.status_code() == aa.STATUS_ERROR:
+                raise RuntimeError(api.last_error())
+            torch.cuda.synchronize(device)
+            walls.append(time.perf_counter() - t0)
+        wall = statistics.median(walls[1:])  # the first run also allocates
+        if world > 1:
+            t = torch.tensor([wall], device=device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        h2d = sum((strat["t_processed"][0][k] + strat["maxshift"]) * cfg["nchans"] * 2
+                  for k in range(strat["num_tchunks"]))
+        e2e = {"value": units * world / wall, "unit": "DM-trial*samples/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": units * 4, "ms_per_step": wall * 1e3,
+               "realtime_x": sum(strat["t_processed"][0]) * cfg["tsamp"] / wall}
+        x_host = xh.numpy().view(np.uint16)
+        api.cleanUp()
+        api.delete()
+    else:
+        x_host = x[:min(131040, strat["t_processed"][0][0]) + strat["maxshift"]].cpu().numpy().view(np.uint16)
+    plan.delete()
+
+    # ---------------- roofline of the dominant kernel ----------------
+    dd_ms, dd_n = kern["dedisperse"]
+    nch = cfg["nchans"]
+    alg_bytes = alg_adds = 0
+    for r in range(len(cfg["plan"])):
+        for k in range(strat["num_tchunks"]):
+            tp = strat["t_processed"][r][k]
+            ms_r = strat["maxshift"] // cfg["plan"][r][3]
+            alg_bytes += nch * (tp + ms_r) + strat["ndms"][r] * tp * 4
+            alg_adds += strat["ndms"][r] * tp * nch
+    launches_per_step = len(cfg["plan"]) * strat["num_tchunks"]
+    avg_launch_s = dd_ms / 1e3 / max(1, dd_n)
+    achieved = alg_bytes / launches_per_step / avg_launch_s / 1e9
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": None, "kernel": "k_ddtr_u8",
+                "peak_source": "MEASURED_PEAKS.json (measured)" if "hbm_gbs" in peaks else "fallback",
+                "note": "the DDTR kernel is integer/shared-memory bound, not HBM bound; see integer_rate"}
+    integer_rate = {"channel_adds_per_s": alg_adds / (dd_ms / 1e3 / (dd_n / launches_per_step)),
+                    "kernel_share_of_step": dd_ms / max(1e-9, ms_total)}
+
+    result = None
+    if rank == 0:
+        cb_value, cb_threads, cb_desc = cpu_baseline(cfg, x_host, strat, args.cpu_seconds) if world == 1 else (
+            None, None, None)
+        result = {
+            "metric": METRIC, "value": value, "unit": "DM-trial*samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic", "config": workload_config(cfg),
+            "realtime_x": sum(strat["t_processed"][0]) * cfg["tsamp"] / (ms_step / 1e3),
+            "published_realtime_x": PUBLISHED_REALTIME,
+            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "integer_rate": integer_rate,
+            "kernels_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()},
+            "kernel_launches_per_step": {k: v[1] / args.steps for k, v in kern.items()},
+            "ranges": ranges, "pulses": len(pulses), "clocks": clk.summary(),
+            "cpu_baseline": None if cb_value is None else {"value": cb_value, "unit": "DM-trial*samples/s",
+                                                            "cores": cb_threads, "kind": "port", "sample": cb_desc},
+        }
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_ushort_ptr(t):
+    import ctypes
+    return ctypes.cast(ctypes.c_void_p(t.data_ptr()), ctypes.POINTER(ctypes.c_ushort))
+
+
+if __name__ == "__main__":
+    sys.exit(main())

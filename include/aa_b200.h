@@ -1,0 +1,236 @@
+/*
+ * aa_b200.h -- C ABI of the B200-native dedispersion (DDTR) library
+ * (libaa_b200.so, built from astro-accelerate_b200/csrc/).
+ *
+ * Two layers:
+ *
+ *  1. aa_py_* : the entry points of the reference's own C ABI for the DDTR
+ *     path (AstroAccelerate v1.3.1, src/aa_py_*.cpp, bound by ctypes in
+ *     cmake/py_astro_accelerate.py.in).  Same names, argument meaning, return
+ *     values and status codes, so the reference's Python wrapper binds this
+ *     library by changing the library path.  Only the dedispersion component
+ *     is implemented; plans of other components are refused (return false).
+ *
+ *  2. aa_b200_* : the seam the reference's runner calls internally
+ *     (load/corner turn/binning/dedisperse, include/aa_permitted_pipelines_generic.hpp),
+ *     made stateless (explicit strides and streams instead of __constant__
+ *     state), plus the pipeline extensions this library adds (whole-job run,
+ *     rewind, device-resident input/output, options).
+ *
+ * All pointers are plain; "stream" is a cudaStream_t passed as void*.
+ * Functions returning int return 0 on success unless stated otherwise;
+ * aa_b200_last_error() gives the message of the last failure of this thread.
+ */
+#ifndef AA_B200_H
+#define AA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+#include <cstdbool>
+extern "C" {
+#else
+#include <stdbool.h>
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* 1. Reference C ABI (aa_py_*)                                              */
+/* ------------------------------------------------------------------------ */
+
+/* include/aa_py_filterbank_metadata.hpp:15-25 */
+typedef struct {
+    double m_tstart;
+    double m_tsamp;
+    double m_fch1;
+    double m_foff;
+    int m_nbits;
+    int m_nsamples;
+    int m_nchans;
+    double m_src_raj;
+} aa_py_filterbank_metadata_struct;
+
+/* include/aa_py_pipeline_api.hpp:20-25 */
+typedef struct {
+    bool dedispersion;
+    bool analysis;
+    bool periodicity;
+    bool fdas;
+} pipeline_components_struct;
+
+/* include/aa_py_pipeline_api.hpp:32-48 */
+typedef struct {
+    bool zero_dm;
+    bool zero_dm_with_outliers;
+    bool input_DDTR_normalization;
+    bool output_DDTR_normalization;
+    bool set_bandpass_average;
+    bool old_rfi;
+    bool copy_ddtr_data_to_host;
+    bool msd_baseline_noise;
+    bool output_dmt;
+    bool output_ffdot_plan;
+    bool output_fdas_list;
+    bool candidate_algorithm;
+    bool fdas_custom_fft;
+    bool fdas_inbin;
+    bool fdas_norm;
+} pipeline_component_option_struct;
+
+/* src/aa_py_filterbank_metadata.cpp:7-28, :30-32, :34-36 */
+aa_py_filterbank_metadata_struct *aa_py_filterbank_metadata(double tstart, double tsamp, int nbits, int nsamples,
+                                                            double fch1, double foff, int nchans, double src_raj);
+void aa_py_filterbank_metadata_delete(const aa_py_filterbank_metadata_struct *obj);
+double aa_py_filterbank_metadata_tstart(const aa_py_filterbank_metadata_struct *obj);
+
+/* src/aa_py_ddtr_plan.cpp:7-46 (aa_ddtr_plan*, opaque) */
+void *aa_py_ddtr_plan(void);
+void aa_py_ddtr_plan_delete(const void *obj);
+bool aa_py_ddtr_plan_add_dm(void *obj, float low, float high, float step, int inBin, int outBin);
+size_t aa_py_ddtr_plan_range(const void *obj);
+bool aa_py_ddtr_plan_set_power(void *obj, float power);
+float aa_py_ddtr_plan_power(const void *obj);
+bool aa_py_ddtr_plan_set_enable_msd_baseline(void *obj, bool flag);
+bool aa_py_ddtr_plan_enable_msd_baseline_noise(const void *obj);
+bool aa_py_ddtr_plan_bind_bandpass_normalization(void *obj, const float *data, int data_size);
+
+/* src/aa_py_pipeline_api.cpp:9-40 (aa_pipeline_api<unsigned short>*, opaque).
+ * input_data: host [nsamples][nchans] unsigned short, one value per sample. */
+void *aa_py_pipeline_api(pipeline_components_struct pipeline, pipeline_component_option_struct options,
+                         aa_py_filterbank_metadata_struct metadata, const unsigned short *input_data,
+                         int card_number);
+/* :42-44 */
+void aa_py_pipeline_api_delete(const void *obj);
+/* :46-48 */
+bool aa_py_pipeline_api_bind_ddtr_plan(void *obj, const void *plan);
+/* :50-52: a new strategy object; free with aa_py_ddtr_strategy_delete */
+void *aa_py_pipeline_api_ddtr_strategy(void *obj);
+/* src/aa_py_ddtr_strategy.cpp:6-8 */
+void aa_py_ddtr_strategy_delete(const void *obj);
+/* :54-56 */
+size_t aa_py_get_ddtr_nRanges(void *obj);
+/* :58-60 */
+const int *aa_py_get_ndms_array(void *obj);
+/* :62-64 t_processed[i][j] */
+int aa_py_get_t_proc(void *obj, int i, int j);
+/* :66-68 (the reference truncates the float DM to int) */
+int aa_py_dm_low(void *obj, int range);
+/* :70-72 */
+int aa_py_total_computed_samples(void *obj);
+/* :74-76, :82-85, :87-90: components other than dedispersion are out of
+ * scope for this library and are refused (false). */
+bool aa_py_pipeline_api_bind_analysis_plan(void *obj, const void *plan);
+bool aa_py_pipeline_api_bind_periodicity_plan(void *obj, float sigma_cutoff, bool enable_outlier_rejection,
+                                              float sigma_outlier_rejection_threshold, int nHarmonics,
+                                              int candidate_selection_algorithm);
+bool aa_py_pipeline_api_bind_fdas_plan(void *obj, float sigma_cutoff, float sigma_constant,
+                                       bool enable_msd_baseline_noise);
+/* :92-103: one (time chunk, DM range) step; *status_code receives
+ * aa_pipeline_runner::status (-1 error, 0 finished, 1 has_more,
+ * 2 finished_component, include/aa_pipeline_runner.hpp:25-30). */
+bool aa_py_pipeline_api_run(void *obj, int *status_code);
+/* :105-107 float*** [range][dm][sum_k t_processed[range][k]] */
+float ***aa_py_buffer(void *obj);
+/* :143-157 */
+int aa_py_current_range(void *obj);
+int aa_py_current_time_chunk(void *obj);
+long aa_py_current_inc(void *obj);
+bool aa_py_cleanup(void *obj);
+
+/* ------------------------------------------------------------------------ */
+/* 2. Seam and extensions (aa_b200_*)                                        */
+/* ------------------------------------------------------------------------ */
+
+/* aa_ddtr_plan::dm, include/aa_ddtr_plan.hpp:28-34 */
+typedef struct {
+    float low;
+    float high;
+    float step;
+    int inBin;
+    int outBin;
+} aa_b200_dm;
+
+/* The strategy of src/aa_ddtr_strategy.cpp:27-428 on the host (no GPU
+ * needed).  t_processed is [nranges][max_chunks].  Returns 0, or the
+ * strategy's refusal code (<0). */
+int aa_b200_strategy(const aa_b200_dm *plan, int nranges, float power, int nchans, int nsamp, double fch1,
+                     double foff, double tsamp, int nbits, size_t free_memory, int enable_analysis,
+                     int max_chunks, float *dmshifts, int *ndms, aa_b200_dm *str_dm, int *maxshift,
+                     int *max_ndms, int *num_tchunks, int *t_processed);
+
+/* Kernel choice of src/aa_dedisperse.cpp:8-11,20,48-51,62,88-92,101,133:
+ * 0 shared 8-bit, 1 shared 16-bit, 2 shared 4-bit, 3 cache ("failsafe"). */
+int aa_b200_select_kernel(int nbits, float dm_step, float tsamp, float dmshift_last, int failsafe);
+
+/* corner_turn_SM_inplace (src/aa_corner_turn.cpp:118-121) fused with the
+ * chunk narrowing: d_in_tc [nsamp][nchans] uint16 -> d_out [nchans][out_stride]
+ * uint8 (nbits <= 8) or uint16 (nbits 16/32).  Samples above the bit depth's
+ * range are reported as an error. */
+int aa_b200_corner_turn(const unsigned short *d_in_tc, void *d_out, int nbits, int nchans, long long nsamp,
+                        long long out_stride, void *stream);
+
+/* bin_gpu (src/aa_bin_gpu.cpp:8-44) as it acts on the flat buffer: d_dst
+ * [0, nchans*nsamp/2) = (a+b)>>1 of [c][nsamp] pairs, [.., nchans*nsamp) = 0.
+ * Element type as for aa_b200_corner_turn.  nsamp must be even. */
+int aa_b200_bin_gpu(const void *d_src, void *d_dst, int nbits, int nchans, long long nsamp, void *stream);
+
+/* dedisperse() (src/aa_dedisperse.cpp:5) for DM range i: reads d_input
+ * [nchans][i_nsamp] (the reference's i_nsamp constant, set by
+ * set_dedispersion_constants, src/aa_device_load_data.cu:58-61) and writes
+ * d_output [ndms[i]][out_pitch] (the reference uses out_pitch = t_processed).
+ * tsamp points at the range's sampling time (tsamp_original * inBin[i]),
+ * dmshifts is the host delay table.  d_input_elems is the number of elements
+ * the caller allocated at d_input: the staged windows read up to a few KB
+ * past the last sample a valid output uses, and a call whose reads would
+ * leave the allocation is refused with the padding it needs.  Allocates its
+ * own device scratch (delay, window and offset tables) for the call.
+ * Returns 0 or 1 like the reference; the device work is complete when it
+ * returns. */
+int aa_b200_dedisperse(int i, int t_processed, const int *inBin, const float *dmshifts, const void *d_input,
+                       long long i_nsamp, size_t d_input_elems, float *d_output, long long out_pitch, int nchans,
+                       const float *tsamp, const float *dm_low, const float *dm_step, const int *ndms, int nbits,
+                       int failsafe, void *stream);
+
+/* Message of the last failure of this thread ("" if none). */
+const char *aa_b200_last_error(void);
+/* Kernels this library has launched in this process. */
+long long aa_b200_kernel_launches(void);
+/* Library build identification. */
+const char *aa_b200_version(void);
+
+/* Pipeline extensions (obj from aa_py_pipeline_api or aa_b200_pipeline_create). */
+/* Options, before bind: stride_mode 0 = the reference runner's binning length
+ * (bit-exact with the reference), 1 = true row stride; fma_mode bit mask of
+ * fused delay expressions (7 = all, the reference's --fmad=true build);
+ * free_memory 0 = query the device; tile_words/group_dms 0 = autotune. */
+bool aa_b200_pipeline_set_options(void *obj, int stride_mode, int fma_mode, int failsafe, size_t free_memory,
+                                  int tile_words, int group_dms);
+/* A pipeline whose input (and optionally output) stay in device memory:
+ * input [nsamples][nchans] uint16 on the device when device_input != 0;
+ * device_output != 0 keeps [range][dm][t] on the device
+ * (aa_b200_pipeline_device_output). */
+void *aa_b200_pipeline_create(aa_py_filterbank_metadata_struct metadata, const unsigned short *input,
+                              int device_input, int device_output, int copy_to_host, void *stream,
+                              int card_number);
+bool aa_b200_pipeline_run_all(void *obj);
+bool aa_b200_pipeline_rewind(void *obj);
+bool aa_b200_pipeline_synchronize(void *obj);
+float *aa_b200_pipeline_device_output(void *obj, int range);
+/* kind, DMs per thread block, window span (samples), time words per lane */
+int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms, int *span, int *tile_words);
+long long aa_b200_pipeline_kernel_launches(void *obj);
+const char *aa_b200_pipeline_last_error(void *obj);
+int aa_b200_pipeline_num_tchunks(void *obj);
+int aa_b200_pipeline_maxshift(void *obj);
+/* CUDA-event timing of every kernel launch (off by default).  family:
+ * 0 dedispersion, 1 corner turn, 2 binning.  Times are collected when the
+ * pipeline synchronises; reset clears them. */
+bool aa_b200_pipeline_time_kernels(void *obj, int on);
+int aa_b200_pipeline_kernel_time(void *obj, int family, double *ms, long long *count);
+bool aa_b200_pipeline_reset_kernel_times(void *obj);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AA_B200_H */

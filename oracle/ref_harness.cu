@@ -1,0 +1,163 @@
+/*
+ * ref_harness.cu -- drives the reference's own DDTR code (AstroAccelerate
+ * v1.3.1, compiled from its sources by oracle/Makefile.ref into oracle/_ref/)
+ * so that its results can be captured as golden vectors.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product links this file.
+ *
+ *   aaref_strategy()  runs aa_ddtr_strategy (src/aa_ddtr_strategy.cpp:27-428)
+ *                     on the host; it needs no GPU.
+ *   aaref_run_ddtr()  runs the reference's generic pipeline runner
+ *                     (include/aa_permitted_pipelines_generic.hpp:606-914) with
+ *                     only the dedispersion component and copy-to-host, exactly
+ *                     as tests/test_ddtr_fakesignal_single.cpp:82-103 does, and
+ *                     copies output_buffer() into a flat array.  Needs a GPU.
+ *                     The reference's aa_device_info destructor resets the
+ *                     device, so call this from a process of its own.
+ */
+#include <stdio.h>
+#include <string.h>
+#include <vector>
+
+/* aa_device_info keeps the memory budget private and only fills it in when a
+ * GPU answers; the host-only strategy run sets it directly. */
+#define private public
+#include "aa_device_info.hpp"
+#undef private
+
+#include "aa_ddtr_plan.hpp"
+#include "aa_ddtr_strategy.hpp"
+#include "aa_filterbank_metadata.hpp"
+#include "aa_permitted_pipelines_generic.hpp"
+#include "aa_pipeline.hpp"
+
+using namespace astroaccelerate;
+
+/* Mirrors include/aa_ddtr_plan.hpp:28-34 struct dm for the C ABI below. */
+struct harness_dm {
+    float low, high, step;
+    int inBin, outBin;
+};
+
+namespace {
+
+int copy_strategy(const aa_ddtr_strategy &s, int nchans, int max_chunks,
+                  float *dmshifts, int *ndms, harness_dm *str_dm,
+                  int *maxshift, int *max_ndms, int *num_tchunks,
+                  int *t_processed)
+{
+    const size_t nr = s.get_nRanges();
+    std::vector<float> sh = s.dmshifts();
+    for (int c = 0; c < nchans; c++)
+        dmshifts[c] = sh[c];
+    for (size_t i = 0; i < nr; i++) {
+        ndms[i] = s.ndms(i);
+        aa_ddtr_plan::dm d = s.dm(i);
+        str_dm[i].low = d.low;
+        str_dm[i].high = d.high;
+        str_dm[i].step = d.step;
+        str_dm[i].inBin = d.inBin;
+        str_dm[i].outBin = d.outBin;
+    }
+    *maxshift = s.maxshift();
+    *max_ndms = s.max_ndms();
+    *num_tchunks = s.num_tchunks();
+    if (*num_tchunks > max_chunks)
+        return -5;
+    for (size_t i = 0; i < nr; i++)
+        for (int k = 0; k < *num_tchunks; k++)
+            t_processed[i * max_chunks + k] = s.t_processed()[i][k];
+    return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int aaref_strategy(const harness_dm *plan, int nranges, float power, int nchans,
+                   int nsamp, double fch1, double foff, double tsamp, int nbits,
+                   size_t free_memory, int enable_analysis, int max_chunks,
+                   float *dmshifts, int *ndms, harness_dm *str_dm,
+                   int *maxshift, int *max_ndms, int *num_tchunks,
+                   int *t_processed)
+{
+    aa_ddtr_plan p;
+    for (int i = 0; i < nranges; i++)
+        p.add_dm(plan[i].low, plan[i].high, plan[i].step, plan[i].inBin, plan[i].outBin);
+    p.set_power(power);
+    aa_filterbank_metadata meta(0.0, tsamp, nbits, nsamp, fch1, foff, nchans);
+    aa_device_info dev(0);
+    dev.selected_card_info.available_memory = free_memory;
+    aa_ddtr_strategy s(p, meta, free_memory, enable_analysis != 0, &dev);
+    if (!s.ready())
+        return -1;
+    return copy_strategy(s, nchans, max_chunks, dmshifts, ndms, str_dm, maxshift,
+                         max_ndms, num_tchunks, t_processed);
+}
+
+/* free_memory == 0 uses the device's own free memory, like the reference's
+ * pipeline API (include/aa_pipeline_api.hpp:149); a smaller value forces
+ * time chunking on small inputs. */
+int aaref_run_ddtr(const unsigned short *input_tc, int nchans, int nsamp,
+                   double tsamp, double fch1, double foff, int nbits,
+                   const harness_dm *plan, int nranges, size_t free_memory,
+                   int max_chunks, float *dmshifts, int *ndms,
+                   harness_dm *str_dm, int *maxshift, int *max_ndms,
+                   int *num_tchunks, int *t_processed, float *out,
+                   size_t out_len)
+{
+    aa_device_info dev(0);
+    aa_ddtr_plan p;
+    for (int i = 0; i < nranges; i++)
+        p.add_dm(plan[i].low, plan[i].high, plan[i].step, plan[i].inBin, plan[i].outBin);
+    aa_filterbank_metadata meta(0.0, tsamp, nbits, nsamp, fch1, foff, nchans);
+    size_t dev_free = dev.free_memory();
+    size_t fm = free_memory ? free_memory : dev_free;
+    int rc = 0;
+    size_t written = 0;
+    {
+        aa_ddtr_strategy s(p, meta, fm, false, &dev);
+        if (!s.ready())
+            return -1;
+        rc = copy_strategy(s, nchans, max_chunks, dmshifts, ndms, str_dm, maxshift,
+                           max_ndms, num_tchunks, t_processed);
+        if (rc)
+            return rc;
+
+        aa_pipeline::pipeline comps;
+        comps.insert(aa_pipeline::component::dedispersion);
+        aa_pipeline::pipeline_option opts;
+        opts.insert(aa_pipeline::component_option::copy_ddtr_data_to_host);
+        aa_analysis_strategy an;
+        aa_periodicity_strategy per;
+        aa_fdas_strategy fd;
+        aa_jerk_strategy jk;
+        aa_permitted_pipelines_generic runner(comps, opts, s, an, per, fd, jk,
+                                              false, false, false, false, false,
+                                              input_tc);
+        if (!runner.setup())
+            return -2;
+        aa_pipeline_runner::status st;
+        while (runner.next(st)) {
+            if (st == aa_pipeline_runner::status::error)
+                return -3;
+        }
+        if (st == aa_pipeline_runner::status::error)
+            return -3;
+        float ***buf = runner.output_buffer();
+        for (int r = 0; r < nranges; r++) {
+            size_t tot = 0;
+            for (int k = 0; k < *num_tchunks; k++)
+                tot += (size_t)t_processed[r * max_chunks + k];
+            for (int d = 0; d < ndms[r]; d++) {
+                if (written + tot > out_len)
+                    return -4;
+                memcpy(out + written, buf[r][d], tot * sizeof(float));
+                written += tot;
+            }
+        }
+    }
+    return 0;
+}
+
+} // extern "C"

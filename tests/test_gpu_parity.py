@@ -1,0 +1,145 @@
+"""GPU parity of the B200 DDTR path, called through the C ABI.
+
+For every seeded case of tests/golden/cases.py the pipeline runs through the
+reference-facing entry points (aa_py_pipeline_api, bind, run loop,
+aa_py_buffer) and its float DM-time output is compared
+  * with the CPU oracle: bit-exact when nchans*bin is a power of two (the
+    reference's fast-math division is exact there); otherwise the integer
+    channel sums must agree exactly and the float within 2 ulp (the oracle
+    divides with IEEE division, the device with the reference's fast-math
+    division);
+  * with the reference's own GPU output (golden SHA-256 per DM range,
+    tests/golden/ddtr_golden.json): bit-exact.
+"""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+import cases as C
+
+pytestmark = pytest.mark.gpu
+
+LIGHT = [n for n, c in C.CASES.items() if not c.get("heavy")]
+
+
+def run_pipeline(aa, case, x, stride_mode=0, **opts):
+    md = aa.filterbank_metadata_struct(0.0, case["tsamp"], case["fch1"], case["foff"], case["nbits"],
+                                       case["nsamp"], case["nchans"], 0.0)
+    comps = aa.aa_py_pipeline_components(True, False, False, False)
+    o = aa.aa_py_pipeline_component_options()
+    o.copy_ddtr_data_to_host = True
+    pipe = aa.aa_py_pipeline(comps, o, md, np.ascontiguousarray(x.reshape(-1)), 0)
+    pipe.set_options(stride_mode=stride_mode, free_memory=C.strategy_free_memory(case), **opts)
+    plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in case["plan"]])
+    assert pipe.bind_ddtr_plan(plan), pipe.last_error()
+    steps = 0
+    while pipe.run():
+        steps += 1
+        assert pipe.status_code() != aa.STATUS_ERROR, pipe.last_error()
+    assert pipe.status_code() == aa.STATUS_FINISHED, pipe.last_error()
+    outs = [a.copy() for a in pipe.output_arrays()]
+    info = [pipe.range_info(r) for r in range(len(case["plan"]))]
+    launches = pipe.kernel_launches()
+    pipe.cleanUp()
+    pipe.delete()
+    plan.delete()
+    return outs, info, steps, launches
+
+
+def oracle_run(oracle_mod, case, x, stride_mode=0):
+    s = oracle_mod.strategy(case["plan"], case["nchans"], case["nsamp"], case["fch1"], case["foff"], case["tsamp"],
+                            case["nbits"], C.strategy_free_memory(case))
+    outs, kern = oracle_mod.run_ddtr(x, s, case["nchans"], case["nsamp"], case["tsamp"], case["nbits"],
+                                     stride_mode=stride_mode)
+    return s, outs, kern
+
+
+def assert_matches_oracle(case, s, got, want, kern):
+    for r in range(len(want)):
+        g, w = got[r], want[r]
+        assert g.shape == w.shape, (r, g.shape, w.shape)
+        inbin = s.dm[r][3]
+        div = case["nchans"] * (1 if kern[r][0] == 2 else inbin)
+        if div & (div - 1) == 0:
+            bad = np.flatnonzero(g.view(np.uint32) != w.view(np.uint32))
+            assert bad.size == 0, f"range {r}: {bad.size} outputs differ, first at {np.unravel_index(bad[0], g.shape)}"
+        else:
+            sg = np.rint(g.astype(np.float64) * div)
+            sw = np.rint(w.astype(np.float64) * div)
+            assert np.array_equal(sg, sw), f"range {r}: integer sums differ"
+            ulp = np.abs(g.view(np.int32).astype(np.int64) - w.view(np.int32).astype(np.int64))
+            assert ulp.max() <= 2, f"range {r}: {ulp.max()} ulp"
+
+
+@pytest.mark.parametrize("name", LIGHT)
+def test_pipeline_matches_oracle(aa, oracle_mod, cuda_device, name):
+    case = C.CASES[name]
+    x = C.make_input(case)
+    s, want, kern = oracle_run(oracle_mod, case, x)
+    got, info, steps, launches = run_pipeline(aa, case, x)
+    assert steps == s.num_tchunks * len(case["plan"]) + 1
+    assert launches > 0
+    for r in range(len(case["plan"])):
+        assert info[r]["kind"] == oracle_mod.KERNEL_NAMES[kern[r][0]]
+    assert_matches_oracle(case, s, got, want, kern)
+
+
+@pytest.mark.parametrize("name", list(C.CASES))
+def test_pipeline_matches_reference_gpu(aa, golden_ddtr, cuda_device, name):
+    if name not in golden_ddtr:
+        pytest.skip("case not in the golden file")
+    case = C.CASES[name]
+    rec = golden_ddtr[name]
+    x = C.make_input(case)
+    got, _, _, _ = run_pipeline(aa, case, x)
+    for r, rr in enumerate(rec["ranges"]):
+        g = got[r]
+        assert list(g.shape) == rr["shape"]
+        if hashlib.sha256(g.tobytes()).hexdigest() != rr["sha256"]:
+            bad = [(i, j) for i, j, bits in rr["samples"] if int(g[i, j].view(np.uint32)) != bits]
+            pytest.fail(f"range {r}: output differs from the reference GPU ({len(bad)}/{len(rr['samples'])} "
+                        f"sampled values differ, e.g. {bad[:3]})")
+
+
+@pytest.mark.parametrize("name", ["shared8_binned", "shared8_2bit", "shared16"])
+def test_true_stride_mode_matches_oracle(aa, oracle_mod, cuda_device, name):
+    """The corrected binning (true row stride, repeated x2 steps)."""
+    case = C.CASES[name]
+    x = C.make_input(case)
+    s, want, kern = oracle_run(oracle_mod, case, x, stride_mode=1)
+    got, _, _, _ = run_pipeline(aa, case, x, stride_mode=1)
+    assert_matches_oracle(case, s, got, want, kern)
+
+
+@pytest.mark.parametrize("tile_words,group_dms", [(2, 64), (4, 32), (4, 16), (2, 8)])
+def test_tile_shapes_agree(aa, oracle_mod, cuda_device, tile_words, group_dms):
+    case = C.CASES["shared8_binned"]
+    x = C.make_input(case)
+    s, want, kern = oracle_run(oracle_mod, case, x)
+    got, info, _, _ = run_pipeline(aa, case, x, tile_words=tile_words, group_dms=group_dms)
+    assert info[0]["tile_words"] == tile_words and info[0]["group_dms"] == group_dms
+    assert_matches_oracle(case, s, got, want, kern)
+
+
+def test_kat_fake_signal(aa, oracle_mod, cuda_device):
+    """tests/test_ddtr_fakesignal_single.cpp:109-117 with fixed seeds: all 128
+    channels of the injected pulse align, so the output is exactly 255."""
+    rng = np.random.Generator(np.random.PCG64(77))
+    case = dict(nchans=128, nbits=8, fch1=1550.0, foff=-300.0 / 128, tsamp=6.4e-5, nsamp=int(2 / 6.4e-5),
+                plan=[(0, 250.0, 1, 1, 1)], free_memory=0)
+    s = oracle_mod.strategy(case["plan"], 128, case["nsamp"], 1550.0, case["foff"], 6.4e-5, 8, 180 * 2**30)
+    hits = 0
+    for _ in range(5):
+        dm_position = float(int(rng.integers(0, 200)))
+        start = int(rng.integers(0, 10)) * 1000 + int(rng.integers(0, 10)) * 100 + int(rng.integers(0, 10)) * 10
+        x, _ = oracle_mod.fake_signal(128, case["nsamp"], 6.4e-5, s.dmshifts, s.maxshift, dm_position,
+                                      int(1 / (6.4e-5 * 25)), start, 0.5)
+        x = x.reshape(case["nsamp"], 128)
+        got, _, _, _ = run_pipeline(aa, case, x)
+        want, _ = oracle_mod.run_ddtr(x, s, 128, case["nsamp"], 6.4e-5, 8)
+        assert np.array_equal(got[0].view(np.uint32), want[0].view(np.uint32))
+        hits += int(got[0][int(dm_position) // 1, start] == 255.0)
+    assert hits == 5
