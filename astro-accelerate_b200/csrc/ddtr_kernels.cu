@@ -34,7 +34,7 @@ namespace aab200 {
 namespace {
 
 constexpr int CS = 16;      // channels per shared-memory stage
-constexpr int NSTAGE = 3;   // depth of the cp.async ring
+constexpr int NSTAGE = 3;   // depth of the staging ring
 constexpr int DMW = 4;      // DM trials per warp
 constexpr int MAX_NCH = 16384;
 
@@ -259,22 +259,29 @@ __global__ void k_bin_flat_scalar(const T *__restrict__ src, T *__restrict__ dst
 //           fetched from HBM once and served from L2 to the other groups.
 //   block = 32 * group_dms / 4; lane l of warp w accumulates DM trial w*4+j of
 //           the group at time words l + 32k, i.e. outputs t0+128k+4l+{0,1,2,3}.
-// Shared memory is addressed in 32-bit words from one extern array so every
-// access is a plain shared load/store with a 32-bit address.
+// Pipeline per stage of CS channels:
+//   * one warp issues TMA bulk copies (cp.async.bulk) of the CS raw channel
+//     windows and of their DM offsets into a ring of NSTAGE slots, completing
+//     on an mbarrier per slot;
+//   * all threads wait on the mbarrier (bounded: a copy that never lands sets
+//     DERR_TIMEOUT and the thread stops accumulating), expand the rows of the
+//     next stage into four byte-phase copies (double buffered), accumulate
+//     the current stage, and meet at one barrier.
+// Shared memory is addressed in 32-bit words from one extern array.
 // ---------------------------------------------------------------------------
 struct U8Smem {
-    int rw;      // words per phase row
+    int rw;      // words per phase row (multiple of 4)
     int raww;    // words per staged raw row (multiple of 4)
     int nch_pad; // channels rounded up to 4
-    int o_ent, o_wtab, o_wrow, o_ph; // word offsets
-    size_t total;                    // bytes
+    int o_ent, o_wtab, o_bar, o_wrow, o_ph; // word offsets
+    size_t total;                           // bytes
 };
 
 __host__ __device__ inline U8Smem u8_layout(int span, int group_dms, int tile_words, int nchans)
 {
     U8Smem L;
-    L.rw = (span >> 2) + 32 * tile_words + 1;
-    L.raww = ((L.rw + 8) + 3) & ~3;
+    L.rw = (((span >> 2) + 32 * tile_words + 1) + 3) & ~3;
+    L.raww = (L.rw + 8 + 3) & ~3;
     L.nch_pad = (nchans + 3) & ~3;
     int o = NSTAGE * CS * L.raww;
     L.o_ent = o;
@@ -282,13 +289,58 @@ __host__ __device__ inline U8Smem u8_layout(int span, int group_dms, int tile_wo
     L.o_wtab = o;
     o += NSTAGE * CS * 2;
     o = (o + 3) & ~3;
+    L.o_bar = o;
+    o += 2 * NSTAGE;
+    o = (o + 3) & ~3;
     L.o_wrow = o;
     o += L.nch_pad;
     o = (o + 3) & ~3;
     L.o_ph = o;
-    o += CS * 4 * L.rw;
+    o += 2 * CS * 4 * L.rw;
     L.total = static_cast<size_t>(o) * 4;
     return L;
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void *p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity)
+{
+    unsigned done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}\n"
+                 : "=r"(done)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+
+// Bounded wait: about a second at the try_wait suspend time; false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
+{
+    for (int i = 0; i < (1 << 22); ++i)
+        if (mbar_try_wait(bar, parity))
+            return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_1d(unsigned dst, const void *src, unsigned bytes, unsigned bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
 }
 
 template <int K>
@@ -296,54 +348,87 @@ __global__ void __launch_bounds__(512, 1) k_ddtr_u8(const DdtrLaunch p, const in
                                                     const U8Smem L, const uint32_t one)
 {
     extern __shared__ __align__(16) uint32_t sm[];
-    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
+    const int nwarps = blockDim.x >> 5;
     const int GD = p.group_dms;
     const int g = blockIdx.x;
     const int dm0 = g * GD;
     const long long t0 = static_cast<long long>(blockIdx.y) * (128 * K);
     const int RW = L.rw, RAWW = L.raww;
-
     const unsigned char *in = static_cast<const unsigned char *>(p.in);
     const int nstages = (p.nch_used + CS - 1) / CS;
-    const int cpr = RAWW >> 2;   // 16-byte chunks per raw row
-    const int epr = GD >> 2;     // 16-byte chunks of offsets per channel
+    const unsigned bar0 = smem_addr(&sm[L.o_bar]);
 
-    // window starts of this DM group for every channel
-    for (int q = tid; q < (L.nch_pad >> 2); q += nthr)
+    // window starts of this DM group for every channel, and the barriers
+    for (int q = tid; q < (L.nch_pad >> 2); q += blockDim.x)
         cp_async16(&sm[L.o_wrow + 4 * q], p.wmin + static_cast<size_t>(g) * L.nch_pad + 4 * q);
     cp_async_commit();
+    if (tid == 0)
+        for (int i = 0; i < NSTAGE; ++i)
+            mbar_init(bar0 + 8 * i, 1);
     cp_async_wait<0>();
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     __syncthreads();
 
+    // warp 0 stages stage s: lane cl copies channel cl's raw window and offsets
     auto issue = [&](int s) {
-        if (s < nstages) {
-            const int slot = s % NSTAGE;
-            const int cbase = s * CS;
-            for (int q = tid; q < CS * cpr; q += nthr) {
-                const int cl = q / cpr, part = q - cl * cpr;
-                const int c = cbase + cl;
-                if (c < p.nch_used) {
-                    const int w0 = sm[L.o_wrow + c];
-                    const unsigned char *src = in + static_cast<long long>(c) * p.stride + t0 + w0;
-                    const uintptr_t a = reinterpret_cast<uintptr_t>(src);
-                    const unsigned char *a16 = reinterpret_cast<const unsigned char *>(a & ~static_cast<uintptr_t>(15));
-                    cp_async16(&sm[(slot * CS + cl) * RAWW + part * 4], a16 + part * 16);
-                    if (part == 0) {
-                        sm[L.o_wtab + (slot * CS + cl) * 2 + 0] = static_cast<uint32_t>(w0);
-                        sm[L.o_wtab + (slot * CS + cl) * 2 + 1] = static_cast<uint32_t>(a & 15);
-                    }
-                }
-            }
-            for (int q = tid; q < CS * epr; q += nthr) {
-                const int cl = q / epr, part = q - cl * epr;
-                const int c = cbase + cl;
-                if (c < p.nch_used)
-                    cp_async16(&sm[L.o_ent + (slot * CS + cl) * GD + part * 4],
-                               offtab + static_cast<size_t>(c) * p.ndms + dm0 + part * 4);
+        if (warp != 0 || s >= nstages)
+            return;
+        const int slot = s % NSTAGE;
+        const int ncl = min(CS, p.nch_used - s * CS);
+        const unsigned bar = bar0 + 8 * slot;
+        // the slot was last read through the generic proxy; order those reads
+        // before the async-proxy writes of the copies
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        if (lane == 0)
+            mbar_expect_tx(bar, static_cast<unsigned>(ncl) * static_cast<unsigned>(RAWW * 4 + GD * 4));
+        __syncwarp();
+        if (lane < ncl) {
+            const int c = s * CS + lane;
+            const int w0 = static_cast<int>(sm[L.o_wrow + c]);
+            const unsigned char *src = in + static_cast<long long>(c) * p.stride + t0 + w0;
+            const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+            sm[L.o_wtab + (slot * CS + lane) * 2 + 0] = static_cast<uint32_t>(w0);
+            sm[L.o_wtab + (slot * CS + lane) * 2 + 1] = static_cast<uint32_t>(a & 15);
+            tma_load_1d(smem_addr(&sm[(slot * CS + lane) * RAWW]),
+                        reinterpret_cast<const void *>(a & ~static_cast<uintptr_t>(15)),
+                        static_cast<unsigned>(RAWW * 4), bar);
+            tma_load_1d(smem_addr(&sm[L.o_ent + (slot * CS + lane) * GD]),
+                        offtab + static_cast<size_t>(c) * p.ndms + dm0, static_cast<unsigned>(GD * 4), bar);
+        }
+    };
+
+    bool ok = true;
+    // expand stage s (raw slot) into phase buffer b: phase q word j = raw bytes
+    // [sh + q + 4j, +4); each warp takes channels, lanes take (phase, 4 words)
+    auto build = [&](int s, int b) {
+        const int slot = s % NSTAGE;
+        if (!mbar_wait_bounded(bar0 + 8 * slot, static_cast<unsigned>((s / NSTAGE) & 1))) {
+            if (ok)
+                atomicOr(p.err, DERR_TIMEOUT);
+            ok = false;
+        }
+        const int ncl = min(CS, p.nch_used - s * CS);
+        const int n4 = RW >> 2;
+        for (int cl = warp; cl < ncl; cl += nwarps) {
+            const int sh = static_cast<int>(sm[L.o_wtab + (slot * CS + cl) * 2 + 1]) & 15;
+            const int rbase = (slot * CS + cl) * RAWW;
+            const int pbase = L.o_ph + (b * CS + cl) * 4 * RW;
+            for (int idx = lane; idx < 4 * n4; idx += 32) {
+                const int q = idx & 3, j4 = idx >> 2;
+                const int a = sh + q;
+                const int rb = rbase + 4 * j4 + (a >> 2);
+                const unsigned amt = 8u * static_cast<unsigned>(a & 3);
+                const uint32_t r0 = sm[rb], r1 = sm[rb + 1], r2 = sm[rb + 2], r3 = sm[rb + 3], r4 = sm[rb + 4];
+                uint4 v;
+                v.x = __funnelshift_r(r0, r1, amt);
+                v.y = __funnelshift_r(r1, r2, amt);
+                v.z = __funnelshift_r(r2, r3, amt);
+                v.w = __funnelshift_r(r3, r4, amt);
+                *reinterpret_cast<uint4 *>(&sm[pbase + q * RW + 4 * j4]) = v;
             }
         }
-        cp_async_commit();
     };
 
     uint32_t a16[DMW][K][2];
@@ -359,87 +444,73 @@ __global__ void __launch_bounds__(512, 1) k_ddtr_u8(const DdtrLaunch p, const in
 #pragma unroll
     for (int s = 0; s < NSTAGE - 1; ++s)
         issue(s);
+    __syncthreads(); // window shifts written by warp 0 become visible
+    build(0, 0);
+    __syncthreads();
+    issue(NSTAGE - 1);
 
     int since_flush = 0;
     for (int s = 0; s < nstages; ++s) {
-        cp_async_wait<NSTAGE - 2>();
-        __syncthreads();
+        if (s + 1 < nstages)
+            build(s + 1, (s + 1) & 1);
         const int slot = s % NSTAGE;
         const int ncl = min(CS, p.nch_used - s * CS);
-
-        // expand the raw rows into four byte-phase copies
-        for (int q = tid; q < ncl * RW; q += nthr) {
-            const int cl = q / RW, j = q - cl * RW;
-            const int sh = static_cast<int>(sm[L.o_wtab + (slot * CS + cl) * 2 + 1]);
-            const int rb = (slot * CS + cl) * RAWW + j + (sh >> 2);
-            const int r = sh & 3;
-            const uint32_t w0 = sm[rb], w1 = sm[rb + 1], w2 = sm[rb + 2];
-            const int pb = L.o_ph + cl * 4 * RW + j;
-#pragma unroll
-            for (int pp = 0; pp < 4; ++pp) {
-                const int b = r + pp;
-                const uint32_t lo = (b < 4) ? w0 : w1;
-                const uint32_t hi = (b < 4) ? w1 : w2;
-                sm[pb + pp * RW] = __funnelshift_r(lo, hi, 8 * (b & 3));
-            }
-        }
-        __syncthreads();
-        issue(s + NSTAGE - 1);
-
         const int ebase = L.o_ent + slot * CS * GD + warp * DMW;
-        for (int cl = 0; cl < ncl; ++cl) {
-            const int4 e4 = *reinterpret_cast<const int4 *>(&sm[ebase + cl * GD]);
-            const int prow = L.o_ph + cl * 4 * RW + lane;
-            if ((e4.x | e4.y | e4.z | e4.w) >= 0) {
-                const int ej[DMW] = {e4.x, e4.y, e4.z, e4.w};
-                // two DM trials at a time: 2*K loads in flight, then their adds
+        const int phb = L.o_ph + (s & 1) * CS * 4 * RW + lane;
+        if (ok) {
+            for (int cl = 0; cl < ncl; ++cl) {
+                const int4 e4 = *reinterpret_cast<const int4 *>(&sm[ebase + cl * GD]);
+                const int prow = phb + cl * 4 * RW;
+                if ((e4.x | e4.y | e4.z | e4.w) >= 0) {
+                    const int ej[DMW] = {e4.x, e4.y, e4.z, e4.w};
 #pragma unroll
-                for (int h = 0; h < DMW; h += 2) {
-                    uint32_t w[2][K];
+                    for (int h = 0; h < DMW; h += 2) {
+                        uint32_t w[2][K];
 #pragma unroll
-                    for (int j = 0; j < 2; ++j)
+                        for (int j = 0; j < 2; ++j)
 #pragma unroll
-                        for (int k = 0; k < K; ++k)
-                            w[j][k] = sm[prow + ej[h + j] + 32 * k];
+                            for (int k = 0; k < K; ++k)
+                                w[j][k] = sm[prow + ej[h + j] + 32 * k];
 #pragma unroll
-                    for (int j = 0; j < 2; ++j)
+                        for (int j = 0; j < 2; ++j)
+#pragma unroll
+                            for (int k = 0; k < K; ++k) {
+                                a16[h + j][k][0] = (w[j][k] & 0x00FF00FFu) * one + a16[h + j][k][0];
+                                a16[h + j][k][1] = __byte_perm(w[j][k], 0u, 0x4341) * one + a16[h + j][k][1];
+                            }
+                    }
+                } else {
+                    // per-class path (rare): some thread classes read one sample
+                    // later, or a delay falls outside the window
+                    const int c = s * CS + cl;
+                    const int wmin = static_cast<int>(sm[L.o_wtab + (slot * CS + cl) * 2 + 0]);
+#pragma unroll
+                    for (int j = 0; j < DMW; ++j) {
+                        const int dm = dm0 + warp * DMW + j;
+                        const int ee = p.table[static_cast<size_t>(c) * p.ndms + dm];
+                        const int o = (ee & 0xFFFFFF) - wmin;
+                        const unsigned mask = static_cast<unsigned>(ee) >> 24;
+                        int dA, dB;
+                        if (p.kind == KIND_SHARED4) {
+                            dA = dB = (mask >> (lane & 7)) & 1;
+                        } else {
+                            dA = (mask >> (2 * (lane & 3))) & 1;
+                            dB = (mask >> (2 * (lane & 3) + 1)) & 1;
+                        }
+                        const int oA = o + dA, oB = o + dB;
+                        if (oA < 0 || oB < 0 || oA > p.span || oB > p.span) {
+                            if (lane == 0)
+                                atomicOr(p.err, DERR_WINDOW);
+                            continue;
+                        }
+                        const int pa = prow - lane + (oA & 3) * RW + (oA >> 2) + lane;
+                        const int pb = prow - lane + (oB & 3) * RW + (oB >> 2) + lane;
 #pragma unroll
                         for (int k = 0; k < K; ++k) {
-                            a16[h + j][k][0] = (w[j][k] & 0x00FF00FFu) * one + a16[h + j][k][0];
-                            a16[h + j][k][1] = __byte_perm(w[j][k], 0u, 0x4341) * one + a16[h + j][k][1];
+                            const uint32_t wa = sm[pa + 32 * k], wb = sm[pb + 32 * k];
+                            a16[j][k][0] += (wa & 0x000000FFu) | (wb & 0x00FF0000u);
+                            a16[j][k][1] += ((wa >> 8) & 0x000000FFu) | ((wb >> 8) & 0x00FF0000u);
                         }
-                }
-            } else {
-                // per-class path (rare): some thread classes read one sample
-                // later, or a delay falls outside the window
-                const int c = s * CS + cl;
-                const int wmin = static_cast<int>(sm[L.o_wtab + (slot * CS + cl) * 2 + 0]);
-#pragma unroll
-                for (int j = 0; j < DMW; ++j) {
-                    const int dm = dm0 + warp * DMW + j;
-                    const int ee = p.table[static_cast<size_t>(c) * p.ndms + dm];
-                    const int o = (ee & 0xFFFFFF) - wmin;
-                    const unsigned mask = static_cast<unsigned>(ee) >> 24;
-                    int dA, dB;
-                    if (p.kind == KIND_SHARED4) {
-                        dA = dB = (mask >> (lane & 7)) & 1;
-                    } else {
-                        dA = (mask >> (2 * (lane & 3))) & 1;
-                        dB = (mask >> (2 * (lane & 3) + 1)) & 1;
-                    }
-                    const int oA = o + dA, oB = o + dB;
-                    if (oA < 0 || oB < 0 || oA > p.span || oB > p.span) {
-                        if (lane == 0)
-                            atomicOr(p.err, DERR_WINDOW);
-                        continue;
-                    }
-                    const int pa = L.o_ph + cl * 4 * RW + (oA & 3) * RW + (oA >> 2) + lane;
-                    const int pb = L.o_ph + cl * 4 * RW + (oB & 3) * RW + (oB >> 2) + lane;
-#pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        const uint32_t wa = sm[pa + 32 * k], wb = sm[pb + 32 * k];
-                        a16[j][k][0] += (wa & 0x000000FFu) | (wb & 0x00FF0000u);
-                        a16[j][k][1] += ((wa >> 8) & 0x000000FFu) | ((wb >> 8) & 0x00FF0000u);
                     }
                 }
             }
@@ -458,8 +529,9 @@ __global__ void __launch_bounds__(512, 1) k_ddtr_u8(const DdtrLaunch p, const in
                 }
             since_flush = 0;
         }
+        __syncthreads();
+        issue(s + NSTAGE);
     }
-    cp_async_wait<0>();
 #pragma unroll
     for (int j = 0; j < DMW; ++j)
 #pragma unroll
@@ -469,6 +541,8 @@ __global__ void __launch_bounds__(512, 1) k_ddtr_u8(const DdtrLaunch p, const in
             a32[j][k][1] += a16[j][k][1] & 0xFFFFu;
             a32[j][k][3] += a16[j][k][1] >> 16;
         }
+    if (!ok)
+        return;
 
     // epilogue: (float)S / nchans / bin, the reference's expression
 #pragma unroll
@@ -614,7 +688,7 @@ size_t ddtr_u8_smem_bytes(int span, int group_dms, int tile_words, int nchans)
 
 int ddtr_u8_rw(int span, int tile_words)
 {
-    return (span >> 2) + 32 * tile_words + 1;
+    return (((span >> 2) + 32 * tile_words + 1) + 3) & ~3;
 }
 
 cudaError_t launch_ddtr_u8(const DdtrLaunch &p, const int32_t *offtab, int tile_words, cudaStream_t st)

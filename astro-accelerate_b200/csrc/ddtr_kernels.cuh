@@ -31,6 +31,7 @@ enum DevErr : int {
     DERR_DELAY_RANGE = 1, // a delay outside [0, 2^24) or a class step > 1
     DERR_INPUT_RANGE = 2, // a sample above the bit depth's range
     DERR_WINDOW = 4,      // a delay outside the staged window
+    DERR_TIMEOUT = 8,     // a staging copy did not complete within the wait limit
 };
 
 struct DdtrLaunch {
