@@ -15,6 +15,7 @@
  *                     The reference's aa_device_info destructor resets the
  *                     device, so call this from a process of its own.
  */
+#include <chrono>
 #include <stdio.h>
 #include <string.h>
 #include <vector>
@@ -123,6 +124,8 @@ int aaref_run_ddtr(const unsigned short *input_tc, int nchans, int nsamp,
                            max_ndms, num_tchunks, t_processed);
         if (rc)
             return rc;
+        if ((long long)nchans * (long long)(s.t_processed()[0][0] + s.maxshift()) >= (1LL << 31))
+            return -6; /* 32-bit index overflow in the reference kernels */
 
         aa_pipeline::pipeline comps;
         comps.insert(aa_pipeline::component::dedispersion);
@@ -156,6 +159,57 @@ int aaref_run_ddtr(const unsigned short *input_tc, int nchans, int nsamp,
                 written += tot;
             }
         }
+    }
+    return 0;
+}
+
+/* Times the reference's pipeline runner over the whole input: setup outside
+ * the timed region, then the run(status) loop (load, corner turn, binning,
+ * dedispersion and, with copy_to_host, the D2H into float***), wall clock. */
+int aaref_time_ddtr(const unsigned short *input_tc, int nchans, int nsamp, double tsamp, double fch1,
+                    double foff, int nbits, const harness_dm *plan, int nranges, int copy_to_host,
+                    double *seconds, int *num_tchunks)
+{
+    aa_device_info dev(0);
+    aa_ddtr_plan p;
+    for (int i = 0; i < nranges; i++)
+        p.add_dm(plan[i].low, plan[i].high, plan[i].step, plan[i].inBin, plan[i].outBin);
+    aa_filterbank_metadata meta(0.0, tsamp, nbits, nsamp, fch1, foff, nchans);
+    size_t fm = dev.free_memory();
+    {
+        aa_ddtr_strategy s(p, meta, fm, false, &dev);
+        if (!s.ready())
+            return -1;
+        *num_tchunks = s.num_tchunks();
+        /* the reference's shared kernels index the flat chunk with a 32-bit
+         * int (src/aa_device_dedispersion_kernel.cu:194,214); a chunk of more
+         * than 2^31 elements makes them read out of bounds, so it is refused */
+        if ((long long)nchans * (long long)(s.t_processed()[0][0] + s.maxshift()) >= (1LL << 31))
+            return -4;
+        aa_pipeline::pipeline comps;
+        comps.insert(aa_pipeline::component::dedispersion);
+        aa_pipeline::pipeline_option opts;
+        if (copy_to_host)
+            opts.insert(aa_pipeline::component_option::copy_ddtr_data_to_host);
+        aa_analysis_strategy an;
+        aa_periodicity_strategy per;
+        aa_fdas_strategy fd;
+        aa_jerk_strategy jk;
+        aa_permitted_pipelines_generic runner(comps, opts, s, an, per, fd, jk, false, false, false, false, false,
+                                              input_tc);
+        if (!runner.setup())
+            return -2;
+        cudaDeviceSynchronize();
+        auto t0 = std::chrono::steady_clock::now();
+        aa_pipeline_runner::status st;
+        while (runner.next(st)) {
+            if (st == aa_pipeline_runner::status::error)
+                return -3;
+        }
+        if (st == aa_pipeline_runner::status::error || cudaDeviceSynchronize() != cudaSuccess)
+            return -3;
+        auto t1 = std::chrono::steady_clock::now();
+        *seconds = std::chrono::duration<double>(t1 - t0).count();
     }
     return 0;
 }
