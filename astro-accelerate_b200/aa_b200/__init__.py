@@ -127,6 +127,9 @@ def lib():
         "aa_b200_corner_turn": ([vp, vp, i, i, ll, ll, vp], i),
         "aa_b200_bin_gpu": ([vp, vp, i, i, ll, vp], i),
         "aa_b200_dedisperse": ([i, i, P(i), P(f), vp, ll, sz, vp, ll, i, P(f), P(f), P(f), P(i), i, i, vp], i),
+        "aa_b200_dedisperse_noalloc": ([i, i, P(i), P(f), vp, ll, sz, vp, ll, i, P(f), P(f), P(f), P(i), i, i, vp],
+                                       i),
+        "aa_b200_noalloc_last_error": ([], ctypes.c_char_p),
         "aa_b200_last_error": ([], ctypes.c_char_p),
         "aa_b200_kernel_launches": ([], ll),
         "aa_b200_version": ([], ctypes.c_char_p),
@@ -446,6 +449,28 @@ def corner_turn(d_in_tc, d_out, nbits, nchans, nsamp, out_stride, stream=0):
 def bin_gpu(d_src, d_dst, nbits, nchans, nsamp, stream=0):
     if lib().aa_b200_bin_gpu(_ptr(d_src), _ptr(d_dst), nbits, nchans, nsamp, stream):
         raise RuntimeError(last_error())
+
+
+def _dedisperse_args(i, t_processed, inBin, dmshifts, d_input, i_nsamp, d_input_elems, d_output, out_pitch, nchans,
+                     tsamp, dm_low, dm_step, ndms, nbits, failsafe, stream):
+    nr = len(ndms)
+    keep = dict(inb=(ctypes.c_int * nr)(*inBin), sh=np.ascontiguousarray(dmshifts, dtype=np.float32),
+                ts=ctypes.c_float(tsamp), lo=(ctypes.c_float * nr)(*dm_low), st=(ctypes.c_float * nr)(*dm_step),
+                nd=(ctypes.c_int * nr)(*ndms))
+    args = (i, t_processed, keep["inb"], keep["sh"].ctypes.data_as(PFLOAT), _ptr(d_input), i_nsamp, d_input_elems,
+            _ptr(d_output), out_pitch, nchans, ctypes.byref(keep["ts"]), keep["lo"], keep["st"], keep["nd"], nbits,
+            failsafe, stream)
+    return args, keep
+
+
+def dedisperse_noalloc(i, t_processed, inBin, dmshifts, d_input, i_nsamp, d_input_elems, d_output, out_pitch,
+                       nchans, tsamp, dm_low, dm_step, ndms, nbits, failsafe=0, stream=0):
+    """aa_b200_dedisperse_noalloc: the same work with the library's fixed
+    device scratch array instead of allocated scratch."""
+    args, keep = _dedisperse_args(i, t_processed, inBin, dmshifts, d_input, i_nsamp, d_input_elems, d_output,
+                                  out_pitch, nchans, tsamp, dm_low, dm_step, ndms, nbits, failsafe, stream)
+    if lib().aa_b200_dedisperse_noalloc(*args):
+        raise RuntimeError(lib().aa_b200_noalloc_last_error().decode())
 
 
 def dedisperse(i, t_processed, inBin, dmshifts, d_input, i_nsamp, d_input_elems, d_output, out_pitch, nchans,

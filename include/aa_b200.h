@@ -191,6 +191,32 @@ int aa_b200_dedisperse(int i, int t_processed, const int *inBin, const float *dm
                        const float *tsamp, const float *dm_low, const float *dm_step, const int *ndms, int nbits,
                        int failsafe, void *stream);
 
+/* aa_b200_dedisperse without device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc/cudaFree --
+ * code running inside a memory pool or arena that owns the GPU's memory,
+ * real-time loops that must not synchronise with the allocator, hosts that
+ * reserve all device memory at start-up.  Same arguments, results and return
+ * values as aa_b200_dedisperse; the delay, window and offset tables live in
+ * one fixed array of AA_B200_NOALLOC_SCRATCH_BYTES in the library's device
+ * image, which every GPU that loads the library holds until the process
+ * exits.  Limits: nchans <= AA_B200_NOALLOC_MAX_CHANS and
+ * nchans * ndms[i] <= AA_B200_NOALLOC_MAX_ENTRIES; larger calls are refused
+ * (return 1, message in aa_b200_noalloc_last_error).  The first call on each
+ * device looks up the array's device address (cudaGetSymbolAddress), so make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (other threads, other streams) race and must
+ * be serialised by the caller.  Each call clears what must start at zero. */
+#define AA_B200_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define AA_B200_NOALLOC_MAX_CHANS 16384
+#define AA_B200_NOALLOC_MAX_ENTRIES (1u << 20)
+int aa_b200_dedisperse_noalloc(int i, int t_processed, const int *inBin, const float *dmshifts, const void *d_input,
+                               long long i_nsamp, size_t d_input_elems, float *d_output, long long out_pitch,
+                               int nchans, const float *tsamp, const float *dm_low, const float *dm_step,
+                               const int *ndms, int nbits, int failsafe, void *stream);
+/* Message of the last refusal or failure of aa_b200_dedisperse_noalloc in
+ * this thread ("" if the last call succeeded). */
+const char *aa_b200_noalloc_last_error(void);
+
 /* Message of the last failure of this thread ("" if none). */
 const char *aa_b200_last_error(void);
 /* Kernels this library has launched in this process. */
