@@ -135,6 +135,7 @@ def lib():
         "aa_b200_version": ([], ctypes.c_char_p),
         "aa_b200_pipeline_set_options": ([vp, i, i, i, sz, i, i], b),
         "aa_b200_pipeline_create": ([filterbank_metadata_struct, vp, i, i, i, vp, i], vp),
+        "aa_b200_pipeline_set_kernel_variant": ([vp, i], b),
         "aa_b200_pipeline_run_all": ([vp], b),
         "aa_b200_pipeline_rewind": ([vp], b),
         "aa_b200_pipeline_synchronize": ([vp], b),
@@ -326,6 +327,12 @@ class aa_py_pipeline:
             raise ValueError(self.last_error())
         return ok
 
+    def set_kernel_variant(self, variant: int):
+        """0 auto, 1 byte-phase kernel, 2 channel-quad kernel (before bind)."""
+        if not lib().aa_b200_pipeline_set_kernel_variant(self.m_obj, variant):
+            raise ValueError(self.last_error())
+        return True
+
     def run_all(self):
         return bool(lib().aa_b200_pipeline_run_all(self.m_obj))
 
@@ -352,7 +359,8 @@ class aa_py_pipeline:
         if lib().aa_b200_pipeline_range_info(self.m_obj, r, ctypes.byref(k), ctypes.byref(g), ctypes.byref(s),
                                               ctypes.byref(t)):
             raise RuntimeError(self.last_error())
-        return {"kind": KIND_NAMES[k.value], "group_dms": g.value, "span": s.value, "tile_words": t.value}
+        return {"kind": KIND_NAMES[k.value & 0xFF], "kernel": "quad" if k.value & 0x100 else "phase",
+                "group_dms": g.value, "span": s.value, "tile_words": t.value}
 
     def time_kernels(self, on: bool = True):
         return bool(lib().aa_b200_pipeline_time_kernels(self.m_obj, int(on)))

@@ -514,6 +514,17 @@ void *aa_b200_pipeline_create(aa_py_filterbank_metadata_struct metadata, const u
     return a;
 }
 
+bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant)
+{
+    Api *a = as_api(obj);
+    if (a->pipe)
+        return api_fail(a, "the kernel variant must be set before the plan is bound");
+    if (variant < 0 || variant > 2)
+        return api_fail(a, "kernel variant must be 0 (auto), 1 (byte-phase) or 2 (channel-quad)");
+    a->popt.kernel_variant = variant;
+    return true;
+}
+
 bool aa_b200_pipeline_run_all(void *obj)
 {
     Api *a = as_api(obj);
@@ -556,6 +567,11 @@ int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms,
     *group_dms = rc.group_dms;
     *span = rc.span;
     *tile_words = rc.tile_words;
+    if (rc.variant == 2) {
+        *kind |= 0x100;
+        *span = rc.quad_span;
+        *tile_words = rc.quad.M / 4;
+    }
     return 0;
 }
 

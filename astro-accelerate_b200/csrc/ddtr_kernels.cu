@@ -25,6 +25,7 @@
 //    words of one DM trial, so delays, class exceptions and window checks are
 //    warp-uniform.
 #include "ddtr_kernels.cuh"
+#include "device_util.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -33,21 +34,13 @@ namespace aab200 {
 
 namespace {
 
+using namespace dev;
+
 constexpr int CS = 16;      // channels per shared-memory stage
 constexpr int NSTAGE = 3;   // depth of the staging ring
 constexpr int DMW = 4;      // DM trials per warp
 constexpr int MAX_NCH = 16384;
 
-__device__ __forceinline__ void cp_async16(void *smem_ptr, const void *gptr)
-{
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_ptr));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gptr) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait()
-{
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
 
 __device__ __forceinline__ int findex_of(int kind, int tx)
 {
@@ -301,48 +294,6 @@ __host__ __device__ inline U8Smem u8_layout(int span, int group_dms, int tile_wo
     return L;
 }
 
-__device__ __forceinline__ unsigned smem_addr(const void *p)
-{
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity)
-{
-    unsigned done;
-    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                 "selp.u32 %0, 1, 0, p;\n\t}\n"
-                 : "=r"(done)
-                 : "r"(bar), "r"(parity)
-                 : "memory");
-    return done != 0;
-}
-
-// Bounded wait: about a second at the try_wait suspend time; false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
-{
-    for (int i = 0; i < (1 << 22); ++i)
-        if (mbar_try_wait(bar, parity))
-            return true;
-    return false;
-}
-
-__device__ __forceinline__ void tma_load_1d(unsigned dst, const void *src, unsigned bytes, unsigned bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-
 template <int K>
 __global__ void __launch_bounds__(512, 1) k_ddtr_u8(const DdtrLaunch p, const int32_t *__restrict__ offtab,
                                                     const U8Smem L, const uint32_t one)
@@ -368,7 +319,7 @@ __global__ void __launch_bounds__(512, 1) k_ddtr_u8(const DdtrLaunch p, const in
         for (int i = 0; i < NSTAGE; ++i)
             mbar_init(bar0 + 8 * i, 1);
     cp_async_wait<0>();
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    mbar_init_fence();
     __syncthreads();
 
     // warp 0 stages stage s: lane cl copies channel cl's raw window and offsets
@@ -380,7 +331,7 @@ __global__ void __launch_bounds__(512, 1) k_ddtr_u8(const DdtrLaunch p, const in
         const unsigned bar = bar0 + 8 * slot;
         // the slot was last read through the generic proxy; order those reads
         // before the async-proxy writes of the copies
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        fence_proxy_async();
         if (lane == 0)
             mbar_expect_tx(bar, static_cast<unsigned>(ncl) * static_cast<unsigned>(RAWW * 4 + GD * 4));
         __syncwarp();

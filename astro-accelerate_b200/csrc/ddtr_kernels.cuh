@@ -78,4 +78,32 @@ cudaError_t launch_ddtr_u16(const DdtrLaunch &p, cudaStream_t st);
 size_t ddtr_u8_smem_bytes(int span, int group_dms, int tile_words, int nchans);
 int ddtr_u8_rw(int span, int tile_words);
 
+// Channel-quad kernel (ddtr_quad.cu).  Tables per range:
+//   qpat [group][nquads][16] int32: skews (d1 | d2<<8 | d3<<16) in 0..14, count in 15
+//   qwin [group][nq_pad] int32: smallest base-channel delay of the group
+//   qtmp [nquads][ndms] int32: slot<<24 | tau (tau = delay - window start), -1 per-byte path
+//   qoff [nquads][ndms] int32: slot*W + tau, -1 per-byte path
+struct QuadLaunch {
+    const int32_t *qpat;
+    const int32_t *qwin;
+    const int32_t *qoff;
+    int nquads, nq_pad;
+    int W;     // words per pre-skewed row
+    int raww;  // words per staged raw row
+    int qs;    // channel quads per stage
+    int npool; // pre-skewed rows per stage buffer
+    int M;     // outputs per lane per DM trial (tile = 32*M)
+};
+
+struct QuadGeometry {
+    int M, W, raww, qs, npool, nq_pad;
+    size_t smem_bytes;
+};
+
+QuadGeometry quad_geometry(int span, int dmax, int maxcnt, int group_dms, int nquads, int out_words, int qs);
+cudaError_t launch_quad_patterns(const int32_t *table, int nch_used, int ndms, int group_dms, int nquads, int nq_pad,
+                                 int32_t *qpat, int32_t *qwin, int32_t *qtmp, int *stats, cudaStream_t st);
+cudaError_t launch_quad_offsets(const int32_t *qtmp, size_t n, int W, int32_t *qoff, cudaStream_t st);
+cudaError_t launch_ddtr_quad(const DdtrLaunch &p, const QuadLaunch &q, cudaStream_t st);
+
 } // namespace aab200

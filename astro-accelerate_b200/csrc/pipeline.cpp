@@ -126,6 +126,10 @@ bool DdtrPipeline::build_range(int r)
         return fail(error_.empty() ? "no DM-group size fits the delay span of range " + std::to_string(r) : error_);
     if (!check_device_flags())
         return false;
+    if (elem_bytes_ == 1 && opt_.kernel_variant != 1 && rc.group_dms == 64) {
+        if (!build_quad_tables(r))
+            return false;
+    }
     if (elem_bytes_ == 1) {
         if (!check_cuda(cudaMalloc(&rc.d_offtab, nent * sizeof(int32_t)), "cudaMalloc(offset table)"))
             return false;
@@ -136,6 +140,67 @@ bool DdtrPipeline::build_range(int r)
         ++launches_;
     }
     return true;
+}
+
+// Channel-quad tables: skew patterns per (quad, DM group), window starts and
+// word offsets; chooses the channel-quad kernel when its stage fits shared memory.
+bool DdtrPipeline::build_quad_tables(int r)
+{
+    RangeConfig &rc = ranges_[r];
+    const int ndms = strategy_.ndms(r);
+    const int nquads = (rc.nch_used + 3) / 4;
+    const int nq_pad = (nquads + 3) & ~3;
+    const int ngroups = ndms / rc.group_dms;
+    int *d_stats = nullptr;
+    int32_t *d_qtmp = nullptr;
+    int hs[3] = {0, 0, 0};
+    const size_t nq_ent = static_cast<size_t>(nquads) * ndms;
+    if (!check_cuda(cudaMalloc(&rc.d_qpat, static_cast<size_t>(ngroups) * nquads * 16 * sizeof(int32_t)), "cudaMalloc") ||
+        !check_cuda(cudaMalloc(&rc.d_qwin, static_cast<size_t>(ngroups) * nq_pad * sizeof(int32_t)), "cudaMalloc") ||
+        !check_cuda(cudaMemsetAsync(rc.d_qwin, 0, static_cast<size_t>(ngroups) * nq_pad * sizeof(int32_t), st_), "memset") ||
+        !check_cuda(cudaMalloc(&rc.d_qoff, nq_ent * sizeof(int32_t)), "cudaMalloc") ||
+        !check_cuda(cudaMalloc(&d_qtmp, nq_ent * sizeof(int32_t)), "cudaMalloc") ||
+        !check_cuda(cudaMalloc(&d_stats, 3 * sizeof(int)), "cudaMalloc") ||
+        !check_cuda(cudaMemsetAsync(d_stats, 0, 3 * sizeof(int), st_), "memset"))
+        return false;
+    bool ok = check_cuda(launch_quad_patterns(rc.d_table, rc.nch_used, ndms, rc.group_dms, nquads, nq_pad, rc.d_qpat,
+                                              rc.d_qwin, d_qtmp, d_stats, st_),
+                         "quad patterns") &&
+              check_cuda(cudaMemcpyAsync(hs, d_stats, 3 * sizeof(int), cudaMemcpyDeviceToHost, st_), "D2H") &&
+              check_cuda(cudaStreamSynchronize(st_), "sync");
+    ++launches_;
+    if (ok) {
+        rc.quad_span = hs[0];
+        rc.quad_dmax = hs[1];
+        rc.quad_maxcnt = hs[2];
+        rc.nquads = nquads;
+        const int M = (opt_.tile_words == 2) ? 8 : 16;
+        int qs = 4;
+        QuadGeometry G = quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, nquads, M, qs);
+        while (G.smem_bytes > 227 * 1024 && qs > 1) {
+            qs /= 2;
+            G = quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, nquads, M, qs);
+        }
+        if (G.smem_bytes <= 227 * 1024 && rc.quad_dmax <= 255) {
+            rc.quad = G;
+            rc.variant = 2;
+            ok = check_cuda(launch_quad_offsets(d_qtmp, nq_ent, G.W, rc.d_qoff, st_), "quad offsets");
+            ++launches_;
+        }
+    }
+    if (ok)
+        ok = check_cuda(cudaStreamSynchronize(st_), "sync");
+    cudaFree(d_qtmp);
+    cudaFree(d_stats);
+    if (rc.variant != 2) {
+        cudaFree(rc.d_qpat);
+        cudaFree(rc.d_qwin);
+        cudaFree(rc.d_qoff);
+        rc.d_qpat = rc.d_qwin = rc.d_qoff = nullptr;
+        if (opt_.kernel_variant == 2)
+            return fail("the channel-quad kernel does not fit range " + std::to_string(r));
+    }
+    return ok;
 }
 
 bool DdtrPipeline::check_device_flags()
@@ -268,6 +333,7 @@ bool DdtrPipeline::setup()
         span_max = std::max(span_max, ranges_[r].span);
         delay_max = std::max(delay_max, ranges_[r].delay_max);
         rawb_max = std::max(rawb_max, 4 * ddtr_u8_rw(ranges_[r].span, ranges_[r].tile_words) + 32);
+        rawb_max = std::max(rawb_max, 4 * ranges_[r].quad.raww + 64);
     }
 
     const long long L0 = static_cast<long long>(strategy_.t_processed()[0][0]) + strategy_.maxshift();
@@ -443,9 +509,12 @@ bool DdtrPipeline::do_range()
         i_nsamp = cur_stride_;
     }
 
-    const int tile = 128 * rc.tile_words;
+    const int tile = (rc.variant == 2) ? 32 * rc.quad.M : 128 * rc.tile_words;
     long long need;
-    if (elem_bytes_ == 1)
+    if (elem_bytes_ == 1 && rc.variant == 2)
+        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ((tp + tile - 1) / tile) * static_cast<long long>(tile) +
+               rc.delay_max + 4LL * rc.quad.raww + 64;
+    else if (elem_bytes_ == 1)
         need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ((tp + tile - 1) / tile) * static_cast<long long>(tile) +
                rc.delay_max + 4LL * ddtr_u8_rw(rc.span, rc.tile_words) + 64;
     else
@@ -480,11 +549,27 @@ bool DdtrPipeline::do_range()
         p.out = d_tile_[slot];
         p.out_pitch = tp;
     }
-    if ((reinterpret_cast<uintptr_t>(p.out) & 15) || (p.out_pitch & 3) || (tp & 3))
+    if (rc.variant != 2 && ((reinterpret_cast<uintptr_t>(p.out) & 15) || (p.out_pitch & 3) || (tp & 3)))
         return fail("output rows are not 16-byte aligned");
     if (!timed_launch_begin(KF_DDTR))
         return false;
-    cudaError_t e = (elem_bytes_ == 1) ? launch_ddtr_u8(p, rc.d_offtab, rc.tile_words, st_) : launch_ddtr_u16(p, st_);
+    cudaError_t e;
+    if (elem_bytes_ == 1 && rc.variant == 2) {
+        QuadLaunch q;
+        q.qpat = rc.d_qpat;
+        q.qwin = rc.d_qwin;
+        q.qoff = rc.d_qoff;
+        q.nquads = rc.nquads;
+        q.nq_pad = rc.quad.nq_pad;
+        q.W = rc.quad.W;
+        q.raww = rc.quad.raww;
+        q.qs = rc.quad.qs;
+        q.npool = rc.quad.npool;
+        q.M = rc.quad.M;
+        e = launch_ddtr_quad(p, q, st_);
+    } else {
+        e = (elem_bytes_ == 1) ? launch_ddtr_u8(p, rc.d_offtab, rc.tile_words, st_) : launch_ddtr_u16(p, st_);
+    }
     if (!check_cuda(e, "dedispersion") || !timed_launch_end())
         return false;
     ++launches_;
@@ -585,7 +670,11 @@ bool DdtrPipeline::cleanup()
         cudaFree(rc.d_table);
         cudaFree(rc.d_wmin);
         cudaFree(rc.d_offtab);
+        cudaFree(rc.d_qpat);
+        cudaFree(rc.d_qwin);
+        cudaFree(rc.d_qoff);
         rc.d_table = rc.d_wmin = rc.d_offtab = nullptr;
+        rc.d_qpat = rc.d_qwin = rc.d_qoff = nullptr;
     }
     ranges_.clear();
     for (int i = 0; i < 2; ++i) {

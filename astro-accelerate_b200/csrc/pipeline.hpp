@@ -21,6 +21,7 @@
 
 #include <cuda_runtime.h>
 
+#include "ddtr_kernels.cuh"
 #include "planner.hpp"
 
 namespace aab200 {
@@ -39,6 +40,7 @@ struct PipelineOptions {
     int failsafe = 0;           // force the cache-kernel delay semantics
     size_t free_memory = 0;     // 0: query the device like aa_device_info::free_memory()
     int tile_words = 0;         // 0: autotune
+    int kernel_variant = 0;     // 0: autotune, 1: byte-phase kernel, 2: channel-quad kernel
     int group_dms = 0;          // 0: autotune
     bool device_input = false;  // the input pointer is device memory ([t][c] uint16)
     bool device_output = false; // keep the whole output on the device ([range][dm][t])
@@ -63,6 +65,13 @@ struct RangeConfig {
     int32_t *d_table = nullptr;
     int32_t *d_wmin = nullptr;
     int32_t *d_offtab = nullptr;
+    // channel-quad kernel
+    int variant = 1;            // 1: byte-phase kernel (k_ddtr_u8), 2: channel-quad kernel (k_ddtr_quad)
+    QuadGeometry quad{};
+    int quad_span = 0, quad_dmax = 0, quad_maxcnt = 0, nquads = 0;
+    int32_t *d_qpat = nullptr;
+    int32_t *d_qwin = nullptr;
+    int32_t *d_qoff = nullptr;
 };
 
 class DdtrPipeline {
@@ -109,6 +118,7 @@ private:
     bool check_cuda(cudaError_t e, const char *what);
     bool check_device_flags();
     bool build_range(int r);
+    bool build_quad_tables(int r);
     bool step(bool allow_sync);
     bool do_chunk_start();
     bool do_range();

@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--tile-words", type=int, default=0)
     ap.add_argument("--group-dms", type=int, default=0)
+    ap.add_argument("--variant", type=int, default=0, help="0 auto, 1 byte-phase kernel, 2 channel-quad kernel")
     return ap.parse_args()
 
 
@@ -260,6 +261,7 @@ def main():
     pipe = aa.create_pipeline(md, x.data_ptr(), device_input=True, device_output=True, copy_to_host=False,
                               stream=stream.cuda_stream, card_number=local)
     pipe.set_options(tile_words=args.tile_words, group_dms=args.group_dms)
+    pipe.set_kernel_variant(args.variant)
     plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in cfg["plan"]])
     if not pipe.bind_ddtr_plan(plan):
         raise RuntimeError(pipe.last_error())
@@ -360,8 +362,10 @@ def main():
     except OSError:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
+    kernel_names = {"quad": "k_ddtr_quad", "phase": "k_ddtr_u8"}
+    used = sorted({kernel_names.get(ri.get("kernel"), "k_ddtr_u16") for ri in ranges})
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": None, "kernel": "k_ddtr_u8",
+                "traffic": None, "kernel": "+".join(used),
                 "peak_source": "MEASURED_PEAKS.json (measured)" if "hbm_gbs" in peaks else "fallback",
                 "note": "the DDTR kernel is integer/shared-memory bound, not HBM bound; see integer_rate"}
     integer_rate = {"channel_adds_per_s": alg_adds / (dd_ms / 1e3 / (dd_n / launches_per_step)),

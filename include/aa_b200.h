@@ -231,6 +231,11 @@ const char *aa_b200_version(void);
  * free_memory 0 = query the device; tile_words/group_dms 0 = autotune. */
 bool aa_b200_pipeline_set_options(void *obj, int stride_mode, int fma_mode, int failsafe, size_t free_memory,
                                   int tile_words, int group_dms);
+/* Dedispersion kernel for one-byte data, before bind: 0 chooses per range
+ * (the channel-quad kernel where its stage fits shared memory), 1 the
+ * byte-phase kernel, 2 the channel-quad kernel (refused where it does not
+ * fit).  Both give identical results. */
+bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant);
 /* A pipeline whose input (and optionally output) stay in device memory:
  * input [nsamples][nchans] uint16 on the device when device_input != 0;
  * device_output != 0 keeps [range][dm][t] on the device
@@ -242,7 +247,8 @@ bool aa_b200_pipeline_run_all(void *obj);
 bool aa_b200_pipeline_rewind(void *obj);
 bool aa_b200_pipeline_synchronize(void *obj);
 float *aa_b200_pipeline_device_output(void *obj, int range);
-/* kind, DMs per thread block, window span (samples), time words per lane */
+/* kind (| 0x100 when the range runs the channel-quad kernel), DMs per thread
+ * block, window span (samples), time words per lane */
 int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms, int *span, int *tile_words);
 long long aa_b200_pipeline_kernel_launches(void *obj);
 const char *aa_b200_pipeline_last_error(void *obj);

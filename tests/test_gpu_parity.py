@@ -25,7 +25,7 @@ pytestmark = pytest.mark.gpu
 LIGHT = [n for n, c in C.CASES.items() if not c.get("heavy")]
 
 
-def run_pipeline(aa, case, x, stride_mode=0, **opts):
+def run_pipeline(aa, case, x, stride_mode=0, variant=0, **opts):
     md = aa.filterbank_metadata_struct(0.0, case["tsamp"], case["fch1"], case["foff"], case["nbits"],
                                        case["nsamp"], case["nchans"], 0.0)
     comps = aa.aa_py_pipeline_components(True, False, False, False)
@@ -33,6 +33,7 @@ def run_pipeline(aa, case, x, stride_mode=0, **opts):
     o.copy_ddtr_data_to_host = True
     pipe = aa.aa_py_pipeline(comps, o, md, np.ascontiguousarray(x.reshape(-1)), 0)
     pipe.set_options(stride_mode=stride_mode, free_memory=C.strategy_free_memory(case), **opts)
+    pipe.set_kernel_variant(variant)
     plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in case["plan"]])
     assert pipe.bind_ddtr_plan(plan), pipe.last_error()
     steps = 0
@@ -74,12 +75,13 @@ def assert_matches_oracle(case, s, got, want, kern):
             assert ulp.max() <= 2, f"range {r}: {ulp.max()} ulp"
 
 
+@pytest.mark.parametrize("variant", [1, 0])
 @pytest.mark.parametrize("name", LIGHT)
-def test_pipeline_matches_oracle(aa, oracle_mod, cuda_device, name):
+def test_pipeline_matches_oracle(aa, oracle_mod, cuda_device, name, variant):
     case = C.CASES[name]
     x = C.make_input(case)
     s, want, kern = oracle_run(oracle_mod, case, x)
-    got, info, steps, launches = run_pipeline(aa, case, x)
+    got, info, steps, launches = run_pipeline(aa, case, x, variant=variant)
     assert steps == s.num_tchunks * len(case["plan"]) + 1
     assert launches > 0
     for r in range(len(case["plan"])):
@@ -87,14 +89,15 @@ def test_pipeline_matches_oracle(aa, oracle_mod, cuda_device, name):
     assert_matches_oracle(case, s, got, want, kern)
 
 
+@pytest.mark.parametrize("variant", [1, 0])
 @pytest.mark.parametrize("name", list(C.CASES))
-def test_pipeline_matches_reference_gpu(aa, golden_ddtr, cuda_device, name):
+def test_pipeline_matches_reference_gpu(aa, golden_ddtr, cuda_device, name, variant):
     if name not in golden_ddtr:
         pytest.skip("case not in the golden file")
     case = C.CASES[name]
     rec = golden_ddtr[name]
     x = C.make_input(case)
-    got, _, _, _ = run_pipeline(aa, case, x)
+    got, _, _, _ = run_pipeline(aa, case, x, variant=variant)
     for r, rr in enumerate(rec["ranges"]):
         g = got[r]
         assert list(g.shape) == rr["shape"]
@@ -114,13 +117,15 @@ def test_true_stride_mode_matches_oracle(aa, oracle_mod, cuda_device, name):
     assert_matches_oracle(case, s, got, want, kern)
 
 
-@pytest.mark.parametrize("tile_words,group_dms", [(2, 64), (4, 32), (4, 16), (2, 8)])
-def test_tile_shapes_agree(aa, oracle_mod, cuda_device, tile_words, group_dms):
+@pytest.mark.parametrize("tile_words,group_dms,variant", [(2, 64, 1), (4, 32, 1), (4, 16, 1), (2, 8, 1), (2, 64, 2),
+                                                           (4, 64, 2)])
+def test_tile_shapes_agree(aa, oracle_mod, cuda_device, tile_words, group_dms, variant):
     case = C.CASES["shared8_binned"]
     x = C.make_input(case)
     s, want, kern = oracle_run(oracle_mod, case, x)
-    got, info, _, _ = run_pipeline(aa, case, x, tile_words=tile_words, group_dms=group_dms)
-    assert info[0]["tile_words"] == tile_words and info[0]["group_dms"] == group_dms
+    got, info, _, _ = run_pipeline(aa, case, x, variant=variant, tile_words=tile_words, group_dms=group_dms)
+    assert info[0]["group_dms"] == group_dms
+    assert info[0]["kernel"] == ("quad" if variant == 2 else "phase")
     assert_matches_oracle(case, s, got, want, kern)
 
 
