@@ -359,7 +359,8 @@ class aa_py_pipeline:
         if lib().aa_b200_pipeline_range_info(self.m_obj, r, ctypes.byref(k), ctypes.byref(g), ctypes.byref(s),
                                               ctypes.byref(t)):
             raise RuntimeError(self.last_error())
-        return {"kind": KIND_NAMES[k.value & 0xFF], "kernel": "quad" if k.value & 0x100 else "phase",
+        return {"kind": KIND_NAMES[k.value & 0xFF], "kernel": ("quad" if k.value & 0x100 else "f32" if k.value & 0x200 else
+                           "gather" if k.value & 0x400 else "phase"),
                 "group_dms": g.value, "span": s.value, "tile_words": t.value}
 
     def time_kernels(self, on: bool = True):

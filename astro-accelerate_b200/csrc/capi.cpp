@@ -520,7 +520,7 @@ bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant)
     if (a->pipe)
         return api_fail(a, "the kernel variant must be set before the plan is bound");
     if (variant < 0 || variant > 2)
-        return api_fail(a, "kernel variant must be 0 (auto), 1 (byte-phase) or 2 (channel-quad)");
+        return api_fail(a, "kernel variant must be 0 (auto), 1 (generic kernels) or 2 (staged kernels)");
     a->popt.kernel_variant = variant;
     return true;
 }
@@ -571,6 +571,11 @@ int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms,
         *kind |= 0x100;
         *span = rc.quad_span;
         *tile_words = rc.quad.M / 4;
+    } else if (rc.variant == 3) {
+        *kind |= 0x200;
+        *tile_words = 4;
+    } else if (rc.elem_bytes == 2) {
+        *kind |= 0x400;
     }
     return 0;
 }

@@ -1,0 +1,487 @@
+// ddtr_bodies.cuh -- the per-CTA work of the staged sm_100a dedispersion
+// kernels, as device functions shared by the one-launch-per-(chunk, range)
+// kernels (ddtr_quad.cu, ddtr_f32.cu) and the persistent multi-beam kernel
+// (ddtr_batch.cu).
+//
+// One call computes one output tile: 64 DM trials (one DM group g) x 32*M
+// samples starting at t0, of one (chunk, range) job.  Both bodies stage the
+// job's channels through shared memory in a ring of QNSTAGE slots filled by
+// 1-D TMA bulk copies that complete on one mbarrier per slot; warp 0 issues
+// the copies.  The mbarriers live in a fixed area owned by the caller, and a
+// running stage counter carries their phases from one tile to the next, so
+// a persistent CTA can run tile after tile without re-initialising them.
+// Every wait is bounded: a copy that never lands sets DERR_TIMEOUT, the rest
+// of the tile is skipped and the body returns false after it has waited, with
+// the same bound, for every copy it issued.
+//
+// 512 threads: warp w owns DM trials g*64 + 4w .. 4w+3, lane l owns outputs
+// t0 + l + 32m (m < M).
+#pragma once
+#include "ddtr_kernels.cuh"
+#include "device_util.cuh"
+
+namespace aab200 {
+namespace body {
+
+using namespace dev;
+
+constexpr int QNSTAGE = 3; // TMA ring depth
+constexpr int QDMW = 4;    // DM trials per warp
+constexpr int NTHREADS = 512;
+
+// Words of the caller-owned barrier area (QNSTAGE mbarriers + scratch).
+constexpr int BAR_WORDS = 2 * QNSTAGE + 2;
+
+__device__ __forceinline__ int output_class(int kind, long long t)
+{
+    return (kind == KIND_SHARED4) ? static_cast<int>((t & 31) >> 2) : static_cast<int>((t & 15) >> 1);
+}
+
+__device__ __forceinline__ void init_barriers(unsigned bar0)
+{
+    if (threadIdx.x == 0)
+        for (int i = 0; i < QNSTAGE; ++i)
+            mbar_init(bar0 + 8 * i, 1);
+    mbar_init_fence();
+}
+
+// ---------------------------------------------------------------------------
+// Channel-quad body (one-byte samples, integer sums with IDP4A).
+//
+// Shared memory (words from sm): qwin[nq_pad] | raw[QNSTAGE][QS*4][RAWW] |
+// ent[QNSTAGE][QS][64] | pat[QNSTAGE][QS][16] | rsh[QNSTAGE][QS*4] |
+// P[2][npool][W].
+// ---------------------------------------------------------------------------
+__host__ __device__ inline size_t quad_body_words(int qs, int group_dms, int raww, int nq_pad, int npool, int W)
+{
+    size_t o = static_cast<size_t>(nq_pad);
+    o += static_cast<size_t>(QNSTAGE) * qs * 4 * raww;
+    o += static_cast<size_t>(QNSTAGE) * qs * group_dms;
+    o += static_cast<size_t>(QNSTAGE) * qs * 16;
+    o += static_cast<size_t>(QNSTAGE) * qs * 4;
+    o = (o + 3) & ~static_cast<size_t>(3);
+    o += 2 * static_cast<size_t>(npool) * W;
+    return o;
+}
+
+template <int M>
+__device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long long t0, uint32_t *sm, unsigned bar0,
+                          unsigned &stage_ctr)
+{
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int nwarps = NTHREADS >> 5;
+    const int GD = p.group_dms;
+    const int dm0 = g * GD;
+    const int W = Q.W, RAWW = Q.raww, QS = Q.qs;
+    const unsigned char *in = static_cast<const unsigned char *>(p.in);
+    const int nstages = (Q.nquads + QS - 1) / QS;
+    const unsigned sbase = stage_ctr;
+
+    const int o_qw = 0;
+    const int o_raw = o_qw + Q.nq_pad;
+    const int o_ent = o_raw + QNSTAGE * QS * 4 * RAWW;
+    const int o_pat = o_ent + QNSTAGE * QS * GD;
+    const int o_rsh = o_pat + QNSTAGE * QS * 16;
+    const int o_P = ((o_rsh + QNSTAGE * QS * 4) + 3) & ~3;
+
+    for (int i = tid; i < (Q.nq_pad >> 2); i += NTHREADS)
+        cp_async16(&sm[o_qw + 4 * i], Q.qwin + static_cast<size_t>(g) * Q.nq_pad + 4 * i);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+
+    // warp 0: raw rows of the stage's channels, their DM offsets, patterns
+    auto issue = [&](int s) {
+        if (warp != 0 || s >= nstages)
+            return;
+        const unsigned gs = sbase + static_cast<unsigned>(s);
+        const int slot = static_cast<int>(gs % QNSTAGE);
+        const int q0 = s * QS;
+        const int nq = min(QS, Q.nquads - q0);
+        const int c0 = 4 * q0;
+        const int nrows = max(0, min(4 * nq, p.nch_used - c0));
+        const unsigned bar = bar0 + 8 * slot;
+        fence_proxy_async();
+        if (lane == 0)
+            mbar_expect_tx(bar, static_cast<unsigned>(nrows * RAWW * 4 + nq * GD * 4 + nq * 64));
+        __syncwarp();
+        if (lane < 4 * nq) {
+            const int c = c0 + lane;
+            if (lane < nrows) {
+                const int w0 = static_cast<int>(sm[o_qw + q0 + (lane >> 2)]);
+                const uintptr_t a = reinterpret_cast<uintptr_t>(in + static_cast<long long>(c) * p.stride + t0 + w0);
+                sm[o_rsh + slot * QS * 4 + lane] = static_cast<uint32_t>(a & 15);
+                tma_load_1d(smem_addr(&sm[o_raw + (slot * QS * 4 + lane) * RAWW]),
+                            reinterpret_cast<const void *>(a & ~static_cast<uintptr_t>(15)),
+                            static_cast<unsigned>(RAWW * 4), bar);
+            } else {
+                sm[o_rsh + slot * QS * 4 + lane] = 0xFFFFFFFFu; // channel contributes nothing
+            }
+        }
+        if (lane < nq)
+            tma_load_1d(smem_addr(&sm[o_ent + (slot * QS + lane) * GD]),
+                        Q.qoff + static_cast<size_t>(q0 + lane) * p.ndms + dm0, static_cast<unsigned>(GD * 4), bar);
+        if (lane == 0)
+            tma_load_1d(smem_addr(&sm[o_pat + slot * QS * 16]), Q.qpat + (static_cast<size_t>(g) * Q.nquads + q0) * 16,
+                        static_cast<unsigned>(nq * 64), bar);
+    };
+
+    bool ok = true;
+    auto wait_stage = [&](int s) -> int {
+        const unsigned gs = sbase + static_cast<unsigned>(s);
+        const int slot = static_cast<int>(gs % QNSTAGE);
+        if (!mbar_wait_bounded(bar0 + 8 * slot, (gs / QNSTAGE) & 1u)) {
+            if (ok)
+                atomicOr(p.err, DERR_TIMEOUT);
+            ok = false;
+        }
+        return slot;
+    };
+
+    // pre-skewed quad rows of stage s into P buffer b; one warp per pattern
+    // row, the lanes walk the row four words at a time
+    auto build = [&](int s, int b) {
+        const int slot = wait_stage(s);
+        const int q0 = s * QS;
+        const int nq = min(QS, Q.nquads - q0);
+        int total = 0;
+        for (int q = 0; q < nq; ++q)
+            total += static_cast<int>(sm[o_pat + (slot * QS + q) * 16 + 15]);
+        total = min(total, Q.npool);
+        const int n4 = W >> 2;
+        int q = 0, base = 0;
+        int cnt_q = (nq > 0) ? static_cast<int>(sm[o_pat + (slot * QS) * 16 + 15]) : 0;
+        for (int r = warp; r < total; r += nwarps) {
+            while (r >= base + cnt_q && q + 1 < nq) {
+                base += cnt_q;
+                ++q;
+                cnt_q = static_cast<int>(sm[o_pat + (slot * QS + q) * 16 + 15]);
+            }
+            const unsigned pw = sm[o_pat + (slot * QS + q) * 16 + (r - base)];
+            int d[4], rs[4], rb[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                d[i] = (i == 0) ? 0 : static_cast<int>((pw >> (8 * (i - 1))) & 255u);
+                rs[i] = static_cast<int>(sm[o_rsh + slot * QS * 4 + 4 * q + i]);
+                rb[i] = o_raw + (slot * QS * 4 + 4 * q + i) * RAWW;
+            }
+            const int prow = o_P + (b * Q.npool + r) * W;
+            for (int t4 = lane; t4 < n4; t4 += 32) {
+                const int tau = 4 * t4;
+                uint32_t a[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if (rs[i] < 0) {
+                        a[i] = 0u;
+                    } else {
+                        const int bb = rs[i] + tau + d[i];
+                        const int wi = rb[i] + (bb >> 2);
+                        a[i] = __funnelshift_r(sm[wi], sm[wi + 1], 8u * static_cast<unsigned>(bb & 3));
+                    }
+                }
+                // 4x4 byte transpose: word k of the result holds sample tau+k of the four channels
+                const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), hi01 = __byte_perm(a[0], a[1], 0x7362);
+                const uint32_t lo23 = __byte_perm(a[2], a[3], 0x5140), hi23 = __byte_perm(a[2], a[3], 0x7362);
+                uint4 v;
+                v.x = __byte_perm(lo01, lo23, 0x5410);
+                v.y = __byte_perm(lo01, lo23, 0x7632);
+                v.z = __byte_perm(hi01, hi23, 0x5410);
+                v.w = __byte_perm(hi01, hi23, 0x7632);
+                *reinterpret_cast<uint4 *>(&sm[prow + tau]) = v;
+            }
+        }
+    };
+
+    uint32_t acc[QDMW][M];
+#pragma unroll
+    for (int j = 0; j < QDMW; ++j)
+#pragma unroll
+        for (int m = 0; m < M; ++m)
+            acc[j][m] = 0u;
+
+    // per-byte path for one (quad, DM trial): every channel with its own class delays
+    auto slow = [&](int j, int slot, int q0, int q) {
+        const int dm = dm0 + warp * QDMW + j;
+        const int lo = static_cast<int>(sm[o_qw + q0 + q]);
+#pragma unroll 1
+        for (int i = 0; i < 4; ++i) {
+            const int c = 4 * (q0 + q) + i;
+            const int rs = static_cast<int>(sm[o_rsh + slot * QS * 4 + 4 * q + i]);
+            if (c >= p.nch_used || rs < 0)
+                continue;
+            const int rb = o_raw + (slot * QS * 4 + 4 * q + i) * RAWW;
+            const int ee = p.table[static_cast<size_t>(c) * p.ndms + dm];
+            const int dd = (ee & 0xFFFFFF) - lo;
+            const unsigned mask = static_cast<unsigned>(ee) >> 24;
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                const int tl = lane + 32 * m;
+                const int o = dd + static_cast<int>((mask >> output_class(p.kind, t0 + tl)) & 1u) + tl;
+                const int bb = rs + o;
+                if (o < 0 || bb >= RAWW * 4) {
+                    atomicOr(p.err, DERR_WINDOW);
+                    continue;
+                }
+                acc[j][m] += (sm[rb + (bb >> 2)] >> (8u * static_cast<unsigned>(bb & 3))) & 255u;
+            }
+        }
+    };
+
+#pragma unroll
+    for (int s = 0; s < QNSTAGE - 1; ++s)
+        issue(s);
+    __syncthreads(); // raw-row shifts written by warp 0 become visible
+    if (nstages > 0)
+        build(0, 0);
+    fence_proxy_async();
+    __syncthreads();
+    issue(QNSTAGE - 1);
+
+    for (int s = 0; s < nstages; ++s) {
+        if (s + 1 < nstages)
+            build(s + 1, (s + 1) & 1);
+        const int slot = static_cast<int>((sbase + static_cast<unsigned>(s)) % QNSTAGE);
+        const int q0 = s * QS;
+        const int nq = min(QS, Q.nquads - q0);
+        if (ok) {
+            int rbase = 0;
+            for (int q = 0; q < nq; ++q) {
+                const int4 e4 = *reinterpret_cast<const int4 *>(&sm[o_ent + (slot * QS + q) * GD + warp * QDMW]);
+                const int prow = o_P + ((s & 1) * Q.npool + rbase) * W + lane;
+                const int ej[QDMW] = {e4.x, e4.y, e4.z, e4.w};
+                if ((e4.x | e4.y | e4.z | e4.w) >= 0) {
+#pragma unroll
+                    for (int j = 0; j < QDMW; ++j) {
+                        uint32_t w[M];
+#pragma unroll
+                        for (int m = 0; m < M; ++m)
+                            w[m] = sm[prow + ej[j] + 32 * m];
+#pragma unroll
+                        for (int m = 0; m < M; ++m)
+                            acc[j][m] = __dp4a(w[m], 0x01010101u, acc[j][m]);
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < QDMW; ++j) {
+                        if (ej[j] >= 0) {
+#pragma unroll
+                            for (int m = 0; m < M; ++m)
+                                acc[j][m] = __dp4a(sm[prow + ej[j] + 32 * m], 0x01010101u, acc[j][m]);
+                        } else {
+                            slow(j, slot, q0, q);
+                        }
+                    }
+                }
+                rbase += static_cast<int>(sm[o_pat + (slot * QS + q) * 16 + 15]);
+            }
+        }
+        fence_proxy_async();
+        __syncthreads();
+        issue(s + QNSTAGE);
+    }
+    stage_ctr = sbase + static_cast<unsigned>(nstages);
+    if (!ok)
+        return false;
+
+    // (float)S / nchans / bin, the reference's expression (4-bit: / nchans)
+#pragma unroll
+    for (int j = 0; j < QDMW; ++j) {
+        const int dm = dm0 + warp * QDMW + j;
+        if (dm >= p.ndms)
+            continue;
+        float *orow = p.out + static_cast<long long>(dm) * p.out_pitch;
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            const long long t = t0 + lane + 32 * m;
+            if (t < p.tp) {
+                const float v = static_cast<float>(static_cast<int>(acc[j][m]));
+                orow[t] = p.divide_by_bin ? (v / p.nchans_f / p.bin_f) : (v / p.nchans_f);
+            }
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// fp32 body (two-byte samples): the reference's 16-bit kernel accumulates
+// (float)sample in channel order with IEEE single additions
+// (src/aa_device_dedispersion_kernel.cu:303-362); the order is kept, so the
+// sums round exactly as there.  The staged raw rows are converted once into
+// float rows, and every lane adds its outputs channel by channel.
+//
+// Shared memory (words from sm): wm[nch_pad] | ent[QNSTAGE][CS][64] |
+// rsh[QNSTAGE][CS] | raw[QNSTAGE][CS][RAWH/2] | F[2][CS][W].
+// ---------------------------------------------------------------------------
+__host__ __device__ inline size_t f32_body_words(int cs, int group_dms, int rawh, int nch_pad, int W)
+{
+    size_t o = static_cast<size_t>(nch_pad);
+    o += static_cast<size_t>(QNSTAGE) * cs * group_dms;
+    o += static_cast<size_t>(QNSTAGE) * cs;
+    o = (o + 3) & ~static_cast<size_t>(3);
+    o += static_cast<size_t>(QNSTAGE) * cs * (rawh >> 1);
+    o += 2 * static_cast<size_t>(cs) * W;
+    return o;
+}
+
+template <int M>
+__device__ bool f32_body(const DdtrLaunch &p, const F32Launch &F, int g, long long t0, uint32_t *sm, unsigned bar0,
+                         unsigned &stage_ctr)
+{
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int GD = p.group_dms;
+    const int dm0 = g * GD;
+    const int CS = F.cs, W = F.W, RW = F.rawh >> 1;
+    const uint16_t *in = static_cast<const uint16_t *>(p.in);
+    const int nstages = (p.nch_used + CS - 1) / CS;
+    const unsigned sbase = stage_ctr;
+
+    const int o_wm = 0;
+    const int o_ent = o_wm + F.nch_pad;
+    const int o_rsh = o_ent + QNSTAGE * CS * GD;
+    const int o_raw = ((o_rsh + QNSTAGE * CS) + 3) & ~3;
+    const int o_F = o_raw + QNSTAGE * CS * RW;
+    float *fsm = reinterpret_cast<float *>(sm);
+
+    for (int i = tid; i < (F.nch_pad >> 2); i += NTHREADS)
+        cp_async16(&sm[o_wm + 4 * i], p.wmin + static_cast<size_t>(g) * F.nch_pad + 4 * i);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+
+    auto issue = [&](int s) {
+        if (warp != 0 || s >= nstages)
+            return;
+        const unsigned gs = sbase + static_cast<unsigned>(s);
+        const int slot = static_cast<int>(gs % QNSTAGE);
+        const int c0 = s * CS;
+        const int nrows = min(CS, p.nch_used - c0);
+        const unsigned bar = bar0 + 8 * slot;
+        fence_proxy_async();
+        if (lane == 0)
+            mbar_expect_tx(bar, static_cast<unsigned>(nrows * (RW * 4 + GD * 4)));
+        __syncwarp();
+        if (lane < nrows) {
+            const int c = c0 + lane;
+            const int w0 = static_cast<int>(sm[o_wm + c]);
+            const uintptr_t a = reinterpret_cast<uintptr_t>(in + static_cast<long long>(c) * p.stride + t0 + w0);
+            sm[o_rsh + slot * CS + lane] = static_cast<uint32_t>((a & 15) >> 1);
+            tma_load_1d(smem_addr(&sm[o_raw + (slot * CS + lane) * RW]),
+                        reinterpret_cast<const void *>(a & ~static_cast<uintptr_t>(15)), static_cast<unsigned>(RW * 4),
+                        bar);
+            tma_load_1d(smem_addr(&sm[o_ent + (slot * CS + lane) * GD]), p.table + static_cast<size_t>(c) * p.ndms + dm0,
+                        static_cast<unsigned>(GD * 4), bar);
+        }
+    };
+
+    bool ok = true;
+    // raw rows of stage s -> float rows of buffer b: CS/16 rows per warp or
+    // 16/CS warps per row
+    auto build = [&](int s, int b) {
+        const unsigned gs = sbase + static_cast<unsigned>(s);
+        const int slot = static_cast<int>(gs % QNSTAGE);
+        if (!mbar_wait_bounded(bar0 + 8 * slot, (gs / QNSTAGE) & 1u)) {
+            if (ok)
+                atomicOr(p.err, DERR_TIMEOUT);
+            ok = false;
+        }
+        const int nrows = min(CS, p.nch_used - s * CS);
+        const int wpr = (CS >= 16) ? 1 : (16 / CS);
+        const int rows_per_warp = (CS >= 16) ? (CS / 16) : 1;
+        const int sub = warp % wpr;
+        const int n4 = W >> 2;
+        for (int k = 0; k < rows_per_warp; ++k) {
+            const int ci = (warp / wpr) * rows_per_warp + k;
+            if (ci >= nrows)
+                break;
+            const uint16_t *r16 = reinterpret_cast<const uint16_t *>(&sm[o_raw + (slot * CS + ci) * RW]) +
+                                  sm[o_rsh + slot * CS + ci];
+            float *frow = fsm + o_F + (b * CS + ci) * W;
+            for (int x4 = sub * 32 + lane; x4 < n4; x4 += wpr * 32) {
+                float4 v;
+                v.x = __uint2float_rn(r16[4 * x4 + 0]);
+                v.y = __uint2float_rn(r16[4 * x4 + 1]);
+                v.z = __uint2float_rn(r16[4 * x4 + 2]);
+                v.w = __uint2float_rn(r16[4 * x4 + 3]);
+                *reinterpret_cast<float4 *>(frow + 4 * x4) = v;
+            }
+        }
+    };
+
+    float acc[QDMW][M];
+#pragma unroll
+    for (int j = 0; j < QDMW; ++j)
+#pragma unroll
+        for (int m = 0; m < M; ++m)
+            acc[j][m] = 0.f;
+    // class of output t0 + lane + 32m (t0 and 32m are multiples of 32)
+    const int cls = output_class(p.kind, lane);
+    const int omax = W - 32 * M; // largest offset whose last read stays in the row
+
+#pragma unroll
+    for (int s = 0; s < QNSTAGE - 1; ++s)
+        issue(s);
+    __syncthreads();
+    if (nstages > 0)
+        build(0, 0);
+    fence_proxy_async();
+    __syncthreads();
+    issue(QNSTAGE - 1);
+
+    for (int s = 0; s < nstages; ++s) {
+        if (s + 1 < nstages)
+            build(s + 1, (s + 1) & 1);
+        const int slot = static_cast<int>((sbase + static_cast<unsigned>(s)) % QNSTAGE);
+        const int c0 = s * CS;
+        const int nrows = min(CS, p.nch_used - c0);
+        if (ok) {
+            for (int ci = 0; ci < nrows; ++ci) { // channel order: the reference's summation order
+                const int w = static_cast<int>(sm[o_wm + c0 + ci]);
+                const int4 e4 = *reinterpret_cast<const int4 *>(&sm[o_ent + (slot * CS + ci) * GD + warp * QDMW]);
+                const int ej[QDMW] = {e4.x, e4.y, e4.z, e4.w};
+                const float *frow = fsm + o_F + ((s & 1) * CS + ci) * W + lane;
+#pragma unroll
+                for (int j = 0; j < QDMW; ++j) {
+                    const int e = ej[j];
+                    int o = (e & 0xFFFFFF) - w + static_cast<int>((static_cast<unsigned>(e) >> (24 + cls)) & 1u);
+                    if (o < 0 || o > omax) {
+                        atomicOr(p.err, DERR_WINDOW);
+                        o = 0;
+                    }
+                    float v[M];
+#pragma unroll
+                    for (int m = 0; m < M; ++m)
+                        v[m] = frow[o + 32 * m];
+#pragma unroll
+                    for (int m = 0; m < M; ++m)
+                        acc[j][m] = __fadd_rn(acc[j][m], v[m]);
+                }
+            }
+        }
+        fence_proxy_async();
+        __syncthreads();
+        issue(s + QNSTAGE);
+    }
+    stage_ctr = sbase + static_cast<unsigned>(nstages);
+    if (!ok)
+        return false;
+
+#pragma unroll
+    for (int j = 0; j < QDMW; ++j) {
+        const int dm = dm0 + warp * QDMW + j;
+        if (dm >= p.ndms)
+            continue;
+        float *orow = p.out + static_cast<long long>(dm) * p.out_pitch;
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            const long long t = t0 + lane + 32 * m;
+            if (t < p.tp)
+                orow[t] = p.divide_by_bin ? (acc[j][m] / p.nchans_f / p.bin_f) : (acc[j][m] / p.nchans_f);
+        }
+    }
+    return true;
+}
+
+} // namespace body
+} // namespace aab200

@@ -194,8 +194,10 @@ __global__ void __launch_bounds__(256) k_corner_turn(const uint16_t *__restrict_
 // Reference x2 binning as it acts on the flat buffer (bin + swap,
 // src/aa_device_binning_kernel.cu:33-45, src/aa_device_corner_turn_kernel.cu:91-98):
 // (a+b)/2.0f truncated back to the integer type is (a+b)>>1.
-// For nsamp % 16 == 0 rows of the binned output start on 8-element
-// boundaries, so each thread writes 8 elements of one row.
+// When nchans and nsamp are multiples of 32 the reference's grids cover the
+// whole buffer: dst[0, nchans*nsamp/2) = binned, dst[.., nchans*nsamp) = 0,
+// and rows of the binned output start on 8-element boundaries, so each thread
+// writes 8 elements of one row.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_bin_flat(const T *__restrict__ src, T *__restrict__ dst, long long nchans,
@@ -225,22 +227,38 @@ __global__ void k_bin_flat(const T *__restrict__ src, T *__restrict__ dst, long 
         dst[i0 + k] = v[k];
 }
 
-// Same semantics, one element per thread, for binning lengths that are not a
-// multiple of 16 (rows of the binned output then start off the 8-element grid).
+// The general case, one element per thread.  The reference's bin kernel runs
+// on a grid of 32-channel x 8-sample blocks, (nsamp+1)/16 blocks in time and
+// nchans/32 in frequency (src/aa_bin_gpu.cpp:10-14), so it bins channels
+// c < 32*floor(nchans/32) and output samples t < 8*floor((nsamp+1)/16) into a
+// zeroed float buffer; its swap kernel runs on 32 x 8 blocks
+// (src/aa_bin_gpu.cpp:25-28) and copies that buffer back, in place, only for
+// flat positions c*nsamp + t with c < 8*floor(nchans/8) and
+// t < 32*floor(nsamp/32).  Positions the swap does not reach keep the
+// unbinned input.  nsamp must be even (the runner's lengths always are).
 template <typename T>
-__global__ void k_bin_flat_scalar(const T *__restrict__ src, T *__restrict__ dst, long long nchans,
-                                  long long nsamp)
+__global__ void k_bin_flat_general(const T *__restrict__ src, T *__restrict__ dst, long long nchans,
+                                   long long nsamp)
 {
-    const long long half = nsamp / 2;
+    const long long n = nchans * nsamp;
     const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= nchans * nsamp)
+    if (i >= n)
         return;
-    T v = 0;
-    if (i < nchans * half) {
-        const long long c = i / half;
-        const long long t = i - c * half;
-        const T *s = src + c * nsamp + 2 * t;
-        v = static_cast<T>((static_cast<unsigned>(s[0]) + static_cast<unsigned>(s[1])) >> 1);
+    const long long half = nsamp / 2;
+    const long long c = i / nsamp;
+    const long long t = i - c * nsamp;
+    T v;
+    if (c < 8 * (nchans / 8) && t < 32 * (nsamp / 32)) {
+        const long long c2 = i / half;
+        const long long t2 = i - c2 * half;
+        v = 0;
+        if (c2 < 32 * (nchans / 32) && t2 < 8 * ((nsamp + 1) / 16)) {
+            const long long s0 = c2 * nsamp + 2 * t2;
+            if (s0 + 1 < n)
+                v = static_cast<T>((static_cast<unsigned>(src[s0]) + static_cast<unsigned>(src[s0 + 1])) >> 1);
+        }
+    } else {
+        v = src[i];
     }
     dst[i] = v;
 }
@@ -611,14 +629,16 @@ cudaError_t launch_bin_flat(const void *src, void *dst, int elem_bytes, int ncha
                             cudaStream_t st)
 {
     const long long ntot = static_cast<long long>(nchans) * nsamp;
-    if (nsamp % 16) {
+    if (nsamp < 2 || (nsamp & 1) || nchans < 1)
+        return cudaErrorInvalidValue;
+    if ((nsamp % 32) || (nchans % 32)) {
         const unsigned b = static_cast<unsigned>((ntot + 255) / 256);
         if (elem_bytes == 1)
-            k_bin_flat_scalar<uint8_t><<<b, 256, 0, st>>>(static_cast<const uint8_t *>(src),
-                                                           static_cast<uint8_t *>(dst), nchans, nsamp);
+            k_bin_flat_general<uint8_t><<<b, 256, 0, st>>>(static_cast<const uint8_t *>(src),
+                                                            static_cast<uint8_t *>(dst), nchans, nsamp);
         else
-            k_bin_flat_scalar<uint16_t><<<b, 256, 0, st>>>(static_cast<const uint16_t *>(src),
-                                                            static_cast<uint16_t *>(dst), nchans, nsamp);
+            k_bin_flat_general<uint16_t><<<b, 256, 0, st>>>(static_cast<const uint16_t *>(src),
+                                                             static_cast<uint16_t *>(dst), nchans, nsamp);
         return cudaGetLastError();
     }
     const long long nthreads = (ntot + 7) / 8;

@@ -66,8 +66,11 @@ cudaError_t launch_corner_turn(const uint16_t *in_tc, void *out_ct, int elem_byt
                                long long nsamp, long long out_stride, int max_value, int *err,
                                cudaStream_t st);
 
-// Reference x2 binning on the flat buffer (src/aa_bin_gpu.cpp:8-44):
-// dst[0, nchans*nsamp/2) = binned [c][nsamp/2], dst[.., nchans*nsamp) = 0.
+// Reference x2 binning on the flat buffer (src/aa_bin_gpu.cpp:8-44), out of
+// place: for nchans and nsamp multiples of 32, dst[0, nchans*nsamp/2) = binned
+// [c][nsamp/2] and dst[.., nchans*nsamp) = 0; otherwise the reference grids'
+// partial coverage (channels beyond 32*floor(nchans/32) are not binned,
+// positions its copy-back does not reach keep src).  nsamp must be even.
 cudaError_t launch_bin_flat(const void *src, void *dst, int elem_bytes, int nchans, long long nsamp,
                             cudaStream_t st);
 
@@ -105,5 +108,23 @@ cudaError_t launch_quad_patterns(const int32_t *table, int nch_used, int ndms, i
                                  int32_t *qpat, int32_t *qwin, int32_t *qtmp, int *stats, cudaStream_t st);
 cudaError_t launch_quad_offsets(const int32_t *qtmp, size_t n, int W, int32_t *qoff, cudaStream_t st);
 cudaError_t launch_ddtr_quad(const DdtrLaunch &p, const QuadLaunch &q, cudaStream_t st);
+
+// Staged fp32 kernel for two-byte samples (ddtr_f32.cu).
+struct F32Launch {
+    int cs;      // channels per stage (4, 8, 16 or 32)
+    int W;       // floats per converted row (multiple of 4, >= span + 32*M)
+    int rawh;    // samples per staged raw row (multiple of 8, >= W + 8)
+    int nch_pad; // channels rounded up to 4 (row length of the window table)
+};
+
+struct F32Geometry {
+    F32Launch f;
+    size_t smem_bytes;
+};
+
+// Geometry for a delay span; cs = 0 picks the largest stage that fits the
+// shared-memory limit.  smem_bytes = 0 when nothing fits.
+F32Geometry f32_geometry(int span, int group_dms, int nchans, int cs);
+cudaError_t launch_ddtr_f32(const DdtrLaunch &p, const F32Launch &f, cudaStream_t st);
 
 } // namespace aab200

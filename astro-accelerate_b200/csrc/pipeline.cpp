@@ -130,6 +130,15 @@ bool DdtrPipeline::build_range(int r)
         if (!build_quad_tables(r))
             return false;
     }
+    if (elem_bytes_ == 2 && opt_.kernel_variant != 1 && rc.group_dms == 64 && nchans <= 16384) {
+        const F32Geometry G = f32_geometry(rc.span, rc.group_dms, nchans, 0);
+        if (G.smem_bytes > 0) {
+            rc.f32 = G.f;
+            rc.variant = 3;
+        } else if (opt_.kernel_variant == 2) {
+            return fail("the staged fp32 kernel does not fit range " + std::to_string(r));
+        }
+    }
     if (elem_bytes_ == 1) {
         if (!check_cuda(cudaMalloc(&rc.d_offtab, nent * sizeof(int32_t)), "cudaMalloc(offset table)"))
             return false;
@@ -334,6 +343,7 @@ bool DdtrPipeline::setup()
         delay_max = std::max(delay_max, ranges_[r].delay_max);
         rawb_max = std::max(rawb_max, 4 * ddtr_u8_rw(ranges_[r].span, ranges_[r].tile_words) + 32);
         rawb_max = std::max(rawb_max, 4 * ranges_[r].quad.raww + 64);
+        rawb_max = std::max(rawb_max, ranges_[r].f32.rawh + 16);
     }
 
     const long long L0 = static_cast<long long>(strategy_.t_processed()[0][0]) + strategy_.maxshift();
@@ -509,7 +519,7 @@ bool DdtrPipeline::do_range()
         i_nsamp = cur_stride_;
     }
 
-    const int tile = (rc.variant == 2) ? 32 * rc.quad.M : 128 * rc.tile_words;
+    const int tile = (rc.variant == 2) ? 32 * rc.quad.M : (rc.variant == 3 ? 512 : 128 * rc.tile_words);
     long long need;
     if (elem_bytes_ == 1 && rc.variant == 2)
         need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ((tp + tile - 1) / tile) * static_cast<long long>(tile) +
@@ -517,6 +527,9 @@ bool DdtrPipeline::do_range()
     else if (elem_bytes_ == 1)
         need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ((tp + tile - 1) / tile) * static_cast<long long>(tile) +
                rc.delay_max + 4LL * ddtr_u8_rw(rc.span, rc.tile_words) + 64;
+    else if (rc.variant == 3)
+        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ((tp + tile - 1) / tile) * static_cast<long long>(tile) +
+               rc.delay_max + rc.f32.rawh + 8;
     else
         need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + tp + rc.delay_max + 2;
     if (need > static_cast<long long>(flat_elems_))
@@ -549,7 +562,7 @@ bool DdtrPipeline::do_range()
         p.out = d_tile_[slot];
         p.out_pitch = tp;
     }
-    if (rc.variant != 2 && ((reinterpret_cast<uintptr_t>(p.out) & 15) || (p.out_pitch & 3) || (tp & 3)))
+    if (rc.variant == 1 && elem_bytes_ == 1 && ((reinterpret_cast<uintptr_t>(p.out) & 15) || (p.out_pitch & 3) || (tp & 3)))
         return fail("output rows are not 16-byte aligned");
     if (!timed_launch_begin(KF_DDTR))
         return false;
@@ -567,6 +580,8 @@ bool DdtrPipeline::do_range()
         q.npool = rc.quad.npool;
         q.M = rc.quad.M;
         e = launch_ddtr_quad(p, q, st_);
+    } else if (rc.variant == 3) {
+        e = launch_ddtr_f32(p, rc.f32, st_);
     } else {
         e = (elem_bytes_ == 1) ? launch_ddtr_u8(p, rc.d_offtab, rc.tile_words, st_) : launch_ddtr_u16(p, st_);
     }

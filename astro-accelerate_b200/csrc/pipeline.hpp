@@ -40,7 +40,7 @@ struct PipelineOptions {
     int failsafe = 0;           // force the cache-kernel delay semantics
     size_t free_memory = 0;     // 0: query the device like aa_device_info::free_memory()
     int tile_words = 0;         // 0: autotune
-    int kernel_variant = 0;     // 0: autotune, 1: byte-phase kernel, 2: channel-quad kernel
+    int kernel_variant = 0;     // 0: autotune, 1: generic kernels, 2: staged kernels (channel-quad / fp32)
     int group_dms = 0;          // 0: autotune
     bool device_input = false;  // the input pointer is device memory ([t][c] uint16)
     bool device_output = false; // keep the whole output on the device ([range][dm][t])
@@ -66,12 +66,16 @@ struct RangeConfig {
     int32_t *d_wmin = nullptr;
     int32_t *d_offtab = nullptr;
     // channel-quad kernel
-    int variant = 1;            // 1: byte-phase kernel (k_ddtr_u8), 2: channel-quad kernel (k_ddtr_quad)
+    // 1: generic kernel (k_ddtr_u8 byte-phase / k_ddtr_u16 gather), 2: channel-quad
+    // kernel (k_ddtr_quad, one-byte data), 3: staged fp32 kernel (k_ddtr_f32, two-byte data)
+    int variant = 1;
     QuadGeometry quad{};
     int quad_span = 0, quad_dmax = 0, quad_maxcnt = 0, nquads = 0;
     int32_t *d_qpat = nullptr;
     int32_t *d_qwin = nullptr;
     int32_t *d_qoff = nullptr;
+    // staged fp32 kernel
+    F32Launch f32{};
 };
 
 class DdtrPipeline {

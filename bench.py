@@ -60,7 +60,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--tile-words", type=int, default=0)
     ap.add_argument("--group-dms", type=int, default=0)
-    ap.add_argument("--variant", type=int, default=0, help="0 auto, 1 byte-phase kernel, 2 channel-quad kernel")
+    ap.add_argument("--variant", type=int, default=0, help="0 auto, 1 generic kernels, 2 staged kernels")
+    ap.add_argument("--nbits", type=int, default=0, help="bit depth of the synthetic filterbank (default: the config's)")
     return ap.parse_args()
 
 
@@ -72,19 +73,21 @@ def synth_input_device(cfg, seed, device):
     nchans, nsamp = cfg["nchans"], cfg["nsamp"]
     g = torch.Generator(device=device)
     g.manual_seed(seed)
+    vmax = (1 << min(cfg["nbits"], 16)) - 1
+    mid, sig = (vmax + 1) / 2.0 - 0.5, (vmax + 1) / 16.0
     x = torch.empty((nsamp, nchans), dtype=torch.int16, device=device)
     rows = 1 << 16
     for t0 in range(0, nsamp, rows):
         n = min(rows, nsamp - t0)
-        v = torch.randn((n, nchans), generator=g, device=device) * 16.0 + 127.5
-        x[t0:t0 + n] = v.round_().clamp_(0, 255).to(torch.int16)
+        v = torch.randn((n, nchans), generator=g, device=device) * sig + mid
+        x[t0:t0 + n] = v.round_().clamp_(0, vmax).to(torch.int32).to(torch.int16)
     rng = np.random.Generator(np.random.PCG64(seed))
     f = cfg["fch1"] + cfg["foff"] * np.arange(nchans, dtype=np.float64)
     pulses = []
     for _ in range(cfg["npulses"]):
         dm = float(rng.uniform(50, 2900)) if len(cfg["plan"]) > 1 else 300.0
         width = max(1, int(round(math.exp(rng.uniform(math.log(0.25), math.log(8.0))) * 1e-3 / cfg["tsamp"])))
-        amp = float(rng.uniform(3, 10)) * 16.0
+        amp = float(rng.uniform(3, 10)) * sig
         start = int(rng.integers(0, nsamp // 2))
         d = np.floor(4.148808e3 * dm * (f ** -2 - cfg["fch1"] ** -2) / cfg["tsamp"]).astype(np.int64)
         tt = (start + d[None, :] + np.arange(width)[:, None])
@@ -92,9 +95,9 @@ def synth_input_device(cfg, seed, device):
         ok = tt < nsamp
         ti = torch.as_tensor(tt[ok], device=device)
         ci = torch.as_tensor(cc[ok], device=device)
-        vals = (x[ti, ci].to(torch.float32) + amp).clamp_(0, 255).to(torch.int16)
-        x[ti, ci] = vals
-        pulses.append(dict(dm=dm, width=width, amp_sigma=amp / 16.0, start=start))
+        vals = ((x[ti, ci].to(torch.int32) & 0xFFFF).to(torch.float32) + amp).clamp_(0, vmax)
+        x[ti, ci] = vals.to(torch.int32).to(torch.int16)
+        pulses.append(dict(dm=dm, width=width, amp_sigma=amp / sig, start=start))
     torch.cuda.synchronize(device)
     return x, pulses
 
@@ -218,7 +221,8 @@ def run_reference_arm(args, cfg, rank, world):
 
 
 def workload_config(cfg):
-    name = "survey-scale plain DDTR" if cfg is SURVEY else "reduced plain DDTR"
+    full = cfg["nsamp"] == SURVEY["nsamp"] and cfg["nchans"] == SURVEY["nchans"] and cfg["nbits"] == 8
+    name = "survey-scale plain DDTR" if full else "reduced plain DDTR"
     return {"workload": f"{name}: {cfg['nchans']} ch x {cfg['nsamp']} samples, {cfg['nbits']}-bit, "
                         f"{len(cfg['plan'])}-range plan to DM {cfg['plan'][-1][1]}",
             "nchans": cfg["nchans"], "nsamp": cfg["nsamp"], "nbits": cfg["nbits"], "tsamp": cfg["tsamp"],
@@ -229,6 +233,8 @@ def workload_config(cfg):
 def main():
     args = parse()
     cfg = {"survey": SURVEY, "mid": MID, "small": SMALL}[args.config]
+    if args.nbits:
+        cfg = dict(cfg, nbits=args.nbits)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -362,8 +368,8 @@ def main():
     except OSError:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
-    kernel_names = {"quad": "k_ddtr_quad", "phase": "k_ddtr_u8"}
-    used = sorted({kernel_names.get(ri.get("kernel"), "k_ddtr_u16") for ri in ranges})
+    kernel_names = {"quad": "k_ddtr_quad", "phase": "k_ddtr_u8", "f32": "k_ddtr_f32", "gather": "k_ddtr_u16"}
+    used = sorted({kernel_names[ri["kernel"]] for ri in ranges})
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": None, "kernel": "+".join(used),
                 "peak_source": "MEASURED_PEAKS.json (measured)" if "hbm_gbs" in peaks else "fallback",
@@ -378,7 +384,7 @@ def main():
         result = {
             "metric": METRIC, "value": value, "unit": "DM-trial*samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u8", "data": "synthetic", "config": workload_config(cfg),
+            "vs_baseline": None, "dtype": "u8" if cfg["nbits"] <= 8 else "f32", "data": "synthetic", "config": workload_config(cfg),
             "realtime_x": sum(strat["t_processed"][0]) * cfg["tsamp"] / (ms_step / 1e3),
             "published_realtime_x": PUBLISHED_REALTIME,
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "integer_rate": integer_rate,

@@ -231,10 +231,11 @@ const char *aa_b200_version(void);
  * free_memory 0 = query the device; tile_words/group_dms 0 = autotune. */
 bool aa_b200_pipeline_set_options(void *obj, int stride_mode, int fma_mode, int failsafe, size_t free_memory,
                                   int tile_words, int group_dms);
-/* Dedispersion kernel for one-byte data, before bind: 0 chooses per range
- * (the channel-quad kernel where its stage fits shared memory), 1 the
- * byte-phase kernel, 2 the channel-quad kernel (refused where it does not
- * fit).  Both give identical results. */
+/* Dedispersion kernels, before bind: 0 chooses per range (the staged kernel
+ * where its stage fits shared memory), 1 the generic kernels (byte-phase for
+ * one-byte data, a global-memory gather for two-byte data), 2 the staged
+ * kernels (channel-quad for one-byte data, TMA-staged fp32 for two-byte
+ * data; refused where they do not fit).  All give identical results. */
 bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant);
 /* A pipeline whose input (and optionally output) stay in device memory:
  * input [nsamples][nchans] uint16 on the device when device_input != 0;
@@ -247,7 +248,8 @@ bool aa_b200_pipeline_run_all(void *obj);
 bool aa_b200_pipeline_rewind(void *obj);
 bool aa_b200_pipeline_synchronize(void *obj);
 float *aa_b200_pipeline_device_output(void *obj, int range);
-/* kind (| 0x100 when the range runs the channel-quad kernel), DMs per thread
+/* kind (| 0x100 when the range runs the channel-quad kernel, | 0x200 for the
+ * staged fp32 kernel, | 0x400 for the two-byte gather kernel), DMs per thread
  * block, window span (samples), time words per lane */
 int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms, int *span, int *tile_words);
 long long aa_b200_pipeline_kernel_launches(void *obj);

@@ -52,6 +52,10 @@ CASES = {
     "shared16": dict(nchans=1024, nbits=16, fch1=1670.0, foff=-0.29296875, tsamp=64e-6, nsamp=1 << 14,
                      plan=[(0, 6.3, 0.1, 1, 1), (6.4, 19.1, 0.2, 2, 1)], free_memory=0, seed=18,
                      pulses=[(10.0, 8, 3.0)]),
+    # 16-bit, 1000 channels (stages end mid-row), two binning steps, three time chunks
+    "shared16_ragged": dict(nchans=1000, nbits=16, fch1=1670.0, foff=-0.3, tsamp=64e-6, nsamp=1 << 15,
+                            plan=[(0, 6.3, 0.1, 1, 1), (6.4, 19.1, 0.2, 2, 1), (19.2, 44.7, 0.4, 4, 1)],
+                            free_memory=104857600 + 9000 * 1000 * 10, seed=22, pulses=[(12.0, 8, 3.0)]),
     # 16-bit data on the cache kernel
     "cache16": dict(nchans=512, nbits=16, fch1=1550.0, foff=-0.78125, tsamp=64e-6, nsamp=1 << 14,
                     plan=[(0, 63, 0.5, 1, 1)], free_memory=0, seed=19, pulses=[(30.0, 8, 3.0)]),

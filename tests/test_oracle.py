@@ -118,4 +118,6 @@ def test_oracle_matches_reference_gpu(oracle_mod, golden_ddtr, name):
         else:
             for i, j, bits in rr["samples"]:
                 ref = np.uint32(bits).view(np.float32)
-                assert np.rint(float(outs[r][i, j]) * div) == np.rint(float(ref) * div)
+                if abs(float(ref) * div) < 2**24:  # integer sums; fp32 sums of 16-bit data above 2^24 are rounded
+                    assert np.rint(float(outs[r][i, j]) * div) == np.rint(float(ref) * div)
+                assert abs(int(outs[r][i, j].view(np.int32)) - int(np.int32(bits))) <= 2
