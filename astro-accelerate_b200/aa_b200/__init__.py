@@ -148,6 +148,18 @@ def lib():
         "aa_b200_pipeline_time_kernels": ([vp, i], b),
         "aa_b200_pipeline_kernel_time": ([vp, i, P(d), P(ll)], i),
         "aa_b200_pipeline_reset_kernel_times": ([vp], b),
+        "aa_b200_batch_create": ([i, i, sz, i, i, i, vp], vp),
+        "aa_b200_batch_add_beam": ([vp, filterbank_metadata_struct, vp, vp], i),
+        "aa_b200_batch_setup": ([vp], b),
+        "aa_b200_batch_run": ([vp], b),
+        "aa_b200_batch_synchronize": ([vp], b),
+        "aa_b200_batch_device_output": ([vp, i, i], vp),
+        "aa_b200_batch_range_shape": ([vp, i, i, P(i), P(ll), P(i)], i),
+        "aa_b200_batch_info": ([vp, P(ll), P(i), P(i), P(i), P(sz), P(sz), P(ll)], i),
+        "aa_b200_batch_last_ms": ([vp, i], d),
+        "aa_b200_batch_estimate_bytes": ([filterbank_metadata_struct, vp, sz, P(sz)], i),
+        "aa_b200_batch_last_error": ([vp], ctypes.c_char_p),
+        "aa_b200_batch_delete": ([vp], None),
     }
     for name, (args, res) in protos.items():
         fn = getattr(L, name)
@@ -497,3 +509,92 @@ def dedisperse(i, t_processed, inBin, dmshifts, d_input, i_nsamp, d_input_elems,
                                   nbits, failsafe, stream)
     if rc:
         raise RuntimeError(last_error())
+
+
+# ---------------------------------------------------------------------------
+# Multi-beam batch (one CUDA graph, one persistent dedispersion kernel)
+# ---------------------------------------------------------------------------
+class _DeviceRows:
+    """__cuda_array_interface__ of a float32 device array owned by the library."""
+
+    def __init__(self, ptr: int, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f4", "data": (ptr, False),
+                                         "version": 2, "strides": None}
+
+
+class batch:
+    """Many beams' DDTR in one graph (aa_b200_batch_*).  Inputs are
+    [nsamples][nchans] uint16 device buffers (torch tensors or pointers) that
+    must stay alive while the batch runs."""
+
+    def __init__(self, stride_mode: int = STRIDE_REFERENCE, fma_mode: int = 7, free_memory: int = 0,
+                 persistent: bool = True, use_graph: bool = True, autotune: bool = True, stream: int = 0):
+        self.m_obj = lib().aa_b200_batch_create(stride_mode, fma_mode, free_memory, int(persistent), int(use_graph),
+                                                int(autotune), ctypes.c_void_p(stream))
+        if not self.m_obj:
+            raise RuntimeError(self.last_error())
+        self._keep = []
+
+    def last_error(self) -> str:
+        m = lib().aa_b200_batch_last_error(getattr(self, "m_obj", None))
+        return m.decode() if m else ""
+
+    def add_beam(self, metadata: filterbank_metadata_struct, plan: "aa_py_ddtr_plan", d_input) -> int:
+        ptr = d_input if isinstance(d_input, int) else d_input.data_ptr()
+        self._keep.append(d_input)
+        i = lib().aa_b200_batch_add_beam(self.m_obj, metadata, plan.pointer(), ctypes.c_void_p(ptr))
+        if i < 0:
+            raise RuntimeError(self.last_error())
+        return i
+
+    def _check(self, ok):
+        if not ok:
+            raise RuntimeError(self.last_error())
+        return True
+
+    def setup(self):
+        return self._check(lib().aa_b200_batch_setup(self.m_obj))
+
+    def run(self):
+        return self._check(lib().aa_b200_batch_run(self.m_obj))
+
+    def synchronize(self):
+        return self._check(lib().aa_b200_batch_synchronize(self.m_obj))
+
+    def range_shape(self, beam: int, r: int):
+        n, t, b = ctypes.c_int(), ctypes.c_longlong(), ctypes.c_int()
+        if lib().aa_b200_batch_range_shape(self.m_obj, beam, r, ctypes.byref(n), ctypes.byref(t), ctypes.byref(b)):
+            raise RuntimeError(self.last_error())
+        return n.value, t.value, b.value
+
+    def output(self, beam: int, r: int):
+        """Zero-copy torch view (ndms, total_samps) of one range of one beam."""
+        import torch
+        ptr = lib().aa_b200_batch_device_output(self.m_obj, beam, r)
+        if not ptr:
+            raise RuntimeError("no output for this beam/range (is the batch set up?)")
+        ndms, tot, _ = self.range_shape(beam, r)
+        return torch.as_tensor(_DeviceRows(ptr, (ndms, tot)), device="cuda")
+
+    def info(self) -> dict:
+        w, pj, oj, g, sm, lb, lp = (ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(),
+                                    ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_longlong())
+        lib().aa_b200_batch_info(self.m_obj, *(ctypes.byref(v) for v in (w, pj, oj, g, sm, lb, lp)))
+        return {"work_items": w.value, "persistent_jobs": pj.value, "other_jobs": oj.value, "grid": g.value,
+                "smem_bytes": sm.value, "level_bytes": lb.value, "launches_per_run": lp.value}
+
+    def last_ms(self, which: int = 0) -> float:
+        return lib().aa_b200_batch_last_ms(self.m_obj, which)
+
+    def delete(self):
+        if getattr(self, "m_obj", None):
+            lib().aa_b200_batch_delete(self.m_obj)
+            self.m_obj = None
+            self._keep = []
+
+
+def batch_estimate_bytes(metadata: filterbank_metadata_struct, plan: "aa_py_ddtr_plan", free_memory: int) -> int:
+    n = ctypes.c_size_t()
+    if lib().aa_b200_batch_estimate_bytes(metadata, plan.pointer(), free_memory, ctypes.byref(n)):
+        raise RuntimeError(lib().aa_b200_batch_last_error(None).decode())
+    return n.value

@@ -1,0 +1,116 @@
+// ddtr_batch.cu -- persistent dedispersion over many beams in one launch.
+//
+// The grid is sized to the GPU (SMs x resident CTAs); every CTA takes work
+// items from a device counter until the table is exhausted.  An item is one
+// output tile (64 DM trials x 512 samples) of one (beam, chunk, range) job;
+// the jobs are ordered heaviest first on the host, so the items that finish
+// last are the cheap ones.  Consecutive items are the DM groups of one time
+// tile, so the input rows they stage are fetched from HBM once and served
+// from L2 to the others.  The tile itself is computed by the same device
+// bodies as the one-launch-per-job kernels (ddtr_bodies.cuh), so every beam's
+// output is bit-identical to its plain run.
+//
+// Shared memory: [mbarriers][job descriptor][body area], the body area sized
+// for the largest job.  The mbarriers are initialised once; a running stage
+// counter carries their phases from item to item.
+#include "ddtr_bodies.cuh"
+
+namespace aab200 {
+
+namespace {
+
+using namespace dev;
+
+constexpr int JD_WORDS = 64; // shared-memory words kept for the job descriptor
+static_assert(sizeof(BatchJobDev) <= 4 * JD_WORDS, "job descriptor larger than its shared-memory slot");
+static_assert(sizeof(BatchJobDev) % 4 == 0, "job descriptor is copied word by word");
+constexpr int BATCH_M = 16;
+
+__global__ void __launch_bounds__(body::NTHREADS, 1)
+    k_ddtr_persistent(const BatchJobDev *__restrict__ jobs, int njobs, long long total_items,
+                      unsigned long long *__restrict__ counter)
+{
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ long long s_item;
+    __shared__ int s_job;
+    const int tid = threadIdx.x;
+    const unsigned bar0 = smem_addr(sm);
+    uint32_t *jd_words = sm + body::BAR_WORDS;
+    const BatchJobDev &jd = *reinterpret_cast<const BatchJobDev *>(jd_words);
+    uint32_t *area = sm + body::BAR_WORDS + JD_WORDS;
+    body::init_barriers(bar0);
+    unsigned stage_ctr = 0;
+    int jcur = 0; // thread 0: job of the last item (items arrive in increasing order)
+    for (;;) {
+        if (tid == 0) {
+            const long long item = static_cast<long long>(atomicAdd(counter, 1ull));
+            if (item < total_items)
+                while (jcur + 1 < njobs && jobs[jcur + 1].item0 <= item)
+                    ++jcur;
+            s_item = item;
+            s_job = jcur;
+        }
+        __syncthreads();
+        const long long item = s_item;
+        if (item >= total_items)
+            break;
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(jobs + s_job);
+        if (tid < static_cast<int>(sizeof(BatchJobDev) / 4))
+            jd_words[tid] = src[tid];
+        __syncthreads();
+        const long long li = item - jd.item0;
+        const int g = static_cast<int>(li % jd.groups);
+        const long long t0 = (li / jd.groups) * (32 * BATCH_M);
+        bool ok;
+        if (jd.variant == 2)
+            ok = body::quad_body<BATCH_M>(jd.p, jd.q, g, t0, area, bar0, stage_ctr);
+        else
+            ok = body::f32_body<BATCH_M>(jd.p, jd.f, g, t0, area, bar0, stage_ctr);
+        fence_proxy_async();
+        // a tile whose copies timed out ends this CTA (the flag is set); the
+        // decision is block-wide so that no thread is left at a barrier
+        if (__syncthreads_or(!ok))
+            break;
+    }
+}
+
+} // namespace
+
+size_t persistent_job_smem(const BatchJobDev &j)
+{
+    size_t words;
+    if (j.variant == 2)
+        words = body::quad_body_words(j.q.qs, j.p.group_dms, j.q.raww, j.q.nq_pad, j.q.npool, j.q.W);
+    else
+        words = body::f32_body_words(j.f.cs, j.p.group_dms, j.f.rawh, j.f.nch_pad, j.f.W);
+    return 4 * (body::BAR_WORDS + JD_WORDS + words);
+}
+
+int persistent_blocks_per_sm(size_t smem_bytes)
+{
+    if (cudaFuncSetAttribute(k_ddtr_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem_bytes)) != cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ddtr_persistent, body::NTHREADS, smem_bytes) !=
+        cudaSuccess)
+        return 0;
+    return n;
+}
+
+cudaError_t launch_ddtr_persistent(const BatchJobDev *jobs, int njobs, long long total_items,
+                                   unsigned long long *counter, size_t smem_bytes, int grid, cudaStream_t st)
+{
+    if (njobs <= 0 || total_items <= 0)
+        return cudaSuccess;
+    if (grid <= 0 || smem_bytes > 227 * 1024)
+        return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(k_ddtr_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem_bytes));
+    if (e != cudaSuccess)
+        return e;
+    k_ddtr_persistent<<<grid, body::NTHREADS, smem_bytes, st>>>(jobs, njobs, total_items, counter);
+    return cudaGetLastError();
+}
+
+} // namespace aab200

@@ -36,7 +36,7 @@ F32Geometry f32_geometry(int span, int group_dms, int nchans, int cs)
         if (cs > 0 && c != cs)
             continue;
         const size_t bytes = 4 * (body::BAR_WORDS + body::f32_body_words(c, group_dms, G.f.rawh, G.f.nch_pad, G.f.W));
-        if (bytes <= 227 * 1024) {
+        if (bytes <= kStagedSmemLimit) {
             G.f.cs = c;
             G.smem_bytes = bytes;
             return G;

@@ -109,6 +109,11 @@ cudaError_t launch_quad_patterns(const int32_t *table, int nch_used, int ndms, i
 cudaError_t launch_quad_offsets(const int32_t *qtmp, size_t n, int W, int32_t *qoff, cudaStream_t st);
 cudaError_t launch_ddtr_quad(const DdtrLaunch &p, const QuadLaunch &q, cudaStream_t st);
 
+// Dynamic shared memory the staged kernels may use per CTA (the sm_100a
+// opt-in limit less 1 KB, which the persistent kernel keeps for its job
+// descriptor).
+constexpr size_t kStagedSmemLimit = 227 * 1024 - 1024;
+
 // Staged fp32 kernel for two-byte samples (ddtr_f32.cu).
 struct F32Launch {
     int cs;      // channels per stage (4, 8, 16 or 32)
@@ -126,5 +131,26 @@ struct F32Geometry {
 // shared-memory limit.  smem_bytes = 0 when nothing fits.
 F32Geometry f32_geometry(int span, int group_dms, int nchans, int cs);
 cudaError_t launch_ddtr_f32(const DdtrLaunch &p, const F32Launch &f, cudaStream_t st);
+
+// Persistent multi-beam dedispersion (ddtr_batch.cu).  One descriptor per
+// (beam, chunk, range) job of the staged kernels; a job is groups x tiles
+// work items (one 64-DM x 512-sample tile each, DM group fastest), numbered
+// from item0 in the order of the table.
+struct BatchJobDev {
+    DdtrLaunch p;
+    QuadLaunch q;
+    F32Launch f;
+    int variant; // 2 channel-quad, 3 staged fp32
+    int groups;
+    long long item0;
+};
+
+// Dynamic shared memory of one job in the persistent kernel.
+size_t persistent_job_smem(const BatchJobDev &j);
+// CTAs of the persistent kernel that fit one SM at this dynamic shared memory.
+int persistent_blocks_per_sm(size_t smem_bytes);
+// counter: device work counter, zero before the launch.
+cudaError_t launch_ddtr_persistent(const BatchJobDev *jobs, int njobs, long long total_items,
+                                   unsigned long long *counter, size_t smem_bytes, int grid, cudaStream_t st);
 
 } // namespace aab200

@@ -186,11 +186,11 @@ bool DdtrPipeline::build_quad_tables(int r)
         const int M = (opt_.tile_words == 2) ? 8 : 16;
         int qs = 4;
         QuadGeometry G = quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, nquads, M, qs);
-        while (G.smem_bytes > 227 * 1024 && qs > 1) {
+        while (G.smem_bytes > kStagedSmemLimit && qs > 1) {
             qs /= 2;
             G = quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, nquads, M, qs);
         }
-        if (G.smem_bytes <= 227 * 1024 && rc.quad_dmax <= 255) {
+        if (G.smem_bytes <= kStagedSmemLimit && rc.quad_dmax <= 255) {
             rc.quad = G;
             rc.variant = 2;
             ok = check_cuda(launch_quad_offsets(d_qtmp, nq_ent, G.W, rc.d_qoff, st_), "quad offsets");
@@ -348,8 +348,13 @@ bool DdtrPipeline::setup()
 
     const long long L0 = static_cast<long long>(strategy_.t_processed()[0][0]) + strategy_.maxshift();
     const long long pad = 4LL * (512 + span_max + delay_max) + rawb_max + 65536;
+    pad_elems_ = static_cast<size_t>(pad);
     flat_elems_ = static_cast<size_t>(nchans) * static_cast<size_t>(L0) + static_cast<size_t>(pad);
-    for (int i = 0; i < 2; ++i) {
+    if (!enumerate_ops())
+        return false;
+    if (opt_.external_buffers && (opt_.copy_to_host || !opt_.device_output || !opt_.device_input))
+        return fail("a pipeline run by a batch engine keeps its input and output on the device");
+    for (int i = 0; i < 2 && !opt_.external_buffers; ++i) {
         if (!check_cuda(cudaMalloc(&d_flat_[i], flat_elems_ * elem_bytes_), "cudaMalloc(filterbank)") ||
             !check_cuda(cudaMemsetAsync(d_flat_[i], 0, flat_elems_ * elem_bytes_, st_), "memset"))
             return false;
@@ -414,27 +419,179 @@ bool DdtrPipeline::setup()
 
 bool DdtrPipeline::rewind()
 {
+    op_cursor_ = 0;
     cur_chunk_ = 0;
     cur_range_ = 0;
     inc_ = 0;
-    old_bin_ = 1;
     finished_component_sent_ = false;
     return true;
 }
 
-bool DdtrPipeline::do_chunk_start()
+// The runner's loop as a list: per chunk the load and corner turn (:741),
+// then per range a single x2 binning whenever inBin grows (:797-808) with the
+// length the runner passes, and the dedispersion with row stride
+// t_processed + maxshift/inBin (:782-786); output rows at inc/inBin
+// (src/aa_device_save_data.cu:41).  STRIDE_TRUE bins on the true row stride
+// as many times as inBin needs.
+bool DdtrPipeline::enumerate_ops()
+{
+    ops_.clear();
+    const int nr = static_cast<int>(strategy_.nranges());
+    const auto &T = strategy_.t_processed();
+    long long inc = 0;
+    for (int k = 0; k < strategy_.num_tchunks(); ++k) {
+        const long long L = static_cast<long long>(T[0][k]) + strategy_.maxshift();
+        if (inc + L > meta_.nsamples)
+            return fail("chunk extends past the end of the input");
+        DdtrOp ct;
+        ct.kind = DdtrOp::CORNER_TURN;
+        ct.chunk = k;
+        ct.len = L;
+        ct.inc = inc;
+        ops_.push_back(ct);
+        int level = 0, old_bin = 1, cur_bin = 1;
+        long long cur_stride = L;
+        for (int r = 0; r < nr; ++r) {
+            const DmRange &d = strategy_.dm(r);
+            const int tp = T[r][k];
+            const int ms_r = strategy_.maxshift() / d.inBin; // :782
+            auto bin_once = [&](long long nsb) -> bool {
+                if (nsb <= 0 || (nsb & 1))
+                    return fail("binning length must be positive and even");
+                DdtrOp b;
+                b.kind = DdtrOp::BIN;
+                b.chunk = k;
+                b.range = r;
+                b.src_level = level;
+                b.dst_level = level + 1;
+                b.len = nsb;
+                b.inc = inc;
+                ops_.push_back(b);
+                ++level;
+                return true;
+            };
+            long long i_nsamp;
+            if (opt_.stride_mode == STRIDE_REFERENCE) {
+                if (d.inBin > old_bin &&
+                    !bin_once(static_cast<long long>(T[r - 1][k]) + static_cast<long long>(ms_r) * d.inBin)) // :797-798
+                    return false;
+                i_nsamp = static_cast<long long>(tp) + ms_r; // :786
+            } else {
+                while (cur_bin < d.inBin) {
+                    if (!bin_once(cur_stride))
+                        return false;
+                    cur_stride /= 2;
+                    cur_bin *= 2;
+                }
+                i_nsamp = cur_stride;
+            }
+            DdtrOp dd;
+            dd.kind = DdtrOp::DDTR;
+            dd.chunk = k;
+            dd.range = r;
+            dd.src_level = level;
+            dd.i_nsamp = i_nsamp;
+            dd.tp = tp;
+            dd.inc = inc;
+            dd.out_off = inc / d.inBin;
+            ops_.push_back(dd);
+            old_bin = d.inBin;
+        }
+        inc += T[0][k]; // :898
+    }
+    return true;
+}
+
+bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, float *out, long long out_pitch,
+                            DdtrJob &job)
+{
+    const int r = op.range;
+    const RangeConfig &rc = ranges_[r];
+    const DmRange &d = strategy_.dm(r);
+    const int tp = op.tp;
+    const long long i_nsamp = op.i_nsamp;
+    job = DdtrJob();
+    job.variant = (elem_bytes_ == 1 && rc.variant == 2) ? 2 : (elem_bytes_ == 2 && rc.variant == 3) ? 3 : 1;
+    job.elem_bytes = elem_bytes_;
+    job.tile_words = rc.tile_words;
+    job.offtab = rc.d_offtab;
+    const int tile = (job.variant == 2) ? 32 * rc.quad.M : (job.variant == 3 ? 512 : 128 * rc.tile_words);
+    const long long ntiles = (tp + tile - 1) / tile;
+    long long need;
+    if (elem_bytes_ == 1 && job.variant == 2)
+        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ntiles * tile + rc.delay_max + 4LL * rc.quad.raww + 64;
+    else if (elem_bytes_ == 1)
+        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ntiles * tile + rc.delay_max +
+               4LL * ddtr_u8_rw(rc.span, rc.tile_words) + 64;
+    else if (job.variant == 3)
+        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ntiles * tile + rc.delay_max + rc.f32.rawh + 8;
+    else
+        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + tp + rc.delay_max + 2;
+    if (need > static_cast<long long>(in_elems))
+        return fail("dedispersion window exceeds the filterbank buffer");
+
+    DdtrLaunch &p = job.p;
+    p.in = in;
+    p.stride = i_nsamp;
+    p.nchans = meta_.nchans;
+    p.nch_used = rc.nch_used;
+    p.tp = tp;
+    p.ndms = strategy_.ndms(r);
+    p.table = rc.d_table;
+    p.wmin = rc.d_wmin;
+    p.group_dms = rc.group_dms;
+    p.span = rc.span;
+    p.kind = rc.kind;
+    p.nchans_f = static_cast<float>(meta_.nchans);
+    p.bin_f = static_cast<float>(d.inBin);
+    p.divide_by_bin = (rc.kind == KIND_SHARED4) ? 0 : 1;
+    p.out = out;
+    p.out_pitch = out_pitch;
+    p.err = d_err_;
+    if (job.variant == 1 && elem_bytes_ == 1 &&
+        ((reinterpret_cast<uintptr_t>(p.out) & 15) || (p.out_pitch & 3) || (tp & 3)))
+        return fail("output rows are not 16-byte aligned");
+    if (job.variant == 2) {
+        QuadLaunch &q = job.q;
+        q.qpat = rc.d_qpat;
+        q.qwin = rc.d_qwin;
+        q.qoff = rc.d_qoff;
+        q.nquads = rc.nquads;
+        q.nq_pad = rc.quad.nq_pad;
+        q.W = rc.quad.W;
+        q.raww = rc.quad.raww;
+        q.qs = rc.quad.qs;
+        q.npool = rc.quad.npool;
+        q.M = rc.quad.M;
+    } else if (job.variant == 3) {
+        job.f = rc.f32;
+    }
+    job.groups = p.ndms / p.group_dms;
+    job.tiles = ntiles;
+    job.tile_samples = tile;
+    return true;
+}
+
+cudaError_t launch_job(const DdtrJob &job, cudaStream_t st)
+{
+    if (job.variant == 2)
+        return launch_ddtr_quad(job.p, job.q, st);
+    if (job.variant == 3)
+        return launch_ddtr_f32(job.p, job.f, st);
+    return (job.elem_bytes == 1) ? launch_ddtr_u8(job.p, job.offtab, job.tile_words, st) : launch_ddtr_u16(job.p, st);
+}
+
+bool DdtrPipeline::exec_corner_turn(const DdtrOp &op)
 {
     const int nchans = meta_.nchans;
-    const int k = cur_chunk_;
-    const long long L = static_cast<long long>(strategy_.t_processed()[0][k]) + strategy_.maxshift();
-    if (inc_ + L > meta_.nsamples)
-        return fail("chunk extends past the end of the input");
+    const int k = op.chunk;
+    const long long L = op.len;
     if (static_cast<size_t>(nchans) * static_cast<size_t>(L) > flat_elems_)
         return fail("chunk larger than the filterbank buffer");
     const uint16_t *src;
     const int slot = k & 1;
     if (opt_.device_input) {
-        src = input_ + static_cast<size_t>(inc_) * nchans;
+        src = input_ + static_cast<size_t>(op.inc) * nchans;
     } else {
         // issue this chunk's copy if it was not prefetched, and prefetch the next
         auto issue = [&](int kk, long long inc_kk) -> bool {
@@ -452,7 +609,7 @@ bool DdtrPipeline::do_chunk_start()
         if (k == 0 && !issue(0, 0))
             return false;
         if (k + 1 < strategy_.num_tchunks()) {
-            const long long inc_next = inc_ + strategy_.t_processed()[0][k];
+            const long long inc_next = op.inc + strategy_.t_processed()[0][k];
             if (!issue(k + 1, inc_next))
                 return false;
         }
@@ -461,131 +618,53 @@ bool DdtrPipeline::do_chunk_start()
         src = d_raw_[slot];
     }
     const int max_value = (meta_.nbits == 4) ? 15 : (meta_.nbits <= 8 ? 255 : 65535);
-    cur_flat_ = 0;
     if (!timed_launch_begin(KF_CORNER_TURN) ||
-        !check_cuda(launch_corner_turn(src, d_flat_[0], elem_bytes_, nchans, L, L, max_value, d_err_, st_),
+        !check_cuda(launch_corner_turn(src, d_flat_[op.dst_level & 1], elem_bytes_, nchans, L, L, max_value, d_err_,
+                                       st_),
                     "corner turn") ||
         !timed_launch_end())
         return false;
     ++launches_;
     if (!opt_.device_input && !check_cuda(cudaEventRecord(ev_raw_free_[slot], st_), "event"))
         return false;
-    old_bin_ = 1;
-    cur_stride_ = L;
-    cur_bin_ = 1;
     return true;
 }
 
-bool DdtrPipeline::do_range()
+bool DdtrPipeline::exec_bin(const DdtrOp &op)
 {
     const int nchans = meta_.nchans;
-    const int r = cur_range_, k = cur_chunk_;
-    const RangeConfig &rc = ranges_[r];
-    const DmRange &d = strategy_.dm(r);
-    const int tp = strategy_.t_processed()[r][k];
-    const int ms_r = strategy_.maxshift() / d.inBin; // :782
-    long long i_nsamp;
+    if (static_cast<size_t>(nchans) * static_cast<size_t>(op.len) > flat_elems_)
+        return fail("binning length exceeds the filterbank buffer");
+    if (!timed_launch_begin(KF_BIN) ||
+        !check_cuda(launch_bin_flat(d_flat_[op.src_level & 1], d_flat_[op.dst_level & 1], elem_bytes_, nchans, op.len,
+                                    st_),
+                    "binning") ||
+        !timed_launch_end())
+        return false;
+    ++launches_;
+    return true;
+}
 
-    auto bin_once = [&](long long nsb) -> bool {
-        if (nsb <= 0 || (nsb & 1))
-            return fail("binning length must be positive and even");
-        if (static_cast<size_t>(nchans) * static_cast<size_t>(nsb) > flat_elems_)
-            return fail("binning length exceeds the filterbank buffer");
-        if (!timed_launch_begin(KF_BIN) ||
-            !check_cuda(launch_bin_flat(d_flat_[cur_flat_], d_flat_[cur_flat_ ^ 1], elem_bytes_, nchans, nsb, st_),
-                        "binning") ||
-            !timed_launch_end())
-            return false;
-        ++launches_;
-        cur_flat_ ^= 1;
-        return true;
-    };
-
-    if (opt_.stride_mode == STRIDE_REFERENCE) {
-        if (d.inBin > old_bin_) {
-            const long long nsb = static_cast<long long>(strategy_.t_processed()[r - 1][k]) +
-                                  static_cast<long long>(ms_r) * d.inBin; // :797-798
-            if (!bin_once(nsb))
-                return false;
-        }
-        i_nsamp = static_cast<long long>(tp) + ms_r; // :786
-    } else {
-        while (cur_bin_ < d.inBin) {
-            if (!bin_once(cur_stride_))
-                return false;
-            cur_stride_ /= 2;
-            cur_bin_ *= 2;
-        }
-        i_nsamp = cur_stride_;
-    }
-
-    const int tile = (rc.variant == 2) ? 32 * rc.quad.M : (rc.variant == 3 ? 512 : 128 * rc.tile_words);
-    long long need;
-    if (elem_bytes_ == 1 && rc.variant == 2)
-        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ((tp + tile - 1) / tile) * static_cast<long long>(tile) +
-               rc.delay_max + 4LL * rc.quad.raww + 64;
-    else if (elem_bytes_ == 1)
-        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ((tp + tile - 1) / tile) * static_cast<long long>(tile) +
-               rc.delay_max + 4LL * ddtr_u8_rw(rc.span, rc.tile_words) + 64;
-    else if (rc.variant == 3)
-        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ((tp + tile - 1) / tile) * static_cast<long long>(tile) +
-               rc.delay_max + rc.f32.rawh + 8;
-    else
-        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + tp + rc.delay_max + 2;
-    if (need > static_cast<long long>(flat_elems_))
-        return fail("dedispersion window exceeds the filterbank buffer");
-
-    DdtrLaunch p;
-    p.in = d_flat_[cur_flat_];
-    p.stride = i_nsamp;
-    p.nchans = nchans;
-    p.nch_used = rc.nch_used;
-    p.tp = tp;
-    p.ndms = strategy_.ndms(r);
-    p.table = rc.d_table;
-    p.wmin = rc.d_wmin;
-    p.group_dms = rc.group_dms;
-    p.span = rc.span;
-    p.kind = rc.kind;
-    p.nchans_f = static_cast<float>(nchans);
-    p.bin_f = static_cast<float>(d.inBin);
-    p.divide_by_bin = (rc.kind == KIND_SHARED4) ? 0 : 1;
-    p.err = d_err_;
-    const long long host_off = inc_ / d.inBin; // src/aa_device_save_data.cu:41
+bool DdtrPipeline::exec_ddtr(const DdtrOp &op)
+{
+    const int r = op.range;
+    const long long host_off = op.out_off; // src/aa_device_save_data.cu:41
     const int slot = tile_slot_;
+    float *out;
+    long long pitch;
     if (opt_.device_output) {
-        p.out = d_out_full_[r] + host_off;
-        p.out_pitch = strategy_.total_samps(r);
+        out = d_out_full_[r] + host_off;
+        pitch = strategy_.total_samps(r);
     } else {
         if (!check_cuda(cudaStreamWaitEvent(st_, ev_tile_free_[slot], 0), "wait"))
             return false;
-        p.out = d_tile_[slot];
-        p.out_pitch = tp;
+        out = d_tile_[slot];
+        pitch = op.tp;
     }
-    if (rc.variant == 1 && elem_bytes_ == 1 && ((reinterpret_cast<uintptr_t>(p.out) & 15) || (p.out_pitch & 3) || (tp & 3)))
-        return fail("output rows are not 16-byte aligned");
-    if (!timed_launch_begin(KF_DDTR))
+    DdtrJob job;
+    if (!make_job(op, d_flat_[op.src_level & 1], flat_elems_, out, pitch, job))
         return false;
-    cudaError_t e;
-    if (elem_bytes_ == 1 && rc.variant == 2) {
-        QuadLaunch q;
-        q.qpat = rc.d_qpat;
-        q.qwin = rc.d_qwin;
-        q.qoff = rc.d_qoff;
-        q.nquads = rc.nquads;
-        q.nq_pad = rc.quad.nq_pad;
-        q.W = rc.quad.W;
-        q.raww = rc.quad.raww;
-        q.qs = rc.quad.qs;
-        q.npool = rc.quad.npool;
-        q.M = rc.quad.M;
-        e = launch_ddtr_quad(p, q, st_);
-    } else if (rc.variant == 3) {
-        e = launch_ddtr_f32(p, rc.f32, st_);
-    } else {
-        e = (elem_bytes_ == 1) ? launch_ddtr_u8(p, rc.d_offtab, rc.tile_words, st_) : launch_ddtr_u16(p, st_);
-    }
-    if (!check_cuda(e, "dedispersion") || !timed_launch_end())
+    if (!timed_launch_begin(KF_DDTR) || !check_cuda(launch_job(job, st_), "dedispersion") || !timed_launch_end())
         return false;
     ++launches_;
 
@@ -596,9 +675,10 @@ bool DdtrPipeline::do_range()
             !check_cuda(cudaStreamWaitEvent(st_d2h_, ev_tile_done_[slot], 0), "wait"))
             return false;
         const size_t tot = static_cast<size_t>(strategy_.total_samps(r));
-        if (!check_cuda(cudaMemcpy2DAsync(host_rows_[r][0] + host_off, tot * sizeof(float), p.out,
-                                          static_cast<size_t>(p.out_pitch) * sizeof(float), static_cast<size_t>(tp) * sizeof(float),
-                                          static_cast<size_t>(p.ndms), cudaMemcpyDeviceToHost, st_d2h_),
+        if (!check_cuda(cudaMemcpy2DAsync(host_rows_[r][0] + host_off, tot * sizeof(float), out,
+                                          static_cast<size_t>(pitch) * sizeof(float),
+                                          static_cast<size_t>(op.tp) * sizeof(float),
+                                          static_cast<size_t>(job.p.ndms), cudaMemcpyDeviceToHost, st_d2h_),
                         "D2H output"))
             return false;
         if (!opt_.device_output && !check_cuda(cudaEventRecord(ev_tile_free_[slot], st_d2h_), "event"))
@@ -606,21 +686,36 @@ bool DdtrPipeline::do_range()
     }
     if (!opt_.device_output)
         tile_slot_ ^= 1;
-    old_bin_ = d.inBin;
     return true;
 }
 
+// One (chunk, range) step: the ops up to and including the next dedispersion.
 bool DdtrPipeline::step(bool /*allow_sync*/)
 {
-    if (cur_range_ == 0 && !do_chunk_start())
-        return false;
-    if (!do_range())
-        return false;
-    ++cur_range_;
-    if (cur_range_ >= static_cast<int>(strategy_.nranges())) {
-        inc_ += strategy_.t_processed()[0][cur_chunk_]; // :898
-        ++cur_chunk_;
-        cur_range_ = 0;
+    if (opt_.external_buffers)
+        return fail("this pipeline's ops are run by a batch engine");
+    while (op_cursor_ < ops_.size()) {
+        const DdtrOp &op = ops_[op_cursor_++];
+        if (op.kind == DdtrOp::CORNER_TURN) {
+            if (!exec_corner_turn(op))
+                return false;
+        } else if (op.kind == DdtrOp::BIN) {
+            if (!exec_bin(op))
+                return false;
+        } else {
+            if (!exec_ddtr(op))
+                return false;
+            // reference :1053-1054, :898: the position after this step
+            cur_range_ = op.range + 1;
+            cur_chunk_ = op.chunk;
+            inc_ = op.inc;
+            if (cur_range_ >= static_cast<int>(strategy_.nranges())) {
+                cur_range_ = 0;
+                cur_chunk_ = op.chunk + 1;
+                inc_ = op.inc + strategy_.t_processed()[0][op.chunk];
+            }
+            return true;
+        }
     }
     return true;
 }
@@ -641,7 +736,7 @@ bool DdtrPipeline::next(RunStatus &status)
         status = RunStatus::error;
         return false;
     }
-    if (cur_chunk_ >= strategy_.num_tchunks()) {
+    if (op_cursor_ >= ops_.size()) {
         if (!finished_component_sent_) {
             finished_component_sent_ = true;
             if (!synchronize()) {
@@ -666,7 +761,7 @@ bool DdtrPipeline::run_all()
 {
     if (!error_.empty() || !setup())
         return false;
-    while (cur_chunk_ < strategy_.num_tchunks())
+    while (op_cursor_ < ops_.size())
         if (!step(false))
             return false;
     finished_component_sent_ = true;

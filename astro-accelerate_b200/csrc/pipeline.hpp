@@ -45,8 +45,41 @@ struct PipelineOptions {
     bool device_input = false;  // the input pointer is device memory ([t][c] uint16)
     bool device_output = false; // keep the whole output on the device ([range][dm][t])
     bool time_kernels = false;  // CUDA events around every kernel launch
+    bool external_buffers = false; // no filterbank/raw/tile buffers: the caller runs the ops (batch engine)
     cudaStream_t stream = nullptr;
 };
+
+// One step of the reference runner's DDTR loop
+// (include/aa_permitted_pipelines_generic.hpp:606-914), in order.  Filterbank
+// "levels" name the copies a chunk goes through: level 0 is the corner-turned
+// chunk, every x2 binning makes the next level from the current one.
+struct DdtrOp {
+    enum Kind : int { CORNER_TURN = 0, BIN = 1, DDTR = 2 };
+    int kind = CORNER_TURN;
+    int chunk = 0, range = 0;
+    int src_level = 0, dst_level = 0;
+    long long len = 0;     // CORNER_TURN: samples per channel row; BIN: the binning length
+    long long inc = 0;     // first input sample of the chunk
+    long long i_nsamp = 0; // DDTR: row stride of the level it reads
+    int tp = 0;            // DDTR: outputs per DM row
+    long long out_off = 0; // DDTR: first column of the chunk in the range's output rows (inc / inBin)
+};
+
+// A dedispersion launch, ready for a stream (launch_job) or a batch queue.
+struct DdtrJob {
+    int variant = 1; // 1 generic, 2 channel-quad, 3 staged fp32
+    int elem_bytes = 1;
+    int tile_words = 4;
+    const int32_t *offtab = nullptr;
+    DdtrLaunch p{};
+    QuadLaunch q{};
+    F32Launch f{};
+    int groups = 0;       // CTAs along DM
+    long long tiles = 0;  // CTAs along time
+    int tile_samples = 0; // samples per CTA tile
+};
+
+cudaError_t launch_job(const DdtrJob &job, cudaStream_t st);
 
 // Kernel families timed when PipelineOptions::time_kernels is set.
 enum KernelFamily : int { KF_DDTR = 0, KF_CORNER_TURN = 1, KF_BIN = 2, KF_COUNT = 3 };
@@ -104,6 +137,17 @@ public:
     long long current_inc() const { return inc_; }
     const RangeConfig &range_config(int r) const { return ranges_[r]; }
     const std::string &last_error() const { return error_; }
+    // The run as a list of steps (valid after setup()).
+    const std::vector<DdtrOp> &ops() const { return ops_; }
+    // Elements a filterbank level must hold past nchans x its row length for
+    // the staged windows' over-read (valid after setup()).
+    size_t pad_elems() const { return pad_elems_; }
+    int elem_bytes() const { return elem_bytes_; }
+    int *device_flags() const { return d_err_; }
+    // The launch of a DDTR op reading level buffer `in` (in_elems elements)
+    // and writing rows of `out` with pitch out_pitch.
+    bool make_job(const DdtrOp &op, const void *in, size_t in_elems, float *out, long long out_pitch, DdtrJob &job);
+    bool check_flags() { return check_device_flags(); }
     long long kernel_launches() const { return launches_; }
     // Device time (ms) and launch count of one kernel family since the last
     // reset, collected at synchronize().
@@ -124,8 +168,10 @@ private:
     bool build_range(int r);
     bool build_quad_tables(int r);
     bool step(bool allow_sync);
-    bool do_chunk_start();
-    bool do_range();
+    bool enumerate_ops();
+    bool exec_corner_turn(const DdtrOp &op);
+    bool exec_bin(const DdtrOp &op);
+    bool exec_ddtr(const DdtrOp &op);
     size_t buffer_elems() const { return flat_elems_; }
     bool timed_launch_begin(int family);
     bool timed_launch_end();
@@ -169,13 +215,12 @@ private:
     std::vector<std::vector<float *>> host_row_ptrs_;
 
     // iteration state (reference :1053-1054 current_time_chunk/current_range)
+    std::vector<DdtrOp> ops_;
+    size_t op_cursor_ = 0;
+    size_t pad_elems_ = 0;
     int cur_chunk_ = 0;
     int cur_range_ = 0;
     long long inc_ = 0;
-    int old_bin_ = 1;
-    int cur_flat_ = 0;
-    long long cur_stride_ = 0;
-    int cur_bin_ = 1;
     int tile_slot_ = 0;
     long long launches_ = 0;
 

@@ -263,6 +263,47 @@ bool aa_b200_pipeline_time_kernels(void *obj, int on);
 int aa_b200_pipeline_kernel_time(void *obj, int family, double *ms, long long *count);
 bool aa_b200_pipeline_reset_kernel_times(void *obj);
 
+/* ---------------------------------------------------------------------------
+ * Multi-beam dedispersion (no counterpart in the reference, which runs one
+ * beam per aa_pipeline_api and one kernel launch per (chunk, range)).
+ *
+ * Beams of different channel counts, bit depths, lengths and DM plans are
+ * added with their [nsamples][nchans] uint16 input already on the device;
+ * setup computes each beam's strategy (as aa_ddtr_strategy would with
+ * free_memory bytes free; 0 = the device's free memory at setup), its delay
+ * tables and device outputs, gives every (beam, chunk, binning level) its own
+ * filterbank buffer, and records the whole job as one CUDA graph: corner
+ * turns and binning of all beams on parallel streams, then one persistent
+ * dedispersion kernel over all (beam, chunk, range, DM group, time tile) work
+ * items (persistent = 0: one launch per (beam, chunk, range) instead).
+ * autotune != 0 times the shared-memory stage depth per range shape at setup.
+ * Each beam's output [range][dm][t] is bit-identical to a plain pipeline's
+ * (aa_b200_pipeline_create with device_output) for the same free_memory.
+ * run is asynchronous on `stream` (a cudaStream_t as void*, 0 = a stream of
+ * the batch's own); synchronize waits and checks every beam's device flags.
+ * --------------------------------------------------------------------------- */
+void *aa_b200_batch_create(int stride_mode, int fma_mode, size_t free_memory, int persistent, int use_graph,
+                           int autotune, void *stream);
+/* returns the beam index, or -1 (message in aa_b200_batch_last_error) */
+int aa_b200_batch_add_beam(void *batch, aa_py_filterbank_metadata_struct metadata, void *ddtr_plan,
+                           const unsigned short *d_input);
+bool aa_b200_batch_setup(void *batch);
+bool aa_b200_batch_run(void *batch);
+bool aa_b200_batch_synchronize(void *batch);
+/* [ndms][total_samps] float rows of one range of one beam (device memory) */
+float *aa_b200_batch_device_output(void *batch, int beam, int range);
+int aa_b200_batch_range_shape(void *batch, int beam, int range, int *ndms, long long *total_samps, int *inBin);
+int aa_b200_batch_info(void *batch, long long *work_items, int *persistent_jobs, int *other_jobs, int *grid,
+                       size_t *smem_bytes, size_t *level_bytes, long long *launches_per_run);
+/* device time (ms) of the last run: which = 0 whole run, 1 dedispersion part */
+double aa_b200_batch_last_ms(void *batch, int which);
+/* device bytes a beam needs inside a batch (outputs, tables, filterbank
+ * levels), to split a beam list into batches that fit */
+int aa_b200_batch_estimate_bytes(aa_py_filterbank_metadata_struct metadata, void *ddtr_plan, size_t free_memory,
+                                 size_t *bytes);
+const char *aa_b200_batch_last_error(void *batch);
+void aa_b200_batch_delete(void *batch);
+
 #ifdef __cplusplus
 }
 #endif
