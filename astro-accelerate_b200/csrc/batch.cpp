@@ -475,8 +475,9 @@ bool BatchDdtr::synchronize()
     if (ran_) {
         float ms = 0.f;
         run_ms_ = (cudaEventElapsedTime(&ms, ev_run0_, ev_run1_) == cudaSuccess) ? ms : -1.0;
-        ddtr_ms_ = (cudaEventElapsedTime(&ms, ev_dd0_, ev_dd1_) == cudaSuccess) ? ms : -1.0;
-        cudaGetLastError(); // an event pair recorded inside a graph may not be timeable
+        // events recorded inside a graph do not time; the split is measured without one
+        ddtr_ms_ = (!opt_.use_graph && cudaEventElapsedTime(&ms, ev_dd0_, ev_dd1_) == cudaSuccess) ? ms : -1.0;
+        cudaGetLastError();
     }
     for (size_t bi = 0; bi < beams_.size(); ++bi)
         if (!beams_[bi].pipe->check_flags())

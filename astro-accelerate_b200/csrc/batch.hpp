@@ -70,7 +70,8 @@ public:
     int other_jobs() const { return static_cast<int>(ojobs_.size()); }
     int grid() const { return grid_; }
     size_t smem_bytes() const { return smem_; }
-    // device time of the last run: whole graph and the dedispersion part
+    // device time of the last run: whole graph, and the dedispersion part
+    // (only without the graph; -1 otherwise)
     double last_run_ms() const { return run_ms_; }
     double last_ddtr_ms() const { return ddtr_ms_; }
     const std::string &last_error() const { return error_; }

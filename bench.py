@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="survey", choices=["survey", "mid", "small"])
+    ap.add_argument("--config", default="survey", choices=["survey", "mid", "small", "batched"])
+    ap.add_argument("--beams", type=int, default=48, help="beams of the multi-beam draw (batched config)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -230,14 +231,171 @@ def workload_config(cfg):
             "parallelism": "one beam per GPU"}
 
 
+# ---------------------------------------------------------------------------
+MULTIBEAM_FREE_MEMORY = 64 << 30  # memory the beams' strategies are computed for (both arms)
+
+
+def dev_rows(aa, ptr, shape):
+    import torch
+    return torch.as_tensor(aa._DeviceRows(ptr, shape), device="cuda")
+
+
+def run_batched(args, rank, world, local):
+    """Multi-beam workload: the seeded 48-beam draw (aa_b200.workloads), run
+    (a) as batches -- one CUDA graph with one persistent dedispersion kernel
+    per batch, batches sized to device memory -- and (b) beam by beam through
+    the plain pipeline, both with the input resident in HBM and the output
+    kept in HBM, both timed with CUDA events on the same stream.  Every
+    beam's batched output is compared with its plain output bit for bit."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import aa_b200 as aa
+    from aa_b200 import workloads as WL
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    beams = WL.multibeam_draw(seed=3 + 1000 * rank, nbeams=args.beams)
+    stream = torch.cuda.Stream(device)
+    stream.wait_stream(torch.cuda.current_stream(device))
+    mds, plans, sizes, units_b = [], [], [], []
+    for b in beams:
+        md = aa.filterbank_metadata_struct(0.0, b["tsamp"], b["fch1"], b["foff"], b["nbits"], b["nsamp"],
+                                           b["nchans"], 0.0)
+        plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in b["plan"]])
+        st = aa.strategy(b["plan"], b["nchans"], b["nsamp"], b["fch1"], b["foff"], b["tsamp"], b["nbits"],
+                         MULTIBEAM_FREE_MEMORY)
+        mds.append(md)
+        plans.append(plan)
+        units_b.append(units_per_step(st))
+        sizes.append(aa.batch_estimate_bytes(md, plan, MULTIBEAM_FREE_MEMORY) + 2 * b["nsamp"] * b["nchans"])
+    free, _ = torch.cuda.mem_get_info(device)
+    plain_reserve = max(b["nsamp"] * b["nchans"] * 2 * 3 + u * 4 for b, u in zip(beams, units_b))
+    budget = int(free * 0.9) - plain_reserve
+    waves = WL.plan_waves(sizes, budget)
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tot = dict(batched_ms=0.0, plain_ms=0.0, plain_fresh_s=0.0, setup_s=0.0, units=0, launches=0, items=0)
+    bit_exact, mismatches, n_cmp = True, [], 0
+    wave_info = []
+    with ClockSampler(local) as clk:
+        for w in waves:
+            xs = {i: WL.synth_beam_device(beams[i], device) for i in w}
+            torch.cuda.synchronize(device)
+            B = aa.batch(free_memory=MULTIBEAM_FREE_MEMORY, stream=stream.cuda_stream)
+            t0 = time.perf_counter()
+            for i in w:
+                B.add_beam(mds[i], plans[i], xs[i])
+            B.setup()
+            tot["setup_s"] += time.perf_counter() - t0
+            for _ in range(max(1, args.warmup)):
+                B.run()
+                B.synchronize()
+            ms = []
+            for _ in range(args.steps):
+                ev0.record(stream)
+                B.run()
+                ev1.record(stream)
+                B.synchronize()
+                ms.append(ev0.elapsed_time(ev1))
+            info = B.info()
+            tot["batched_ms"] += statistics.median(ms)
+            tot["launches"] += info["launches_per_run"]
+            tot["items"] += info["work_items"]
+            wave_info.append({"beams": len(w), "ms": statistics.median(ms), "work_items": info["work_items"],
+                              "persistent_jobs": info["persistent_jobs"], "other_jobs": info["other_jobs"],
+                              "grid": info["grid"], "smem_bytes": info["smem_bytes"]})
+            # plain arm, beam by beam on the same stream
+            for j, i in enumerate(w):
+                b = beams[i]
+                t0 = time.perf_counter()
+                pipe = aa.create_pipeline(mds[i], xs[i].data_ptr(), device_input=True, device_output=True,
+                                          copy_to_host=False, stream=stream.cuda_stream, card_number=local)
+                pipe.set_options(free_memory=MULTIBEAM_FREE_MEMORY)
+                if not pipe.bind_ddtr_plan(plans[i]) or not (pipe.run_all() and pipe.synchronize()):
+                    raise RuntimeError(pipe.last_error())
+                tot["plain_fresh_s"] += time.perf_counter() - t0
+                pms = []
+                for _ in range(args.steps):
+                    pipe.rewind()
+                    ev0.record(stream)
+                    if not pipe.run_all():
+                        raise RuntimeError(pipe.last_error())
+                    ev1.record(stream)
+                    if not pipe.synchronize():
+                        raise RuntimeError(pipe.last_error())
+                    pms.append(ev0.elapsed_time(ev1))
+                tot["plain_ms"] += statistics.median(pms)
+                for r in range(len(b["plan"])):
+                    ndms, total, _ = B.range_shape(j, r)
+                    a = B.output(j, r).view(torch.int32)
+                    p = dev_rows(aa, pipe.device_output(r), (ndms, total)).view(torch.int32)
+                    n_cmp += 1
+                    if not torch.equal(a, p):
+                        bit_exact = False
+                        mismatches.append([i, r])
+                pipe.cleanUp()
+                pipe.delete()
+                tot["units"] += units_b[i]
+            B.delete()
+            del xs
+            torch.cuda.synchronize(device)
+            torch.cuda.empty_cache()
+    for p in plans:
+        p.delete()
+    batched_s = tot["batched_ms"] / 1e3
+    plain_s = tot["plain_ms"] / 1e3
+    if world > 1:
+        t = torch.tensor([batched_s, plain_s], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        batched_s, plain_s = float(t[0]), float(t[1])
+    value = tot["units"] * world / batched_s
+    obs_s = sum(b["nsamp"] * b["tsamp"] for b in beams)
+    nbits_count = {n: sum(1 for b in beams if b["nbits"] == n) for n in (4, 8, 16)}
+    if rank == 0:
+        line = {
+            "metric": "DM-trial*samples/s (batched multi-beam DDTR, bit-exact vs plain per-beam launch)",
+            "value": value, "unit": "DM-trial*samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(1, args.warmup), "ms_per_step": batched_s * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8+u16", "data": "synthetic",
+            "config": {"workload": f"multi-beam DDTR: {len(beams)} beams, 2048-4096 ch, 4/8/16-bit, 2^16-2^21 "
+                                   f"samples, 2-6-range prefixes of the survey plan cut at DM 500-3000",
+                       "beams": len(beams), "nbits_count": nbits_count, "seed": 3,
+                       "strategy_free_memory": MULTIBEAM_FREE_MEMORY, "waves": len(waves),
+                       "l2_policy": "inputs larger than L2", "parallelism": "beams per GPU, batched"},
+            "realtime_x": obs_s / batched_s,
+            "plain": {"value": tot["units"] * world / plain_s, "ms_per_step": plain_s * 1e3,
+                      "realtime_x": obs_s / plain_s,
+                      "fresh_pipeline_s": tot["plain_fresh_s"],
+                      "note": "beam by beam through the plain pipeline (device input/output), set-up excluded; "
+                              "fresh_pipeline_s = wall time of create+bind+first run per beam, summed"},
+            "batched_over_plain": plain_s / batched_s,
+            "bit_exact": bit_exact, "compared_ranges": n_cmp, "mismatches": mismatches[:10],
+            "batched": {"setup_s": tot["setup_s"], "work_items": tot["items"],
+                        "waves": wave_info},
+            "gpu_launches": tot["launches"] * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0 if bit_exact else 1
+
+
 def main():
     args = parse()
-    cfg = {"survey": SURVEY, "mid": MID, "small": SMALL}[args.config]
-    if args.nbits:
-        cfg = dict(cfg, nbits=args.nbits)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.config == "batched" and args.impl != "reference":
+        return run_batched(args, rank, world, local)
+    cfg = {"survey": SURVEY, "mid": MID, "small": SMALL, "batched": SURVEY}[args.config]
+    if args.nbits:
+        cfg = dict(cfg, nbits=args.nbits)
     if args.impl == "reference":
         return run_reference_arm(args, cfg, rank, world)
 

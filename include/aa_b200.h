@@ -295,7 +295,8 @@ float *aa_b200_batch_device_output(void *batch, int beam, int range);
 int aa_b200_batch_range_shape(void *batch, int beam, int range, int *ndms, long long *total_samps, int *inBin);
 int aa_b200_batch_info(void *batch, long long *work_items, int *persistent_jobs, int *other_jobs, int *grid,
                        size_t *smem_bytes, size_t *level_bytes, long long *launches_per_run);
-/* device time (ms) of the last run: which = 0 whole run, 1 dedispersion part */
+/* device time (ms) of the last run: which = 0 whole run, 1 dedispersion part
+ * (measured only when the batch runs without a graph; -1 otherwise) */
 double aa_b200_batch_last_ms(void *batch, int which);
 /* device bytes a beam needs inside a batch (outputs, tables, filterbank
  * levels), to split a beam list into batches that fit */
