@@ -1,0 +1,266 @@
+// frac.cu -- differentiable fractional-delay dedispersion and boxcar S/N for
+// candidate refinement (no counterpart in the reference, whose DDTR uses
+// integer delays only).
+//
+// Snippets x[b][c][t] (float32, B x C x T) are dedispersed at a continuous
+// trial DM per snippet:
+//     tau_c = dm_b * kc_c                      (samples; kc_c >= 0 per unit DM)
+//     n_c = floor(tau_c), w_c = tau_c - n_c    (evaluated in FP64)
+//     y[b][t] = sum_c x[c][t+n_c] + w_c * (x[c][t+n_c+1] - x[c][t+n_c])
+// with samples outside [0, T) read as 0.  Since t is an integer, n_c and w_c
+// do not depend on t: the adjoint is a shifted, interpolated copy of the
+// output gradient per channel (the transpose of the scatter), and
+//     dL/ddm_b = sum_c kc_c * sum_t gy[t] * (x[c][t+n_c+1] - x[c][t+n_c]).
+// Every kernel recomputes n_c and w_c from dm and kc instead of storing them.
+//
+// Boxcar S/N of y for widths w (ascending, <= 1024):
+//     snr[b][i][t] = (sum_{k<w_i} y'[t+k] - w_i mu_b) / (sigma_b sqrt(w_i))
+// with y' = y inside [0, T) and mu_b beyond it; mu and sigma are constants.
+#include <cmath>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "frac.cuh"
+
+namespace aab200 {
+
+namespace {
+
+constexpr int FT = 256; // threads per block (samples per block in the time-parallel kernels)
+
+__device__ __forceinline__ void delay_of(float dm, double kc, int &n, float &w)
+{
+    const double tau = static_cast<double>(dm) * kc;
+    const double f = floor(tau);
+    n = static_cast<int>(f);
+    w = static_cast<float>(tau - f);
+}
+
+__device__ __forceinline__ float at(const float *row, int i, int T) { return (i >= 0 && i < T) ? __ldg(row + i) : 0.f; }
+
+// y[b][t]: one thread per output sample, channels in order.
+__global__ void __launch_bounds__(FT) k_frac_fwd(const float *__restrict__ x, const float *__restrict__ dm,
+                                                 const double *__restrict__ kc, int C, int T, float *__restrict__ y)
+{
+    extern __shared__ int s_nw[]; // n[C] then w[C]
+    int *s_n = s_nw;
+    float *s_w = reinterpret_cast<float *>(s_nw + C);
+    const int b = blockIdx.y;
+    const float d = dm[b];
+    for (int c = threadIdx.x; c < C; c += blockDim.x)
+        delay_of(d, kc[c], s_n[c], s_w[c]);
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T)
+        return;
+    const float *xb = x + static_cast<size_t>(b) * C * T;
+    float acc = 0.f;
+#pragma unroll 8
+    for (int c = 0; c < C; ++c) {
+        const float *row = xb + static_cast<size_t>(c) * T;
+        const int i = t + s_n[c];
+        const float a0 = at(row, i, T);
+        const float a1 = at(row, i + 1, T);
+        acc += fmaf(s_w[c], a1 - a0, a0);
+    }
+    y[static_cast<size_t>(b) * T + t] = acc;
+}
+
+// gx[b][c][j] = (1 - w_c) gy[j - n_c] + w_c gy[j - n_c - 1]
+__global__ void __launch_bounds__(FT) k_frac_adj_x(const float *__restrict__ gy, const float *__restrict__ dm,
+                                                   const double *__restrict__ kc, int C, int T, float *__restrict__ gx)
+{
+    const int b = blockIdx.z, c = blockIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= T)
+        return;
+    int n;
+    float w;
+    delay_of(dm[b], kc[c], n, w);
+    const float *g = gy + static_cast<size_t>(b) * T;
+    const float v = (1.f - w) * at(g, j - n, T) + w * at(g, j - n - 1, T);
+    gx[(static_cast<size_t>(b) * C + c) * T + j] = v;
+}
+
+// partial[b][c] = kc_c * sum_t gy[t] (x[c][t+n+1] - x[c][t+n]), in FP64
+__global__ void __launch_bounds__(FT) k_frac_adj_dm_partial(const float *__restrict__ x, const float *__restrict__ gy,
+                                                            const float *__restrict__ dm, const double *__restrict__ kc,
+                                                            int C, int T, double *__restrict__ partial)
+{
+    __shared__ double red[FT / 32];
+    const int b = blockIdx.y, c = blockIdx.x;
+    int n;
+    float w;
+    delay_of(dm[b], kc[c], n, w);
+    const float *row = x + (static_cast<size_t>(b) * C + c) * T;
+    const float *g = gy + static_cast<size_t>(b) * T;
+    double acc = 0.0;
+    for (int t = threadIdx.x; t < T; t += blockDim.x) {
+        const int i = t + n;
+        acc += static_cast<double>(__ldg(g + t)) * static_cast<double>(at(row, i + 1, T) - at(row, i, T));
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0)
+        red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < FT / 32; ++k)
+            s += red[k];
+        partial[static_cast<size_t>(b) * C + c] = kc[c] * s;
+    }
+}
+
+// gdm[b] = sum_c partial[b][c], fixed order
+__global__ void __launch_bounds__(FT) k_frac_adj_dm_sum(const double *__restrict__ partial, int C,
+                                                        float *__restrict__ gdm)
+{
+    __shared__ double red[FT];
+    const int b = blockIdx.x;
+    double s = 0.0;
+    for (int c = threadIdx.x; c < C; c += blockDim.x)
+        s += partial[static_cast<size_t>(b) * C + c];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = FT / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h)
+            red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        gdm[b] = static_cast<float>(red[0]);
+}
+
+// snr[b][i][t]; the block stages y[t0, t0 + FT + wmax - 1) (mu beyond T).
+__global__ void __launch_bounds__(FT) k_boxcar_fwd(const float *__restrict__ y, int T, BoxcarWidths W,
+                                                   const float *__restrict__ mu, const float *__restrict__ sigma,
+                                                   float *__restrict__ snr)
+{
+    extern __shared__ float ys[];
+    const int b = blockIdx.y;
+    const int t0 = blockIdx.x * FT;
+    const int wmax = W.w[W.n - 1];
+    const float m = mu[b], sg = sigma[b];
+    const float *yb = y + static_cast<size_t>(b) * T;
+    for (int k = threadIdx.x; k < FT + wmax - 1; k += blockDim.x) {
+        const int t = t0 + k;
+        ys[k] = (t < T) ? yb[t] : m;
+    }
+    __syncthreads();
+    const int t = t0 + threadIdx.x;
+    if (t >= T)
+        return;
+    float s = 0.f;
+    int k = 0;
+    for (int i = 0; i < W.n; ++i) {
+        for (; k < W.w[i]; ++k)
+            s += ys[threadIdx.x + k];
+        const float wf = static_cast<float>(W.w[i]);
+        snr[(static_cast<size_t>(b) * W.n + i) * T + t] = (s - wf * m) / (sg * sqrtf(wf));
+    }
+}
+
+// gy[b][t] = sum_i 1/(sigma sqrt(w_i)) sum_{k<w_i, t-k>=0} gsnr[b][i][t-k]
+__global__ void __launch_bounds__(FT) k_boxcar_adj(const float *__restrict__ gsnr, int T, BoxcarWidths W,
+                                                   const float *__restrict__ sigma, float *__restrict__ gy)
+{
+    extern __shared__ float gs[]; // [n][FT + wmax - 1], covering t0 - wmax + 1 .. t0 + FT - 1
+    const int b = blockIdx.y;
+    const int t0 = blockIdx.x * FT;
+    const int wmax = W.w[W.n - 1];
+    const int span = FT + wmax - 1;
+    for (int i = 0; i < W.n; ++i) {
+        const float *g = gsnr + (static_cast<size_t>(b) * W.n + i) * T;
+        for (int k = threadIdx.x; k < span; k += blockDim.x) {
+            const int t = t0 - wmax + 1 + k;
+            gs[i * span + k] = (t >= 0 && t < T) ? g[t] : 0.f;
+        }
+    }
+    __syncthreads();
+    const int t = t0 + threadIdx.x;
+    if (t >= T)
+        return;
+    const float sg = sigma[b];
+    float acc = 0.f;
+    for (int i = 0; i < W.n; ++i) {
+        float s = 0.f;
+        const float *row = gs + i * span + (threadIdx.x + wmax - 1);
+        for (int k = 0; k < W.w[i]; ++k)
+            s += row[-k];
+        acc += s / (sg * sqrtf(static_cast<float>(W.w[i])));
+    }
+    gy[static_cast<size_t>(b) * T + t] = acc;
+}
+
+} // namespace
+
+cudaError_t launch_frac_fwd(const float *x, const float *dm, const double *kc, int B, int C, int T, float *y,
+                            cudaStream_t st)
+{
+    if (B <= 0 || C <= 0 || T <= 0 || B > 65535 || C > 16384)
+        return cudaErrorInvalidValue;
+    const size_t smem = static_cast<size_t>(C) * 8;
+    if (smem > 48 * 1024) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(k_frac_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess)
+            return e;
+    }
+    dim3 grid((T + FT - 1) / FT, B);
+    k_frac_fwd<<<grid, FT, smem, st>>>(x, dm, kc, C, T, y);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_frac_adj(const float *x, const float *dm, const double *kc, const float *gy, int B, int C, int T,
+                            float *gx, float *gdm, double *partial, cudaStream_t st)
+{
+    if (B <= 0 || C <= 0 || T <= 0 || B > 65535 || C > 65535)
+        return cudaErrorInvalidValue;
+    if (gx) {
+        dim3 grid((T + FT - 1) / FT, C, B);
+        k_frac_adj_x<<<grid, FT, 0, st>>>(gy, dm, kc, C, T, gx);
+    }
+    if (gdm) {
+        if (!partial)
+            return cudaErrorInvalidValue;
+        k_frac_adj_dm_partial<<<dim3(C, B), FT, 0, st>>>(x, gy, dm, kc, C, T, partial);
+        k_frac_adj_dm_sum<<<B, FT, 0, st>>>(partial, C, gdm);
+    }
+    return cudaGetLastError();
+}
+
+static bool widths_ok(const BoxcarWidths &W)
+{
+    if (W.n < 1 || W.n > kMaxBoxcarWidths)
+        return false;
+    for (int i = 0; i < W.n; ++i)
+        if (W.w[i] < 1 || W.w[i] > 1024 || (i > 0 && W.w[i] <= W.w[i - 1]))
+            return false;
+    return true;
+}
+
+cudaError_t launch_boxcar_fwd(const float *y, int B, int T, const BoxcarWidths &W, const float *mu, const float *sigma,
+                              float *snr, cudaStream_t st)
+{
+    if (B <= 0 || T <= 0 || B > 65535 || !widths_ok(W))
+        return cudaErrorInvalidValue;
+    const size_t smem = static_cast<size_t>(FT + W.w[W.n - 1] - 1) * sizeof(float);
+    k_boxcar_fwd<<<dim3((T + FT - 1) / FT, B), FT, smem, st>>>(y, T, W, mu, sigma, snr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_boxcar_adj(const float *gsnr, int B, int T, const BoxcarWidths &W, const float *sigma, float *gy,
+                              cudaStream_t st)
+{
+    if (B <= 0 || T <= 0 || B > 65535 || !widths_ok(W))
+        return cudaErrorInvalidValue;
+    const size_t smem = static_cast<size_t>(W.n) * (FT + W.w[W.n - 1] - 1) * sizeof(float);
+    if (smem > 48 * 1024)
+        return cudaErrorInvalidValue;
+    k_boxcar_adj<<<dim3((T + FT - 1) / FT, B), FT, smem, st>>>(gsnr, T, W, sigma, gy);
+    return cudaGetLastError();
+}
+
+} // namespace aab200
