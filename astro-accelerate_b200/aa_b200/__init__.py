@@ -160,11 +160,14 @@ def lib():
         "aa_b200_batch_estimate_bytes": ([filterbank_metadata_struct, vp, sz, P(sz)], i),
         "aa_b200_batch_last_error": ([vp], ctypes.c_char_p),
         "aa_b200_batch_delete": ([vp], None),
-        "aa_b200_frac_dedisperse_fwd": ([vp, vp, vp, i, i, i, vp, vp], i),
-        "aa_b200_frac_dedisperse_adj": ([vp, vp, vp, vp, i, i, i, vp, vp, vp, vp], i),
+        "aa_b200_frac_dedisperse_fwd": ([vp, vp, vp, vp, i, i, i, vp, vp], i),
+        "aa_b200_frac_dedisperse_adj": ([vp, vp, vp, vp, vp, i, i, i, vp, vp, vp, vp], i),
         "aa_b200_boxcar_snr_fwd": ([vp, i, i, P(i), i, vp, vp, vp, vp], i),
         "aa_b200_boxcar_snr_adj": ([vp, i, i, P(i), i, vp, vp, vp], i),
         "aa_b200_frac_last_error": ([], ctypes.c_char_p),
+        "aa_b200_sps_row_stats": ([vp, i, ll, ll, vp, vp, vp], i),
+        "aa_b200_sps_block_peaks": ([vp, i, ll, ll, vp, vp, P(i), i, vp, vp, vp, vp], i),
+        "aa_b200_sps_block_samples": ([], i),
     }
     for name, (args, res) in protos.items():
         fn = getattr(L, name)

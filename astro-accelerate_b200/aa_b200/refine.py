@@ -4,7 +4,8 @@ FracDedisperse and BoxcarSNR are torch.autograd.Functions whose forward and
 backward passes are the hand-written kernels of csrc/frac.cu, called through
 the C ABI (aa_b200_frac_*, aa_b200_boxcar_*); there is no PyTorch fallback.
 
-    y   = FracDedisperse.apply(x, dm, kc)        x [S][C][T] f32, dm [S] f32, kc [C] f64
+    y   = FracDedisperse.apply(x, dm, kc, base)  x [S][C][T] f32, dm [S] f32, kc [C] f64,
+                                                 base [S][C] int32 row shifts or None
     snr = BoxcarSNR.apply(y, widths, mu, sigma)  snr [S][len(widths)][T]
 
 The delays are recomputed from (dm, kc) in the backward pass.  mu and sigma
@@ -49,7 +50,7 @@ class FracDedisperse(torch.autograd.Function):
     """Fractional-delay (linearly interpolated) dedispersion; gradients to x and dm."""
 
     @staticmethod
-    def forward(ctx, x, dm, kc):
+    def forward(ctx, x, dm, kc, base=None):
         if x.dtype != torch.float32 or dm.dtype != torch.float32 or kc.dtype != torch.float64:
             raise TypeError("x, dm must be float32 and kc float64")
         x, dm, kc = x.contiguous(), dm.contiguous(), kc.contiguous()
@@ -57,16 +58,22 @@ class FracDedisperse(torch.autograd.Function):
         S, C, T = x.shape
         if dm.shape != (S,) or kc.shape != (C,):
             raise ValueError("dm must be [S] and kc [C]")
+        if base is not None:
+            base = base.to(torch.int32).contiguous()
+            _check_cuda(base)
+            if base.shape != (S, C):
+                raise ValueError("base must be [S][C]")
         y = torch.empty((S, T), dtype=torch.float32, device=x.device)
-        if lib().aa_b200_frac_dedisperse_fwd(x.data_ptr(), dm.data_ptr(), kc.data_ptr(), S, C, T, y.data_ptr(),
+        if lib().aa_b200_frac_dedisperse_fwd(x.data_ptr(), dm.data_ptr(), kc.data_ptr(),
+                                             base.data_ptr() if base is not None else None, S, C, T, y.data_ptr(),
                                              _stream()):
             raise RuntimeError(_err())
-        ctx.save_for_backward(x, dm, kc)
+        ctx.save_for_backward(x, dm, kc, base)
         return y
 
     @staticmethod
     def backward(ctx, gy):
-        x, dm, kc = ctx.saved_tensors
+        x, dm, kc, base = ctx.saved_tensors
         gy = gy.contiguous()
         S, C, T = x.shape
         need_x, need_dm = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
@@ -74,12 +81,13 @@ class FracDedisperse(torch.autograd.Function):
         gdm = torch.empty_like(dm) if need_dm else None
         partial = torch.empty((S, C), dtype=torch.float64, device=x.device) if need_dm else None
         if need_x or need_dm:
-            if lib().aa_b200_frac_dedisperse_adj(x.data_ptr(), dm.data_ptr(), kc.data_ptr(), gy.data_ptr(), S, C, T,
+            if lib().aa_b200_frac_dedisperse_adj(x.data_ptr(), dm.data_ptr(), kc.data_ptr(),
+                                                 base.data_ptr() if base is not None else None, gy.data_ptr(), S, C, T,
                                                  gx.data_ptr() if need_x else None,
                                                  gdm.data_ptr() if need_dm else None,
                                                  partial.data_ptr() if need_dm else None, _stream()):
                 raise RuntimeError(_err())
-        return gx, gdm, None
+        return gx, gdm, None, None
 
 
 class BoxcarSNR(torch.autograd.Function):
@@ -118,19 +126,19 @@ def smooth_peak(snr: torch.Tensor, temperature: float = 0.5) -> torch.Tensor:
     return temperature * torch.logsumexp(snr.flatten(1) / temperature, dim=1)
 
 
-def peak_snr(x, dm, kc, widths=DEFAULT_WIDTHS, mu=None, sigma=None, temperature: float = 0.5):
+def peak_snr(x, dm, kc, widths=DEFAULT_WIDTHS, mu=None, sigma=None, temperature: float = 0.5, base=None):
     """Smooth peak S/N [S] of snippets x at trial DMs dm (differentiable)."""
     S, C, _ = x.shape
     if mu is None:
         mu = torch.zeros(S, dtype=torch.float32, device=x.device)
     if sigma is None:
         sigma = torch.full((S,), float(np.sqrt(C)), dtype=torch.float32, device=x.device)
-    y = FracDedisperse.apply(x, dm, kc)
+    y = FracDedisperse.apply(x, dm, kc, base)
     return smooth_peak(BoxcarSNR.apply(y, tuple(widths), mu, sigma), temperature)
 
 
 def refine_dm(x, dm0, kc, steps: int = 50, lr: float = 0.05, widths=DEFAULT_WIDTHS, mu=None, sigma=None,
-              temperature: float = 0.5):
+              temperature: float = 0.5, base=None):
     """Adam ascent of the smooth peak S/N in DM, one trial DM per snippet.
     Returns (refined dm [S], peak S/N history [steps+1][S])."""
     dm = dm0.detach().clone().to(torch.float32).contiguous().requires_grad_(True)
@@ -138,12 +146,12 @@ def refine_dm(x, dm0, kc, steps: int = 50, lr: float = 0.05, widths=DEFAULT_WIDT
     hist = []
     for _ in range(steps):
         opt.zero_grad(set_to_none=True)
-        p = peak_snr(x, dm, kc, widths, mu, sigma, temperature)
+        p = peak_snr(x, dm, kc, widths, mu, sigma, temperature, base)
         hist.append(p.detach())
         (-p.sum()).backward()
         opt.step()
     with torch.no_grad():
-        hist.append(peak_snr(x, dm, kc, widths, mu, sigma, temperature))
+        hist.append(peak_snr(x, dm, kc, widths, mu, sigma, temperature, base))
     return dm.detach(), torch.stack(hist)
 
 

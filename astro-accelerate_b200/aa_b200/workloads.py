@@ -69,3 +69,46 @@ def plan_waves(sizes: list, budget: int) -> list:
         waves.append(cur)
     return waves
 
+
+
+# End-to-end search workload: 16 beams of 4096 channels, 8-bit, 2^20 samples,
+# the survey band and plan, 4-32 dispersed boxcar pulses per beam (DM U[50,
+# 2900], width log-U[0.25, 8] ms, 3-10 sigma per channel, cold-plasma delay
+# 4.148808e3 DM (f^-2 - fch1^-2) s), placed so that every sweep ends inside
+# the beam.
+def e2e_beams(seed: int = 5, nbeams: int = 16, nsamp: int = 1 << 20) -> list:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    beams = []
+    nch, fch1, foff, tsamp = 4096, 1670.0, -0.0732421875, 64e-6
+    f = fch1 + foff * np.arange(nch, dtype=np.float64)
+    kc = 4.148808e3 * (f ** -2 - fch1 ** -2) / tsamp
+    for b in range(nbeams):
+        pulses = []
+        for _ in range(int(rng.integers(4, 33))):
+            dm = float(rng.uniform(50, 2900))
+            width = max(1, int(round(np.exp(rng.uniform(np.log(0.25), np.log(8.0))) * 1e-3 / tsamp)))
+            amp = float(rng.uniform(3, 10))
+            sweep = int(np.ceil(dm * kc[-1])) + width
+            start = int(rng.integers(0, nsamp - sweep))
+            pulses.append(dict(dm=dm, width=width, amp_sigma=amp, start=start))
+        beams.append(dict(nchans=nch, nbits=8, nsamp=nsamp, fch1=fch1, foff=foff, tsamp=tsamp, plan=list(SURVEY_PLAN),
+                          seed=seed * 1000 + b, pulses=pulses))
+    return beams
+
+
+def synth_e2e_beam(beam: dict, device):
+    """The beam's noise (synth_beam_device) plus its pulses."""
+    import torch
+    x = synth_beam_device(beam, device)
+    nch = beam["nchans"]
+    f = beam["fch1"] + beam["foff"] * np.arange(nch, dtype=np.float64)
+    sig = 16.0
+    c = torch.arange(nch, device=device)
+    for p in beam["pulses"]:
+        d = torch.as_tensor(np.floor(4.148808e3 * p["dm"] * (f ** -2 - beam["fch1"] ** -2) / beam["tsamp"]),
+                            dtype=torch.int64, device=device)
+        for k in range(p["width"]):
+            tt = p["start"] + d + k
+            v = (x[tt, c].to(torch.int32) & 0xFFFF).to(torch.float32) + p["amp_sigma"] * sig
+            x[tt, c] = v.clamp_(0, 255).to(torch.int32).to(torch.int16)
+    return x

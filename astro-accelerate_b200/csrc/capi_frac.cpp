@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include "frac.cuh"
+#include "sps.cuh"
 
 using namespace aab200;
 
@@ -38,17 +39,19 @@ bool make_widths(const int *widths, int nwidths, BoxcarWidths &W)
 
 extern "C" {
 
-int aa_b200_frac_dedisperse_fwd(const float *d_x, const float *d_dm, const double *d_kc, int nsnip, int nchans,
-                                int nsamp, float *d_y, void *stream)
+int aa_b200_frac_dedisperse_fwd(const float *d_x, const float *d_dm, const double *d_kc, const int *d_base, int nsnip,
+                                int nchans, int nsamp, float *d_y, void *stream)
 {
-    return frac_status(launch_frac_fwd(d_x, d_dm, d_kc, nsnip, nchans, nsamp, d_y, static_cast<cudaStream_t>(stream)),
-                       "fractional dedispersion");
+    return frac_status(
+        launch_frac_fwd(d_x, d_dm, d_kc, d_base, nsnip, nchans, nsamp, d_y, static_cast<cudaStream_t>(stream)),
+        "fractional dedispersion");
 }
 
-int aa_b200_frac_dedisperse_adj(const float *d_x, const float *d_dm, const double *d_kc, const float *d_gy, int nsnip,
-                                int nchans, int nsamp, float *d_gx, float *d_gdm, double *d_partial, void *stream)
+int aa_b200_frac_dedisperse_adj(const float *d_x, const float *d_dm, const double *d_kc, const int *d_base,
+                                const float *d_gy, int nsnip, int nchans, int nsamp, float *d_gx, float *d_gdm,
+                                double *d_partial, void *stream)
 {
-    return frac_status(launch_frac_adj(d_x, d_dm, d_kc, d_gy, nsnip, nchans, nsamp, d_gx, d_gdm, d_partial,
+    return frac_status(launch_frac_adj(d_x, d_dm, d_kc, d_base, d_gy, nsnip, nchans, nsamp, d_gx, d_gdm, d_partial,
                                        static_cast<cudaStream_t>(stream)),
                        "fractional dedispersion adjoint");
 }
@@ -72,6 +75,27 @@ int aa_b200_boxcar_snr_adj(const float *d_gsnr, int nsnip, int nsamp, const int 
     return frac_status(launch_boxcar_adj(d_gsnr, nsnip, nsamp, W, d_sigma, d_gy, static_cast<cudaStream_t>(stream)),
                        "boxcar S/N adjoint");
 }
+
+int aa_b200_sps_row_stats(const float *d_y, int nrows, long long pitch, long long nsamp, float *d_mean,
+                          float *d_stdev, void *stream)
+{
+    return frac_status(launch_row_stats(d_y, nrows, pitch, nsamp, d_mean, d_stdev, static_cast<cudaStream_t>(stream)),
+                       "row statistics");
+}
+
+int aa_b200_sps_block_peaks(const float *d_y, int nrows, long long pitch, long long nsamp, const float *d_mean,
+                            const float *d_stdev, const int *widths, int nwidths, float *d_peak_snr, int *d_peak_t,
+                            int *d_peak_w, void *stream)
+{
+    BoxcarWidths W;
+    if (!make_widths(widths, nwidths, W))
+        return 1;
+    return frac_status(launch_block_peaks(d_y, nrows, pitch, nsamp, d_mean, d_stdev, W, d_peak_snr, d_peak_t, d_peak_w,
+                                          static_cast<cudaStream_t>(stream)),
+                       "block peaks");
+}
+
+int aa_b200_sps_block_samples(void) { return SPS_BLOCK; }
 
 const char *aa_b200_frac_last_error(void) { return g_frac_error.c_str(); }
 

@@ -5,13 +5,16 @@
 // Snippets x[b][c][t] (float32, B x C x T) are dedispersed at a continuous
 // trial DM per snippet:
 //     tau_c = dm_b * kc_c                      (samples; kc_c >= 0 per unit DM)
-//     n_c = floor(tau_c), w_c = tau_c - n_c    (evaluated in FP64)
+//     n_c = floor(tau_c) - base_c, w_c = frac(tau_c)   (evaluated in FP64)
 //     y[b][t] = sum_c x[c][t+n_c] + w_c * (x[c][t+n_c+1] - x[c][t+n_c])
 // with samples outside [0, T) read as 0.  Since t is an integer, n_c and w_c
 // do not depend on t: the adjoint is a shifted, interpolated copy of the
 // output gradient per channel (the transpose of the scatter), and
 //     dL/ddm_b = sum_c kc_c * sum_t gy[t] * (x[c][t+n_c+1] - x[c][t+n_c]).
-// Every kernel recomputes n_c and w_c from dm and kc instead of storing them.
+// base[b][c] (optional) is an integer shift of the snippet's channel rows: a
+// snippet cut with channel c starting base_c samples late is dedispersed at
+// the same DM as the uncut data.  Every kernel recomputes n_c and w_c from
+// dm, kc and base instead of storing them.
 //
 // Boxcar S/N of y for widths w (ascending, <= 1024):
 //     snr[b][i][t] = (sum_{k<w_i} y'[t+k] - w_i mu_b) / (sigma_b sqrt(w_i))
@@ -29,19 +32,25 @@ namespace {
 
 constexpr int FT = 256; // threads per block (samples per block in the time-parallel kernels)
 
-__device__ __forceinline__ void delay_of(float dm, double kc, int &n, float &w)
+__device__ __forceinline__ void delay_of(float dm, double kc, int base, int &n, float &w)
 {
     const double tau = static_cast<double>(dm) * kc;
     const double f = floor(tau);
-    n = static_cast<int>(f);
+    n = static_cast<int>(f) - base;
     w = static_cast<float>(tau - f);
+}
+
+__device__ __forceinline__ int base_of(const int *base, int b, int C, int c)
+{
+    return base ? base[static_cast<size_t>(b) * C + c] : 0;
 }
 
 __device__ __forceinline__ float at(const float *row, int i, int T) { return (i >= 0 && i < T) ? __ldg(row + i) : 0.f; }
 
-// y[b][t]: one thread per output sample, channels in order.
+// y[b][t]: one thread per output sample, channels in order, FP64 sum.
 __global__ void __launch_bounds__(FT) k_frac_fwd(const float *__restrict__ x, const float *__restrict__ dm,
-                                                 const double *__restrict__ kc, int C, int T, float *__restrict__ y)
+                                                 const double *__restrict__ kc, const int *__restrict__ base, int C,
+                                                 int T, float *__restrict__ y)
 {
     extern __shared__ int s_nw[]; // n[C] then w[C]
     int *s_n = s_nw;
@@ -49,27 +58,28 @@ __global__ void __launch_bounds__(FT) k_frac_fwd(const float *__restrict__ x, co
     const int b = blockIdx.y;
     const float d = dm[b];
     for (int c = threadIdx.x; c < C; c += blockDim.x)
-        delay_of(d, kc[c], s_n[c], s_w[c]);
+        delay_of(d, kc[c], base_of(base, b, C, c), s_n[c], s_w[c]);
     __syncthreads();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T)
         return;
     const float *xb = x + static_cast<size_t>(b) * C * T;
-    float acc = 0.f;
+    double acc = 0.0; // the kernel is bound by HBM: FP64 sums cost nothing and round once
 #pragma unroll 8
     for (int c = 0; c < C; ++c) {
         const float *row = xb + static_cast<size_t>(c) * T;
         const int i = t + s_n[c];
         const float a0 = at(row, i, T);
         const float a1 = at(row, i + 1, T);
-        acc += fmaf(s_w[c], a1 - a0, a0);
+        acc += static_cast<double>(fmaf(s_w[c], a1 - a0, a0));
     }
-    y[static_cast<size_t>(b) * T + t] = acc;
+    y[static_cast<size_t>(b) * T + t] = static_cast<float>(acc);
 }
 
 // gx[b][c][j] = (1 - w_c) gy[j - n_c] + w_c gy[j - n_c - 1]
 __global__ void __launch_bounds__(FT) k_frac_adj_x(const float *__restrict__ gy, const float *__restrict__ dm,
-                                                   const double *__restrict__ kc, int C, int T, float *__restrict__ gx)
+                                                   const double *__restrict__ kc, const int *__restrict__ base, int C,
+                                                   int T, float *__restrict__ gx)
 {
     const int b = blockIdx.z, c = blockIdx.y;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -77,7 +87,7 @@ __global__ void __launch_bounds__(FT) k_frac_adj_x(const float *__restrict__ gy,
         return;
     int n;
     float w;
-    delay_of(dm[b], kc[c], n, w);
+    delay_of(dm[b], kc[c], base_of(base, b, C, c), n, w);
     const float *g = gy + static_cast<size_t>(b) * T;
     const float v = (1.f - w) * at(g, j - n, T) + w * at(g, j - n - 1, T);
     gx[(static_cast<size_t>(b) * C + c) * T + j] = v;
@@ -86,13 +96,14 @@ __global__ void __launch_bounds__(FT) k_frac_adj_x(const float *__restrict__ gy,
 // partial[b][c] = kc_c * sum_t gy[t] (x[c][t+n+1] - x[c][t+n]), in FP64
 __global__ void __launch_bounds__(FT) k_frac_adj_dm_partial(const float *__restrict__ x, const float *__restrict__ gy,
                                                             const float *__restrict__ dm, const double *__restrict__ kc,
-                                                            int C, int T, double *__restrict__ partial)
+                                                            const int *__restrict__ base, int C, int T,
+                                                            double *__restrict__ partial)
 {
     __shared__ double red[FT / 32];
     const int b = blockIdx.y, c = blockIdx.x;
     int n;
     float w;
-    delay_of(dm[b], kc[c], n, w);
+    delay_of(dm[b], kc[c], base_of(base, b, C, c), n, w);
     const float *row = x + (static_cast<size_t>(b) * C + c) * T;
     const float *g = gy + static_cast<size_t>(b) * T;
     double acc = 0.0;
@@ -196,8 +207,8 @@ __global__ void __launch_bounds__(FT) k_boxcar_adj(const float *__restrict__ gsn
 
 } // namespace
 
-cudaError_t launch_frac_fwd(const float *x, const float *dm, const double *kc, int B, int C, int T, float *y,
-                            cudaStream_t st)
+cudaError_t launch_frac_fwd(const float *x, const float *dm, const double *kc, const int *base, int B, int C, int T,
+                            float *y, cudaStream_t st)
 {
     if (B <= 0 || C <= 0 || T <= 0 || B > 65535 || C > 16384)
         return cudaErrorInvalidValue;
@@ -209,23 +220,23 @@ cudaError_t launch_frac_fwd(const float *x, const float *dm, const double *kc, i
             return e;
     }
     dim3 grid((T + FT - 1) / FT, B);
-    k_frac_fwd<<<grid, FT, smem, st>>>(x, dm, kc, C, T, y);
+    k_frac_fwd<<<grid, FT, smem, st>>>(x, dm, kc, base, C, T, y);
     return cudaGetLastError();
 }
 
-cudaError_t launch_frac_adj(const float *x, const float *dm, const double *kc, const float *gy, int B, int C, int T,
-                            float *gx, float *gdm, double *partial, cudaStream_t st)
+cudaError_t launch_frac_adj(const float *x, const float *dm, const double *kc, const int *base, const float *gy, int B,
+                            int C, int T, float *gx, float *gdm, double *partial, cudaStream_t st)
 {
     if (B <= 0 || C <= 0 || T <= 0 || B > 65535 || C > 65535)
         return cudaErrorInvalidValue;
     if (gx) {
         dim3 grid((T + FT - 1) / FT, C, B);
-        k_frac_adj_x<<<grid, FT, 0, st>>>(gy, dm, kc, C, T, gx);
+        k_frac_adj_x<<<grid, FT, 0, st>>>(gy, dm, kc, base, C, T, gx);
     }
     if (gdm) {
         if (!partial)
             return cudaErrorInvalidValue;
-        k_frac_adj_dm_partial<<<dim3(C, B), FT, 0, st>>>(x, gy, dm, kc, C, T, partial);
+        k_frac_adj_dm_partial<<<dim3(C, B), FT, 0, st>>>(x, gy, dm, kc, base, C, T, partial);
         k_frac_adj_dm_sum<<<B, FT, 0, st>>>(partial, C, gdm);
     }
     return cudaGetLastError();

@@ -12,13 +12,14 @@ struct BoxcarWidths {
     int w[kMaxBoxcarWidths]; // ascending, 1..1024
 };
 
-// y[B][T] from x[B][C][T], dm[B] (device), kc[C] (device, FP64 samples per unit DM)
-cudaError_t launch_frac_fwd(const float *x, const float *dm, const double *kc, int B, int C, int T, float *y,
-                            cudaStream_t st);
+// y[B][T] from x[B][C][T], dm[B] (device), kc[C] (device, FP64 samples per
+// unit DM), base[B][C] (device, integer row shifts, or null)
+cudaError_t launch_frac_fwd(const float *x, const float *dm, const double *kc, const int *base, int B, int C, int T,
+                            float *y, cudaStream_t st);
 // gx[B][C][T] (skipped when null) and gdm[B] (skipped when null; needs
 // partial[B][C] FP64 scratch) from the output gradient gy[B][T]
-cudaError_t launch_frac_adj(const float *x, const float *dm, const double *kc, const float *gy, int B, int C, int T,
-                            float *gx, float *gdm, double *partial, cudaStream_t st);
+cudaError_t launch_frac_adj(const float *x, const float *dm, const double *kc, const int *base, const float *gy, int B,
+                            int C, int T, float *gx, float *gdm, double *partial, cudaStream_t st);
 // snr[B][W.n][T] from y[B][T], mu[B], sigma[B] (device)
 cudaError_t launch_boxcar_fwd(const float *y, int B, int T, const BoxcarWidths &W, const float *mu, const float *sigma,
                               float *snr, cudaStream_t st);

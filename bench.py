@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="survey", choices=["survey", "mid", "small", "batched"])
+    ap.add_argument("--config", default="survey", choices=["survey", "mid", "small", "batched", "refine", "e2e"])
     ap.add_argument("--beams", type=int, default=48, help="beams of the multi-beam draw (batched config)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
@@ -386,6 +386,267 @@ def run_batched(args, rank, world, local):
     return 0 if bit_exact else 1
 
 
+def _search_and_refine(aa, SR, R, x, kc, outputs, strat, k=64, steps=50):
+    """Candidates >= 6 sigma of every range, the k strongest events, their
+    snippets and refined DMs.  outputs[r] = (rows tensor, nsamp)."""
+    cands = []
+    for r, (rows, nsamp) in enumerate(outputs):
+        d = strat["dm"][r]
+        cands.append(SR.candidates(rows, nsamp, d[0], d[2], d[3], threshold=6.0))
+    top = SR.select(cands, k=k)
+    if top["dm"].numel() == 0:
+        return top, None, None
+    snip, base = SR.cut_snippets(x, kc, top["dm"], top["t"], top["w"])
+    return top, snip, base
+
+
+def _match_errors(top, dm_ref, pulses, inbin_tol=512):
+    """|DM error| before and after refinement for candidates that match an
+    injected pulse (arrival within inbin_tol samples)."""
+    before, after, found = [], [], set()
+    t = top["t"].cpu().numpy()
+    d0 = top["dm"].cpu().numpy()
+    d1 = dm_ref.cpu().numpy()
+    for i in range(len(t)):
+        best = None
+        for j, p in enumerate(pulses):
+            dt = abs(int(t[i]) - p["start"])
+            if dt <= inbin_tol + p["width"] and (best is None or dt < best[0]):
+                best = (dt, j)
+        if best is not None:
+            p = pulses[best[1]]
+            before.append(abs(float(d0[i]) - p["dm"]))
+            after.append(abs(float(d1[i]) - p["dm"]))
+            found.add(best[1])
+    return before, after, len(found)
+
+
+def run_e2e(args, rank, world, local):
+    """End-to-end search: 16 beams x 4096 channels x 2^20 8-bit samples with
+    4-32 injected pulses each; batched DDTR (one graph per batch), 6-sigma
+    boxcar candidates, the 64 strongest events per beam cut to 1024-sample
+    per-channel snippets, 50 Adam steps on DM through the adjoint kernels.
+    The same search runs after the plain per-beam pipeline; wall times
+    exclude data generation; every DDTR output is compared bit for bit."""
+    import numpy as np
+    import torch
+    import aa_b200 as aa
+    from aa_b200 import refine as R
+    from aa_b200 import search as SR
+    from aa_b200 import workloads as WL
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    beams = WL.e2e_beams(seed=5 + 1000 * rank, nbeams=args.beams if args.beams != 48 else 16)
+    b0 = beams[0]
+    kc = R.delay_per_dm(b0["nchans"], b0["fch1"], b0["foff"], b0["tsamp"])
+    mds, plans, strats, sizes = [], [], [], []
+    for b in beams:
+        md = aa.filterbank_metadata_struct(0.0, b["tsamp"], b["fch1"], b["foff"], 8, b["nsamp"], b["nchans"], 0.0)
+        plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in b["plan"]])
+        mds.append(md)
+        plans.append(plan)
+        strats.append(aa.strategy(b["plan"], b["nchans"], b["nsamp"], b["fch1"], b["foff"], b["tsamp"], 8,
+                                  MULTIBEAM_FREE_MEMORY))
+        sizes.append(aa.batch_estimate_bytes(md, plan, MULTIBEAM_FREE_MEMORY) + 2 * b["nsamp"] * b["nchans"])
+    free, _ = torch.cuda.mem_get_info(device)
+    reserve = max(sizes) + (64 * 4096 * 1024 * 4) * 6
+    waves = WL.plan_waves(sizes, int(free * 0.85) - reserve)
+    T = dict(b_ddtr=0.0, b_setup=0.0, b_search=0.0, b_refine=0.0, p_ddtr=0.0, p_setup=0.0, p_search=0.0,
+             p_refine=0.0)
+    errs_b, errs_p, bit_exact, n_found, n_injected, n_cand = [], [], True, 0, 0, 0
+
+    def sync_time(t0):
+        torch.cuda.synchronize(device)
+        return time.perf_counter() - t0
+
+    for w in waves:
+        xs = {i: WL.synth_e2e_beam(beams[i], device) for i in w}
+        torch.cuda.synchronize(device)
+        # ---- batched path
+        t0 = time.perf_counter()
+        B = aa.batch(free_memory=MULTIBEAM_FREE_MEMORY)
+        for i in w:
+            B.add_beam(mds[i], plans[i], xs[i])
+        B.setup()
+        T["b_setup"] += sync_time(t0)
+        t0 = time.perf_counter()
+        B.run()
+        B.synchronize()
+        T["b_ddtr"] += sync_time(t0)
+        t0 = time.perf_counter()
+        per_beam = []
+        for j, i in enumerate(w):
+            outs = [(B.output(j, r), B.range_shape(j, r)[1]) for r in range(len(beams[i]["plan"]))]
+            per_beam.append(_search_and_refine(aa, SR, R, xs[i], kc, outs, strats[i]))
+        T["b_search"] += sync_time(t0)
+        t0 = time.perf_counter()
+        snips = [pb for pb in per_beam if pb[1] is not None]
+        if snips:
+            x_all = torch.cat([s[1] for s in snips])
+            base_all = torch.cat([s[2] for s in snips])
+            dm0 = torch.cat([s[0]["dm"] for s in snips])
+            dm_ref, _ = R.refine_dm(x_all, dm0, kc, steps=50, lr=0.05, base=base_all)
+        T["b_refine"] += sync_time(t0)
+        off = 0
+        for (top, snip, _), i in zip(per_beam, w):
+            if snip is None:
+                continue
+            n = top["dm"].numel()
+            bf, af, nf = _match_errors(top, dm_ref[off:off + n], beams[i]["pulses"])
+            off += n
+            errs_b.append((bf, af))
+            n_found += nf
+            n_cand += n
+            n_injected += len(beams[i]["pulses"])
+        # ---- plain path, beam by beam
+        for j, i in enumerate(w):
+            t0 = time.perf_counter()
+            pipe = aa.create_pipeline(mds[i], xs[i].data_ptr(), device_input=True, device_output=True,
+                                      copy_to_host=False)
+            pipe.set_options(free_memory=MULTIBEAM_FREE_MEMORY)
+            if not pipe.bind_ddtr_plan(plans[i]):
+                raise RuntimeError(pipe.last_error())
+            T["p_setup"] += sync_time(t0)
+            t0 = time.perf_counter()
+            if not (pipe.run_all() and pipe.synchronize()):
+                raise RuntimeError(pipe.last_error())
+            T["p_ddtr"] += sync_time(t0)
+            outs = []
+            for r in range(len(beams[i]["plan"])):
+                ndms, tot, _ = B.range_shape(j, r)
+                rows = dev_rows(aa, pipe.device_output(r), (ndms, tot))
+                if not torch.equal(rows.view(torch.int32), B.output(j, r).view(torch.int32)):
+                    bit_exact = False
+                outs.append((rows, tot))
+            t0 = time.perf_counter()
+            top, snip, base = _search_and_refine(aa, SR, R, xs[i], kc, outs, strats[i])
+            T["p_search"] += sync_time(t0)
+            t0 = time.perf_counter()
+            if snip is not None:
+                dm_p, _ = R.refine_dm(snip, top["dm"], kc, steps=50, lr=0.05, base=base)
+                bf, af, _ = _match_errors(top, dm_p, beams[i]["pulses"])
+                errs_p.append((bf, af))
+            T["p_refine"] += sync_time(t0)
+            pipe.cleanUp()
+            pipe.delete()
+        B.delete()
+        del xs
+        torch.cuda.empty_cache()
+    for p in plans:
+        p.delete()
+    eb = [v for bf, _ in errs_b for v in bf]
+    ea = [v for _, af in errs_b for v in af]
+    batched_s = T["b_ddtr"] + T["b_search"] + T["b_refine"]
+    plain_s = T["p_ddtr"] + T["p_search"] + T["p_refine"]
+    line = {"metric": "end-to-end search wall time (batched DDTR + 6-sigma search + top-64 + 50 Adam DM steps)",
+            "value": batched_s, "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": False,
+            "dtype": "u8+f32", "data": "synthetic",
+            "config": {"workload": f"{len(beams)} beams x 4096 ch x 2^20 8-bit samples, survey plan, 4-32 pulses each",
+                       "waves": len(waves)},
+            "batched_s": batched_s, "plain_s": plain_s, "plain_over_batched": plain_s / batched_s,
+            "batched_with_setup_s": batched_s + T["b_setup"], "plain_with_setup_s": plain_s + T["p_setup"],
+            "times": T, "ddtr_bit_exact": bit_exact,
+            "candidates": n_cand, "injected": n_injected, "injected_recovered": n_found,
+            "dm_error_median": {"before_refinement": float(np.median(eb)) if eb else None,
+                                "after_refinement": float(np.median(ea)) if ea else None,
+                                "matched_candidates": len(eb)},
+            "dm_error_mean": {"before_refinement": float(np.mean(eb)) if eb else None,
+                              "after_refinement": float(np.mean(ea)) if ea else None}}
+    print(json.dumps(line), flush=True)
+    return 0 if bit_exact else 1
+
+
+def run_refine(args, rank, world, local):
+    """Differentiable refinement workload: 256 snippets x 1024 channels x 8192
+    samples float32 (N(0,1) + one dispersed Gaussian pulse each), one step =
+    smooth peak boxcar S/N forward and its backward to the input and to DM.
+    Kernel times by CUDA events; the gradient error against the FP64 host
+    oracle and a central difference is measured on two snippets."""
+    import numpy as np
+    import torch
+    from aa_b200 import refine as R
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import frac_oracle as F
+
+    torch.cuda.set_device(local)
+    S, C, T = 256, 1024, 8192
+    x, dm_true, dm_trial, kc = R.synth_snippets(S, nchans=C, nsamp=T, seed=4 + rank)
+    widths = R.DEFAULT_WIDTHS
+    mu = torch.zeros(S, device="cuda")
+    sigma = torch.full((S,), float(np.sqrt(C)), device="cuda")
+    xg = x.clone().requires_grad_(True)
+
+    def step():
+        d = dm_trial.clone().requires_grad_(True)
+        y = R.FracDedisperse.apply(xg, d, kc)
+        p = R.smooth_peak(R.BoxcarSNR.apply(y, widths, mu, sigma))
+        p.sum().backward()
+        return d.grad
+
+    for _ in range(max(3, args.warmup)):
+        step()
+        xg.grad = None
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    fwd_ms, adj_ms, step_ms = [], [], []
+    for _ in range(args.steps):
+        d = dm_trial.clone()
+        e[0].record()
+        y = R.FracDedisperse.apply(x, d, kc)
+        e[1].record()
+        gy = torch.ones_like(y)
+        gx = torch.empty_like(x)
+        gdm = torch.empty_like(d)
+        part = torch.empty((S, C), dtype=torch.float64, device="cuda")
+        e[2].record()
+        R.lib().aa_b200_frac_dedisperse_adj(x.data_ptr(), d.data_ptr(), kc.data_ptr(), None, gy.data_ptr(), S, C, T,
+                                            gx.data_ptr(), gdm.data_ptr(), part.data_ptr(), R._stream())
+        e[3].record()
+        torch.cuda.synchronize()
+        fwd_ms.append(e[0].elapsed_time(e[1]))
+        adj_ms.append(e[2].elapsed_time(e[3]))
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        step()
+        t1.record()
+        torch.cuda.synchronize()
+        xg.grad = None
+        step_ms.append(t0.elapsed_time(t1))
+    # gradient error on two snippets against FP64
+    errs = []
+    xh, kch = x[:2].cpu().numpy(), kc.cpu().numpy()
+    d2 = dm_trial[:2].clone().requires_grad_(True)
+    p2 = R.peak_snr(x[:2].contiguous(), d2, kc, widths)
+    p2.sum().backward()
+    for s in range(2):
+        _, g64 = F.loss_and_grad_dm(xh[s], float(dm_trial[s]), kch, widths, 0.0, float(np.sqrt(C)), 0.5)
+        errs.append(abs(float(d2.grad[s]) - g64) / max(1e-30, abs(g64)))
+    bytes_x = S * C * T * 4
+    fwd = statistics.median(fwd_ms)
+    adj = statistics.median(adj_ms)
+    stp = statistics.median(step_ms)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    line = {"metric": "snippets/s (refinement step: forward + adjoint to input and DM)", "value": S / (stp / 1e3),
+            "unit": "snippets/s", "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": stp,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "refinement: 256 snippets x 1024 ch x 8192 samples f32, widths 1..64"},
+            "kernels": {"frac_fwd_ms": fwd, "frac_adj_ms": adj,
+                        "frac_fwd_gbs": bytes_x / fwd / 1e6, "frac_adj_gbs": 2 * bytes_x / adj / 1e6},
+            "roofline": {"bound": "hbm", "kernel": "k_frac_fwd", "achieved": bytes_x / fwd / 1e6, "peak": hbm,
+                         "unit": "GB/s", "frac": bytes_x / fwd / 1e6 / hbm},
+            "grad_rel_err_vs_fp64": errs}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -393,7 +654,12 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.config == "batched" and args.impl != "reference":
         return run_batched(args, rank, world, local)
-    cfg = {"survey": SURVEY, "mid": MID, "small": SMALL, "batched": SURVEY}[args.config]
+    if args.config == "refine" and args.impl != "reference":
+        return run_refine(args, rank, world, local)
+    if args.config == "e2e" and args.impl != "reference":
+        return run_e2e(args, rank, world, local)
+    cfg = {"survey": SURVEY, "mid": MID, "small": SMALL, "batched": SURVEY, "refine": SURVEY,
+           "e2e": SURVEY}[args.config]
     if args.nbits:
         cfg = dict(cfg, nbits=args.nbits)
     if args.impl == "reference":

@@ -312,18 +312,21 @@ void aa_b200_batch_delete(void *batch);
  *
  * Fractional-delay dedispersion of nsnip snippets x[nsnip][nchans][nsamp]
  * (float32) at a continuous DM per snippet dm[nsnip]: with
- * tau_c = dm * kc[c] (kc: FP64 delay in samples per unit DM, >= 0),
- * n = floor(tau_c), w = tau_c - n (FP64),
+ * tau_c = dm * kc[c] (kc: FP64 delay in samples per unit DM),
+ * n = floor(tau_c) - base[s][c], w = tau_c - floor(tau_c) (FP64; d_base, an
+ * int array [nsnip][nchans] of row shifts for snippets cut per channel, may
+ * be null),
  *   y[s][t] = sum_c x[s][c][t+n] + w (x[s][c][t+n+1] - x[s][c][t+n]),
  * samples outside [0, nsamp) read as 0.  The adjoint recomputes the delays and
  * writes gx = dL/dx (skipped when d_gx is null) and gdm = dL/ddm (skipped
  * when d_gdm is null; needs d_partial, nsnip*nchans doubles of scratch the
  * caller provides).
  * --------------------------------------------------------------------------- */
-int aa_b200_frac_dedisperse_fwd(const float *d_x, const float *d_dm, const double *d_kc, int nsnip, int nchans,
-                                int nsamp, float *d_y, void *stream);
-int aa_b200_frac_dedisperse_adj(const float *d_x, const float *d_dm, const double *d_kc, const float *d_gy, int nsnip,
-                                int nchans, int nsamp, float *d_gx, float *d_gdm, double *d_partial, void *stream);
+int aa_b200_frac_dedisperse_fwd(const float *d_x, const float *d_dm, const double *d_kc, const int *d_base, int nsnip,
+                                int nchans, int nsamp, float *d_y, void *stream);
+int aa_b200_frac_dedisperse_adj(const float *d_x, const float *d_dm, const double *d_kc, const int *d_base,
+                                const float *d_gy, int nsnip, int nchans, int nsamp, float *d_gx, float *d_gdm,
+                                double *d_partial, void *stream);
 /* Boxcar S/N: snr[s][i][t] = (sum_{k<w_i} y'[s][t+k] - w_i mu[s]) /
  * (sigma[s] sqrt(w_i)), y' = y inside [0, nsamp) and mu beyond; widths (host
  * array) ascending in 1..1024, at most 16.  mu and sigma are constants of the
@@ -333,6 +336,20 @@ int aa_b200_boxcar_snr_fwd(const float *d_y, int nsnip, int nsamp, const int *wi
 int aa_b200_boxcar_snr_adj(const float *d_gsnr, int nsnip, int nsamp, const int *widths, int nwidths,
                            const float *d_sigma, float *d_gy, void *stream);
 const char *aa_b200_frac_last_error(void);
+
+/* Single-pulse search on a DM-time range (rows of nsamp floats, row pitch in
+ * floats), a reduced form of the reference's analysis step
+ * (src/aa_device_analysis.cu:130-510): row mean and standard deviation (FP64
+ * sums), then per (row, block of aa_b200_sps_block_samples() samples) the
+ * largest white-noise boxcar S/N (sum_{k<w} y[t+k] - w mean) / (std sqrt w)
+ * over the block's start samples t and the widths (ascending, 1..1024, at
+ * most 16), with its t and w.  Peak arrays hold nrows * nblocks entries. */
+int aa_b200_sps_row_stats(const float *d_y, int nrows, long long pitch, long long nsamp, float *d_mean,
+                          float *d_stdev, void *stream);
+int aa_b200_sps_block_peaks(const float *d_y, int nrows, long long pitch, long long nsamp, const float *d_mean,
+                            const float *d_stdev, const int *widths, int nwidths, float *d_peak_snr, int *d_peak_t,
+                            int *d_peak_w, void *stream);
+int aa_b200_sps_block_samples(void);
 
 #ifdef __cplusplus
 }

@@ -7,7 +7,7 @@ with their analytic gradients, and the central finite differences that pin
 those gradients.  Only tests/, __graft_entry__.smoke() and bench.py's
 baseline leg use it.
 
-    tau_c = dm * kc_c, n_c = floor(tau_c), w_c = tau_c - n_c
+    tau_c = dm * kc_c, n_c = floor(tau_c) - base_c, w_c = tau_c - floor(tau_c)
     y[t]  = sum_c x[c][t+n_c] + w_c (x[c][t+n_c+1] - x[c][t+n_c])   (0 outside [0, T))
     snr[i][t] = (sum_{k<w_i} y'[t+k] - w_i mu) / (sigma sqrt(w_i)),  y' = mu beyond T
 """
@@ -34,12 +34,12 @@ def _shift(row: np.ndarray, n: int) -> np.ndarray:
     return out
 
 
-def frac_forward(x: np.ndarray, dm: float, kc: np.ndarray) -> np.ndarray:
-    """y[T] for one snippet x[C][T]."""
+def frac_forward(x: np.ndarray, dm: float, kc: np.ndarray, base=None) -> np.ndarray:
+    """y[T] for one snippet x[C][T]; base[C]: integer row shifts (or None)."""
     x = np.asarray(x, dtype=np.float64)
     tau = float(np.float32(dm)) * kc
-    n = np.floor(tau).astype(np.int64)
-    w = tau - n
+    w = tau - np.floor(tau)
+    n = np.floor(tau).astype(np.int64) - (0 if base is None else np.asarray(base, np.int64))
     y = np.zeros(x.shape[1], dtype=np.float64)
     for c in range(x.shape[0]):
         a0 = _shift(x[c], int(n[c]))
@@ -48,13 +48,13 @@ def frac_forward(x: np.ndarray, dm: float, kc: np.ndarray) -> np.ndarray:
     return y
 
 
-def frac_adjoint(x: np.ndarray, dm: float, kc: np.ndarray, gy: np.ndarray):
+def frac_adjoint(x: np.ndarray, dm: float, kc: np.ndarray, gy: np.ndarray, base=None):
     """(gx[C][T], gdm) for one snippet."""
     x = np.asarray(x, dtype=np.float64)
     gy = np.asarray(gy, dtype=np.float64)
     tau = float(np.float32(dm)) * kc
-    n = np.floor(tau).astype(np.int64)
-    w = tau - n
+    w = tau - np.floor(tau)
+    n = np.floor(tau).astype(np.int64) - (0 if base is None else np.asarray(base, np.int64))
     gx = np.zeros_like(x)
     gdm = 0.0
     for c in range(x.shape[0]):
