@@ -5,8 +5,12 @@ backward passes are the hand-written kernels of csrc/frac.cu, called through
 the C ABI (aa_b200_frac_*, aa_b200_boxcar_*); there is no PyTorch fallback.
 
     y   = FracDedisperse.apply(x, dm, kc, base)  x [S][C][T] f32, dm [S] f32, kc [C] f64,
-                                                 base [S][C] int32 row shifts or None
-    snr = BoxcarSNR.apply(y, widths, mu, sigma)  snr [S][len(widths)][T]
+                                                 base [S][C] int32 row shifts or None; y [S][T] f64
+    snr = BoxcarSNR.apply(y, widths, mu, sigma)  snr [S][len(widths)][T] f64
+
+The snippets stay float32; the channel sums, the series y and the S/N and
+their gradients are FP64, so that a smooth maximum of the S/N at a low
+temperature (which amplifies rounding) keeps an FP64-accurate DM gradient.
 
 The delays are recomputed from (dm, kc) in the backward pass.  mu and sigma
 (per snippet) are constants of the S/N: by default the noise level of the
@@ -63,7 +67,7 @@ class FracDedisperse(torch.autograd.Function):
             _check_cuda(base)
             if base.shape != (S, C):
                 raise ValueError("base must be [S][C]")
-        y = torch.empty((S, T), dtype=torch.float32, device=x.device)
+        y = torch.empty((S, T), dtype=torch.float64, device=x.device)
         if lib().aa_b200_frac_dedisperse_fwd(x.data_ptr(), dm.data_ptr(), kc.data_ptr(),
                                              base.data_ptr() if base is not None else None, S, C, T, y.data_ptr(),
                                              _stream()):
@@ -74,7 +78,7 @@ class FracDedisperse(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gy):
         x, dm, kc, base = ctx.saved_tensors
-        gy = gy.contiguous()
+        gy = gy.to(torch.float64).contiguous()
         S, C, T = x.shape
         need_x, need_dm = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
         gx = torch.empty_like(x) if need_x else None
@@ -95,11 +99,11 @@ class BoxcarSNR(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, y, widths, mu, sigma):
-        y = y.contiguous()
+        y = y.to(torch.float64).contiguous()
         _check_cuda(y, mu, sigma)
         S, T = y.shape
         w = (ctypes.c_int * len(widths))(*widths)
-        snr = torch.empty((S, len(widths), T), dtype=torch.float32, device=y.device)
+        snr = torch.empty((S, len(widths), T), dtype=torch.float64, device=y.device)
         if lib().aa_b200_boxcar_snr_fwd(y.data_ptr(), S, T, w, len(widths), mu.data_ptr(), sigma.data_ptr(),
                                         snr.data_ptr(), _stream()):
             raise RuntimeError(_err())
@@ -111,10 +115,10 @@ class BoxcarSNR(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gsnr):
         (sigma,) = ctx.saved_tensors
-        gsnr = gsnr.contiguous()
+        gsnr = gsnr.to(torch.float64).contiguous()
         S = gsnr.shape[0]
         w = (ctypes.c_int * len(ctx.widths))(*ctx.widths)
-        gy = torch.empty((S, ctx.T), dtype=torch.float32, device=gsnr.device)
+        gy = torch.empty((S, ctx.T), dtype=torch.float64, device=gsnr.device)
         if lib().aa_b200_boxcar_snr_adj(gsnr.data_ptr(), S, ctx.T, w, len(ctx.widths), sigma.data_ptr(),
                                         gy.data_ptr(), _stream()):
             raise RuntimeError(_err())
@@ -142,6 +146,10 @@ def refine_dm(x, dm0, kc, steps: int = 50, lr: float = 0.05, widths=DEFAULT_WIDT
     """Adam ascent of the smooth peak S/N in DM, one trial DM per snippet.
     Returns (refined dm [S], peak S/N history [steps+1][S])."""
     dm = dm0.detach().clone().to(torch.float32).contiguous().requires_grad_(True)
+    if mu is not None:
+        mu = mu.to(torch.float32).contiguous()
+    if sigma is not None:
+        sigma = sigma.to(torch.float32).contiguous()
     opt = torch.optim.Adam([dm], lr=lr)
     hist = []
     for _ in range(steps):

@@ -40,7 +40,7 @@ bool make_widths(const int *widths, int nwidths, BoxcarWidths &W)
 extern "C" {
 
 int aa_b200_frac_dedisperse_fwd(const float *d_x, const float *d_dm, const double *d_kc, const int *d_base, int nsnip,
-                                int nchans, int nsamp, float *d_y, void *stream)
+                                int nchans, int nsamp, double *d_y, void *stream)
 {
     return frac_status(
         launch_frac_fwd(d_x, d_dm, d_kc, d_base, nsnip, nchans, nsamp, d_y, static_cast<cudaStream_t>(stream)),
@@ -48,7 +48,7 @@ int aa_b200_frac_dedisperse_fwd(const float *d_x, const float *d_dm, const doubl
 }
 
 int aa_b200_frac_dedisperse_adj(const float *d_x, const float *d_dm, const double *d_kc, const int *d_base,
-                                const float *d_gy, int nsnip, int nchans, int nsamp, float *d_gx, float *d_gdm,
+                                const double *d_gy, int nsnip, int nchans, int nsamp, float *d_gx, float *d_gdm,
                                 double *d_partial, void *stream)
 {
     return frac_status(launch_frac_adj(d_x, d_dm, d_kc, d_base, d_gy, nsnip, nchans, nsamp, d_gx, d_gdm, d_partial,
@@ -56,8 +56,8 @@ int aa_b200_frac_dedisperse_adj(const float *d_x, const float *d_dm, const doubl
                        "fractional dedispersion adjoint");
 }
 
-int aa_b200_boxcar_snr_fwd(const float *d_y, int nsnip, int nsamp, const int *widths, int nwidths, const float *d_mu,
-                           const float *d_sigma, float *d_snr, void *stream)
+int aa_b200_boxcar_snr_fwd(const double *d_y, int nsnip, int nsamp, const int *widths, int nwidths, const float *d_mu,
+                           const float *d_sigma, double *d_snr, void *stream)
 {
     BoxcarWidths W;
     if (!make_widths(widths, nwidths, W))
@@ -66,8 +66,8 @@ int aa_b200_boxcar_snr_fwd(const float *d_y, int nsnip, int nsamp, const int *wi
                        "boxcar S/N");
 }
 
-int aa_b200_boxcar_snr_adj(const float *d_gsnr, int nsnip, int nsamp, const int *widths, int nwidths,
-                           const float *d_sigma, float *d_gy, void *stream)
+int aa_b200_boxcar_snr_adj(const double *d_gsnr, int nsnip, int nsamp, const int *widths, int nwidths,
+                           const float *d_sigma, double *d_gy, void *stream)
 {
     BoxcarWidths W;
     if (!make_widths(widths, nwidths, W))

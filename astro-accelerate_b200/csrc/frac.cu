@@ -4,8 +4,8 @@
 //
 // Snippets x[b][c][t] (float32, B x C x T) are dedispersed at a continuous
 // trial DM per snippet:
-//     tau_c = dm_b * kc_c                      (samples; kc_c >= 0 per unit DM)
-//     n_c = floor(tau_c) - base_c, w_c = frac(tau_c)   (evaluated in FP64)
+//     tau_c = dm_b * kc_c                      (samples; kc_c per unit DM)
+//     n_c = floor(tau_c) - base_c, w_c = frac(tau_c)
 //     y[b][t] = sum_c x[c][t+n_c] + w_c * (x[c][t+n_c+1] - x[c][t+n_c])
 // with samples outside [0, T) read as 0.  Since t is an integer, n_c and w_c
 // do not depend on t: the adjoint is a shifted, interpolated copy of the
@@ -15,6 +15,13 @@
 // snippet cut with channel c starting base_c samples late is dedispersed at
 // the same DM as the uncut data.  Every kernel recomputes n_c and w_c from
 // dm, kc and base instead of storing them.
+//
+// Precision: the snippets (the only large tensors) stay float32; delays,
+// weights, the channel sums and the per-snippet series y, S/N and their
+// gradients are FP64.  The kernels are bound by HBM traffic of x, so the
+// FP64 arithmetic costs nothing, and a smooth maximum of the S/N at a low
+// temperature (which amplifies rounding of the S/N) keeps its gradient to
+// FP64 accuracy.
 //
 // Boxcar S/N of y for widths w (ascending, <= 1024):
 //     snr[b][i][t] = (sum_{k<w_i} y'[t+k] - w_i mu_b) / (sigma_b sqrt(w_i))
@@ -32,12 +39,12 @@ namespace {
 
 constexpr int FT = 256; // threads per block (samples per block in the time-parallel kernels)
 
-__device__ __forceinline__ void delay_of(float dm, double kc, int base, int &n, float &w)
+__device__ __forceinline__ void delay_of(float dm, double kc, int base, int &n, double &w)
 {
     const double tau = static_cast<double>(dm) * kc;
     const double f = floor(tau);
     n = static_cast<int>(f) - base;
-    w = static_cast<float>(tau - f);
+    w = tau - f;
 }
 
 __device__ __forceinline__ int base_of(const int *base, int b, int C, int c)
@@ -47,14 +54,15 @@ __device__ __forceinline__ int base_of(const int *base, int b, int C, int c)
 
 __device__ __forceinline__ float at(const float *row, int i, int T) { return (i >= 0 && i < T) ? __ldg(row + i) : 0.f; }
 
-// y[b][t]: one thread per output sample, channels in order, FP64 sum.
+__device__ __forceinline__ double atd(const double *row, int i, int T) { return (i >= 0 && i < T) ? row[i] : 0.0; }
+
+// y[b][t]: one thread per output sample, channels in order.
 __global__ void __launch_bounds__(FT) k_frac_fwd(const float *__restrict__ x, const float *__restrict__ dm,
                                                  const double *__restrict__ kc, const int *__restrict__ base, int C,
-                                                 int T, float *__restrict__ y)
+                                                 int T, double *__restrict__ y)
 {
-    extern __shared__ int s_nw[]; // n[C] then w[C]
-    int *s_n = s_nw;
-    float *s_w = reinterpret_cast<float *>(s_nw + C);
+    extern __shared__ double s_w[]; // w[C] then n[C]
+    int *s_n = reinterpret_cast<int *>(s_w + C);
     const int b = blockIdx.y;
     const float d = dm[b];
     for (int c = threadIdx.x; c < C; c += blockDim.x)
@@ -64,20 +72,20 @@ __global__ void __launch_bounds__(FT) k_frac_fwd(const float *__restrict__ x, co
     if (t >= T)
         return;
     const float *xb = x + static_cast<size_t>(b) * C * T;
-    double acc = 0.0; // the kernel is bound by HBM: FP64 sums cost nothing and round once
+    double acc = 0.0;
 #pragma unroll 8
     for (int c = 0; c < C; ++c) {
         const float *row = xb + static_cast<size_t>(c) * T;
         const int i = t + s_n[c];
-        const float a0 = at(row, i, T);
-        const float a1 = at(row, i + 1, T);
-        acc += static_cast<double>(fmaf(s_w[c], a1 - a0, a0));
+        const double a0 = at(row, i, T);
+        const double a1 = at(row, i + 1, T);
+        acc += fma(s_w[c], a1 - a0, a0);
     }
-    y[static_cast<size_t>(b) * T + t] = static_cast<float>(acc);
+    y[static_cast<size_t>(b) * T + t] = acc;
 }
 
 // gx[b][c][j] = (1 - w_c) gy[j - n_c] + w_c gy[j - n_c - 1]
-__global__ void __launch_bounds__(FT) k_frac_adj_x(const float *__restrict__ gy, const float *__restrict__ dm,
+__global__ void __launch_bounds__(FT) k_frac_adj_x(const double *__restrict__ gy, const float *__restrict__ dm,
                                                    const double *__restrict__ kc, const int *__restrict__ base, int C,
                                                    int T, float *__restrict__ gx)
 {
@@ -86,15 +94,15 @@ __global__ void __launch_bounds__(FT) k_frac_adj_x(const float *__restrict__ gy,
     if (j >= T)
         return;
     int n;
-    float w;
+    double w;
     delay_of(dm[b], kc[c], base_of(base, b, C, c), n, w);
-    const float *g = gy + static_cast<size_t>(b) * T;
-    const float v = (1.f - w) * at(g, j - n, T) + w * at(g, j - n - 1, T);
-    gx[(static_cast<size_t>(b) * C + c) * T + j] = v;
+    const double *g = gy + static_cast<size_t>(b) * T;
+    const double v = (1.0 - w) * atd(g, j - n, T) + w * atd(g, j - n - 1, T);
+    gx[(static_cast<size_t>(b) * C + c) * T + j] = static_cast<float>(v);
 }
 
-// partial[b][c] = kc_c * sum_t gy[t] (x[c][t+n+1] - x[c][t+n]), in FP64
-__global__ void __launch_bounds__(FT) k_frac_adj_dm_partial(const float *__restrict__ x, const float *__restrict__ gy,
+// partial[b][c] = kc_c * sum_t gy[t] (x[c][t+n+1] - x[c][t+n])
+__global__ void __launch_bounds__(FT) k_frac_adj_dm_partial(const float *__restrict__ x, const double *__restrict__ gy,
                                                             const float *__restrict__ dm, const double *__restrict__ kc,
                                                             const int *__restrict__ base, int C, int T,
                                                             double *__restrict__ partial)
@@ -102,14 +110,14 @@ __global__ void __launch_bounds__(FT) k_frac_adj_dm_partial(const float *__restr
     __shared__ double red[FT / 32];
     const int b = blockIdx.y, c = blockIdx.x;
     int n;
-    float w;
+    double w;
     delay_of(dm[b], kc[c], base_of(base, b, C, c), n, w);
     const float *row = x + (static_cast<size_t>(b) * C + c) * T;
-    const float *g = gy + static_cast<size_t>(b) * T;
+    const double *g = gy + static_cast<size_t>(b) * T;
     double acc = 0.0;
     for (int t = threadIdx.x; t < T; t += blockDim.x) {
         const int i = t + n;
-        acc += static_cast<double>(__ldg(g + t)) * static_cast<double>(at(row, i + 1, T) - at(row, i, T));
+        acc += g[t] * (static_cast<double>(at(row, i + 1, T)) - static_cast<double>(at(row, i, T)));
     }
     for (int o = 16; o > 0; o >>= 1)
         acc += __shfl_down_sync(0xffffffffu, acc, o);
@@ -145,16 +153,16 @@ __global__ void __launch_bounds__(FT) k_frac_adj_dm_sum(const double *__restrict
 }
 
 // snr[b][i][t]; the block stages y[t0, t0 + FT + wmax - 1) (mu beyond T).
-__global__ void __launch_bounds__(FT) k_boxcar_fwd(const float *__restrict__ y, int T, BoxcarWidths W,
+__global__ void __launch_bounds__(FT) k_boxcar_fwd(const double *__restrict__ y, int T, BoxcarWidths W,
                                                    const float *__restrict__ mu, const float *__restrict__ sigma,
-                                                   float *__restrict__ snr)
+                                                   double *__restrict__ snr)
 {
-    extern __shared__ float ys[];
+    extern __shared__ double ys[];
     const int b = blockIdx.y;
     const int t0 = blockIdx.x * FT;
     const int wmax = W.w[W.n - 1];
-    const float m = mu[b], sg = sigma[b];
-    const float *yb = y + static_cast<size_t>(b) * T;
+    const double m = mu[b], sg = sigma[b];
+    const double *yb = y + static_cast<size_t>(b) * T;
     for (int k = threadIdx.x; k < FT + wmax - 1; k += blockDim.x) {
         const int t = t0 + k;
         ys[k] = (t < T) ? yb[t] : m;
@@ -163,44 +171,44 @@ __global__ void __launch_bounds__(FT) k_boxcar_fwd(const float *__restrict__ y, 
     const int t = t0 + threadIdx.x;
     if (t >= T)
         return;
-    float s = 0.f;
+    double s = 0.0;
     int k = 0;
     for (int i = 0; i < W.n; ++i) {
         for (; k < W.w[i]; ++k)
             s += ys[threadIdx.x + k];
-        const float wf = static_cast<float>(W.w[i]);
-        snr[(static_cast<size_t>(b) * W.n + i) * T + t] = (s - wf * m) / (sg * sqrtf(wf));
+        const double wf = static_cast<double>(W.w[i]);
+        snr[(static_cast<size_t>(b) * W.n + i) * T + t] = (s - wf * m) / (sg * sqrt(wf));
     }
 }
 
 // gy[b][t] = sum_i 1/(sigma sqrt(w_i)) sum_{k<w_i, t-k>=0} gsnr[b][i][t-k]
-__global__ void __launch_bounds__(FT) k_boxcar_adj(const float *__restrict__ gsnr, int T, BoxcarWidths W,
-                                                   const float *__restrict__ sigma, float *__restrict__ gy)
+__global__ void __launch_bounds__(FT) k_boxcar_adj(const double *__restrict__ gsnr, int T, BoxcarWidths W,
+                                                   const float *__restrict__ sigma, double *__restrict__ gy)
 {
-    extern __shared__ float gs[]; // [n][FT + wmax - 1], covering t0 - wmax + 1 .. t0 + FT - 1
+    extern __shared__ double gs[]; // [n][FT + wmax - 1], covering t0 - wmax + 1 .. t0 + FT - 1
     const int b = blockIdx.y;
     const int t0 = blockIdx.x * FT;
     const int wmax = W.w[W.n - 1];
     const int span = FT + wmax - 1;
     for (int i = 0; i < W.n; ++i) {
-        const float *g = gsnr + (static_cast<size_t>(b) * W.n + i) * T;
+        const double *g = gsnr + (static_cast<size_t>(b) * W.n + i) * T;
         for (int k = threadIdx.x; k < span; k += blockDim.x) {
             const int t = t0 - wmax + 1 + k;
-            gs[i * span + k] = (t >= 0 && t < T) ? g[t] : 0.f;
+            gs[i * span + k] = (t >= 0 && t < T) ? g[t] : 0.0;
         }
     }
     __syncthreads();
     const int t = t0 + threadIdx.x;
     if (t >= T)
         return;
-    const float sg = sigma[b];
-    float acc = 0.f;
+    const double sg = sigma[b];
+    double acc = 0.0;
     for (int i = 0; i < W.n; ++i) {
-        float s = 0.f;
-        const float *row = gs + i * span + (threadIdx.x + wmax - 1);
+        double s = 0.0;
+        const double *row = gs + i * span + (threadIdx.x + wmax - 1);
         for (int k = 0; k < W.w[i]; ++k)
             s += row[-k];
-        acc += s / (sg * sqrtf(static_cast<float>(W.w[i])));
+        acc += s / (sg * sqrt(static_cast<double>(W.w[i])));
     }
     gy[static_cast<size_t>(b) * T + t] = acc;
 }
@@ -208,11 +216,11 @@ __global__ void __launch_bounds__(FT) k_boxcar_adj(const float *__restrict__ gsn
 } // namespace
 
 cudaError_t launch_frac_fwd(const float *x, const float *dm, const double *kc, const int *base, int B, int C, int T,
-                            float *y, cudaStream_t st)
+                            double *y, cudaStream_t st)
 {
     if (B <= 0 || C <= 0 || T <= 0 || B > 65535 || C > 16384)
         return cudaErrorInvalidValue;
-    const size_t smem = static_cast<size_t>(C) * 8;
+    const size_t smem = static_cast<size_t>(C) * 12;
     if (smem > 48 * 1024) {
         const cudaError_t e =
             cudaFuncSetAttribute(k_frac_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -224,7 +232,7 @@ cudaError_t launch_frac_fwd(const float *x, const float *dm, const double *kc, c
     return cudaGetLastError();
 }
 
-cudaError_t launch_frac_adj(const float *x, const float *dm, const double *kc, const int *base, const float *gy, int B,
+cudaError_t launch_frac_adj(const float *x, const float *dm, const double *kc, const int *base, const double *gy, int B,
                             int C, int T, float *gx, float *gdm, double *partial, cudaStream_t st)
 {
     if (B <= 0 || C <= 0 || T <= 0 || B > 65535 || C > 65535)
@@ -252,22 +260,22 @@ static bool widths_ok(const BoxcarWidths &W)
     return true;
 }
 
-cudaError_t launch_boxcar_fwd(const float *y, int B, int T, const BoxcarWidths &W, const float *mu, const float *sigma,
-                              float *snr, cudaStream_t st)
+cudaError_t launch_boxcar_fwd(const double *y, int B, int T, const BoxcarWidths &W, const float *mu,
+                              const float *sigma, double *snr, cudaStream_t st)
 {
     if (B <= 0 || T <= 0 || B > 65535 || !widths_ok(W))
         return cudaErrorInvalidValue;
-    const size_t smem = static_cast<size_t>(FT + W.w[W.n - 1] - 1) * sizeof(float);
+    const size_t smem = static_cast<size_t>(FT + W.w[W.n - 1] - 1) * sizeof(double);
     k_boxcar_fwd<<<dim3((T + FT - 1) / FT, B), FT, smem, st>>>(y, T, W, mu, sigma, snr);
     return cudaGetLastError();
 }
 
-cudaError_t launch_boxcar_adj(const float *gsnr, int B, int T, const BoxcarWidths &W, const float *sigma, float *gy,
+cudaError_t launch_boxcar_adj(const double *gsnr, int B, int T, const BoxcarWidths &W, const float *sigma, double *gy,
                               cudaStream_t st)
 {
     if (B <= 0 || T <= 0 || B > 65535 || !widths_ok(W))
         return cudaErrorInvalidValue;
-    const size_t smem = static_cast<size_t>(W.n) * (FT + W.w[W.n - 1] - 1) * sizeof(float);
+    const size_t smem = static_cast<size_t>(W.n) * (FT + W.w[W.n - 1] - 1) * sizeof(double);
     if (smem > 48 * 1024)
         return cudaErrorInvalidValue;
     k_boxcar_adj<<<dim3((T + FT - 1) / FT, B), FT, smem, st>>>(gsnr, T, W, sigma, gy);

@@ -311,30 +311,32 @@ void aa_b200_batch_delete(void *batch);
  * (message in aa_b200_frac_last_error).
  *
  * Fractional-delay dedispersion of nsnip snippets x[nsnip][nchans][nsamp]
- * (float32) at a continuous DM per snippet dm[nsnip]: with
+ * (float32) at a continuous DM per snippet dm[nsnip] (float32) into FP64
+ * series y[nsnip][nsamp]: with
  * tau_c = dm * kc[c] (kc: FP64 delay in samples per unit DM),
  * n = floor(tau_c) - base[s][c], w = tau_c - floor(tau_c) (FP64; d_base, an
  * int array [nsnip][nchans] of row shifts for snippets cut per channel, may
  * be null),
  *   y[s][t] = sum_c x[s][c][t+n] + w (x[s][c][t+n+1] - x[s][c][t+n]),
  * samples outside [0, nsamp) read as 0.  The adjoint recomputes the delays and
- * writes gx = dL/dx (skipped when d_gx is null) and gdm = dL/ddm (skipped
+ * writes, from gy = dL/dy (FP64), gx = dL/dx (float32, skipped when d_gx is
+ * null) and gdm = dL/ddm (float32, skipped
  * when d_gdm is null; needs d_partial, nsnip*nchans doubles of scratch the
  * caller provides).
  * --------------------------------------------------------------------------- */
 int aa_b200_frac_dedisperse_fwd(const float *d_x, const float *d_dm, const double *d_kc, const int *d_base, int nsnip,
-                                int nchans, int nsamp, float *d_y, void *stream);
+                                int nchans, int nsamp, double *d_y, void *stream);
 int aa_b200_frac_dedisperse_adj(const float *d_x, const float *d_dm, const double *d_kc, const int *d_base,
-                                const float *d_gy, int nsnip, int nchans, int nsamp, float *d_gx, float *d_gdm,
+                                const double *d_gy, int nsnip, int nchans, int nsamp, float *d_gx, float *d_gdm,
                                 double *d_partial, void *stream);
-/* Boxcar S/N: snr[s][i][t] = (sum_{k<w_i} y'[s][t+k] - w_i mu[s]) /
+/* Boxcar S/N (FP64 in and out): snr[s][i][t] = (sum_{k<w_i} y'[s][t+k] - w_i mu[s]) /
  * (sigma[s] sqrt(w_i)), y' = y inside [0, nsamp) and mu beyond; widths (host
  * array) ascending in 1..1024, at most 16.  mu and sigma are constants of the
  * adjoint, which writes gy = dL/dy from gsnr. */
-int aa_b200_boxcar_snr_fwd(const float *d_y, int nsnip, int nsamp, const int *widths, int nwidths, const float *d_mu,
-                           const float *d_sigma, float *d_snr, void *stream);
-int aa_b200_boxcar_snr_adj(const float *d_gsnr, int nsnip, int nsamp, const int *widths, int nwidths,
-                           const float *d_sigma, float *d_gy, void *stream);
+int aa_b200_boxcar_snr_fwd(const double *d_y, int nsnip, int nsamp, const int *widths, int nwidths, const float *d_mu,
+                           const float *d_sigma, double *d_snr, void *stream);
+int aa_b200_boxcar_snr_adj(const double *d_gsnr, int nsnip, int nsamp, const int *widths, int nwidths,
+                           const float *d_sigma, double *d_gy, void *stream);
 const char *aa_b200_frac_last_error(void);
 
 /* Single-pulse search on a DM-time range (rows of nsamp floats, row pitch in

@@ -4,7 +4,8 @@ differences (h = 1e-3 in DM).
 
 Tolerances: forward outputs within 1e-5 of the FP64 result relative to the
 largest magnitude; gradients (to the input and to DM) within 1e-5 relative
-to the FP64 analytic gradient and to the central difference.  The central
+to the FP64 analytic gradient and to the central difference (the series and
+S/N are FP64 on the device; only the snippets are float32).  The central
 difference is taken at trial DMs where no channel's delay crosses a whole
 sample inside dm +- h, where the interpolated function is smooth in DM.
 """
@@ -46,7 +47,8 @@ def test_adjoint_matches_fp64(cuda_device):
     x = x.clone().requires_grad_(True)
     d = dm.clone().requires_grad_(True)
     y = R.FracDedisperse.apply(x, d, kc)
-    g = torch.randn(y.shape, generator=torch.Generator(device="cuda").manual_seed(3), device="cuda")
+    g = torch.randn(y.shape, generator=torch.Generator(device="cuda").manual_seed(3), device="cuda",
+                    dtype=torch.float64)
     y.backward(g)
     xh, kch, gh = x.detach().cpu().numpy(), kc.cpu().numpy(), g.cpu().numpy()
     for s in range(x.shape[0]):
@@ -63,7 +65,7 @@ def test_row_shifts_match_fp64(cuda_device):
     xg = x.clone().requires_grad_(True)
     d = dm.clone().requires_grad_(True)
     y = R.FracDedisperse.apply(xg, d, kc, base)
-    g = torch.randn(y.shape, generator=gen, device="cuda")
+    g = torch.randn(y.shape, generator=gen, device="cuda", dtype=torch.float64)
     y.backward(g)
     xh, kch, gh, bh = x.cpu().numpy(), kc.cpu().numpy(), g.cpu().numpy(), base.cpu().numpy()
     for s in range(x.shape[0]):
@@ -77,11 +79,11 @@ def test_boxcar_matches_fp64(cuda_device):
     import torch
     from aa_b200 import refine as R
     gen = torch.Generator(device="cuda").manual_seed(5)
-    y = torch.randn((2, 3000), generator=gen, device="cuda").requires_grad_(True)
+    y = torch.randn((2, 3000), generator=gen, device="cuda", dtype=torch.float64).requires_grad_(True)
     mu = torch.tensor([0.1, -0.2], device="cuda")
     sigma = torch.tensor([1.5, 2.0], device="cuda")
     snr = R.BoxcarSNR.apply(y, WIDTHS, mu, sigma)
-    g = torch.randn(snr.shape, generator=gen, device="cuda")
+    g = torch.randn(snr.shape, generator=gen, device="cuda", dtype=torch.float64)
     snr.backward(g)
     for s in range(2):
         want = F.boxcar_forward(y[s].detach().cpu().numpy(), WIDTHS, float(mu[s]), float(sigma[s]))
@@ -133,5 +135,6 @@ def test_refinement_rejects_bad_inputs(cuda_device):
     with pytest.raises(TypeError):
         R.FracDedisperse.apply(x.double(), torch.zeros(2, device="cuda"), kc)
     with pytest.raises(RuntimeError, match="widths"):
-        R.BoxcarSNR.apply(torch.zeros((2, 64), device="cuda"), tuple(range(1, 20)), torch.zeros(2, device="cuda"),
+        R.BoxcarSNR.apply(torch.zeros((2, 64), device="cuda", dtype=torch.float64), tuple(range(1, 20)),
+                          torch.zeros(2, device="cuda"),
                           torch.ones(2, device="cuda"))
