@@ -251,12 +251,16 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
                 const int prow = o_P + ((s & 1) * Q.npool + rbase) * W + lane;
                 const int ej[QDMW] = {e4.x, e4.y, e4.z, e4.w};
                 if ((e4.x | e4.y | e4.z | e4.w) >= 0) {
+                    // neighbouring DM trials often share the quad's offset:
+                    // their words are already in registers (warp-uniform test)
+                    uint32_t w[M];
 #pragma unroll
                     for (int j = 0; j < QDMW; ++j) {
-                        uint32_t w[M];
+                        if (j == 0 || ej[j] != ej[j - 1]) {
 #pragma unroll
-                        for (int m = 0; m < M; ++m)
-                            w[m] = sm[prow + ej[j] + 32 * m];
+                            for (int m = 0; m < M; ++m)
+                                w[m] = sm[prow + ej[j] + 32 * m];
+                        }
 #pragma unroll
                         for (int m = 0; m < M; ++m)
                             acc[j][m] = __dp4a(w[m], 0x01010101u, acc[j][m]);
@@ -441,18 +445,22 @@ __device__ bool f32_body(const DdtrLaunch &p, const F32Launch &F, int g, long lo
                 const int4 e4 = *reinterpret_cast<const int4 *>(&sm[o_ent + (slot * CS + ci) * GD + warp * QDMW]);
                 const int ej[QDMW] = {e4.x, e4.y, e4.z, e4.w};
                 const float *frow = fsm + o_F + ((s & 1) * CS + ci) * W + lane;
+                // a DM trial whose table entry (delay and class mask) equals the
+                // previous trial's adds the samples already in registers
+                float v[M];
 #pragma unroll
                 for (int j = 0; j < QDMW; ++j) {
                     const int e = ej[j];
-                    int o = (e & 0xFFFFFF) - w + static_cast<int>((static_cast<unsigned>(e) >> (24 + cls)) & 1u);
-                    if (o < 0 || o > omax) {
-                        atomicOr(p.err, DERR_WINDOW);
-                        o = 0;
-                    }
-                    float v[M];
+                    if (j == 0 || e != ej[j - 1]) {
+                        int o = (e & 0xFFFFFF) - w + static_cast<int>((static_cast<unsigned>(e) >> (24 + cls)) & 1u);
+                        if (o < 0 || o > omax) {
+                            atomicOr(p.err, DERR_WINDOW);
+                            o = 0;
+                        }
 #pragma unroll
-                    for (int m = 0; m < M; ++m)
-                        v[m] = frow[o + 32 * m];
+                        for (int m = 0; m < M; ++m)
+                            v[m] = frow[o + 32 * m];
+                    }
 #pragma unroll
                     for (int m = 0; m < M; ++m)
                         acc[j][m] = __fadd_rn(acc[j][m], v[m]);
