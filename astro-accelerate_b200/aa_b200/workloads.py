@@ -112,3 +112,22 @@ def synth_e2e_beam(beam: dict, device):
             v = (x[tt, c].to(torch.int32) & 0xFFFF).to(torch.float32) + p["amp_sigma"] * sig
             x[tt, c] = v.clamp_(0, 255).to(torch.int32).to(torch.int16)
     return x
+
+
+def partition(costs: list, nranks: int) -> list:
+    """Beams to ranks, heaviest first onto the least loaded rank (longest
+    processing time first); returns one list of beam indices per rank, each in
+    ascending order.  Beams are independent, so no data moves between ranks."""
+    loads = [0.0] * nranks
+    parts = [[] for _ in range(nranks)]
+    for i in sorted(range(len(costs)), key=lambda k: (-costs[k], k)):
+        r = min(range(nranks), key=lambda k: (loads[k], k))
+        parts[r].append(i)
+        loads[r] += costs[i]
+    return [sorted(p) for p in parts]
+
+
+def beam_cost(beam: dict, strategy: dict) -> float:
+    """Channel-adds of one beam's dedispersion (fp32 work counted 3x)."""
+    units = sum(strategy["ndms"][r] * sum(strategy["t_processed"][r]) for r in range(len(strategy["ndms"])))
+    return float(units) * beam["nchans"] * (3.0 if beam["nbits"] > 8 else 1.0)

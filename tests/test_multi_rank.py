@@ -1,0 +1,69 @@
+"""Multi-rank host logic on CPU (gloo, world size 2): the beam partition
+every rank computes independently must agree across ranks, cover every beam
+once and balance the work; step times are reduced as the maximum over ranks
+(the bench's rule).  No GPU and no collective on the data path."""
+from __future__ import annotations
+
+import os
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _worker(rank, world, port, q):
+    sys.path.insert(0, os.path.join(ROOT, "astro-accelerate_b200"))
+    import torch
+    import torch.distributed as dist
+    import aa_b200 as aa
+    from aa_b200 import workloads as WL
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        beams = WL.multibeam_draw(seed=3, nbeams=12)
+        costs = []
+        for b in beams:
+            s = aa.strategy(b["plan"], b["nchans"], b["nsamp"], b["fch1"], b["foff"], b["tsamp"], b["nbits"],
+                            64 << 30)
+            costs.append(WL.beam_cost(b, s))
+        mine = WL.partition(costs, world)[rank]
+        got = [None] * world
+        dist.all_gather_object(got, mine)
+        t = torch.tensor([float(rank + 1)])
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        q.put((rank, got, costs, float(t)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_partition_agrees_across_ranks_and_covers_every_beam():
+    world = 2
+    port = 29500 + (os.getpid() % 2000)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    res.sort()
+    parts = res[0][1]
+    assert all(r[1] == parts for r in res)  # every rank computed the same partition
+    flat = sorted(i for p in parts for i in p)
+    assert flat == list(range(12))
+    costs = res[0][2]
+    loads = [sum(costs[i] for i in p) for p in parts]
+    assert max(loads) <= sum(loads) / world + max(costs)  # LPT bound
+    assert all(r[3] == float(world) for r in res)  # max over ranks
+
+
+def test_partition_single_rank():
+    sys.path.insert(0, os.path.join(ROOT, "astro-accelerate_b200"))
+    from aa_b200 import workloads as WL
+    assert WL.partition([3.0, 1.0, 2.0], 1) == [[0, 1, 2]]
+    assert WL.partition([5.0, 4.0, 3.0, 3.0], 2) == [[0, 3], [1, 2]]
