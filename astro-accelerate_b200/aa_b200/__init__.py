@@ -142,6 +142,7 @@ def lib():
         "aa_b200_pipeline_device_output": ([vp, i], vp),
         "aa_b200_pipeline_range_info": ([vp, i, P(i), P(i), P(i), P(i)], i),
         "aa_b200_pipeline_kernel_launches": ([vp], ll),
+        "aa_b200_pipeline_stage_depth": ([vp, i], i),
         "aa_b200_pipeline_last_error": ([vp], ctypes.c_char_p),
         "aa_b200_pipeline_num_tchunks": ([vp], i),
         "aa_b200_pipeline_maxshift": ([vp], i),
@@ -381,6 +382,7 @@ class aa_py_pipeline:
             raise RuntimeError(self.last_error())
         return {"kind": KIND_NAMES[k.value & 0xFF], "kernel": ("quad" if k.value & 0x100 else "f32" if k.value & 0x200 else
                            "gather" if k.value & 0x400 else "phase"),
+                "stage_depth": lib().aa_b200_pipeline_stage_depth(self.m_obj, r),
                 "group_dms": g.value, "span": s.value, "tile_words": t.value}
 
     def time_kernels(self, on: bool = True):

@@ -1,0 +1,29 @@
+// autotune.hpp -- stage depth of the staged dedispersion kernels, by
+// measurement.
+//
+// The channel-quad kernel stages qs channel quads per shared-memory stage and
+// the fp32 kernel cs channels; deeper stages mean fewer CTA barriers per
+// channel but more shared memory (and, for the quad kernel, more pattern rows
+// built per stage).  tune_stage_depth times every depth that fits (also
+// inside the persistent kernel, which keeps 256 bytes for its job descriptor)
+// on a slice of the job -- about two CTAs per SM -- with CUDA events, keeps
+// the fastest, and caches it by the job's shape.  The slice writes into the
+// job's own output rows, which the real run overwrites.
+#pragma once
+#include <map>
+#include <string>
+#include <tuple>
+
+#include <cuda_runtime.h>
+
+#include "pipeline.hpp"
+
+namespace aab200 {
+
+struct StageTuneCache {
+    std::map<std::tuple<int, int, int, int, int, int, long long>, int> best;
+};
+
+bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache &cache, std::string &err);
+
+} // namespace aab200

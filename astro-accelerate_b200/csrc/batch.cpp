@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cstdio>
 
+#include "autotune.hpp"
 #include "ddtr_kernels.cuh"
 
 namespace aab200 {
@@ -119,88 +120,11 @@ bool BatchDdtr::build_levels(Beam &b)
     return true;
 }
 
-// Stage depth of a staged job, by timing the candidates on a slice of the job
-// (about two CTAs per SM) with CUDA events.  The slice writes into the job's
-// own output rows, which the real run overwrites.
 bool BatchDdtr::tune_job(DdtrJob &job)
 {
-    const bool quad = (job.variant == 2);
-    const auto key = std::make_tuple(job.variant, job.p.nch_used, quad ? job.q.W : job.f.W,
-                                     quad ? job.q.raww : job.f.rawh, quad ? job.q.npool / std::max(1, job.q.qs) : 0,
-                                     job.p.kind, static_cast<long long>(job.p.stride % 16));
-    int best = -1;
-    auto it = tune_cache_.find(key);
-    if (it != tune_cache_.end()) {
-        best = it->second;
-    } else {
-        int nsm = 148;
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
-        const long long want_tiles = std::max<long long>(1, (2LL * nsm + job.groups - 1) / job.groups);
-        DdtrJob slice = job;
-        slice.p.tp = static_cast<int>(std::min<long long>(job.p.tp, want_tiles * job.tile_samples));
-        const int cands[] = {1, 2, 4, 8, 16, 32};
-        cudaEvent_t e0, e1;
-        if (!check_cuda(cudaEventCreate(&e0), "event") || !check_cuda(cudaEventCreate(&e1), "event"))
-            return false;
-        float best_ms = 1e30f;
-        const int maxcnt = quad ? std::max(1, job.q.npool / std::max(1, job.q.qs)) : 0;
-        for (int c : cands) {
-            DdtrJob t = slice;
-            size_t bytes;
-            if (quad) {
-                if (c > 8)
-                    continue;
-                t.q.qs = c;
-                t.q.npool = c * maxcnt;
-                BatchJobDev d{};
-                d.p = t.p;
-                d.q = t.q;
-                d.variant = 2;
-                bytes = persistent_job_smem(d);
-            } else {
-                if (c < 4)
-                    continue;
-                t.f.cs = c;
-                BatchJobDev d{};
-                d.p = t.p;
-                d.f = t.f;
-                d.variant = 3;
-                bytes = persistent_job_smem(d);
-            }
-            if (bytes > 227 * 1024)
-                continue;
-            float ms_min = 1e30f;
-            bool ok = check_cuda(launch_job(t, st_), "autotune launch");
-            for (int rep = 0; ok && rep < 2; ++rep) {
-                float ms = 0.f;
-                ok = check_cuda(cudaEventRecord(e0, st_), "event") && check_cuda(launch_job(t, st_), "autotune launch") &&
-                     check_cuda(cudaEventRecord(e1, st_), "event") && check_cuda(cudaEventSynchronize(e1), "sync") &&
-                     check_cuda(cudaEventElapsedTime(&ms, e0, e1), "event time");
-                ms_min = std::min(ms_min, ms);
-            }
-            if (!ok) {
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                return false;
-            }
-            if (ms_min < best_ms) {
-                best_ms = ms_min;
-                best = c;
-            }
-        }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        if (best < 0)
-            return fail("no stage depth of the staged kernel fits the persistent kernel's shared memory");
-        tune_cache_[key] = best;
-    }
-    if (quad) {
-        const int maxcnt = std::max(1, job.q.npool / std::max(1, job.q.qs));
-        job.q.qs = best;
-        job.q.npool = best * maxcnt;
-    } else {
-        job.f.cs = best;
-    }
+    std::string err;
+    if (!tune_stage_depth(job, st_, device_, tune_cache_, err))
+        return fail(err);
     return true;
 }
 

@@ -31,6 +31,7 @@
 
 #include <cuda_runtime.h>
 
+#include "autotune.hpp"
 #include "pipeline.hpp"
 
 namespace aab200 {
@@ -125,8 +126,7 @@ private:
     double run_ms_ = 0.0, ddtr_ms_ = 0.0;
     long long launches_per_run_ = 0;
     bool ran_ = false;
-    // autotuner cache: shape -> stage depth
-    std::map<std::tuple<int, int, int, int, int, int, long long>, int> tune_cache_;
+    StageTuneCache tune_cache_;
 };
 
 } // namespace aab200

@@ -580,6 +580,15 @@ int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms,
     return 0;
 }
 
+int aa_b200_pipeline_stage_depth(void *obj, int range)
+{
+    Api *a = as_api(obj);
+    if (!a->pipe || !a->pipe->setup() || range < 0 || range >= static_cast<int>(a->pipe->strategy().nranges()))
+        return 0;
+    const RangeConfig &rc = a->pipe->range_config(range);
+    return rc.variant == 2 ? rc.quad.qs : (rc.variant == 3 ? rc.f32.cs : 0);
+}
+
 long long aa_b200_pipeline_kernel_launches(void *obj)
 {
     Api *a = as_api(obj);

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 
+#include "autotune.hpp"
 #include "ddtr_kernels.cuh"
 
 namespace aab200 {
@@ -296,6 +297,8 @@ bool DdtrPipeline::setup()
         meta_.nbits != 32)
         return fail("unsupported nbits");
     elem_bytes_ = (meta_.nbits <= 8) ? 1 : 2;
+    if (!check_cuda(cudaGetDevice(&device_), "cudaGetDevice"))
+        return false;
     for (int r = 0; r < nr; ++r) {
         const int b = strategy_.dm(r).inBin;
         if (b < 1 || (b & (b - 1)))
@@ -410,11 +413,49 @@ bool DdtrPipeline::setup()
         cudaEventRecord(ev_tile_free_[i], st_d2h_);
         cudaEventRecord(ev_raw_free_[i], st_);
     }
+    if (opt_.autotune && !opt_.external_buffers && !tune_ranges())
+        return false;
     if (!check_device_flags())
         return false;
     setup_done_ = true;
     rewind();
     return true;
+}
+
+// Stage depth of every range that runs a staged kernel, timed on chunk 0's
+// job (the buffers hold zeros at this point; the kernels' work does not
+// depend on the sample values).
+bool DdtrPipeline::tune_ranges()
+{
+    StageTuneCache cache;
+    for (size_t r = 0; r < ranges_.size(); ++r) {
+        RangeConfig &rc = ranges_[r];
+        if (rc.variant != 2 && rc.variant != 3)
+            continue;
+        const DdtrOp *op = nullptr;
+        for (const DdtrOp &o : ops_)
+            if (o.kind == DdtrOp::DDTR && o.range == static_cast<int>(r)) {
+                op = &o;
+                break;
+            }
+        if (!op)
+            continue;
+        float *out = opt_.device_output ? d_out_full_[r] + op->out_off : d_tile_[0];
+        const long long pitch = opt_.device_output ? strategy_.total_samps(static_cast<int>(r)) : op->tp;
+        DdtrJob job;
+        if (!make_job(*op, d_flat_[op->src_level & 1], flat_elems_, out, pitch, job))
+            return false;
+        std::string err;
+        if (!tune_stage_depth(job, st_, device_, cache, err))
+            return fail(err);
+        if (rc.variant == 2) {
+            rc.quad.qs = job.q.qs;
+            rc.quad.npool = job.q.npool;
+        } else {
+            rc.f32.cs = job.f.cs;
+        }
+    }
+    return check_cuda(cudaStreamSynchronize(st_), "sync");
 }
 
 bool DdtrPipeline::rewind()

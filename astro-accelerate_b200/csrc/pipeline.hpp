@@ -46,6 +46,7 @@ struct PipelineOptions {
     bool device_output = false; // keep the whole output on the device ([range][dm][t])
     bool time_kernels = false;  // CUDA events around every kernel launch
     bool external_buffers = false; // no filterbank/raw/tile buffers: the caller runs the ops (batch engine)
+    bool autotune = true;          // time the staged kernels' stage depth per range at setup
     cudaStream_t stream = nullptr;
 };
 
@@ -167,6 +168,7 @@ private:
     bool check_device_flags();
     bool build_range(int r);
     bool build_quad_tables(int r);
+    bool tune_ranges();
     bool step(bool allow_sync);
     bool enumerate_ops();
     bool exec_corner_turn(const DdtrOp &op);

@@ -252,6 +252,10 @@ float *aa_b200_pipeline_device_output(void *obj, int range);
  * staged fp32 kernel, | 0x400 for the two-byte gather kernel), DMs per thread
  * block, window span (samples), time words per lane */
 int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms, int *span, int *tile_words);
+/* channel quads (channel-quad kernel) or channels (fp32 kernel) per
+ * shared-memory stage of a range, as the autotuner chose it; 0 for the
+ * generic kernels */
+int aa_b200_pipeline_stage_depth(void *obj, int range);
 long long aa_b200_pipeline_kernel_launches(void *obj);
 const char *aa_b200_pipeline_last_error(void *obj);
 int aa_b200_pipeline_num_tchunks(void *obj);
