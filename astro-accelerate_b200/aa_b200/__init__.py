@@ -381,7 +381,7 @@ class aa_py_pipeline:
                                               ctypes.byref(t)):
             raise RuntimeError(self.last_error())
         return {"kind": KIND_NAMES[k.value & 0xFF], "kernel": ("quad" if k.value & 0x100 else "f32" if k.value & 0x200 else
-                           "gather" if k.value & 0x400 else "phase"),
+                           "gather" if k.value & 0x400 else "sub" if k.value & 0x800 else "phase"),
                 "stage_depth": lib().aa_b200_pipeline_stage_depth(self.m_obj, r),
                 "group_dms": g.value, "span": s.value, "tile_words": t.value}
 

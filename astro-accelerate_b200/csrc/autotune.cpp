@@ -99,4 +99,40 @@ bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache 
     return true;
 }
 
+float time_job_slice(const DdtrJob &job, cudaStream_t st, int device, std::string &err)
+{
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    const long long want_tiles = std::max<long long>(1, (2LL * nsm + job.groups - 1) / std::max(1, job.groups));
+    DdtrJob t = job;
+    t.p.tp = static_cast<int>(std::min<long long>(job.p.tp, want_tiles * job.tile_samples));
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        err = "autotune: cudaEventCreate failed";
+        return -1.f;
+    }
+    float best = 1e30f;
+    cudaError_t e = launch_job(t, st);
+    for (int rep = 0; e == cudaSuccess && rep < 2; ++rep) {
+        float ms = 0.f;
+        e = cudaEventRecord(e0, st);
+        if (e == cudaSuccess)
+            e = launch_job(t, st);
+        if (e == cudaSuccess)
+            e = cudaEventRecord(e1, st);
+        if (e == cudaSuccess)
+            e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess)
+            e = cudaEventElapsedTime(&ms, e0, e1);
+        best = std::min(best, ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) {
+        err = std::string("autotune launch: ") + cudaGetErrorString(e);
+        return -1.f;
+    }
+    return best;
+}
+
 } // namespace aab200

@@ -26,4 +26,8 @@ struct StageTuneCache {
 
 bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache &cache, std::string &err);
 
+// Device time (ms, best of two after a warm-up launch) of a slice of the job
+// of about two CTAs per SM; negative on a launch error (message in err).
+float time_job_slice(const DdtrJob &job, cudaStream_t st, int device, std::string &err);
+
 } // namespace aab200

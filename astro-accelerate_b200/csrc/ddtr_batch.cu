@@ -24,6 +24,7 @@ using namespace dev;
 constexpr int JD_WORDS = 64; // shared-memory words kept for the job descriptor
 static_assert(sizeof(BatchJobDev) <= 4 * JD_WORDS, "job descriptor larger than its shared-memory slot");
 static_assert(sizeof(BatchJobDev) % 4 == 0, "job descriptor is copied word by word");
+static_assert((body::BAR_WORDS + JD_WORDS) % 4 == 0, "the body area must start on a 16-byte boundary");
 constexpr int BATCH_M = 16;
 
 __global__ void __launch_bounds__(body::NTHREADS, 1)
@@ -63,7 +64,7 @@ __global__ void __launch_bounds__(body::NTHREADS, 1)
         const long long t0 = (li / jd.groups) * (32 * BATCH_M);
         bool ok;
         if (jd.variant == 2)
-            ok = body::quad_body<BATCH_M>(jd.p, jd.q, g, t0, area, bar0, stage_ctr);
+            ok = body::quad_body<BATCH_M, 4>(jd.p, jd.q, g, t0, area, bar0, stage_ctr);
         else
             ok = body::f32_body<BATCH_M>(jd.p, jd.f, g, t0, area, bar0, stage_ctr);
         fence_proxy_async();

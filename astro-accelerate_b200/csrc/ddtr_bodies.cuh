@@ -14,8 +14,9 @@
 // of the tile is skipped and the body returns false after it has waited, with
 // the same bound, for every copy it issued.
 //
-// 512 threads: warp w owns DM trials g*64 + 4w .. 4w+3, lane l owns outputs
-// t0 + l + 32m (m < M).
+// 64/DW warps (512 threads for DW = 4, 256 for DW = 8): warp w owns DM trials
+// g*64 + DW*w .. DW*w + DW-1, lane l owns outputs t0 + l + 32m (m < M).  The
+// fp32 body uses DW = 4.
 #pragma once
 #include "ddtr_kernels.cuh"
 #include "device_util.cuh"
@@ -25,22 +26,28 @@ namespace body {
 
 using namespace dev;
 
-constexpr int QNSTAGE = 3; // TMA ring depth
+constexpr int QNSTAGE = 3;   // TMA ring depth of the channel-quad and fp32 bodies
+constexpr int SUB_SLOTS = 6; // TMA ring depth of the subband body
 constexpr int QDMW = 4;    // DM trials per warp
 constexpr int NTHREADS = 512;
 
-// Words of the caller-owned barrier area (QNSTAGE mbarriers + scratch).
-constexpr int BAR_WORDS = 2 * QNSTAGE + 2;
+// Words of the caller-owned barrier area (QNSTAGE 8-byte mbarriers), rounded
+// up to 16 bytes: the body area behind it holds TMA destinations and 16-byte
+// vector accesses.
+constexpr int BAR_WORDS = ((2 * (QNSTAGE > SUB_SLOTS ? QNSTAGE : SUB_SLOTS) + 2) + 3) & ~3;
+static_assert(BAR_WORDS % 4 == 0, "the body area must start on a 16-byte boundary");
 
 __device__ __forceinline__ int output_class(int kind, long long t)
 {
     return (kind == KIND_SHARED4) ? static_cast<int>((t & 31) >> 2) : static_cast<int>((t & 15) >> 1);
 }
 
+constexpr int NBARS = BAR_WORDS / 2; // mbarriers in the area
+
 __device__ __forceinline__ void init_barriers(unsigned bar0)
 {
     if (threadIdx.x == 0)
-        for (int i = 0; i < QNSTAGE; ++i)
+        for (int i = 0; i < NBARS; ++i)
             mbar_init(bar0 + 8 * i, 1);
     mbar_init_fence();
 }
@@ -64,13 +71,15 @@ __host__ __device__ inline size_t quad_body_words(int qs, int group_dms, int raw
     return o;
 }
 
-template <int M>
+template <int M, int DW>
 __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long long t0, uint32_t *sm, unsigned bar0,
                           unsigned &stage_ctr)
 {
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int nwarps = NTHREADS >> 5;
+    constexpr int NW = 64 / DW; // warps (64 DM trials per CTA)
+    constexpr int NT = 32 * NW;
+    const int nwarps = NW;
     const int GD = p.group_dms;
     const int dm0 = g * GD;
     const int W = Q.W, RAWW = Q.raww, QS = Q.qs;
@@ -85,7 +94,7 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
     const int o_rsh = o_pat + QNSTAGE * QS * 16;
     const int o_P = ((o_rsh + QNSTAGE * QS * 4) + 3) & ~3;
 
-    for (int i = tid; i < (Q.nq_pad >> 2); i += NTHREADS)
+    for (int i = tid; i < (Q.nq_pad >> 2); i += NT)
         cp_async16(&sm[o_qw + 4 * i], Q.qwin + static_cast<size_t>(g) * Q.nq_pad + 4 * i);
     cp_async_commit();
     cp_async_wait<0>();
@@ -193,16 +202,16 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
         }
     };
 
-    uint32_t acc[QDMW][M];
+    uint32_t acc[DW][M];
 #pragma unroll
-    for (int j = 0; j < QDMW; ++j)
+    for (int j = 0; j < DW; ++j)
 #pragma unroll
         for (int m = 0; m < M; ++m)
             acc[j][m] = 0u;
 
     // per-byte path for one (quad, DM trial): every channel with its own class delays
     auto slow = [&](int j, int slot, int q0, int q) {
-        const int dm = dm0 + warp * QDMW + j;
+        const int dm = dm0 + warp * DW + j;
         const int lo = static_cast<int>(sm[o_qw + q0 + q]);
 #pragma unroll 1
         for (int i = 0; i < 4; ++i) {
@@ -247,15 +256,25 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
         if (ok) {
             int rbase = 0;
             for (int q = 0; q < nq; ++q) {
-                const int4 e4 = *reinterpret_cast<const int4 *>(&sm[o_ent + (slot * QS + q) * GD + warp * QDMW]);
                 const int prow = o_P + ((s & 1) * Q.npool + rbase) * W + lane;
-                const int ej[QDMW] = {e4.x, e4.y, e4.z, e4.w};
-                if ((e4.x | e4.y | e4.z | e4.w) >= 0) {
+                int ej[DW];
+                int any_neg = 0;
+#pragma unroll
+                for (int h = 0; h < DW / 4; ++h) {
+                    const int4 e4 =
+                        *reinterpret_cast<const int4 *>(&sm[o_ent + (slot * QS + q) * GD + warp * DW + 4 * h]);
+                    ej[4 * h] = e4.x;
+                    ej[4 * h + 1] = e4.y;
+                    ej[4 * h + 2] = e4.z;
+                    ej[4 * h + 3] = e4.w;
+                    any_neg |= e4.x | e4.y | e4.z | e4.w;
+                }
+                if (any_neg >= 0) {
                     // neighbouring DM trials often share the quad's offset:
                     // their words are already in registers (warp-uniform test)
                     uint32_t w[M];
 #pragma unroll
-                    for (int j = 0; j < QDMW; ++j) {
+                    for (int j = 0; j < DW; ++j) {
                         if (j == 0 || ej[j] != ej[j - 1]) {
 #pragma unroll
                             for (int m = 0; m < M; ++m)
@@ -267,7 +286,7 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
                     }
                 } else {
 #pragma unroll
-                    for (int j = 0; j < QDMW; ++j) {
+                    for (int j = 0; j < DW; ++j) {
                         if (ej[j] >= 0) {
 #pragma unroll
                             for (int m = 0; m < M; ++m)
@@ -290,8 +309,8 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
 
     // (float)S / nchans / bin, the reference's expression (4-bit: / nchans)
 #pragma unroll
-    for (int j = 0; j < QDMW; ++j) {
-        const int dm = dm0 + warp * QDMW + j;
+    for (int j = 0; j < DW; ++j) {
+        const int dm = dm0 + warp * DW + j;
         if (dm >= p.ndms)
             continue;
         float *orow = p.out + static_cast<long long>(dm) * p.out_pitch;
@@ -486,6 +505,302 @@ __device__ bool f32_body(const DdtrLaunch &p, const F32Launch &F, int g, long lo
             const long long t = t0 + lane + 32 * m;
             if (t < p.tp)
                 orow[t] = p.divide_by_bin ? (acc[j][m] / p.nchans_f / p.bin_f) : (acc[j][m] / p.nchans_f);
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Subband body (one-byte samples): 16-channel partial sums per skew pattern,
+// then two outputs per 32-bit add (ddtr_sub.cu has the tables).
+//
+// One subband per stage, a ring of SUB_SLOTS TMA slots (the copies of stage
+// s+2 are issued SUB_SLOTS-2 iterations before they are needed).  Iteration s builds the
+// quad-sum rows of stage s+2 (for every distinct skew of every quad: the
+// 4-channel sums, IDP4A of the byte-transposed channels, as 16-bit pairs),
+// the partial-sum rows of stage s+1 (per pattern: four quad-sum pairs added
+// in 16-bit lanes, stored in an even- and an odd-phase copy so that every
+// later read is one aligned word; a quad offset of odd parity is realigned
+// with one byte permute), and adds stage s: lane l owns outputs
+// t0 + 2l + 64m + {0, 1} (m < 8) of its 4 DM trials in 16-bit lanes, flushed
+// to 32-bit sums every 16 subbands (16 x 16 x 255 < 2^16).  The builds are
+// spread over all 512 threads; one CTA barrier per iteration.
+//
+// Shared memory (words from sm): win[nsub_pad] | raw[SLOTS][16][RAWW] |
+// ent[SLOTS][64] | blk[SLOTS][128] | rsh[SLOTS][16] | Q[2][nqrow][wq/2] |
+// P[2 buffers][2 phases][npat * W/2].
+// ---------------------------------------------------------------------------
+__host__ __device__ inline size_t sub_body_words(int raww, int nsub_pad, int nqrow, int wq, int npat, int W)
+{
+    size_t o = static_cast<size_t>(nsub_pad);
+    o += static_cast<size_t>(SUB_SLOTS) * 16 * raww;
+    o += static_cast<size_t>(SUB_SLOTS) * 64;
+    o += static_cast<size_t>(SUB_SLOTS) * SUB_BLK_WORDS;
+    o += static_cast<size_t>(SUB_SLOTS) * 16;
+    o = (o + 3) & ~static_cast<size_t>(3);
+    o += 2 * static_cast<size_t>(nqrow) * (wq / 2);
+    o += 4 * static_cast<size_t>(npat) * (W / 2);
+    return o;
+}
+
+__device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S, int g, long long t0, uint32_t *sm,
+                                         unsigned bar0, unsigned &stage_ctr)
+{
+    static_assert(NBARS >= SUB_SLOTS, "the barrier area holds one mbarrier per TMA slot");
+    constexpr int M2 = 8; // output pairs per lane per DM trial
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int dm0 = g * 64;
+    const int RAWW = S.raww, WQ = S.wq, HQ = S.wq >> 1, HALF = S.W >> 1;
+    const unsigned char *in = static_cast<const unsigned char *>(p.in);
+    const int nstages = S.nsub;
+    const unsigned sbase = stage_ctr;
+
+    const int o_win = 0;
+    const int o_raw = o_win + S.nsub_pad;
+    const int o_ent = o_raw + SUB_SLOTS * 16 * RAWW;
+    const int o_blk = o_ent + SUB_SLOTS * 64;
+    const int o_rsh = o_blk + SUB_SLOTS * SUB_BLK_WORDS;
+    const int o_Q = ((o_rsh + SUB_SLOTS * 16) + 3) & ~3;
+    const int o_P = o_Q + 2 * S.nqrow * HQ;
+    const int PBUF = 2 * S.npat * HALF; // words per partial-sum buffer (both phases)
+
+    for (int i = tid; i < (S.nsub_pad >> 2); i += NTHREADS)
+        cp_async16(&sm[o_win + 4 * i], S.swin + static_cast<size_t>(g) * S.nsub_pad + 4 * i);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+
+    auto slot_of = [&](int s) { return static_cast<int>((sbase + static_cast<unsigned>(s)) % SUB_SLOTS); };
+
+    // warp 0: the subband's 16 raw rows, its DM offsets and pattern block
+    auto issue = [&](int s) {
+        if (warp != 0 || s >= nstages)
+            return;
+        const int slot = slot_of(s);
+        const int c0 = 16 * s;
+        const int nrows = max(0, min(16, p.nch_used - c0));
+        const unsigned bar = bar0 + 8 * slot;
+        fence_proxy_async();
+        if (lane == 0)
+            mbar_expect_tx(bar, static_cast<unsigned>(nrows * RAWW * 4 + 64 * 4 + SUB_BLK_WORDS * 4));
+        __syncwarp();
+        if (lane < 16) {
+            if (lane < nrows) {
+                const int w0 = static_cast<int>(sm[o_win + s]);
+                const uintptr_t a =
+                    reinterpret_cast<uintptr_t>(in + static_cast<long long>(c0 + lane) * p.stride + t0 + w0);
+                sm[o_rsh + slot * 16 + lane] = static_cast<uint32_t>(a & 15);
+                tma_load_1d(smem_addr(&sm[o_raw + (slot * 16 + lane) * RAWW]),
+                            reinterpret_cast<const void *>(a & ~static_cast<uintptr_t>(15)),
+                            static_cast<unsigned>(RAWW * 4), bar);
+            } else {
+                sm[o_rsh + slot * 16 + lane] = 0xFFFFFFFFu;
+            }
+        } else if (lane == 16) {
+            tma_load_1d(smem_addr(&sm[o_ent + slot * 64]), S.soff + static_cast<size_t>(s) * p.ndms + dm0, 256u, bar);
+        } else if (lane == 17) {
+            tma_load_1d(smem_addr(&sm[o_blk + slot * SUB_BLK_WORDS]),
+                        S.sblk + (static_cast<size_t>(g) * S.nsub + s) * SUB_BLK_WORDS,
+                        static_cast<unsigned>(SUB_BLK_WORDS * 4), bar);
+        }
+    };
+
+    bool ok = true;
+    // The builds are spread over all 512 threads, one item per (row, group
+    // of words), so that no warp carries a whole row while the others wait at
+    // the stage barrier; item -> (row, column) divides with a float
+    // reciprocal and one correction step.
+    auto split = [](int it, int n, float inv, int &row, int &col) {
+        row = static_cast<int>(static_cast<float>(it) * inv);
+        col = it - row * n;
+        if (col >= n) {
+            ++row;
+            col -= n;
+        } else if (col < 0) {
+            --row;
+            col += n;
+        }
+    };
+
+    // quad-sum rows of stage s into Q buffer qb (waits for the stage's copies)
+    auto buildA = [&](int s, int qb) {
+        const int slot = slot_of(s);
+        const unsigned gs = sbase + static_cast<unsigned>(s);
+        if (!mbar_wait_bounded(bar0 + 8 * slot, (gs / SUB_SLOTS) & 1u)) {
+            if (ok)
+                atomicOr(p.err, DERR_TIMEOUT);
+            ok = false;
+        }
+        const int *blk = reinterpret_cast<const int *>(&sm[o_blk + slot * SUB_BLK_WORDS]);
+        const int q1 = blk[1], q2 = q1 + blk[2], q3 = q2 + blk[3];
+        const int total = min(q3 + blk[4], S.nqrow);
+        const int n4 = WQ >> 2;
+        const float inv = 1.0f / static_cast<float>(n4);
+        for (int it = tid; it < total * n4; it += NTHREADS) {
+            int r, t4;
+            split(it, n4, inv, r, t4);
+            const int i = (r >= q3) ? 3 : (r >= q2) ? 2 : (r >= q1) ? 1 : 0;
+            const int base = (i == 3) ? q3 : (i == 2) ? q2 : (i == 1) ? q1 : 0;
+            const unsigned pw = static_cast<unsigned>(blk[8 + 8 * i + (r - base)]);
+            const int tau = 4 * t4;
+            uint32_t a[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int rs = static_cast<int>(sm[o_rsh + slot * 16 + 4 * i + k]);
+                if (rs < 0) {
+                    a[k] = 0u;
+                } else {
+                    const int d = (k == 0) ? 0 : static_cast<int>((pw >> (8 * (k - 1))) & 255u);
+                    const int bb = rs + tau + d;
+                    const int wi = o_raw + (slot * 16 + 4 * i + k) * RAWW + (bb >> 2);
+                    a[k] = __funnelshift_r(sm[wi], sm[wi + 1], 8u * static_cast<unsigned>(bb & 3));
+                }
+            }
+            // 4x4 byte transpose, then the four channels of each sample summed
+            const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), hi01 = __byte_perm(a[0], a[1], 0x7362);
+            const uint32_t lo23 = __byte_perm(a[2], a[3], 0x5140), hi23 = __byte_perm(a[2], a[3], 0x7362);
+            const uint32_t s0 = __dp4a(__byte_perm(lo01, lo23, 0x5410), 0x01010101u, 0u);
+            const uint32_t s1 = __dp4a(__byte_perm(lo01, lo23, 0x7632), 0x01010101u, 0u);
+            const uint32_t s2 = __dp4a(__byte_perm(hi01, hi23, 0x5410), 0x01010101u, 0u);
+            const uint32_t s3 = __dp4a(__byte_perm(hi01, hi23, 0x7632), 0x01010101u, 0u);
+            uint2 v;
+            v.x = s0 | (s1 << 16);
+            v.y = s2 | (s3 << 16);
+            *reinterpret_cast<uint2 *>(&sm[o_Q + (qb * S.nqrow + r) * HQ + 2 * t4]) = v;
+        }
+    };
+
+    // partial-sum rows of stage s (from Q buffer qb) into P buffer pb
+    auto buildB = [&](int s, int qb, int pb) {
+        const int slot = slot_of(s);
+        const int *blk = reinterpret_cast<const int *>(&sm[o_blk + slot * SUB_BLK_WORDS]);
+        const int npat = min(blk[0], S.npat);
+        const int nq = min(4, (p.nch_used - 16 * s + 3) >> 2);
+        int qbase[4];
+        qbase[0] = 0;
+#pragma unroll
+        for (int i = 1; i < 4; ++i)
+            qbase[i] = qbase[i - 1] + blk[i];
+        const float inv = 1.0f / static_cast<float>(HALF);
+        for (int it = tid; it < npat * HALF; it += NTHREADS) {
+            int pp, k;
+            split(it, HALF, inv, pp, k);
+            const int key = blk[40 + pp];
+            uint32_t ev = 0u, od = 0u; // (P[2k], P[2k+1]) and (P[2k+1], P[2k+2]) in 16-bit lanes
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                if (i < nq) {
+                    const int off = (i == 0) ? 0 : blk[56 + 3 * pp + i - 1];
+                    const int u = o_Q + (qb * S.nqrow + qbase[i] + ((key >> (4 * i)) & 15)) * HQ + ((2 * k + off) >> 1);
+                    const uint32_t w0 = sm[u], w1 = sm[u + 1];
+                    const uint32_t mid = __byte_perm(w0, w1, 0x5432); // high half of w0, low half of w1
+                    if (off & 1) {
+                        ev += mid;
+                        od += w1;
+                    } else {
+                        ev += w0;
+                        od += mid;
+                    }
+                }
+            }
+            const int even = o_P + pb * PBUF + pp * HALF + k;
+            sm[even] = ev;
+            sm[even + S.npat * HALF] = od;
+        }
+    };
+
+    uint32_t acc[4][2 * M2];
+    uint32_t a16[4][M2];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int m = 0; m < 2 * M2; ++m)
+            acc[j][m] = 0u;
+#pragma unroll
+        for (int m = 0; m < M2; ++m)
+            a16[j][m] = 0u;
+    }
+    auto flush = [&]() {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int m = 0; m < M2; ++m) {
+                acc[j][2 * m] += a16[j][m] & 0xFFFFu;
+                acc[j][2 * m + 1] += a16[j][m] >> 16;
+                a16[j][m] = 0u;
+            }
+    };
+
+    // prologue: copies for the first SUB_SLOTS stages, quad rows of 0 and 1, sums of 0
+#pragma unroll
+    for (int s = 0; s < SUB_SLOTS; ++s)
+        issue(s);
+    __syncthreads();
+    if (nstages > 0)
+        buildA(0, 0);
+    fence_proxy_async();
+    __syncthreads();
+    if (nstages > 1)
+        buildA(1, 1);
+    if (nstages > 0)
+        buildB(0, 0, 0);
+    fence_proxy_async();
+    __syncthreads();
+
+    for (int s = 0; s < nstages; ++s) {
+        if (s + 2 < nstages)
+            buildA(s + 2, s & 1);
+        if (s + 1 < nstages)
+            buildB(s + 1, (s + 1) & 1, (s + 1) & 1);
+        if (ok) {
+            const int slot = slot_of(s);
+            const int4 e4 = *reinterpret_cast<const int4 *>(&sm[o_ent + slot * 64 + 4 * warp]);
+            const int ej[4] = {e4.x, e4.y, e4.z, e4.w};
+            const int pbase = o_P + (s & 1) * PBUF + lane;
+            uint32_t w[M2];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int e = ej[j];
+                if (e < 0) {
+                    atomicOr(p.err, DERR_WINDOW);
+                    continue;
+                }
+                if (j == 0 || e != ej[j - 1]) {
+                    const int row = pbase + (e & 1) * S.npat * HALF + (e >> 1);
+#pragma unroll
+                    for (int m = 0; m < M2; ++m)
+                        w[m] = sm[row + 32 * m];
+                }
+#pragma unroll
+                for (int m = 0; m < M2; ++m)
+                    a16[j][m] += w[m];
+            }
+            if ((s & 15) == 15)
+                flush();
+        }
+        fence_proxy_async();
+        __syncthreads();
+        issue(s + SUB_SLOTS);
+    }
+    flush();
+    stage_ctr = sbase + static_cast<unsigned>(nstages);
+    if (!ok)
+        return false;
+
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int dm = dm0 + 4 * warp + j;
+        if (dm >= p.ndms)
+            continue;
+        float *orow = p.out + static_cast<long long>(dm) * p.out_pitch;
+#pragma unroll
+        for (int m = 0; m < 2 * M2; ++m) {
+            const long long t = t0 + 2 * lane + 64 * (m >> 1) + (m & 1);
+            if (t < p.tp) {
+                const float v = static_cast<float>(static_cast<int>(acc[j][m]));
+                orow[t] = p.divide_by_bin ? (v / p.nchans_f / p.bin_f) : (v / p.nchans_f);
+            }
         }
     }
     return true;

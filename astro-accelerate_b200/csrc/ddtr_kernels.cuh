@@ -109,6 +109,35 @@ cudaError_t launch_quad_patterns(const int32_t *table, int nch_used, int ndms, i
 cudaError_t launch_quad_offsets(const int32_t *qtmp, size_t n, int W, int32_t *qoff, cudaStream_t st);
 cudaError_t launch_ddtr_quad(const DdtrLaunch &p, const QuadLaunch &q, cudaStream_t st);
 
+// Subband kernel (ddtr_sub.cu): 16-channel partial sums per skew pattern.
+constexpr int SUB_BLK_WORDS = 128; // pattern block per (subband, DM group)
+constexpr int SUB_MAX_PAT = 16;    // patterns per (subband, DM group)
+constexpr int SUB_MAX_QPAT = 8;    // distinct skews per quad and group
+constexpr int SUB_MAX_OFF = 1023;  // largest quad offset inside a subband
+
+struct SubLaunch {
+    const int32_t *sblk; // [group][nsub][SUB_BLK_WORDS]
+    const int32_t *swin; // [group][nsub_pad]
+    const int32_t *soff; // [nsub][ndms]
+    int nsub, nsub_pad;
+    int W;     // samples per partial-sum row (even)
+    int wq;    // samples per quad-sum row (a multiple of 4; 16-bit sums, two per word)
+    int raww;  // words per staged raw row
+    int npat;  // partial-sum rows per buffer (max patterns)
+    int nqrow; // quad rows per buffer (max distinct skews per subband)
+};
+
+struct SubGeometry {
+    int W, wq, raww, npat, nqrow, nsub_pad;
+    size_t smem_bytes;
+};
+
+SubGeometry sub_geometry(int maxtau, int maxoff, int maxd, int maxpat, int maxqrows, int nsub);
+cudaError_t launch_sub_patterns(const int32_t *table, int nch_used, int ndms, int nsub, int nsub_pad, int32_t *sblk,
+                                int32_t *swin, int32_t *stmp, int *stats, cudaStream_t st);
+cudaError_t launch_sub_offsets(const int32_t *stmp, size_t n, int W, int32_t *soff, cudaStream_t st);
+cudaError_t launch_ddtr_sub(const DdtrLaunch &p, const SubLaunch &s, cudaStream_t st);
+
 // Dynamic shared memory the staged kernels may use per CTA (the sm_100a
 // opt-in limit less 1 KB, which the persistent kernel keeps for its job
 // descriptor).

@@ -127,10 +127,20 @@ bool DdtrPipeline::build_range(int r)
         return fail(error_.empty() ? "no DM-group size fits the delay span of range " + std::to_string(r) : error_);
     if (!check_device_flags())
         return false;
-    if (elem_bytes_ == 1 && opt_.kernel_variant != 1 && rc.group_dms == 64) {
+    if (elem_bytes_ == 1 && (opt_.kernel_variant == 0 || opt_.kernel_variant == 3) && rc.group_dms == 64) {
+        if (!build_sub_tables(r))
+            return false;
+    }
+    if (elem_bytes_ == 1 && (opt_.kernel_variant == 0 || opt_.kernel_variant == 2) && rc.group_dms == 64) {
         if (!build_quad_tables(r))
             return false;
     }
+    // both available (variant 0): the channel-quad kernel until the autotuner
+    // has timed the two
+    if (rc.has_quad)
+        rc.variant = 2;
+    else if (rc.has_sub)
+        rc.variant = 4;
     if (elem_bytes_ == 2 && opt_.kernel_variant != 1 && rc.group_dms == 64 && nchans <= 16384) {
         const F32Geometry G = f32_geometry(rc.span, rc.group_dms, nchans, 0);
         if (G.smem_bytes > 0) {
@@ -194,6 +204,7 @@ bool DdtrPipeline::build_quad_tables(int r)
         if (G.smem_bytes <= kStagedSmemLimit && rc.quad_dmax <= 255) {
             rc.quad = G;
             rc.variant = 2;
+            rc.has_quad = true;
             ok = check_cuda(launch_quad_offsets(d_qtmp, nq_ent, G.W, rc.d_qoff, st_), "quad offsets");
             ++launches_;
         }
@@ -202,13 +213,70 @@ bool DdtrPipeline::build_quad_tables(int r)
         ok = check_cuda(cudaStreamSynchronize(st_), "sync");
     cudaFree(d_qtmp);
     cudaFree(d_stats);
-    if (rc.variant != 2) {
+    if (!rc.has_quad) {
         cudaFree(rc.d_qpat);
         cudaFree(rc.d_qwin);
         cudaFree(rc.d_qoff);
         rc.d_qpat = rc.d_qwin = rc.d_qoff = nullptr;
         if (opt_.kernel_variant == 2)
             return fail("the channel-quad kernel does not fit range " + std::to_string(r));
+    }
+    return ok;
+}
+
+// Subband tables: skew patterns of every (16-channel subband, DM group),
+// subband windows and offsets; the subband kernel runs the range when every
+// (subband, DM trial) has an exact pattern and the stage fits shared memory.
+bool DdtrPipeline::build_sub_tables(int r)
+{
+    RangeConfig &rc = ranges_[r];
+    const int ndms = strategy_.ndms(r);
+    const int nsub = (rc.nch_used + 15) / 16;
+    const int nsub_pad = (nsub + 3) & ~3;
+    const int ngroups = ndms / 64;
+    int *d_stats = nullptr;
+    int32_t *d_stmp = nullptr;
+    int hs[6] = {0, 0, 0, 0, 0, 0};
+    const size_t n_ent = static_cast<size_t>(nsub) * ndms;
+    if (!check_cuda(cudaMalloc(&rc.d_sblk, static_cast<size_t>(ngroups) * nsub * SUB_BLK_WORDS * sizeof(int32_t)),
+                    "cudaMalloc") ||
+        !check_cuda(cudaMalloc(&rc.d_swin, static_cast<size_t>(ngroups) * nsub_pad * sizeof(int32_t)), "cudaMalloc") ||
+        !check_cuda(cudaMemsetAsync(rc.d_swin, 0, static_cast<size_t>(ngroups) * nsub_pad * sizeof(int32_t), st_),
+                    "memset") ||
+        !check_cuda(cudaMalloc(&rc.d_soff, n_ent * sizeof(int32_t)), "cudaMalloc") ||
+        !check_cuda(cudaMalloc(&d_stmp, n_ent * sizeof(int32_t)), "cudaMalloc") ||
+        !check_cuda(cudaMalloc(&d_stats, 6 * sizeof(int)), "cudaMalloc") ||
+        !check_cuda(cudaMemsetAsync(d_stats, 0, 6 * sizeof(int), st_), "memset"))
+        return false;
+    bool ok = check_cuda(launch_sub_patterns(rc.d_table, rc.nch_used, ndms, nsub, nsub_pad, rc.d_sblk, rc.d_swin,
+                                             d_stmp, d_stats, st_),
+                         "subband patterns") &&
+              check_cuda(cudaMemcpyAsync(hs, d_stats, 6 * sizeof(int), cudaMemcpyDeviceToHost, st_), "D2H") &&
+              check_cuda(cudaStreamSynchronize(st_), "sync");
+    ++launches_;
+    if (ok && hs[5] == 0 && hs[3] >= 1) {
+        const SubGeometry G = sub_geometry(hs[0], hs[1], hs[2], hs[3], hs[4], nsub);
+        if (G.smem_bytes <= kStagedSmemLimit) {
+            rc.sub = G;
+            rc.nsub = nsub;
+            rc.variant = 4;
+            rc.has_sub = true;
+            ok = check_cuda(launch_sub_offsets(d_stmp, n_ent, G.W, rc.d_soff, st_), "subband offsets");
+            ++launches_;
+        }
+    }
+    if (ok)
+        ok = check_cuda(cudaStreamSynchronize(st_), "sync");
+    cudaFree(d_stmp);
+    cudaFree(d_stats);
+    if (!rc.has_sub) {
+        cudaFree(rc.d_sblk);
+        cudaFree(rc.d_swin);
+        cudaFree(rc.d_soff);
+        rc.d_sblk = rc.d_swin = rc.d_soff = nullptr;
+        if (opt_.kernel_variant == 3)
+            return fail("the subband kernel cannot run range " + std::to_string(r) +
+                        " (patterns without an exact split, or its stage does not fit shared memory)");
     }
     return ok;
 }
@@ -347,6 +415,7 @@ bool DdtrPipeline::setup()
         rawb_max = std::max(rawb_max, 4 * ddtr_u8_rw(ranges_[r].span, ranges_[r].tile_words) + 32);
         rawb_max = std::max(rawb_max, 4 * ranges_[r].quad.raww + 64);
         rawb_max = std::max(rawb_max, ranges_[r].f32.rawh + 16);
+        rawb_max = std::max(rawb_max, 4 * ranges_[r].sub.raww + 64);
     }
 
     const long long L0 = static_cast<long long>(strategy_.t_processed()[0][0]) + strategy_.maxshift();
@@ -454,6 +523,18 @@ bool DdtrPipeline::tune_ranges()
         } else {
             rc.f32.cs = job.f.cs;
         }
+        if (rc.variant == 2 && rc.has_sub) {
+            // the subband kernel against the tuned channel-quad kernel
+            const float t_quad = time_job_slice(job, st_, device_, err);
+            rc.variant = 4;
+            DdtrJob js;
+            if (t_quad < 0.f || !make_job(*op, d_flat_[op->src_level & 1], flat_elems_, out, pitch, js))
+                return fail(err.empty() ? error_ : err);
+            const float t_sub = time_job_slice(js, st_, device_, err);
+            if (t_sub < 0.f)
+                return fail(err);
+            rc.variant = (t_sub < t_quad) ? 4 : 2;
+        }
     }
     return check_cuda(cudaStreamSynchronize(st_), "sync");
 }
@@ -552,15 +633,20 @@ bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, f
     const int tp = op.tp;
     const long long i_nsamp = op.i_nsamp;
     job = DdtrJob();
-    job.variant = (elem_bytes_ == 1 && rc.variant == 2) ? 2 : (elem_bytes_ == 2 && rc.variant == 3) ? 3 : 1;
+    job.variant = (elem_bytes_ == 1 && rc.variant == 2)   ? 2
+                  : (elem_bytes_ == 2 && rc.variant == 3) ? 3
+                  : (elem_bytes_ == 1 && rc.variant == 4) ? 4
+                                                          : 1;
     job.elem_bytes = elem_bytes_;
     job.tile_words = rc.tile_words;
     job.offtab = rc.d_offtab;
-    const int tile = (job.variant == 2) ? 32 * rc.quad.M : (job.variant == 3 ? 512 : 128 * rc.tile_words);
+    const int tile = (job.variant == 2) ? 32 * rc.quad.M : ((job.variant == 3 || job.variant == 4) ? 512 : 128 * rc.tile_words);
     const long long ntiles = (tp + tile - 1) / tile;
     long long need;
     if (elem_bytes_ == 1 && job.variant == 2)
         need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ntiles * tile + rc.delay_max + 4LL * rc.quad.raww + 64;
+    else if (job.variant == 4)
+        need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ntiles * tile + rc.delay_max + 4LL * rc.sub.raww + 64;
     else if (elem_bytes_ == 1)
         need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ntiles * tile + rc.delay_max +
                4LL * ddtr_u8_rw(rc.span, rc.tile_words) + 64;
@@ -606,6 +692,18 @@ bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, f
         q.M = rc.quad.M;
     } else if (job.variant == 3) {
         job.f = rc.f32;
+    } else if (job.variant == 4) {
+        SubLaunch &s = job.s;
+        s.sblk = rc.d_sblk;
+        s.swin = rc.d_swin;
+        s.soff = rc.d_soff;
+        s.nsub = rc.nsub;
+        s.nsub_pad = rc.sub.nsub_pad;
+        s.W = rc.sub.W;
+        s.wq = rc.sub.wq;
+        s.raww = rc.sub.raww;
+        s.npat = rc.sub.npat;
+        s.nqrow = rc.sub.nqrow;
     }
     job.groups = p.ndms / p.group_dms;
     job.tiles = ntiles;
@@ -619,6 +717,8 @@ cudaError_t launch_job(const DdtrJob &job, cudaStream_t st)
         return launch_ddtr_quad(job.p, job.q, st);
     if (job.variant == 3)
         return launch_ddtr_f32(job.p, job.f, st);
+    if (job.variant == 4)
+        return launch_ddtr_sub(job.p, job.s, st);
     return (job.elem_bytes == 1) ? launch_ddtr_u8(job.p, job.offtab, job.tile_words, st) : launch_ddtr_u16(job.p, st);
 }
 
@@ -824,8 +924,12 @@ bool DdtrPipeline::cleanup()
         cudaFree(rc.d_qpat);
         cudaFree(rc.d_qwin);
         cudaFree(rc.d_qoff);
+        cudaFree(rc.d_sblk);
+        cudaFree(rc.d_swin);
+        cudaFree(rc.d_soff);
         rc.d_table = rc.d_wmin = rc.d_offtab = nullptr;
         rc.d_qpat = rc.d_qwin = rc.d_qoff = nullptr;
+        rc.d_sblk = rc.d_swin = rc.d_soff = nullptr;
     }
     ranges_.clear();
     for (int i = 0; i < 2; ++i) {

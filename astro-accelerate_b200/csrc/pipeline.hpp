@@ -40,7 +40,8 @@ struct PipelineOptions {
     int failsafe = 0;           // force the cache-kernel delay semantics
     size_t free_memory = 0;     // 0: query the device like aa_device_info::free_memory()
     int tile_words = 0;         // 0: autotune
-    int kernel_variant = 0;     // 0: autotune, 1: generic kernels, 2: staged kernels (channel-quad / fp32)
+    int kernel_variant = 0;     // 0: choose per range, 1: generic kernels, 2: channel-quad / fp32 kernels,
+                                // 3: subband / fp32 kernels
     int group_dms = 0;          // 0: autotune
     bool device_input = false;  // the input pointer is device memory ([t][c] uint16)
     bool device_output = false; // keep the whole output on the device ([range][dm][t])
@@ -68,13 +69,14 @@ struct DdtrOp {
 
 // A dedispersion launch, ready for a stream (launch_job) or a batch queue.
 struct DdtrJob {
-    int variant = 1; // 1 generic, 2 channel-quad, 3 staged fp32
+    int variant = 1; // 1 generic, 2 channel-quad, 3 staged fp32, 4 subband
     int elem_bytes = 1;
     int tile_words = 4;
     const int32_t *offtab = nullptr;
     DdtrLaunch p{};
     QuadLaunch q{};
     F32Launch f{};
+    SubLaunch s{};
     int groups = 0;       // CTAs along DM
     long long tiles = 0;  // CTAs along time
     int tile_samples = 0; // samples per CTA tile
@@ -101,7 +103,8 @@ struct RangeConfig {
     int32_t *d_offtab = nullptr;
     // channel-quad kernel
     // 1: generic kernel (k_ddtr_u8 byte-phase / k_ddtr_u16 gather), 2: channel-quad
-    // kernel (k_ddtr_quad, one-byte data), 3: staged fp32 kernel (k_ddtr_f32, two-byte data)
+    // kernel (k_ddtr_quad, one-byte data), 3: staged fp32 kernel (k_ddtr_f32, two-byte data),
+    // 4: subband kernel (k_ddtr_sub, one-byte data)
     int variant = 1;
     QuadGeometry quad{};
     int quad_span = 0, quad_dmax = 0, quad_maxcnt = 0, nquads = 0;
@@ -110,6 +113,14 @@ struct RangeConfig {
     int32_t *d_qoff = nullptr;
     // staged fp32 kernel
     F32Launch f32{};
+    // subband kernel (variant 4); with the variant chosen per range both the
+    // subband and the channel-quad tables may exist until the autotuner picks
+    bool has_sub = false, has_quad = false;
+    SubGeometry sub{};
+    int nsub = 0;
+    int32_t *d_sblk = nullptr;
+    int32_t *d_swin = nullptr;
+    int32_t *d_soff = nullptr;
 };
 
 class DdtrPipeline {
@@ -168,6 +179,7 @@ private:
     bool check_device_flags();
     bool build_range(int r);
     bool build_quad_tables(int r);
+    bool build_sub_tables(int r);
     bool tune_ranges();
     bool step(bool allow_sync);
     bool enumerate_ops();

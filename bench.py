@@ -792,7 +792,8 @@ def main():
     except OSError:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
-    kernel_names = {"quad": "k_ddtr_quad", "phase": "k_ddtr_u8", "f32": "k_ddtr_f32", "gather": "k_ddtr_u16"}
+    kernel_names = {"quad": "k_ddtr_quad", "phase": "k_ddtr_u8", "f32": "k_ddtr_f32", "gather": "k_ddtr_u16",
+                    "sub": "k_ddtr_sub"}
     used = sorted({kernel_names[ri["kernel"]] for ri in ranges})
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": None, "kernel": "+".join(used),
