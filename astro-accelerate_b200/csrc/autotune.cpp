@@ -8,7 +8,7 @@ namespace aab200 {
 
 bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache &cache, std::string &err)
 {
-    const bool quad = (job.variant == 2);
+    const bool quad = (job.variant == 2 || job.variant == 5);
     const auto key = std::make_tuple(job.variant, job.p.nch_used, quad ? job.q.W : job.f.W,
                                      quad ? job.q.raww : job.f.rawh, quad ? job.q.npool / std::max(1, job.q.qs) : 0,
                                      job.p.kind, static_cast<long long>(job.groups));
@@ -38,11 +38,15 @@ bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache 
                     continue;
                 t.q.qs = c;
                 t.q.npool = c * maxcnt;
-                BatchJobDev d{};
-                d.p = t.p;
-                d.q = t.q;
-                d.variant = 2;
-                bytes = persistent_job_smem(d);
+                if (job.variant == 5) {
+                    bytes = quadws_smem_bytes(t.q);
+                } else {
+                    BatchJobDev d{};
+                    d.p = t.p;
+                    d.q = t.q;
+                    d.variant = 2;
+                    bytes = persistent_job_smem(d);
+                }
             } else {
                 if (c < 4)
                     continue;

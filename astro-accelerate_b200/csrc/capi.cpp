@@ -519,9 +519,9 @@ bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant)
     Api *a = as_api(obj);
     if (a->pipe)
         return api_fail(a, "the kernel variant must be set before the plan is bound");
-    if (variant < 0 || variant > 3)
-        return api_fail(a, "kernel variant must be 0 (auto), 1 (generic kernels), 2 (channel-quad / fp32 kernels) or "
-                           "3 (subband / fp32 kernels)");
+    if (variant < 0 || variant > 4)
+        return api_fail(a, "kernel variant must be 0 (auto), 1 (generic kernels), 2 (channel-quad / fp32 kernels), "
+                           "3 (subband / fp32 kernels) or 4 (warp-specialised channel-quad / fp32 kernels)");
     a->popt.kernel_variant = variant;
     return true;
 }
@@ -575,6 +575,10 @@ int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms,
     } else if (rc.variant == 3) {
         *kind |= 0x200;
         *tile_words = 4;
+    } else if (rc.variant == 5) {
+        *kind |= 0x1000;
+        *span = rc.quad_span;
+        *tile_words = rc.quad.M / 4;
     } else if (rc.variant == 4) {
         *kind |= 0x800;
         *span = rc.sub.W - 514;
@@ -591,7 +595,7 @@ int aa_b200_pipeline_stage_depth(void *obj, int range)
     if (!a->pipe || !a->pipe->setup() || range < 0 || range >= static_cast<int>(a->pipe->strategy().nranges()))
         return 0;
     const RangeConfig &rc = a->pipe->range_config(range);
-    return rc.variant == 2 ? rc.quad.qs : (rc.variant == 3 ? rc.f32.cs : (rc.variant == 4 ? 1 : 0));
+    return (rc.variant == 2 || rc.variant == 5) ? rc.quad.qs : (rc.variant == 3 ? rc.f32.cs : (rc.variant == 4 ? 1 : 0));
 }
 
 long long aa_b200_pipeline_kernel_launches(void *obj)

@@ -53,6 +53,86 @@ __device__ __forceinline__ void init_barriers(unsigned bar0)
 }
 
 // ---------------------------------------------------------------------------
+// Pre-skewed quad rows of one shared-memory stage (warp-specialised body).
+//
+// Row k of quad q holds, per sample tau of the window, the four channels'
+// bytes x_i[tau + d_i] in one word (d_0 = 0, d_1..3 the skews of the quad's
+// pattern k).  Work items are (quad, 128-sample column block): a lane takes
+// four samples of one quad and walks the quad's patterns in order.  Patterns
+// are found in DM order, so consecutive ones mostly share a channel's skew:
+// the lane keeps each channel's last funnel-shifted word and reloads it only
+// when that skew changes; channel 0 (skew 0) is loaded once.
+//   stage: raw rows at o_raw + (slot*QS*4 + 4q + i) * RAWW, byte shift of
+//   each row at o_rsh (-1: channel past the last used channel), patterns at
+//   o_pat + (slot*QS + q)*16 (word 15: pattern count); rows of the stage are
+//   numbered quad by quad and written to P at o_P + (b*npool + row) * W.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void build_quad_rows(uint32_t *sm, int o_raw, int o_pat, int o_rsh, int o_P, int slot,
+                                                int QS, int nq, int RAWW, int W, int npool, int b, int worker,
+                                                int nworkers, int lane)
+{
+    const int n4 = W >> 2;
+    const int nblk = (n4 + 31) >> 5;
+    int q = 0, rbase = 0;
+    for (int item = worker; item < nq * nblk; item += nworkers) {
+        const int qi = item / nblk;
+        const int blk = item - qi * nblk;
+        if (qi < q) {
+            q = 0;
+            rbase = 0;
+        }
+        while (q < qi) {
+            rbase += static_cast<int>(sm[o_pat + (slot * QS + q) * 16 + 15]);
+            ++q;
+        }
+        const int pbase = o_pat + (slot * QS + q) * 16;
+        const int cnt = min(static_cast<int>(sm[pbase + 15]), npool - rbase);
+        const int t4 = (blk << 5) + lane;
+        const bool live = t4 < n4;
+        const int tau = 4 * t4;
+        int rs[4], rb[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            rs[i] = static_cast<int>(sm[o_rsh + slot * QS * 4 + 4 * q + i]);
+            rb[i] = o_raw + (slot * QS * 4 + 4 * q + i) * RAWW;
+        }
+        auto word = [&](int i, int d) -> uint32_t {
+            if (!live || rs[i] < 0)
+                return 0u;
+            const int bb = rs[i] + tau + d;
+            const int wi = rb[i] + (bb >> 2);
+            return __funnelshift_r(sm[wi], sm[wi + 1], 8u * static_cast<unsigned>(bb & 3));
+        };
+        uint32_t a[4];
+        int dl[4] = {0, -1, -1, -1};
+        a[0] = word(0, 0);
+        a[1] = a[2] = a[3] = 0u;
+        int prow = o_P + (b * npool + rbase) * W + tau;
+        for (int k = 0; k < cnt; ++k, prow += W) {
+            const unsigned pwd = sm[pbase + k];
+#pragma unroll
+            for (int i = 1; i < 4; ++i) {
+                const int d = static_cast<int>((pwd >> (8 * (i - 1))) & 255u);
+                if (d != dl[i]) {
+                    dl[i] = d;
+                    a[i] = word(i, d);
+                }
+            }
+            // 4x4 byte transpose: word k of the result holds sample tau+k of the four channels
+            const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), hi01 = __byte_perm(a[0], a[1], 0x7362);
+            const uint32_t lo23 = __byte_perm(a[2], a[3], 0x5140), hi23 = __byte_perm(a[2], a[3], 0x7362);
+            uint4 v;
+            v.x = __byte_perm(lo01, lo23, 0x5410);
+            v.y = __byte_perm(lo01, lo23, 0x7632);
+            v.z = __byte_perm(hi01, hi23, 0x5410);
+            v.w = __byte_perm(hi01, hi23, 0x7632);
+            if (live)
+                *reinterpret_cast<uint4 *>(&sm[prow]) = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Channel-quad body (one-byte samples, integer sums with IDP4A).
 //
 // Shared memory (words from sm): qwin[nq_pad] | raw[QNSTAGE][QS*4][RAWW] |
@@ -804,6 +884,244 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
         }
     }
     return true;
+}
+
+// ---------------------------------------------------------------------------
+// Warp-specialised channel-quad body: 16 consumer warps sum (as quad_body)
+// while WS_PROD producer warps build the next stage's pre-skewed rows, so the
+// two overlap instead of alternating between CTA barriers.
+//
+// WS_THREADS threads.  Warp 16 (a producer) issues the TMA copies.  Hand-offs are
+// mbarriers (all waits bounded; every thread of a role arrives, so each
+// thread's own shared-memory accesses are ordered by its arrival):
+//   tfull[slot]  the stage's copies landed             (TMA transaction count)
+//   sempty[slot] producers and consumers are done with the slot (all threads)
+//   pfull[b]     the stage's rows are built in buffer b (producer threads)
+//   pempty[b]    consumers are done with buffer b       (512 consumer threads)
+// After a wait gives up, a thread stops waiting (and the copy warp stops
+// issuing), so a failing CTA ends after one bounded wait per barrier; the
+// copy warp then waits once more for copies it issued before the CTA exits.
+// Phases follow the running stage counter, so a persistent CTA could carry
+// them from one tile to the next.
+//
+// Shared memory (words from sm): mbar[8 + 2*WS_NB ... rounded to 4] |
+// qwin[nq_pad] | raw[3][QS*4][RAWW] | ent[3][QS][64] | pat[3][QS][16] |
+// rsh[3][QS*4] | P[WS_NB][npool][W].
+// ---------------------------------------------------------------------------
+constexpr int WS_NB = 2;                      // pattern-row buffers
+constexpr int WS_PROD = 4;                    // producer warps
+constexpr int WS_THREADS = 32 * (16 + WS_PROD); // 16 consumer warps + producers
+constexpr int WS_MB_WORDS = ((2 * (QNSTAGE + 2 * WS_NB)) + 3) & ~3; // sempty, pfull, pempty
+
+__host__ __device__ inline size_t quad_ws_body_words(int qs, int raww, int nq_pad, int npool, int W)
+{
+    size_t o = WS_MB_WORDS + static_cast<size_t>(nq_pad);
+    o += static_cast<size_t>(QNSTAGE) * qs * 4 * raww;
+    o += static_cast<size_t>(QNSTAGE) * qs * 64;
+    o += static_cast<size_t>(QNSTAGE) * qs * 16;
+    o += static_cast<size_t>(QNSTAGE) * qs * 4;
+    o = (o + 3) & ~static_cast<size_t>(3);
+    o += static_cast<size_t>(WS_NB) * npool * W;
+    return o;
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool quad_ws_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long long t0,
+                                             uint32_t *sm, unsigned bar0, unsigned &stage_ctr)
+{
+    constexpr int M = 16;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const bool producer = warp >= 16;
+    const int pw = warp - 16; // producer index 0..WS_PROD-1
+    const int GD = 64;
+    const int dm0 = g * GD;
+    const int W = Q.W, RAWW = Q.raww, QS = Q.qs;
+    const unsigned char *in = static_cast<const unsigned char *>(p.in);
+    const int nstages = (Q.nquads + QS - 1) / QS;
+    const unsigned sbase = stage_ctr;
+
+    const unsigned mb = smem_addr(sm);
+    const unsigned mb_sempty = mb;                         // QNSTAGE
+    const unsigned mb_pfull = mb + 8 * QNSTAGE;            // WS_NB
+    const unsigned mb_pempty = mb + 8 * (QNSTAGE + WS_NB); // WS_NB
+    const int o_qw = WS_MB_WORDS;
+    const int o_raw = o_qw + Q.nq_pad;
+    const int o_ent = o_raw + QNSTAGE * QS * 4 * RAWW;
+    const int o_pat = o_ent + QNSTAGE * QS * GD;
+    const int o_rsh = o_pat + QNSTAGE * QS * 16;
+    const int o_P = ((o_rsh + QNSTAGE * QS * 4) + 3) & ~3;
+
+    if (tid == 0 && sbase == 0) {
+        for (int i = 0; i < QNSTAGE; ++i)
+            mbar_init(mb_sempty + 8 * i, WS_THREADS);
+        for (int i = 0; i < WS_NB; ++i) {
+            mbar_init(mb_pfull + 8 * i, 32 * WS_PROD);
+            mbar_init(mb_pempty + 8 * i, 512);
+        }
+        mbar_init_fence();
+    }
+    for (int i = tid; i < (Q.nq_pad >> 2); i += WS_THREADS)
+        cp_async16(&sm[o_qw + 4 * i], Q.qwin + static_cast<size_t>(g) * Q.nq_pad + 4 * i);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+
+    bool ok = true;
+    auto wait = [&](unsigned bar, unsigned parity) {
+        if (ok && !mbar_wait_bounded(bar, parity)) {
+            atomicOr(p.err, DERR_TIMEOUT);
+            ok = false;
+        }
+    };
+
+    // producer warp 0: copies of stage s (after every user of its slot is
+    // done).  The raw-row shifts are written before the arrival that opens
+    // the stage, so the stage's readers see them once its copies land.
+    int last_issued = -1;
+    auto issue = [&](int s) {
+        if (s >= nstages)
+            return;
+        const unsigned gs = sbase + static_cast<unsigned>(s);
+        const int slot = static_cast<int>(gs % QNSTAGE);
+        if (gs >= QNSTAGE)
+            wait(mb_sempty + 8 * slot, ((gs / QNSTAGE) - 1) & 1u);
+        if (!ok)
+            return;
+        const int q0 = s * QS;
+        const int nq = min(QS, Q.nquads - q0);
+        const int c0 = 4 * q0;
+        const int nrows = max(0, min(4 * nq, p.nch_used - c0));
+        const unsigned bar = bar0 + 8 * slot;
+        uintptr_t a = 0;
+        if (lane < 4 * nq) {
+            if (lane < nrows) {
+                const int w0 = static_cast<int>(sm[o_qw + q0 + (lane >> 2)]);
+                a = reinterpret_cast<uintptr_t>(in + static_cast<long long>(c0 + lane) * p.stride + t0 + w0);
+                sm[o_rsh + slot * QS * 4 + lane] = static_cast<uint32_t>(a & 15);
+            } else {
+                sm[o_rsh + slot * QS * 4 + lane] = 0xFFFFFFFFu; // channel contributes nothing
+            }
+        }
+        __syncwarp();
+        fence_proxy_async();
+        if (lane == 0)
+            mbar_expect_tx(bar, static_cast<unsigned>(nrows * RAWW * 4 + nq * GD * 4 + nq * 64));
+        __syncwarp();
+        last_issued = s;
+        if (lane < nrows)
+            tma_load_1d(smem_addr(&sm[o_raw + (slot * QS * 4 + lane) * RAWW]),
+                        reinterpret_cast<const void *>(a & ~static_cast<uintptr_t>(15)),
+                        static_cast<unsigned>(RAWW * 4), bar);
+        if (lane < nq)
+            tma_load_1d(smem_addr(&sm[o_ent + (slot * QS + lane) * GD]),
+                        Q.qoff + static_cast<size_t>(q0 + lane) * p.ndms + dm0, static_cast<unsigned>(GD * 4), bar);
+        if (lane == 0)
+            tma_load_1d(smem_addr(&sm[o_pat + slot * QS * 16]), Q.qpat + (static_cast<size_t>(g) * Q.nquads + q0) * 16,
+                        static_cast<unsigned>(nq * 64), bar);
+    };
+
+    // The two roles share nothing after the split (the accumulators live only
+    // in the consumer branch), so each fits the 96 registers a thread has
+    // with five warps per scheduler.
+    if (producer) {
+        if (pw == 0)
+            for (int s = 0; s < QNSTAGE - 1; ++s)
+                issue(s);
+        for (int s = 0; s < nstages; ++s) {
+            const unsigned gs = sbase + static_cast<unsigned>(s);
+            const int slot = static_cast<int>(gs % QNSTAGE);
+            const int b = static_cast<int>(gs % WS_NB);
+            wait(bar0 + 8 * slot, (gs / QNSTAGE) & 1u);
+            if (gs >= WS_NB)
+                wait(mb_pempty + 8 * b, ((gs / WS_NB) - 1) & 1u);
+            const int nq = min(QS, Q.nquads - s * QS);
+            build_quad_rows(sm, o_raw, o_pat, o_rsh, o_P, slot, QS, nq, RAWW, W, Q.npool, b, pw, WS_PROD, lane);
+            mbar_arrive(mb_pfull + 8 * b);
+            mbar_arrive(mb_sempty + 8 * slot);
+            if (pw == 0)
+                issue(s + QNSTAGE - 1);
+        }
+        if (pw == 0 && !ok)
+            for (int s = max(0, last_issued - (QNSTAGE - 1)); s <= last_issued; ++s) {
+                const unsigned gs = sbase + static_cast<unsigned>(s);
+                mbar_wait_bounded(bar0 + 8 * (gs % QNSTAGE), (gs / QNSTAGE) & 1u);
+            }
+    } else {
+        uint32_t acc[4][M];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int m = 0; m < M; ++m)
+                acc[j][m] = 0u;
+        for (int s = 0; s < nstages; ++s) {
+            const unsigned gs = sbase + static_cast<unsigned>(s);
+            const int slot = static_cast<int>(gs % QNSTAGE);
+            const int b = static_cast<int>(gs % WS_NB);
+            wait(bar0 + 8 * slot, (gs / QNSTAGE) & 1u);
+            wait(mb_pfull + 8 * b, (gs / WS_NB) & 1u);
+            const int q0 = s * QS;
+            const int nq = min(QS, Q.nquads - q0);
+            if (ok) {
+                int rbase = 0;
+                for (int q = 0; q < nq; ++q) {
+                    const int4 e4 = *reinterpret_cast<const int4 *>(&sm[o_ent + (slot * QS + q) * GD + warp * 4]);
+                    const int prow = o_P + (b * Q.npool + rbase) * W + lane;
+                    const int ej[4] = {e4.x, e4.y, e4.z, e4.w};
+                    // the host runs this body only on ranges whose every (quad, DM
+                    // trial) has a pre-skewed row (no per-byte path)
+                    if ((e4.x | e4.y | e4.z | e4.w) < 0)
+                        atomicOr(p.err, DERR_WINDOW);
+                    // neighbouring DM trials often share the quad's offset: a
+                    // word loaded for one serves the next (warp-uniform tests)
+                    int e[4];
+                    bool fresh[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        e[j] = prow + max(ej[j], 0);
+                        fresh[j] = (j == 0) || ej[j] != ej[j - 1];
+                    }
+#pragma unroll
+                    for (int m = 0; m < M; ++m) {
+                        uint32_t v = 0u;
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            if (fresh[j])
+                                v = sm[e[j] + 32 * m];
+                            acc[j][m] = __dp4a(v, 0x01010101u, acc[j][m]);
+                        }
+                    }
+                    rbase += static_cast<int>(sm[o_pat + (slot * QS + q) * 16 + 15]);
+                }
+            }
+            mbar_arrive(mb_pempty + 8 * b);
+            mbar_arrive(mb_sempty + 8 * slot);
+        }
+        if (ok) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int dm = dm0 + warp * 4 + j;
+                if (dm >= p.ndms)
+                    continue;
+                float *orow = p.out + static_cast<long long>(dm) * p.out_pitch;
+#pragma unroll
+                for (int m = 0; m < M; ++m) {
+                    const long long t = t0 + lane + 32 * m;
+                    if (t < p.tp) {
+                        const float v = static_cast<float>(static_cast<int>(acc[j][m]));
+                        orow[t] = p.divide_by_bin ? (v / p.nchans_f / p.bin_f) : (v / p.nchans_f);
+                    }
+                }
+            }
+        }
+    }
+    stage_ctr = sbase + static_cast<unsigned>(nstages);
+    __syncthreads();
+    return ok;
 }
 
 } // namespace body

@@ -85,6 +85,7 @@ int ddtr_u8_rw(int span, int tile_words);
 //   qpat [group][nquads][16] int32: skews (d1 | d2<<8 | d3<<16) in 0..14, count in 15
 //   qwin [group][nq_pad] int32: smallest base-channel delay of the group
 //   qtmp [nquads][ndms] int32: slot<<24 | tau (tau = delay - window start), -1 per-byte path
+//   stats [4]: max tau, max skew, max patterns, entries on the per-byte path
 //   qoff [nquads][ndms] int32: slot*W + tau, -1 per-byte path
 struct QuadLaunch {
     const int32_t *qpat;
@@ -108,6 +109,11 @@ cudaError_t launch_quad_patterns(const int32_t *table, int nch_used, int ndms, i
                                  int32_t *qpat, int32_t *qwin, int32_t *qtmp, int *stats, cudaStream_t st);
 cudaError_t launch_quad_offsets(const int32_t *qtmp, size_t n, int W, int32_t *qoff, cudaStream_t st);
 cudaError_t launch_ddtr_quad(const DdtrLaunch &p, const QuadLaunch &q, cudaStream_t st);
+// Warp-specialised channel-quad kernel (M = 16 only): producer warps build the
+// pre-skewed rows of the next stage while consumer warps sum the current one.
+// Runs only ranges without per-byte entries (stats[3] of the pattern kernel = 0).
+cudaError_t launch_ddtr_quadws(const DdtrLaunch &p, const QuadLaunch &q, cudaStream_t st);
+size_t quadws_smem_bytes(const QuadLaunch &q);
 
 // Subband kernel (ddtr_sub.cu): 16-channel partial sums per skew pattern.
 constexpr int SUB_BLK_WORDS = 128; // pattern block per (subband, DM group)

@@ -43,7 +43,7 @@ __global__ void k_quad_patterns(const int32_t *__restrict__ table, int nch_used,
     for (int j = 0; j < group_dms; ++j)
         lo = min(lo, table[static_cast<size_t>(c0) * ndms + dm0 + j] & 0xFFFFFF);
     int pats[QMAXPAT];
-    int cnt = 0, maxtau = 0, maxd = 0;
+    int cnt = 0, maxtau = 0, maxd = 0, nbyte = 0;
     for (int j = 0; j < group_dms; ++j) {
         const int dm = dm0 + j;
         const int e0 = table[static_cast<size_t>(c0) * ndms + dm];
@@ -77,6 +77,8 @@ __global__ void k_quad_patterns(const int32_t *__restrict__ table, int nch_used,
             }
         }
         qtmp[static_cast<size_t>(q) * ndms + dm] = (slot < 0) ? -1 : ((slot << 24) | tau);
+        if (slot < 0)
+            ++nbyte;
     }
     int32_t *pr = qpat + (static_cast<size_t>(g) * nquads + q) * 16;
     for (int k = 0; k < QMAXPAT; ++k)
@@ -86,6 +88,8 @@ __global__ void k_quad_patterns(const int32_t *__restrict__ table, int nch_used,
     atomicMax(stats + 0, maxtau);
     atomicMax(stats + 1, maxd);
     atomicMax(stats + 2, cnt);
+    if (nbyte)
+        atomicAdd(stats + 3, nbyte); // (quad, DM) entries that need the per-byte path
 }
 
 __global__ void k_quad_offsets(const int32_t *__restrict__ qtmp, size_t n, int W, int32_t *__restrict__ qoff)
@@ -112,7 +116,41 @@ __global__ void __launch_bounds__(32 * 64 / DW, (DW == 8) ? 2 : 1) k_ddtr_quad(c
                            bar0, stage_ctr);
 }
 
+// 16 consumer + WS_PROD producer warps (body::quad_ws_body); five warps per
+// scheduler leave 96 registers a thread.
+__global__ void __launch_bounds__(body::WS_THREADS, 1) k_ddtr_quadws(const DdtrLaunch p, const QuadLaunch Q)
+{
+    extern __shared__ __align__(16) uint32_t sm[];
+    const unsigned bar0 = smem_addr(sm);
+    body::init_barriers(bar0);
+    __syncthreads();
+    unsigned stage_ctr = 0;
+    body::quad_ws_body(p, Q, blockIdx.x, static_cast<long long>(blockIdx.y) * 512, sm + body::BAR_WORDS, bar0,
+                       stage_ctr);
+}
+
 } // namespace
+
+size_t quadws_smem_bytes(const QuadLaunch &q)
+{
+    return 4 * (body::BAR_WORDS + body::quad_ws_body_words(q.qs, q.raww, q.nq_pad, q.npool, q.W));
+}
+
+cudaError_t launch_ddtr_quadws(const DdtrLaunch &p, const QuadLaunch &q, cudaStream_t st)
+{
+    if (p.group_dms != 64 || q.qs < 1 || q.qs > 8 || q.M != 16)
+        return cudaErrorInvalidValue;
+    const size_t smem = quadws_smem_bytes(q);
+    if (smem > 227 * 1024)
+        return cudaErrorInvalidValue;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_ddtr_quadws, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess)
+        return e;
+    dim3 grid(p.ndms / p.group_dms, static_cast<unsigned>((p.tp + 511) / 512));
+    k_ddtr_quadws<<<grid, body::WS_THREADS, smem, st>>>(p, q);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_quad_patterns(const int32_t *table, int nch_used, int ndms, int group_dms, int nquads, int nq_pad,
                                  int32_t *qpat, int32_t *qwin, int32_t *qtmp, int *stats, cudaStream_t st)

@@ -131,7 +131,8 @@ bool DdtrPipeline::build_range(int r)
         if (!build_sub_tables(r))
             return false;
     }
-    if (elem_bytes_ == 1 && (opt_.kernel_variant == 0 || opt_.kernel_variant == 2) && rc.group_dms == 64) {
+    if (elem_bytes_ == 1 && (opt_.kernel_variant == 0 || opt_.kernel_variant == 2 || opt_.kernel_variant == 4) &&
+        rc.group_dms == 64) {
         if (!build_quad_tables(r))
             return false;
     }
@@ -141,6 +142,12 @@ bool DdtrPipeline::build_range(int r)
         rc.variant = 2;
     else if (rc.has_sub)
         rc.variant = 4;
+    if (elem_bytes_ == 1 && opt_.kernel_variant == 4) {
+        if (!quad_ws_fits(rc))
+            return fail("the warp-specialised channel-quad kernel cannot run range " + std::to_string(r) +
+                        " (entries on the per-byte path, or its stage does not fit shared memory)");
+        rc.variant = 5;
+    }
     if (elem_bytes_ == 2 && opt_.kernel_variant != 1 && rc.group_dms == 64 && nchans <= 16384) {
         const F32Geometry G = f32_geometry(rc.span, rc.group_dms, nchans, 0);
         if (G.smem_bytes > 0) {
@@ -173,23 +180,24 @@ bool DdtrPipeline::build_quad_tables(int r)
     const int ngroups = ndms / rc.group_dms;
     int *d_stats = nullptr;
     int32_t *d_qtmp = nullptr;
-    int hs[3] = {0, 0, 0};
+    int hs[4] = {0, 0, 0, 0};
     const size_t nq_ent = static_cast<size_t>(nquads) * ndms;
     if (!check_cuda(cudaMalloc(&rc.d_qpat, static_cast<size_t>(ngroups) * nquads * 16 * sizeof(int32_t)), "cudaMalloc") ||
         !check_cuda(cudaMalloc(&rc.d_qwin, static_cast<size_t>(ngroups) * nq_pad * sizeof(int32_t)), "cudaMalloc") ||
         !check_cuda(cudaMemsetAsync(rc.d_qwin, 0, static_cast<size_t>(ngroups) * nq_pad * sizeof(int32_t), st_), "memset") ||
         !check_cuda(cudaMalloc(&rc.d_qoff, nq_ent * sizeof(int32_t)), "cudaMalloc") ||
         !check_cuda(cudaMalloc(&d_qtmp, nq_ent * sizeof(int32_t)), "cudaMalloc") ||
-        !check_cuda(cudaMalloc(&d_stats, 3 * sizeof(int)), "cudaMalloc") ||
-        !check_cuda(cudaMemsetAsync(d_stats, 0, 3 * sizeof(int), st_), "memset"))
+        !check_cuda(cudaMalloc(&d_stats, 4 * sizeof(int)), "cudaMalloc") ||
+        !check_cuda(cudaMemsetAsync(d_stats, 0, 4 * sizeof(int), st_), "memset"))
         return false;
     bool ok = check_cuda(launch_quad_patterns(rc.d_table, rc.nch_used, ndms, rc.group_dms, nquads, nq_pad, rc.d_qpat,
                                               rc.d_qwin, d_qtmp, d_stats, st_),
                          "quad patterns") &&
-              check_cuda(cudaMemcpyAsync(hs, d_stats, 3 * sizeof(int), cudaMemcpyDeviceToHost, st_), "D2H") &&
+              check_cuda(cudaMemcpyAsync(hs, d_stats, 4 * sizeof(int), cudaMemcpyDeviceToHost, st_), "D2H") &&
               check_cuda(cudaStreamSynchronize(st_), "sync");
     ++launches_;
     if (ok) {
+        rc.quad_ws_ok = (hs[3] == 0);
         rc.quad_span = hs[0];
         rc.quad_dmax = hs[1];
         rc.quad_maxcnt = hs[2];
@@ -279,6 +287,21 @@ bool DdtrPipeline::build_sub_tables(int r)
                         " (patterns without an exact split, or its stage does not fit shared memory)");
     }
     return ok;
+}
+
+// The warp-specialised channel-quad kernel needs 512-sample tiles, a
+// pre-skewed row for every (quad, DM trial) and its stage in shared memory.
+bool DdtrPipeline::quad_ws_fits(const RangeConfig &rc) const
+{
+    if (!rc.has_quad || !rc.quad_ws_ok || rc.quad.M != 16)
+        return false;
+    QuadLaunch q{};
+    q.qs = rc.quad.qs;
+    q.raww = rc.quad.raww;
+    q.nq_pad = rc.quad.nq_pad;
+    q.npool = rc.quad.npool;
+    q.W = rc.quad.W;
+    return quadws_smem_bytes(q) <= kStagedSmemLimit;
 }
 
 bool DdtrPipeline::check_device_flags()
@@ -499,7 +522,7 @@ bool DdtrPipeline::tune_ranges()
     StageTuneCache cache;
     for (size_t r = 0; r < ranges_.size(); ++r) {
         RangeConfig &rc = ranges_[r];
-        if (rc.variant != 2 && rc.variant != 3)
+        if (rc.variant != 2 && rc.variant != 3 && rc.variant != 5)
             continue;
         const DdtrOp *op = nullptr;
         for (const DdtrOp &o : ops_)
@@ -517,7 +540,7 @@ bool DdtrPipeline::tune_ranges()
         std::string err;
         if (!tune_stage_depth(job, st_, device_, cache, err))
             return fail(err);
-        if (rc.variant == 2) {
+        if (rc.variant == 2 || rc.variant == 5) {
             rc.quad.qs = job.q.qs;
             rc.quad.npool = job.q.npool;
         } else {
@@ -526,14 +549,19 @@ bool DdtrPipeline::tune_ranges()
         if (rc.variant == 2 && rc.has_sub) {
             // the subband kernel against the tuned channel-quad kernel
             const float t_quad = time_job_slice(job, st_, device_, err);
+            if (t_quad < 0.f)
+                return fail(err);
             rc.variant = 4;
             DdtrJob js;
-            if (t_quad < 0.f || !make_job(*op, d_flat_[op->src_level & 1], flat_elems_, out, pitch, js))
-                return fail(err.empty() ? error_ : err);
+            const bool made = make_job(*op, d_flat_[op->src_level & 1], flat_elems_, out, pitch, js);
+            rc.variant = 2;
+            if (!made)
+                return false;
             const float t_sub = time_job_slice(js, st_, device_, err);
             if (t_sub < 0.f)
                 return fail(err);
-            rc.variant = (t_sub < t_quad) ? 4 : 2;
+            if (t_sub < t_quad)
+                rc.variant = 4;
         }
     }
     return check_cuda(cudaStreamSynchronize(st_), "sync");
@@ -636,14 +664,17 @@ bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, f
     job.variant = (elem_bytes_ == 1 && rc.variant == 2)   ? 2
                   : (elem_bytes_ == 2 && rc.variant == 3) ? 3
                   : (elem_bytes_ == 1 && rc.variant == 4) ? 4
+                  : (elem_bytes_ == 1 && rc.variant == 5) ? 5
                                                           : 1;
     job.elem_bytes = elem_bytes_;
     job.tile_words = rc.tile_words;
     job.offtab = rc.d_offtab;
-    const int tile = (job.variant == 2) ? 32 * rc.quad.M : ((job.variant == 3 || job.variant == 4) ? 512 : 128 * rc.tile_words);
+    const int tile = (job.variant == 2 || job.variant == 5)
+                         ? 32 * rc.quad.M
+                         : ((job.variant == 3 || job.variant == 4) ? 512 : 128 * rc.tile_words);
     const long long ntiles = (tp + tile - 1) / tile;
     long long need;
-    if (elem_bytes_ == 1 && job.variant == 2)
+    if (elem_bytes_ == 1 && (job.variant == 2 || job.variant == 5))
         need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ntiles * tile + rc.delay_max + 4LL * rc.quad.raww + 64;
     else if (job.variant == 4)
         need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ntiles * tile + rc.delay_max + 4LL * rc.sub.raww + 64;
@@ -678,7 +709,7 @@ bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, f
     if (job.variant == 1 && elem_bytes_ == 1 &&
         ((reinterpret_cast<uintptr_t>(p.out) & 15) || (p.out_pitch & 3) || (tp & 3)))
         return fail("output rows are not 16-byte aligned");
-    if (job.variant == 2) {
+    if (job.variant == 2 || job.variant == 5) {
         QuadLaunch &q = job.q;
         q.qpat = rc.d_qpat;
         q.qwin = rc.d_qwin;
@@ -719,6 +750,8 @@ cudaError_t launch_job(const DdtrJob &job, cudaStream_t st)
         return launch_ddtr_f32(job.p, job.f, st);
     if (job.variant == 4)
         return launch_ddtr_sub(job.p, job.s, st);
+    if (job.variant == 5)
+        return launch_ddtr_quadws(job.p, job.q, st);
     return (job.elem_bytes == 1) ? launch_ddtr_u8(job.p, job.offtab, job.tile_words, st) : launch_ddtr_u16(job.p, st);
 }
 

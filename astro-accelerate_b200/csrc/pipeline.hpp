@@ -41,7 +41,8 @@ struct PipelineOptions {
     size_t free_memory = 0;     // 0: query the device like aa_device_info::free_memory()
     int tile_words = 0;         // 0: autotune
     int kernel_variant = 0;     // 0: choose per range, 1: generic kernels, 2: channel-quad / fp32 kernels,
-                                // 3: subband / fp32 kernels
+                                // 3: subband / fp32 kernels, 4: warp-specialised channel-quad
+                                // / fp32 kernels
     int group_dms = 0;          // 0: autotune
     bool device_input = false;  // the input pointer is device memory ([t][c] uint16)
     bool device_output = false; // keep the whole output on the device ([range][dm][t])
@@ -69,7 +70,7 @@ struct DdtrOp {
 
 // A dedispersion launch, ready for a stream (launch_job) or a batch queue.
 struct DdtrJob {
-    int variant = 1; // 1 generic, 2 channel-quad, 3 staged fp32, 4 subband
+    int variant = 1; // 1 generic, 2 channel-quad, 3 staged fp32, 4 subband, 5 warp-specialised quad
     int elem_bytes = 1;
     int tile_words = 4;
     const int32_t *offtab = nullptr;
@@ -104,7 +105,8 @@ struct RangeConfig {
     // channel-quad kernel
     // 1: generic kernel (k_ddtr_u8 byte-phase / k_ddtr_u16 gather), 2: channel-quad
     // kernel (k_ddtr_quad, one-byte data), 3: staged fp32 kernel (k_ddtr_f32, two-byte data),
-    // 4: subband kernel (k_ddtr_sub, one-byte data)
+    // 4: subband kernel (k_ddtr_sub, one-byte data), 5: warp-specialised channel-quad
+    // kernel (k_ddtr_quadws, one-byte data)
     int variant = 1;
     QuadGeometry quad{};
     int quad_span = 0, quad_dmax = 0, quad_maxcnt = 0, nquads = 0;
@@ -116,6 +118,7 @@ struct RangeConfig {
     // subband kernel (variant 4); with the variant chosen per range both the
     // subband and the channel-quad tables may exist until the autotuner picks
     bool has_sub = false, has_quad = false;
+    bool quad_ws_ok = false; // no per-byte entries: the warp-specialised quad kernel may run it
     SubGeometry sub{};
     int nsub = 0;
     int32_t *d_sblk = nullptr;
@@ -178,6 +181,7 @@ private:
     bool check_cuda(cudaError_t e, const char *what);
     bool check_device_flags();
     bool build_range(int r);
+    bool quad_ws_fits(const RangeConfig &rc) const;
     bool build_quad_tables(int r);
     bool build_sub_tables(int r);
     bool tune_ranges();

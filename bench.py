@@ -61,7 +61,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--tile-words", type=int, default=0)
     ap.add_argument("--group-dms", type=int, default=0)
-    ap.add_argument("--variant", type=int, default=0, help="0 auto, 1 generic kernels, 2 staged kernels")
+    ap.add_argument("--variant", type=int, default=0,
+                    help="0 auto, 1 generic kernels, 2 channel-quad, 3 subband, 4 warp-specialised channel-quad "
+                         "(2-4 run the staged fp32 kernel on two-byte data)")
     ap.add_argument("--nbits", type=int, default=0, help="bit depth of the synthetic filterbank (default: the config's)")
     return ap.parse_args()
 
@@ -793,7 +795,7 @@ def main():
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     kernel_names = {"quad": "k_ddtr_quad", "phase": "k_ddtr_u8", "f32": "k_ddtr_f32", "gather": "k_ddtr_u16",
-                    "sub": "k_ddtr_sub"}
+                    "sub": "k_ddtr_sub", "quadws": "k_ddtr_quadws"}
     used = sorted({kernel_names[ri["kernel"]] for ri in ranges})
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": None, "kernel": "+".join(used),

@@ -232,11 +232,14 @@ const char *aa_b200_version(void);
 bool aa_b200_pipeline_set_options(void *obj, int stride_mode, int fma_mode, int failsafe, size_t free_memory,
                                   int tile_words, int group_dms);
 /* Dedispersion kernels, before bind: 0 chooses per range (for one-byte data
- * the subband kernel, else the channel-quad kernel, else the byte-phase
- * kernel; for two-byte data the staged fp32 kernel where it fits), 1 the
- * generic kernels (byte-phase for one-byte data, a global-memory gather for
- * two-byte data), 2 the channel-quad kernel for one-byte data, 3 the subband
- * kernel for one-byte data (2 and 3 run the staged fp32 kernel on two-byte
+ * the faster, timed at setup, of the channel-quad and subband kernels where
+ * they fit, else the byte-phase kernel; for two-byte data the staged fp32
+ * kernel where it fits), 1 the generic kernels
+ * (byte-phase for one-byte data, a global-memory gather for two-byte data),
+ * 2 the channel-quad kernel for one-byte data, 3 the subband kernel for
+ * one-byte data, 4 the warp-specialised channel-quad kernel for one-byte data
+ * (never chosen by 0: its four row-building warps cannot keep up with the
+ * sixteen summing warps) (2, 3 and 4 run the staged fp32 kernel on two-byte
  * data; refused where they do not fit).  All give identical results. */
 bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant);
 /* A pipeline whose input (and optionally output) stay in device memory:
@@ -252,8 +255,8 @@ bool aa_b200_pipeline_synchronize(void *obj);
 float *aa_b200_pipeline_device_output(void *obj, int range);
 /* kind (| 0x100 when the range runs the channel-quad kernel, | 0x200 for the
  * staged fp32 kernel, | 0x400 for the two-byte gather kernel, | 0x800 for the
- * subband kernel), DMs per thread block, window span (samples), time words
- * per lane */
+ * subband kernel, | 0x1000 for the warp-specialised channel-quad kernel), DMs
+ * per thread block, window span (samples), time words per lane */
 int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms, int *span, int *tile_words);
 /* channel quads (channel-quad kernel) or channels (fp32 kernel) per
  * shared-memory stage of a range, as the autotuner chose it; 0 for the
