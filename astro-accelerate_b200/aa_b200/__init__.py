@@ -49,6 +49,18 @@ class filterbank_metadata_struct(ctypes.Structure):
                 ("m_nchans", ctypes.c_int), ("m_src_raj", ctypes.c_double)]
 
 
+class sigproc_header_struct(ctypes.Structure):
+    """aa_b200_sigproc_header_struct (include/aa_b200.h)."""
+    _fields_ = [("telescope_id", ctypes.c_int), ("machine_id", ctypes.c_int), ("data_type", ctypes.c_int),
+                ("barycentric", ctypes.c_int), ("pulsarcentric", ctypes.c_int), ("az_start", ctypes.c_double),
+                ("za_start", ctypes.c_double), ("src_raj", ctypes.c_double), ("src_dej", ctypes.c_double),
+                ("tstart", ctypes.c_double), ("tsamp", ctypes.c_double), ("nbits", ctypes.c_int),
+                ("nsamples_keyword", ctypes.c_int), ("nchans", ctypes.c_int), ("nifs", ctypes.c_int),
+                ("fch1", ctypes.c_double), ("foff", ctypes.c_double), ("fchannel", ctypes.c_double),
+                ("refdm", ctypes.c_double), ("period", ctypes.c_double), ("data_start", ctypes.c_longlong),
+                ("data_bytes", ctypes.c_longlong), ("nsamp", ctypes.c_longlong)]
+
+
 class aa_py_pipeline_components(ctypes.Structure):
     """include/aa_py_pipeline_api.hpp:20-25."""
 
@@ -136,6 +148,17 @@ def lib():
         "aa_b200_pipeline_set_options": ([vp, i, i, i, sz, i, i], b),
         "aa_b200_pipeline_create": ([filterbank_metadata_struct, vp, i, i, i, vp, i], vp),
         "aa_b200_pipeline_set_kernel_variant": ([vp, i], b),
+        "aa_b200_pipeline_set_packed_input": ([vp, vp], b),
+        "aa_py_sigproc_input": ([ctypes.c_char_p], vp),
+        "aa_py_sigproc_input_del": ([vp], None),
+        "aa_py_sigproc_input_read_metadata": ([vp], filterbank_metadata_struct),
+        "aa_py_sigproc_input_read_signal": ([vp], b),
+        "aa_py_sigproc_input_input_buffer": ([vp], P(ctypes.c_ushort)),
+        "aa_b200_sigproc_read_packed": ([vp], b),
+        "aa_b200_sigproc_packed_buffer": ([vp], vp),
+        "aa_b200_sigproc_packed_bytes": ([vp], ll),
+        "aa_b200_sigproc_header": ([vp, P(sigproc_header_struct)], b),
+        "aa_b200_sigproc_last_error": ([vp], ctypes.c_char_p),
         "aa_b200_pipeline_run_all": ([vp], b),
         "aa_b200_pipeline_rewind": ([vp], b),
         "aa_b200_pipeline_synchronize": ([vp], b),
@@ -348,6 +371,19 @@ class aa_py_pipeline:
             raise ValueError(self.last_error())
         return ok
 
+    def set_packed_input(self, packed):
+        """Read the SIGPROC data section as stored instead of the unsigned-short
+        input (before bind): a uint8 array [nsamples][nchans*nbits/8] (a 16-bit
+        array for nbits 16 and 32), or a pointer (int)."""
+        if isinstance(packed, np.ndarray):
+            if not packed.flags["C_CONTIGUOUS"]:
+                raise ValueError("the packed input must be C-contiguous")
+            self._packed_keepalive = packed
+            packed = packed.ctypes.data
+        if not lib().aa_b200_pipeline_set_packed_input(self.m_obj, ctypes.c_void_p(packed)):
+            raise ValueError(self.last_error())
+        return True
+
     def set_kernel_variant(self, variant: int):
         """Kernel family per range (before bind): 0 auto (timed per range), 1
         generic kernels, 2 channel-quad / fp32, 3 subband / fp32, 4
@@ -420,6 +456,72 @@ class aa_py_pipeline:
             arr = np.ctypeslib.as_array((ctypes.c_float * (n * tot)).from_address(base)).reshape(n, tot)
             out.append(arr)
         return out
+
+
+class aa_py_sigproc_input:
+    """SIGPROC filterbank reader (the reference's aa_py_sigproc_input,
+    cmake/py_astro_accelerate.py.in:71-101): read_metadata, read_signal and
+    input_buffer as there, plus numpy views and the packed read."""
+
+    def __init__(self, path: str):
+        self.m_obj = lib().aa_py_sigproc_input(os.fsencode(path))
+        self._meta = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, exc_type, exc_value, traceback):
+        self.delete()
+
+    def delete(self):
+        if self.m_obj:
+            lib().aa_py_sigproc_input_del(self.m_obj)
+            self.m_obj = None
+
+    def read_metadata(self) -> filterbank_metadata_struct:
+        self._meta = lib().aa_py_sigproc_input_read_metadata(self.m_obj)
+        return self._meta
+
+    def read_signal(self) -> bool:
+        return bool(lib().aa_py_sigproc_input_read_signal(self.m_obj))
+
+    def input_buffer(self):
+        """ctypes pointer to [nsamples][nchans] unsigned short (as the reference)."""
+        return lib().aa_py_sigproc_input_input_buffer(self.m_obj)
+
+    def input_array(self) -> np.ndarray:
+        """input_buffer as a [nsamples][nchans] uint16 view (valid while this object lives)."""
+        m = self._meta
+        p = self.input_buffer()
+        if m is None or not p:
+            raise RuntimeError("read_metadata and read_signal first: " + self.last_error())
+        return np.ctypeslib.as_array(p, shape=(m.m_nsamples, m.m_nchans))
+
+    def read_packed(self) -> bool:
+        return bool(lib().aa_b200_sigproc_read_packed(self.m_obj))
+
+    def packed_array(self) -> np.ndarray:
+        """The data section as stored, [nsamples][record bytes] uint8 (16-bit
+        [nsamples][nchans] for nbits 16 and 32)."""
+        m = self._meta
+        n = lib().aa_b200_sigproc_packed_bytes(self.m_obj)
+        p = lib().aa_b200_sigproc_packed_buffer(self.m_obj)
+        if m is None or not p:
+            raise RuntimeError("read_metadata and read_packed first: " + self.last_error())
+        raw = np.ctypeslib.as_array((ctypes.c_uint8 * n).from_address(p))
+        if m.m_nbits >= 16:
+            return raw.view(np.uint16).reshape(m.m_nsamples, m.m_nchans)
+        return raw.reshape(m.m_nsamples, -1) if m.m_nsamples else raw.reshape(0, 0)
+
+    def header(self) -> dict:
+        h = sigproc_header_struct()
+        if not lib().aa_b200_sigproc_header(self.m_obj, ctypes.byref(h)):
+            raise RuntimeError(self.last_error())
+        return {k: getattr(h, k) for k, _ in h._fields_}
+
+    def last_error(self) -> str:
+        e = lib().aa_b200_sigproc_last_error(self.m_obj)
+        return e.decode() if e else ""
 
 
 def create_pipeline(metadata: filterbank_metadata_struct, input_ptr: int, device_input: bool,

@@ -29,6 +29,7 @@ struct Api {
     pipeline_component_option_struct options;
     FilterbankMetadata meta;
     const unsigned short *input = nullptr;
+    const void *packed = nullptr; // stored SIGPROC records (aa_b200_pipeline_set_packed_input)
     int card = 0;
     PipelineOptions popt;
     std::unique_ptr<DdtrPipeline> pipe;
@@ -147,7 +148,8 @@ bool aa_py_pipeline_api_bind_ddtr_plan(void *obj, const void *plan)
         return api_fail(a, "a DDTR plan is already bound");
     if (cudaSetDevice(a->card) != cudaSuccess)
         return api_fail(a, "cannot select CUDA device " + std::to_string(a->card));
-    a->pipe.reset(new DdtrPipeline(a->meta, a->input, a->popt));
+    a->pipe.reset(new DdtrPipeline(a->meta, a->popt.packed_input ? a->packed : static_cast<const void *>(a->input),
+                                   a->popt));
     if (!a->pipe->bind(*static_cast<const DdtrPlan *>(plan))) {
         api_fail(a, a->pipe->last_error());
         a->pipe.reset();
@@ -512,6 +514,18 @@ void *aa_b200_pipeline_create(aa_py_filterbank_metadata_struct metadata, const u
     a->popt.device_output = device_output != 0;
     a->popt.stream = static_cast<cudaStream_t>(stream);
     return a;
+}
+
+bool aa_b200_pipeline_set_packed_input(void *obj, const void *packed)
+{
+    Api *a = as_api(obj);
+    if (a->pipe)
+        return api_fail(a, "the packed input must be set before the plan is bound");
+    if (!packed)
+        return api_fail(a, "the packed input pointer is null");
+    a->packed = packed;
+    a->popt.packed_input = true;
+    return true;
 }
 
 bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant)

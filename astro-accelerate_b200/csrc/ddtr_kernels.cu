@@ -190,6 +190,57 @@ __global__ void __launch_bounds__(256) k_corner_turn(const uint16_t *__restrict_
         atomicOr(err, DERR_INPUT_RANGE);
 }
 
+// Sample c of one stored SIGPROC record: 4-bit high nibble first, 2-bit most
+// significant pair first, 1-bit least significant bit first.
+template <int NBITS>
+__device__ __forceinline__ uint16_t packed_sample(const uint8_t *__restrict__ rec, int c)
+{
+    if constexpr (NBITS == 16) {
+        return reinterpret_cast<const uint16_t *>(rec)[c];
+    } else if constexpr (NBITS == 8) {
+        return rec[c];
+    } else if constexpr (NBITS == 4) {
+        const unsigned b = rec[c >> 1];
+        return static_cast<uint16_t>((c & 1) ? (b & 15u) : (b >> 4));
+    } else if constexpr (NBITS == 2) {
+        const unsigned b = rec[c >> 2];
+        return static_cast<uint16_t>((b >> (6 - 2 * (c & 3))) & 3u);
+    } else {
+        const unsigned b = rec[c >> 3];
+        return static_cast<uint16_t>((b >> (c & 7)) & 1u);
+    }
+}
+
+// Unpack + corner turn in one pass: the H2D copy carries the stored bytes
+// (1/2, 1/4, 1/8 or 1/16 of the unsigned-short input) and the transpose
+// tile is filled from them.
+template <int NBITS, typename T>
+__global__ void __launch_bounds__(256) k_corner_turn_packed(const uint8_t *__restrict__ in, T *__restrict__ out,
+                                                            int nchans, long long nsamp, long long stride)
+{
+    __shared__ uint16_t tile[64][65];
+    const long long t0 = static_cast<long long>(blockIdx.x) * 64;
+    const int c0 = blockIdx.y * 64;
+    const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;
+    const long long rec = static_cast<long long>(nchans) * NBITS / 8;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int tt = ty + 4 * i;
+        const long long t = t0 + tt;
+        const int c = c0 + tx;
+        tile[tt][tx] = (t < nsamp && c < nchans) ? packed_sample<NBITS>(in + t * rec, c) : uint16_t(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int cc = ty + 4 * i;
+        const int c = c0 + cc;
+        const long long t = t0 + tx;
+        if (t < nsamp && c < nchans)
+            out[static_cast<long long>(c) * stride + t] = static_cast<T>(tile[tx][cc]);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Reference x2 binning as it acts on the flat buffer (bin + swap,
 // src/aa_device_binning_kernel.cu:33-45, src/aa_device_corner_turn_kernel.cu:91-98):
@@ -622,6 +673,40 @@ cudaError_t launch_corner_turn(const uint16_t *in_tc, void *out_ct, int elem_byt
     else
         k_corner_turn<uint16_t><<<grid, 256, 0, st>>>(in_tc, static_cast<uint16_t *>(out_ct), nchans, nsamp,
                                                       out_stride, max_value, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_corner_turn_packed(const uint8_t *in_rec, int nbits, void *out_ct, int nchans, long long nsamp,
+                                      long long out_stride, cudaStream_t st)
+{
+    if (nchans < 1 || nsamp < 0 || (static_cast<long long>(nchans) * nbits) % 8)
+        return cudaErrorInvalidValue;
+    if (nbits == 16 && (reinterpret_cast<uintptr_t>(in_rec) & 1))
+        return cudaErrorInvalidValue;
+    if (nsamp == 0)
+        return cudaSuccess;
+    dim3 grid(static_cast<unsigned>((nsamp + 63) / 64), (nchans + 63) / 64);
+    uint8_t *o8 = static_cast<uint8_t *>(out_ct);
+    switch (nbits) {
+    case 1:
+        k_corner_turn_packed<1, uint8_t><<<grid, 256, 0, st>>>(in_rec, o8, nchans, nsamp, out_stride);
+        break;
+    case 2:
+        k_corner_turn_packed<2, uint8_t><<<grid, 256, 0, st>>>(in_rec, o8, nchans, nsamp, out_stride);
+        break;
+    case 4:
+        k_corner_turn_packed<4, uint8_t><<<grid, 256, 0, st>>>(in_rec, o8, nchans, nsamp, out_stride);
+        break;
+    case 8:
+        k_corner_turn_packed<8, uint8_t><<<grid, 256, 0, st>>>(in_rec, o8, nchans, nsamp, out_stride);
+        break;
+    case 16:
+        k_corner_turn_packed<16, uint16_t><<<grid, 256, 0, st>>>(in_rec, static_cast<uint16_t *>(out_ct), nchans,
+                                                                  nsamp, out_stride);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

@@ -65,6 +65,13 @@ cudaError_t launch_offset_table(const int32_t *table, const int32_t *wmin, int n
 cudaError_t launch_corner_turn(const uint16_t *in_tc, void *out_ct, int elem_bytes, int nchans,
                                long long nsamp, long long out_stride, int max_value, int *err,
                                cudaStream_t st);
+// A chunk of the SIGPROC data section as stored, [t][nchans*nbits/8 bytes]
+// (nbits 1, 2, 4, 8; 16 for 16-bit records, also used for the 16-bit
+// rescaled samples of a 32-bit file) -> [c][stride], one byte per sample for
+// nbits <= 8, uint16 otherwise.  Channels inside a byte in the reference
+// reader's order (src/aa_sigproc_input.cpp:441-521).
+cudaError_t launch_corner_turn_packed(const uint8_t *in_rec, int nbits, void *out_ct, int nchans, long long nsamp,
+                                      long long out_stride, cudaStream_t st);
 
 // Reference x2 binning on the flat buffer (src/aa_bin_gpu.cpp:8-44), out of
 // place: for nchans and nsamp multiples of 32, dst[0, nchans*nsamp/2) = binned

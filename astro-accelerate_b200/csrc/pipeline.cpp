@@ -14,8 +14,8 @@ namespace {
 constexpr int kMaxSmemOptin = 227 * 1024;
 }
 
-DdtrPipeline::DdtrPipeline(const FilterbankMetadata &meta, const uint16_t *input, const PipelineOptions &opt)
-    : meta_(meta), input_(input), opt_(opt)
+DdtrPipeline::DdtrPipeline(const FilterbankMetadata &meta, const void *input, const PipelineOptions &opt)
+    : meta_(meta), input_(static_cast<const uint8_t *>(input)), opt_(opt)
 {
 }
 
@@ -388,6 +388,14 @@ bool DdtrPipeline::setup()
         meta_.nbits != 32)
         return fail("unsupported nbits");
     elem_bytes_ = (meta_.nbits <= 8) ? 1 : 2;
+    in_rec_bytes_ = 2LL * nchans;
+    if (opt_.packed_input) {
+        if ((static_cast<long long>(nchans) * meta_.nbits) % 8)
+            return fail("packed input needs nchans * nbits to be a multiple of 8");
+        in_rec_bytes_ = (meta_.nbits >= 16) ? 2LL * nchans : static_cast<long long>(nchans) * meta_.nbits / 8;
+        if (meta_.nbits >= 16 && (reinterpret_cast<uintptr_t>(input_) & 1))
+            return fail("16-bit packed input must be 2-byte aligned");
+    }
     if (!check_cuda(cudaGetDevice(&device_), "cudaGetDevice"))
         return false;
     for (int r = 0; r < nr; ++r) {
@@ -456,7 +464,7 @@ bool DdtrPipeline::setup()
     }
     if (!opt_.device_input) {
         for (int i = 0; i < 2; ++i)
-            if (!check_cuda(cudaMalloc(&d_raw_[i], static_cast<size_t>(L0) * nchans * sizeof(uint16_t)),
+            if (!check_cuda(cudaMalloc(&d_raw_[i], static_cast<size_t>(L0) * static_cast<size_t>(in_rec_bytes_)),
                             "cudaMalloc(raw chunk)"))
                 return false;
     }
@@ -762,10 +770,10 @@ bool DdtrPipeline::exec_corner_turn(const DdtrOp &op)
     const long long L = op.len;
     if (static_cast<size_t>(nchans) * static_cast<size_t>(L) > flat_elems_)
         return fail("chunk larger than the filterbank buffer");
-    const uint16_t *src;
+    const uint8_t *src;
     const int slot = k & 1;
     if (opt_.device_input) {
-        src = input_ + static_cast<size_t>(op.inc) * nchans;
+        src = input_ + static_cast<size_t>(op.inc) * static_cast<size_t>(in_rec_bytes_);
     } else {
         // issue this chunk's copy if it was not prefetched, and prefetch the next
         auto issue = [&](int kk, long long inc_kk) -> bool {
@@ -773,8 +781,8 @@ bool DdtrPipeline::exec_corner_turn(const DdtrOp &op)
             const int s = kk & 1;
             if (!check_cuda(cudaStreamWaitEvent(st_h2d_, ev_raw_free_[s], 0), "wait"))
                 return false;
-            if (!check_cuda(cudaMemcpyAsync(d_raw_[s], input_ + static_cast<size_t>(inc_kk) * nchans,
-                                            static_cast<size_t>(Lk) * nchans * sizeof(uint16_t),
+            if (!check_cuda(cudaMemcpyAsync(d_raw_[s], input_ + static_cast<size_t>(inc_kk) * in_rec_bytes_,
+                                            static_cast<size_t>(Lk) * static_cast<size_t>(in_rec_bytes_),
                                             cudaMemcpyHostToDevice, st_h2d_),
                             "H2D chunk"))
                 return false;
@@ -792,11 +800,15 @@ bool DdtrPipeline::exec_corner_turn(const DdtrOp &op)
         src = d_raw_[slot];
     }
     const int max_value = (meta_.nbits == 4) ? 15 : (meta_.nbits <= 8 ? 255 : 65535);
-    if (!timed_launch_begin(KF_CORNER_TURN) ||
-        !check_cuda(launch_corner_turn(src, d_flat_[op.dst_level & 1], elem_bytes_, nchans, L, L, max_value, d_err_,
-                                       st_),
-                    "corner turn") ||
-        !timed_launch_end())
+    if (!timed_launch_begin(KF_CORNER_TURN))
+        return false;
+    const cudaError_t ce =
+        opt_.packed_input
+            ? launch_corner_turn_packed(src, meta_.nbits >= 16 ? 16 : meta_.nbits, d_flat_[op.dst_level & 1], nchans,
+                                        L, L, st_)
+            : launch_corner_turn(reinterpret_cast<const uint16_t *>(src), d_flat_[op.dst_level & 1], elem_bytes_,
+                                 nchans, L, L, max_value, d_err_, st_);
+    if (!check_cuda(ce, "corner turn") || !timed_launch_end())
         return false;
     ++launches_;
     if (!opt_.device_input && !check_cuda(cudaEventRecord(ev_raw_free_[slot], st_), "event"))

@@ -45,6 +45,10 @@ struct PipelineOptions {
                                 // / fp32 kernels
     int group_dms = 0;          // 0: autotune
     bool device_input = false;  // the input pointer is device memory ([t][c] uint16)
+    // the input holds the SIGPROC data section as stored ([t][nchans*nbits/8]
+    // bytes; 16-bit samples for nbits 16, and the reader's 16-bit rescaled
+    // samples for nbits 32) instead of one uint16 per sample
+    bool packed_input = false;
     bool device_output = false; // keep the whole output on the device ([range][dm][t])
     bool time_kernels = false;  // CUDA events around every kernel launch
     bool external_buffers = false; // no filterbank/raw/tile buffers: the caller runs the ops (batch engine)
@@ -128,7 +132,8 @@ struct RangeConfig {
 
 class DdtrPipeline {
 public:
-    DdtrPipeline(const FilterbankMetadata &meta, const uint16_t *input, const PipelineOptions &opt);
+    // input: [t][c] uint16, or the stored records with opt.packed_input
+    DdtrPipeline(const FilterbankMetadata &meta, const void *input, const PipelineOptions &opt);
     ~DdtrPipeline();
     DdtrPipeline(const DdtrPipeline &) = delete;
     DdtrPipeline &operator=(const DdtrPipeline &) = delete;
@@ -196,7 +201,8 @@ private:
     bool collect_kernel_times();
 
     FilterbankMetadata meta_;
-    const uint16_t *input_;
+    const uint8_t *input_;
+    long long in_rec_bytes_ = 0; // bytes of one input time sample (all channels)
     PipelineOptions opt_;
     DdtrPlan plan_;
     DdtrStrategy strategy_;
@@ -214,7 +220,7 @@ private:
     int elem_bytes_ = 1;
     size_t flat_elems_ = 0;           // elements per flat buffer incl. padding
     void *d_flat_[2] = {nullptr, nullptr};
-    uint16_t *d_raw_[2] = {nullptr, nullptr};
+    uint8_t *d_raw_[2] = {nullptr, nullptr}; // staged H2D chunks, in_rec_bytes_ per time sample
     float *d_dmshifts_ = nullptr;
     int *d_err_ = nullptr;
     int *h_err_ = nullptr;            // pinned

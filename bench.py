@@ -770,6 +770,44 @@ def main():
         x_host = xh.numpy().view(np.uint16)
         api.cleanUp()
         api.delete()
+        # the same run fed the samples as a SIGPROC file stores them
+        # (aa_b200_pipeline_set_packed_input): nbits/16 of the H2D bytes
+        if cfg["nbits"] <= 8:
+            from aa_b200.sigproc import pack
+            if cfg["nbits"] == 8:
+                xp = torch.empty((xh.shape[0], xh.shape[1]), dtype=torch.uint8, pin_memory=True)
+                xp.copy_(xh.to(torch.uint8))
+            else:
+                xp = torch.from_numpy(pack(x_host, cfg["nbits"])).pin_memory()
+            api = aa.aa_py_pipeline(comps, opts, md, None, local)
+            api.set_packed_input(xp.data_ptr())
+            if not api.bind_ddtr_plan(plan):
+                raise RuntimeError(api.last_error())
+            walls = []
+            for step in range(1 + args.e2e_steps):
+                torch.cuda.synchronize(device)
+                barrier()
+                t0 = time.perf_counter()
+                api.rewind()
+                while api.run():
+                    pass
+                if api.status_code() == aa.STATUS_ERROR:
+                    raise RuntimeError(api.last_error())
+                torch.cuda.synchronize(device)
+                walls.append(time.perf_counter() - t0)
+            wall = statistics.median(walls[1:])
+            if world > 1:
+                t = torch.tensor([wall], device=device)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                wall = float(t.item())
+            e2e["packed_input"] = {
+                "value": units * world / wall, "unit": "DM-trial*samples/s", "ms_per_step": wall * 1e3,
+                "h2d_bytes_per_step": sum((strat["t_processed"][0][k] + strat["maxshift"]) * cfg["nchans"] *
+                                          cfg["nbits"] // 8 for k in range(strat["num_tchunks"])),
+                "d2h_bytes_per_step": units * 4, "api": "aa_b200_pipeline_set_packed_input"}
+            api.cleanUp()
+            api.delete()
+            del xp
     else:
         x_host = x[:min(131040, strat["t_processed"][0][0]) + strat["maxshift"]].cpu().numpy().view(np.uint16)
     plan.delete()

@@ -224,6 +224,41 @@ long long aa_b200_kernel_launches(void);
 /* Library build identification. */
 const char *aa_b200_version(void);
 
+/* ---------------------------------------------------------------------------
+ * SIGPROC filterbank input (src/aa_py_sigproc_input.cpp:7-33, reader
+ * src/aa_sigproc_input.cpp:85-543): the reference's header keyword rules,
+ * sample count from the file size and unpacking into one unsigned short per
+ * sample ([t][c]; 4-bit high nibble first, 2-bit most significant pair first,
+ * 1-bit least significant bit first; 32-bit rescaled by the file's min/max).
+ * Files whose channels do not fill whole bytes, or with nifs != 1, are
+ * refused (read_metadata returns nbits = 0; the reason is in
+ * aa_b200_sigproc_last_error).
+ * ------------------------------------------------------------------------- */
+void *aa_py_sigproc_input(const char *path);
+void aa_py_sigproc_input_del(const void *obj);
+aa_py_filterbank_metadata_struct aa_py_sigproc_input_read_metadata(void *obj);
+/* true once, after the samples were read and unpacked */
+bool aa_py_sigproc_input_read_signal(void *obj);
+/* [nsamples][nchans] unsigned short owned by obj; null before read_signal */
+const unsigned short *aa_py_sigproc_input_input_buffer(const void *obj);
+
+/* Extensions (no reference counterpart): the data section as stored, for
+ * aa_b200_pipeline_set_packed_input; for 32-bit files the 16-bit rescaled
+ * samples of read_signal.  True once, after a successful read. */
+bool aa_b200_sigproc_read_packed(void *obj);
+const void *aa_b200_sigproc_packed_buffer(const void *obj);
+long long aa_b200_sigproc_packed_bytes(const void *obj);
+typedef struct {
+    int telescope_id, machine_id, data_type, barycentric, pulsarcentric;
+    double az_start, za_start, src_raj, src_dej, tstart, tsamp;
+    int nbits, nsamples_keyword, nchans, nifs;
+    double fch1, foff, fchannel, refdm, period;
+    long long data_start, data_bytes, nsamp; /* byte offset and size of the data; samples per channel */
+} aa_b200_sigproc_header_struct;
+/* every header value read (false before a successful read_metadata) */
+bool aa_b200_sigproc_header(const void *obj, aa_b200_sigproc_header_struct *out);
+const char *aa_b200_sigproc_last_error(const void *obj);
+
 /* Pipeline extensions (obj from aa_py_pipeline_api or aa_b200_pipeline_create). */
 /* Options, before bind: stride_mode 0 = the reference runner's binning length
  * (bit-exact with the reference), 1 = true row stride; fma_mode bit mask of
@@ -241,6 +276,15 @@ bool aa_b200_pipeline_set_options(void *obj, int stride_mode, int fma_mode, int 
  * (never chosen by 0: its four row-building warps cannot keep up with the
  * sixteen summing warps) (2, 3 and 4 run the staged fp32 kernel on two-byte
  * data; refused where they do not fit).  All give identical results. */
+/* Before bind: the pipeline reads `packed` (host memory, or device memory
+ * for a pipeline created with device_input) instead of the unsigned-short
+ * input: the SIGPROC data section as stored, [nsamples][nchans*nbits/8]
+ * bytes for nbits 1, 2, 4, 8, [nsamples][nchans] uint16 for nbits 16, and for
+ * nbits 32 the 16-bit rescaled samples (aa_b200_sigproc_read_packed).  Each
+ * chunk crosses PCIe at nbits/16 of the unsigned-short size (1/2 for 8-bit)
+ * and is unpacked on the GPU in the corner-turn kernel; outputs are
+ * identical to the unsigned-short input of the same samples. */
+bool aa_b200_pipeline_set_packed_input(void *obj, const void *packed);
 bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant);
 /* A pipeline whose input (and optionally output) stay in device memory:
  * input [nsamples][nchans] uint16 on the device when device_input != 0;

@@ -14,6 +14,9 @@
  *                     copies output_buffer() into a flat array.  Needs a GPU.
  *                     The reference's aa_device_info destructor resets the
  *                     device, so call this from a process of its own.
+ *   aaref_sigproc_read() reads a SIGPROC file with the reference's
+ *                     aa_sigproc_input (src/aa_sigproc_input.cpp:85-543):
+ *                     metadata and the unsigned-short input buffer.  No GPU.
  */
 #include <chrono>
 #include <stdio.h>
@@ -31,6 +34,7 @@
 #include "aa_filterbank_metadata.hpp"
 #include "aa_permitted_pipelines_generic.hpp"
 #include "aa_pipeline.hpp"
+#include "aa_sigproc_input.hpp"
 
 using namespace astroaccelerate;
 
@@ -212,6 +216,31 @@ int aaref_time_ddtr(const unsigned short *input_tc, int nchans, int nsamp, doubl
         *seconds = std::chrono::duration<double>(t1 - t0).count();
     }
     return 0;
+}
+
+/* meta: tstart, tsamp, fch1, foff; imeta: nbits, nsamples, nchans, nifs.
+ * buf (capacity cap elements) receives input_buffer() when read_signal
+ * succeeds.  Returns the number of elements of input_buffer(), or -1 when
+ * read_signal refused. */
+long long aaref_sigproc_read(const char *path, double *meta, int *imeta, unsigned short *buf, long long cap)
+{
+    aa_sigproc_input in(path);
+    aa_filterbank_metadata m = in.read_metadata();
+    meta[0] = m.tstart();
+    meta[1] = m.tsamp();
+    meta[2] = m.fch1();
+    meta[3] = m.foff();
+    imeta[0] = m.nbits();
+    imeta[1] = m.nsamples();
+    imeta[2] = m.nchans();
+    imeta[3] = m.nifs();
+    if (!in.read_signal())
+        return -1;
+    const std::vector<unsigned short> &b = in.input_buffer();
+    const long long n = (long long)b.size();
+    if (buf && n <= cap)
+        memcpy(buf, b.data(), (size_t)n * sizeof(unsigned short));
+    return n;
 }
 
 } // extern "C"
