@@ -149,6 +149,9 @@ def lib():
         "aa_b200_pipeline_create": ([filterbank_metadata_struct, vp, i, i, i, vp, i], vp),
         "aa_b200_pipeline_set_kernel_variant": ([vp, i], b),
         "aa_b200_pipeline_set_packed_input": ([vp, vp], b),
+        "aa_b200_pipeline_set_export_base": ([vp, ctypes.c_char_p], b),
+        "aa_b200_export_dd_data": ([i, PPPFLOAT, sz, P(i), P(i), ctypes.c_char_p, P(i), i], i),
+        "aa_b200_sd_per_file_from_file_size": ([sz, sz, sz], sz),
         "aa_py_sigproc_input": ([ctypes.c_char_p], vp),
         "aa_py_sigproc_input_del": ([vp], None),
         "aa_py_sigproc_input_read_metadata": ([vp], filterbank_metadata_struct),
@@ -381,6 +384,12 @@ class aa_py_pipeline:
             self._packed_keepalive = packed
             packed = packed.ctypes.data
         if not lib().aa_b200_pipeline_set_packed_input(self.m_obj, ctypes.c_void_p(packed)):
+            raise ValueError(self.last_error())
+        return True
+
+    def set_export_base(self, base: str):
+        """Base name of the output_dmt files (default "DD_data" in the working directory)."""
+        if not lib().aa_b200_pipeline_set_export_base(self.m_obj, os.fsencode(base)):
             raise ValueError(self.last_error())
         return True
 

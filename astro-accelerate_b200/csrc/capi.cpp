@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include "ddtr_kernels.cuh"
+#include "export.hpp"
 #include "pipeline.hpp"
 #include "planner.hpp"
 
@@ -35,7 +36,10 @@ struct Api {
     std::unique_ptr<DdtrPipeline> pipe;
     std::string error;
     bool supported = true;
+    std::string export_base = "DD_data"; // output_dmt files (the reference's base name)
+    bool exported = false;
 };
+
 
 FilterbankMetadata to_meta(const aa_py_filterbank_metadata_struct &m)
 {
@@ -61,6 +65,34 @@ bool api_fail(Api *a, const std::string &m)
 }
 
 int elem_bytes_for(int nbits) { return nbits <= 8 ? 1 : 2; }
+
+// output_dmt: the DM-time output of every range in the reference's
+// Export_DD_data files, DM rows per file for 1000 MB files
+// (include/aa_permitted_pipelines_1.hpp:312-323 with
+// include/aa_pipeline_runner.hpp:165-223).
+bool export_outputs(Api *a)
+{
+    DdtrPipeline &P = *a->pipe;
+    const DdtrStrategy &s = P.strategy();
+    float ***rows = P.output_buffer();
+    if (!rows)
+        return api_fail(a, "output_dmt needs copy_ddtr_data_to_host");
+    const int nr = static_cast<int>(s.nranges());
+    const size_t inc = s.nProcessedTimesamples();
+    std::vector<int> in_bin(nr), all(nr, 1);
+    for (int r = 0; r < nr; ++r) {
+        in_bin[r] = s.dm(r).inBin;
+        if (inc / static_cast<size_t>(in_bin[r]) > static_cast<size_t>(s.total_samps(r)))
+            return api_fail(a, "output_dmt: range " + std::to_string(r) + " holds fewer samples than inc/inBin");
+    }
+    std::string err;
+    const size_t per_file = sd_per_file_from_file_size(1000, inc, 1);
+    if (!export_dd_data(nr, rows, inc, s.ndms_data(), in_bin.data(), a->export_base, all.data(),
+                        static_cast<int>(per_file), err))
+        return api_fail(a, "output_dmt: " + err);
+    a->exported = true;
+    return true;
+}
 
 } // namespace
 
@@ -130,9 +162,9 @@ void *aa_py_pipeline_api(pipeline_components_struct pipeline, pipeline_component
         api_fail(a, "only the dedispersion component is implemented by this library");
     }
     if (options.zero_dm || options.zero_dm_with_outliers || options.input_DDTR_normalization ||
-        options.output_DDTR_normalization || options.set_bandpass_average || options.old_rfi || options.output_dmt) {
+        options.output_DDTR_normalization || options.set_bandpass_average || options.old_rfi) {
         a->supported = false;
-        api_fail(a, "pre/post-processing options (zero DM, normalisation, RFI, output_dmt) are not implemented");
+        api_fail(a, "pre/post-processing options (zero DM, normalisation, RFI) are not implemented");
     }
     return a;
 }
@@ -220,6 +252,13 @@ bool aa_py_pipeline_api_run(void *obj, int *status_code)
     *status_code = static_cast<int>(st);
     if (st == RunStatus::error) {
         api_fail(a, a->pipe->last_error());
+        return false;
+    }
+    if (!more && st == RunStatus::finished && a->options.output_dmt && !a->exported &&
+        (!a->pipe->synchronize() || !export_outputs(a))) {
+        if (a->error.empty())
+            api_fail(a, a->pipe->last_error());
+        *status_code = static_cast<int>(RunStatus::error);
         return false;
     }
     return more;
@@ -547,13 +586,49 @@ bool aa_b200_pipeline_run_all(void *obj)
         return api_fail(a, "no DDTR plan bound");
     if (!a->pipe->run_all())
         return api_fail(a, a->pipe->last_error());
+    if (a->options.output_dmt) {
+        if (!a->pipe->synchronize())
+            return api_fail(a, a->pipe->last_error());
+        return export_outputs(a);
+    }
     return true;
 }
 
 bool aa_b200_pipeline_rewind(void *obj)
 {
     Api *a = as_api(obj);
+    a->exported = false;
     return a->pipe ? a->pipe->rewind() : api_fail(a, "no DDTR plan bound");
+}
+
+bool aa_b200_pipeline_set_export_base(void *obj, const char *base)
+{
+    Api *a = as_api(obj);
+    if (!base || !*base)
+        return api_fail(a, "empty export base name");
+    a->export_base = base;
+    return true;
+}
+
+int aa_b200_export_dd_data(int range, float ***dedispersed_data, size_t max_nTimesamples, const int *ndms,
+                           const int *inBin, const char *base_filename, const int *ranges_to_export, int DMs_per_file)
+{
+    std::string err;
+    if (!dedispersed_data || !ndms || !inBin || !base_filename || !ranges_to_export) {
+        set_error("aa_b200_export_dd_data: null argument");
+        return 1;
+    }
+    if (!export_dd_data(range, dedispersed_data, max_nTimesamples, ndms, inBin, base_filename, ranges_to_export,
+                        DMs_per_file, err)) {
+        set_error(err);
+        return 1;
+    }
+    return 0;
+}
+
+size_t aa_b200_sd_per_file_from_file_size(size_t size_in_MB, size_t primary_dimension, size_t floats_per_element)
+{
+    return sd_per_file_from_file_size(size_in_MB, primary_dimension, floats_per_element);
 }
 
 bool aa_b200_pipeline_synchronize(void *obj)

@@ -286,6 +286,24 @@ bool aa_b200_pipeline_set_options(void *obj, int stride_mode, int fma_mode, int 
  * identical to the unsigned-short input of the same samples. */
 bool aa_b200_pipeline_set_packed_input(void *obj, const void *packed);
 bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant);
+/* output_dmt (pipeline_component_option_struct): when the run finishes, the
+ * DM-time output of every range is written in the reference's
+ * Export_DD_data files (include/aa_pipeline_runner.hpp:165-216), DM rows per
+ * file for 1000 MB files as include/aa_permitted_pipelines_1.hpp:312-323
+ * computes them; needs copy_ddtr_data_to_host.  Base name "DD_data" in the
+ * working directory, or this one: */
+bool aa_b200_pipeline_set_export_base(void *obj, const char *base);
+/* include/aa_pipeline_runner.hpp:165-216 Export_DD_data: per range r with
+ * ranges_to_export[r] != 0, <base>_<r>.txt (nTimesamples, nDMs,
+ * DMs_per_file, number of files; one per line) and <base>_<r>_<i>.dat
+ * (float32 [DMs][nTimesamples]), nTimesamples = max_nTimesamples/inBin[r];
+ * DMs_per_file < 0: all of a range's DM trials in one file (the first
+ * exported range's count, kept for later ranges as there).  Every row must
+ * hold nTimesamples values.  0 on success, 1 on error (aa_b200_last_error). */
+int aa_b200_export_dd_data(int range, float ***dedispersed_data, size_t max_nTimesamples, const int *ndms,
+                           const int *inBin, const char *base_filename, const int *ranges_to_export, int DMs_per_file);
+/* include/aa_pipeline_runner.hpp:219-223 Calculate_sd_per_file_from_file_size */
+size_t aa_b200_sd_per_file_from_file_size(size_t size_in_MB, size_t primary_dimension, size_t floats_per_element);
 /* A pipeline whose input (and optionally output) stay in device memory:
  * input [nsamples][nchans] uint16 on the device when device_input != 0;
  * device_output != 0 keeps [range][dm][t] on the device

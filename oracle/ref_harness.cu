@@ -14,6 +14,9 @@
  *                     copies output_buffer() into a flat array.  Needs a GPU.
  *                     The reference's aa_device_info destructor resets the
  *                     device, so call this from a process of its own.
+ *   aaref_export_dd_data() writes DM-time files with the reference's
+ *                     Export_DD_data (include/aa_pipeline_runner.hpp:165-216)
+ *                     through a runner that only exposes it.  No GPU.
  *   aaref_sigproc_read() reads a SIGPROC file with the reference's
  *                     aa_sigproc_input (src/aa_sigproc_input.cpp:85-543):
  *                     metadata and the unsigned-short input buffer.  No GPU.
@@ -216,6 +219,31 @@ int aaref_time_ddtr(const unsigned short *input_tc, int nchans, int nsamp, doubl
         *seconds = std::chrono::duration<double>(t1 - t0).count();
     }
     return 0;
+}
+
+namespace {
+struct export_runner : public aa_pipeline_runner {
+    bool setup() override { return true; }
+    void run(int range, float ***data, size_t max_nt, int *ndms, int *inBin, const char *base, int *ranges,
+             int per_file)
+    {
+        Export_DD_data(range, data, max_nt, ndms, inBin, std::string(base), ranges, per_file);
+    }
+    size_t per_file(size_t mb, size_t primary, size_t floats) { return Calculate_sd_per_file_from_file_size(mb, primary, floats); }
+};
+} // namespace
+
+void aaref_export_dd_data(int range, float ***data, size_t max_nt, int *ndms, int *inBin, const char *base,
+                          int *ranges_to_export, int DMs_per_file)
+{
+    export_runner e;
+    e.run(range, data, max_nt, ndms, inBin, base, ranges_to_export, DMs_per_file);
+}
+
+size_t aaref_sd_per_file(size_t mb, size_t primary, size_t floats)
+{
+    export_runner e;
+    return e.per_file(mb, primary, floats);
 }
 
 /* meta: tstart, tsamp, fch1, foff; imeta: nbits, nsamples, nchans, nifs.

@@ -122,3 +122,43 @@ def test_packed_input_set_after_bind_is_refused(aa, cuda_device, tmp_path):
     pipe.delete()
     p.delete()
     r.delete()
+
+
+def test_output_dmt_writes_export_files(aa, cuda_device, tmp_path):
+    """output_dmt: when the run finishes, every range's output is written in
+    the reference's Export_DD_data files (include/aa_pipeline_runner.hpp:165-216)
+    with the DM rows per file of include/aa_permitted_pipelines_1.hpp:312-323."""
+    import os
+
+    import dmt_oracle as O
+
+    case = C.CASES["shared8_binned"]
+    x = C.make_input(case)
+    md = aa.filterbank_metadata_struct(0.0, case["tsamp"], case["fch1"], case["foff"], case["nbits"], case["nsamp"],
+                                       case["nchans"], 0.0)
+    comps = aa.aa_py_pipeline_components(True, False, False, False)
+    o = aa.aa_py_pipeline_component_options()
+    o.copy_ddtr_data_to_host = True
+    o.output_dmt = True
+    pipe = aa.aa_py_pipeline(comps, o, md, np.ascontiguousarray(x.reshape(-1)), 0)
+    pipe.set_export_base(str(tmp_path / "lib" / "DD_data"))
+    os.makedirs(tmp_path / "lib")
+    plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in case["plan"]])
+    assert pipe.bind_ddtr_plan(plan), pipe.last_error()
+    while pipe.run():
+        pass
+    assert pipe.status_code() == aa.STATUS_FINISHED, pipe.last_error()
+    outs = [a.copy() for a in pipe.output_arrays()]
+    inc = aa.lib().aa_py_total_computed_samples(pipe.m_obj)
+    ndms = [a.shape[0] for a in outs]
+    in_bin = [p[3] for p in case["plan"]]
+    os.makedirs(tmp_path / "oracle")
+    want = O.export(outs, inc, ndms, in_bin, str(tmp_path / "oracle" / "DD_data"), [1] * len(outs),
+                    O.sd_per_file(1000, inc, 1))
+    for w in want:
+        g = tmp_path / "lib" / os.path.basename(w)
+        assert g.read_bytes() == open(w, "rb").read(), os.path.basename(w)
+    assert sorted(os.listdir(tmp_path / "lib")) == sorted(os.path.basename(w) for w in want)
+    pipe.cleanUp()
+    pipe.delete()
+    plan.delete()
