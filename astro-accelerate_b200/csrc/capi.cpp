@@ -161,11 +161,13 @@ void *aa_py_pipeline_api(pipeline_components_struct pipeline, pipeline_component
         a->supported = false;
         api_fail(a, "only the dedispersion component is implemented by this library");
     }
-    if (options.zero_dm || options.zero_dm_with_outliers || options.input_DDTR_normalization ||
-        options.output_DDTR_normalization || options.set_bandpass_average || options.old_rfi) {
-        a->supported = false;
-        api_fail(a, "pre/post-processing options (zero DM, normalisation, RFI) are not implemented");
-    }
+    // include/aa_py_pipeline_api.cpp:24-35 -> the runner's options
+    a->popt.zero_dm = options.zero_dm;
+    a->popt.zero_dm_outliers = options.zero_dm_with_outliers;
+    a->popt.input_norm = options.input_DDTR_normalization;
+    a->popt.output_norm = options.output_DDTR_normalization;
+    a->popt.old_rfi = options.old_rfi;
+    a->popt.bandpass_average = options.set_bandpass_average;
     return a;
 }
 

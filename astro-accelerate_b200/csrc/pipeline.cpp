@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "autotune.hpp"
+#include "preproc.cuh"
 #include "ddtr_kernels.cuh"
 
 namespace aab200 {
@@ -304,6 +305,53 @@ bool DdtrPipeline::quad_ws_fits(const RangeConfig &rc) const
     return quadws_smem_bytes(q) <= kStagedSmemLimit;
 }
 
+// Optional processing of the reference runner: the bandpass normalisation
+// of zero DM (the plan's, else (2^nbits - 1)/2 per channel,
+// src/aa_ddtr_strategy.cpp:48-60; with set_bandpass_average the block means
+// of include/aa_permitted_pipelines_generic.hpp:533-552) and a writable
+// unsigned-short chunk where the input is not one.
+bool DdtrPipeline::setup_processing(long long L0)
+{
+    const int nchans = meta_.nchans;
+    const bool pre_in = opt_.zero_dm || opt_.zero_dm_outliers || opt_.input_norm;
+    if ((pre_in || opt_.old_rfi || opt_.output_norm) && opt_.external_buffers)
+        return fail("input/output processing options are not available to the batch engine");
+    if (!pre_in)
+        return true;
+    if (meta_.nbits != 4 && meta_.nbits != 8 && meta_.nbits != 16)
+        return fail("zero DM and input normalisation need 4, 8 or 16-bit samples");
+    if (plan_.bandpass().size() == static_cast<size_t>(nchans))
+        bandpass_ = plan_.bandpass();
+    else
+        bandpass_.assign(nchans, static_cast<float>(((1 << meta_.nbits) - 1.0) / 2.0));
+    if (opt_.bandpass_average && (opt_.zero_dm || opt_.zero_dm_outliers)) {
+        // src/aa_host_cpu_msd.cpp:5-35 with (nchans, nsamples) over the [t][c]
+        // input: value c is the mean of elements [c*nsamples, (c+1)*nsamples)
+        if (opt_.device_input || opt_.packed_input)
+            return fail("set_bandpass_average needs the unsigned-short input in host memory");
+        const uint16_t *in = reinterpret_cast<const uint16_t *>(input_);
+        const size_t ns = static_cast<size_t>(meta_.nsamples);
+        for (int c = 0; c < nchans; ++c) {
+            double sum = 0.0;
+            size_t n = 0;
+            for (size_t j = 0; j < ns; ++j) {
+                sum += in[static_cast<size_t>(c) * ns + j];
+                n += 1;
+            }
+            bandpass_[c] = static_cast<float>(sum / n);
+        }
+    }
+    if (!check_cuda(cudaMalloc(&d_norm_, nchans * sizeof(float)), "cudaMalloc(bandpass)") ||
+        !check_cuda(cudaMemcpyAsync(d_norm_, bandpass_.data(), nchans * sizeof(float), cudaMemcpyHostToDevice, st_),
+                    "H2D bandpass") ||
+        !check_cuda(cudaStreamSynchronize(st_), "sync"))
+        return false;
+    if ((opt_.device_input || opt_.packed_input) &&
+        !check_cuda(cudaMalloc(&d_stage_, static_cast<size_t>(L0) * nchans * sizeof(uint16_t)), "cudaMalloc(stage)"))
+        return false;
+    return true;
+}
+
 bool DdtrPipeline::check_device_flags()
 {
     if (!check_cuda(cudaMemcpyAsync(h_err_, d_err_, sizeof(int), cudaMemcpyDeviceToHost, st_), "D2H flags") ||
@@ -468,6 +516,8 @@ bool DdtrPipeline::setup()
                             "cudaMalloc(raw chunk)"))
                 return false;
     }
+    if (!setup_processing(L0))
+        return false;
 
     // outputs
     if (opt_.device_output) {
@@ -800,16 +850,57 @@ bool DdtrPipeline::exec_corner_turn(const DdtrOp &op)
         src = d_raw_[slot];
     }
     const int max_value = (meta_.nbits == 4) ? 15 : (meta_.nbits <= 8 ? 255 : 65535);
+    const bool pre_in = opt_.zero_dm || opt_.zero_dm_outliers || opt_.input_norm;
+    bool packed_src = opt_.packed_input;
+    if (pre_in) {
+        // include/aa_permitted_pipelines_generic.hpp:704-737: zero DM (or with
+        // outliers), then input normalisation, on the [t][c] chunk
+        uint16_t *w = reinterpret_cast<uint16_t *>(const_cast<uint8_t *>(src));
+        if (opt_.packed_input) {
+            w = d_stage_;
+            if (!check_cuda(launch_unpack_records(src, meta_.nbits, nchans, L, w, st_), "unpack"))
+                return false;
+            ++launches_;
+        } else if (opt_.device_input) {
+            w = d_stage_;
+            if (!check_cuda(cudaMemcpyAsync(w, src, static_cast<size_t>(L) * nchans * sizeof(uint16_t),
+                                            cudaMemcpyDeviceToDevice, st_),
+                            "D2D chunk"))
+                return false;
+        }
+        if (opt_.zero_dm) {
+            if (!check_cuda(launch_zero_dm(w, nchans, L, meta_.nbits, d_norm_, st_), "zero DM"))
+                return false;
+            ++launches_;
+        } else if (opt_.zero_dm_outliers) {
+            if (!check_cuda(launch_zero_dm_outliers(w, nchans, L, meta_.nbits, d_norm_, st_), "zero DM (outliers)"))
+                return false;
+            ++launches_;
+        }
+        if (opt_.input_norm) {
+            if (!check_cuda(launch_input_normalization(w, nchans, L, meta_.nbits, st_), "input normalisation"))
+                return false;
+            ++launches_;
+        }
+        src = reinterpret_cast<const uint8_t *>(w);
+        packed_src = false;
+    }
     if (!timed_launch_begin(KF_CORNER_TURN))
         return false;
     const cudaError_t ce =
-        opt_.packed_input
+        packed_src
             ? launch_corner_turn_packed(src, meta_.nbits >= 16 ? 16 : meta_.nbits, d_flat_[op.dst_level & 1], nchans,
                                         L, L, st_)
             : launch_corner_turn(reinterpret_cast<const uint16_t *>(src), d_flat_[op.dst_level & 1], elem_bytes_,
                                  nchans, L, L, max_value, d_err_, st_);
     if (!check_cuda(ce, "corner turn") || !timed_launch_end())
         return false;
+    if (opt_.old_rfi) {
+        // :741-757, on the corner-turned chunk
+        if (!check_cuda(launch_old_rfi(d_flat_[op.dst_level & 1], elem_bytes_, nchans, L, st_), "old RFI"))
+            return false;
+        ++launches_;
+    }
     ++launches_;
     if (!opt_.device_input && !check_cuda(cudaEventRecord(ev_raw_free_[slot], st_), "event"))
         return false;
@@ -853,6 +944,12 @@ bool DdtrPipeline::exec_ddtr(const DdtrOp &op)
     if (!timed_launch_begin(KF_DDTR) || !check_cuda(launch_job(job, st_), "dedispersion") || !timed_launch_end())
         return false;
     ++launches_;
+    if (opt_.output_norm) {
+        // include/aa_permitted_pipelines_generic.hpp:821-831
+        if (!check_cuda(launch_output_normalization(out, pitch, op.tp, job.p.ndms, st_), "output normalisation"))
+            return false;
+        ++launches_;
+    }
 
     if (opt_.copy_to_host) {
         // src/aa_device_save_data.cu:19-62: row dm of this chunk lands at
@@ -977,6 +1074,10 @@ bool DdtrPipeline::cleanup()
         rc.d_sblk = rc.d_swin = rc.d_soff = nullptr;
     }
     ranges_.clear();
+    cudaFree(d_stage_);
+    cudaFree(d_norm_);
+    d_stage_ = nullptr;
+    d_norm_ = nullptr;
     for (int i = 0; i < 2; ++i) {
         cudaFree(d_flat_[i]);
         cudaFree(d_raw_[i]);

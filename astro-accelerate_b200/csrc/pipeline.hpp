@@ -53,6 +53,13 @@ struct PipelineOptions {
     bool time_kernels = false;  // CUDA events around every kernel launch
     bool external_buffers = false; // no filterbank/raw/tile buffers: the caller runs the ops (batch engine)
     bool autotune = true;          // time the staged kernels' stage depth per range at setup
+    // the reference runner's optional processing (aa_pipeline::component_option)
+    bool zero_dm = false;          // zero_dm
+    bool zero_dm_outliers = false; // zero_dm_with_outliers (zero_dm takes precedence)
+    bool input_norm = false;       // input_DDTR_normalization
+    bool output_norm = false;      // output_DDTR_normalization
+    bool old_rfi = false;          // old_rfi
+    bool bandpass_average = false; // set_bandpass_average
     cudaStream_t stream = nullptr;
 };
 
@@ -186,6 +193,7 @@ private:
     bool check_cuda(cudaError_t e, const char *what);
     bool check_device_flags();
     bool build_range(int r);
+    bool setup_processing(long long L0);
     bool quad_ws_fits(const RangeConfig &rc) const;
     bool build_quad_tables(int r);
     bool build_sub_tables(int r);
@@ -221,6 +229,9 @@ private:
     size_t flat_elems_ = 0;           // elements per flat buffer incl. padding
     void *d_flat_[2] = {nullptr, nullptr};
     uint8_t *d_raw_[2] = {nullptr, nullptr}; // staged H2D chunks, in_rec_bytes_ per time sample
+    uint16_t *d_stage_ = nullptr;             // writable [t][c] chunk for input processing of device or packed input
+    float *d_norm_ = nullptr;                 // bandpass normalisation [nchans] (zero DM)
+    std::vector<float> bandpass_;             // its host copy
     float *d_dmshifts_ = nullptr;
     int *d_err_ = nullptr;
     int *h_err_ = nullptr;            // pinned

@@ -105,19 +105,24 @@ int aaref_strategy(const harness_dm *plan, int nranges, float power, int nchans,
 
 /* free_memory == 0 uses the device's own free memory, like the reference's
  * pipeline API (include/aa_pipeline_api.hpp:149); a smaller value forces
- * time chunking on small inputs. */
-int aaref_run_ddtr(const unsigned short *input_tc, int nchans, int nsamp,
-                   double tsamp, double fch1, double foff, int nbits,
-                   const harness_dm *plan, int nranges, size_t free_memory,
-                   int max_chunks, float *dmshifts, int *ndms,
-                   harness_dm *str_dm, int *maxshift, int *max_ndms,
-                   int *num_tchunks, int *t_processed, float *out,
-                   size_t out_len)
+ * time chunking on small inputs.  options: bit 0 zero_dm, 1
+ * zero_dm_with_outliers, 2 input_DDTR_normalization, 3
+ * output_DDTR_normalization, 4 old_rfi, 5 set_bandpass_average; bandpass
+ * (bandpass_size values, may be 0) is bound to the plan. */
+int aaref_run_ddtr_opts(const unsigned short *input_tc, int nchans, int nsamp,
+                        double tsamp, double fch1, double foff, int nbits,
+                        const harness_dm *plan, int nranges, size_t free_memory,
+                        int max_chunks, float *dmshifts, int *ndms,
+                        harness_dm *str_dm, int *maxshift, int *max_ndms,
+                        int *num_tchunks, int *t_processed, float *out,
+                        size_t out_len, int options, const float *bandpass, int bandpass_size)
 {
     aa_device_info dev(0);
     aa_ddtr_plan p;
     for (int i = 0; i < nranges; i++)
         p.add_dm(plan[i].low, plan[i].high, plan[i].step, plan[i].inBin, plan[i].outBin);
+    if (bandpass && bandpass_size > 0)
+        p.bind_bandpass_normalization(bandpass, bandpass_size);
     aa_filterbank_metadata meta(0.0, tsamp, nbits, nsamp, fch1, foff, nchans);
     size_t dev_free = dev.free_memory();
     size_t fm = free_memory ? free_memory : dev_free;
@@ -138,6 +143,18 @@ int aaref_run_ddtr(const unsigned short *input_tc, int nchans, int nsamp,
         comps.insert(aa_pipeline::component::dedispersion);
         aa_pipeline::pipeline_option opts;
         opts.insert(aa_pipeline::component_option::copy_ddtr_data_to_host);
+        if (options & 1)
+            opts.insert(aa_pipeline::component_option::zero_dm);
+        if (options & 2)
+            opts.insert(aa_pipeline::component_option::zero_dm_with_outliers);
+        if (options & 4)
+            opts.insert(aa_pipeline::component_option::input_DDTR_normalization);
+        if (options & 8)
+            opts.insert(aa_pipeline::component_option::output_DDTR_normalization);
+        if (options & 16)
+            opts.insert(aa_pipeline::component_option::old_rfi);
+        if (options & 32)
+            opts.insert(aa_pipeline::component_option::set_bandpass_average);
         aa_analysis_strategy an;
         aa_periodicity_strategy per;
         aa_fdas_strategy fd;
@@ -168,6 +185,19 @@ int aaref_run_ddtr(const unsigned short *input_tc, int nchans, int nsamp,
         }
     }
     return 0;
+}
+
+int aaref_run_ddtr(const unsigned short *input_tc, int nchans, int nsamp,
+                   double tsamp, double fch1, double foff, int nbits,
+                   const harness_dm *plan, int nranges, size_t free_memory,
+                   int max_chunks, float *dmshifts, int *ndms,
+                   harness_dm *str_dm, int *maxshift, int *max_ndms,
+                   int *num_tchunks, int *t_processed, float *out,
+                   size_t out_len)
+{
+    return aaref_run_ddtr_opts(input_tc, nchans, nsamp, tsamp, fch1, foff, nbits, plan, nranges, free_memory,
+                               max_chunks, dmshifts, ndms, str_dm, maxshift, max_ndms, num_tchunks, t_processed,
+                               out, out_len, 0, nullptr, 0);
 }
 
 /* Times the reference's pipeline runner over the whole input: setup outside

@@ -29,6 +29,8 @@ def load():
     L.aaref_run_ddtr.argtypes = [ctypes.c_void_p, i, i, d, d, d, i, P(DM), i, sz, i, P(f), P(i), P(DM), P(i),
                                  P(i), P(i), P(i), ctypes.c_void_p, sz]
     L.aaref_run_ddtr.restype = i
+    L.aaref_run_ddtr_opts.argtypes = L.aaref_run_ddtr.argtypes + [i, ctypes.c_void_p, i]
+    L.aaref_run_ddtr_opts.restype = i
     return L
 
 
@@ -69,8 +71,10 @@ def strategy(L, plan, nchans, nsamp, fch1, foff, tsamp, nbits, free_memory, powe
 
 
 def run_ddtr(L, input_tc, plan, nchans, nsamp, fch1, foff, tsamp, nbits, free_memory, max_chunks=4096,
-             out_len=None):
-    """Runs the reference pipeline on the GPU; returns (strategy, flat output)."""
+             out_len=None, options=0, bandpass=None):
+    """Runs the reference pipeline on the GPU; returns (strategy, flat output).
+    options: bit mask of the runner's processing options (oracle/ref_harness.cu
+    aaref_run_ddtr_opts); bandpass: float32 values bound to the plan."""
     nr = len(plan)
     sh = np.zeros(nchans, np.float32)
     nd, sdm = (ctypes.c_int * nr)(), (DM * nr)()
@@ -80,10 +84,12 @@ def run_ddtr(L, input_tc, plan, nchans, nsamp, fch1, foff, tsamp, nbits, free_me
         out_len = 1 << 28
     out = np.zeros(out_len, np.float32)
     x = np.ascontiguousarray(input_tc, dtype=np.uint16)
-    rc = L.aaref_run_ddtr(x.ctypes.data, nchans, nsamp, tsamp, fch1, foff, nbits, _plan(plan), nr, free_memory,
-                          max_chunks, sh.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), nd, sdm, ctypes.byref(ms),
-                          ctypes.byref(mx), ctypes.byref(nt), tp.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                          out.ctypes.data, out_len)
+    bp = None if bandpass is None else np.ascontiguousarray(bandpass, dtype=np.float32)
+    rc = L.aaref_run_ddtr_opts(x.ctypes.data, nchans, nsamp, tsamp, fch1, foff, nbits, _plan(plan), nr, free_memory,
+                               max_chunks, sh.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), nd, sdm,
+                               ctypes.byref(ms), ctypes.byref(mx), ctypes.byref(nt),
+                               tp.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), out.ctypes.data, out_len, options,
+                               None if bp is None else bp.ctypes.data, 0 if bp is None else bp.size)
     if rc != 0:
         raise RuntimeError(f"reference pipeline failed (code {rc})")
     s = _unpack(nr, nchans, sh, nd, sdm, ms, mx, nt, tp, max_chunks)
