@@ -152,6 +152,160 @@ __global__ void __launch_bounds__(FT) k_frac_adj_dm_sum(const double *__restrict
         gdm[b] = static_cast<float>(red[0]);
 }
 
+// ---------------------------------------------------------------------------
+// Vector forms for T % 4 == 0 (rows of whole float4s): a thread takes four
+// consecutive samples.  The window x[c][t+n .. t+n+4] of its four outputs
+// lies in the float4s k = floor((t+n)/4) and k+1; since t is a multiple of
+// 4, the offset o = (t+n) mod 4 is the same for every thread of the channel,
+// so picking the five values is a branch-free uniform choice.  A float4 is
+// either wholly inside [0, T) or wholly outside (read as 0), matching the
+// per-sample bounds of the scalar kernels.
+// ---------------------------------------------------------------------------
+constexpr int F4T = 256;       // threads of the forward block
+constexpr int F4_TILE = 4 * F4T; // outputs per forward block
+
+__device__ __forceinline__ void window5(const float4 *__restrict__ row, int i, int T4, float (&v)[5])
+{
+    const int k = i >> 2; // floor division (arithmetic shift)
+    const int o = i & 3;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 p = (k >= 0 && k < T4) ? __ldg(row + k) : z;
+    const float4 q = (k + 1 >= 0 && k + 1 < T4) ? __ldg(row + k + 1) : z;
+    const float e[8] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w};
+    switch (o) {
+    case 0:
+#pragma unroll
+        for (int j = 0; j < 5; ++j)
+            v[j] = e[j];
+        break;
+    case 1:
+#pragma unroll
+        for (int j = 0; j < 5; ++j)
+            v[j] = e[j + 1];
+        break;
+    case 2:
+#pragma unroll
+        for (int j = 0; j < 5; ++j)
+            v[j] = e[j + 2];
+        break;
+    default:
+#pragma unroll
+        for (int j = 0; j < 5; ++j)
+            v[j] = e[j + 3];
+        break;
+    }
+}
+
+// y[b][t..t+3], channels in order with the scalar kernel's expression, so
+// the sums are the same bits.
+__global__ void __launch_bounds__(F4T) k_frac_fwd4(const float *__restrict__ x, const float *__restrict__ dm,
+                                                   const double *__restrict__ kc, const int *__restrict__ base, int C,
+                                                   int T, double *__restrict__ y)
+{
+    extern __shared__ double s_w[]; // w[C] then n[C]
+    int *s_n = reinterpret_cast<int *>(s_w + C);
+    const int b = blockIdx.y;
+    const float d = dm[b];
+    for (int c = threadIdx.x; c < C; c += blockDim.x)
+        delay_of(d, kc[c], base_of(base, b, C, c), s_n[c], s_w[c]);
+    __syncthreads();
+    const int t = blockIdx.x * F4_TILE + 4 * threadIdx.x;
+    if (t >= T)
+        return;
+    const int T4 = T >> 2;
+    const float4 *xb = reinterpret_cast<const float4 *>(x) + static_cast<size_t>(b) * C * T4;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+    for (int c = 0; c < C; ++c) {
+        float v[5];
+        window5(xb + static_cast<size_t>(c) * T4, t + s_n[c], T4, v);
+        const double w = s_w[c];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double a0 = v[j];
+            const double a1 = v[j + 1];
+            acc[j] += fma(w, a1 - a0, a0);
+        }
+    }
+    double2 *yo = reinterpret_cast<double2 *>(y + static_cast<size_t>(b) * T + t);
+    yo[0] = make_double2(acc[0], acc[1]);
+    yo[1] = make_double2(acc[2], acc[3]);
+}
+
+// Both adjoints of a group of channels of one snippet in one pass: the
+// output gradient gy[b] is staged in shared memory once per block; per
+// channel the input gradient row is written and the x row is read once for
+// the DM gradient's partial sum.
+constexpr int FA_THREADS = 512;
+constexpr int FA_CPB = 16; // channels per block
+
+__global__ void __launch_bounds__(FA_THREADS) k_frac_adj_rows(const float *__restrict__ x,
+                                                               const double *__restrict__ gy,
+                                                               const float *__restrict__ dm,
+                                                               const double *__restrict__ kc,
+                                                               const int *__restrict__ base, int C, int T,
+                                                               float *__restrict__ gx, double *__restrict__ partial)
+{
+    extern __shared__ double g[]; // gy[b][0..T), then [FA_CPB][FA_THREADS/32] warp sums
+    double *red = g + T;
+    const int b = blockIdx.y;
+    const int T4 = T >> 2;
+    const double2 *gsrc = reinterpret_cast<const double2 *>(gy + static_cast<size_t>(b) * T);
+    for (int i = threadIdx.x; i < (T >> 1); i += FA_THREADS)
+        reinterpret_cast<double2 *>(g)[i] = gsrc[i];
+    __syncthreads();
+    auto gat = [&](int i) -> double { return (i >= 0 && i < T) ? g[i] : 0.0; };
+    const float d = dm[b];
+    const int c_end = min(C, (blockIdx.x + 1) * FA_CPB);
+    for (int c = blockIdx.x * FA_CPB; c < c_end; ++c) {
+        int n;
+        double w;
+        delay_of(d, kc[c], base_of(base, b, C, c), n, w);
+        const float4 *xrow = reinterpret_cast<const float4 *>(x) + (static_cast<size_t>(b) * C + c) * T4;
+        float4 *gxrow = gx ? reinterpret_cast<float4 *>(gx) + (static_cast<size_t>(b) * C + c) * T4 : nullptr;
+        double acc = 0.0;
+#pragma unroll 4
+        for (int t = 4 * threadIdx.x; t < T; t += 4 * FA_THREADS) {
+            if (gxrow) {
+                // gx[j] = (1 - w) gy[j - n] + w gy[j - n - 1]
+                double gv[5];
+#pragma unroll
+                for (int k = 0; k < 5; ++k)
+                    gv[k] = gat(t - n - 1 + k);
+                float4 o;
+                o.x = static_cast<float>((1.0 - w) * gv[1] + w * gv[0]);
+                o.y = static_cast<float>((1.0 - w) * gv[2] + w * gv[1]);
+                o.z = static_cast<float>((1.0 - w) * gv[3] + w * gv[2]);
+                o.w = static_cast<float>((1.0 - w) * gv[4] + w * gv[3]);
+                gxrow[t >> 2] = o;
+            }
+            if (partial) {
+                float v[5];
+                window5(xrow, t + n, T4, v);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    acc += g[t + j] * (static_cast<double>(v[j + 1]) - static_cast<double>(v[j]));
+            }
+        }
+        if (partial) {
+            for (int o = 16; o > 0; o >>= 1)
+                acc += __shfl_down_sync(0xffffffffu, acc, o);
+            if ((threadIdx.x & 31) == 0)
+                red[(c - blockIdx.x * FA_CPB) * (FA_THREADS / 32) + (threadIdx.x >> 5)] = acc;
+        }
+    }
+    if (partial) {
+        __syncthreads();
+        const int c = blockIdx.x * FA_CPB + threadIdx.x;
+        if (threadIdx.x < FA_CPB && c < c_end) {
+            double s = 0.0;
+            for (int k = 0; k < FA_THREADS / 32; ++k)
+                s += red[threadIdx.x * (FA_THREADS / 32) + k];
+            partial[static_cast<size_t>(b) * C + c] = kc[c] * s;
+        }
+    }
+}
+
 // snr[b][i][t]; the block stages y[t0, t0 + FT + wmax - 1) (mu beyond T).
 __global__ void __launch_bounds__(FT) k_boxcar_fwd(const double *__restrict__ y, int T, BoxcarWidths W,
                                                    const float *__restrict__ mu, const float *__restrict__ sigma,
@@ -227,6 +381,16 @@ cudaError_t launch_frac_fwd(const float *x, const float *dm, const double *kc, c
         if (e != cudaSuccess)
             return e;
     }
+    if ((T & 3) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0 && (reinterpret_cast<uintptr_t>(y) & 15) == 0) {
+        if (smem > 48 * 1024) {
+            const cudaError_t e = cudaFuncSetAttribute(k_frac_fwd4, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       static_cast<int>(smem));
+            if (e != cudaSuccess)
+                return e;
+        }
+        k_frac_fwd4<<<dim3((T + F4_TILE - 1) / F4_TILE, B), F4T, smem, st>>>(x, dm, kc, base, C, T, y);
+        return cudaGetLastError();
+    }
     dim3 grid((T + FT - 1) / FT, B);
     k_frac_fwd<<<grid, FT, smem, st>>>(x, dm, kc, base, C, T, y);
     return cudaGetLastError();
@@ -237,6 +401,21 @@ cudaError_t launch_frac_adj(const float *x, const float *dm, const double *kc, c
 {
     if (B <= 0 || C <= 0 || T <= 0 || B > 65535 || C > 65535)
         return cudaErrorInvalidValue;
+    if (gdm && !partial)
+        return cudaErrorInvalidValue;
+    const size_t rows_smem = (static_cast<size_t>(T) + FA_CPB * (FA_THREADS / 32)) * sizeof(double);
+    if ((T & 3) == 0 && rows_smem <= 200 * 1024 && (reinterpret_cast<uintptr_t>(x) & 15) == 0 &&
+        (reinterpret_cast<uintptr_t>(gy) & 15) == 0 && (reinterpret_cast<uintptr_t>(gx) & 15) == 0 && (gx || gdm)) {
+        cudaError_t e = cudaFuncSetAttribute(k_frac_adj_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(rows_smem));
+        if (e != cudaSuccess)
+            return e;
+        k_frac_adj_rows<<<dim3((C + FA_CPB - 1) / FA_CPB, B), FA_THREADS, rows_smem, st>>>(
+            x, gy, dm, kc, base, C, T, gx, gdm ? partial : nullptr);
+        if (gdm)
+            k_frac_adj_dm_sum<<<B, FT, 0, st>>>(partial, C, gdm);
+        return cudaGetLastError();
+    }
     if (gx) {
         dim3 grid((T + FT - 1) / FT, C, B);
         k_frac_adj_x<<<grid, FT, 0, st>>>(gy, dm, kc, base, C, T, gx);
