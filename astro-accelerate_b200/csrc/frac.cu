@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(F4T) k_frac_fwd4(const float *__restrict__ x, 
 // Both adjoints of a group of channels of one snippet in one pass: the
 // output gradient gy[b] is staged in shared memory once per block; per
 // channel the input gradient row is written and the x row is read once for
-// the DM gradient's partial sum.
+// the DM gradient's partial sum.  Needs T % 4 == 0.
 constexpr int FA_THREADS = 512;
 constexpr int FA_CPB = 16; // channels per block
 
@@ -249,7 +249,6 @@ __global__ void __launch_bounds__(FA_THREADS) k_frac_adj_rows(const float *__res
     extern __shared__ double g[]; // gy[b][0..T), then [FA_CPB][FA_THREADS/32] warp sums
     double *red = g + T;
     const int b = blockIdx.y;
-    const int T4 = T >> 2;
     const double2 *gsrc = reinterpret_cast<const double2 *>(gy + static_cast<size_t>(b) * T);
     for (int i = threadIdx.x; i < (T >> 1); i += FA_THREADS)
         reinterpret_cast<double2 *>(g)[i] = gsrc[i];
@@ -261,30 +260,30 @@ __global__ void __launch_bounds__(FA_THREADS) k_frac_adj_rows(const float *__res
         int n;
         double w;
         delay_of(d, kc[c], base_of(base, b, C, c), n, w);
-        const float4 *xrow = reinterpret_cast<const float4 *>(x) + (static_cast<size_t>(b) * C + c) * T4;
-        float4 *gxrow = gx ? reinterpret_cast<float4 *>(gx) + (static_cast<size_t>(b) * C + c) * T4 : nullptr;
-        double acc = 0.0;
+        // input gradient: one sample per lane and step, so that the staged
+        // gradient is read and the gx row written warp-contiguously
+        if (gx) {
+            float *gr = gx + (static_cast<size_t>(b) * C + c) * T;
 #pragma unroll 4
-        for (int t = 4 * threadIdx.x; t < T; t += 4 * FA_THREADS) {
-            if (gxrow) {
-                // gx[j] = (1 - w) gy[j - n] + w gy[j - n - 1]
-                double gv[5];
-#pragma unroll
-                for (int k = 0; k < 5; ++k)
-                    gv[k] = gat(t - n - 1 + k);
-                float4 o;
-                o.x = static_cast<float>((1.0 - w) * gv[1] + w * gv[0]);
-                o.y = static_cast<float>((1.0 - w) * gv[2] + w * gv[1]);
-                o.z = static_cast<float>((1.0 - w) * gv[3] + w * gv[2]);
-                o.w = static_cast<float>((1.0 - w) * gv[4] + w * gv[3]);
-                gxrow[t >> 2] = o;
-            }
-            if (partial) {
+            for (int t = threadIdx.x; t < T; t += FA_THREADS) // gx[j] = (1 - w) gy[j - n] + w gy[j - n - 1]
+                gr[t] = static_cast<float>((1.0 - w) * gat(t - n) + w * gat(t - n - 1));
+        }
+        // DM gradient: four samples per lane from two aligned float4s of the
+        // x row (T % 4 == 0), the gradient in aligned pairs
+        double acc = 0.0;
+        if (partial) {
+            const int T4 = T >> 2;
+            const float4 *xrow = reinterpret_cast<const float4 *>(x) + (static_cast<size_t>(b) * C + c) * T4;
+#pragma unroll 4
+            for (int t = 4 * threadIdx.x; t < T; t += 4 * FA_THREADS) {
                 float v[5];
                 window5(xrow, t + n, T4, v);
+                const double2 g01 = *reinterpret_cast<const double2 *>(g + t);
+                const double2 g23 = *reinterpret_cast<const double2 *>(g + t + 2);
+                const double gt[4] = {g01.x, g01.y, g23.x, g23.y};
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
-                    acc += g[t + j] * (static_cast<double>(v[j + 1]) - static_cast<double>(v[j]));
+                    acc += gt[j] * (static_cast<double>(v[j + 1]) - static_cast<double>(v[j]));
             }
         }
         if (partial) {
