@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="survey", choices=["survey", "mid", "small", "batched", "refine", "e2e"])
     ap.add_argument("--beams", type=int, default=48, help="beams of the multi-beam draw (batched config)")
+    ap.add_argument("--snippets", type=int, default=256, help="snippets per step (refine config)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -572,7 +573,7 @@ def run_refine(args, rank, world, local):
     import frac_oracle as F
 
     torch.cuda.set_device(local)
-    S, C, T = 256, 1024, 8192
+    S, C, T = args.snippets, 1024, 8192
     x, dm_true, dm_trial, kc = R.synth_snippets(S, nchans=C, nsamp=T, seed=4 + rank)
     widths = R.DEFAULT_WIDTHS
     mu = torch.zeros(S, device="cuda")
@@ -639,7 +640,7 @@ def run_refine(args, rank, world, local):
     line = {"metric": "snippets/s (refinement step: forward + adjoint to input and DM)", "value": S / (stp / 1e3),
             "unit": "snippets/s", "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": stp,
             "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "refinement: 256 snippets x 1024 ch x 8192 samples f32, widths 1..64"},
+            "config": {"workload": f"refinement: {S} snippets x 1024 ch x 8192 samples f32, widths 1..64"},
             "kernels": {"frac_fwd_ms": fwd, "frac_adj_ms": adj,
                         "frac_fwd_gbs": bytes_x / fwd / 1e6, "frac_adj_gbs": 2 * bytes_x / adj / 1e6},
             "roofline": {"bound": "hbm", "kernel": "k_frac_fwd", "achieved": bytes_x / fwd / 1e6, "peak": hbm,
