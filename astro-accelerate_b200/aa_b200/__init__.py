@@ -149,6 +149,9 @@ def lib():
         "aa_b200_pipeline_create": ([filterbank_metadata_struct, vp, i, i, i, vp, i], vp),
         "aa_b200_pipeline_set_kernel_variant": ([vp, i], b),
         "aa_b200_pipeline_set_packed_input": ([vp, vp], b),
+        "aa_b200_selftest_bounded_wait": ([i, P(i)], i),
+        "aa_b200_debug_fail_after": ([ll], None),
+        "aa_b200_debug_fail_countdown": ([], ll),
         "aa_b200_pipeline_set_export_base": ([vp, ctypes.c_char_p], b),
         "aa_b200_export_dd_data": ([i, PPPFLOAT, sz, P(i), P(i), ctypes.c_char_p, P(i), i], i),
         "aa_b200_sd_per_file_from_file_size": ([sz, sz, sz], sz),

@@ -5,6 +5,7 @@
 #include <cstdio>
 
 #include "autotune.hpp"
+#include "fault.hpp"
 #include "ddtr_kernels.cuh"
 
 namespace aab200 {
@@ -22,9 +23,9 @@ bool BatchDdtr::fail(const std::string &msg)
 
 bool BatchDdtr::check_cuda(cudaError_t e, const char *what)
 {
-    if (e == cudaSuccess)
+    if (e == cudaSuccess && !injected_failure_now())
         return true;
-    return fail(std::string(what) + ": " + cudaGetErrorString(e));
+    return fail(std::string(what) + ": " + (e == cudaSuccess ? "injected failure" : cudaGetErrorString(e)));
 }
 
 int BatchDdtr::add_beam(const FilterbankMetadata &meta, const DdtrPlan &plan, const uint16_t *d_input)

@@ -47,13 +47,19 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity)
     return done != 0;
 }
 
-// Bounded wait (about a second at the try_wait suspend time); false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
+// Wait of at most `limit` polls; false when the phase did not complete.
+__device__ __forceinline__ bool mbar_wait_limit(unsigned bar, unsigned parity, int limit)
 {
-    for (int i = 0; i < (1 << 22); ++i)
+    for (int i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity))
             return true;
     return false;
+}
+
+// Bounded wait (about a second at the try_wait suspend time); false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
+{
+    return mbar_wait_limit(bar, parity, 1 << 22);
 }
 
 // Orders earlier generic-proxy accesses of shared memory before later

@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "autotune.hpp"
+#include "fault.hpp"
 #include "preproc.cuh"
 #include "ddtr_kernels.cuh"
 
@@ -31,9 +32,9 @@ bool DdtrPipeline::fail(const std::string &msg)
 
 bool DdtrPipeline::check_cuda(cudaError_t e, const char *what)
 {
-    if (e == cudaSuccess)
+    if (e == cudaSuccess && !injected_failure_now())
         return true;
-    return fail(std::string(what) + ": " + cudaGetErrorString(e));
+    return fail(std::string(what) + ": " + (e == cudaSuccess ? "injected failure" : cudaGetErrorString(e)));
 }
 
 bool DdtrPipeline::bind(const DdtrPlan &plan)

@@ -225,6 +225,20 @@ long long aa_b200_kernel_launches(void);
 const char *aa_b200_version(void);
 
 /* ---------------------------------------------------------------------------
+ * Failure handling checks (no reference counterpart; they fault nothing).
+ * ------------------------------------------------------------------------- */
+/* Runs a kernel whose bounded mbarrier wait is made to run out (an expected
+ * arrival never comes) after `limit` polls (1..2^22); *status receives the
+ * device error flags (8 = the wait ran out, as the staged kernels report an
+ * overdue copy).  Returns 0 when the kernel ran and the flags were read. */
+int aa_b200_selftest_bounded_wait(int limit, int *status);
+/* Host-side failure injection: the n-th CUDA result checked by any pipeline
+ * or batch engine after this call reads as a failure ("injected failure" in
+ * the error message); n <= 0 disarms.  For tests of the error paths. */
+void aa_b200_debug_fail_after(long long n);
+long long aa_b200_debug_fail_countdown(void);
+
+/* ---------------------------------------------------------------------------
  * SIGPROC filterbank input (src/aa_py_sigproc_input.cpp:7-33, reader
  * src/aa_sigproc_input.cpp:85-543): the reference's header keyword rules,
  * sample count from the file size and unpacking into one unsigned short per

@@ -58,3 +58,12 @@ def test_strategy_refusal_codes(aa):
         aa.strategy([(0, 3000, 1.0, 1, 1)], 4096, 1 << 12, 1670.0, -0.0732421875, 64e-6, 8)  # maxshift >= nsamp
     with pytest.raises(ValueError):
         aa.strategy([], 4096, 1 << 20, 1670.0, -0.0732421875, 64e-6, 8)
+
+
+def test_failure_injection_counter(aa):
+    """aa_b200_debug_fail_after arms a host-side countdown (no GPU needed to set it)."""
+    L = aa.lib()
+    L.aa_b200_debug_fail_after(7)
+    assert L.aa_b200_debug_fail_countdown() == 7
+    L.aa_b200_debug_fail_after(-1)
+    assert L.aa_b200_debug_fail_countdown() == 0
