@@ -67,3 +67,66 @@ def test_partition_single_rank():
     from aa_b200 import workloads as WL
     assert WL.partition([3.0, 1.0, 2.0], 1) == [[0, 1, 2]]
     assert WL.partition([5.0, 4.0, 3.0, 3.0], 2) == [[0, 3], [1, 2]]
+
+
+def _queue_worker(rank, world, port, nbeams, die_rank, q):
+    """Beams from aa_b200.beamqueue over a TCPStore; rank `die_rank` takes one
+    beam and exits without finishing it (a rank that stops mid-beam)."""
+    sys.path.insert(0, os.path.join(ROOT, "astro-accelerate_b200"))
+    import hashlib
+    import time
+    from datetime import timedelta
+
+    import torch.distributed as dist
+    from aa_b200.beamqueue import BeamQueue
+
+    store = dist.TCPStore("127.0.0.1", port, world, rank == 0, timeout=timedelta(seconds=60))
+    bq = BeamQueue(store, nbeams, rank, lease_s=1.5)
+
+    def work(i):
+        time.sleep(0.05)
+        return hashlib.sha256(f"beam-{i}".encode()).hexdigest()
+
+    if rank == die_rank:
+        bq._claim_next()
+        os._exit(0)  # stops holding a lease: no done mark, no renewal
+    mine = bq.run(work, timeout_s=120)
+    results = {i: bq.result(i).decode() for i in range(nbeams)} if rank == 0 else None
+    q.put((rank, mine, results, bq.ndone()))
+    # keep the store (hosted by rank 0) up until every live rank has finished
+    store.add("finished", 1)
+    while int(store.add("finished", 0)) < world - (1 if die_rank is not None else 0):
+        time.sleep(0.05)
+    bq.close()
+
+
+def _run_queue(world, nbeams, die_rank):
+    port = 31000 + (os.getpid() % 2000)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_queue_worker, args=(r, world, port, nbeams, die_rank, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    live = world - (1 if die_rank is not None else 0)
+    res = [q.get(timeout=300) for _ in range(live)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    return sorted(res, key=lambda r: r[0])
+
+
+def test_beam_queue_every_beam_once():
+    import hashlib
+    res = _run_queue(world=2, nbeams=10, die_rank=None)
+    done = sorted(i for r in res for i in r[1])
+    assert done == list(range(10))  # each beam by exactly one rank
+    assert all(r[3] == 10 for r in res)
+    assert res[0][2] == {i: hashlib.sha256(f"beam-{i}".encode()).hexdigest() for i in range(10)}
+
+
+def test_beam_queue_recovers_the_beam_of_a_stopped_rank():
+    import hashlib
+    res = _run_queue(world=3, nbeams=9, die_rank=2)
+    done = sorted(i for r in res for i in r[1])
+    assert done == list(range(9))  # the stopped rank's beam was taken over, once
+    assert res[0][2] == {i: hashlib.sha256(f"beam-{i}".encode()).hexdigest() for i in range(9)}
