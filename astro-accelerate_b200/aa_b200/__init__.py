@@ -198,6 +198,16 @@ def lib():
         "aa_b200_sps_row_stats": ([vp, i, ll, ll, vp, vp, vp], i),
         "aa_b200_sps_block_peaks": ([vp, i, ll, ll, vp, vp, P(i), i, vp, vp, vp, vp], i),
         "aa_b200_sps_block_samples": ([], i),
+        "aa_b200_spd_create": ([ll, ll], vp),
+        "aa_b200_spd_destroy": ([vp], None),
+        "aa_b200_spd_last_error": ([vp], ctypes.c_char_p),
+        "aa_b200_spd_clear": ([vp, vp], i),
+        "aa_b200_spd_run": ([vp, vp, i, i, f, i, f, f, f, i, i, vp, sz, vp, vp, vp, vp, P(sz)], i),
+        "aa_b200_spd_profile": ([vp, vp, i, vp, P(i), P(i), P(i), P(i)], i),
+        "aa_b200_spd_keep_planes": ([vp, i], i),
+        "aa_b200_spd_planes": ([vp, vp, vp, ll], ll),
+        "aa_b200_spd_kernel_launches": ([], ll),
+        "aa_b200_spd_write_candidates": ([ctypes.c_char_p, i, f, f, f, f, f, i, vp, vp, vp, vp, sz], i),
     }
     for name, (args, res) in protos.items():
         fn = getattr(L, name)
@@ -724,3 +734,104 @@ def batch_estimate_bytes(metadata: filterbank_metadata_struct, plan: "aa_py_ddtr
     if lib().aa_b200_batch_estimate_bytes(metadata, plan.pointer(), free_memory, ctypes.byref(n)):
         raise RuntimeError(lib().aa_b200_batch_last_error(None).decode())
     return n.value
+
+
+class single_pulse_detection:
+    """analysis_GPU (src/aa_device_analysis.cu:130-345) on DM-time planes in
+    device memory (aa_b200_spd_*): the reference's MSD profile, boxcar S/N
+    planes and candidate lists (peak finding or thresholding), bit for bit.
+
+    max_elems bounds nDMs * nT of the planes run; max_time_samples is the
+    reference's batch size in elements (0 = one batch for the whole plane).
+    run() overwrites the plane, like the reference's search."""
+
+    def __init__(self, max_elems: int, max_time_samples: int = 0):
+        self.m_obj = lib().aa_b200_spd_create(int(max_elems), int(max_time_samples))
+        if not self.m_obj:
+            raise RuntimeError(lib().aa_b200_spd_last_error(None).decode())
+
+    def last_error(self) -> str:
+        m = lib().aa_b200_spd_last_error(self.m_obj)
+        return m.decode() if m else ""
+
+    def clear(self, stream: int = 0):
+        if lib().aa_b200_spd_clear(self.m_obj, ctypes.c_void_p(stream)):
+            raise RuntimeError(self.last_error())
+
+    def keep_planes(self, on: bool = True):
+        lib().aa_b200_spd_keep_planes(self.m_obj, int(on))
+
+    def run(self, d_plane, ndms: int, nt: int, tsamp: float, inBin: int, sigma_cutoff: float, sigma_constant: float,
+            max_boxcar_width_in_sec: float, candidate_algorithm: int = 0, enable_msd_baseline_noise: bool = False,
+            max_candidates: int | None = None, stream: int = 0) -> dict:
+        """Candidates of one plane as numpy arrays: dm (trial index), ts
+        (sample), snr, bw (boxcar width in samples of the range)."""
+        import numpy as np
+        ptr = d_plane if isinstance(d_plane, int) else d_plane.data_ptr()
+        cap = int(max_candidates) if max_candidates is not None else max(1, int(ndms) * int(nt) // 2)
+        dm = np.zeros(cap, np.uint32)
+        ts = np.zeros(cap, np.uint32)
+        snr = np.zeros(cap, np.float32)
+        bw = np.zeros(cap, np.uint32)
+        n = ctypes.c_size_t()
+        rc = lib().aa_b200_spd_run(self.m_obj, ctypes.c_void_p(ptr), int(ndms), int(nt), float(tsamp), int(inBin),
+                                   float(sigma_cutoff), float(sigma_constant), float(max_boxcar_width_in_sec),
+                                   int(candidate_algorithm), int(bool(enable_msd_baseline_noise)),
+                                   ctypes.c_void_p(stream), cap, dm.ctypes.data, ts.ctypes.data, snr.ctypes.data,
+                                   bw.ctypes.data, ctypes.byref(n))
+        if rc:
+            raise RuntimeError(self.last_error())
+        k = n.value
+        return {"dm": dm[:k].copy(), "ts": ts[:k].copy(), "snr": snr[:k].copy(), "bw": bw[:k].copy()}
+
+    def profile(self) -> dict:
+        """The plan and the interpolated (mean, deviation) per width of the last run."""
+        import numpy as np
+        cap = 1024
+        msd = np.zeros(2 * cap, np.float32)
+        widths = np.zeros(cap, np.int32)
+        nw, mwp, mit, drop = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        lib().aa_b200_spd_profile(self.m_obj, msd.ctypes.data, cap, widths.ctypes.data, ctypes.byref(nw),
+                                  ctypes.byref(mwp), ctypes.byref(mit), ctypes.byref(drop))
+        k = nw.value
+        return {"widths": widths[:k].copy(), "msd": msd[:2 * k].copy(), "max_width_performed": mwp.value,
+                "max_iteration": mit.value, "dropped_batches": drop.value}
+
+    def planes(self):
+        """(snr, taps) of the last batch of the last run (keep_planes on)."""
+        import numpy as np
+        n = lib().aa_b200_spd_planes(self.m_obj, None, None, 0)
+        snr = np.zeros(n, np.float32)
+        taps = np.zeros(n, np.uint16)
+        lib().aa_b200_spd_planes(self.m_obj, snr.ctypes.data, taps.ctypes.data, n)
+        return snr, taps
+
+    def delete(self):
+        if getattr(self, "m_obj", None):
+            lib().aa_b200_spd_destroy(self.m_obj)
+            self.m_obj = None
+
+    def __del__(self):
+        try:
+            self.delete()
+        except Exception:
+            pass
+
+
+def spd_kernel_launches() -> int:
+    return lib().aa_b200_spd_kernel_launches()
+
+
+def write_candidates(directory: str, candidate_algorithm: int, tstart: float, dm_low: float, dm_high: float,
+                     dm_step: float, tsamp: float, inBin: int, cands: dict) -> None:
+    """The reference's candidate file (peak_analysed-/analysed-t_..-dm_..-...dat)."""
+    import numpy as np
+    dm = np.ascontiguousarray(cands["dm"], np.uint32)
+    ts = np.ascontiguousarray(cands["ts"], np.uint32)
+    snr = np.ascontiguousarray(cands["snr"], np.float32)
+    bw = np.ascontiguousarray(cands["bw"], np.uint32)
+    if lib().aa_b200_spd_write_candidates(directory.encode() if directory else None, int(candidate_algorithm),
+                                          float(tstart), float(dm_low), float(dm_high), float(dm_step),
+                                          float(tsamp), int(inBin), dm.ctypes.data, ts.ctypes.data,
+                                          snr.ctypes.data, bw.ctypes.data, dm.size):
+        raise RuntimeError(lib().aa_b200_spd_last_error(None).decode())

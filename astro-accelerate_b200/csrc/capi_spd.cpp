@@ -1,0 +1,196 @@
+// capi_spd.cpp -- extern "C" entry points of the single-pulse detection
+// (aa_b200_spd_*, declared in include/aa_b200.h): analysis_GPU of
+// src/aa_device_analysis.cu:130-345 on one DM-time plane in device memory,
+// and the candidate file it writes.
+#include "aa_b200.h"
+
+#include <cstdio>
+#include <new>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "spd.cuh"
+
+using namespace aab200;
+
+namespace {
+
+struct SpdHandle {
+    SpdPlane plane;
+    std::string error;
+};
+
+thread_local std::string g_spd_error;
+
+SpdHandle *as_spd(void *obj) { return static_cast<SpdHandle *>(obj); }
+
+} // namespace
+
+extern "C" {
+
+void *aa_b200_spd_create(long long max_elems, long long max_time_samples)
+{
+    SpdHandle *h = new (std::nothrow) SpdHandle();
+    if (!h) {
+        g_spd_error = "single-pulse detection: out of host memory";
+        return nullptr;
+    }
+    std::string err;
+    if (!h->plane.setup(max_elems, max_time_samples, err)) {
+        g_spd_error = err;
+        delete h;
+        return nullptr;
+    }
+    return h;
+}
+
+void aa_b200_spd_destroy(void *obj) { delete as_spd(obj); }
+
+const char *aa_b200_spd_last_error(const void *obj)
+{
+    return obj ? static_cast<const SpdHandle *>(obj)->error.c_str() : g_spd_error.c_str();
+}
+
+int aa_b200_spd_clear(void *obj, void *stream)
+{
+    SpdHandle *h = as_spd(obj);
+    if (!h)
+        return 1;
+    const cudaError_t e = h->plane.clear(static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) {
+        h->error = std::string("single-pulse detection: ") + cudaGetErrorString(e);
+        return 1;
+    }
+    return 0;
+}
+
+int aa_b200_spd_keep_planes(void *obj, int on)
+{
+    SpdHandle *h = as_spd(obj);
+    if (!h)
+        return 1;
+    h->plane.keep_planes = on != 0;
+    return 0;
+}
+
+int aa_b200_spd_run(void *obj, float *d_plane, int nDMs, int nTimesamples, float tsamp, int inBin,
+                    float sigma_cutoff, float sigma_constant, float max_boxcar_width_in_sec, int candidate_algorithm,
+                    int enable_msd_baseline_noise, void *stream, size_t max_candidates, unsigned *h_dm,
+                    unsigned *h_ts, float *h_snr, unsigned *h_bw, size_t *n_candidates)
+{
+    SpdHandle *h = as_spd(obj);
+    if (!h)
+        return 1;
+    if (!d_plane || !n_candidates || (max_candidates > 0 && (!h_dm || !h_ts || !h_snr || !h_bw))) {
+        h->error = "single-pulse detection: null argument";
+        return 1;
+    }
+    SpdSettings s;
+    s.sigma_cutoff = sigma_cutoff;
+    s.sigma_constant = sigma_constant;
+    s.max_boxcar_width_in_sec = max_boxcar_width_in_sec;
+    s.candidate_algorithm = candidate_algorithm;
+    s.enable_msd_baseline_noise = enable_msd_baseline_noise;
+    SpdCandidates c;
+    std::string err;
+    h->plane.dropped_batches = 0;
+    if (!h->plane.run(d_plane, nDMs, nTimesamples, tsamp, inBin, s, c, static_cast<cudaStream_t>(stream), err,
+                      max_candidates)) {
+        h->error = err;
+        return 1;
+    }
+    const size_t k = c.dm.size();
+    for (size_t i = 0; i < k; ++i) {
+        h_dm[i] = c.dm[i];
+        h_ts[i] = c.ts[i];
+        h_snr[i] = c.snr[i];
+        h_bw[i] = c.bw[i];
+    }
+    *n_candidates = k;
+    return 0;
+}
+
+int aa_b200_spd_profile(const void *obj, float *msd, int msd_cap, int *widths, int *nwidths,
+                        int *max_width_performed, int *max_iteration, int *dropped_batches)
+{
+    const SpdHandle *h = static_cast<const SpdHandle *>(obj);
+    if (!h)
+        return 1;
+    const SpdPlane &p = h->plane;
+    const int nw = static_cast<int>(p.last_widths.size());
+    if (nwidths)
+        *nwidths = nw;
+    if (max_width_performed)
+        *max_width_performed = p.last_max_width_performed;
+    if (max_iteration)
+        *max_iteration = p.last_max_iteration;
+    if (dropped_batches)
+        *dropped_batches = p.dropped_batches;
+    if (widths)
+        for (int i = 0; i < nw && i < msd_cap; ++i)
+            widths[i] = p.last_widths[i];
+    if (msd)
+        for (int i = 0; i < static_cast<int>(p.last_msd.size()) && i < 2 * msd_cap; ++i)
+            msd[i] = p.last_msd[i];
+    return 0;
+}
+
+long long aa_b200_spd_planes(const void *obj, float *snr, unsigned short *taps, long long cap)
+{
+    const SpdHandle *h = static_cast<const SpdHandle *>(obj);
+    if (!h)
+        return -1;
+    const long long n = static_cast<long long>(h->plane.last_snr.size());
+    if (snr && taps && cap >= n) {
+        for (long long i = 0; i < n; ++i) {
+            snr[i] = h->plane.last_snr[i];
+            taps[i] = h->plane.last_taps[i];
+        }
+    }
+    return n;
+}
+
+long long aa_b200_spd_kernel_launches(void) { return spd_kernel_launches(); }
+
+// src/aa_device_analysis.cu:420-466: float records (DM, time, S/N, width) --
+// DM = trial * dm_step + dm_low, time = sample * tsamp + tstart (tsamp of
+// the range), width = boxcar width * inBin -- in a file named
+// "peak_analysed-t_%.2f-dm_%.2f-%.2f.dat" (algorithms 0 and 2) or
+// "analysed-..." (algorithm 1) after tstart, dm_low and dm_high, under dir
+// (the working directory when dir is null or empty).  Nothing is written for
+// no candidates.  Returns 0, or 1 when the file could not be written.
+int aa_b200_spd_write_candidates(const char *dir, int candidate_algorithm, float tstart, float dm_low, float dm_high,
+                                 float dm_step, float tsamp, int inBin, const unsigned *dm, const unsigned *ts,
+                                 const float *snr, const unsigned *bw, size_t n)
+{
+    if (n == 0)
+        return 0;
+    char name[256];
+    std::snprintf(name, sizeof(name), "%s-t_%.2f-dm_%.2f-%.2f.dat",
+                  candidate_algorithm == 1 ? "analysed" : "peak_analysed", tstart, dm_low, dm_high);
+    std::string path = (dir && *dir) ? std::string(dir) + "/" + name : std::string(name);
+    float *rec = new (std::nothrow) float[4 * n];
+    if (!rec) {
+        g_spd_error = "single-pulse detection: out of host memory";
+        return 1;
+    }
+    for (size_t i = 0; i < n; ++i) {
+        rec[4 * i] = static_cast<float>(static_cast<double>(dm[i]) * dm_step + dm_low);
+        rec[4 * i + 1] = static_cast<float>(static_cast<double>(ts[i]) * tsamp + tstart);
+        rec[4 * i + 2] = static_cast<float>(static_cast<double>(snr[i]));
+        rec[4 * i + 3] = static_cast<float>(static_cast<double>(bw[i]) * inBin);
+    }
+    FILE *fp = std::fopen(path.c_str(), "wb");
+    int rc = 0;
+    if (!fp || std::fwrite(rec, n * sizeof(float), 4, fp) != 4) {
+        g_spd_error = "single-pulse detection: cannot write " + path;
+        rc = 1;
+    }
+    if (fp)
+        std::fclose(fp);
+    delete[] rec;
+    return rc;
+}
+
+} // extern "C"

@@ -1,0 +1,933 @@
+// spd.cu -- kernels of the single-pulse detection (see spd.cuh).  Each keeps
+// the arithmetic of the reference kernel it corresponds to (cited per
+// kernel): the streaming mean/variance updates and pairwise merges in float,
+// the merge trees of its thread blocks, the boxcar partial sums exchanged
+// between threads through shared memory, the fast divisions, and the
+// neighbourhood rules of the peak finder.
+#include "spd.cuh"
+
+#include <atomic>
+#include <cmath>
+
+namespace aab200 {
+
+namespace {
+std::atomic<long long> g_spd_launches{0};
+}
+
+long long spd_kernel_launches() { return g_spd_launches.load(); }
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// Streaming statistics (include/aa_device_MSD_shared_kernel_functions.cuh:13-35)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void st_first(float &M, float &S, float &j, float e)
+{
+    M = e;
+    S = 0;
+    j = 1.0f;
+}
+
+__device__ __forceinline__ void st_add(float &M, float &S, float &j, float e)
+{
+    float ftemp;
+    j = j + 1.0f;
+    M = M + e;
+    ftemp = (j * e - M);
+    S = S + 1.0f / (j * (j - 1.0f)) * ftemp * ftemp;
+}
+
+__device__ __forceinline__ void st_merge(float &AM, float &AS, float &Aj, float BM, float BS, float Bj)
+{
+    float ftemp;
+    ftemp = (Bj / Aj) * AM - BM;
+    AS = AS + BS + (Aj / (Bj * (Aj + Bj))) * ftemp * ftemp;
+    AM = AM + BM;
+    Aj = Aj + Bj;
+}
+
+// Block tree over s[3][bd] (M, S, j) down to 32 values, skipping empty ones
+// (:36-66); then the warp tree (:120-139).
+__device__ __forceinline__ void tree_sm(float &M, float &S, float &j, float *s)
+{
+    const int t = threadIdx.x, bd = blockDim.x;
+    M = s[t];
+    S = s[bd + t];
+    j = s[2 * bd + t];
+    for (int i = (bd >> 1); i > 16; i >>= 1) {
+        if (t < i) {
+            const float jv = s[2 * bd + i + t];
+            if (((int)jv) != 0) {
+                if (j == 0) {
+                    S = s[bd + i + t];
+                    M = s[i + t];
+                    j = jv;
+                } else {
+                    st_merge(M, S, j, s[i + t], s[bd + i + t], jv);
+                }
+            }
+            s[t] = M;
+            s[bd + t] = S;
+            s[2 * bd + t] = j;
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void tree_warp(float &M, float &S, float &j)
+{
+    for (int q = 16; q > 0; q >>= 1) {
+        const float BM = __shfl_down_sync(FULL, M, q);
+        const float BS = __shfl_down_sync(FULL, S, q);
+        const float Bj = __shfl_down_sync(FULL, j, q);
+        if (Bj > 0) {
+            if (j == 0) {
+                S = BS;
+                M = BM;
+                j = Bj;
+            } else {
+                st_merge(M, S, j, BM, BS, Bj);
+            }
+        }
+    }
+}
+
+// with running maxima and minima (:67-119, :140-169; the reference keeps
+// the larger of the two minima in the warp tree, reproduced)
+__device__ __forceinline__ void tree_sm_max(float &M, float &S, float &j, float &mx, float &mn, float *s)
+{
+    const int t = threadIdx.x, bd = blockDim.x;
+    M = s[t];
+    S = s[bd + t];
+    j = s[2 * bd + t];
+    mx = s[3 * bd + t];
+    mn = s[4 * bd + t];
+    for (int i = (bd >> 1); i > 16; i >>= 1) {
+        if (t < i) {
+            const int jv = (int)s[2 * bd + i + t];
+            if (jv != 0) {
+                if (j == 0) {
+                    M = s[i + t];
+                    S = s[bd + i + t];
+                    mx = s[3 * bd + i + t];
+                    mn = s[4 * bd + i + t];
+                    j = (float)jv;
+                } else {
+                    st_merge(M, S, j, s[i + t], s[bd + i + t], (float)jv);
+                    mx = fmaxf(mx, s[3 * bd + i + t]);
+                    mn = fminf(mn, s[4 * bd + i + t]);
+                }
+            }
+            s[t] = M;
+            s[bd + t] = S;
+            s[2 * bd + t] = j;
+            s[3 * bd + t] = mx;
+            s[4 * bd + t] = mn;
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void tree_warp_max(float &M, float &S, float &j, float &mx, float &mn)
+{
+    for (int q = 16; q > 0; q >>= 1) {
+        const float BM = __shfl_down_sync(FULL, M, q);
+        const float BS = __shfl_down_sync(FULL, S, q);
+        const float Bmx = __shfl_down_sync(FULL, mx, q);
+        const float Bmn = __shfl_down_sync(FULL, mn, q);
+        const float Bj = __shfl_down_sync(FULL, j, q);
+        if (Bj > 0) {
+            if (j == 0) {
+                S = BS;
+                M = BM;
+                j = Bj;
+                mx = Bmx;
+                mn = Bmn;
+            } else {
+                st_merge(M, S, j, BM, BS, Bj);
+                mx = fmaxf(mx, Bmx);
+                mn = fmaxf(mn, Bmn);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Partial statistics per block of 512 columns x y_steps rows
+// (src/aa_device_MSD_normal_kernel.cu:10-47,
+//  src/aa_device_MSD_outlier_rejection_kernel.cu:11-115)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(SPD_NTHREADS) k_msd_partials(const float *__restrict__ in, float *__restrict__ part,
+                                                               int y_steps, long long nT, long long offset)
+{
+    __shared__ float s[3 * SPD_NTHREADS];
+    float M = 0, S = 0, j = 0;
+    const long long spos = static_cast<long long>(blockIdx.x) * SPD_NTHREADS + threadIdx.x;
+    long long g = static_cast<long long>(blockIdx.y) * y_steps * nT + spos;
+    if (spos < nT - offset) {
+        st_first(M, S, j, __ldg(in + g));
+        g += nT;
+        for (int y = 1; y < y_steps; ++y) {
+            st_add(M, S, j, __ldg(in + g));
+            g += nT;
+        }
+    }
+    s[threadIdx.x] = M;
+    s[blockDim.x + threadIdx.x] = S;
+    s[2 * blockDim.x + threadIdx.x] = j;
+    __syncthreads();
+    tree_sm(M, S, j, s);
+    tree_warp(M, S, j);
+    if (threadIdx.x == 0) {
+        const long long b = static_cast<long long>(blockIdx.y) * gridDim.x + blockIdx.x;
+        part[5 * b] = M;
+        part[5 * b + 1] = S;
+        part[5 * b + 2] = j;
+    }
+}
+
+__global__ void __launch_bounds__(SPD_NTHREADS) k_msd_partials_minmax(const float *__restrict__ in,
+                                                                      float *__restrict__ part, int y_steps,
+                                                                      long long nT, long long offset)
+{
+    __shared__ float s[5 * SPD_NTHREADS];
+    float M = 0, S = 0, j = 0, mx = 0, mn = 0;
+    const long long spos = static_cast<long long>(blockIdx.x) * SPD_NTHREADS + threadIdx.x;
+    long long g = static_cast<long long>(blockIdx.y) * y_steps * nT + spos;
+    if (spos < nT - offset) {
+        float e = in[g];
+        st_first(M, S, j, e);
+        mx = e;
+        mn = e;
+        g += nT;
+        for (int y = 1; y < y_steps; ++y) {
+            e = in[g];
+            mx = fmaxf(mx, e);
+            mn = fminf(mn, e);
+            st_add(M, S, j, e);
+            g += nT;
+        }
+    }
+    s[threadIdx.x] = M;
+    s[blockDim.x + threadIdx.x] = S;
+    s[2 * blockDim.x + threadIdx.x] = j;
+    s[3 * blockDim.x + threadIdx.x] = mx;
+    s[4 * blockDim.x + threadIdx.x] = mn;
+    __syncthreads();
+    tree_sm_max(M, S, j, mx, mn, s);
+    tree_warp_max(M, S, j, mx, mn);
+    if (threadIdx.x == 0) {
+        const long long b = static_cast<long long>(blockIdx.y) * gridDim.x + blockIdx.x;
+        part[5 * b] = M;
+        part[5 * b + 1] = S;
+        part[5 * b + 2] = j;
+        part[5 * b + 3] = mx;
+        part[5 * b + 4] = mn;
+    }
+}
+
+// A block whose previous extremes lie inside the cut keeps its partials.
+__global__ void __launch_bounds__(SPD_NTHREADS) k_msd_partials_rejection(const float *__restrict__ in,
+                                                                         float *__restrict__ part,
+                                                                         const float *__restrict__ msd, int y_steps,
+                                                                         long long nT, long long offset, float sigma)
+{
+    __shared__ float s[5 * SPD_NTHREADS];
+    const float limit_down = msd[0] - sigma * msd[1];
+    const float limit_up = msd[0] + sigma * msd[1];
+    const long long b = static_cast<long long>(blockIdx.y) * gridDim.x + blockIdx.x;
+    float mx = part[5 * b + 3];
+    float mn = part[5 * b + 4];
+    if ((mn > limit_down) && (mx < limit_up))
+        return; // the whole block
+    float M = 0, S = 0, j = 0;
+    mx = 0;
+    mn = 0;
+    const long long spos = static_cast<long long>(blockIdx.x) * SPD_NTHREADS + threadIdx.x;
+    long long g = static_cast<long long>(blockIdx.y) * y_steps * nT + spos;
+    if (spos < nT - offset) {
+        for (int y = 0; y < y_steps; ++y) {
+            const float e = in[g];
+            if ((e > limit_down) && (e < limit_up)) {
+                if (j == 0) {
+                    st_first(M, S, j, e);
+                    mx = e;
+                    mn = e;
+                } else {
+                    st_add(M, S, j, e);
+                    mx = fmaxf(mx, e);
+                    mn = fminf(mn, e);
+                }
+            }
+            g += nT;
+        }
+    }
+    s[threadIdx.x] = M;
+    s[blockDim.x + threadIdx.x] = S;
+    s[2 * blockDim.x + threadIdx.x] = j;
+    s[3 * blockDim.x + threadIdx.x] = mx;
+    s[4 * blockDim.x + threadIdx.x] = mn;
+    __syncthreads();
+    tree_sm_max(M, S, j, mx, mn, s);
+    tree_warp_max(M, S, j, mx, mn);
+    if (threadIdx.x == 0) {
+        part[5 * b] = M;
+        part[5 * b + 1] = S;
+        part[5 * b + 2] = j;
+        part[5 * b + 3] = mx;
+        part[5 * b + 4] = mn;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Merging the partials in one block (src/aa_device_MSD_shared_kernel_functions.cu:7-85
+// with include/aa_device_MSD_shared_kernel_functions.cuh:81-240).  "Regular"
+// partials are all non-empty and are merged unconditionally; "non-regular"
+// ones (after outlier rejection) skip empty partials -- and, below one
+// partial per thread, also skip partial 0, as the reference does.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void sum_regular(float &M, float &S, float &j, const float *p, float *s, int size)
+{
+    const int t = threadIdx.x, bd = blockDim.x;
+    int pos = t;
+    if (size > bd) {
+        M = p[5 * pos];
+        S = p[5 * pos + 1];
+        j = p[5 * pos + 2];
+        pos += bd;
+        while (pos < size) {
+            st_merge(M, S, j, p[5 * pos], p[5 * pos + 1], p[5 * pos + 2]);
+            pos += bd;
+        }
+        s[t] = M;
+        s[bd + t] = S;
+        s[2 * bd + t] = j;
+        __syncthreads();
+        M = s[t];
+        S = s[bd + t];
+        j = s[2 * bd + t];
+        for (int i = (bd >> 1); i > 16; i >>= 1) {
+            if (t < i) {
+                st_merge(M, S, j, s[i + t], s[bd + i + t], s[2 * bd + i + t]);
+                s[t] = M;
+                s[bd + t] = S;
+                s[2 * bd + t] = j;
+            }
+            __syncthreads();
+        }
+        for (int q = 16; q > 0; q >>= 1)
+            st_merge(M, S, j, __shfl_down_sync(FULL, M, q), __shfl_down_sync(FULL, S, q),
+                     __shfl_down_sync(FULL, j, q));
+    } else if (t == 0) {
+        M = p[0];
+        S = p[1];
+        j = p[2];
+        for (pos = 1; pos < size; ++pos)
+            st_merge(M, S, j, p[5 * pos], p[5 * pos + 1], p[5 * pos + 2]);
+    }
+}
+
+__device__ __forceinline__ void sum_nonregular(float &M, float &S, float &j, const float *p, float *s, int size)
+{
+    const int t = threadIdx.x, bd = blockDim.x;
+    int pos = t;
+    if (size > bd) {
+        M = 0;
+        S = 0;
+        j = 0;
+        while (pos < size) {
+            const float jv = p[5 * pos + 2];
+            if (((int)jv) > 0) {
+                if ((int)j == 0) {
+                    M = p[5 * pos];
+                    S = p[5 * pos + 1];
+                    j = jv;
+                } else {
+                    st_merge(M, S, j, p[5 * pos], p[5 * pos + 1], jv);
+                }
+            }
+            pos += bd;
+        }
+        s[t] = M;
+        s[bd + t] = S;
+        s[2 * bd + t] = j;
+        __syncthreads();
+        tree_sm(M, S, j, s);
+        tree_warp(M, S, j);
+    } else if (t == 0) {
+        M = 0;
+        S = 0;
+        j = 0;
+        for (pos = 1; pos < size; ++pos) {
+            const float jv = p[5 * pos + 2];
+            if (((int)jv) != 0) {
+                if ((int)j == 0) {
+                    M = p[5 * pos];
+                    S = p[5 * pos + 1];
+                    j = jv;
+                } else {
+                    st_merge(M, S, j, p[5 * pos], p[5 * pos + 1], jv);
+                }
+            }
+        }
+    }
+}
+
+// d_msd = (M / j, sqrt(S / j), j); with d_pp, earlier (M, S, j) are merged
+// in first and the merged totals kept in d_pp.
+__global__ void k_msd_final(const float *__restrict__ p, float *__restrict__ msd, float *pp, int size, int regular)
+{
+    __shared__ float s[3 * 32 * 32];
+    float M, S, j;
+    if (regular)
+        sum_regular(M, S, j, p, s, size);
+    else
+        sum_nonregular(M, S, j, p, s, size);
+    if (pp && pp[2] > 0)
+        st_merge(M, S, j, pp[0], pp[1], pp[2]);
+    if (threadIdx.x == 0) {
+        msd[0] = M / j;
+        msd[1] = sqrt(S / j);
+        msd[2] = j;
+        if (pp) {
+            pp[0] = M;
+            pp[1] = S;
+            pp[2] = j;
+        }
+    }
+}
+
+// src/aa_device_binning_kernel.cu:48-64 (rows 0 .. 2*(nDMs/2)-1)
+__global__ void k_dit_pairs(const float *__restrict__ in, float *__restrict__ out, int rows, long long nT, long long dts)
+{
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (y >= rows || 2 * i + 1 >= nT)
+        return;
+    out[y * dts + i] = in[y * nT + 2 * i] + in[y * nT + 2 * i + 1];
+}
+
+// src/aa_device_single_FIR_kernel.cu:95-107
+__global__ void k_fir_rows(const float *__restrict__ in, float *__restrict__ out, int nTaps, long long nT)
+{
+    const long long x = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const long long y = blockIdx.y;
+    if (x < nT - nTaps + 1) {
+        float f = 0;
+        for (int t = 0; t < nTaps; ++t)
+            f += __ldg(in + y * nT + x + t);
+        out[y * nT + x] = f;
+    }
+}
+
+// src/aa_device_MSD_shared_kernel_functions.cu:86-120
+__global__ void k_msd_interpolate(const float *__restrict__ dit, float *__restrict__ out, const int *__restrict__ dw,
+                                  int n_dit, const int *__restrict__ widths, int max_width_performed)
+{
+    const int tid = threadIdx.x;
+    if (widths[tid] <= max_width_performed) {
+        const int desired = widths[tid];
+        const int position = (int)floorf(log2f((float)desired));
+        const float width1 = dw[position];
+        const float mean1 = dit[position * 3];
+        const float sd1 = dit[position * 3 + 1];
+        if (position == n_dit - 1 && width1 == (int)desired) {
+            out[tid * 2] = mean1;
+            out[tid * 2 + 1] = sd1;
+        } else {
+            const float width2 = dw[position + 1];
+            const float distance_in_width = width2 - width1;
+            const float mean2 = dit[(position + 1) * 3];
+            const float distance_in_mean = mean2 - mean1;
+            const float sd2 = dit[(position + 1) * 3 + 1];
+            const float distance_in_sd = sd2 - sd1;
+            out[tid * 2] = mean1 + (distance_in_mean / distance_in_width) * ((float)desired - width1);
+            out[tid * 2 + 1] = sd1 + (distance_in_sd / distance_in_width) * ((float)desired - width1);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Boxcar S/N planes (src/aa_device_SPS_long_kernel.cu:42-168 and :170-283).
+// A block of 512 threads covers 2*512 - nBoxcars samples of one DM trial,
+// two per thread.  Thread t holds the sums of 1..4 samples starting at its
+// two samples (Bw[0..3] from sample 2t, Bw[4..7] from 2t+1); a boxcar of
+// width d+1..d+4 adds the 4-sample sum of thread t + d/2 - ... exchanged
+// through shared memory, so thread t at step d updates the best S/N of
+// thread t - d/2.  S/N = (sum - mean_w) / sd_w with the fast division; the
+// width of the best S/N is kept with it.  Each plane also writes the
+// 2-sample sums (the next iteration's input at half resolution) and the
+// 4-sample sums at half resolution (the running boxcar values).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float snr_of(float bw, float2 st) { return __fdividef(bw - st.x, st.y); }
+
+__device__ __forceinline__ float snr_of_bv(float bv, float bw, float2 st) { return __fdividef(bv + (bw - st.x), st.y); }
+
+__global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_first(const float *__restrict__ in, float *bv_out, float *dec,
+                                                             float *snr_out, uint16_t *taps_out,
+                                                             const float2 *__restrict__ msd, int nT, int nBoxcars,
+                                                             int dtm)
+{
+    __shared__ float2 s_in[SPD_NTHREADS];
+    __shared__ float2 s_snr[SPD_NTHREADS];
+    __shared__ ushort2 s_taps[SPD_NTHREADS];
+    const int t = threadIdx.x;
+    float Bw[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    float2 f1, f2, f3, SNR = make_float2(0, 0);
+    ushort2 taps, taps1, taps2;
+    int spos = blockIdx.x * (2 * SPD_NTHREADS - nBoxcars) + 2 * t;
+    const long long row = static_cast<long long>(blockIdx.y) * nT;
+    if ((spos + 4) < nT) {
+        const long long g = row + spos;
+        f1.x = in[g];
+        f1.y = in[g + 1];
+        f2.x = in[g + 2];
+        f2.y = in[g + 3];
+        f3.x = in[g + 4];
+        Bw[0] = f1.x;
+        Bw[4] = f1.y;
+        Bw[1] = f1.x + f1.y;
+        Bw[5] = f1.y + f2.x;
+        Bw[2] = Bw[1] + f2.x;
+        Bw[6] = Bw[5] + f2.y;
+        Bw[3] = Bw[1] + f2.x + f2.y;
+        Bw[7] = Bw[5] + f2.y + f3.x;
+    }
+    spos = blockIdx.x * (SPD_NTHREADS - (nBoxcars >> 1)) + t;
+    if (t < (SPD_NTHREADS - (nBoxcars >> 1)) && spos < dtm)
+        dec[static_cast<long long>(blockIdx.y) * dtm + spos] = Bw[1];
+    s_in[t].x = Bw[3];
+    s_in[t].y = Bw[7];
+    __syncthreads();
+    float2 st = msd[0];
+    f1.x = snr_of(Bw[0], st);
+    f1.y = snr_of(Bw[4], st);
+    st = msd[1];
+    f2.x = snr_of(Bw[1], st);
+    f2.y = snr_of(Bw[5], st);
+    if (f2.x > f1.x) { f1.x = f2.x; taps1.x = 2; } else taps1.x = 1;
+    if (f2.y > f1.y) { f1.y = f2.y; taps1.y = 2; } else taps1.y = 1;
+    st = msd[2];
+    f2.x = snr_of(Bw[2], st);
+    f2.y = snr_of(Bw[6], st);
+    st = msd[3];
+    f3.x = snr_of(Bw[3], st);
+    f3.y = snr_of(Bw[7], st);
+    if (f3.x > f2.x) { f2.x = f3.x; taps2.x = 4; } else taps2.x = 3;
+    if (f3.y > f2.y) { f2.y = f3.y; taps2.y = 4; } else taps2.y = 3;
+    if (f1.x > f2.x) { SNR.x = f1.x; taps.x = taps1.x; } else { SNR.x = f2.x; taps.x = taps2.x; }
+    if (f1.y > f2.y) { SNR.y = f1.y; taps.y = taps1.y; } else { SNR.y = f2.y; taps.y = taps2.y; }
+    s_snr[t] = SNR;
+    s_taps[t] = taps;
+    for (int d = 4; d < nBoxcars; d += 4) {
+        __syncthreads();
+        spos = t - (d >> 1);
+        if (spos >= 0) {
+            f1 = s_in[spos];
+            SNR = s_snr[spos];
+            taps = s_taps[spos];
+            Bw[0] = Bw[0] + f1.x; Bw[4] = Bw[4] + f1.y;
+            Bw[1] = Bw[1] + f1.x; Bw[5] = Bw[5] + f1.y;
+            Bw[2] = Bw[2] + f1.x; Bw[6] = Bw[6] + f1.y;
+            Bw[3] = Bw[3] + f1.x; Bw[7] = Bw[7] + f1.y;
+            st = msd[d];
+            f1.x = snr_of(Bw[0], st);
+            f1.y = snr_of(Bw[4], st);
+            st = msd[d + 1];
+            f2.x = snr_of(Bw[1], st);
+            f2.y = snr_of(Bw[5], st);
+            if (f2.x > f1.x) { f1.x = f2.x; taps1.x = d + 2; } else taps1.x = d + 1;
+            if (f2.y > f1.y) { f1.y = f2.y; taps1.y = d + 2; } else taps1.y = d + 1;
+            st = msd[d + 2];
+            f2.x = snr_of(Bw[2], st);
+            f2.y = snr_of(Bw[6], st);
+            st = msd[d + 3];
+            f3.x = snr_of(Bw[3], st);
+            f3.y = snr_of(Bw[7], st);
+            if (f3.x > f2.x) { f2.x = f3.x; taps2.x = d + 4; } else taps2.x = d + 3;
+            if (f3.y > f2.y) { f2.y = f3.y; taps2.y = d + 4; } else taps2.y = d + 3;
+            if (f2.x > f1.x) { f1.x = f2.x; taps1.x = taps2.x; }
+            if (f2.y > f1.y) { f1.y = f2.y; taps1.y = taps2.y; }
+            if (f1.x > SNR.x) { SNR.x = f1.x; taps.x = taps1.x; }
+            if (f1.y > SNR.y) { SNR.y = f1.y; taps.y = taps1.y; }
+            s_snr[spos] = SNR;
+            s_taps[spos] = taps;
+        }
+    }
+    if (spos >= 0)
+        s_in[spos].x = Bw[3];
+    __syncthreads();
+    spos = blockIdx.x * (2 * SPD_NTHREADS - nBoxcars) + 2 * t;
+    if (t < (SPD_NTHREADS - (nBoxcars >> 1)) && spos < nT) {
+        const long long g = row + spos;
+        snr_out[g] = s_snr[t].x;
+        snr_out[g + 1] = s_snr[t].y;
+        taps_out[g] = s_taps[t].x;
+        taps_out[g + 1] = s_taps[t].y;
+        spos = blockIdx.x * (SPD_NTHREADS - (nBoxcars >> 1)) + t;
+        if (spos < dtm)
+            bv_out[static_cast<long long>(blockIdx.y) * dtm + spos] = s_in[t].x;
+    }
+}
+
+// Later iterations: the input is the previous iteration's 2-sample sums, and
+// the running boxcar values of the previous widths (bv_in) are added in front.
+__global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_nth(const float *__restrict__ in, const float *bv_in,
+                                                           float *bv_out, float *dec, float *snr_out,
+                                                           uint16_t *taps_out, const float2 *__restrict__ msd, int nT,
+                                                           int nBoxcars, int startTaps, int dit_value, int dtm)
+{
+    __shared__ float2 s_in[SPD_NTHREADS];
+    __shared__ float2 s_bv[SPD_NTHREADS];
+    __shared__ float2 s_snr[SPD_NTHREADS];
+    __shared__ ushort2 s_taps[SPD_NTHREADS];
+    const int t = threadIdx.x;
+    float Bw[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    float2 f1, f2, f3, SNR;
+    ushort2 taps, taps1, taps2;
+    s_bv[t].x = 0;
+    s_bv[t].y = 0;
+    int spos = blockIdx.x * (2 * SPD_NTHREADS - nBoxcars) + 2 * t;
+    const long long row = static_cast<long long>(blockIdx.y) * nT;
+    if ((spos + 4) < nT) {
+        const long long g = row + spos;
+        f1.x = in[g];
+        f1.y = in[g + 1];
+        f2.x = in[g + 2];
+        f2.y = in[g + 3];
+        f3.x = in[g + 4];
+        Bw[0] = f1.x;
+        Bw[4] = f1.y;
+        Bw[1] = f1.x + f1.y;
+        Bw[5] = f1.y + f2.x;
+        Bw[2] = Bw[1] + f2.x;
+        Bw[6] = Bw[5] + f2.y;
+        Bw[3] = Bw[1] + f2.x + f2.y;
+        Bw[7] = Bw[5] + f2.y + f3.x;
+        s_bv[t].x = bv_in[g];
+        s_bv[t].y = bv_in[g + 1];
+    }
+    spos = blockIdx.x * (SPD_NTHREADS - (nBoxcars >> 1)) + t;
+    if (t < (SPD_NTHREADS - (nBoxcars >> 1)) && spos < dtm)
+        dec[static_cast<long long>(blockIdx.y) * dtm + spos] = Bw[1];
+    s_in[t].x = Bw[3];
+    s_in[t].y = Bw[7];
+    SNR.x = 0;
+    SNR.y = 0;
+    __syncthreads();
+    float2 st = msd[0];
+    f1.x = snr_of_bv(s_bv[t].x, Bw[0], st);
+    f1.y = snr_of_bv(s_bv[t].y, Bw[4], st);
+    st = msd[1];
+    f2.x = snr_of_bv(s_bv[t].x, Bw[1], st);
+    f2.y = snr_of_bv(s_bv[t].y, Bw[5], st);
+    if (f2.x > f1.x) { f1.x = f2.x; taps1.x = 2; } else taps1.x = 1;
+    if (f2.y > f1.y) { f1.y = f2.y; taps1.y = 2; } else taps1.y = 1;
+    st = msd[2];
+    f2.x = snr_of_bv(s_bv[t].x, Bw[2], st);
+    f2.y = snr_of_bv(s_bv[t].y, Bw[6], st);
+    st = msd[3];
+    f3.x = snr_of_bv(s_bv[t].x, Bw[3], st);
+    f3.y = snr_of_bv(s_bv[t].y, Bw[7], st);
+    if (f3.x > f2.x) { f2.x = f3.x; taps2.x = 4; } else taps2.x = 3;
+    if (f3.y > f2.y) { f2.y = f3.y; taps2.y = 4; } else taps2.y = 3;
+    if (f1.x > f2.x) { SNR.x = f1.x; taps.x = taps1.x; } else { SNR.x = f2.x; taps.x = taps2.x; }
+    if (f1.y > f2.y) { SNR.y = f1.y; taps.y = taps1.y; } else { SNR.y = f2.y; taps.y = taps2.y; }
+    s_snr[t] = SNR;
+    s_taps[t] = taps;
+    for (int d = 4; d < nBoxcars; d += 4) {
+        __syncthreads();
+        spos = t - (d >> 1);
+        if (spos >= 0) {
+            f1 = s_in[spos];
+            SNR = s_snr[spos];
+            taps = s_taps[spos];
+            Bw[0] = Bw[0] + f1.x; Bw[4] = Bw[4] + f1.y;
+            Bw[1] = Bw[1] + f1.x; Bw[5] = Bw[5] + f1.y;
+            Bw[2] = Bw[2] + f1.x; Bw[6] = Bw[6] + f1.y;
+            Bw[3] = Bw[3] + f1.x; Bw[7] = Bw[7] + f1.y;
+            st = msd[d];
+            f1.x = snr_of_bv(s_bv[spos].x, Bw[0], st);
+            f1.y = snr_of_bv(s_bv[spos].y, Bw[4], st);
+            st = msd[d + 1];
+            f2.x = snr_of_bv(s_bv[spos].x, Bw[1], st);
+            f2.y = snr_of_bv(s_bv[spos].y, Bw[5], st);
+            if (f2.x > f1.x) { f1.x = f2.x; taps1.x = d + 2; } else taps1.x = d + 1;
+            if (f2.y > f1.y) { f1.y = f2.y; taps1.y = d + 2; } else taps1.y = d + 1;
+            st = msd[d + 2];
+            f2.x = snr_of_bv(s_bv[spos].x, Bw[2], st);
+            f2.y = snr_of_bv(s_bv[spos].y, Bw[6], st);
+            st = msd[d + 3];
+            f3.x = snr_of_bv(s_bv[spos].x, Bw[3], st);
+            f3.y = snr_of_bv(s_bv[spos].y, Bw[7], st);
+            if (f3.x > f2.x) { f2.x = f3.x; taps2.x = d + 4; } else taps2.x = d + 3;
+            if (f3.y > f2.y) { f2.y = f3.y; taps2.y = d + 4; } else taps2.y = d + 3;
+            if (f2.x > f1.x) { f1.x = f2.x; taps1.x = taps2.x; }
+            if (f2.y > f1.y) { f1.y = f2.y; taps1.y = taps2.y; }
+            if (f1.x > SNR.x) { SNR.x = f1.x; taps.x = taps1.x; }
+            if (f1.y > SNR.y) { SNR.y = f1.y; taps.y = taps1.y; }
+            s_snr[spos] = SNR;
+            s_taps[spos] = taps;
+        }
+    }
+    if (spos >= 0)
+        s_in[spos].x = s_bv[spos].x + Bw[3];
+    __syncthreads();
+    spos = blockIdx.x * (2 * SPD_NTHREADS - nBoxcars) + 2 * t;
+    if (t < (SPD_NTHREADS - (nBoxcars >> 1)) && spos < nT) {
+        const long long g = row + spos;
+        snr_out[g] = s_snr[t].x;
+        snr_out[g + 1] = s_snr[t].y;
+        taps_out[g] = startTaps + s_taps[t].x * dit_value;
+        taps_out[g + 1] = startTaps + s_taps[t].y * dit_value;
+        spos = blockIdx.x * (SPD_NTHREADS - (nBoxcars >> 1)) + t;
+        if (spos < dtm)
+            bv_out[static_cast<long long>(blockIdx.y) * dtm + spos] = s_in[t].x;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Candidates.  Peak finding (src/aa_device_peak_find_kernel.cu:72-156 with
+// include/aa_device_peak_find_shared_kernel_functions.cuh): a sample is a
+// candidate when it is above the cut and equal to the maximum of its
+// neighbourhood -- 3 x 3 inside, the rows or columns that exist at the
+// edges, 2 x 2 at the corners, where the last processed column
+// (width - offset - 1) counts as the right edge.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float max_rows(const float *in, int x0, int x1, int y0, int y1, int width)
+{
+    // same maximum as the reference's fmaxf chains (order does not matter
+    // for fmaxf except with NaN, which the planes do not hold)
+    float m = __ldg(in + static_cast<long long>(y0) * width + x0);
+    for (int y = y0; y <= y1; ++y)
+        for (int x = x0; x <= x1; ++x)
+            m = fmaxf(m, __ldg(in + static_cast<long long>(y) * width + x));
+    return m;
+}
+
+__global__ void k_peak_find(const float *__restrict__ in, const uint16_t *__restrict__ taps, unsigned *c_dm,
+                            unsigned *c_ts, float *c_snr, unsigned *c_bw, int width, int height, int offset,
+                            float threshold, int max_cands, int *count, int shift, int dit_value)
+{
+    const int x = blockDim.x * blockIdx.x + threadIdx.x;
+    const int y = blockDim.y * blockIdx.y + threadIdx.y;
+    if (x >= width - offset || y >= height)
+        return;
+    const int last = width - offset - 1;
+    float my, dil;
+    if (width == 1 && (y == 0 || y == height - 1)) {
+        my = dil = in[static_cast<long long>(y) * width];
+    } else if ((y == 0 || y == height - 1) && (x == 0 || x == last)) {
+        const int xa = (x == 0) ? 0 : width - offset - 2;
+        const int ya = (y == 0) ? 0 : height - 2;
+        dil = max_rows(in, xa, xa + 1, ya, ya + 1, width);
+        my = __ldg(in + static_cast<long long>(y) * width + x);
+    } else {
+        const int x0 = (x == 0) ? x : x - 1, x1 = (x == last) ? x : x + 1;
+        const int y0 = (y == 0) ? y : y - 1, y1 = (y == height - 1) ? y : y + 1;
+        dil = max_rows(in, x0, x1, y0, y1, width);
+        my = __ldg(in + static_cast<long long>(y) * width + x);
+    }
+    if (my > threshold && my == dil) {
+        const int pos = atomicAdd(count, 1);
+        if (pos < max_cands) {
+            const unsigned tp = taps[static_cast<long long>(y) * width + x];
+            c_dm[pos] = y + shift;
+            c_ts[pos] = x * dit_value + tp / 2;
+            c_snr[pos] = my;
+            c_bw[pos] = tp;
+        }
+    }
+}
+
+// Thresholding (src/aa_device_threshold_kernel.cu:10-41): every sample of
+// the rows 0 .. 4*floor(nDMs/4)-1 and columns < offset above the cut.
+__global__ void k_threshold(const float *__restrict__ in, const uint16_t *__restrict__ taps, unsigned *c_dm,
+                            unsigned *c_ts, float *c_snr, unsigned *c_bw, int *count, float threshold, int nT,
+                            int offset, int shift, int max_cands, int dit_value)
+{
+    const int y = blockIdx.y;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= offset)
+        return;
+    const float R = __ldg(in + static_cast<long long>(y) * nT + x);
+    if (R > threshold) {
+        const int pos = atomicAdd(count, 1);
+        if (pos < max_cands) {
+            const unsigned tp = taps[static_cast<long long>(y) * nT + x];
+            c_dm[pos] = y + shift;
+            c_ts[pos] = dit_value * x + tp / 2;
+            c_snr[pos] = R;
+            c_bw[pos] = tp;
+        }
+    }
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+MsdConf msd_conf(long long nTimesamples, long long nDMs, long long offset)
+{
+    // include/aa_device_MSD_Configuration.hpp:33-99
+    MsdConf c{};
+    c.nTimesamples = nTimesamples;
+    c.nDMs = nDMs;
+    c.offset = offset;
+    const int nsx = SPD_NTHREADS;
+    c.nBlocks_x = static_cast<int>((nTimesamples - offset) / nsx);
+    if ((nTimesamples - offset) - static_cast<long long>(c.nBlocks_x) * nsx > 0)
+        c.nBlocks_x++;
+    // largest product of small prime factors of nDMs not above 64
+    {
+        const int seive[12] = {2, 3, 4, 5, 7, 11, 13, 17, 19, 23, 29, 31};
+        int number = static_cast<int>(nDMs), N = 1, N_accepted = 1;
+        do {
+            N = 1;
+            for (int f = 0; f < 12; ++f) {
+                const int nb = number / seive[f];
+                if (number - nb * seive[f] == 0) {
+                    N = seive[f];
+                    N_accepted *= N;
+                    break;
+                }
+            }
+            number /= N;
+        } while (N_accepted <= 64 && N > 1);
+        c.nSteps_y = N_accepted / N;
+    }
+    c.nBlocks_y = static_cast<int>(nDMs / c.nSteps_y);
+    c.nBlocks_total = c.nBlocks_x * c.nBlocks_y;
+    int nThreads = 2048, itemp = 0;
+    while (itemp == 0 && nThreads > 32) {
+        nThreads >>= 1;
+        itemp = c.nBlocks_total / (nThreads * 32);
+    }
+    c.final_threads = nThreads < 32 ? 32 : nThreads;
+    return c;
+}
+
+cudaError_t msd_plane(float *d_msd, const float *d_input, float *d_partials, const MsdConf &c, bool outlier_rejection,
+                      float sigma, float *d_pp, cudaStream_t st)
+{
+    if (c.nBlocks_x < 1 || c.nBlocks_y < 1)
+        return cudaErrorInvalidValue;
+    const dim3 grid(c.nBlocks_x, c.nBlocks_y);
+    if (!outlier_rejection) {
+        k_msd_partials<<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_partials, c.nSteps_y, c.nTimesamples, c.offset);
+        ++g_spd_launches;
+        k_msd_final<<<1, c.final_threads, 0, st>>>(d_partials, d_msd, d_pp, c.nBlocks_total, 1);
+        ++g_spd_launches;
+        return cudaGetLastError();
+    }
+    // src/aa_device_MSD.cu:110-196
+    k_msd_partials_minmax<<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_partials, c.nSteps_y, c.nTimesamples, c.offset);
+    ++g_spd_launches;
+    k_msd_final<<<1, c.final_threads, 0, st>>>(d_partials, d_msd, nullptr, c.nBlocks_total, 1);
+    ++g_spd_launches;
+    for (int i = 0; i < 5; ++i) {
+        k_msd_partials_rejection<<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_partials, d_msd, c.nSteps_y, c.nTimesamples,
+                                                                c.offset, sigma);
+        ++g_spd_launches;
+        k_msd_final<<<1, c.final_threads, 0, st>>>(d_partials, d_msd, nullptr, c.nBlocks_total, 0);
+        ++g_spd_launches;
+    }
+    if (d_pp) {
+        k_msd_final<<<1, c.final_threads, 0, st>>>(d_partials, d_msd, d_pp, c.nBlocks_total, 0);
+        ++g_spd_launches;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t dit_pairs(const float *d_in, float *d_out, int nDMs, int nT, cudaStream_t st)
+{
+    const long long dts = nT >> 1;
+    if (dts == 0)
+        return cudaErrorInvalidValue;
+    const int rows = (nDMs / 2) * 2;
+    if (rows == 0)
+        return cudaSuccess;
+    k_dit_pairs<<<dim3(static_cast<unsigned>((dts + 255) / 256), rows), 256, 0, st>>>(d_in, d_out, rows, nT, dts);
+    ++g_spd_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t fir_rows(const float *d_in, float *d_out, int nDMs, int nT, int nTaps, cudaStream_t st)
+{
+    const int n = nT - nTaps + 1;
+    if (n <= 0 || nDMs <= 0)
+        return cudaErrorInvalidValue;
+    k_fir_rows<<<dim3((n + 255) / 256, nDMs), 256, 0, st>>>(d_in, d_out, nTaps, nT);
+    ++g_spd_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t msd_interpolate(const float *d_msd_dit, float *d_msd_interp, const int *d_dit_widths, int n_dit,
+                            const int *d_widths, int n_widths, int max_width_performed, cudaStream_t st)
+{
+    if (n_widths < 1 || n_widths > 1024)
+        return cudaErrorInvalidValue;
+    k_msd_interpolate<<<1, n_widths, 0, st>>>(d_msd_dit, d_msd_interp, d_dit_widths, n_dit, d_widths,
+                                              max_width_performed);
+    ++g_spd_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t spdt_first_plane(const float *d_input, float *d_bv_out, float *d_decimated, float *d_snr, uint16_t *d_taps,
+                             const float2 *d_msd, int nTimesamples, int nBoxcars, int dtm, int nBlocks, int nDMs,
+                             cudaStream_t st)
+{
+    if (nBlocks <= 0)
+        return cudaSuccess;
+    k_spdt_first<<<dim3(nBlocks, nDMs), SPD_NTHREADS, 0, st>>>(d_input, d_bv_out, d_decimated, d_snr, d_taps, d_msd,
+                                                               nTimesamples, nBoxcars, dtm);
+    ++g_spd_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t spdt_nth_plane(const float *d_input, const float *d_bv_in, float *d_bv_out, float *d_decimated,
+                           float *d_snr, uint16_t *d_taps, const float2 *d_msd, int nTimesamples, int nBoxcars,
+                           int startTaps, int dit_value, int dtm, int nBlocks, int nDMs, cudaStream_t st)
+{
+    if (nBlocks <= 0)
+        return cudaSuccess;
+    k_spdt_nth<<<dim3(nBlocks, nDMs), SPD_NTHREADS, 0, st>>>(d_input, d_bv_in, d_bv_out, d_decimated, d_snr, d_taps,
+                                                             d_msd, nTimesamples, nBoxcars, startTaps, dit_value, dtm);
+    ++g_spd_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t spd_peak_find(const float *d_snr, const uint16_t *d_taps, unsigned *d_dm, unsigned *d_ts, float *d_csnr,
+                          unsigned *d_bw, int width, int height, int offset, float threshold, int max_cands,
+                          int *d_count, int shift, int dit_value, cudaStream_t st)
+{
+    if (width - offset - 1 <= 0)
+        return cudaSuccess;
+    const dim3 block(32, 2);
+    const dim3 grid(1 + (width - offset - 1) / 32, 1 + (height - 1) / 2);
+    k_peak_find<<<grid, block, 0, st>>>(d_snr, d_taps, d_dm, d_ts, d_csnr, d_bw, width, height, offset, threshold,
+                                        max_cands, d_count, shift, dit_value);
+    ++g_spd_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t spd_threshold(const float *d_snr, const uint16_t *d_taps, unsigned *d_dm, unsigned *d_ts, float *d_csnr,
+                          unsigned *d_bw, int *d_count, float threshold, int nTimesamples, int offset, int shift,
+                          int max_cands, int dit_value, int nDMs, cudaStream_t st)
+{
+    const int rows = (nDMs / 4) * 4;
+    if (offset <= 0 || rows == 0)
+        return cudaSuccess;
+    // the reference's blocks cover 128 columns each; columns >= offset are skipped
+    const int nb = (offset + 127) / 128;
+    k_threshold<<<dim3(nb * 4, rows), 32, 0, st>>>(d_snr, d_taps, d_dm, d_ts, d_csnr, d_bw, d_count, threshold,
+                                                   nTimesamples, offset, shift, max_cands, dit_value);
+    ++g_spd_launches;
+    return cudaGetLastError();
+}
+
+} // namespace aab200

@@ -439,6 +439,59 @@ int aa_b200_sps_block_peaks(const float *d_y, int nrows, long long pitch, long l
                             int *d_peak_w, void *stream);
 int aa_b200_sps_block_samples(void);
 
+/* ---------------------------------------------------------------------------
+ * Single-pulse detection with the reference's own rules: analysis_GPU
+ * (src/aa_device_analysis.cu:130-345) on one DM-time plane [nDMs][nT] of
+ * float32 in device memory, for candidate algorithms 0 (peak finding) and 1
+ * (thresholding).  The MSD profile (src/aa_device_MSD_plane_profile.cu), the
+ * boxcar S/N planes (src/aa_device_SPS_long.cu:32-80) and the candidate
+ * lists are bit-identical to the reference's; the order of the candidates
+ * inside one batch follows the GPU's atomics, as in the reference.
+ *
+ * create: buffers for planes of up to max_elems elements; the search takes
+ * the DM trials in batches of floor(max_time_samples / nT), rounded down to
+ * a multiple of 4 (the reference's maxTimeSamples of
+ * include/aa_analysis_strategy.hpp:209-258; 0 = the whole plane).  The work
+ * area starts zeroed; samples the reference's kernels read without writing
+ * them first come from it.  clear zeroes it again.
+ * run: tsamp is the range's sampling time (the data's tsamp times inBin, as
+ * float), the settings those of aa_analysis_plan
+ * (include/aa_analysis_plan.hpp:36-47).  The plane is overwritten (the
+ * reference's search decimates into it).  Candidates -- DM trial index,
+ * sample, S/N, boxcar width in samples of the range -- go to the host arrays
+ * of max_candidates entries; a batch whose candidates would reach
+ * max_candidates is dropped whole, as in the reference
+ * (src/aa_device_analysis.cu:319-354).  Returns 0, or 1 with a message in
+ * aa_b200_spd_last_error.  stream: cudaStream_t as void*, 0 = the legacy
+ * stream; run returns after the candidates are on the host.
+ * --------------------------------------------------------------------------- */
+void *aa_b200_spd_create(long long max_elems, long long max_time_samples);
+void aa_b200_spd_destroy(void *obj);
+/* obj == NULL: the message of the last failed create or write */
+const char *aa_b200_spd_last_error(const void *obj);
+int aa_b200_spd_clear(void *obj, void *stream);
+int aa_b200_spd_run(void *obj, float *d_plane, int nDMs, int nTimesamples, float tsamp, int inBin,
+                    float sigma_cutoff, float sigma_constant, float max_boxcar_width_in_sec, int candidate_algorithm,
+                    int enable_msd_baseline_noise, void *stream, size_t max_candidates, unsigned *h_dm,
+                    unsigned *h_ts, float *h_snr, unsigned *h_bw, size_t *n_candidates);
+/* The plan and the interpolated (mean, deviation) per boxcar width of the
+ * last run: widths[msd_cap], msd[2 * msd_cap]; dropped_batches counts the
+ * batches dropped for max_candidates. */
+int aa_b200_spd_profile(const void *obj, float *msd, int msd_cap, int *widths, int *nwidths,
+                        int *max_width_performed, int *max_iteration, int *dropped_batches);
+/* on != 0: run keeps the S/N and width planes of its last batch (2 * batch
+ * elements each, the reference's d_output_SNR and d_output_taps), which
+ * aa_b200_spd_planes copies out when cap is large enough; returns their
+ * length. */
+int aa_b200_spd_keep_planes(void *obj, int on);
+long long aa_b200_spd_planes(const void *obj, float *snr, unsigned short *taps, long long cap);
+long long aa_b200_spd_kernel_launches(void);
+/* The candidate file of src/aa_device_analysis.cu:420-466 (float records
+ * DM, time, S/N, width) under dir; returns 0 or 1. */
+int aa_b200_spd_write_candidates(const char *dir, int candidate_algorithm, float tstart, float dm_low, float dm_high,
+                                 float dm_step, float tsamp, int inBin, const unsigned *dm, const unsigned *ts,
+                                 const float *snr, const unsigned *bw, size_t n);
+
 #ifdef __cplusplus
 }
 #endif

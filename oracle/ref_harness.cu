@@ -17,6 +17,12 @@
  *   aaref_export_dd_data() writes DM-time files with the reference's
  *                     Export_DD_data (include/aa_pipeline_runner.hpp:165-216)
  *                     through a runner that only exposes it.  No GPU.
+ *   aaref_spd()       the reference's single-pulse detection on one DM-time
+ *                     plane: the stages of analysis_GPU
+ *                     (src/aa_device_analysis.cu:130-245) one by one -- the
+ *                     interpolated MSD profile, the boxcar S/N and width planes
+ *                     -- and then analysis_GPU itself for the candidates.
+ *                     Needs a GPU.
  *   aaref_sigproc_read() reads a SIGPROC file with the reference's
  *                     aa_sigproc_input (src/aa_sigproc_input.cpp:85-543):
  *                     metadata and the unsigned-short input buffer.  No GPU.
@@ -38,6 +44,17 @@
 #include "aa_permitted_pipelines_generic.hpp"
 #include "aa_pipeline.hpp"
 #include "aa_sigproc_input.hpp"
+#include "aa_device_analysis.hpp"
+#include "aa_device_BC_plan.hpp"
+#include "aa_device_MSD_plane_profile.hpp"
+#include "aa_device_SPS_long.hpp"
+
+namespace astroaccelerate {
+/* defined in src/aa_device_analysis.cu without a header declaration */
+void Create_list_of_boxcar_widths(std::vector<int> *boxcar_widths, std::vector<int> *BC_widths, int max_boxcar_width);
+void Create_PD_plan(std::vector<PulseDetection_plan> *PD_plan, std::vector<int> *BC_widths, int nDMs, int nTimesamples);
+int Get_max_iteration(int max_boxcar_width, std::vector<int> *BC_widths, int *max_width_performed);
+} // namespace astroaccelerate
 
 using namespace astroaccelerate;
 
@@ -249,6 +266,107 @@ int aaref_time_ddtr(const unsigned short *input_tc, int nchans, int nsamp, doubl
         *seconds = std::chrono::duration<double>(t1 - t0).count();
     }
     return 0;
+}
+
+/* plane: host [nDMs][nT] float.  Outputs (caller-sized): msd [2 * nwidths]
+ * (nwidths <= 256) and widths [nwidths]; snr/taps: the whole S/N and width
+ * planes SPDT writes (plane_cap elements, at least 2 * nDMs * nT); the
+ * candidates of analysis_GPU (max_cands).  Returns 0, or < 0 on a failure. */
+int aaref_spd(const float *plane, int nDMs, int nT, float tsamp, int inBin, float max_boxcar_width_in_sec,
+              float sigma_constant, int enable_msd_baseline_noise, float cutoff, int candidate_algorithm, float tstart,
+              float dm_low, float dm_high, float dm_step, float *msd, int *widths, int *nwidths, int *max_width_performed,
+              int *max_iteration, float *snr, unsigned short *taps, long long plane_cap, unsigned *c_dm, unsigned *c_ts,
+              float *c_snr, unsigned *c_bw, int max_cands, int *ncands)
+{
+    const size_t n = (size_t)nDMs * (size_t)nT;
+    if ((long long)(2 * n) > plane_cap)
+        return -1;
+    /* the plan analysis_GPU builds (:138-179) */
+    int max_boxcar_width = (int)(max_boxcar_width_in_sec / tsamp);
+    int mwp = 0;
+    int t_BC_widths[10] = {PD_MAXTAPS, 16, 16, 16, 8, 8, 8, 8, 8, 8};
+    std::vector<int> BC_widths(t_BC_widths, t_BC_widths + 10);
+    std::vector<PulseDetection_plan> PD_plan;
+    int max_it = Get_max_iteration(max_boxcar_width / inBin, &BC_widths, &mwp);
+    Create_PD_plan(&PD_plan, &BC_widths, 1, nT);
+    std::vector<int> h_boxcar_widths;
+    Create_list_of_boxcar_widths(&h_boxcar_widths, &BC_widths, mwp);
+    *max_width_performed = mwp;
+    *max_iteration = max_it;
+    *nwidths = (int)h_boxcar_widths.size();
+    if (*nwidths > 256)
+        return -2;
+    for (int i = 0; i < *nwidths; i++)
+        widths[i] = h_boxcar_widths[i];
+
+    /* buffers as the runner sizes them for maxTimeSamples = nDMs * nT
+     * (include/aa_permitted_pipelines_generic.hpp:391-412) */
+    unsigned long int maxTS = (unsigned long int)n;
+    float *d_plane = NULL, *d_work = NULL, *d_msd = NULL;
+    unsigned short *d_taps = NULL;
+    size_t msd_bytes = 0, dit_bytes = 0, work_bytes = 0;
+    Get_MSD_plane_profile_memory_requirements(&msd_bytes, &dit_bytes, &work_bytes, nT, nDMs, &h_boxcar_widths);
+    if (cudaMalloc((void **)&d_plane, n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_work, maxTS * 5.5 * sizeof(float) + work_bytes) != cudaSuccess ||
+        cudaMalloc((void **)&d_taps, 2 * maxTS * sizeof(unsigned short)) != cudaSuccess ||
+        cudaMalloc((void **)&d_msd, msd_bytes + 4096) != cudaSuccess)
+        return -3;
+    int rc = 0;
+    /* stage 1: MSD plane profile (:199) */
+    cudaMemcpy(d_plane, plane, n * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemset(d_work, 0, maxTS * 5.5 * sizeof(float));
+    double t0, t1, t2;
+    MSD_plane_profile(d_msd, d_plane, NULL, d_work, false, nT, nDMs, &h_boxcar_widths, tstart, dm_low, dm_high,
+                      sigma_constant, enable_msd_baseline_noise, false, &t0, &t1, &t2);
+    cudaMemcpy(msd, d_msd, 2 * (*nwidths) * sizeof(float), cudaMemcpyDeviceToHost);
+    /* stage 2: the boxcar planes of one DM batch (:206-253) */
+    {
+        size_t mem_idx = 0;
+        int DMs_per_cycle = nDMs;
+        mem_idx += 4 * ((size_t)nT * DMs_per_cycle) / 4;
+        float *d_decimated = &d_work[mem_idx];
+        mem_idx += ((size_t)DMs_per_cycle * nT) / 2 + PD_MAXTAPS;
+        float *d_boxcar_values = &d_work[mem_idx];
+        mem_idx += (size_t)DMs_per_cycle * nT;
+        float *d_output_SNR = &d_work[mem_idx];
+        cudaMemset(d_output_SNR, 0, 2 * n * sizeof(float));
+        cudaMemset(d_taps, 0, 2 * n * sizeof(unsigned short));
+        SPDT_search_long_MSD_plane(d_plane, d_boxcar_values, d_decimated, d_output_SNR, d_taps, d_msd, &PD_plan, max_it,
+                                   nT, nDMs);
+        cudaMemcpy(snr, d_output_SNR, 2 * n * sizeof(float), cudaMemcpyDeviceToHost);
+        cudaMemcpy(taps, d_taps, 2 * n * sizeof(unsigned short), cudaMemcpyDeviceToHost);
+    }
+    /* stage 3: analysis_GPU on a fresh copy of the plane */
+    {
+        cudaMemcpy(d_plane, plane, n * sizeof(float), cudaMemcpyHostToDevice);
+        size_t peak_pos = 0;
+        int ndms_arr[1] = {nDMs};
+        int maxshift = 0;
+        float lo[1] = {dm_low}, hi[1] = {dm_high}, st[1] = {dm_step};
+        analysis_output out;
+        std::vector<unsigned> a(max_cands), b(max_cands), d(max_cands);
+        std::vector<float> c(max_cands);
+        bool ok = analysis_GPU(a.data(), b.data(), c.data(), d.data(), &peak_pos, (size_t)max_cands, 0, tstart, nT,
+                               inBin, &maxshift, nDMs, ndms_arr, cutoff, sigma_constant, max_boxcar_width_in_sec,
+                               d_plane, lo, hi, st, tsamp, candidate_algorithm, d_work, d_taps, d_msd, maxTS,
+                               enable_msd_baseline_noise, false, false, out);
+        if (!ok)
+            rc = -4;
+        *ncands = (int)peak_pos;
+        for (size_t k = 0; k < peak_pos && (int)k < max_cands; k++) {
+            c_dm[k] = a[k];
+            c_ts[k] = b[k];
+            c_snr[k] = c[k];
+            c_bw[k] = d[k];
+        }
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess)
+        rc = -5;
+    cudaFree(d_plane);
+    cudaFree(d_work);
+    cudaFree(d_taps);
+    cudaFree(d_msd);
+    return rc;
 }
 
 namespace {

@@ -1,0 +1,41 @@
+"""Seeded DM-time planes for the single-pulse detection tests: Gaussian
+noise with dispersed pulses (a peak at one DM trial and sample, falling off
+over neighbouring trials and widening with DM distance), and the analysis
+settings of each run."""
+from __future__ import annotations
+
+import numpy as np
+
+# name -> plane shape, plane seed, settings
+CASES = {
+    "small_peak": dict(ndms=64, nt=16384, seed=1, tsamp=64e-6, inbin=1, max_width_s=0.004, sigma_constant=3.0,
+                       baseline_noise=0, cutoff=6.0, algorithm=0),
+    "small_threshold": dict(ndms=64, nt=16384, seed=1, tsamp=64e-6, inbin=1, max_width_s=0.004, sigma_constant=3.0,
+                            baseline_noise=0, cutoff=6.0, algorithm=1),
+    "wide_outliers_peak": dict(ndms=128, nt=32768, seed=2, tsamp=64e-6, inbin=1, max_width_s=0.016,
+                               sigma_constant=3.0, baseline_noise=1, cutoff=6.0, algorithm=0),
+    "binned_outliers": dict(ndms=64, nt=16384, seed=3, tsamp=128e-6, inbin=2, max_width_s=0.02, sigma_constant=2.5,
+                            baseline_noise=1, cutoff=5.5, algorithm=0),
+    "very_wide_threshold": dict(ndms=64, nt=65536, seed=4, tsamp=64e-6, inbin=1, max_width_s=0.065,
+                                sigma_constant=3.0, baseline_noise=0, cutoff=7.0, algorithm=1),
+}
+
+
+def make_plane(case) -> np.ndarray:
+    rng = np.random.Generator(np.random.PCG64(case["seed"]))
+    nd, nt = case["ndms"], case["nt"]
+    x = rng.normal(100.0, 4.0, (nd, nt)).astype(np.float32)
+    t_idx = np.arange(nt)
+    for k in range(6):
+        d0 = int(rng.integers(4, nd - 4))
+        t0 = int(rng.integers(100, nt - 2000))
+        w = float(rng.uniform(1.0, 60.0))
+        amp = float(rng.uniform(3.0, 12.0))
+        for d in range(nd):
+            dd = abs(d - d0)
+            ww = w + 3.0 * dd
+            a = amp * np.exp(-0.5 * (dd / 3.0) ** 2) * np.sqrt(w / ww)
+            if a < 0.05:
+                continue
+            x[d] += (a * np.exp(-0.5 * ((t_idx - t0) / ww) ** 2)).astype(np.float32)
+    return x

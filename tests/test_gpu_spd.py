@@ -1,0 +1,123 @@
+"""Single-pulse detection (the reference's analysis_GPU,
+src/aa_device_analysis.cu:130-345) on the GPU through the C ABI, against the
+reference's own GPU run on the same seeded planes
+(tests/golden/spd_golden.json from tests/golden/make_spd_golden.py):
+
+* the plan (boxcar widths, widest width, iterations),
+* the interpolated mean and deviation per boxcar width, bit for bit,
+* the boxcar S/N and width planes of the search (sha256 of the
+  reference's d_output_SNR and d_output_taps), bit for bit,
+* the candidate lists (DM trial, sample, S/N bits, width), as sets: their
+  order inside a batch follows the GPU's atomics in both implementations.
+
+Like the reference's harness, the first run starts on a zeroed work area
+(planes compared), the second on a fresh copy of the plane without clearing
+(candidates compared)."""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import spd_cases as S
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "spd_golden.json")
+
+
+@pytest.fixture(scope="module")
+def golden():
+    with open(GOLDEN) as f:
+        return json.load(f)["runs"]
+
+
+def cand_key(r):
+    snr_bits = r["snr"].view(np.uint32)
+    return sorted((int(r["dm"][j]), int(r["ts"][j]), int(snr_bits[j]), int(r["bw"][j])) for j in range(r["dm"].size))
+
+
+def run_case(aa, c, max_ts=0, clear=True, keep=True, spd=None):
+    import torch
+    x = S.make_plane(c)
+    if spd is None:
+        spd = aa.single_pulse_detection(x.size, max_ts)
+    spd.keep_planes(keep)
+    if clear:
+        spd.clear()
+    d = torch.from_numpy(x).cuda()
+    tsamp_r = float(np.float32(c["tsamp"] * c["inbin"]))
+    r = spd.run(d, c["ndms"], c["nt"], tsamp_r, c["inbin"], c["cutoff"], c["sigma_constant"], c["max_width_s"],
+                c["algorithm"], bool(c["baseline_noise"]))
+    torch.cuda.synchronize()
+    return spd, r
+
+
+@pytest.mark.parametrize("name", list(S.CASES))
+def test_spd_matches_reference(aa, golden, name):
+    c = S.CASES[name]
+    g = golden[name]
+    assert g["rc"] == 0
+    launches0 = aa.spd_kernel_launches()
+    spd, r1 = run_case(aa, c)
+    assert aa.spd_kernel_launches() > launches0
+    prof = spd.profile()
+    assert prof["widths"].tolist() == g["widths"]
+    assert prof["max_width_performed"] == g["max_width_performed"]
+    assert prof["max_iteration"] == g["max_iteration"]
+    assert prof["msd"].view(np.uint32).tolist() == g["msd_bits"]
+    snr, taps = spd.planes()
+    assert snr.size == 2 * c["ndms"] * c["nt"]
+    assert hashlib.sha256(snr.tobytes()).hexdigest() == g["snr_sha256"]
+    assert hashlib.sha256(taps.tobytes()).hexdigest() == g["taps_sha256"]
+    # second run: the work area as the first left it, as in the reference's third stage
+    _, r2 = run_case(aa, c, clear=False, keep=False, spd=spd)
+    cands = cand_key(r2)
+    assert len(cands) == g["ncands"]
+    assert [list(t) for t in cands[:64]] == g["cands_head"]
+    assert hashlib.sha256(json.dumps(cands).encode()).hexdigest() == g["cands_sha256"]
+    spd.delete()
+
+
+@pytest.mark.parametrize("name", ["small_peak", "very_wide_threshold"])
+def test_spd_repeatable(aa, name):
+    """Candidates do not depend on what earlier runs left in the work area."""
+    c = S.CASES[name]
+    spd, r1 = run_case(aa, c, keep=False)
+    _, r2 = run_case(aa, c, clear=False, keep=False, spd=spd)
+    assert cand_key(r1) == cand_key(r2)
+    spd.delete()
+
+
+def test_spd_host_capacity_drops_whole_batch(aa):
+    """A batch whose candidates would reach the host list's size is dropped
+    whole, as the reference does (src/aa_device_analysis.cu:319-354)."""
+    c = S.CASES["small_threshold"]
+    spd, r = run_case(aa, c, keep=False)
+    k = r["dm"].size
+    assert k > 10
+    import torch
+    x = S.make_plane(c)
+    d = torch.from_numpy(x).cuda()
+    tsamp_r = float(np.float32(c["tsamp"] * c["inbin"]))
+    r_small = spd.run(d, c["ndms"], c["nt"], tsamp_r, c["inbin"], c["cutoff"], c["sigma_constant"],
+                      c["max_width_s"], c["algorithm"], bool(c["baseline_noise"]), max_candidates=k)
+    assert r_small["dm"].size == 0
+    assert spd.profile()["dropped_batches"] == 1
+    spd.delete()
+
+
+def test_spd_refuses_bad_arguments(aa):
+    import torch
+    spd = aa.single_pulse_detection(64 * 4096)
+    d = torch.zeros(64 * 4096, device="cuda")
+    with pytest.raises(RuntimeError, match="larger than set up"):
+        spd.run(d, 64, 8192, 6.4e-5, 1, 6.0, 3.0, 0.004)
+    with pytest.raises(RuntimeError, match="candidate_algorithm"):
+        spd.run(d, 64, 4096, 6.4e-5, 1, 6.0, 3.0, 0.004, candidate_algorithm=3)
+    with pytest.raises(RuntimeError, match="at least 4 DM trials"):
+        spd.run(d, 2, 4096, 6.4e-5, 1, 6.0, 3.0, 0.004)
+    spd.delete()
