@@ -198,6 +198,19 @@ def lib():
         "aa_b200_sps_row_stats": ([vp, i, ll, ll, vp, vp, vp], i),
         "aa_b200_sps_block_peaks": ([vp, i, ll, ll, vp, vp, P(i), i, vp, vp, vp, vp], i),
         "aa_b200_sps_block_samples": ([], i),
+        "aa_py_analysis_plan": ([vp, f, f, f, i, b], vp),
+        "aa_analysis_plan_delete": ([vp], None),
+        "aa_py_analysis_plan_sigma_cutoff": ([vp], f),
+        "aa_py_analysis_plan_sigma_constant": ([vp], f),
+        "aa_py_analysis_plan_max_boxcar_width_in_sec": ([vp], f),
+        "aa_py_analysis_plan_enable_msd_baseline_noise": ([vp], b),
+        "aa_py_spd_nCandidates": ([vp], sz),
+        "aa_py_h_dm": ([vp], P(ctypes.c_uint)),
+        "aa_py_h_ts": ([vp], P(ctypes.c_uint)),
+        "aa_py_h_snr": ([vp], P(f)),
+        "aa_py_h_width": ([vp], P(ctypes.c_uint)),
+        "aa_b200_pipeline_set_candidate_output": ([vp, i, ctypes.c_char_p], b),
+        "aa_b200_pipeline_set_analysis_batch": ([vp, ll], b),
         "aa_b200_spd_create": ([ll, ll], vp),
         "aa_b200_spd_destroy": ([vp], None),
         "aa_b200_spd_last_error": ([vp], ctypes.c_char_p),
@@ -207,6 +220,9 @@ def lib():
         "aa_b200_spd_keep_planes": ([vp, i], i),
         "aa_b200_spd_planes": ([vp, vp, vp, ll], ll),
         "aa_b200_spd_kernel_launches": ([], ll),
+        "aa_b200_spd_plan": ([i, f, i, f, vp, i, P(i), P(i), P(i), vp, i, P(i)], i),
+        "aa_b200_spd_time_kernels": ([vp, i], i),
+        "aa_b200_spd_family_time": ([vp, i, P(d), P(ll)], i),
         "aa_b200_spd_write_candidates": ([ctypes.c_char_p, i, f, f, f, f, f, i, vp, vp, vp, vp, sz], i),
     }
     for name, (args, res) in protos.items():
@@ -317,6 +333,40 @@ class aa_py_ddtr_plan:
         return lib().aa_py_ddtr_plan_range(self.m_obj)
 
 
+class aa_py_analysis_plan:
+    """The single-pulse detection settings (cmake/py_astro_accelerate.py.in
+    aa_py_analysis_plan): candidate_algorithm 0 peak finding, 1 thresholding."""
+
+    def __init__(self, sigma_cutoff: float, sigma_constant: float, max_boxcar_width_in_sec: float,
+                 candidate_algorithm: int, enable_msd_baseline_noise: bool):
+        self.m_sigma_cutoff = sigma_cutoff
+        self.m_sigma_constant = sigma_constant
+        self.m_max_boxcar_width_in_sec = max_boxcar_width_in_sec
+        self.m_candidate_algorithm = candidate_algorithm
+        self.m_enable_msd_baseline_noise = enable_msd_baseline_noise
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, exc_type, exc_value, traceback):
+        pass
+
+    def sigma_cutoff(self):
+        return self.m_sigma_cutoff
+
+    def sigma_constant(self):
+        return self.m_sigma_constant
+
+    def max_boxcar_width_in_sec(self):
+        return self.m_max_boxcar_width_in_sec
+
+    def candidate_algorithm(self):
+        return self.m_candidate_algorithm
+
+    def enable_msd_baseline_noise(self):
+        return self.m_enable_msd_baseline_noise
+
+
 class aa_py_pipeline:
     """aa_pipeline_api<unsigned short> through the C ABI."""
 
@@ -351,8 +401,49 @@ class aa_py_pipeline:
     def ddtr_ndms(self):
         return lib().aa_py_get_ndms_array(self.m_obj)
 
-    def bind_analysis_plan(self, plan):
-        return lib().aa_py_pipeline_api_bind_analysis_plan(self.m_obj, None)
+    def bind_analysis_plan(self, plan: "aa_py_analysis_plan"):
+        """The analysis plan over this pipeline's DDTR strategy (bind the DDTR
+        plan first), as the reference's wrapper does."""
+        strat = lib().aa_py_pipeline_api_ddtr_strategy(self.m_obj)
+        ptr = lib().aa_py_analysis_plan(strat, plan.sigma_cutoff(), plan.sigma_constant(),
+                                        plan.max_boxcar_width_in_sec(), int(plan.candidate_algorithm()),
+                                        bool(plan.enable_msd_baseline_noise()))
+        if strat:
+            lib().aa_py_ddtr_strategy_delete(strat)
+        self.m_analysis_plan_ptr = ptr
+        return bool(lib().aa_py_pipeline_api_bind_analysis_plan(self.m_obj, ptr))
+
+    def get_candidates(self):
+        """After a run() step with status 1 (has_more): nCandidates, dm,
+        time_sample, snr, width (ctypes arrays), current_range,
+        current_tchunk, current_inc -- the position after the step, as the
+        reference's wrapper returns it."""
+        if self.m_status_code_c_int.value == 1:
+            n = lib().aa_py_spd_nCandidates(self.m_obj)
+            return (n, lib().aa_py_h_dm(self.m_obj), lib().aa_py_h_ts(self.m_obj), lib().aa_py_h_snr(self.m_obj),
+                    lib().aa_py_h_width(self.m_obj), lib().aa_py_current_range(self.m_obj),
+                    lib().aa_py_current_time_chunk(self.m_obj), lib().aa_py_current_inc(self.m_obj))
+        return None, [], [], [], [], None, None, None
+
+    def candidates(self) -> dict:
+        """The last step's candidates as numpy arrays (dm, ts, snr, bw)."""
+        n = lib().aa_py_spd_nCandidates(self.m_obj)
+        out = {}
+        for key, fn, dt in (("dm", lib().aa_py_h_dm, np.uint32), ("ts", lib().aa_py_h_ts, np.uint32),
+                            ("snr", lib().aa_py_h_snr, np.float32), ("bw", lib().aa_py_h_width, np.uint32)):
+            ptr = fn(self.m_obj)
+            out[key] = np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, dt)
+        return out
+
+    def set_candidate_output(self, write_files: bool = True, directory: str | None = None):
+        """Whether and where the reference's candidate files are written."""
+        return bool(lib().aa_b200_pipeline_set_candidate_output(self.m_obj, int(write_files),
+                                                                os.fsencode(directory) if directory else None))
+
+    def set_analysis_batch(self, max_time_samples: int):
+        if not lib().aa_b200_pipeline_set_analysis_batch(self.m_obj, int(max_time_samples)):
+            raise ValueError(self.last_error())
+        return True
 
     def bind_periodicity_plan(self, plan):
         return lib().aa_py_pipeline_api_bind_periodicity_plan(self.m_obj, 0.0, False, 0.0, 0, 0)
@@ -797,6 +888,18 @@ class single_pulse_detection:
         return {"widths": widths[:k].copy(), "msd": msd[:2 * k].copy(), "max_width_performed": mwp.value,
                 "max_iteration": mit.value, "dropped_batches": drop.value}
 
+    def time_kernels(self, on: bool = True):
+        lib().aa_b200_spd_time_kernels(self.m_obj, int(on))
+
+    def family_times(self) -> dict:
+        """Device ms and launches per launch family of the last run (time_kernels on)."""
+        out = {}
+        for k, name in enumerate(("msd", "decimation", "snr_planes", "candidates")):
+            ms, n = ctypes.c_double(), ctypes.c_longlong()
+            lib().aa_b200_spd_family_time(self.m_obj, k, ctypes.byref(ms), ctypes.byref(n))
+            out[name] = (ms.value, n.value)
+        return out
+
     def planes(self):
         """(snr, taps) of the last batch of the last run (keep_planes on)."""
         import numpy as np
@@ -816,6 +919,19 @@ class single_pulse_detection:
             self.delete()
         except Exception:
             pass
+
+
+def spd_plan(nt: int, tsamp: float, inBin: int, max_boxcar_width_in_sec: float) -> dict:
+    """The boxcar plan of the single-pulse detection (host only)."""
+    w = np.zeros(1024, np.int32)
+    pl = np.zeros(10 * 64, np.int32)
+    nw, mwp, mit, npl = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    if lib().aa_b200_spd_plan(int(nt), float(tsamp), int(inBin), float(max_boxcar_width_in_sec), w.ctypes.data,
+                              1024, ctypes.byref(nw), ctypes.byref(mwp), ctypes.byref(mit), pl.ctypes.data, 64,
+                              ctypes.byref(npl)):
+        raise ValueError(lib().aa_b200_spd_last_error(None).decode())
+    return {"widths": w[:nw.value].tolist(), "max_width_performed": mwp.value, "max_iteration": mit.value,
+            "plan": pl[:10 * npl.value].reshape(-1, 10).tolist()}
 
 
 def spd_kernel_launches() -> int:

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include "ddtr_kernels.cuh"
+#include "spd.cuh"
 #include "export.hpp"
 #include "pipeline.hpp"
 #include "planner.hpp"
@@ -23,6 +24,14 @@ thread_local std::string g_last_error;
 std::atomic<long long> g_launches{0};
 
 void set_error(const std::string &m) { g_last_error = m; }
+
+// aa_analysis_plan (include/aa_analysis_plan.hpp:34-47) as the C ABI holds it
+struct AnalysisPlan {
+    float sigma_cutoff = 0.f, sigma_constant = 0.f, max_boxcar_width_in_sec = 0.f;
+    int candidate_algorithm = 0;
+    bool enable_msd_baseline_noise = false;
+    bool strategy_ready = false, strategy_for_analysis = false;
+};
 
 // The object behind aa_py_pipeline_api (aa_pipeline_api<unsigned short>).
 struct Api {
@@ -38,7 +47,19 @@ struct Api {
     bool supported = true;
     std::string export_base = "DD_data"; // output_dmt files (the reference's base name)
     bool exported = false;
+    // analysis (single-pulse detection) after every dedispersion step
+    bool analysis_bound = false;
+    AnalysisPlan aplan{};
+    std::unique_ptr<SpdPlane> spd;
+    float *d_spd_plane = nullptr; // a copy of the step's rows when they must be kept
+    long long spd_max_ts = 0;     // batch size; 0 = the reference's rule from free memory
+    size_t spd_capacity = 0;      // host candidate list size (SPD_max_peak_size)
+    SpdCandidates cands;          // the last step's candidates
+    bool write_candidates = true; // the reference's peak_analysed/analysed files
+    std::string candidate_dir;    // where they go ("" = the working directory)
+    ~Api() { cudaFree(d_spd_plane); }
 };
+
 
 
 FilterbankMetadata to_meta(const aa_py_filterbank_metadata_struct &m)
@@ -91,6 +112,81 @@ bool export_outputs(Api *a)
                         static_cast<int>(per_file), err))
         return api_fail(a, "output_dmt: " + err);
     a->exported = true;
+    return true;
+}
+
+// Single-pulse detection on the rows the last dedispersion step wrote, as the
+// reference runner does after each (chunk, range) step
+// (include/aa_permitted_pipelines_generic.hpp:848-889): analysis_GPU with
+// the range's tsamp (tsamp * inBin, float), tstart = tsamp * inc (float) and
+// the range's DMs; the candidates replace the previous step's and go to the
+// reference's candidate file.
+bool run_analysis(Api *a)
+{
+    a->cands = SpdCandidates{};
+    DdtrPipeline &P = *a->pipe;
+    StepPlane sp;
+    if (!P.last_step_plane(sp))
+        return api_fail(a, "analysis: no dedispersed rows");
+    // the rows are copied to the host first (save_data before the analysis)
+    if (!P.synchronize())
+        return api_fail(a, P.last_error());
+    const DdtrStrategy &s = P.strategy();
+    std::string err;
+    if (!a->spd) {
+        long long max_elems = 0;
+        for (size_t r = 0; r < s.nranges(); ++r)
+            for (int tp : s.t_processed()[r])
+                max_elems = std::max(max_elems, static_cast<long long>(s.ndms(r)) * tp);
+        long long max_ts = a->spd_max_ts;
+        if (max_ts <= 0) {
+            // include/aa_analysis_strategy.hpp:219-224: 95% of the free memory
+            // at 5.5 floats and 2 ushorts per sample
+            size_t fr = 0, tot = 0;
+            if (cudaMemGetInfo(&fr, &tot) != cudaSuccess)
+                return api_fail(a, "analysis: cudaMemGetInfo failed");
+            max_ts = static_cast<long long>((static_cast<double>(fr) * 0.95) / (5.5 * 4 + 2 * 2));
+        }
+        std::unique_ptr<SpdPlane> spd(new SpdPlane());
+        if (!spd->setup(max_elems, max_ts, err))
+            return api_fail(a, "analysis: " + err);
+        if (a->popt.device_output &&
+            cudaMalloc(&a->d_spd_plane, static_cast<size_t>(max_elems) * sizeof(float)) != cudaSuccess)
+            return api_fail(a, "analysis: cudaMalloc failed");
+        // include/aa_permitted_pipelines_generic.hpp:376-377
+        a->spd_capacity = static_cast<size_t>(s.max_ndms()) * static_cast<size_t>(s.t_processed()[0][0]) / 2;
+        a->spd = std::move(spd);
+    }
+    float *plane = sp.d;
+    if (a->popt.device_output || sp.pitch != sp.tp) {
+        // the search decimates into its input: work on a copy of rows that are kept
+        if (!a->d_spd_plane &&
+            cudaMalloc(&a->d_spd_plane, static_cast<size_t>(sp.ndms) * sp.tp * sizeof(float)) != cudaSuccess)
+            return api_fail(a, "analysis: cudaMalloc failed");
+        if (cudaMemcpy2DAsync(a->d_spd_plane, static_cast<size_t>(sp.tp) * sizeof(float), sp.d,
+                              static_cast<size_t>(sp.pitch) * sizeof(float), static_cast<size_t>(sp.tp) * sizeof(float),
+                              static_cast<size_t>(sp.ndms), cudaMemcpyDeviceToDevice, P.stream()) != cudaSuccess)
+            return api_fail(a, "analysis: cudaMemcpy2DAsync failed");
+        plane = a->d_spd_plane;
+    }
+    const DmRange &d = s.dm(sp.range);
+    const float tsamp_original = static_cast<float>(a->meta.tsamp);
+    const float tsamp = tsamp_original * static_cast<float>(d.inBin);
+    SpdSettings st;
+    st.sigma_cutoff = a->aplan.sigma_cutoff;
+    st.sigma_constant = a->aplan.sigma_constant;
+    st.max_boxcar_width_in_sec = a->aplan.max_boxcar_width_in_sec;
+    st.candidate_algorithm = a->aplan.candidate_algorithm;
+    st.enable_msd_baseline_noise = a->aplan.enable_msd_baseline_noise ? 1 : 0;
+    if (!a->spd->run(plane, sp.ndms, sp.tp, tsamp, d.inBin, st, a->cands, P.stream(), err, a->spd_capacity))
+        return api_fail(a, "analysis: " + err);
+    if (a->write_candidates && !a->cands.dm.empty()) {
+        const float tstart = tsamp_original * static_cast<float>(sp.inc);
+        if (aa_b200_spd_write_candidates(a->candidate_dir.c_str(), st.candidate_algorithm, tstart, d.low, d.high,
+                                         d.step, tsamp, d.inBin, a->cands.dm.data(), a->cands.ts.data(),
+                                         a->cands.snr.data(), a->cands.bw.data(), a->cands.dm.size()))
+            return api_fail(a, aa_b200_spd_last_error(nullptr));
+    }
     return true;
 }
 
@@ -157,10 +253,11 @@ void *aa_py_pipeline_api(pipeline_components_struct pipeline, pipeline_component
     a->input = input_data;
     a->card = card_number;
     a->popt.copy_to_host = options.copy_ddtr_data_to_host;
-    if (pipeline.analysis || pipeline.periodicity || pipeline.fdas || !pipeline.dedispersion) {
+    if (pipeline.periodicity || pipeline.fdas || !pipeline.dedispersion) {
         a->supported = false;
-        api_fail(a, "only the dedispersion component is implemented by this library");
+        api_fail(a, "only the dedispersion and analysis components are implemented by this library");
     }
+    a->popt.enable_analysis = pipeline.analysis;
     // include/aa_py_pipeline_api.cpp:24-35 -> the runner's options
     a->popt.zero_dm = options.zero_dm;
     a->popt.zero_dm_outliers = options.zero_dm_with_outliers;
@@ -227,9 +324,82 @@ int aa_py_total_computed_samples(void *obj)
     return a->pipe ? static_cast<int>(a->pipe->strategy().nProcessedTimesamples()) : 0;
 }
 
-bool aa_py_pipeline_api_bind_analysis_plan(void *obj, const void *)
+// src/aa_py_analysis_plan.cpp:6-17: the plan keeps the DDTR strategy's state
+void *aa_py_analysis_plan(const void *ddtr_strategy, float sigma_cutoff, float sigma_constant,
+                          float max_boxcar_width_in_sec, int candidate_algorithm, bool enable_msd_baseline_noise)
 {
-    return api_fail(as_api(obj), "analysis (single-pulse search) is not implemented by this library");
+    AnalysisPlan *p = new AnalysisPlan();
+    p->sigma_cutoff = sigma_cutoff;
+    p->sigma_constant = sigma_constant;
+    p->max_boxcar_width_in_sec = max_boxcar_width_in_sec;
+    // values other than 1 and 2 select peak finding (:7-14)
+    p->candidate_algorithm = (candidate_algorithm == 1 || candidate_algorithm == 2) ? candidate_algorithm : 0;
+    p->enable_msd_baseline_noise = enable_msd_baseline_noise;
+    const DdtrStrategy *s = static_cast<const DdtrStrategy *>(ddtr_strategy);
+    p->strategy_ready = s && s->ready();
+    p->strategy_for_analysis = s && s->configured_for_analysis();
+    return p;
+}
+void aa_analysis_plan_delete(const void *obj) { delete static_cast<const AnalysisPlan *>(obj); }
+float aa_py_analysis_plan_sigma_cutoff(const void *obj) { return static_cast<const AnalysisPlan *>(obj)->sigma_cutoff; }
+float aa_py_analysis_plan_sigma_constant(const void *obj)
+{
+    return static_cast<const AnalysisPlan *>(obj)->sigma_constant;
+}
+float aa_py_analysis_plan_max_boxcar_width_in_sec(const void *obj)
+{
+    return static_cast<const AnalysisPlan *>(obj)->max_boxcar_width_in_sec;
+}
+bool aa_py_analysis_plan_enable_msd_baseline_noise(const void *obj)
+{
+    return static_cast<const AnalysisPlan *>(obj)->enable_msd_baseline_noise;
+}
+
+// include/aa_pipeline_api.hpp:182-219 with the readiness rules of
+// include/aa_analysis_strategy.hpp:67-93
+bool aa_py_pipeline_api_bind_analysis_plan(void *obj, const void *plan)
+{
+    Api *a = as_api(obj);
+    if (!a->supported)
+        return false;
+    if (!a->components.analysis)
+        return api_fail(a, "the analysis component was not requested");
+    if (a->analysis_bound)
+        return api_fail(a, "an analysis plan is already bound");
+    const AnalysisPlan *p = static_cast<const AnalysisPlan *>(plan);
+    if (!p || !p->strategy_ready)
+        return api_fail(a, "the analysis plan's DDTR strategy is not ready");
+    if (!(p->sigma_cutoff > 0) || !(p->sigma_constant > 0) || !(p->max_boxcar_width_in_sec > 0))
+        return api_fail(a, "analysis needs sigma_cutoff, sigma_constant and max_boxcar_width_in_sec above 0");
+    if (!p->strategy_for_analysis)
+        return api_fail(a, "the DDTR strategy was not computed for analysis");
+    if (p->candidate_algorithm == 2)
+        return api_fail(a, "candidate algorithm 2 (peak filtering) is not implemented by this library");
+    a->aplan = *p;
+    a->analysis_bound = true;
+    return true;
+}
+
+size_t aa_py_spd_nCandidates(void *obj) { return as_api(obj)->cands.dm.size(); }
+unsigned int *aa_py_h_dm(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->cands.dm.empty() ? nullptr : a->cands.dm.data();
+}
+unsigned int *aa_py_h_ts(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->cands.ts.empty() ? nullptr : a->cands.ts.data();
+}
+float *aa_py_h_snr(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->cands.snr.empty() ? nullptr : a->cands.snr.data();
+}
+unsigned int *aa_py_h_width(void *obj)
+{
+    Api *a = as_api(obj);
+    return a->cands.bw.empty() ? nullptr : a->cands.bw.data();
 }
 bool aa_py_pipeline_api_bind_periodicity_plan(void *obj, float, bool, float, int, int)
 {
@@ -249,11 +419,19 @@ bool aa_py_pipeline_api_run(void *obj, int *status_code)
             api_fail(a, "no DDTR plan bound");
         return false;
     }
+    if (a->components.analysis && !a->analysis_bound) {
+        *status_code = static_cast<int>(RunStatus::error);
+        return api_fail(a, "the analysis component needs an analysis plan bound");
+    }
     RunStatus st = RunStatus::finished;
     const bool more = a->pipe->next(st);
     *status_code = static_cast<int>(st);
     if (st == RunStatus::error) {
         api_fail(a, a->pipe->last_error());
+        return false;
+    }
+    if (st == RunStatus::has_more && a->analysis_bound && !run_analysis(a)) {
+        *status_code = static_cast<int>(RunStatus::error);
         return false;
     }
     if (!more && st == RunStatus::finished && a->options.output_dmt && !a->exported &&
@@ -601,6 +779,25 @@ bool aa_b200_pipeline_rewind(void *obj)
     Api *a = as_api(obj);
     a->exported = false;
     return a->pipe ? a->pipe->rewind() : api_fail(a, "no DDTR plan bound");
+}
+
+bool aa_b200_pipeline_set_candidate_output(void *obj, int write_files, const char *dir)
+{
+    Api *a = as_api(obj);
+    a->write_candidates = write_files != 0;
+    a->candidate_dir = dir ? dir : "";
+    return true;
+}
+
+bool aa_b200_pipeline_set_analysis_batch(void *obj, long long max_time_samples)
+{
+    Api *a = as_api(obj);
+    if (a->spd)
+        return api_fail(a, "the analysis batch must be set before the first step");
+    if (max_time_samples < 0)
+        return api_fail(a, "max_time_samples must be >= 0");
+    a->spd_max_ts = max_time_samples;
+    return true;
 }
 
 bool aa_b200_pipeline_set_export_base(void *obj, const char *base)

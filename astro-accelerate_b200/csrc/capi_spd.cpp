@@ -153,6 +153,63 @@ long long aa_b200_spd_planes(const void *obj, float *snr, unsigned short *taps, 
 
 long long aa_b200_spd_kernel_launches(void) { return spd_kernel_launches(); }
 
+int aa_b200_spd_time_kernels(void *obj, int on)
+{
+    SpdHandle *h = as_spd(obj);
+    if (!h)
+        return 1;
+    h->plane.time_kernels = on != 0;
+    return 0;
+}
+
+int aa_b200_spd_family_time(const void *obj, int family, double *ms, long long *launches)
+{
+    const SpdHandle *h = static_cast<const SpdHandle *>(obj);
+    if (!h || family < 0 || family > 3)
+        return 1;
+    if (ms)
+        *ms = h->plane.family_ms[family];
+    if (launches)
+        *launches = h->plane.family_n[family];
+    return 0;
+}
+
+int aa_b200_spd_plan(int nTimesamples, float tsamp, int inBin, float max_boxcar_width_in_sec, int *widths,
+                     int widths_cap, int *nwidths, int *max_width_performed, int *max_iteration, int *plan,
+                     int plan_cap, int *nplan)
+{
+    if (inBin < 1 || !(tsamp > 0.f) || nTimesamples < 1) {
+        g_spd_error = "single-pulse detection: inBin >= 1, tsamp > 0 and nTimesamples >= 1 needed";
+        return 1;
+    }
+    const std::vector<int> bc = spd_bc_widths();
+    const int mbw = static_cast<int>(max_boxcar_width_in_sec / tsamp);
+    int mwp = 0;
+    const int it = spd_max_iteration(mbw / inBin, bc, mwp);
+    const std::vector<int> w = spd_boxcar_widths(bc, mwp);
+    const std::vector<PdPlan> pd = spd_pd_plan(bc, nTimesamples);
+    if (nwidths)
+        *nwidths = static_cast<int>(w.size());
+    if (max_width_performed)
+        *max_width_performed = mwp;
+    if (max_iteration)
+        *max_iteration = it;
+    if (widths)
+        for (int i = 0; i < static_cast<int>(w.size()) && i < widths_cap; ++i)
+            widths[i] = w[i];
+    if (nplan)
+        *nplan = static_cast<int>(pd.size());
+    if (plan)
+        for (int i = 0; i < static_cast<int>(pd.size()) && i < plan_cap; ++i) {
+            const PdPlan &q = pd[i];
+            const int v[10] = {q.decimated_timesamples, q.dtm, q.iteration, q.nBoxcars, q.nBlocks,
+                               q.output_shift, q.shift, q.startTaps, q.unprocessed_samples, q.total_ut};
+            for (int k = 0; k < 10; ++k)
+                plan[10 * i + k] = v[k];
+        }
+    return 0;
+}
+
 // src/aa_device_analysis.cu:420-466: float records (DM, time, S/N, width) --
 // DM = trial * dm_step + dm_low, time = sample * tsamp + tstart (tsamp of
 // the range), width = boxcar width * inBin -- in a file named

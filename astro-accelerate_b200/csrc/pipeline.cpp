@@ -50,7 +50,7 @@ bool DdtrPipeline::bind(const DdtrPlan &plan)
             return false;
         free_mem = fr;
     }
-    const StrategyStatus s = strategy_.compute(plan_, meta_, free_mem, false);
+    const StrategyStatus s = strategy_.compute(plan_, meta_, free_mem, opt_.enable_analysis);
     if (s != STRAT_OK) {
         char buf[160];
         std::snprintf(buf, sizeof(buf), "DDTR strategy refused the plan (code %d)", static_cast<int>(s));
@@ -633,6 +633,7 @@ bool DdtrPipeline::rewind()
     cur_range_ = 0;
     inc_ = 0;
     finished_component_sent_ = false;
+    last_plane_ = StepPlane{};
     return true;
 }
 
@@ -968,6 +969,13 @@ bool DdtrPipeline::exec_ddtr(const DdtrOp &op)
         if (!opt_.device_output && !check_cuda(cudaEventRecord(ev_tile_free_[slot], st_d2h_), "event"))
             return false;
     }
+    last_plane_.d = out;
+    last_plane_.pitch = pitch;
+    last_plane_.ndms = job.p.ndms;
+    last_plane_.tp = op.tp;
+    last_plane_.range = op.range;
+    last_plane_.chunk = op.chunk;
+    last_plane_.inc = op.inc;
     if (!opt_.device_output)
         tile_slot_ ^= 1;
     return true;

@@ -60,7 +60,18 @@ struct PipelineOptions {
     bool output_norm = false;      // output_DDTR_normalization
     bool old_rfi = false;          // old_rfi
     bool bandpass_average = false; // set_bandpass_average
+    // the analysis component is requested: the strategy keeps room for it
+    // (include/aa_pipeline_api.hpp:142-154)
+    bool enable_analysis = false;
     cudaStream_t stream = nullptr;
+};
+
+// The DM-time rows one dedispersion step wrote (device memory).
+struct StepPlane {
+    float *d = nullptr;
+    long long pitch = 0; // floats between rows
+    int ndms = 0, tp = 0, range = -1, chunk = -1;
+    long long inc = 0;   // first input sample of the chunk
 };
 
 // One step of the reference runner's DDTR loop
@@ -187,6 +198,14 @@ public:
         return true;
     }
     bool cleanup();
+    // The rows of the last dedispersion step; in copy_to_host mode they sit
+    // in a tile the next steps reuse, so they are valid until the next step.
+    bool last_step_plane(StepPlane &p) const
+    {
+        p = last_plane_;
+        return last_plane_.d != nullptr;
+    }
+    cudaStream_t stream() const { return st_; }
 
 private:
     bool fail(const std::string &msg);
@@ -257,6 +276,7 @@ private:
     int cur_range_ = 0;
     long long inc_ = 0;
     int tile_slot_ = 0;
+    StepPlane last_plane_;
     long long launches_ = 0;
 
     struct TimedLaunch {

@@ -50,6 +50,7 @@ StrategyStatus DdtrStrategy::compute(const DdtrPlan &plan, const FilterbankMetad
                                      bool enable_analysis)
 {
     ready_ = false;
+    analysis_ = enable_analysis;
     meta_ = meta;
     power_ = plan.power();
     const int nchans = meta.nchans;

@@ -87,6 +87,8 @@ public:
                            bool enable_analysis);
 
     bool ready() const { return ready_; }
+    // computed with room for the analysis component (aa_ddtr_strategy::configured_for_analysis)
+    bool configured_for_analysis() const { return analysis_; }
     int maxshift() const { return maxshift_; }
     int max_ndms() const { return max_ndms_; }
     int num_tchunks() const { return num_tchunks_; }
@@ -116,6 +118,7 @@ public:
 
 private:
     bool ready_ = false;
+    bool analysis_ = false;
     FilterbankMetadata meta_;
     float power_ = 2.0f;
     std::vector<float> dmshifts_;

@@ -88,9 +88,10 @@ class SpdPlane {
   public:
     // Buffers for planes of up to max_elems (nDMs * nT) elements.  The
     // boxcar search takes the DM trials in batches of
-    // floor(max_time_samples / nT) rounded down to a multiple of 4 (the
-    // reference's maxTimeSamples; 0 = the whole plane in one batch); the
-    // 3 x 3 peak neighbourhoods end at batch edges, as in the reference.
+    // floor(max_time_samples / nT) rounded down to a multiple of 4, the
+    // rest last (the reference's maxTimeSamples; 0 = no limit, the whole
+    // plane in one batch); the 3 x 3 peak neighbourhoods end at batch edges,
+    // as in the reference.
     bool setup(long long max_elems, long long max_time_samples, std::string &err);
     void release();
     ~SpdPlane() { release(); }
@@ -110,12 +111,24 @@ class SpdPlane {
     int last_max_width_performed = 0, last_max_iteration = 0;
     bool keep_planes = false;
     int dropped_batches = 0; // batches whose candidates did not fit host_capacity
+    // Device time per launch family of the last run, from CUDA events around
+    // each launch when time_kernels is on: 0 MSD statistics, 1 decimations
+    // and boxcars of the MSD profile, 2 boxcar S/N planes, 3 candidates.
+    bool time_kernels = false;
+    double family_ms[4] = {0, 0, 0, 0};
+    long long family_n[4] = {0, 0, 0, 0};
     std::vector<float> last_snr;
     std::vector<uint16_t> last_taps;
 
   private:
     bool msd_profile(const float *d_input, int nDMs, int nT, const std::vector<int> &widths, const SpdSettings &s,
                      cudaStream_t st, std::string &err);
+    void t_begin(int family, cudaStream_t st);
+    void t_end(cudaStream_t st);
+    bool t_collect();
+    std::vector<cudaEvent_t> ev_pool_;
+    std::vector<int> ev_family_;
+    size_t ev_used_ = 0;
     float *d_work_ = nullptr, *d_msd_interp_ = nullptr;
     uint16_t *d_taps_ = nullptr;
     int *d_count_ = nullptr, *d_dit_widths_ = nullptr, *d_widths_ = nullptr;

@@ -116,7 +116,9 @@ bool SpdPlane::setup(long long max_elems, long long max_time_samples, std::strin
         return false;
     }
     max_elems_ = max_elems;
-    max_ts_ = max_time_samples > 0 ? max_time_samples : max_elems;
+    // batches never hold more than the plane, so the work area is sized for
+    // the smaller of the two; the batch rule itself uses max_ts_ as given
+    max_ts_ = max_time_samples > 0 ? max_time_samples : LLONG_MAX;
     // include/aa_permitted_pipelines_generic.hpp:391-412: 5.5 floats per
     // sample of a batch; the MSD profile needs half the whole plane plus its
     // statistics ahead of its partials.
@@ -151,8 +153,55 @@ cudaError_t SpdPlane::clear(cudaStream_t st)
     return e;
 }
 
+// Event pairs around launches of one family; recorded only with time_kernels.
+void SpdPlane::t_begin(int family, cudaStream_t st)
+{
+    if (!time_kernels)
+        return;
+    if (ev_used_ + 2 > ev_pool_.size()) {
+        for (int k = 0; k < 2; ++k) {
+            cudaEvent_t e = nullptr;
+            cudaEventCreate(&e);
+            ev_pool_.push_back(e);
+        }
+    }
+    ev_family_.push_back(family);
+    cudaEventRecord(ev_pool_[ev_used_], st);
+}
+
+void SpdPlane::t_end(cudaStream_t st)
+{
+    if (!time_kernels)
+        return;
+    cudaEventRecord(ev_pool_[ev_used_ + 1], st);
+    ev_used_ += 2;
+}
+
+bool SpdPlane::t_collect()
+{
+    for (int f = 0; f < 4; ++f) {
+        family_ms[f] = 0;
+        family_n[f] = 0;
+    }
+    for (size_t k = 0; k < ev_family_.size(); ++k) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, ev_pool_[2 * k], ev_pool_[2 * k + 1]) != cudaSuccess)
+            return false;
+        family_ms[ev_family_[k]] += ms;
+        family_n[ev_family_[k]] += 1;
+    }
+    ev_family_.clear();
+    ev_used_ = 0;
+    return true;
+}
+
 void SpdPlane::release()
 {
+    for (cudaEvent_t e : ev_pool_)
+        cudaEventDestroy(e);
+    ev_pool_.clear();
+    ev_family_.clear();
+    ev_used_ = 0;
     cudaFree(d_work_);
     cudaFree(d_taps_);
     cudaFree(d_msd_interp_);
@@ -200,14 +249,20 @@ bool SpdPlane::msd_profile(const float *d_input, int nDMs, int nT, const std::ve
     auto do_msd = [&](float *d_msd, const float *in, long long dts, long long rows, long long offset,
                       float *pp) -> bool {
         const MsdConf c = msd_conf(dts, rows, offset);
-        if (msd_plane(d_msd, in, msd_work, c, rej, sig, pp, st) != cudaSuccess) {
+        t_begin(0, st);
+        const cudaError_t e = msd_plane(d_msd, in, msd_work, c, rej, sig, pp, st);
+        t_end(st);
+        if (e != cudaSuccess) {
             err = "single-pulse detection: MSD launch failed";
             return false;
         }
         return true;
     };
     auto dit = [&](const float *in, float *out, int rows, long long dts) -> bool {
-        if (dit_pairs(in, out, rows, static_cast<int>(dts), st) != cudaSuccess) {
+        t_begin(1, st);
+        const cudaError_t e = dit_pairs(in, out, rows, static_cast<int>(dts), st);
+        t_end(st);
+        if (e != cudaSuccess) {
             err = "single-pulse detection: decimation launch failed";
             return false;
         }
@@ -217,7 +272,10 @@ bool SpdPlane::msd_profile(const float *d_input, int nDMs, int nT, const std::ve
     auto boxcar = [&](const float *in, float *out, long long dts, int nTaps) -> long long {
         if (dts - nTaps + 1 <= 0)
             return -1;
-        if (fir_rows(in, out, nDMs, static_cast<int>(dts), nTaps, st) != cudaSuccess)
+        t_begin(1, st);
+        const cudaError_t e = fir_rows(in, out, nDMs, static_cast<int>(dts), nTaps, st);
+        t_end(st);
+        if (e != cudaSuccess)
             return -2;
         return nTaps - 1;
     };
@@ -359,6 +417,8 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
         err = "single-pulse detection: not set up";
         return false;
     }
+    ev_family_.clear();
+    ev_used_ = 0;
     if (s.candidate_algorithm != 0 && s.candidate_algorithm != 1) {
         err = "single-pulse detection: candidate_algorithm must be 0 (peak finding) or 1 (thresholding)";
         return false;
@@ -433,14 +493,17 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
         cudaError_t e = cudaMemsetAsync(d_count_, 0, sizeof(int), st);
         // boxcar S/N planes
         const PdPlan &p0 = plan[0];
+        t_begin(2, st);
         if (e == cudaSuccess)
             e = spdt_first_plane(in, d_bv, d_dec, d_snr, d_taps_, msd2, p0.decimated_timesamples, p0.nBoxcars, p0.dtm,
                                  p0.nBlocks, nd, st);
+        t_end(st);
         int msd_pos = 0;
         for (int f = 1; f < max_it && e == cudaSuccess; ++f) {
             msd_pos += plan[f - 1].nBoxcars;
             const PdPlan &p = plan[f];
             const size_t o = static_cast<size_t>(nd) * static_cast<size_t>(p.output_shift);
+            t_begin(2, st);
             if (f % 2 == 0)
                 e = spdt_nth_plane(in + p.shift, d_bv + half_off, d_bv, d_dec, d_snr + o, d_taps_ + o, msd2 + msd_pos,
                                    p.decimated_timesamples, p.nBoxcars, p.startTaps, 1 << p.iteration, p.dtm,
@@ -449,11 +512,13 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
                 e = spdt_nth_plane(d_dec + p.shift, d_bv, d_bv + half_off, in, d_snr + o, d_taps_ + o, msd2 + msd_pos,
                                    p.decimated_timesamples, p.nBoxcars, p.startTaps, 1 << p.iteration, p.dtm,
                                    p.nBlocks, nd, st);
+            t_end(st);
         }
         // candidates of every iteration
         for (int f = 0; f < max_it && e == cudaSuccess; ++f) {
             const PdPlan &p = plan[f];
             const size_t o = static_cast<size_t>(nd) * static_cast<size_t>(p.output_shift);
+            t_begin(3, st);
             if (s.candidate_algorithm == 0)
                 e = spd_peak_find(d_snr + o, d_taps_ + o, c_dm, c_ts, c_snr, c_bw, p.decimated_timesamples, nd,
                                   p.unprocessed_samples, s.sigma_cutoff, local_max, d_count_, dm_shift, 1 << f, st);
@@ -461,6 +526,7 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
                 e = spd_threshold(d_snr + o, d_taps_ + o, c_dm, c_ts, c_snr, c_bw, d_count_, s.sigma_cutoff,
                                   p.decimated_timesamples, p.decimated_timesamples - p.unprocessed_samples, dm_shift,
                                   local_max, 1 << f, nd, st);
+            t_end(st);
         }
         int count = 0;
         if (e == cudaSuccess)
@@ -493,6 +559,10 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
             ++dropped_batches;
         }
         dm_shift += nd;
+    }
+    if (time_kernels && !t_collect()) {
+        err = "single-pulse detection: event timing failed";
+        return false;
     }
     if (keep_planes) {
         last_snr.assign(2 * b, 0.f);

@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="survey", choices=["survey", "mid", "small", "batched", "refine", "e2e"])
+    ap.add_argument("--config", default="survey", choices=["survey", "mid", "small", "batched", "refine", "e2e", "spd"])
     ap.add_argument("--beams", type=int, default=48, help="beams of the multi-beam draw (batched config)")
     ap.add_argument("--snippets", type=int, default=256, help="snippets per step (refine config)")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -650,6 +650,149 @@ def run_refine(args, rank, world, local):
     return 0
 
 
+SPD_WORKLOAD = dict(ndms=1536, nt=1 << 20, tsamp=64e-6, inbin=1, max_width_s=0.0164, sigma_cutoff=6.0,
+                    sigma_constant=3.0, baseline_noise=1, algorithm=0, npulses=16, seed=31)
+
+
+def synth_plane_device(w, seed, device):
+    """A DM-time plane [ndms][nt] float32 on the device: N(0, 1) noise plus
+    dispersed-looking pulses (a Gaussian in time whose amplitude falls off
+    and width grows with the distance from the pulse's DM trial)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    nd, nt = w["ndms"], w["nt"]
+    x = torch.randn((nd, nt), generator=g, device=device, dtype=torch.float32)
+    rng = torch.Generator()
+    rng.manual_seed(seed)
+    for _ in range(w["npulses"]):
+        d0 = int(torch.randint(8, nd - 8, (1,), generator=rng))
+        t0 = int(torch.randint(4096, nt - 4096, (1,), generator=rng))
+        wid = float(torch.empty(1).uniform_(1.0, 64.0, generator=rng))
+        amp = float(torch.empty(1).uniform_(0.5, 3.0, generator=rng))
+        lo, hi = max(0, d0 - 24), min(nd, d0 + 25)
+        dd = torch.arange(lo, hi, device=device, dtype=torch.float32)[:, None] - d0
+        tt = torch.arange(t0 - 2048, t0 + 2048, device=device, dtype=torch.float32)[None, :] - t0
+        ww = wid + 3.0 * dd.abs()
+        a = amp * torch.exp(-0.5 * (dd / 6.0) ** 2) * torch.sqrt(wid / ww)
+        x[lo:hi, t0 - 2048:t0 + 2048] += a * torch.exp(-0.5 * (tt / ww) ** 2)
+    return x
+
+
+def spd_snr_plane_bytes(aa, w):
+    """Algorithmic bytes of the boxcar S/N planes (the dominant family): per
+    iteration the input and the running boxcar values read once (the first
+    iteration has no running values), the S/N (float) and width (ushort)
+    planes written, and the half-resolution sums and boxcar values written."""
+    tsamp = float(__import__("numpy").float32(w["tsamp"] * w["inbin"]))
+    pl = aa.spd_plan(w["nt"], tsamp, w["inbin"], w["max_width_s"])
+    total = 0
+    for f in range(pl["max_iteration"]):
+        dts, dtm, nblocks = pl["plan"][f][0], pl["plan"][f][1], pl["plan"][f][4]
+        if nblocks <= 0:
+            continue
+        per_row = dts * 4 + (0 if f == 0 else dts * 4) + dts * (4 + 2) + dtm * 4 * 2
+        total += per_row * w["ndms"]
+    return total, pl
+
+
+def run_spd(args, rank, world, local):
+    """Single-pulse detection (the reference's analysis_GPU rules, bit-exact)
+    on one DM-time plane of 1536 DM trials x 2^20 samples float32 (6.4 GB,
+    far above L2), resident in HBM: one step = MSD profile with outlier
+    rejection, boxcar S/N planes up to 256 samples and peak finding.  The
+    plane is restored from a pristine copy before each step (the search
+    decimates into it) outside the timed region.  e2e: the same through the
+    C ABI from a pinned host plane (H2D inside the timed region) to the host
+    candidate lists."""
+    import numpy as np
+    import torch
+    import aa_b200 as aa
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    w = SPD_WORKLOAD
+    n = w["ndms"] * w["nt"]
+    pristine = synth_plane_device(w, w["seed"] + rank, device)
+    plane = torch.empty_like(pristine)
+    spd = aa.single_pulse_detection(n, 0)
+    tsamp = float(np.float32(w["tsamp"] * w["inbin"]))
+    kw = dict(candidate_algorithm=w["algorithm"], enable_msd_baseline_noise=bool(w["baseline_noise"]))
+
+    def one():
+        return spd.run(plane, w["ndms"], w["nt"], tsamp, w["inbin"], w["sigma_cutoff"], w["sigma_constant"],
+                       w["max_width_s"], **kw)
+
+    for _ in range(max(3, args.warmup)):
+        plane.copy_(pristine)
+        one()
+    torch.cuda.synchronize()
+    launches0 = aa.spd_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    ncand = 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            plane.copy_(pristine)
+            torch.cuda.synchronize()
+            e0.record()
+            r = one()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            ncand = int(r["dm"].size)
+    launches = (aa.spd_kernel_launches() - launches0) // max(1, args.steps)
+    # per-family device time on one more step
+    spd.time_kernels(True)
+    plane.copy_(pristine)
+    one()
+    fam = spd.family_times()
+    spd.time_kernels(False)
+    step_ms = statistics.median(ms)
+    # e2e: pinned host plane -> device -> analysis -> host candidates
+    host = torch.empty((w["ndms"], w["nt"]), dtype=torch.float32, pin_memory=True)
+    host.copy_(pristine)
+    e2e_ms = []
+    for _ in range(max(1, args.e2e_steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        plane.copy_(host, non_blocking=True)
+        r = one()
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e = statistics.median(e2e_ms)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    snr_bytes, pl = spd_snr_plane_bytes(aa, w)
+    snr_ms = fam["snr_planes"][0]
+    achieved = snr_bytes / (snr_ms / 1e3) / 1e9 if snr_ms > 0 else None
+    line = {"metric": "DM-trial*samples/s analysed (single-pulse detection, reference rules, bit-exact)",
+            "value": n / (step_ms / 1e3), "unit": "DM-trial*samples/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"single-pulse detection: {w['ndms']} DM trials x {w['nt']} samples f32 "
+                                   f"(6.4 GB), widths to {pl['max_width_performed']}, {pl['max_iteration']} "
+                                   "iterations, MSD with outlier rejection, peak finding at 6 sigma",
+                       "l2": "inputs larger than L2"},
+            "candidates": ncand, "gpu_launches": int(launches),
+            "families_ms": {k: v[0] for k, v in fam.items()},
+            "families_launches": {k: v[1] for k, v in fam.items()},
+            "roofline": {"bound": "hbm", "kernel": "k_spdt_first + k_spdt_nth (S/N planes)", "achieved": achieved,
+                         "peak": hbm, "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
+                         "traffic": None, "algorithmic_bytes": snr_bytes},
+            "e2e": {"value": n / (e2e / 1e3), "unit": "DM-trial*samples/s", "h2d_bytes_per_step": n * 4,
+                    "d2h_bytes_per_step": ncand * 16},
+            "clocks": clk.summary()}
+    spd.delete()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -661,8 +804,10 @@ def main():
         return run_refine(args, rank, world, local)
     if args.config == "e2e" and args.impl != "reference":
         return run_e2e(args, rank, world, local)
+    if args.config == "spd" and args.impl != "reference":
+        return run_spd(args, rank, world, local)
     cfg = {"survey": SURVEY, "mid": MID, "small": SMALL, "batched": SURVEY, "refine": SURVEY,
-           "e2e": SURVEY}[args.config]
+           "e2e": SURVEY, "spd": SURVEY}[args.config]
     if args.nbits:
         cfg = dict(cfg, nbits=args.nbits)
     if args.impl == "reference":

@@ -1,5 +1,6 @@
 /*
- * aa_b200.h -- C ABI of the B200-native dedispersion (DDTR) library
+ * aa_b200.h -- C ABI of the B200-native dedispersion (DDTR) and
+ * single-pulse detection library
  * (libaa_b200.so, built from astro-accelerate_b200/csrc/).
  *
  * Two layers:
@@ -8,8 +9,9 @@
  *     path (AstroAccelerate v1.3.1, src/aa_py_*.cpp, bound by ctypes in
  *     cmake/py_astro_accelerate.py.in).  Same names, argument meaning, return
  *     values and status codes, so the reference's Python wrapper binds this
- *     library by changing the library path.  Only the dedispersion component
- *     is implemented; plans of other components are refused (return false).
+ *     library by changing the library path.  The dedispersion and analysis
+ *     (single-pulse detection) components are implemented; periodicity and
+ *     FDAS plans are refused (return false).
  *
  *  2. aa_b200_* : the seam the reference's runner calls internally
  *     (load/corner turn/binning/dedisperse, include/aa_permitted_pipelines_generic.hpp),
@@ -117,9 +119,35 @@ int aa_py_get_t_proc(void *obj, int i, int j);
 int aa_py_dm_low(void *obj, int range);
 /* :70-72 */
 int aa_py_total_computed_samples(void *obj);
-/* :74-76, :82-85, :87-90: components other than dedispersion are out of
- * scope for this library and are refused (false). */
+/* src/aa_py_analysis_plan.cpp:6-44 (aa_analysis_plan*, opaque): the
+ * single-pulse detection settings; ddtr_strategy from
+ * aa_py_pipeline_api_ddtr_strategy.  candidate_algorithm 0 peak finding,
+ * 1 thresholding (2, peak filtering, is refused at bind). */
+void *aa_py_analysis_plan(const void *ddtr_strategy, float sigma_cutoff, float sigma_constant,
+                          float max_boxcar_width_in_sec, int candidate_algorithm, bool enable_msd_baseline_noise);
+void aa_analysis_plan_delete(const void *obj);
+float aa_py_analysis_plan_sigma_cutoff(const void *obj);
+float aa_py_analysis_plan_sigma_constant(const void *obj);
+float aa_py_analysis_plan_max_boxcar_width_in_sec(const void *obj);
+bool aa_py_analysis_plan_enable_msd_baseline_noise(const void *obj);
+/* src/aa_py_pipeline_api.cpp:74-76 (include/aa_pipeline_api.hpp:182-219):
+ * needs the analysis component requested, the DDTR plan bound (its strategy
+ * is then computed for analysis) and sigma_cutoff, sigma_constant and
+ * max_boxcar_width_in_sec above 0.  With it bound, every
+ * aa_py_pipeline_api_run step that dedisperses also runs analysis_GPU on the
+ * step's rows (include/aa_permitted_pipelines_generic.hpp:848-889) and writes
+ * the reference's candidate file (aa_b200_pipeline_set_candidate_output). */
 bool aa_py_pipeline_api_bind_analysis_plan(void *obj, const void *plan);
+/* :109-127: the candidates of the last step (DM trial index in the range,
+ * sample, S/N, boxcar width in samples of the range); the arrays stay valid
+ * until the next step (NULL when there are none). */
+size_t aa_py_spd_nCandidates(void *obj);
+unsigned int *aa_py_h_dm(void *obj);
+unsigned int *aa_py_h_ts(void *obj);
+float *aa_py_h_snr(void *obj);
+unsigned int *aa_py_h_width(void *obj);
+/* :82-85, :87-90: periodicity and FDAS are out of scope for this library
+ * and are refused (false). */
 bool aa_py_pipeline_api_bind_periodicity_plan(void *obj, float sigma_cutoff, bool enable_outlier_rejection,
                                               float sigma_outlier_rejection_threshold, int nHarmonics,
                                               int candidate_selection_algorithm);
@@ -307,6 +335,15 @@ bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant);
  * computes them; needs copy_ddtr_data_to_host.  Base name "DD_data" in the
  * working directory, or this one: */
 bool aa_b200_pipeline_set_export_base(void *obj, const char *base);
+/* Analysis output: write_files != 0 writes the reference's candidate files
+ * (the default) under dir (NULL or "" = the working directory, as the
+ * reference). */
+bool aa_b200_pipeline_set_candidate_output(void *obj, int write_files, const char *dir);
+/* The analysis batch in elements (the reference's maxtimesamples); 0 (the
+ * default) takes the reference's rule, 95% of the free device memory at 26
+ * bytes per element, capped at the largest step's rows.  Set before the
+ * first step. */
+bool aa_b200_pipeline_set_analysis_batch(void *obj, long long max_time_samples);
 /* include/aa_pipeline_runner.hpp:165-216 Export_DD_data: per range r with
  * ranges_to_export[r] != 0, <base>_<r>.txt (nTimesamples, nDMs,
  * DMs_per_file, number of files; one per line) and <base>_<r>_<i>.dat
@@ -486,6 +523,22 @@ int aa_b200_spd_profile(const void *obj, float *msd, int msd_cap, int *widths, i
 int aa_b200_spd_keep_planes(void *obj, int on);
 long long aa_b200_spd_planes(const void *obj, float *snr, unsigned short *taps, long long cap);
 long long aa_b200_spd_kernel_launches(void);
+/* on != 0: CUDA events around every launch of the following runs; family_time
+ * gives the last run's device time (ms) and launches of a family: 0 MSD
+ * statistics, 1 decimations and boxcars of the MSD profile, 2 boxcar S/N
+ * planes, 3 candidate selection. */
+int aa_b200_spd_time_kernels(void *obj, int on);
+int aa_b200_spd_family_time(const void *obj, int family, double *ms, long long *launches);
+/* The plan analysis_GPU builds (src/aa_device_analysis.cu:24-121, :138-179)
+ * for rows of nTimesamples at the range's tsamp (no GPU needed): the boxcar
+ * widths (widths_cap), the widest width performed, the iterations run, and
+ * per iteration (plan_cap) the ten fields of PulseDetection_plan
+ * (include/aa_device_BC_plan.hpp:12-23) in the order decimated_timesamples,
+ * dtm, iteration, nBoxcars, nBlocks, output_shift, shift, startTaps,
+ * unprocessed_samples, total_ut. */
+int aa_b200_spd_plan(int nTimesamples, float tsamp, int inBin, float max_boxcar_width_in_sec, int *widths,
+                     int widths_cap, int *nwidths, int *max_width_performed, int *max_iteration, int *plan,
+                     int plan_cap, int *nplan);
 /* The candidate file of src/aa_device_analysis.cu:420-466 (float records
  * DM, time, S/N, width) under dir; returns 0 or 1. */
 int aa_b200_spd_write_candidates(const char *dir, int candidate_algorithm, float tstart, float dm_low, float dm_high,

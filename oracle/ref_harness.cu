@@ -44,6 +44,8 @@
 #include "aa_permitted_pipelines_generic.hpp"
 #include "aa_pipeline.hpp"
 #include "aa_sigproc_input.hpp"
+#include "aa_analysis_plan.hpp"
+#include "aa_analysis_strategy.hpp"
 #include "aa_device_analysis.hpp"
 #include "aa_device_BC_plan.hpp"
 #include "aa_device_MSD_plane_profile.hpp"
@@ -268,6 +270,98 @@ int aaref_time_ddtr(const unsigned short *input_tc, int nchans, int nsamp, doubl
     return 0;
 }
 
+/* The reference runner with dedispersion and analysis (single-pulse
+ * detection) components, as aa_pipeline_api sets them up
+ * (include/aa_pipeline_api.hpp:130-219): the DDTR strategy computed for
+ * analysis, then per (time chunk, range) step the candidates of analysis_GPU
+ * (include/aa_permitted_pipelines_generic.hpp:848-889), read after each step
+ * from the runner's host lists.  The peak_analysed/analysed files go to the
+ * working directory.  Per step k: step_chunk[k], step_range[k],
+ * step_ncands[k]; the candidates of all steps follow one another in
+ * c_dm/c_ts/c_snr/c_bw (max_cands).  *msd_max_ts receives the analysis
+ * strategy's maxtimesamples.  Returns the number of steps, or < 0. */
+int aaref_run_pipeline_spd(const unsigned short *input_tc, int nchans, int nsamp, double tsamp, double fch1,
+                           double foff, int nbits, const harness_dm *plan, int nranges, size_t free_memory,
+                           float sigma_cutoff, float sigma_constant, float max_boxcar_width_in_sec,
+                           int candidate_algorithm, int enable_msd_baseline_noise, int max_steps, int *step_chunk,
+                           int *step_range, long long *step_ncands, unsigned *c_dm, unsigned *c_ts, float *c_snr,
+                           unsigned *c_bw, long long max_cands, long long *msd_max_ts, int *num_tchunks,
+                           int *t_processed, int max_chunks)
+{
+    aa_device_info dev(0);
+    aa_ddtr_plan p;
+    for (int i = 0; i < nranges; i++)
+        p.add_dm(plan[i].low, plan[i].high, plan[i].step, plan[i].inBin, plan[i].outBin);
+    aa_filterbank_metadata meta(0.0, tsamp, nbits, nsamp, fch1, foff, nchans);
+    size_t fm = free_memory ? free_memory : dev.free_memory();
+    int nsteps = 0;
+    long long written = 0;
+    {
+        aa_ddtr_strategy s(p, meta, fm, true, &dev);
+        if (!s.ready())
+            return -1;
+        *num_tchunks = s.num_tchunks();
+        if (*num_tchunks > max_chunks)
+            return -5;
+        for (int r = 0; r < nranges; r++)
+            for (int k = 0; k < *num_tchunks; k++)
+                t_processed[r * max_chunks + k] = s.t_processed()[r][k];
+        if ((long long)nchans * (long long)(s.t_processed()[0][0] + s.maxshift()) >= (1LL << 31))
+            return -6;
+        aa_analysis_plan::selectable_candidate_algorithm alg =
+            candidate_algorithm == 1 ? aa_analysis_plan::selectable_candidate_algorithm::threshold
+                                     : aa_analysis_plan::selectable_candidate_algorithm::peak_find;
+        aa_analysis_plan ap(s, sigma_cutoff, sigma_constant, max_boxcar_width_in_sec, alg,
+                            enable_msd_baseline_noise != 0);
+        aa_analysis_strategy an(ap, &dev);
+        if (!an.ready())
+            return -7;
+        *msd_max_ts = (long long)an.MSD_data_info();
+        aa_pipeline::pipeline comps;
+        comps.insert(aa_pipeline::component::dedispersion);
+        comps.insert(aa_pipeline::component::analysis);
+        aa_pipeline::pipeline_option opts;
+        opts.insert(aa_pipeline::component_option::copy_ddtr_data_to_host);
+        aa_periodicity_strategy per;
+        aa_fdas_strategy fd;
+        aa_jerk_strategy jk;
+        aa_permitted_pipelines_generic runner(comps, opts, s, an, per, fd, jk, false, false, false, false, false,
+                                              input_tc);
+        if (!runner.setup())
+            return -2;
+        aa_pipeline_runner::status st;
+        bool more = true;
+        while (more) {
+            more = runner.next(st);
+            if (st == aa_pipeline_runner::status::error)
+                return -3;
+            if (st != aa_pipeline_runner::status::has_more)
+                continue;
+            if (nsteps >= max_steps)
+                return -4;
+            /* the accessors give the step just run */
+            const int rr = runner.get_current_range(), cc = runner.get_current_tchunk();
+            const size_t k = runner.get_SPD_nCandidates();
+            step_chunk[nsteps] = cc;
+            step_range[nsteps] = rr;
+            step_ncands[nsteps] = (long long)k;
+            if (written + (long long)k > max_cands)
+                return -8;
+            for (size_t j = 0; j < k; j++) {
+                c_dm[written + j] = runner.h_SPD_dm()[j];
+                c_ts[written + j] = runner.h_SPD_ts()[j];
+                c_snr[written + j] = runner.h_SPD_snr()[j];
+                c_bw[written + j] = runner.h_SPD_width()[j];
+            }
+            written += (long long)k;
+            nsteps++;
+        }
+        if (cudaDeviceSynchronize() != cudaSuccess)
+            return -9;
+    }
+    return nsteps;
+}
+
 /* plane: host [nDMs][nT] float.  Outputs (caller-sized): msd [2 * nwidths]
  * (nwidths <= 256) and widths [nwidths]; snr/taps: the whole S/N and width
  * planes SPDT writes (plane_cap elements, at least 2 * nDMs * nT); the
@@ -276,11 +370,14 @@ int aaref_spd(const float *plane, int nDMs, int nT, float tsamp, int inBin, floa
               float sigma_constant, int enable_msd_baseline_noise, float cutoff, int candidate_algorithm, float tstart,
               float dm_low, float dm_high, float dm_step, float *msd, int *widths, int *nwidths, int *max_width_performed,
               int *max_iteration, float *snr, unsigned short *taps, long long plane_cap, unsigned *c_dm, unsigned *c_ts,
-              float *c_snr, unsigned *c_bw, int max_cands, int *ncands)
+              float *c_snr, unsigned *c_bw, int max_cands, int *ncands, long long max_ts)
 {
     const size_t n = (size_t)nDMs * (size_t)nT;
     if ((long long)(2 * n) > plane_cap)
         return -1;
+    /* max_ts: analysis_GPU's maxTimeSamples (0 = the plane).  Below the plane
+     * the search runs in batches and the whole-plane S/N stage is skipped. */
+    const bool whole = (max_ts <= 0 || (size_t)max_ts >= n);
     /* the plan analysis_GPU builds (:138-179) */
     int max_boxcar_width = (int)(max_boxcar_width_in_sec / tsamp);
     int mwp = 0;
@@ -301,7 +398,7 @@ int aaref_spd(const float *plane, int nDMs, int nT, float tsamp, int inBin, floa
 
     /* buffers as the runner sizes them for maxTimeSamples = nDMs * nT
      * (include/aa_permitted_pipelines_generic.hpp:391-412) */
-    unsigned long int maxTS = (unsigned long int)n;
+    unsigned long int maxTS = whole ? (unsigned long int)n : (unsigned long int)max_ts;
     float *d_plane = NULL, *d_work = NULL, *d_msd = NULL;
     unsigned short *d_taps = NULL;
     size_t msd_bytes = 0, dit_bytes = 0, work_bytes = 0;
@@ -320,7 +417,7 @@ int aaref_spd(const float *plane, int nDMs, int nT, float tsamp, int inBin, floa
                       sigma_constant, enable_msd_baseline_noise, false, &t0, &t1, &t2);
     cudaMemcpy(msd, d_msd, 2 * (*nwidths) * sizeof(float), cudaMemcpyDeviceToHost);
     /* stage 2: the boxcar planes of one DM batch (:206-253) */
-    {
+    if (whole) {
         size_t mem_idx = 0;
         int DMs_per_cycle = nDMs;
         mem_idx += 4 * ((size_t)nT * DMs_per_cycle) / 4;

@@ -18,7 +18,39 @@ CASES = {
                             baseline_noise=1, cutoff=5.5, algorithm=0),
     "very_wide_threshold": dict(ndms=64, nt=65536, seed=4, tsamp=64e-6, inbin=1, max_width_s=0.065,
                                 sigma_constant=3.0, baseline_noise=0, cutoff=7.0, algorithm=1),
+    # rows too short to decimate to the widest width: the MSD profile switches
+    # to boxcars over the last decimation (src/aa_device_MSD_plane_profile.cu:267-338)
+    "short_switch": dict(ndms=32, nt=4096, seed=5, tsamp=64e-6, inbin=1, max_width_s=0.06, sigma_constant=3.0,
+                         baseline_noise=0, cutoff=6.0, algorithm=0),
+    # the search in batches of 24 and 20 DM trials (analysis_GPU's maxTimeSamples
+    # below the plane): peak neighbourhoods end at the batch edges
+    "batched_peak": dict(ndms=64, nt=16384, seed=6, tsamp=64e-6, inbin=1, max_width_s=0.008, sigma_constant=3.0,
+                         baseline_noise=0, cutoff=5.5, algorithm=0, max_ts=24 * 16384),
+    "batched_threshold": dict(ndms=48, nt=8192, seed=7, tsamp=64e-6, inbin=1, max_width_s=0.004,
+                              sigma_constant=3.0, baseline_noise=1, cutoff=6.0, algorithm=1, max_ts=20 * 8192),
+    # 66 DM trials: batches of 64 and 2, thresholding skips rows past 4*floor(n/4)
+    "ragged_dms_threshold": dict(ndms=66, nt=8192, seed=8, tsamp=64e-6, inbin=1, max_width_s=0.004,
+                                 sigma_constant=3.0, baseline_noise=0, cutoff=5.0, algorithm=1),
 }
+
+# The reference runner with the analysis component on the DDTR cases of
+# cases.py: analysis settings per run.
+PIPELINE_CASES = {
+    "pipe_binned_peak": dict(ddtr="shared8_binned", sigma_cutoff=6.0, sigma_constant=3.0, max_width_s=0.01,
+                             algorithm=0, baseline_noise=0),
+    "pipe_chunked_threshold": dict(ddtr="shared8_chunked", sigma_cutoff=6.5, sigma_constant=3.0,
+                                   max_width_s=0.005, algorithm=1, baseline_noise=1),
+    "pipe_cache_peak": dict(ddtr="cache8", sigma_cutoff=5.5, sigma_constant=2.5, max_width_s=0.02, algorithm=0,
+                            baseline_noise=1),
+}
+
+
+def single_batch(case) -> bool:
+    """The search runs the whole plane in one batch (the S/N planes of the
+    reference's whole-plane stage are then comparable)."""
+    n = case["ndms"] * case["nt"]
+    mts = case.get("max_ts", 0) or n
+    return (min(mts, n) // case["nt"]) // 4 * 4 >= case["ndms"]
 
 
 def make_plane(case) -> np.ndarray:

@@ -39,7 +39,8 @@ def test_plan_objects_roundtrip(aa):
 
 def test_out_of_scope_components_are_refused(aa):
     md = aa.filterbank_metadata_struct(0.0, 64e-6, 1550.0, -0.39, 8, 1 << 16, 256, 0.0)
-    comps = aa.aa_py_pipeline_components(True, True, False, False)
+    # periodicity is out of scope (dedispersion and analysis are implemented)
+    comps = aa.aa_py_pipeline_components(True, False, True, False)
     opts = aa.aa_py_pipeline_component_options()
     x = np.zeros(256 * (1 << 16), np.uint16)
     p = aa.aa_py_pipeline(comps, opts, md, x, 0)

@@ -22,6 +22,7 @@ import os
 import numpy as np
 import pytest
 
+import cases as C
 import spd_cases as S
 
 pytestmark = pytest.mark.gpu
@@ -40,11 +41,14 @@ def cand_key(r):
     return sorted((int(r["dm"][j]), int(r["ts"][j]), int(snr_bits[j]), int(r["bw"][j])) for j in range(r["dm"].size))
 
 
-def run_case(aa, c, max_ts=0, clear=True, keep=True, spd=None):
+def run_case(aa, c, clear=True, keep=True, spd=None):
+    """The plane of case c through aa_b200_spd_run, with the reference
+    harness's batch size (its maxTimeSamples: the plane unless the case sets
+    one)."""
     import torch
     x = S.make_plane(c)
     if spd is None:
-        spd = aa.single_pulse_detection(x.size, max_ts)
+        spd = aa.single_pulse_detection(x.size, c.get("max_ts", 0) or x.size)
     spd.keep_planes(keep)
     if clear:
         spd.clear()
@@ -69,10 +73,11 @@ def test_spd_matches_reference(aa, golden, name):
     assert prof["max_width_performed"] == g["max_width_performed"]
     assert prof["max_iteration"] == g["max_iteration"]
     assert prof["msd"].view(np.uint32).tolist() == g["msd_bits"]
-    snr, taps = spd.planes()
-    assert snr.size == 2 * c["ndms"] * c["nt"]
-    assert hashlib.sha256(snr.tobytes()).hexdigest() == g["snr_sha256"]
-    assert hashlib.sha256(taps.tobytes()).hexdigest() == g["taps_sha256"]
+    if S.single_batch(c):
+        snr, taps = spd.planes()
+        assert snr.size == 2 * c["ndms"] * c["nt"]
+        assert hashlib.sha256(snr.tobytes()).hexdigest() == g["snr_sha256"]
+        assert hashlib.sha256(taps.tobytes()).hexdigest() == g["taps_sha256"]
     # second run: the work area as the first left it, as in the reference's third stage
     _, r2 = run_case(aa, c, clear=False, keep=False, spd=spd)
     cands = cand_key(r2)
@@ -121,3 +126,68 @@ def test_spd_refuses_bad_arguments(aa):
     with pytest.raises(RuntimeError, match="at least 4 DM trials"):
         spd.run(d, 2, 4096, 6.4e-5, 1, 6.0, 3.0, 0.004)
     spd.delete()
+
+
+def run_pipeline_case(aa, name, directory, max_ts):
+    """A DDTR case through aa_py_pipeline_api with the analysis component:
+    per step (chunk, range) and its candidates."""
+    pc = S.PIPELINE_CASES[name]
+    case = C.CASES[pc["ddtr"]]
+    md = aa.filterbank_metadata_struct(0.0, case["tsamp"], case["fch1"], case["foff"], case["nbits"],
+                                       case["nsamp"], case["nchans"], 0.0)
+    comps = aa.aa_py_pipeline_components(True, True, False, False)
+    o = aa.aa_py_pipeline_component_options()
+    o.copy_ddtr_data_to_host = True
+    x = C.make_input(case)
+    pipe = aa.aa_py_pipeline(comps, o, md, np.ascontiguousarray(x.reshape(-1)), 0)
+    pipe.set_options(free_memory=C.strategy_free_memory(case))
+    plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in case["plan"]])
+    assert pipe.bind_ddtr_plan(plan), pipe.last_error()
+    ap = aa.aa_py_analysis_plan(pc["sigma_cutoff"], pc["sigma_constant"], pc["max_width_s"], pc["algorithm"],
+                                bool(pc["baseline_noise"]))
+    assert pipe.bind_analysis_plan(ap), pipe.last_error()
+    pipe.set_candidate_output(True, str(directory))
+    pipe.set_analysis_batch(max_ts)
+    steps = []
+    pos = (0, 0)
+    while pipe.run():
+        assert pipe.status_code() != aa.STATUS_ERROR, pipe.last_error()
+        if pipe.status_code() == 1:
+            steps.append((pos, pipe.candidates()))
+            pos = (pipe.get_candidates()[6], pipe.get_candidates()[5])
+    assert pipe.status_code() == aa.STATUS_FINISHED, pipe.last_error()
+    nt = pipe.num_tchunks()
+    tp = [[pipe.t_processed(r, k) for k in range(nt)] for r in range(len(case["plan"]))]
+    pipe.cleanUp()
+    pipe.delete()
+    plan.delete()
+    return steps, tp
+
+
+@pytest.fixture(scope="module")
+def pipeline_golden():
+    with open(GOLDEN) as f:
+        return json.load(f)["pipeline_runs"]
+
+
+@pytest.mark.parametrize("name", list(S.PIPELINE_CASES))
+def test_pipeline_analysis_matches_reference(aa, pipeline_golden, name, tmp_path):
+    """Dedispersion plus analysis through the reference-facing pipeline API:
+    the candidates of every (chunk, range) step and the candidate files equal
+    the reference runner's."""
+    g = pipeline_golden[name]
+    assert g["rc"] > 0
+    steps, tp = run_pipeline_case(aa, name, tmp_path, g["msd_max_ts"])
+    assert tp == g["t_processed"]
+    assert len(steps) == len(g["steps"])
+    for (pos, r), gs in zip(steps, g["steps"]):
+        assert [pos[0], pos[1]] == [gs["chunk"], gs["range"]]
+        cands = cand_key(r)
+        assert len(cands) == gs["ncands"], (pos, len(cands), gs["ncands"])
+        assert hashlib.sha256(json.dumps(cands).encode()).hexdigest() == gs["cands_sha256"], pos
+    files = {}
+    for fn in sorted(os.listdir(tmp_path)):
+        rec = np.fromfile(os.path.join(tmp_path, fn), np.float32).reshape(-1, 4)
+        rows = sorted(tuple(int(v) for v in row.view(np.uint32)) for row in rec)
+        files[fn] = {"n": len(rows), "sha256": hashlib.sha256(json.dumps(rows).encode()).hexdigest()}
+    assert files == g["files"]

@@ -13,6 +13,15 @@ import torch.multiprocessing as mp
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+def _free_port() -> int:
+    """A port nothing listens on now (each run gets its own, so a store that
+    is still closing from an earlier test cannot collide with it)."""
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
 def _worker(rank, world, port, q):
     sys.path.insert(0, os.path.join(ROOT, "astro-accelerate_b200"))
     import torch
@@ -41,7 +50,7 @@ def _worker(rank, world, port, q):
 
 def test_partition_agrees_across_ranks_and_covers_every_beam():
     world = 2
-    port = 29500 + (os.getpid() % 2000)
+    port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
@@ -93,15 +102,19 @@ def _queue_worker(rank, world, port, nbeams, die_rank, q):
     mine = bq.run(work, timeout_s=120)
     results = {i: bq.result(i).decode() for i in range(nbeams)} if rank == 0 else None
     q.put((rank, mine, results, bq.ndone()))
-    # keep the store (hosted by rank 0) up until every live rank has finished
-    store.add("finished", 1)
-    while int(store.add("finished", 0)) < world - (1 if die_rank is not None else 0):
-        time.sleep(0.05)
+    # keep the store (hosted by rank 0) up until every other live rank has
+    # made its last store call
+    live = world - (1 if die_rank is not None else 0)
     bq.close()
+    if rank == 0:
+        while int(store.add("left", 0)) < live - 1:
+            time.sleep(0.05)
+    else:
+        store.add("left", 1)
 
 
 def _run_queue(world, nbeams, die_rank):
-    port = 31000 + (os.getpid() % 2000)
+    port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     procs = [ctx.Process(target=_queue_worker, args=(r, world, port, nbeams, die_rank, q)) for r in range(world)]
