@@ -856,10 +856,13 @@ class single_pulse_detection:
             max_boxcar_width_in_sec: float, candidate_algorithm: int = 0, enable_msd_baseline_noise: bool = False,
             max_candidates: int | None = None, stream: int = 0) -> dict:
         """Candidates of one plane as numpy arrays: dm (trial index), ts
-        (sample), snr, bw (boxcar width in samples of the range)."""
+        (sample), snr, bw (boxcar width in samples of the range).
+        max_candidates sizes the host lists (default: half the plane, at most
+        2^24); a batch that would fill them is dropped, as in the reference."""
         import numpy as np
         ptr = d_plane if isinstance(d_plane, int) else d_plane.data_ptr()
-        cap = int(max_candidates) if max_candidates is not None else max(1, int(ndms) * int(nt) // 2)
+        cap = (int(max_candidates) if max_candidates is not None
+               else max(1, min(int(ndms) * int(nt) // 2, 1 << 24)))
         dm = np.zeros(cap, np.uint32)
         ts = np.zeros(cap, np.uint32)
         snr = np.zeros(cap, np.float32)
@@ -894,7 +897,7 @@ class single_pulse_detection:
     def family_times(self) -> dict:
         """Device ms and launches per launch family of the last run (time_kernels on)."""
         out = {}
-        for k, name in enumerate(("msd", "decimation", "snr_planes", "candidates")):
+        for k, name in enumerate(("msd", "decimation", "snr_first", "snr_later", "candidates")):
             ms, n = ctypes.c_double(), ctypes.c_longlong()
             lib().aa_b200_spd_family_time(self.m_obj, k, ctypes.byref(ms), ctypes.byref(n))
             out[name] = (ms.value, n.value)

@@ -165,7 +165,7 @@ int aa_b200_spd_time_kernels(void *obj, int on)
 int aa_b200_spd_family_time(const void *obj, int family, double *ms, long long *launches)
 {
     const SpdHandle *h = static_cast<const SpdHandle *>(obj);
-    if (!h || family < 0 || family > 3)
+    if (!h || family < 0 || family >= SpdPlane::kFamilies)
         return 1;
     if (ms)
         *ms = h->plane.family_ms[family];

@@ -20,6 +20,7 @@ long long spd_kernel_launches() { return g_spd_launches.load(); }
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
+constexpr int MSD_BATCH = 8; // rows loaded ahead per thread in the MSD passes
 
 // ---------------------------------------------------------------------------
 // Streaming statistics (include/aa_device_MSD_shared_kernel_functions.cuh:13-35)
@@ -168,12 +169,22 @@ __global__ void __launch_bounds__(SPD_NTHREADS) k_msd_partials(const float *__re
     const long long spos = static_cast<long long>(blockIdx.x) * SPD_NTHREADS + threadIdx.x;
     long long g = static_cast<long long>(blockIdx.y) * y_steps * nT + spos;
     if (spos < nT - offset) {
-        st_first(M, S, j, __ldg(in + g));
-        g += nT;
-        for (int y = 1; y < y_steps; ++y) {
-            st_add(M, S, j, __ldg(in + g));
-            g += nT;
+        // loads batched ahead of the (sequential) updates: same order of
+        // arithmetic, more loads in flight per thread
+        const float *p = in + g;
+        st_first(M, S, j, __ldg(p));
+        int y = 1;
+        for (; y + MSD_BATCH <= y_steps; y += MSD_BATCH) {
+            float e[MSD_BATCH];
+#pragma unroll
+            for (int k = 0; k < MSD_BATCH; ++k)
+                e[k] = __ldg(p + static_cast<long long>(y + k) * nT);
+#pragma unroll
+            for (int k = 0; k < MSD_BATCH; ++k)
+                st_add(M, S, j, e[k]);
         }
+        for (; y < y_steps; ++y)
+            st_add(M, S, j, __ldg(p + static_cast<long long>(y) * nT));
     }
     s[threadIdx.x] = M;
     s[blockDim.x + threadIdx.x] = S;
@@ -198,17 +209,29 @@ __global__ void __launch_bounds__(SPD_NTHREADS) k_msd_partials_minmax(const floa
     const long long spos = static_cast<long long>(blockIdx.x) * SPD_NTHREADS + threadIdx.x;
     long long g = static_cast<long long>(blockIdx.y) * y_steps * nT + spos;
     if (spos < nT - offset) {
-        float e = in[g];
-        st_first(M, S, j, e);
-        mx = e;
-        mn = e;
-        g += nT;
-        for (int y = 1; y < y_steps; ++y) {
-            e = in[g];
+        const float *p = in + g;
+        const float e0 = __ldg(p);
+        st_first(M, S, j, e0);
+        mx = e0;
+        mn = e0;
+        int y = 1;
+        for (; y + MSD_BATCH <= y_steps; y += MSD_BATCH) {
+            float e[MSD_BATCH];
+#pragma unroll
+            for (int k = 0; k < MSD_BATCH; ++k)
+                e[k] = __ldg(p + static_cast<long long>(y + k) * nT);
+#pragma unroll
+            for (int k = 0; k < MSD_BATCH; ++k) {
+                mx = fmaxf(mx, e[k]);
+                mn = fminf(mn, e[k]);
+                st_add(M, S, j, e[k]);
+            }
+        }
+        for (; y < y_steps; ++y) {
+            const float e = __ldg(p + static_cast<long long>(y) * nT);
             mx = fmaxf(mx, e);
             mn = fminf(mn, e);
             st_add(M, S, j, e);
-            g += nT;
         }
     }
     s[threadIdx.x] = M;
@@ -249,8 +272,8 @@ __global__ void __launch_bounds__(SPD_NTHREADS) k_msd_partials_rejection(const f
     const long long spos = static_cast<long long>(blockIdx.x) * SPD_NTHREADS + threadIdx.x;
     long long g = static_cast<long long>(blockIdx.y) * y_steps * nT + spos;
     if (spos < nT - offset) {
-        for (int y = 0; y < y_steps; ++y) {
-            const float e = in[g];
+        const float *p = in + g;
+        auto take = [&](float e) {
             if ((e > limit_down) && (e < limit_up)) {
                 if (j == 0) {
                     st_first(M, S, j, e);
@@ -262,8 +285,19 @@ __global__ void __launch_bounds__(SPD_NTHREADS) k_msd_partials_rejection(const f
                     mn = fminf(mn, e);
                 }
             }
-            g += nT;
+        };
+        int y = 0;
+        for (; y + MSD_BATCH <= y_steps; y += MSD_BATCH) {
+            float e[MSD_BATCH];
+#pragma unroll
+            for (int k = 0; k < MSD_BATCH; ++k)
+                e[k] = __ldg(p + static_cast<long long>(y + k) * nT);
+#pragma unroll
+            for (int k = 0; k < MSD_BATCH; ++k)
+                take(e[k]);
         }
+        for (; y < y_steps; ++y)
+            take(__ldg(p + static_cast<long long>(y) * nT));
     }
     s[threadIdx.x] = M;
     s[blockDim.x + threadIdx.x] = S;
@@ -410,6 +444,17 @@ __global__ void k_dit_pairs(const float *__restrict__ in, float *__restrict__ ou
     out[y * dts + i] = in[y * nT + 2 * i] + in[y * nT + 2 * i + 1];
 }
 
+// The same sums for even rows on an 8-byte aligned input: one float2 load per pair.
+__global__ void k_dit_pairs2(const float2 *__restrict__ in, float *__restrict__ out, int rows, long long dts)
+{
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (y >= rows || i >= dts)
+        return;
+    const float2 v = __ldg(in + y * dts + i);
+    out[y * dts + i] = v.x + v.y;
+}
+
 // src/aa_device_single_FIR_kernel.cu:95-107
 __global__ void k_fir_rows(const float *__restrict__ in, float *__restrict__ out, int nTaps, long long nT)
 {
@@ -466,10 +511,10 @@ __device__ __forceinline__ float snr_of(float bw, float2 st) { return __fdividef
 
 __device__ __forceinline__ float snr_of_bv(float bv, float bw, float2 st) { return __fdividef(bv + (bw - st.x), st.y); }
 
+template <int nBoxcars>
 __global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_first(const float *__restrict__ in, float *bv_out, float *dec,
-                                                             float *snr_out, uint16_t *taps_out,
-                                                             const float2 *__restrict__ msd, int nT, int nBoxcars,
-                                                             int dtm)
+                                                             float *snr_out, uint16_t *taps_out, const SnrMsd msd,
+                                                             int nT, int dtm)
 {
     __shared__ float2 s_in[SPD_NTHREADS];
     __shared__ float2 s_snr[SPD_NTHREADS];
@@ -502,18 +547,18 @@ __global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_first(const float *__rest
     s_in[t].x = Bw[3];
     s_in[t].y = Bw[7];
     __syncthreads();
-    float2 st = msd[0];
+    float2 st = msd.v[0];
     f1.x = snr_of(Bw[0], st);
     f1.y = snr_of(Bw[4], st);
-    st = msd[1];
+    st = msd.v[1];
     f2.x = snr_of(Bw[1], st);
     f2.y = snr_of(Bw[5], st);
     if (f2.x > f1.x) { f1.x = f2.x; taps1.x = 2; } else taps1.x = 1;
     if (f2.y > f1.y) { f1.y = f2.y; taps1.y = 2; } else taps1.y = 1;
-    st = msd[2];
+    st = msd.v[2];
     f2.x = snr_of(Bw[2], st);
     f2.y = snr_of(Bw[6], st);
-    st = msd[3];
+    st = msd.v[3];
     f3.x = snr_of(Bw[3], st);
     f3.y = snr_of(Bw[7], st);
     if (f3.x > f2.x) { f2.x = f3.x; taps2.x = 4; } else taps2.x = 3;
@@ -522,6 +567,7 @@ __global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_first(const float *__rest
     if (f1.y > f2.y) { SNR.y = f1.y; taps.y = taps1.y; } else { SNR.y = f2.y; taps.y = taps2.y; }
     s_snr[t] = SNR;
     s_taps[t] = taps;
+#pragma unroll
     for (int d = 4; d < nBoxcars; d += 4) {
         __syncthreads();
         spos = t - (d >> 1);
@@ -533,18 +579,18 @@ __global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_first(const float *__rest
             Bw[1] = Bw[1] + f1.x; Bw[5] = Bw[5] + f1.y;
             Bw[2] = Bw[2] + f1.x; Bw[6] = Bw[6] + f1.y;
             Bw[3] = Bw[3] + f1.x; Bw[7] = Bw[7] + f1.y;
-            st = msd[d];
+            st = msd.v[d];
             f1.x = snr_of(Bw[0], st);
             f1.y = snr_of(Bw[4], st);
-            st = msd[d + 1];
+            st = msd.v[d + 1];
             f2.x = snr_of(Bw[1], st);
             f2.y = snr_of(Bw[5], st);
             if (f2.x > f1.x) { f1.x = f2.x; taps1.x = d + 2; } else taps1.x = d + 1;
             if (f2.y > f1.y) { f1.y = f2.y; taps1.y = d + 2; } else taps1.y = d + 1;
-            st = msd[d + 2];
+            st = msd.v[d + 2];
             f2.x = snr_of(Bw[2], st);
             f2.y = snr_of(Bw[6], st);
-            st = msd[d + 3];
+            st = msd.v[d + 3];
             f3.x = snr_of(Bw[3], st);
             f3.y = snr_of(Bw[7], st);
             if (f3.x > f2.x) { f2.x = f3.x; taps2.x = d + 4; } else taps2.x = d + 3;
@@ -575,10 +621,11 @@ __global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_first(const float *__rest
 
 // Later iterations: the input is the previous iteration's 2-sample sums, and
 // the running boxcar values of the previous widths (bv_in) are added in front.
+template <int nBoxcars>
 __global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_nth(const float *__restrict__ in, const float *bv_in,
                                                            float *bv_out, float *dec, float *snr_out,
-                                                           uint16_t *taps_out, const float2 *__restrict__ msd, int nT,
-                                                           int nBoxcars, int startTaps, int dit_value, int dtm)
+                                                           uint16_t *taps_out, const SnrMsd msd, int nT,
+                                                           int startTaps, int dit_value, int dtm)
 {
     __shared__ float2 s_in[SPD_NTHREADS];
     __shared__ float2 s_bv[SPD_NTHREADS];
@@ -618,18 +665,18 @@ __global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_nth(const float *__restri
     SNR.x = 0;
     SNR.y = 0;
     __syncthreads();
-    float2 st = msd[0];
+    float2 st = msd.v[0];
     f1.x = snr_of_bv(s_bv[t].x, Bw[0], st);
     f1.y = snr_of_bv(s_bv[t].y, Bw[4], st);
-    st = msd[1];
+    st = msd.v[1];
     f2.x = snr_of_bv(s_bv[t].x, Bw[1], st);
     f2.y = snr_of_bv(s_bv[t].y, Bw[5], st);
     if (f2.x > f1.x) { f1.x = f2.x; taps1.x = 2; } else taps1.x = 1;
     if (f2.y > f1.y) { f1.y = f2.y; taps1.y = 2; } else taps1.y = 1;
-    st = msd[2];
+    st = msd.v[2];
     f2.x = snr_of_bv(s_bv[t].x, Bw[2], st);
     f2.y = snr_of_bv(s_bv[t].y, Bw[6], st);
-    st = msd[3];
+    st = msd.v[3];
     f3.x = snr_of_bv(s_bv[t].x, Bw[3], st);
     f3.y = snr_of_bv(s_bv[t].y, Bw[7], st);
     if (f3.x > f2.x) { f2.x = f3.x; taps2.x = 4; } else taps2.x = 3;
@@ -638,6 +685,7 @@ __global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_nth(const float *__restri
     if (f1.y > f2.y) { SNR.y = f1.y; taps.y = taps1.y; } else { SNR.y = f2.y; taps.y = taps2.y; }
     s_snr[t] = SNR;
     s_taps[t] = taps;
+#pragma unroll
     for (int d = 4; d < nBoxcars; d += 4) {
         __syncthreads();
         spos = t - (d >> 1);
@@ -649,18 +697,18 @@ __global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_nth(const float *__restri
             Bw[1] = Bw[1] + f1.x; Bw[5] = Bw[5] + f1.y;
             Bw[2] = Bw[2] + f1.x; Bw[6] = Bw[6] + f1.y;
             Bw[3] = Bw[3] + f1.x; Bw[7] = Bw[7] + f1.y;
-            st = msd[d];
+            st = msd.v[d];
             f1.x = snr_of_bv(s_bv[spos].x, Bw[0], st);
             f1.y = snr_of_bv(s_bv[spos].y, Bw[4], st);
-            st = msd[d + 1];
+            st = msd.v[d + 1];
             f2.x = snr_of_bv(s_bv[spos].x, Bw[1], st);
             f2.y = snr_of_bv(s_bv[spos].y, Bw[5], st);
             if (f2.x > f1.x) { f1.x = f2.x; taps1.x = d + 2; } else taps1.x = d + 1;
             if (f2.y > f1.y) { f1.y = f2.y; taps1.y = d + 2; } else taps1.y = d + 1;
-            st = msd[d + 2];
+            st = msd.v[d + 2];
             f2.x = snr_of_bv(s_bv[spos].x, Bw[2], st);
             f2.y = snr_of_bv(s_bv[spos].y, Bw[6], st);
-            st = msd[d + 3];
+            st = msd.v[d + 3];
             f3.x = snr_of_bv(s_bv[spos].x, Bw[3], st);
             f3.y = snr_of_bv(s_bv[spos].y, Bw[7], st);
             if (f3.x > f2.x) { f2.x = f3.x; taps2.x = d + 4; } else taps2.x = d + 3;
@@ -743,25 +791,98 @@ __global__ void k_peak_find(const float *__restrict__ in, const uint16_t *__rest
     }
 }
 
+// The same rule over strips of rows: a thread owns one column of
+// SPD_PF_ROWS rows plus the row above and below the strip, loads them all
+// first (many loads in flight), takes each row's horizontal maximum with its
+// neighbour columns by warp shuffles (the two halo columns of a warp loaded
+// by lanes 0 and 31), then tests each row against the maxima of the rows
+// above, at and below it.  The window is the 3 x 3 neighbourhood clipped to
+// columns 0..last and rows 0..height-1, which is the reference's rule
+// whenever last >= 1 and height >= 2 (corners included); other shapes use
+// k_peak_find.  Which samples pass does not depend on the thread layout, only
+// the order in which they enter the list does (atomics, as in the reference).
+constexpr int SPD_PF_ROWS = 8;
+constexpr int SPD_PF_THREADS = 128;
+
+__global__ void __launch_bounds__(SPD_PF_THREADS) k_peak_find_strips(const float *__restrict__ in,
+                                                                      const uint16_t *__restrict__ taps,
+                                                                      unsigned *c_dm, unsigned *c_ts, float *c_snr,
+                                                                      unsigned *c_bw, int width, int height, int last,
+                                                                      float threshold, int max_cands, int *count,
+                                                                      int shift, int dit_value)
+{
+    constexpr int K = SPD_PF_ROWS + 2;
+    const int x = blockIdx.x * SPD_PF_THREADS + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int y0 = blockIdx.y * SPD_PF_ROWS;
+    const bool xin = x <= last;
+    const bool left_halo = lane == 0 && x >= 1 && x - 1 <= last;
+    const bool right_halo = lane == 31 && x + 1 <= last;
+    float own[K], h[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int y = y0 - 1 + k;
+        const bool yin = y >= 0 && y < height;
+        const float *row = in + static_cast<long long>(y) * width;
+        own[k] = (yin && xin) ? __ldg(row + x) : -INFINITY;
+        h[k] = -INFINITY;
+        if (yin && left_halo)
+            h[k] = __ldg(row + x - 1);
+        else if (yin && right_halo)
+            h[k] = __ldg(row + x + 1);
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        float left = __shfl_up_sync(FULL, own[k], 1);
+        float right = __shfl_down_sync(FULL, own[k], 1);
+        if (lane == 0)
+            left = h[k];
+        if (lane == 31)
+            right = h[k];
+        h[k] = fmaxf(own[k], fmaxf(left, right));
+    }
+#pragma unroll
+    for (int r = 0; r < SPD_PF_ROWS; ++r) {
+        const int y = y0 + r;
+        const float v = own[r + 1];
+        if (xin && y < height && v > threshold && v == fmaxf(h[r], fmaxf(h[r + 1], h[r + 2]))) {
+            const int pos = atomicAdd(count, 1);
+            if (pos < max_cands) {
+                const unsigned tp = taps[static_cast<long long>(y) * width + x];
+                c_dm[pos] = y + shift;
+                c_ts[pos] = x * dit_value + tp / 2;
+                c_snr[pos] = v;
+                c_bw[pos] = tp;
+            }
+        }
+    }
+}
+
 // Thresholding (src/aa_device_threshold_kernel.cu:10-41): every sample of
 // the rows 0 .. 4*floor(nDMs/4)-1 and columns < offset above the cut.
-__global__ void k_threshold(const float *__restrict__ in, const uint16_t *__restrict__ taps, unsigned *c_dm,
-                            unsigned *c_ts, float *c_snr, unsigned *c_bw, int *count, float threshold, int nT,
-                            int offset, int shift, int max_cands, int dit_value)
+// A block of 256 threads covers 1024 columns of one row, four per thread.
+__global__ void __launch_bounds__(256) k_threshold(const float *__restrict__ in, const uint16_t *__restrict__ taps,
+                                                   unsigned *c_dm, unsigned *c_ts, float *c_snr, unsigned *c_bw,
+                                                   int *count, float threshold, int nT, int offset, int shift,
+                                                   int max_cands, int dit_value)
 {
     const int y = blockIdx.y;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= offset)
-        return;
-    const float R = __ldg(in + static_cast<long long>(y) * nT + x);
-    if (R > threshold) {
-        const int pos = atomicAdd(count, 1);
-        if (pos < max_cands) {
-            const unsigned tp = taps[static_cast<long long>(y) * nT + x];
-            c_dm[pos] = y + shift;
-            c_ts[pos] = dit_value * x + tp / 2;
-            c_snr[pos] = R;
-            c_bw[pos] = tp;
+    const float *row = in + static_cast<long long>(y) * nT;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int x = blockIdx.x * 1024 + k * 256 + threadIdx.x;
+        if (x >= offset)
+            break;
+        const float R = __ldg(row + x);
+        if (R > threshold) {
+            const int pos = atomicAdd(count, 1);
+            if (pos < max_cands) {
+                const unsigned tp = taps[static_cast<long long>(y) * nT + x];
+                c_dm[pos] = y + shift;
+                c_ts[pos] = dit_value * x + tp / 2;
+                c_snr[pos] = R;
+                c_bw[pos] = tp;
+            }
         }
     }
 }
@@ -851,7 +972,11 @@ cudaError_t dit_pairs(const float *d_in, float *d_out, int nDMs, int nT, cudaStr
     const int rows = (nDMs / 2) * 2;
     if (rows == 0)
         return cudaSuccess;
-    k_dit_pairs<<<dim3(static_cast<unsigned>((dts + 255) / 256), rows), 256, 0, st>>>(d_in, d_out, rows, nT, dts);
+    const dim3 grid(static_cast<unsigned>((dts + 255) / 256), rows);
+    if (nT % 2 == 0 && (reinterpret_cast<uintptr_t>(d_in) & 7) == 0)
+        k_dit_pairs2<<<grid, 256, 0, st>>>(reinterpret_cast<const float2 *>(d_in), d_out, rows, dts);
+    else
+        k_dit_pairs<<<grid, 256, 0, st>>>(d_in, d_out, rows, nT, dts);
     ++g_spd_launches;
     return cudaGetLastError();
 }
@@ -878,25 +1003,55 @@ cudaError_t msd_interpolate(const float *d_msd_dit, float *d_msd_interp, const i
 }
 
 cudaError_t spdt_first_plane(const float *d_input, float *d_bv_out, float *d_decimated, float *d_snr, uint16_t *d_taps,
-                             const float2 *d_msd, int nTimesamples, int nBoxcars, int dtm, int nBlocks, int nDMs,
+                             const SnrMsd &msd, int nTimesamples, int nBoxcars, int dtm, int nBlocks, int nDMs,
                              cudaStream_t st)
 {
     if (nBlocks <= 0)
         return cudaSuccess;
-    k_spdt_first<<<dim3(nBlocks, nDMs), SPD_NTHREADS, 0, st>>>(d_input, d_bv_out, d_decimated, d_snr, d_taps, d_msd,
-                                                               nTimesamples, nBoxcars, dtm);
+    const dim3 grid(nBlocks, nDMs);
+    switch (nBoxcars) {
+    case 32:
+        k_spdt_first<32><<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_bv_out, d_decimated, d_snr, d_taps, msd,
+                                                        nTimesamples, dtm);
+        break;
+    case 16:
+        k_spdt_first<16><<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_bv_out, d_decimated, d_snr, d_taps, msd,
+                                                        nTimesamples, dtm);
+        break;
+    case 8:
+        k_spdt_first<8><<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_bv_out, d_decimated, d_snr, d_taps, msd,
+                                                       nTimesamples, dtm);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
     ++g_spd_launches;
     return cudaGetLastError();
 }
 
 cudaError_t spdt_nth_plane(const float *d_input, const float *d_bv_in, float *d_bv_out, float *d_decimated,
-                           float *d_snr, uint16_t *d_taps, const float2 *d_msd, int nTimesamples, int nBoxcars,
+                           float *d_snr, uint16_t *d_taps, const SnrMsd &msd, int nTimesamples, int nBoxcars,
                            int startTaps, int dit_value, int dtm, int nBlocks, int nDMs, cudaStream_t st)
 {
     if (nBlocks <= 0)
         return cudaSuccess;
-    k_spdt_nth<<<dim3(nBlocks, nDMs), SPD_NTHREADS, 0, st>>>(d_input, d_bv_in, d_bv_out, d_decimated, d_snr, d_taps,
-                                                             d_msd, nTimesamples, nBoxcars, startTaps, dit_value, dtm);
+    const dim3 grid(nBlocks, nDMs);
+    switch (nBoxcars) {
+    case 32:
+        k_spdt_nth<32><<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_bv_in, d_bv_out, d_decimated, d_snr, d_taps, msd,
+                                                      nTimesamples, startTaps, dit_value, dtm);
+        break;
+    case 16:
+        k_spdt_nth<16><<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_bv_in, d_bv_out, d_decimated, d_snr, d_taps, msd,
+                                                      nTimesamples, startTaps, dit_value, dtm);
+        break;
+    case 8:
+        k_spdt_nth<8><<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_bv_in, d_bv_out, d_decimated, d_snr, d_taps, msd,
+                                                     nTimesamples, startTaps, dit_value, dtm);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
     ++g_spd_launches;
     return cudaGetLastError();
 }
@@ -907,6 +1062,14 @@ cudaError_t spd_peak_find(const float *d_snr, const uint16_t *d_taps, unsigned *
 {
     if (width - offset - 1 <= 0)
         return cudaSuccess;
+    const int last = width - offset - 1;
+    if (height >= 2) {
+        const dim3 grid((last + SPD_PF_THREADS) / SPD_PF_THREADS, (height + SPD_PF_ROWS - 1) / SPD_PF_ROWS);
+        k_peak_find_strips<<<grid, SPD_PF_THREADS, 0, st>>>(d_snr, d_taps, d_dm, d_ts, d_csnr, d_bw, width, height,
+                                                             last, threshold, max_cands, d_count, shift, dit_value);
+        ++g_spd_launches;
+        return cudaGetLastError();
+    }
     const dim3 block(32, 2);
     const dim3 grid(1 + (width - offset - 1) / 32, 1 + (height - 1) / 2);
     k_peak_find<<<grid, block, 0, st>>>(d_snr, d_taps, d_dm, d_ts, d_csnr, d_bw, width, height, offset, threshold,
@@ -922,10 +1085,10 @@ cudaError_t spd_threshold(const float *d_snr, const uint16_t *d_taps, unsigned *
     const int rows = (nDMs / 4) * 4;
     if (offset <= 0 || rows == 0)
         return cudaSuccess;
-    // the reference's blocks cover 128 columns each; columns >= offset are skipped
-    const int nb = (offset + 127) / 128;
-    k_threshold<<<dim3(nb * 4, rows), 32, 0, st>>>(d_snr, d_taps, d_dm, d_ts, d_csnr, d_bw, d_count, threshold,
-                                                   nTimesamples, offset, shift, max_cands, dit_value);
+    // every column < offset of the rows below 4 * floor(nDMs / 4)
+    const int nb = (offset + 1023) / 1024;
+    k_threshold<<<dim3(nb, rows), 256, 0, st>>>(d_snr, d_taps, d_dm, d_ts, d_csnr, d_bw, d_count, threshold,
+                                                nTimesamples, offset, shift, max_cands, dit_value);
     ++g_spd_launches;
     return cudaGetLastError();
 }

@@ -50,11 +50,17 @@ cudaError_t dit_pairs(const float *d_in, float *d_out, int nDMs, int nT, cudaStr
 cudaError_t fir_rows(const float *d_in, float *d_out, int nDMs, int nT, int nTaps, cudaStream_t st);
 cudaError_t msd_interpolate(const float *d_msd_dit, float *d_msd_interp, const int *d_dit_widths, int n_dit,
                             const int *d_widths, int n_widths, int max_width_performed, cudaStream_t st);
+// (mean, deviation) of the boxcar widths one S/N plane uses, passed to the
+// kernels by value (constant-bank operands instead of loads)
+struct SnrMsd {
+    float2 v[SPD_MAXTAPS];
+};
+// nBoxcars: 8, 16 or 32 (the plan's widths per iteration)
 cudaError_t spdt_first_plane(const float *d_input, float *d_bv_out, float *d_decimated, float *d_snr, uint16_t *d_taps,
-                             const float2 *d_msd, int nTimesamples, int nBoxcars, int dtm, int nBlocks, int nDMs,
+                             const SnrMsd &msd, int nTimesamples, int nBoxcars, int dtm, int nBlocks, int nDMs,
                              cudaStream_t st);
 cudaError_t spdt_nth_plane(const float *d_input, const float *d_bv_in, float *d_bv_out, float *d_decimated,
-                           float *d_snr, uint16_t *d_taps, const float2 *d_msd, int nTimesamples, int nBoxcars,
+                           float *d_snr, uint16_t *d_taps, const SnrMsd &msd, int nTimesamples, int nBoxcars,
                            int startTaps, int dit_value, int dtm, int nBlocks, int nDMs, cudaStream_t st);
 // Candidate lists (dm, ts, snr, bw), appended at *d_count (atomic).
 cudaError_t spd_peak_find(const float *d_snr, const uint16_t *d_taps, unsigned *d_dm, unsigned *d_ts, float *d_csnr,
@@ -113,10 +119,12 @@ class SpdPlane {
     int dropped_batches = 0; // batches whose candidates did not fit host_capacity
     // Device time per launch family of the last run, from CUDA events around
     // each launch when time_kernels is on: 0 MSD statistics, 1 decimations
-    // and boxcars of the MSD profile, 2 boxcar S/N planes, 3 candidates.
+    // and boxcars of the MSD profile, 2 first boxcar S/N plane, 3 later S/N
+    // planes, 4 candidates.
+    static constexpr int kFamilies = 5;
     bool time_kernels = false;
-    double family_ms[4] = {0, 0, 0, 0};
-    long long family_n[4] = {0, 0, 0, 0};
+    double family_ms[kFamilies] = {0, 0, 0, 0, 0};
+    long long family_n[kFamilies] = {0, 0, 0, 0, 0};
     std::vector<float> last_snr;
     std::vector<uint16_t> last_taps;
 

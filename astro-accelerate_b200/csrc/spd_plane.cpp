@@ -179,7 +179,7 @@ void SpdPlane::t_end(cudaStream_t st)
 
 bool SpdPlane::t_collect()
 {
-    for (int f = 0; f < 4; ++f) {
+    for (int f = 0; f < kFamilies; ++f) {
         family_ms[f] = 0;
         family_n[f] = 0;
     }
@@ -481,7 +481,22 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
         return false;
     }
     const int local_max = static_cast<int>(std::min<size_t>(b / 4, 2147483640u));
-    const float2 *msd2 = reinterpret_cast<const float2 *>(d_msd_interp_);
+    // the (mean, deviation) values each iteration's kernel takes by value:
+    // iteration f uses the widths from the sum of the earlier nBoxcars on
+    std::vector<SnrMsd> msd_it(std::max(max_it, 1));
+    {
+        int pos = 0;
+        for (int f = 0; f < max_it; ++f) {
+            const int nb = plan[f].nBoxcars;
+            if (nb > SPD_MAXTAPS || pos + nb > static_cast<int>(widths.size())) {
+                err = "single-pulse detection: boxcar plan out of range";
+                return false;
+            }
+            for (int k = 0; k < nb; ++k)
+                msd_it[f].v[k] = make_float2(last_msd[2 * (pos + k)], last_msd[2 * (pos + k) + 1]);
+            pos += nb;
+        }
+    }
 
     int dm_shift = 0;
     std::vector<unsigned> h_a, h_b, h_d;
@@ -495,21 +510,19 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
         const PdPlan &p0 = plan[0];
         t_begin(2, st);
         if (e == cudaSuccess)
-            e = spdt_first_plane(in, d_bv, d_dec, d_snr, d_taps_, msd2, p0.decimated_timesamples, p0.nBoxcars, p0.dtm,
-                                 p0.nBlocks, nd, st);
+            e = spdt_first_plane(in, d_bv, d_dec, d_snr, d_taps_, msd_it[0], p0.decimated_timesamples, p0.nBoxcars,
+                                 p0.dtm, p0.nBlocks, nd, st);
         t_end(st);
-        int msd_pos = 0;
         for (int f = 1; f < max_it && e == cudaSuccess; ++f) {
-            msd_pos += plan[f - 1].nBoxcars;
             const PdPlan &p = plan[f];
             const size_t o = static_cast<size_t>(nd) * static_cast<size_t>(p.output_shift);
-            t_begin(2, st);
+            t_begin(3, st);
             if (f % 2 == 0)
-                e = spdt_nth_plane(in + p.shift, d_bv + half_off, d_bv, d_dec, d_snr + o, d_taps_ + o, msd2 + msd_pos,
+                e = spdt_nth_plane(in + p.shift, d_bv + half_off, d_bv, d_dec, d_snr + o, d_taps_ + o, msd_it[f],
                                    p.decimated_timesamples, p.nBoxcars, p.startTaps, 1 << p.iteration, p.dtm,
                                    p.nBlocks, nd, st);
             else
-                e = spdt_nth_plane(d_dec + p.shift, d_bv, d_bv + half_off, in, d_snr + o, d_taps_ + o, msd2 + msd_pos,
+                e = spdt_nth_plane(d_dec + p.shift, d_bv, d_bv + half_off, in, d_snr + o, d_taps_ + o, msd_it[f],
                                    p.decimated_timesamples, p.nBoxcars, p.startTaps, 1 << p.iteration, p.dtm,
                                    p.nBlocks, nd, st);
             t_end(st);
@@ -518,7 +531,7 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
         for (int f = 0; f < max_it && e == cudaSuccess; ++f) {
             const PdPlan &p = plan[f];
             const size_t o = static_cast<size_t>(nd) * static_cast<size_t>(p.output_shift);
-            t_begin(3, st);
+            t_begin(4, st);
             if (s.candidate_algorithm == 0)
                 e = spd_peak_find(d_snr + o, d_taps_ + o, c_dm, c_ts, c_snr, c_bw, p.decimated_timesamples, nd,
                                   p.unprocessed_samples, s.sigma_cutoff, local_max, d_count_, dm_shift, 1 << f, st);

@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--variant", type=int, default=0,
                     help="0 auto, 1 generic kernels, 2 channel-quad, 3 subband, 4 warp-specialised channel-quad "
                          "(2-4 run the staged fp32 kernel on two-byte data)")
+    ap.add_argument("--spd-nt", type=int, default=0, help="samples per DM trial of the spd config (default 2^19)")
     ap.add_argument("--nbits", type=int, default=0, help="bit depth of the synthetic filterbank (default: the config's)")
     return ap.parse_args()
 
@@ -650,7 +651,10 @@ def run_refine(args, rank, world, local):
     return 0
 
 
-SPD_WORKLOAD = dict(ndms=1536, nt=1 << 20, tsamp=64e-6, inbin=1, max_width_s=0.0164, sigma_cutoff=6.0,
+# 1536 x 2^19: the largest power-of-two plane of 1536 trials whose S/N-plane
+# offsets nDMs * output_shift stay below 2^31 in the reference's int arithmetic
+# (src/aa_device_SPS_long.cu:69,73; at 2^20 samples its analysis faults)
+SPD_WORKLOAD = dict(ndms=1536, nt=1 << 19, tsamp=64e-6, inbin=1, max_width_s=0.0164, sigma_cutoff=6.0,
                     sigma_constant=3.0, baseline_noise=1, algorithm=0, npulses=16, seed=31)
 
 
@@ -680,25 +684,29 @@ def synth_plane_device(w, seed, device):
 
 
 def spd_snr_plane_bytes(aa, w):
-    """Algorithmic bytes of the boxcar S/N planes (the dominant family): per
-    iteration the input and the running boxcar values read once (the first
-    iteration has no running values), the S/N (float) and width (ushort)
-    planes written, and the half-resolution sums and boxcar values written."""
+    """Algorithmic bytes of the boxcar S/N planes, per iteration: the input
+    and the running boxcar values read once (the first iteration has no
+    running values), the S/N (float) and width (ushort) planes written, and
+    the half-resolution sums and boxcar values written.  Returns (bytes of
+    the first plane, bytes of the later planes, plan)."""
     tsamp = float(__import__("numpy").float32(w["tsamp"] * w["inbin"]))
     pl = aa.spd_plan(w["nt"], tsamp, w["inbin"], w["max_width_s"])
-    total = 0
+    first = later = 0
     for f in range(pl["max_iteration"]):
         dts, dtm, nblocks = pl["plan"][f][0], pl["plan"][f][1], pl["plan"][f][4]
         if nblocks <= 0:
             continue
         per_row = dts * 4 + (0 if f == 0 else dts * 4) + dts * (4 + 2) + dtm * 4 * 2
-        total += per_row * w["ndms"]
-    return total, pl
+        if f == 0:
+            first = per_row * w["ndms"]
+        else:
+            later += per_row * w["ndms"]
+    return first, later, pl
 
 
 def run_spd(args, rank, world, local):
     """Single-pulse detection (the reference's analysis_GPU rules, bit-exact)
-    on one DM-time plane of 1536 DM trials x 2^20 samples float32 (6.4 GB,
+    on one DM-time plane of 1536 DM trials x 2^19 samples float32 (3.2 GB,
     far above L2), resident in HBM: one step = MSD profile with outlier
     rejection, boxcar S/N planes up to 256 samples and peak finding.  The
     plane is restored from a pristine copy before each step (the search
@@ -711,7 +719,7 @@ def run_spd(args, rank, world, local):
 
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
-    w = SPD_WORKLOAD
+    w = dict(SPD_WORKLOAD, nt=args.spd_nt) if args.spd_nt else SPD_WORKLOAD
     n = w["ndms"] * w["nt"]
     pristine = synth_plane_device(w, w["seed"] + rank, device)
     plane = torch.empty_like(pristine)
@@ -768,23 +776,29 @@ def run_spd(args, rank, world, local):
     except OSError:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
-    snr_bytes, pl = spd_snr_plane_bytes(aa, w)
-    snr_ms = fam["snr_planes"][0]
-    achieved = snr_bytes / (snr_ms / 1e3) / 1e9 if snr_ms > 0 else None
+    first_bytes, later_bytes, pl = spd_snr_plane_bytes(aa, w)
+    first_ms = fam["snr_first"][0]
+    achieved = first_bytes / (first_ms / 1e3) / 1e9 if first_ms > 0 else None
+    # DRAM bytes of one k_spdt_first launch, from an ncu capture of the
+    # 1536 x 65536 plane (1.3527e9 B) scaled by the samples a launch covers
+    traffic = 1.3527e9 * (n / (1536 * 65536))
     line = {"metric": "DM-trial*samples/s analysed (single-pulse detection, reference rules, bit-exact)",
             "value": n / (step_ms / 1e3), "unit": "DM-trial*samples/s", "n_gpus": 1, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"single-pulse detection: {w['ndms']} DM trials x {w['nt']} samples f32 "
-                                   f"(6.4 GB), widths to {pl['max_width_performed']}, {pl['max_iteration']} "
+                                   f"({n * 4 / 1e9:.1f} GB), widths to {pl['max_width_performed']}, {pl['max_iteration']} "
                                    "iterations, MSD with outlier rejection, peak finding at 6 sigma",
                        "l2": "inputs larger than L2"},
             "candidates": ncand, "gpu_launches": int(launches),
             "families_ms": {k: v[0] for k, v in fam.items()},
             "families_launches": {k: v[1] for k, v in fam.items()},
-            "roofline": {"bound": "hbm", "kernel": "k_spdt_first + k_spdt_nth (S/N planes)", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": "k_spdt_first (first boxcar S/N plane)", "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
-                         "traffic": None, "algorithmic_bytes": snr_bytes},
+                         "traffic": traffic, "algorithmic_bytes": first_bytes,
+                         "note": "issue-bound: 32 fast divisions and max-selects per sample"},
+            "later_snr_planes_gbs": (later_bytes / (fam["snr_later"][0] / 1e3) / 1e9
+                                     if fam["snr_later"][0] > 0 else None),
             "e2e": {"value": n / (e2e / 1e3), "unit": "DM-trial*samples/s", "h2d_bytes_per_step": n * 4,
                     "d2h_bytes_per_step": ncand * 16},
             "clocks": clk.summary()}

@@ -525,8 +525,8 @@ long long aa_b200_spd_planes(const void *obj, float *snr, unsigned short *taps, 
 long long aa_b200_spd_kernel_launches(void);
 /* on != 0: CUDA events around every launch of the following runs; family_time
  * gives the last run's device time (ms) and launches of a family: 0 MSD
- * statistics, 1 decimations and boxcars of the MSD profile, 2 boxcar S/N
- * planes, 3 candidate selection. */
+ * statistics, 1 decimations and boxcars of the MSD profile, 2 the first
+ * boxcar S/N plane, 3 the later S/N planes, 4 candidate selection. */
 int aa_b200_spd_time_kernels(void *obj, int on);
 int aa_b200_spd_family_time(const void *obj, int family, double *ms, long long *launches);
 /* The plan analysis_GPU builds (src/aa_device_analysis.cu:24-121, :138-179)

@@ -466,6 +466,73 @@ int aaref_spd(const float *plane, int nDMs, int nT, float tsamp, int inBin, floa
     return rc;
 }
 
+/* Times the reference's analysis_GPU (src/aa_device_analysis.cu:130-345) on
+ * a device plane [nDMs][nT] (d_src, kept intact): buffers as the runner
+ * allocates them (include/aa_permitted_pipelines_generic.hpp:391-412) for
+ * maxTimeSamples = max_ts (0 = the plane), then per repetition a device copy
+ * of d_src into the plane the search overwrites and CUDA events around
+ * analysis_GPU.  ms[reps] receives the times; *ncands the last run's
+ * candidate count.  Returns 0, or < 0. */
+int aaref_time_spd(const float *d_src, int nDMs, int nT, float tsamp, int inBin, float max_boxcar_width_in_sec,
+                   float sigma_constant, int enable_msd_baseline_noise, float cutoff, int candidate_algorithm,
+                   long long max_ts, int reps, float *ms, long long *ncands)
+{
+    const size_t n = (size_t)nDMs * (size_t)nT;
+    unsigned long int maxTS = (max_ts <= 0) ? (unsigned long int)n : (unsigned long int)max_ts;
+    int max_boxcar_width = (int)(max_boxcar_width_in_sec / tsamp);
+    int mwp = 0;
+    int t_BC_widths[10] = {PD_MAXTAPS, 16, 16, 16, 8, 8, 8, 8, 8, 8};
+    std::vector<int> BC_widths(t_BC_widths, t_BC_widths + 10);
+    Get_max_iteration(max_boxcar_width / inBin, &BC_widths, &mwp);
+    std::vector<int> h_boxcar_widths;
+    Create_list_of_boxcar_widths(&h_boxcar_widths, &BC_widths, mwp);
+    size_t msd_bytes = 0, dit_bytes = 0, work_bytes = 0;
+    Get_MSD_plane_profile_memory_requirements(&msd_bytes, &dit_bytes, &work_bytes, nT, nDMs, &h_boxcar_widths);
+    float *d_plane = NULL, *d_work = NULL, *d_msd = NULL;
+    unsigned short *d_taps = NULL;
+    if (cudaMalloc((void **)&d_plane, n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_work, maxTS * 5.5 * sizeof(float) + work_bytes) != cudaSuccess ||
+        cudaMalloc((void **)&d_taps, 2 * maxTS * sizeof(unsigned short)) != cudaSuccess ||
+        cudaMalloc((void **)&d_msd, msd_bytes + 4096) != cudaSuccess)
+        return -3;
+    const size_t host_cap = n / 2 + 1 < ((size_t)1 << 24) ? n / 2 + 1 : ((size_t)1 << 24);
+    std::vector<unsigned> a(host_cap), b(host_cap), d(host_cap);
+    std::vector<float> c(host_cap);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int rc = 0;
+    for (int r = 0; r < reps && rc == 0; r++) {
+        cudaMemcpy(d_plane, d_src, n * sizeof(float), cudaMemcpyDeviceToDevice);
+        cudaDeviceSynchronize();
+        size_t peak_pos = 0;
+        int ndms_arr[1] = {nDMs};
+        int maxshift = 0;
+        float lo[1] = {0.f}, hi[1] = {(float)nDMs}, st[1] = {1.f};
+        analysis_output out;
+        cudaEventRecord(e0, 0);
+        bool ok = analysis_GPU(a.data(), b.data(), c.data(), d.data(), &peak_pos, host_cap, 0, 0.f, nT, inBin,
+                               &maxshift, nDMs, ndms_arr, cutoff, sigma_constant, max_boxcar_width_in_sec, d_plane,
+                               lo, hi, st, tsamp, candidate_algorithm, d_work, d_taps, d_msd, maxTS,
+                               enable_msd_baseline_noise, false, false, out);
+        cudaEventRecord(e1, 0);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms[r], e0, e1);
+        *ncands = (long long)peak_pos;
+        if (!ok)
+            rc = -4;
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess)
+        rc = -5;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d_plane);
+    cudaFree(d_work);
+    cudaFree(d_taps);
+    cudaFree(d_msd);
+    return rc;
+}
+
 namespace {
 struct export_runner : public aa_pipeline_runner {
     bool setup() override { return true; }
