@@ -222,6 +222,7 @@ def lib():
         "aa_b200_spd_kernel_launches": ([], ll),
         "aa_b200_spd_plan": ([i, f, i, f, vp, i, P(i), P(i), P(i), vp, i, P(i)], i),
         "aa_b200_spd_time_kernels": ([vp, i], i),
+        "aa_b200_spd_first_plane": ([vp, vp, vp, vp, vp, vp, i, i, i, vp], i),
         "aa_b200_spd_family_time": ([vp, i, P(d), P(ll)], i),
         "aa_b200_spd_write_candidates": ([ctypes.c_char_p, i, f, f, f, f, f, i, vp, vp, vp, vp, sz], i),
     }
@@ -335,7 +336,8 @@ class aa_py_ddtr_plan:
 
 class aa_py_analysis_plan:
     """The single-pulse detection settings (cmake/py_astro_accelerate.py.in
-    aa_py_analysis_plan): candidate_algorithm 0 peak finding, 1 thresholding."""
+    aa_py_analysis_plan): candidate_algorithm 0 peak finding, 1 thresholding,
+    2 peak filtering."""
 
     def __init__(self, sigma_cutoff: float, sigma_constant: float, max_boxcar_width_in_sec: float,
                  candidate_algorithm: int, enable_msd_baseline_noise: bool):
@@ -830,7 +832,8 @@ def batch_estimate_bytes(metadata: filterbank_metadata_struct, plan: "aa_py_ddtr
 class single_pulse_detection:
     """analysis_GPU (src/aa_device_analysis.cu:130-345) on DM-time planes in
     device memory (aa_b200_spd_*): the reference's MSD profile, boxcar S/N
-    planes and candidate lists (peak finding or thresholding), bit for bit.
+    planes and candidate lists (peak finding, thresholding or peak
+    filtering), bit for bit.
 
     max_elems bounds nDMs * nT of the planes run; max_time_samples is the
     reference's batch size in elements (0 = one batch for the whole plane).

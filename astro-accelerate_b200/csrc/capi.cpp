@@ -373,8 +373,6 @@ bool aa_py_pipeline_api_bind_analysis_plan(void *obj, const void *plan)
         return api_fail(a, "analysis needs sigma_cutoff, sigma_constant and max_boxcar_width_in_sec above 0");
     if (!p->strategy_for_analysis)
         return api_fail(a, "the DDTR strategy was not computed for analysis");
-    if (p->candidate_algorithm == 2)
-        return api_fail(a, "candidate algorithm 2 (peak filtering) is not implemented by this library");
     a->aplan = *p;
     a->analysis_bound = true;
     return true;

@@ -153,6 +153,31 @@ long long aa_b200_spd_planes(const void *obj, float *snr, unsigned short *taps, 
 
 long long aa_b200_spd_kernel_launches(void) { return spd_kernel_launches(); }
 
+int aa_b200_spd_first_plane(const float *d_input, float *d_boxcar_values, float *d_decimated, float *d_snr,
+                            unsigned short *d_taps, const float *h_msd, int nTimesamples, int nBoxcars, int nDMs,
+                            void *stream)
+{
+    if (!h_msd || nBoxcars < 8 || nBoxcars > SPD_MAXTAPS || nTimesamples < 1 || nDMs < 1) {
+        g_spd_error = "single-pulse detection: nBoxcars 8, 16 or 32 and a non-empty plane needed";
+        return 1;
+    }
+    SnrMsd m{};
+    for (int k = 0; k < nBoxcars; ++k)
+        m.v[k] = make_float2(h_msd[2 * k], h_msd[2 * k + 1]);
+    // src/aa_device_analysis.cu:44-64: blocks of 2*512 - nBoxcars samples, dtm even
+    const int epb = 2 * SPD_NTHREADS - nBoxcars;
+    const int nBlocks = (nTimesamples + epb - 1) / epb;
+    int dtm = nTimesamples >> 1;
+    dtm -= dtm & 1;
+    const cudaError_t e = spdt_first_plane(d_input, d_boxcar_values, d_decimated, d_snr, d_taps, m, nTimesamples,
+                                           nBoxcars, dtm, nBlocks, nDMs, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) {
+        g_spd_error = std::string("single-pulse detection: ") + cudaGetErrorString(e);
+        return 1;
+    }
+    return 0;
+}
+
 int aa_b200_spd_time_kernels(void *obj, int on)
 {
     SpdHandle *h = as_spd(obj);

@@ -858,6 +858,114 @@ __global__ void __launch_bounds__(SPD_PF_THREADS) k_peak_find_strips(const float
     }
 }
 
+// Peak filtering, first stage (src/aa_device_peak_find_kernel.cu:10-70): a
+// sample of the interior (rows 3..height-4, columns 3..width-4) that no
+// sample of its 7 x 7 neighbourhood exceeds and that is above the cut.  The
+// record's width is the width plane's first element, as in the reference;
+// its sample uses the sample's own width.  Row maxima over 7 columns, then
+// the maximum over 7 rows, over strips of SPD_PF7_ROWS rows.
+constexpr int SPD_PF7_ROWS = 8;
+
+__global__ void __launch_bounds__(128) k_peak_find_7x7(const float *__restrict__ in, const uint16_t *__restrict__ taps,
+                                                       unsigned *c_dm, unsigned *c_ts, float *c_snr, unsigned *c_bw,
+                                                       int width, int height, float threshold, int max_cands,
+                                                       int *count, int shift, int dit_value)
+{
+    constexpr int K = SPD_PF7_ROWS + 6;
+    const int x = blockIdx.x * 128 + threadIdx.x;
+    const int y0 = 3 + blockIdx.y * SPD_PF7_ROWS; // first output row of the strip
+    const bool xin = x >= 3 && x <= width - 4;
+    float h[K], own[SPD_PF7_ROWS];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int y = y0 - 3 + k;
+        h[k] = -INFINITY;
+        if (xin && y < height) {
+            const float *r = in + static_cast<long long>(y) * width + x;
+            float m = __ldg(r - 3);
+#pragma unroll
+            for (int i = -2; i <= 3; ++i)
+                m = fmaxf(m, __ldg(r + i));
+            h[k] = m;
+            if (k >= 3 && k < 3 + SPD_PF7_ROWS)
+                own[k - 3] = __ldg(r);
+        }
+    }
+    if (!xin)
+        return;
+#pragma unroll
+    for (int r = 0; r < SPD_PF7_ROWS; ++r) {
+        const int y = y0 + r;
+        if (y > height - 4)
+            break;
+        float m = h[r];
+#pragma unroll
+        for (int i = 1; i < 7; ++i)
+            m = fmaxf(m, h[r + i]);
+        const float c = own[r];
+        if (c == m && c > threshold) {
+            const int pos = atomicAdd(count, 1);
+            if (pos < max_cands) {
+                c_dm[pos] = y + shift;
+                c_ts[pos] = x * dit_value + taps[static_cast<long long>(y) * width + x] / 2;
+                c_snr[pos] = c;
+                c_bw[pos] = taps[0];
+            }
+        }
+    }
+}
+
+// Peak filtering, second stage (src/aa_device_peak_find_kernel.cu:391-486):
+// a candidate is dropped when another one with at least its S/N lies closer
+// than max_distance (squared, in DM trials and samples) but not at distance
+// 0.  One thread per candidate, the others staged through shared memory.
+constexpr int SPD_FILTER_THREADS = 256;
+
+__global__ void __launch_bounds__(SPD_FILTER_THREADS) k_filter_peaks(
+    const unsigned *__restrict__ dm, const unsigned *__restrict__ ts, const unsigned *__restrict__ bw,
+    const float *__restrict__ snr, int n, unsigned max_distance, unsigned *o_dm, unsigned *o_ts, unsigned *o_bw,
+    float *o_snr, int max_cands, int *count)
+{
+    __shared__ int s_dm[SPD_FILTER_THREADS], s_ts[SPD_FILTER_THREADS];
+    __shared__ float s_snr[SPD_FILTER_THREADS];
+    const int p = blockIdx.x * SPD_FILTER_THREADS + threadIdx.x;
+    const bool have = p < n;
+    const int d = have ? static_cast<int>(dm[p]) : 0;
+    const int t = have ? static_cast<int>(ts[p]) : 0;
+    const float sp = have ? snr[p] : 0.f;
+    bool keep = have;
+    for (int base = 0; base < n; base += SPD_FILTER_THREADS) {
+        const int q = base + threadIdx.x;
+        __syncthreads();
+        s_dm[threadIdx.x] = q < n ? static_cast<int>(dm[q]) : 0;
+        s_ts[threadIdx.x] = q < n ? static_cast<int>(ts[q]) : 0;
+        s_snr[threadIdx.x] = q < n ? snr[q] : -1000.f;
+        __syncthreads();
+        if (keep) {
+            for (int k = 0; k < SPD_FILTER_THREADS; ++k) {
+                if (s_snr[k] >= sp) {
+                    const float fs = static_cast<float>(s_dm[k]) - static_cast<float>(d);
+                    const float fd = static_cast<float>(s_ts[k]) - static_cast<float>(t);
+                    const float distance = (fd * fd + fs * fs);
+                    if ((distance < static_cast<float>(max_distance)) && (distance != 0)) {
+                        keep = false;
+                        break;
+                    }
+                }
+            }
+        }
+    }
+    if (keep) {
+        const int pos = atomicAdd(count, 1);
+        if (pos < max_cands) {
+            o_dm[pos] = dm[p];
+            o_ts[pos] = ts[p];
+            o_bw[pos] = bw[p];
+            o_snr[pos] = snr[p];
+        }
+    }
+}
+
 // Thresholding (src/aa_device_threshold_kernel.cu:10-41): every sample of
 // the rows 0 .. 4*floor(nDMs/4)-1 and columns < offset above the cut.
 // A block of 256 threads covers 1024 columns of one row, four per thread.
@@ -1074,6 +1182,33 @@ cudaError_t spd_peak_find(const float *d_snr, const uint16_t *d_taps, unsigned *
     const dim3 grid(1 + (width - offset - 1) / 32, 1 + (height - 1) / 2);
     k_peak_find<<<grid, block, 0, st>>>(d_snr, d_taps, d_dm, d_ts, d_csnr, d_bw, width, height, offset, threshold,
                                         max_cands, d_count, shift, dit_value);
+    ++g_spd_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t spd_peak_find_7x7(const float *d_snr, const uint16_t *d_taps, unsigned *d_dm, unsigned *d_ts, float *d_csnr,
+                              unsigned *d_bw, int width, int height, int offset, float threshold, int max_cands,
+                              int *d_count, int shift, int dit_value, cudaStream_t st)
+{
+    // launched when the iteration has searched columns; the stencil itself
+    // covers the whole interior, the unprocessed tail included
+    if (width - offset - 1 <= 0 || width < 7 || height < 7)
+        return cudaSuccess;
+    const dim3 grid((width + 127) / 128, (height - 6 + SPD_PF7_ROWS - 1) / SPD_PF7_ROWS);
+    k_peak_find_7x7<<<grid, 128, 0, st>>>(d_snr, d_taps, d_dm, d_ts, d_csnr, d_bw, width, height, threshold,
+                                          max_cands, d_count, shift, dit_value);
+    ++g_spd_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t spd_filter_peaks(const unsigned *d_dm, const unsigned *d_ts, const unsigned *d_bw, const float *d_snr,
+                             int n, unsigned max_distance, unsigned *o_dm, unsigned *o_ts, unsigned *o_bw,
+                             float *o_snr, int max_cands, int *d_count, cudaStream_t st)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    k_filter_peaks<<<(n + SPD_FILTER_THREADS - 1) / SPD_FILTER_THREADS, SPD_FILTER_THREADS, 0, st>>>(
+        d_dm, d_ts, d_bw, d_snr, n, max_distance, o_dm, o_ts, o_bw, o_snr, max_cands, d_count);
     ++g_spd_launches;
     return cudaGetLastError();
 }

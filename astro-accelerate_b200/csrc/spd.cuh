@@ -66,6 +66,14 @@ cudaError_t spdt_nth_plane(const float *d_input, const float *d_bv_in, float *d_
 cudaError_t spd_peak_find(const float *d_snr, const uint16_t *d_taps, unsigned *d_dm, unsigned *d_ts, float *d_csnr,
                           unsigned *d_bw, int width, int height, int offset, float threshold, int max_cands,
                           int *d_count, int shift, int dit_value, cudaStream_t st);
+// peak filtering: the 7 x 7 stencil peaks of one S/N plane, then the
+// filter over the whole list (max_distance: squared distance in trials and samples)
+cudaError_t spd_peak_find_7x7(const float *d_snr, const uint16_t *d_taps, unsigned *d_dm, unsigned *d_ts, float *d_csnr,
+                              unsigned *d_bw, int width, int height, int offset, float threshold, int max_cands,
+                              int *d_count, int shift, int dit_value, cudaStream_t st);
+cudaError_t spd_filter_peaks(const unsigned *d_dm, const unsigned *d_ts, const unsigned *d_bw, const float *d_snr,
+                             int n, unsigned max_distance, unsigned *o_dm, unsigned *o_ts, unsigned *o_bw,
+                             float *o_snr, int max_cands, int *d_count, cudaStream_t st);
 cudaError_t spd_threshold(const float *d_snr, const uint16_t *d_taps, unsigned *d_dm, unsigned *d_ts, float *d_csnr,
                           unsigned *d_bw, int *d_count, float threshold, int nTimesamples, int offset, int shift,
                           int max_cands, int dit_value, int nDMs, cudaStream_t st);
@@ -76,7 +84,8 @@ long long spd_kernel_launches();
 // Host side (spd_plane.cpp) -------------------------------------------------------
 
 // The analysis settings of include/aa_analysis_plan.hpp plus the range's
-// sampling; candidate_algorithm 0 peak finding, 1 thresholding.
+// sampling; candidate_algorithm 0 peak finding, 1 thresholding, 2 peak
+// filtering.
 struct SpdSettings {
     float sigma_cutoff = 6.f;
     float sigma_constant = 3.f;          // outlier-rejection multiplier
@@ -131,6 +140,7 @@ class SpdPlane {
   private:
     bool msd_profile(const float *d_input, int nDMs, int nT, const std::vector<int> &widths, const SpdSettings &s,
                      cudaStream_t st, std::string &err);
+    bool filter_peaks(SpdCandidates &out, size_t b, float tsamp, cudaStream_t st, std::string &err);
     void t_begin(int family, cudaStream_t st);
     void t_end(cudaStream_t st);
     bool t_collect();

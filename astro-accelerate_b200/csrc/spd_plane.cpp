@@ -419,8 +419,9 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
     }
     ev_family_.clear();
     ev_used_ = 0;
-    if (s.candidate_algorithm != 0 && s.candidate_algorithm != 1) {
-        err = "single-pulse detection: candidate_algorithm must be 0 (peak finding) or 1 (thresholding)";
+    if (s.candidate_algorithm < 0 || s.candidate_algorithm > 2) {
+        err = "single-pulse detection: candidate_algorithm must be 0 (peak finding), 1 (thresholding) or 2 "
+              "(peak filtering)";
         return false;
     }
     if (nDMs < 4 || nT < 128 || inBin < 1 || !(tsamp > 0.f)) {
@@ -499,6 +500,7 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
     }
 
     int dm_shift = 0;
+    SpdCandidates mine; // this run's list (the reference's host list of one analysis call)
     std::vector<unsigned> h_a, h_b, h_d;
     std::vector<float> h_c;
     for (size_t bi = 0; bi < dm_list.size(); ++bi) {
@@ -535,6 +537,10 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
             if (s.candidate_algorithm == 0)
                 e = spd_peak_find(d_snr + o, d_taps_ + o, c_dm, c_ts, c_snr, c_bw, p.decimated_timesamples, nd,
                                   p.unprocessed_samples, s.sigma_cutoff, local_max, d_count_, dm_shift, 1 << f, st);
+            else if (s.candidate_algorithm == 2)
+                e = spd_peak_find_7x7(d_snr + o, d_taps_ + o, c_dm, c_ts, c_snr, c_bw, p.decimated_timesamples, nd,
+                                      p.unprocessed_samples, s.sigma_cutoff, local_max, d_count_, dm_shift, 1 << f,
+                                      st);
             else if (p.decimated_timesamples - p.unprocessed_samples > 0)
                 e = spd_threshold(d_snr + o, d_taps_ + o, c_dm, c_ts, c_snr, c_bw, d_count_, s.sigma_cutoff,
                                   p.decimated_timesamples, p.decimated_timesamples - p.unprocessed_samples, dm_shift,
@@ -552,7 +558,7 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
         }
         if (count >= local_max)
             count = local_max; // list full: the later candidates were dropped
-        if (out.dm.size() + static_cast<size_t>(count) < host_capacity && count > 0) {
+        if (mine.dm.size() + static_cast<size_t>(count) < host_capacity && count > 0) {
             h_a.resize(count);
             h_b.resize(count);
             h_c.resize(count);
@@ -564,20 +570,17 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
                 err = "single-pulse detection: cudaMemcpy failed";
                 return false;
             }
-            out.dm.insert(out.dm.end(), h_a.begin(), h_a.end());
-            out.ts.insert(out.ts.end(), h_b.begin(), h_b.end());
-            out.snr.insert(out.snr.end(), h_c.begin(), h_c.end());
-            out.bw.insert(out.bw.end(), h_d.begin(), h_d.end());
+            mine.dm.insert(mine.dm.end(), h_a.begin(), h_a.end());
+            mine.ts.insert(mine.ts.end(), h_b.begin(), h_b.end());
+            mine.snr.insert(mine.snr.end(), h_c.begin(), h_c.end());
+            mine.bw.insert(mine.bw.end(), h_d.begin(), h_d.end());
         } else if (count > 0) {
             ++dropped_batches;
         }
         dm_shift += nd;
     }
-    if (time_kernels && !t_collect()) {
-        err = "single-pulse detection: event timing failed";
-        return false;
-    }
     if (keep_planes) {
+        // before peak filtering, which clears the S/N area
         last_snr.assign(2 * b, 0.f);
         last_taps.assign(2 * b, 0);
         if (cudaMemcpy(last_snr.data(), d_snr, 2 * b * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess ||
@@ -585,6 +588,93 @@ bool SpdPlane::run(float *d_plane, int nDMs, int nT, float tsamp, int inBin, con
             err = "single-pulse detection: cudaMemcpy failed";
             return false;
         }
+    }
+    if (s.candidate_algorithm == 2 && !filter_peaks(mine, b, tsamp, st, err))
+        return false;
+    out.dm.insert(out.dm.end(), mine.dm.begin(), mine.dm.end());
+    out.ts.insert(out.ts.end(), mine.ts.begin(), mine.ts.end());
+    out.snr.insert(out.snr.end(), mine.snr.begin(), mine.snr.end());
+    out.bw.insert(out.bw.end(), mine.bw.begin(), mine.bw.end());
+    if (time_kernels && !t_collect()) {
+        err = "single-pulse detection: event timing failed";
+        return false;
+    }
+    return true;
+}
+
+} // namespace aab200
+
+namespace aab200 {
+
+// The clustering step of peak filtering (src/aa_device_analysis.cu:360-412):
+// when the whole list of this run is shorter than one batch, the batch's
+// S/N area and candidate lists are cleared, the list is copied into the S/N
+// area in four consecutive arrays of b/4 entries (DM, sample, width, S/N --
+// in that order, so a list longer than b/4 overlaps its next array as in the
+// reference), filtered against a radius of 15 ms in samples, and the
+// survivors replace the list.
+bool SpdPlane::filter_peaks(SpdCandidates &out, size_t b, float tsamp, cudaStream_t st, std::string &err)
+{
+    const size_t total = out.dm.size();
+    if (!(b > total) || total == 0)
+        return true;
+    float *d_snr = d_work_ + 4 * (b / 4) + b / 2 + SPD_MAXTAPS + b;
+    const size_t q = b / 4;
+    unsigned *l_dm = reinterpret_cast<unsigned *>(d_snr);
+    unsigned *l_ts = reinterpret_cast<unsigned *>(d_snr + q);
+    unsigned *l_bw = reinterpret_cast<unsigned *>(d_snr + 2 * q);
+    float *l_snr = d_snr + 3 * q;
+    unsigned *c_dm = reinterpret_cast<unsigned *>(d_work_);
+    unsigned *c_ts = reinterpret_cast<unsigned *>(d_work_ + q);
+    float *c_snr = d_work_ + 2 * q;
+    unsigned *c_bw = reinterpret_cast<unsigned *>(d_work_ + 3 * q);
+    if (3 * q + total > 2 * b) {
+        err = "single-pulse detection: peak filtering list too long";
+        return false;
+    }
+    // PPF_SEARCH_RANGE_IN_MS = 15 (src/aa_params.hpp)
+    const int filter_size = static_cast<int>(15 * 0.001 / static_cast<double>(tsamp));
+    const unsigned max_distance = static_cast<unsigned>(filter_size) * static_cast<unsigned>(filter_size);
+    cudaError_t e = cudaMemsetAsync(d_snr, 0, b * sizeof(float), st);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(d_work_, 0, 4 * q * sizeof(float), st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(l_dm, out.dm.data(), total * sizeof(unsigned), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(l_ts, out.ts.data(), total * sizeof(unsigned), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(l_bw, out.bw.data(), total * sizeof(unsigned), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(l_snr, out.snr.data(), total * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(d_count_, 0, sizeof(int), st);
+    if (e == cudaSuccess) {
+        t_begin(4, st);
+        e = spd_filter_peaks(l_dm, l_ts, l_bw, l_snr, static_cast<int>(total), max_distance, c_dm, c_ts, c_bw, c_snr,
+                             static_cast<int>(std::min<size_t>(q, 2147483640u)), d_count_, st);
+        t_end(st);
+    }
+    int count = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&count, d_count_, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        err = std::string("single-pulse detection: ") + cudaGetErrorString(e);
+        return false;
+    }
+    const size_t k = std::min<size_t>(static_cast<size_t>(count), q);
+    out.dm.resize(k);
+    out.ts.resize(k);
+    out.snr.resize(k);
+    out.bw.resize(k);
+    if (k > 0 &&
+        (cudaMemcpy(out.dm.data(), c_dm, k * sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess ||
+         cudaMemcpy(out.ts.data(), c_ts, k * sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess ||
+         cudaMemcpy(out.bw.data(), c_bw, k * sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess ||
+         cudaMemcpy(out.snr.data(), c_snr, k * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)) {
+        err = "single-pulse detection: cudaMemcpy failed";
+        return false;
     }
     return true;
 }

@@ -122,7 +122,8 @@ int aa_py_total_computed_samples(void *obj);
 /* src/aa_py_analysis_plan.cpp:6-44 (aa_analysis_plan*, opaque): the
  * single-pulse detection settings; ddtr_strategy from
  * aa_py_pipeline_api_ddtr_strategy.  candidate_algorithm 0 peak finding,
- * 1 thresholding (2, peak filtering, is refused at bind). */
+ * 1 thresholding, 2 peak filtering (7 x 7 stencil peaks, then the
+ * suppression of weaker peaks within 15 ms). */
 void *aa_py_analysis_plan(const void *ddtr_strategy, float sigma_cutoff, float sigma_constant,
                           float max_boxcar_width_in_sec, int candidate_algorithm, bool enable_msd_baseline_noise);
 void aa_analysis_plan_delete(const void *obj);
@@ -479,8 +480,8 @@ int aa_b200_sps_block_samples(void);
 /* ---------------------------------------------------------------------------
  * Single-pulse detection with the reference's own rules: analysis_GPU
  * (src/aa_device_analysis.cu:130-345) on one DM-time plane [nDMs][nT] of
- * float32 in device memory, for candidate algorithms 0 (peak finding) and 1
- * (thresholding).  The MSD profile (src/aa_device_MSD_plane_profile.cu), the
+ * float32 in device memory, for candidate algorithms 0 (peak finding), 1
+ * (thresholding) and 2 (peak filtering).  The MSD profile (src/aa_device_MSD_plane_profile.cu), the
  * boxcar S/N planes (src/aa_device_SPS_long.cu:32-80) and the candidate
  * lists are bit-identical to the reference's; the order of the candidates
  * inside one batch follows the GPU's atomics, as in the reference.
@@ -523,6 +524,15 @@ int aa_b200_spd_profile(const void *obj, float *msd, int msd_cap, int *widths, i
 int aa_b200_spd_keep_planes(void *obj, int on);
 long long aa_b200_spd_planes(const void *obj, float *snr, unsigned short *taps, long long cap);
 long long aa_b200_spd_kernel_launches(void);
+/* The first boxcar S/N plane alone (call_kernel_SPDT_GPU_1st_plane of
+ * src/aa_device_SPS_long_kernel.cu, as tests/test_single_pulse_search_scan_1.cpp
+ * drives it): device input [nDMs][nTimesamples], outputs boxcar values and
+ * decimated sums [nDMs][dtm] (dtm = nTimesamples/2 rounded down to even), S/N
+ * and widths [nDMs][nTimesamples]; h_msd: host (mean, deviation) for widths
+ * 1..nBoxcars (8, 16 or 32).  Asynchronous on stream. */
+int aa_b200_spd_first_plane(const float *d_input, float *d_boxcar_values, float *d_decimated, float *d_snr,
+                            unsigned short *d_taps, const float *h_msd, int nTimesamples, int nBoxcars, int nDMs,
+                            void *stream);
 /* on != 0: CUDA events around every launch of the following runs; family_time
  * gives the last run's device time (ms) and launches of a family: 0 MSD
  * statistics, 1 decimations and boxcars of the MSD profile, 2 the first

@@ -309,8 +309,9 @@ int aaref_run_pipeline_spd(const unsigned short *input_tc, int nchans, int nsamp
         if ((long long)nchans * (long long)(s.t_processed()[0][0] + s.maxshift()) >= (1LL << 31))
             return -6;
         aa_analysis_plan::selectable_candidate_algorithm alg =
-            candidate_algorithm == 1 ? aa_analysis_plan::selectable_candidate_algorithm::threshold
-                                     : aa_analysis_plan::selectable_candidate_algorithm::peak_find;
+            candidate_algorithm == 1   ? aa_analysis_plan::selectable_candidate_algorithm::threshold
+            : candidate_algorithm == 2 ? aa_analysis_plan::selectable_candidate_algorithm::peak_filtering
+                                       : aa_analysis_plan::selectable_candidate_algorithm::peak_find;
         aa_analysis_plan ap(s, sigma_cutoff, sigma_constant, max_boxcar_width_in_sec, alg,
                             enable_msd_baseline_noise != 0);
         aa_analysis_strategy an(ap, &dev);

@@ -51,6 +51,14 @@ def run_one(name, q):
     csnr = np.zeros(MAX_CANDS, np.float32)
     cbw = np.zeros(MAX_CANDS, np.uint32)
     tsamp_r = np.float32(c["tsamp"] * c["inbin"])
+    # analysis_GPU prints the length of the list peak filtering starts from
+    # ("Number of peaks: N"); the C library's stdout goes to a file meanwhile
+    import re
+    import tempfile
+    sys.stdout.flush()
+    cap = tempfile.TemporaryFile(mode="w+b")
+    saved = os.dup(1)
+    os.dup2(cap.fileno(), 1)
     rc = L.aaref_spd(x.ctypes.data_as(P(f)), c["ndms"], c["nt"], float(tsamp_r), c["inbin"], c["max_width_s"],
                      c["sigma_constant"], c["baseline_noise"], c["cutoff"], c["algorithm"], 1.0, 0.0,
                      0.1 * c["ndms"], 0.1, msd.ctypes.data_as(P(f)), widths.ctypes.data_as(P(i)), ctypes.byref(nw),
@@ -58,6 +66,13 @@ def run_one(name, q):
                      taps.ctypes.data_as(P(ctypes.c_ushort)), 2 * n, cdm.ctypes.data_as(P(ctypes.c_uint)),
                      cts.ctypes.data_as(P(ctypes.c_uint)), csnr.ctypes.data_as(P(f)),
                      cbw.ctypes.data_as(P(ctypes.c_uint)), MAX_CANDS, ctypes.byref(nc), int(c.get("max_ts", 0)))
+    libc = ctypes.CDLL(None)
+    libc.fflush(None)
+    os.dup2(saved, 1)
+    os.close(saved)
+    cap.seek(0)
+    text = cap.read().decode(errors="replace")
+    unfiltered = [int(v) for v in re.findall(r"Number of peaks: (\d+);", text)]
     k = nc.value
     cands = sorted((int(cdm[j]), int(cts[j]), int(csnr[j:j + 1].view(np.uint32)[0]), int(cbw[j])) for j in range(k))
     q.put({"run": name, "rc": rc, "nwidths": nw.value, "widths": widths[:nw.value].tolist(),
@@ -66,7 +81,7 @@ def run_one(name, q):
            "snr_sha256": hashlib.sha256(snr.tobytes()).hexdigest(),
            "taps_sha256": hashlib.sha256(taps.tobytes()).hexdigest(),
            "ncands": k, "cands_sha256": hashlib.sha256(json.dumps(cands).encode()).hexdigest(),
-           "cands_head": cands[:64]})
+           "cands_head": cands[:64], "unfiltered_peaks": unfiltered})
 
 
 def run_pipeline(name, q):

@@ -31,6 +31,11 @@ CASES = {
     # 66 DM trials: batches of 64 and 2, thresholding skips rows past 4*floor(n/4)
     "ragged_dms_threshold": dict(ndms=66, nt=8192, seed=8, tsamp=64e-6, inbin=1, max_width_s=0.004,
                                  sigma_constant=3.0, baseline_noise=0, cutoff=5.0, algorithm=1),
+    # peak filtering: 7 x 7 stencil peaks, then weaker peaks within 15 ms dropped
+    "small_filter": dict(ndms=64, nt=16384, seed=1, tsamp=64e-6, inbin=1, max_width_s=0.004, sigma_constant=3.0,
+                         baseline_noise=0, cutoff=5.0, algorithm=2),
+    "wide_filter_outliers": dict(ndms=128, nt=32768, seed=9, tsamp=128e-6, inbin=2, max_width_s=0.03,
+                                 sigma_constant=3.0, baseline_noise=1, cutoff=5.5, algorithm=2),
 }
 
 # The reference runner with the analysis component on the DDTR cases of
@@ -42,6 +47,8 @@ PIPELINE_CASES = {
                                    max_width_s=0.005, algorithm=1, baseline_noise=1),
     "pipe_cache_peak": dict(ddtr="cache8", sigma_cutoff=5.5, sigma_constant=2.5, max_width_s=0.02, algorithm=0,
                             baseline_noise=1),
+    "pipe_binned_filter": dict(ddtr="shared8_binned", sigma_cutoff=5.0, sigma_constant=3.0, max_width_s=0.01,
+                               algorithm=2, baseline_noise=0),
 }
 
 
