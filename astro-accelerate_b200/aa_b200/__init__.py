@@ -205,6 +205,10 @@ def lib():
         "aa_py_analysis_plan_max_boxcar_width_in_sec": ([vp], f),
         "aa_py_analysis_plan_enable_msd_baseline_noise": ([vp], b),
         "aa_py_spd_nCandidates": ([vp], sz),
+        "aa_py_pipeline_api_analysis_strategy": ([vp], vp),
+        "aa_py_get_psr_nCandidates": ([vp], P(f)),
+        "aa_py_get_psr_interbin_nCandidates": ([vp], P(f)),
+        "aa_py_write_to_disk_psr_candidates": ([vp, ctypes.c_char_p], None),
         "aa_py_h_dm": ([vp], P(ctypes.c_uint)),
         "aa_py_h_ts": ([vp], P(ctypes.c_uint)),
         "aa_py_h_snr": ([vp], P(f)),

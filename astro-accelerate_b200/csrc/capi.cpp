@@ -378,6 +378,34 @@ bool aa_py_pipeline_api_bind_analysis_plan(void *obj, const void *plan)
     return true;
 }
 
+// :78-80: a new object per call (the reference never frees it); here the
+// bound analysis settings, or NULL when no analysis plan is bound.  Free with
+// aa_analysis_plan_delete.
+void *aa_py_pipeline_api_analysis_strategy(void *obj)
+{
+    Api *a = as_api(obj);
+    if (!a->analysis_bound)
+        return nullptr;
+    return new AnalysisPlan(a->aplan);
+}
+
+// :129-141: periodicity candidates; the periodicity component is refused by
+// this library, so there are none.
+float *aa_py_get_psr_nCandidates(void *obj)
+{
+    api_fail(as_api(obj), "periodicity search is not implemented by this library");
+    return nullptr;
+}
+float *aa_py_get_psr_interbin_nCandidates(void *obj)
+{
+    api_fail(as_api(obj), "periodicity search is not implemented by this library");
+    return nullptr;
+}
+void aa_py_write_to_disk_psr_candidates(void *obj, const char *)
+{
+    api_fail(as_api(obj), "periodicity search is not implemented by this library");
+}
+
 size_t aa_py_spd_nCandidates(void *obj) { return as_api(obj)->cands.dm.size(); }
 unsigned int *aa_py_h_dm(void *obj)
 {

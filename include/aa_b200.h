@@ -143,6 +143,14 @@ bool aa_py_pipeline_api_bind_analysis_plan(void *obj, const void *plan);
  * sample, S/N, boxcar width in samples of the range); the arrays stay valid
  * until the next step (NULL when there are none). */
 size_t aa_py_spd_nCandidates(void *obj);
+/* :78-80: the bound analysis settings as a new object (NULL when none is
+ * bound); free with aa_analysis_plan_delete. */
+void *aa_py_pipeline_api_analysis_strategy(void *obj);
+/* :129-141: periodicity candidates; periodicity is refused, so these return
+ * NULL (write does nothing) and set the pipeline's error message. */
+float *aa_py_get_psr_nCandidates(void *obj);
+float *aa_py_get_psr_interbin_nCandidates(void *obj);
+void aa_py_write_to_disk_psr_candidates(void *obj, const char *filename);
 unsigned int *aa_py_h_dm(void *obj);
 unsigned int *aa_py_h_ts(void *obj);
 float *aa_py_h_snr(void *obj);

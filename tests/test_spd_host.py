@@ -111,3 +111,19 @@ def test_periodicity_and_fdas_still_refused(aa):
                              np.zeros(256 * (1 << 15), np.uint16), 0)
     assert "periodicity" in pipe.last_error() or "only the dedispersion and analysis" in pipe.last_error()
     pipe.delete()
+
+
+def test_analysis_strategy_and_psr_entries(aa):
+    """aa_py_pipeline_api_analysis_strategy gives the bound settings (none
+    before bind); the periodicity candidate entries exist and return nothing."""
+    md = aa.filterbank_metadata_struct(0.0, 64e-6, 1500.0, -1.0, 8, 1 << 15, 256, 0.0)
+    o = aa.aa_py_pipeline_component_options()
+    pipe = aa.aa_py_pipeline(aa.aa_py_pipeline_components(True, True, False, False), o, md,
+                             np.zeros(256 * (1 << 15), np.uint16), 0)
+    L = aa.lib()
+    assert not L.aa_py_pipeline_api_analysis_strategy(pipe.m_obj)
+    assert not L.aa_py_get_psr_nCandidates(pipe.m_obj)
+    assert not L.aa_py_get_psr_interbin_nCandidates(pipe.m_obj)
+    L.aa_py_write_to_disk_psr_candidates(pipe.m_obj, b"unused")
+    assert "periodicity" in pipe.last_error()
+    pipe.delete()
