@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--variant", type=int, default=0,
                     help="0 auto, 1 generic kernels, 2 channel-quad, 3 subband, 4 warp-specialised channel-quad "
                          "(2-4 run the staged fp32 kernel on two-byte data)")
+    ap.add_argument("--with-analysis", action="store_true",
+                    help="add an e2e run through the C ABI with the analysis component after every step")
     ap.add_argument("--spd-nt", type=int, default=0, help="samples per DM trial of the spd config (default 2^19)")
     ap.add_argument("--nbits", type=int, default=0, help="bit depth of the synthetic filterbank (default: the config's)")
     return ap.parse_args()
@@ -654,6 +656,9 @@ def run_refine(args, rank, world, local):
 # 1536 x 2^19: the largest power-of-two plane of 1536 trials whose S/N-plane
 # offsets nDMs * output_shift stay below 2^31 in the reference's int arithmetic
 # (src/aa_device_SPS_long.cu:69,73; at 2^20 samples its analysis faults)
+# analysis settings of the DDTR + analysis measurement (--with-analysis)
+ANALYSIS = dict(sigma_cutoff=6.0, sigma_constant=3.0, max_width_s=0.01, algorithm=0, baseline_noise=1)
+
 SPD_WORKLOAD = dict(ndms=1536, nt=1 << 19, tsamp=64e-6, inbin=1, max_width_s=0.0164, sigma_cutoff=6.0,
                     sigma_constant=3.0, baseline_noise=1, algorithm=0, npulses=16, seed=31)
 
@@ -930,6 +935,39 @@ def main():
         x_host = xh.numpy().view(np.uint16)
         api.cleanUp()
         api.delete()
+        if args.with_analysis:
+            # the same run with the analysis component (single-pulse detection
+            # of every step's rows and its candidate files), as the reference
+            # runner does it
+            import tempfile
+            a = ANALYSIS
+            comps_a = aa.aa_py_pipeline_components(True, True, False, False)
+            api = aa.aa_py_pipeline(comps_a, opts, md, ctypes_ushort_ptr(xh), local)
+            if not api.bind_ddtr_plan(plan):
+                raise RuntimeError(api.last_error())
+            if not api.bind_analysis_plan(aa.aa_py_analysis_plan(a["sigma_cutoff"], a["sigma_constant"],
+                                                                 a["max_width_s"], a["algorithm"],
+                                                                 bool(a["baseline_noise"]))):
+                raise RuntimeError(api.last_error())
+            api.set_candidate_output(True, tempfile.mkdtemp(prefix="spd_cands_"))
+            walls, ncand = [], 0
+            for step in range(1 + args.e2e_steps):
+                torch.cuda.synchronize(device)
+                t0 = time.perf_counter()
+                api.rewind()
+                ncand = 0
+                while api.run():
+                    if api.status_code() == aa.STATUS_HAS_MORE:
+                        ncand += lib_spd_count(aa, api)
+                if api.status_code() == aa.STATUS_ERROR:
+                    raise RuntimeError(api.last_error())
+                torch.cuda.synchronize(device)
+                walls.append(time.perf_counter() - t0)
+            wall = statistics.median(walls[1:])
+            e2e["with_analysis"] = {"value": units * world / wall, "unit": "DM-trial*samples/s",
+                                    "ms_per_step": wall * 1e3, "candidates": ncand, "settings": a}
+            api.cleanUp()
+            api.delete()
         # the same run fed the samples as a SIGPROC file stores them
         # (aa_b200_pipeline_set_packed_input): nbits/16 of the H2D bytes
         if cfg["nbits"] <= 8:
@@ -1023,6 +1061,10 @@ def main():
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def lib_spd_count(aa, api) -> int:
+    return int(aa.lib().aa_py_spd_nCandidates(api.m_obj))
 
 
 def ctypes_ushort_ptr(t):

@@ -363,6 +363,70 @@ int aaref_run_pipeline_spd(const unsigned short *input_tc, int nchans, int nsamp
     return nsteps;
 }
 
+/* aaref_time_ddtr with the analysis component: the runner's run(status)
+ * loop with dedispersion, D2H (copy_to_host) and analysis_GPU after every
+ * step, wall clock after setup.  Candidate files go to the working
+ * directory; *ncands receives the candidates of all steps. */
+int aaref_time_pipeline_spd(const unsigned short *input_tc, int nchans, int nsamp, double tsamp, double fch1,
+                            double foff, int nbits, const harness_dm *plan, int nranges, int copy_to_host,
+                            float sigma_cutoff, float sigma_constant, float max_boxcar_width_in_sec,
+                            int candidate_algorithm, int enable_msd_baseline_noise, double *seconds,
+                            int *num_tchunks, long long *ncands)
+{
+    aa_device_info dev(0);
+    aa_ddtr_plan p;
+    for (int i = 0; i < nranges; i++)
+        p.add_dm(plan[i].low, plan[i].high, plan[i].step, plan[i].inBin, plan[i].outBin);
+    aa_filterbank_metadata meta(0.0, tsamp, nbits, nsamp, fch1, foff, nchans);
+    size_t fm = dev.free_memory();
+    {
+        aa_ddtr_strategy s(p, meta, fm, true, &dev);
+        if (!s.ready())
+            return -1;
+        *num_tchunks = s.num_tchunks();
+        if ((long long)nchans * (long long)(s.t_processed()[0][0] + s.maxshift()) >= (1LL << 31))
+            return -4;
+        aa_analysis_plan::selectable_candidate_algorithm alg =
+            candidate_algorithm == 1   ? aa_analysis_plan::selectable_candidate_algorithm::threshold
+            : candidate_algorithm == 2 ? aa_analysis_plan::selectable_candidate_algorithm::peak_filtering
+                                       : aa_analysis_plan::selectable_candidate_algorithm::peak_find;
+        aa_analysis_plan ap(s, sigma_cutoff, sigma_constant, max_boxcar_width_in_sec, alg,
+                            enable_msd_baseline_noise != 0);
+        aa_analysis_strategy an(ap, &dev);
+        if (!an.ready())
+            return -7;
+        aa_pipeline::pipeline comps;
+        comps.insert(aa_pipeline::component::dedispersion);
+        comps.insert(aa_pipeline::component::analysis);
+        aa_pipeline::pipeline_option opts;
+        if (copy_to_host)
+            opts.insert(aa_pipeline::component_option::copy_ddtr_data_to_host);
+        aa_periodicity_strategy per;
+        aa_fdas_strategy fd;
+        aa_jerk_strategy jk;
+        aa_permitted_pipelines_generic runner(comps, opts, s, an, per, fd, jk, false, false, false, false, false,
+                                              input_tc);
+        if (!runner.setup())
+            return -2;
+        cudaDeviceSynchronize();
+        long long total = 0;
+        auto t0 = std::chrono::steady_clock::now();
+        aa_pipeline_runner::status st;
+        while (runner.next(st)) {
+            if (st == aa_pipeline_runner::status::error)
+                return -3;
+            if (st == aa_pipeline_runner::status::has_more)
+                total += (long long)runner.get_SPD_nCandidates();
+        }
+        if (st == aa_pipeline_runner::status::error || cudaDeviceSynchronize() != cudaSuccess)
+            return -3;
+        auto t1 = std::chrono::steady_clock::now();
+        *seconds = std::chrono::duration<double>(t1 - t0).count();
+        *ncands = total;
+    }
+    return 0;
+}
+
 /* plane: host [nDMs][nT] float.  Outputs (caller-sized): msd [2 * nwidths]
  * (nwidths <= 256) and widths [nwidths]; snr/taps: the whole S/N and width
  * planes SPDT writes (plane_cap elements, at least 2 * nDMs * nT); the

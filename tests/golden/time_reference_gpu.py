@@ -33,6 +33,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--copy-to-host", action="store_true")
     ap.add_argument("--config", default="mid", choices=["survey", "mid"])
+    ap.add_argument("--analysis", action="store_true",
+                    help="with the analysis component (bench.py's ANALYSIS settings); candidate files go to a "
+                         "scratch directory")
     args = ap.parse_args()
     import torch
     import bench
@@ -48,6 +51,38 @@ def main():
                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
     L.aaref_time_ddtr.restype = ctypes.c_int
     sec, nt = ctypes.c_double(), ctypes.c_int()
+    if args.analysis:
+        import tempfile
+        a = bench.ANALYSIS
+        L.aaref_time_pipeline_spd.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                              ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.POINTER(R.DM),
+                                              ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                              ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_longlong)]
+        L.aaref_time_pipeline_spd.restype = ctypes.c_int
+        nc = ctypes.c_longlong()
+        here = os.getcwd()
+        os.chdir(tempfile.mkdtemp(prefix="spdtime_"))
+        try:
+            rc = L.aaref_time_pipeline_spd(host.ctypes.data, cfg["nchans"], cfg["nsamp"], cfg["tsamp"], cfg["fch1"],
+                                           cfg["foff"], cfg["nbits"], R._plan(cfg["plan"]), len(cfg["plan"]),
+                                           int(args.copy_to_host), a["sigma_cutoff"], a["sigma_constant"],
+                                           a["max_width_s"], a["algorithm"], a["baseline_noise"],
+                                           ctypes.byref(sec), ctypes.byref(nt), ctypes.byref(nc))
+        finally:
+            os.chdir(here)
+        if rc != 0:
+            raise SystemExit(f"reference run failed ({rc})")
+        import aa_b200 as aa
+        s = aa.strategy(cfg["plan"], cfg["nchans"], cfg["nsamp"], cfg["fch1"], cfg["foff"], cfg["tsamp"],
+                        cfg["nbits"])
+        units = sum(s["ndms"][r] * sum(s["t_processed"][r]) for r in range(len(s["ndms"])))
+        print(json.dumps({"impl": "reference-gpu", "config": args.config, "analysis": a,
+                          "copy_to_host": args.copy_to_host, "seconds": sec.value, "num_tchunks": nt.value,
+                          "candidates": nc.value, "units": units, "dm_trial_samples_per_s": units / sec.value}),
+              flush=True)
+        return
     rc = L.aaref_time_ddtr(host.ctypes.data, cfg["nchans"], cfg["nsamp"], cfg["tsamp"], cfg["fch1"], cfg["foff"],
                            cfg["nbits"], R._plan(cfg["plan"]), len(cfg["plan"]), int(args.copy_to_host),
                            ctypes.byref(sec), ctypes.byref(nt))
