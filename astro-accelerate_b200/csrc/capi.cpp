@@ -51,7 +51,7 @@ struct Api {
     bool analysis_bound = false;
     AnalysisPlan aplan{};
     std::unique_ptr<SpdPlane> spd;
-    float *d_spd_plane = nullptr; // a copy of the step's rows when they must be kept
+    float *d_spd_plane = nullptr; // the step's rows, copied for the analysis (which overwrites them)
     long long spd_max_ts = 0;     // batch size; 0 = the reference's rule from free memory
     size_t spd_capacity = 0;      // host candidate list size (SPD_max_peak_size)
     SpdCandidates cands;          // the last step's candidates
@@ -128,9 +128,6 @@ bool run_analysis(Api *a)
     StepPlane sp;
     if (!P.last_step_plane(sp))
         return api_fail(a, "analysis: no dedispersed rows");
-    // the rows are copied to the host first (save_data before the analysis)
-    if (!P.synchronize())
-        return api_fail(a, P.last_error());
     const DdtrStrategy &s = P.strategy();
     std::string err;
     if (!a->spd) {
@@ -150,25 +147,21 @@ bool run_analysis(Api *a)
         std::unique_ptr<SpdPlane> spd(new SpdPlane());
         if (!spd->setup(max_elems, max_ts, err))
             return api_fail(a, "analysis: " + err);
-        if (a->popt.device_output &&
-            cudaMalloc(&a->d_spd_plane, static_cast<size_t>(max_elems) * sizeof(float)) != cudaSuccess)
+        if (cudaMalloc(&a->d_spd_plane, static_cast<size_t>(max_elems) * sizeof(float)) != cudaSuccess)
             return api_fail(a, "analysis: cudaMalloc failed");
         // include/aa_permitted_pipelines_generic.hpp:376-377
         a->spd_capacity = static_cast<size_t>(s.max_ndms()) * static_cast<size_t>(s.t_processed()[0][0]) / 2;
         a->spd = std::move(spd);
     }
-    float *plane = sp.d;
-    if (a->popt.device_output || sp.pitch != sp.tp) {
-        // the search decimates into its input: work on a copy of rows that are kept
-        if (!a->d_spd_plane &&
-            cudaMalloc(&a->d_spd_plane, static_cast<size_t>(sp.ndms) * sp.tp * sizeof(float)) != cudaSuccess)
-            return api_fail(a, "analysis: cudaMalloc failed");
-        if (cudaMemcpy2DAsync(a->d_spd_plane, static_cast<size_t>(sp.tp) * sizeof(float), sp.d,
-                              static_cast<size_t>(sp.pitch) * sizeof(float), static_cast<size_t>(sp.tp) * sizeof(float),
-                              static_cast<size_t>(sp.ndms), cudaMemcpyDeviceToDevice, P.stream()) != cudaSuccess)
-            return api_fail(a, "analysis: cudaMemcpy2DAsync failed");
-        plane = a->d_spd_plane;
-    }
+    // The search decimates into its input, and the step's rows are still
+    // being copied to the host (or are the kept device output): it works on a
+    // device copy, taken on the pipeline's stream after the dedispersion, so
+    // the copy to the host overlaps the search as it overlaps the next step.
+    if (cudaMemcpy2DAsync(a->d_spd_plane, static_cast<size_t>(sp.tp) * sizeof(float), sp.d,
+                          static_cast<size_t>(sp.pitch) * sizeof(float), static_cast<size_t>(sp.tp) * sizeof(float),
+                          static_cast<size_t>(sp.ndms), cudaMemcpyDeviceToDevice, P.stream()) != cudaSuccess)
+        return api_fail(a, "analysis: cudaMemcpy2DAsync failed");
+    float *plane = a->d_spd_plane;
     const DmRange &d = s.dm(sp.range);
     const float tsamp_original = static_cast<float>(a->meta.tsamp);
     const float tsamp = tsamp_original * static_cast<float>(d.inBin);
