@@ -215,6 +215,10 @@ def lib():
         "aa_py_h_width": ([vp], P(ctypes.c_uint)),
         "aa_b200_pipeline_set_candidate_output": ([vp, i, ctypes.c_char_p], b),
         "aa_b200_pipeline_set_analysis_batch": ([vp, ll], b),
+        "aa_b200_psr_power_interbin": ([vp, vp, vp, i, i, vp], i),
+        "aa_b200_psr_harmonic_sum_simple": ([vp, vp, vp, vp, i, i, i, vp], i),
+        "aa_b200_psr_kernel_launches": ([], ll),
+        "aa_b200_psr_last_error": ([], ctypes.c_char_p),
         "aa_b200_spd_create": ([ll, ll], vp),
         "aa_b200_spd_destroy": ([vp], None),
         "aa_b200_spd_last_error": ([vp], ctypes.c_char_p),

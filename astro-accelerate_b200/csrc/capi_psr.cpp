@@ -1,0 +1,47 @@
+// capi_psr.cpp -- extern "C" entry points of the periodicity building blocks
+// (aa_b200_psr_*, declared in include/aa_b200.h).
+#include "aa_b200.h"
+
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "psr.cuh"
+
+using namespace aab200;
+
+namespace {
+thread_local std::string g_psr_error;
+
+int psr_status(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess)
+        return 0;
+    g_psr_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return 1;
+}
+} // namespace
+
+extern "C" {
+
+int aa_b200_psr_power_interbin(const void *d_spectra, float *d_power, float *d_interbin, int nTimesamples, int nDMs,
+                               void *stream)
+{
+    return psr_status(psr_power_interbin(static_cast<const float2 *>(d_spectra), d_power, d_interbin, nTimesamples,
+                                         nDMs, static_cast<cudaStream_t>(stream)),
+                      "power and interbin spectra");
+}
+
+int aa_b200_psr_harmonic_sum_simple(const float *d_input, float *d_snr, unsigned short *d_harmonics,
+                                    const float *d_msd, int nBins, int nSpectra, int nHarmonics, void *stream)
+{
+    return psr_status(psr_harmonic_sum_simple(d_input, d_snr, d_harmonics, d_msd, nBins, nSpectra, nHarmonics,
+                                              static_cast<cudaStream_t>(stream)),
+                      "harmonic sum");
+}
+
+long long aa_b200_psr_kernel_launches(void) { return psr_kernel_launches(); }
+
+const char *aa_b200_psr_last_error(void) { return g_psr_error.c_str(); }
+
+} // extern "C"

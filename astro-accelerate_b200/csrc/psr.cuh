@@ -1,0 +1,31 @@
+// psr.cuh -- building blocks of the reference's periodicity search
+// (src/aa_device_periods.cu:368-541): the power and interbin spectra of
+// batched real-to-complex spectra, and the simple harmonic sum over
+// corner-turned power spectra.  Each keeps the float expressions of the
+// reference kernel it follows (cited per function), so the spectra and the
+// harmonic S/N values are bit-identical to the reference's.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace aab200 {
+
+// in: nDMs spectra of nT/2+1 complex bins (cufftExecR2C output, row pitch
+// nT/2+1); power [nDMs][nT/2] = |X_k / sqrt(nT)|^2 for 0 < k < nT/2 (0 at
+// k = 0); interbin [nDMs][nT]: even entries the power, odd entries
+// 0.616850275 |X_k - X_{k+1}|^2 (normalised).
+cudaError_t psr_power_interbin(const float2 *d_in, float *d_power, float *d_interbin, int nTimesamples, int nDMs,
+                               cudaStream_t st);
+
+// in [nBins][nSpectra] (bins outer, spectra inner); for every bin b and
+// spectrum s the best S/N of the sums of harmonics 0..f at bins b, 2b, ...,
+// (f+1)b (below nBins), S/N_f = (sum - msd[2f]) / msd[2f+1], and the f of
+// the best one.  d_msd: device (mean, deviation) per harmonic count.
+cudaError_t psr_harmonic_sum_simple(const float *d_in, float *d_snr, uint16_t *d_harmonics, const float *d_msd,
+                                    int nBins, int nSpectra, int nHarmonics, cudaStream_t st);
+
+long long psr_kernel_launches();
+
+} // namespace aab200

@@ -563,6 +563,28 @@ int aa_b200_spd_write_candidates(const char *dir, int candidate_algorithm, float
                                  float dm_step, float tsamp, int inBin, const unsigned *dm, const unsigned *ts,
                                  const float *snr, const unsigned *bw, size_t n);
 
+/* ---------------------------------------------------------------------------
+ * Periodicity building blocks (the reference's periodicity component,
+ * src/aa_device_periods.cu:368-541, is not built yet; these are two of its
+ * stages, bit-identical to the reference's kernels).  Device pointers;
+ * return 0 or 1 (message in aa_b200_psr_last_error).
+ *
+ * power_interbin (src/aa_device_power.cu:34-52): d_spectra holds nDMs
+ * spectra of nTimesamples/2+1 complex float bins (cufftExecR2C output);
+ * power [nDMs][nTimesamples/2] and interbin [nDMs][nTimesamples] spectra
+ * normalised by sqrt(nTimesamples).
+ * harmonic_sum_simple (src/aa_device_harmonic_summing.cu:11-37): input
+ * [nBins][nSpectra]; per bin and spectrum the best S/N of harmonic sums up to
+ * nHarmonics (d_msd: device (mean, deviation) per harmonic count) and the
+ * number of added harmonics.
+ * --------------------------------------------------------------------------- */
+int aa_b200_psr_power_interbin(const void *d_spectra, float *d_power, float *d_interbin, int nTimesamples, int nDMs,
+                               void *stream);
+int aa_b200_psr_harmonic_sum_simple(const float *d_input, float *d_snr, unsigned short *d_harmonics,
+                                    const float *d_msd, int nBins, int nSpectra, int nHarmonics, void *stream);
+long long aa_b200_psr_kernel_launches(void);
+const char *aa_b200_psr_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,8 @@
 #include "aa_device_BC_plan.hpp"
 #include "aa_device_MSD_plane_profile.hpp"
 #include "aa_device_SPS_long.hpp"
+#include "aa_device_power.hpp"
+#include "aa_device_harmonic_summing.hpp"
 
 namespace astroaccelerate {
 /* defined in src/aa_device_analysis.cu without a header declaration */
@@ -425,6 +427,50 @@ int aaref_time_pipeline_spd(const unsigned short *input_tc, int nchans, int nsam
         *ncands = total;
     }
     return 0;
+}
+
+/* Two stages of the reference's periodicity search on given host data:
+ * simple_power_and_interbin (src/aa_device_power.cu:34-52) on nDMs spectra
+ * of nT/2+1 complex bins (spectra: 2*nDMs*(nT/2+1) floats) into power
+ * [nDMs][nT/2] and interbin [nDMs][nT]; periodicity_simple_harmonic_summing
+ * (src/aa_device_harmonic_summing.cu:11-37) on hs_in [nBins][nSpectra] with
+ * msd [2*nH] into snr and harmonics [nBins][nSpectra].  Returns 0 or < 0. */
+int aaref_psr_blocks(const float *spectra, int nT, int nDMs, float *power, float *interbin, const float *hs_in,
+                     int nBins, int nSpectra, const float *msd, int nH, float *snr, unsigned short *harm)
+{
+    const size_t ns = 2 * (size_t)nDMs * (size_t)((nT >> 1) + 1);
+    const size_t np = (size_t)nDMs * (size_t)(nT >> 1), ni = (size_t)nDMs * (size_t)nT;
+    const size_t nh = (size_t)nBins * (size_t)nSpectra;
+    float *d_spec = NULL, *d_pow = NULL, *d_ib = NULL, *d_hs = NULL, *d_snr = NULL, *d_msd = NULL;
+    unsigned short *d_harm = NULL;
+    if (cudaMalloc((void **)&d_spec, ns * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_pow, np * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_ib, ni * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_hs, nh * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_snr, nh * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_harm, nh * sizeof(unsigned short)) != cudaSuccess ||
+        cudaMalloc((void **)&d_msd, 2 * (size_t)nH * sizeof(float)) != cudaSuccess)
+        return -3;
+    cudaMemcpy(d_spec, spectra, ns * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_hs, hs_in, nh * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_msd, msd, 2 * (size_t)nH * sizeof(float), cudaMemcpyHostToDevice);
+    simple_power_and_interbin((float2 *)d_spec, d_pow, d_ib, nT, nDMs);
+    periodicity_simple_harmonic_summing(d_hs, d_snr, d_harm, d_msd, nBins, nSpectra, nH);
+    int rc = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess)
+        rc = -5;
+    cudaMemcpy(power, d_pow, np * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaMemcpy(interbin, d_ib, ni * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaMemcpy(snr, d_snr, nh * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaMemcpy(harm, d_harm, nh * sizeof(unsigned short), cudaMemcpyDeviceToHost);
+    cudaFree(d_spec);
+    cudaFree(d_pow);
+    cudaFree(d_ib);
+    cudaFree(d_hs);
+    cudaFree(d_snr);
+    cudaFree(d_harm);
+    cudaFree(d_msd);
+    return rc;
 }
 
 /* plane: host [nDMs][nT] float.  Outputs (caller-sized): msd [2 * nwidths]

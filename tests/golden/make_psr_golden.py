@@ -1,0 +1,78 @@
+"""Generates tests/golden/psr_golden.json from the reference's own GPU
+periodicity stages (oracle/ref_harness.cu aaref_psr_blocks:
+simple_power_and_interbin and periodicity_simple_harmonic_summing) on the
+seeded inputs of psr_cases.py: SHA-256 of every output and its first
+values.  Needs a GPU.
+
+    python tests/golden/make_psr_golden.py --out gpurun_out/golden/psr_golden.json
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+
+import psr_cases as P  # noqa: E402
+import refharness as R  # noqa: E402
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden", "psr_golden.json"))
+    args = ap.parse_args()
+    L = R.load()
+    Pf, i = ctypes.POINTER(ctypes.c_float), ctypes.c_int
+    L.aaref_psr_blocks.argtypes = [Pf, i, i, Pf, Pf, Pf, i, i, Pf, i, Pf, ctypes.POINTER(ctypes.c_ushort)]
+    L.aaref_psr_blocks.restype = i
+    out = {"generator": "tests/golden/make_psr_golden.py", "reference": "AstroAccelerate v1.3.1", "power": {},
+           "harmonic": {}}
+    hc = next(iter(P.HARMONIC_CASES.values()))
+    for name, c in P.POWER_CASES.items():
+        spec = P.make_spectra(c)
+        pw = np.zeros(c["ndms"] * (c["nt"] >> 1), np.float32)
+        ib = np.zeros(c["ndms"] * c["nt"], np.float32)
+        x, msd = P.make_harmonic_input(hc)
+        snr = np.zeros(x.size, np.float32)
+        hm = np.zeros(x.size, np.uint16)
+        rc = L.aaref_psr_blocks(spec.ctypes.data_as(Pf), c["nt"], c["ndms"], pw.ctypes.data_as(Pf),
+                                ib.ctypes.data_as(Pf), x.ctypes.data_as(Pf), hc["nbins"], hc["nspectra"],
+                                msd.ctypes.data_as(Pf), hc["nh"], snr.ctypes.data_as(Pf),
+                                hm.ctypes.data_as(ctypes.POINTER(ctypes.c_ushort)))
+        out["power"][name] = {"rc": rc, "power_sha256": hashlib.sha256(pw.tobytes()).hexdigest(),
+                              "interbin_sha256": hashlib.sha256(ib.tobytes()).hexdigest(),
+                              "power_head": pw[:256].view(np.uint32).tolist(),
+                              "interbin_head": ib[:256].view(np.uint32).tolist()}
+        print(name, rc, flush=True)
+    for name, c in P.HARMONIC_CASES.items():
+        cp = next(iter(P.POWER_CASES.values()))
+        spec = P.make_spectra(cp)
+        pw = np.zeros(cp["ndms"] * (cp["nt"] >> 1), np.float32)
+        ib = np.zeros(cp["ndms"] * cp["nt"], np.float32)
+        x, msd = P.make_harmonic_input(c)
+        snr = np.zeros(x.size, np.float32)
+        hm = np.zeros(x.size, np.uint16)
+        rc = L.aaref_psr_blocks(spec.ctypes.data_as(Pf), cp["nt"], cp["ndms"], pw.ctypes.data_as(Pf),
+                                ib.ctypes.data_as(Pf), x.ctypes.data_as(Pf), c["nbins"], c["nspectra"],
+                                msd.ctypes.data_as(Pf), c["nh"], snr.ctypes.data_as(Pf),
+                                hm.ctypes.data_as(ctypes.POINTER(ctypes.c_ushort)))
+        out["harmonic"][name] = {"rc": rc, "snr_sha256": hashlib.sha256(snr.tobytes()).hexdigest(),
+                                 "harmonics_sha256": hashlib.sha256(hm.tobytes()).hexdigest(),
+                                 "snr_head": snr[:512].view(np.uint32).tolist(), "harmonics_head": hm[:512].tolist()}
+        print(name, rc, flush=True)
+    os.makedirs(os.path.dirname(args.out), exist_ok=True)
+    with open(args.out, "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", args.out)
+
+
+if __name__ == "__main__":
+    main()

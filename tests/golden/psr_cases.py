@@ -1,0 +1,47 @@
+"""Seeded inputs for the periodicity building blocks: complex spectra as
+cufftExecR2C writes them (nT/2+1 bins per DM trial) and corner-turned power
+spectra [bins][spectra] with a (mean, deviation) per harmonic count."""
+from __future__ import annotations
+
+import numpy as np
+
+POWER_CASES = {
+    "pow_8192x24": dict(nt=8192, ndms=24, seed=1),
+    "pow_6000x7": dict(nt=6000, ndms=7, seed=2),
+    "pow_4097x3": dict(nt=4097, ndms=3, seed=3),
+}
+HARMONIC_CASES = {
+    "hs_4097x100_h32": dict(nbins=4097, nspectra=100, nh=32, seed=4),
+    "hs_1000x64_h8": dict(nbins=1000, nspectra=64, nh=8, seed=5),
+    "hs_513x7_h16": dict(nbins=513, nspectra=7, nh=16, seed=6),
+}
+
+
+def make_spectra(c) -> np.ndarray:
+    """[ndms][nt/2+1] complex64 as interleaved float32 pairs: noise spectra of
+    N(0, sqrt(nt)) with a few strong periodic lines."""
+    rng = np.random.Generator(np.random.PCG64(c["seed"]))
+    nb = (c["nt"] >> 1) + 1
+    z = (rng.normal(0, 1, (c["ndms"], nb)) + 1j * rng.normal(0, 1, (c["ndms"], nb))) * np.sqrt(c["nt"] / 2)
+    for d in range(c["ndms"]):
+        k = int(rng.integers(5, nb // 8))
+        for h in range(1, 6):
+            if h * k < nb:
+                z[d, h * k] += (8.0 / h) * np.sqrt(c["nt"]) * np.exp(1j * rng.uniform(0, 2 * np.pi))
+    return np.ascontiguousarray(z.astype(np.complex64)).view(np.float32).reshape(c["ndms"], 2 * nb)
+
+
+def make_harmonic_input(c):
+    """(input [nbins][nspectra] float32, msd [2*nh] float32)."""
+    rng = np.random.Generator(np.random.PCG64(c["seed"]))
+    x = rng.exponential(1.0, (c["nbins"], c["nspectra"])).astype(np.float32)
+    for s in range(c["nspectra"]):
+        k = int(rng.integers(3, max(4, c["nbins"] // 16)))
+        for h in range(1, 9):
+            if h * k < c["nbins"]:
+                x[h * k, s] += np.float32(6.0 / h)
+    f = np.arange(c["nh"], dtype=np.float32)
+    msd = np.empty(2 * c["nh"], np.float32)
+    msd[0::2] = f + 1
+    msd[1::2] = np.sqrt(f + 1)
+    return x, msd

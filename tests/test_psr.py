@@ -1,0 +1,87 @@
+"""Periodicity building blocks (the reference's simple_power_and_interbin
+and simple harmonic sum): the CPU restatement against the reference's GPU
+values (tests/golden/psr_golden.json, no GPU needed), and the library's
+kernels bit for bit against the reference on the GPU."""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import psr_cases as P
+import psr_oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "psr_golden.json")
+
+
+@pytest.fixture(scope="module")
+def golden():
+    if not os.path.exists(GOLDEN):
+        pytest.skip("periodicity golden vectors not generated (tests/golden/make_psr_golden.py)")
+    with open(GOLDEN) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("name", list(P.POWER_CASES))
+def test_power_oracle_matches_reference(golden, name):
+    c = P.POWER_CASES[name]
+    g = golden["power"][name]
+    pw, ib = O.power_interbin(P.make_spectra(c), c["nt"])
+    ref_p = np.array(g["power_head"], np.uint32).view(np.float32)
+    ref_i = np.array(g["interbin_head"], np.uint32).view(np.float32)
+    # the reference divides with the fast division and may fuse the products;
+    # the interbin differences cancel, so their relative error grows
+    assert np.allclose(pw.reshape(-1)[:ref_p.size], ref_p, rtol=2e-6, atol=0)
+    assert np.allclose(ib.reshape(-1)[:ref_i.size], ref_i, rtol=1e-5, atol=1e-7)
+
+
+@pytest.mark.parametrize("name", list(P.HARMONIC_CASES))
+def test_harmonic_oracle_matches_reference(golden, name):
+    c = P.HARMONIC_CASES[name]
+    g = golden["harmonic"][name]
+    x, msd = P.make_harmonic_input(c)
+    snr, harm = O.harmonic_sum_simple(x, msd, c["nh"])
+    ref_s = np.array(g["snr_head"], np.uint32).view(np.float32)
+    ref_h = np.array(g["harmonics_head"], np.uint16)
+    k = ref_s.size
+    assert np.allclose(snr.reshape(-1)[:k], ref_s, rtol=1e-6, atol=1e-6)
+    assert (harm.reshape(-1)[:k] != ref_h).mean() < 0.01  # near-ties may pick another harmonic count
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(P.POWER_CASES))
+def test_power_interbin_matches_reference_gpu(aa, golden, name):
+    import torch
+    c = P.POWER_CASES[name]
+    g = golden["power"][name]
+    spec = torch.from_numpy(P.make_spectra(c)).cuda()
+    pw = torch.zeros(c["ndms"] * (c["nt"] >> 1), device="cuda")
+    ib = torch.zeros(c["ndms"] * c["nt"], device="cuda")
+    n0 = aa.lib().aa_b200_psr_kernel_launches()
+    assert aa.lib().aa_b200_psr_power_interbin(spec.data_ptr(), pw.data_ptr(), ib.data_ptr(), c["nt"], c["ndms"],
+                                                None) == 0
+    torch.cuda.synchronize()
+    assert aa.lib().aa_b200_psr_kernel_launches() > n0
+    assert hashlib.sha256(pw.cpu().numpy().tobytes()).hexdigest() == g["power_sha256"]
+    assert hashlib.sha256(ib.cpu().numpy().tobytes()).hexdigest() == g["interbin_sha256"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(P.HARMONIC_CASES))
+def test_harmonic_sum_matches_reference_gpu(aa, golden, name):
+    import torch
+    c = P.HARMONIC_CASES[name]
+    g = golden["harmonic"][name]
+    x, msd = P.make_harmonic_input(c)
+    dx = torch.from_numpy(x).cuda()
+    dm = torch.from_numpy(msd).cuda()
+    snr = torch.zeros(x.size, device="cuda")
+    hm = torch.zeros(x.size, dtype=torch.int16, device="cuda")
+    assert aa.lib().aa_b200_psr_harmonic_sum_simple(dx.data_ptr(), snr.data_ptr(), hm.data_ptr(), dm.data_ptr(),
+                                                     c["nbins"], c["nspectra"], c["nh"], None) == 0
+    torch.cuda.synchronize()
+    assert hashlib.sha256(snr.cpu().numpy().tobytes()).hexdigest() == g["snr_sha256"]
+    assert hashlib.sha256(hm.cpu().numpy().view(np.uint16).tobytes()).hexdigest() == g["harmonics_sha256"]
