@@ -229,6 +229,7 @@ def lib():
         "aa_b200_spd_planes": ([vp, vp, vp, ll], ll),
         "aa_b200_spd_kernel_launches": ([], ll),
         "aa_b200_spd_plan": ([i, f, i, f, vp, i, P(i), P(i), P(i), vp, i, P(i)], i),
+        "aa_b200_spd_msd_profile": ([vp, vp, i, i, P(i), i, i, f, i, vp, vp], i),
         "aa_b200_spd_time_kernels": ([vp, i], i),
         "aa_b200_spd_first_plane": ([vp, vp, vp, vp, vp, vp, i, i, i, vp], i),
         "aa_b200_spd_family_time": ([vp, i, P(d), P(ll)], i),
@@ -904,6 +905,19 @@ class single_pulse_detection:
 
     def time_kernels(self, on: bool = True):
         lib().aa_b200_spd_time_kernels(self.m_obj, int(on))
+
+    def msd_profile(self, d_plane, ndms: int, nt: int, widths, high_memory: bool = False,
+                    sigma_constant: float = 3.0, outlier_rejection: bool = False, stream: int = 0):
+        """(mean, deviation) per width of the MSD plane profile, float32 [2*len(widths)]."""
+        w = np.ascontiguousarray(widths, np.int32)
+        out = np.zeros(2 * w.size, np.float32)
+        ptr = d_plane if isinstance(d_plane, int) else d_plane.data_ptr()
+        if lib().aa_b200_spd_msd_profile(self.m_obj, ctypes.c_void_p(ptr), int(ndms), int(nt),
+                                         w.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), w.size, int(high_memory),
+                                         float(sigma_constant), int(outlier_rejection), out.ctypes.data,
+                                         ctypes.c_void_p(stream)):
+            raise RuntimeError(self.last_error())
+        return out
 
     def family_times(self) -> dict:
         """Device ms and launches per launch family of the last run (time_kernels on)."""

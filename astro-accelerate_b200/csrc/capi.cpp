@@ -486,6 +486,12 @@ long aa_py_current_inc(void *obj)
 bool aa_py_cleanup(void *obj)
 {
     Api *a = as_api(obj);
+    // the analysis buffers go with the pipeline's (the runner frees its SPD
+    // work area in its cleanup, include/aa_permitted_pipelines_generic.hpp:205-240);
+    // a later step sets them up again
+    a->spd.reset();
+    cudaFree(a->d_spd_plane);
+    a->d_spd_plane = nullptr;
     return a->pipe ? a->pipe->cleanup() : true;
 }
 

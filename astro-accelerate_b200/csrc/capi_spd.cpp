@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <new>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -152,6 +153,29 @@ long long aa_b200_spd_planes(const void *obj, float *snr, unsigned short *taps, 
 }
 
 long long aa_b200_spd_kernel_launches(void) { return spd_kernel_launches(); }
+
+int aa_b200_spd_msd_profile(void *obj, const float *d_input, int nDMs, int nTimesamples, const int *widths,
+                            int nwidths, int high_memory, float sigma_constant, int outlier_rejection, float *h_msd,
+                            void *stream)
+{
+    SpdHandle *h = as_spd(obj);
+    if (!h)
+        return 1;
+    if (!d_input || !widths || nwidths < 1 || !h_msd) {
+        h->error = "MSD profile: null argument";
+        return 1;
+    }
+    std::vector<int> w(widths, widths + nwidths);
+    std::string err;
+    if (!h->plane.profile(d_input, nDMs, nTimesamples, w, high_memory != 0, sigma_constant, outlier_rejection != 0,
+                          static_cast<cudaStream_t>(stream), err)) {
+        h->error = err;
+        return 1;
+    }
+    for (size_t i = 0; i < h->plane.last_msd.size(); ++i)
+        h_msd[i] = h->plane.last_msd[i];
+    return 0;
+}
 
 int aa_b200_spd_first_plane(const float *d_input, float *d_boxcar_values, float *d_decimated, float *d_snr,
                             unsigned short *d_taps, const float *h_msd, int nTimesamples, int nBoxcars, int nDMs,

@@ -120,6 +120,11 @@ class SpdPlane {
              cudaStream_t st, std::string &err, size_t host_capacity = SIZE_MAX);
     // zero the whole work area (the state of a fresh allocation)
     cudaError_t clear(cudaStream_t st);
+    // The MSD plane profile alone on [nDMs][nT] for the given ascending
+    // widths (high_memory: the width-2 decimation in one piece, as the
+    // periodicity search runs it); the result in last_msd.
+    bool profile(const float *d_input, int nDMs, int nT, const std::vector<int> &widths, bool high_memory,
+                 float sigma_constant, bool outlier_rejection, cudaStream_t st, std::string &err);
     // intermediate results of the last run (for tests)
     std::vector<float> last_msd;
     std::vector<int> last_widths;
@@ -139,7 +144,7 @@ class SpdPlane {
 
   private:
     bool msd_profile(const float *d_input, int nDMs, int nT, const std::vector<int> &widths, const SpdSettings &s,
-                     cudaStream_t st, std::string &err);
+                     cudaStream_t st, std::string &err, bool high_memory = false);
     bool filter_peaks(SpdCandidates &out, size_t b, float tsamp, cudaStream_t st, std::string &err);
     void t_begin(int family, cudaStream_t st);
     void t_end(cudaStream_t st);

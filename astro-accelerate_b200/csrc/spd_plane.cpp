@@ -222,14 +222,15 @@ void SpdPlane::release()
 // sudy, lichy and the statistics sit where the reference puts them in its
 // work area.
 bool SpdPlane::msd_profile(const float *d_input, int nDMs, int nT, const std::vector<int> &widths,
-                           const SpdSettings &s, cudaStream_t st, std::string &err)
+                           const SpdSettings &s, cudaStream_t st, std::string &err, bool high_memory)
 {
     const int max_width = widths.back();
     const int nDec = ilog2(max_width) + 1;
     const size_t datasize = static_cast<size_t>(nT) * static_cast<size_t>(nDMs);
     float *sudy = d_work_;
     float *lichy = d_work_ + datasize / 4;
-    float *msd_dit = d_work_ + datasize / 2;
+    // the high-memory form keeps the whole width-2 plane in lichy
+    float *msd_dit = high_memory ? d_work_ + datasize / 4 + datasize / 2 : d_work_ + datasize / 2;
     float *msd_work = msd_dit + (nDec + 1) * 3;
     {
         // the largest partials area of the decimations
@@ -289,18 +290,27 @@ bool SpdPlane::msd_profile(const float *d_input, int nDMs, int nT, const std::ve
     if (!do_msd(msd_dit, d_input, nT, nDMs, 0, nullptr))
         return false;
     dit_widths.push_back(1);
-    // width 2, in two halves of the DM trials, merged by the continuous form
-    const int half = nDMs >> 1;
     long long dts = nT >> 1;
-    if (!dit(d_input, lichy, half, nT) || !do_msd(msd_dit + 3, lichy, dts, half, 0, msd_dit + 6) ||
-        !dit(lichy, sudy, half, dts))
-        return false;
-    if (!dit(d_input + static_cast<size_t>(half) * nT, lichy, half, nT) ||
-        !do_msd(msd_dit + 3, lichy, dts, half, 0, msd_dit + 6))
-        return false;
-    dit_widths.push_back(2);
-    if (!dit(lichy, sudy + static_cast<size_t>(half) * (dts >> 1), half, dts))
-        return false;
+    if (high_memory) {
+        // width 2 over all DM trials at once (:103-126)
+        if (!dit(d_input, lichy, nDMs, nT) || !do_msd(msd_dit + 3, lichy, dts, nDMs, 0, nullptr))
+            return false;
+        dit_widths.push_back(2);
+        if (!dit(lichy, sudy, nDMs, dts))
+            return false;
+    } else {
+        // width 2, in two halves of the DM trials, merged by the continuous form
+        const int half = nDMs >> 1;
+        if (!dit(d_input, lichy, half, nT) || !do_msd(msd_dit + 3, lichy, dts, half, 0, msd_dit + 6) ||
+            !dit(lichy, sudy, half, dts))
+            return false;
+        if (!dit(d_input + static_cast<size_t>(half) * nT, lichy, half, nT) ||
+            !do_msd(msd_dit + 3, lichy, dts, half, 0, msd_dit + 6))
+            return false;
+        dit_widths.push_back(2);
+        if (!dit(lichy, sudy + static_cast<size_t>(half) * (dts >> 1), half, dts))
+            return false;
+    }
     // width 4
     dts = nT >> 2;
     int dit_value = 4;
@@ -677,6 +687,47 @@ bool SpdPlane::filter_peaks(SpdCandidates &out, size_t b, float tsamp, cudaStrea
         return false;
     }
     return true;
+}
+
+} // namespace aab200
+
+namespace aab200 {
+
+// MSD_plane_profile on its own (src/aa_device_MSD_plane_profile.cu:564-604),
+// as the periodicity search calls it on power spectra (high_memory, widths
+// 1..nHarmonics): the interpolated (mean, deviation) per width in last_msd.
+bool SpdPlane::profile(const float *d_input, int nDMs, int nT, const std::vector<int> &widths, bool high_memory,
+                       float sigma_constant, bool outlier_rejection, cudaStream_t st, std::string &err)
+{
+    if (!d_work_) {
+        err = "single-pulse detection: not set up";
+        return false;
+    }
+    if (nDMs < 2 || nT < 128 || widths.empty() || widths.size() > 1024 ||
+        static_cast<long long>(nDMs) * nT > max_elems_) {
+        err = "MSD profile: needs 2 or more rows of 128 or more samples, 1..1024 widths, within the set-up size";
+        return false;
+    }
+    for (size_t k = 0; k < widths.size(); ++k)
+        if ((k == 0 && widths[0] < 1) || (k > 0 && widths[k] <= widths[k - 1])) {
+            err = "MSD profile: widths must ascend from 1 or more";
+            return false;
+        }
+    ev_family_.clear();
+    ev_used_ = 0;
+    SpdSettings s;
+    s.sigma_constant = sigma_constant;
+    s.enable_msd_baseline_noise = outlier_rejection ? 1 : 0;
+    if (!msd_profile(d_input, nDMs, nT, widths, s, st, err, high_memory))
+        return false;
+    last_widths = widths;
+    last_msd.assign(2 * widths.size(), 0.f);
+    if (cudaMemcpy(last_msd.data(), d_msd_interp_, last_msd.size() * sizeof(float), cudaMemcpyDeviceToHost) !=
+        cudaSuccess) {
+        err = "MSD profile: cudaMemcpy failed";
+        return false;
+    }
+    return !time_kernels || t_collect();
 }
 
 } // namespace aab200

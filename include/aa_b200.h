@@ -532,6 +532,16 @@ int aa_b200_spd_profile(const void *obj, float *msd, int msd_cap, int *widths, i
 int aa_b200_spd_keep_planes(void *obj, int on);
 long long aa_b200_spd_planes(const void *obj, float *snr, unsigned short *taps, long long cap);
 long long aa_b200_spd_kernel_launches(void);
+/* The MSD plane profile alone (MSD_plane_profile of
+ * src/aa_device_MSD_plane_profile.cu:564-604) on a device plane
+ * [nDMs][nTimesamples] (not modified) for ascending widths[nwidths]:
+ * h_msd[2 * nwidths] = (mean, deviation) per width.  high_memory != 0 takes
+ * the width-2 decimation in one piece, as the periodicity search does
+ * (src/aa_device_periods.cu:469, widths 1..nHarmonics); 0 splits it in two
+ * halves of the DM trials, as the analysis does.  Uses obj's work area. */
+int aa_b200_spd_msd_profile(void *obj, const float *d_input, int nDMs, int nTimesamples, const int *widths,
+                            int nwidths, int high_memory, float sigma_constant, int outlier_rejection, float *h_msd,
+                            void *stream);
 /* The first boxcar S/N plane alone (call_kernel_SPDT_GPU_1st_plane of
  * src/aa_device_SPS_long_kernel.cu, as tests/test_single_pulse_search_scan_1.cpp
  * drives it): device input [nDMs][nTimesamples], outputs boxcar values and

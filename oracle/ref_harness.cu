@@ -429,6 +429,38 @@ int aaref_time_pipeline_spd(const unsigned short *input_tc, int nchans, int nsam
     return 0;
 }
 
+/* The reference's MSD_plane_profile (src/aa_device_MSD_plane_profile.cu:564-604)
+ * alone on a host plane [nDMs][nT] for widths[nw], on a zeroed work area of
+ * nT*nDMs floats plus its statistics: msd[2*nw] = (mean, deviation) per
+ * width.  high_memory as the periodicity search passes it.  Returns 0 or < 0. */
+int aaref_msd_profile(const float *plane, int nT, int nDMs, const int *widths, int nw, int high_memory,
+                      float sigma, int outlier_rejection, float *msd)
+{
+    const size_t n = (size_t)nT * (size_t)nDMs;
+    std::vector<int> w(widths, widths + nw);
+    size_t msd_bytes = 0, dit_bytes = 0, work_bytes = 0;
+    Get_MSD_plane_profile_memory_requirements(&msd_bytes, &dit_bytes, &work_bytes, nT, nDMs, &w);
+    float *d_plane = NULL, *d_work = NULL, *d_msd = NULL;
+    const size_t work_total = n * sizeof(float) + work_bytes;
+    if (cudaMalloc((void **)&d_plane, n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_work, work_total) != cudaSuccess ||
+        cudaMalloc((void **)&d_msd, msd_bytes + 4096) != cudaSuccess)
+        return -3;
+    cudaMemcpy(d_plane, plane, n * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemset(d_work, 0, work_total);
+    double t0, t1, t2;
+    MSD_plane_profile(d_msd, d_plane, NULL, d_work, high_memory != 0, nT, nDMs, &w, 0, 0, 0, sigma,
+                      outlier_rejection, false, &t0, &t1, &t2);
+    int rc = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess)
+        rc = -5;
+    cudaMemcpy(msd, d_msd, 2 * (size_t)nw * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(d_plane);
+    cudaFree(d_work);
+    cudaFree(d_msd);
+    return rc;
+}
+
 /* Two stages of the reference's periodicity search on given host data:
  * simple_power_and_interbin (src/aa_device_power.cu:34-52) on nDMs spectra
  * of nT/2+1 complex bins (spectra: 2*nDMs*(nT/2+1) floats) into power

@@ -68,6 +68,18 @@ def main():
                                  "harmonics_sha256": hashlib.sha256(hm.tobytes()).hexdigest(),
                                  "snr_head": snr[:512].view(np.uint32).tolist(), "harmonics_head": hm[:512].tolist()}
         print(name, rc, flush=True)
+    L.aaref_msd_profile.argtypes = [Pf, i, i, ctypes.POINTER(ctypes.c_int), i, i, ctypes.c_float, i, Pf]
+    L.aaref_msd_profile.restype = i
+    out["msd"] = {}
+    for name, c in P.MSD_CASES.items():
+        x = np.ascontiguousarray(P.make_power_plane(c))
+        w = np.arange(1, c["nh"] + 1, dtype=np.int32)
+        msd = np.zeros(2 * c["nh"], np.float32)
+        rc = L.aaref_msd_profile(x.ctypes.data_as(Pf), c["nt"], c["ndms"],
+                                 w.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), c["nh"], c["high_memory"],
+                                 c["sigma"], c["outliers"], msd.ctypes.data_as(Pf))
+        out["msd"][name] = {"rc": rc, "msd_bits": msd.view(np.uint32).tolist()}
+        print(name, rc, flush=True)
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     with open(args.out, "w") as f:
         json.dump(out, f, indent=1)

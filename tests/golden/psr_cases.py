@@ -45,3 +45,25 @@ def make_harmonic_input(c):
     msd[0::2] = f + 1
     msd[1::2] = np.sqrt(f + 1)
     return x, msd
+
+
+# MSD plane profiles of power-spectrum planes, as the periodicity search runs
+# them (high_memory, widths 1..nHarmonics), and in the analysis' form
+MSD_CASES = {
+    "msd_power_h32_or": dict(nt=16384, ndms=32, seed=7, nh=32, high_memory=1, sigma=3.0, outliers=1),
+    "msd_power_h16": dict(nt=8192, ndms=48, seed=8, nh=16, high_memory=1, sigma=3.0, outliers=0),
+    "msd_power_h8_low": dict(nt=8192, ndms=20, seed=9, nh=8, high_memory=0, sigma=2.5, outliers=1),
+    "msd_power_h32_odd": dict(nt=10000, ndms=13, seed=10, nh=32, high_memory=1, sigma=3.0, outliers=1),
+}
+
+
+def make_power_plane(c) -> np.ndarray:
+    """[ndms][nt] float32 power-like values (exponential) with a few lines."""
+    rng = np.random.Generator(np.random.PCG64(c["seed"]))
+    x = rng.exponential(1.0, (c["ndms"], c["nt"])).astype(np.float32)
+    for d in range(c["ndms"]):
+        k = int(rng.integers(10, c["nt"] // 16))
+        for h in range(1, 8):
+            if h * k < c["nt"]:
+                x[d, h * k] += np.float32(20.0 / h)
+    return x

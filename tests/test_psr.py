@@ -85,3 +85,21 @@ def test_harmonic_sum_matches_reference_gpu(aa, golden, name):
     torch.cuda.synchronize()
     assert hashlib.sha256(snr.cpu().numpy().tobytes()).hexdigest() == g["snr_sha256"]
     assert hashlib.sha256(hm.cpu().numpy().view(np.uint16).tobytes()).hexdigest() == g["harmonics_sha256"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(P.MSD_CASES))
+def test_msd_profile_matches_reference_gpu(aa, golden, name):
+    """The MSD plane profile alone, high-memory form as the periodicity search
+    runs it on power spectra (widths 1..nHarmonics), bit for bit."""
+    import torch
+    c = P.MSD_CASES[name]
+    g = golden["msd"][name]
+    assert g["rc"] == 0
+    x = torch.from_numpy(P.make_power_plane(c)).cuda()
+    spd = aa.single_pulse_detection(x.numel(), 0)
+    spd.clear()
+    got = spd.msd_profile(x, c["ndms"], c["nt"], np.arange(1, c["nh"] + 1), bool(c["high_memory"]), c["sigma"],
+                          bool(c["outliers"]))
+    spd.delete()
+    assert got.view(np.uint32).tolist() == g["msd_bits"]
