@@ -17,7 +17,7 @@ width log-U[0.25, 8] ms, 3-10 sigma).
          region (wall clock between device synchronisations).
 
 `--impl reference` times the reference path's CPU restatement (the oracle;
-the reference ships no CPU DDTR) on the box's host cores on a bounded sample
+the reference ships no CPU DDTR) on the host's cores on a bounded sample
 of the same workload.  Under torchrun every rank runs its own beam (weak
 scaling, no collective on the data path); rank 0 prints one JSON line.
 """

@@ -11,7 +11,7 @@ CPU oracle (oracle/aa_oracle.c) compares under each FMA-contraction variant.
 Needs a GPU.  Each case runs in a child process because the reference's
 aa_device_info destructor resets the device.
 
-    python tests/golden/make_ddtr_golden.py --out gpurun_out/golden/ddtr_golden.json
+    python tests/golden/make_ddtr_golden.py --out <dir>/ddtr_golden.json
 """
 from __future__ import annotations
 
@@ -120,7 +120,7 @@ def run_one(name, case, q):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden", "ddtr_golden.json"))
+    ap.add_argument("--out", default=os.path.join(HERE, "ddtr_golden.json"))
     ap.add_argument("--only", default="")
     ap.add_argument("--merge", default="", help="existing golden file whose other cases are kept")
     args = ap.parse_args()

@@ -7,7 +7,7 @@ output and a sample of values.
 Needs a GPU.  Each run is a child process (the reference's aa_device_info
 destructor resets the device).
 
-    python tests/golden/make_preproc_golden.py --out gpurun_out/golden/preproc_golden.json
+    python tests/golden/make_preproc_golden.py --out <dir>/preproc_golden.json
 """
 from __future__ import annotations
 
@@ -52,7 +52,7 @@ def run_one(name, q):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden", "preproc_golden.json"))
+    ap.add_argument("--out", default=os.path.join(HERE, "preproc_golden.json"))
     args = ap.parse_args()
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     ctx = mp.get_context("spawn")

@@ -4,7 +4,7 @@ simple_power_and_interbin and periodicity_simple_harmonic_summing) on the
 seeded inputs of psr_cases.py: SHA-256 of every output and its first
 values.  Needs a GPU.
 
-    python tests/golden/make_psr_golden.py --out gpurun_out/golden/psr_golden.json
+    python tests/golden/make_psr_golden.py --out <dir>/psr_golden.json
 """
 from __future__ import annotations
 
@@ -27,7 +27,7 @@ import refharness as R  # noqa: E402
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden", "psr_golden.json"))
+    ap.add_argument("--out", default=os.path.join(HERE, "psr_golden.json"))
     args = ap.parse_args()
     L = R.load()
     Pf, i = ctypes.POINTER(ctypes.c_float), ctypes.c_int

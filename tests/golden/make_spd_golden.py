@@ -7,7 +7,7 @@ component on DDTR cases of cases.py (oracle/ref_harness.cu
 aaref_run_pipeline_spd: per-step candidates and the candidate files it
 writes).  Needs a GPU; each run is a child process.
 
-    python tests/golden/make_spd_golden.py --out gpurun_out/golden/spd_golden.json
+    python tests/golden/make_spd_golden.py --out <dir>/spd_golden.json
 """
 from __future__ import annotations
 
@@ -150,7 +150,7 @@ def run_pipeline(name, q):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden", "spd_golden.json"))
+    ap.add_argument("--out", default=os.path.join(HERE, "spd_golden.json"))
     args = ap.parse_args()
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     ctx = mp.get_context("spawn")
