@@ -70,9 +70,78 @@ __global__ void __launch_bounds__(PSR_PHS_THREADS) k_harmonic_sum_simple(const f
     harm_out[b * nSpectra + s] = best;
 }
 
+// Peak finding for the periodicity search
+// (src/aa_device_peak_find_kernel.cu:340-389 with the neighbourhood rule of
+// include/aa_device_peak_find_shared_kernel_functions.cuh:217-287): a value
+// above the cut that equals the maximum of its 3 x 3 neighbourhood clipped
+// to the plane (width >= 2, height >= 2).  Records of 4 floats: DM trial,
+// frequency bin / DIT, S/N turned back into power with the harmonic's
+// (mean, deviation) as mean + S/N * deviation, harmonic count.
+__device__ __forceinline__ float psr_window_max(const float *in, int x, int y, int width, int height)
+{
+    const int x0 = x > 0 ? x - 1 : x, x1 = x < width - 1 ? x + 1 : x;
+    const int y0 = y > 0 ? y - 1 : y, y1 = y < height - 1 ? y + 1 : y;
+    float m = __ldg(in + static_cast<long long>(y0) * width + x0);
+    for (int yy = y0; yy <= y1; ++yy)
+        for (int xx = x0; xx <= x1; ++xx)
+            m = fmaxf(m, __ldg(in + static_cast<long long>(yy) * width + xx));
+    return m;
+}
+
+__global__ void k_psr_peaks(const float *__restrict__ in, const uint16_t *__restrict__ harm, float *list, int width,
+                            int height, float threshold, int max_peaks, int *count, const float *__restrict__ msd,
+                            int dm_shift, int dit, int transposed, int greedy)
+{
+    const int idxX = blockDim.x * blockIdx.x + threadIdx.x;
+    const int idxY = blockDim.y * blockIdx.y + threadIdx.y;
+    if (idxX >= width || idxY >= height)
+        return;
+    const long long pos = static_cast<long long>(idxY) * width + idxX;
+    const float my_value = __ldg(in + pos);
+    if (!(my_value > threshold && my_value == psr_window_max(in, idxX, idxY, width, height)))
+        return;
+    const int list_pos = atomicAdd(count, 1);
+    if (list_pos >= max_peaks)
+        return;
+    const int raw = static_cast<int>(harm[pos]);
+    int hrms = raw;
+    if (transposed) {
+        list[4 * list_pos] = idxX + dm_shift;
+        list[4 * list_pos + 1] = idxY / dit;
+        list[4 * list_pos + 3] = hrms;
+    } else {
+        list[4 * list_pos] = idxY + dm_shift;
+        list[4 * list_pos + 1] = idxX / dit;
+        if (greedy) {
+            const int temp = hrms / 100;
+            hrms = hrms - 100 * temp;
+        }
+        list[4 * list_pos + 3] = static_cast<float>(raw);
+    }
+    list[4 * list_pos + 2] = my_value * __ldg(&msd[2 * hrms + 1]) + __ldg(&msd[2 * hrms]);
+}
+
 } // namespace
 
 long long psr_kernel_launches() { return g_psr_launches.load(); }
+
+// src/aa_device_peak_find.cu:53-131: transposed planes are [nTimesamples
+// bins][nDMs] (DM trials inner), normal ones [nDMs][nTimesamples]
+cudaError_t psr_peak_find(const float *d_snr, const uint16_t *d_harmonics, float *d_list, int nTimesamples, int nDMs,
+                          float threshold, int max_peaks, int *d_count, const float *d_msd, int dm_shift, int in_bin,
+                          bool transposed, bool greedy, cudaStream_t st)
+{
+    const int width = transposed ? nDMs : nTimesamples;
+    const int height = transposed ? nTimesamples : nDMs;
+    if (width < 2 || height < 2 || in_bin < 1)
+        return cudaErrorInvalidValue;
+    const dim3 block(32, 32);
+    const dim3 grid((width + 31) / 32, (height + 31) / 32);
+    k_psr_peaks<<<grid, block, 0, st>>>(d_snr, d_harmonics, d_list, width, height, threshold, max_peaks, d_count,
+                                        d_msd, dm_shift, in_bin, transposed ? 1 : 0, greedy ? 1 : 0);
+    ++g_psr_launches;
+    return cudaGetLastError();
+}
 
 // src/aa_device_power.cu:34-52: norm = sqrt(nTimesamples) as float
 cudaError_t psr_power_interbin(const float2 *d_in, float *d_power, float *d_interbin, int nTimesamples, int nDMs,

@@ -26,6 +26,14 @@ cudaError_t psr_power_interbin(const float2 *d_in, float *d_power, float *d_inte
 cudaError_t psr_harmonic_sum_simple(const float *d_in, float *d_snr, uint16_t *d_harmonics, const float *d_msd,
                                     int nBins, int nSpectra, int nHarmonics, cudaStream_t st);
 
+// Peaks of a harmonic-sum S/N plane (candidate records of 4 floats appended
+// at *d_count): transposed planes [nTimesamples][nDMs], normal ones
+// [nDMs][nTimesamples]; greedy: harmonic counts carry a multiple of 100 that
+// the S/N conversion drops (normal planes only).
+cudaError_t psr_peak_find(const float *d_snr, const uint16_t *d_harmonics, float *d_list, int nTimesamples, int nDMs,
+                          float threshold, int max_peaks, int *d_count, const float *d_msd, int dm_shift, int in_bin,
+                          bool transposed, bool greedy, cudaStream_t st);
+
 long long psr_kernel_launches();
 
 } // namespace aab200

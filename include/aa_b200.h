@@ -592,6 +592,17 @@ int aa_b200_psr_power_interbin(const void *d_spectra, float *d_power, float *d_i
                                void *stream);
 int aa_b200_psr_harmonic_sum_simple(const float *d_input, float *d_snr, unsigned short *d_harmonics,
                                     const float *d_msd, int nBins, int nSpectra, int nHarmonics, void *stream);
+/* Peak finding for the periodicity search (Peak_find_for_periodicity_search,
+ * src/aa_device_peak_find.cu:53-131): values above threshold that are the
+ * maximum of their clipped 3 x 3 neighbourhood, on a transposed
+ * [nTimesamples][nDMs] or normal [nDMs][nTimesamples] S/N plane with its
+ * harmonic counts; records (DM trial + dm_shift, bin / in_bin, power =
+ * S/N * sd_h + mean_h, harmonic count) appended at *d_count (at most
+ * max_peaks); greedy (normal planes) drops the hundreds of the harmonic count
+ * for the power.  Planes of at least 2 x 2. */
+int aa_b200_psr_peak_find(const float *d_snr, const unsigned short *d_harmonics, float *d_list, int nTimesamples,
+                          int nDMs, float threshold, int max_peaks, int *d_count, const float *d_msd, int dm_shift,
+                          int in_bin, int transposed, int greedy, void *stream);
 long long aa_b200_psr_kernel_launches(void);
 const char *aa_b200_psr_last_error(void);
 

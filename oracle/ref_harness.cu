@@ -52,6 +52,7 @@
 #include "aa_device_SPS_long.hpp"
 #include "aa_device_power.hpp"
 #include "aa_device_harmonic_summing.hpp"
+#include "aa_device_peak_find.hpp"
 
 namespace astroaccelerate {
 /* defined in src/aa_device_analysis.cu without a header declaration */
@@ -458,6 +459,43 @@ int aaref_msd_profile(const float *plane, int nT, int nDMs, const int *widths, i
     cudaFree(d_plane);
     cudaFree(d_work);
     cudaFree(d_msd);
+    return rc;
+}
+
+/* The reference's Peak_find_for_periodicity_search
+ * (src/aa_device_peak_find.cu:53-131) on a host S/N plane with its harmonic
+ * counts (transposed: [nT][nDMs], else [nDMs][nT]) and msd[2*nH]: records of
+ * 4 floats into list (max_peaks), their number in *count.  Returns 0 or < 0. */
+int aaref_psr_peaks(const float *snr, const unsigned short *harm, int nT, int nDMs, float threshold,
+                    const float *msd, int nH, int dm_shift, int in_bin, int transposed, int greedy, float *list,
+                    int max_peaks, int *count)
+{
+    const size_t n = (size_t)nT * (size_t)nDMs;
+    float *d_snr = NULL, *d_list = NULL, *d_msd = NULL;
+    unsigned short *d_harm = NULL;
+    int *d_pos = NULL;
+    if (cudaMalloc((void **)&d_snr, n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_harm, n * sizeof(unsigned short)) != cudaSuccess ||
+        cudaMalloc((void **)&d_list, 4 * (size_t)max_peaks * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_msd, 2 * (size_t)nH * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_pos, sizeof(int)) != cudaSuccess)
+        return -3;
+    cudaMemcpy(d_snr, snr, n * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_harm, harm, n * sizeof(unsigned short), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_msd, msd, 2 * (size_t)nH * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemset(d_pos, 0, sizeof(int));
+    int rc = Peak_find_for_periodicity_search(d_snr, d_harm, d_list, nT, nDMs, threshold, max_peaks, d_pos, d_msd,
+                                              dm_shift, in_bin, transposed != 0, greedy);
+    if (cudaDeviceSynchronize() != cudaSuccess)
+        rc = -5;
+    cudaMemcpy(count, d_pos, sizeof(int), cudaMemcpyDeviceToHost);
+    const int k = *count < max_peaks ? *count : max_peaks;
+    cudaMemcpy(list, d_list, 4 * (size_t)k * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(d_snr);
+    cudaFree(d_harm);
+    cudaFree(d_list);
+    cudaFree(d_msd);
+    cudaFree(d_pos);
     return rc;
 }
 

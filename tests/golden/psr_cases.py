@@ -67,3 +67,29 @@ def make_power_plane(c) -> np.ndarray:
             if h * k < c["nt"]:
                 x[d, h * k] += np.float32(20.0 / h)
     return x
+
+
+# Peak finding on harmonic-sum S/N planes (with their harmonic counts)
+PEAK_CASES = {
+    "peaks_transposed": dict(nt=4096, ndms=48, seed=11, nh=16, threshold=3.0, dm_shift=100, inbin=1, transposed=1,
+                             greedy=0),
+    "peaks_normal": dict(nt=3000, ndms=33, seed=12, nh=16, threshold=3.0, dm_shift=0, inbin=1, transposed=0,
+                         greedy=0),
+    "peaks_normal_greedy": dict(nt=2048, ndms=20, seed=13, nh=8, threshold=2.5, dm_shift=7, inbin=1, transposed=0,
+                                greedy=1),
+}
+
+
+def make_peak_plane(c):
+    """(S/N plane, harmonic counts, msd[2*nh]) in the case's layout."""
+    rng = np.random.Generator(np.random.PCG64(c["seed"]))
+    shape = (c["nt"], c["ndms"]) if c["transposed"] else (c["ndms"], c["nt"])
+    snr = rng.normal(0, 1, shape).astype(np.float32)
+    harm = rng.integers(0, c["nh"], shape).astype(np.uint16)
+    if c["greedy"]:
+        harm = (harm + 100 * rng.integers(0, 3, shape)).astype(np.uint16)
+    f = np.arange(c["nh"], dtype=np.float32)
+    msd = np.empty(2 * c["nh"], np.float32)
+    msd[0::2] = 2.0 * (f + 1)
+    msd[1::2] = np.sqrt(f + 1) * np.float32(1.5)
+    return snr, harm, msd

@@ -103,3 +103,30 @@ def test_msd_profile_matches_reference_gpu(aa, golden, name):
                           bool(c["outliers"]))
     spd.delete()
     assert got.view(np.uint32).tolist() == g["msd_bits"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(P.PEAK_CASES))
+def test_periodicity_peaks_match_reference_gpu(aa, golden, name):
+    """Peak finding for the periodicity search (transposed and normal planes,
+    greedy harmonic counts): the same set of 4-float records, bit for bit."""
+    import torch
+    c = P.PEAK_CASES[name]
+    g = golden["peaks"][name]
+    assert g["rc"] == 0
+    snr, harm, msd = P.make_peak_plane(c)
+    d_snr = torch.from_numpy(np.ascontiguousarray(snr)).cuda()
+    d_harm = torch.from_numpy(np.ascontiguousarray(harm).view(np.int16)).cuda()
+    d_msd = torch.from_numpy(msd).cuda()
+    max_peaks = 1 << 20
+    d_list = torch.zeros(4 * max_peaks, device="cuda")
+    d_cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert aa.lib().aa_b200_psr_peak_find(d_snr.data_ptr(), d_harm.data_ptr(), d_list.data_ptr(), c["nt"], c["ndms"],
+                                          c["threshold"], max_peaks, d_cnt.data_ptr(), d_msd.data_ptr(),
+                                          c["dm_shift"], c["inbin"], c["transposed"], c["greedy"], None) == 0
+    torch.cuda.synchronize()
+    k = int(d_cnt.item())
+    assert k == g["count"]
+    recs = sorted(tuple(int(v) for v in r) for r in d_list[:4 * k].cpu().numpy().view(np.uint32).reshape(-1, 4))
+    assert [list(r) for r in recs[:32]] == g["records_head"]
+    assert hashlib.sha256(json.dumps(recs).encode()).hexdigest() == g["records_sha256"]
