@@ -50,6 +50,16 @@ int aa_b200_psr_peak_find(const float *d_snr, const unsigned short *d_harmonics,
                       "periodicity peak finding");
 }
 
+int aa_b200_psr_threshold(const float *d_snr, const unsigned short *d_harmonics, float *d_list, int nTimesamples,
+                          int nDMs, float threshold, int max_peaks, int *d_count, const float *d_msd, int dm_shift,
+                          int in_bin, int transposed, int greedy, void *stream)
+{
+    return psr_status(psr_threshold(d_snr, d_harmonics, d_list, nTimesamples, nDMs, threshold, max_peaks, d_count,
+                                    d_msd, dm_shift, in_bin, transposed != 0, greedy != 0,
+                                    static_cast<cudaStream_t>(stream)),
+                      "periodicity thresholding");
+}
+
 long long aa_b200_psr_kernel_launches(void) { return psr_kernel_launches(); }
 
 const char *aa_b200_psr_last_error(void) { return g_psr_error.c_str(); }

@@ -121,9 +121,61 @@ __global__ void k_psr_peaks(const float *__restrict__ in, const uint16_t *__rest
     list[4 * list_pos + 2] = my_value * __ldg(&msd[2 * hrms + 1]) + __ldg(&msd[2 * hrms]);
 }
 
+// Thresholding for the periodicity search
+// (src/aa_device_threshold_kernel.cu:43-112): every value above the cut,
+// recorded as the peak finder records it.
+__global__ void k_psr_threshold(const float *__restrict__ in, const uint16_t *__restrict__ harm, float *list,
+                                int width, int height, float threshold, int max_peaks, int *count,
+                                const float *__restrict__ msd, int dm_shift, int dit, int transposed, int greedy)
+{
+    const int x = blockDim.x * blockIdx.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= width || y >= height)
+        return;
+    const long long pos = static_cast<long long>(y) * width + x;
+    const float R = __ldg(in + pos);
+    if (!(R > threshold))
+        return;
+    const int list_pos = atomicAdd(count, 1);
+    if (list_pos >= max_peaks)
+        return;
+    const int raw = static_cast<int>(harm[pos]);
+    int hrms = raw;
+    if (transposed) {
+        list[4 * list_pos] = x + dm_shift;
+        list[4 * list_pos + 1] = y / dit;
+        list[4 * list_pos + 3] = hrms;
+    } else {
+        list[4 * list_pos] = y + dm_shift;
+        list[4 * list_pos + 1] = x / dit;
+        if (greedy) {
+            const int temp = hrms / 100;
+            hrms = hrms - 100 * temp;
+        }
+        list[4 * list_pos + 3] = static_cast<float>(raw);
+    }
+    list[4 * list_pos + 2] = R * __ldg(&msd[2 * hrms + 1]) + __ldg(&msd[2 * hrms]);
+}
+
 } // namespace
 
 long long psr_kernel_launches() { return g_psr_launches.load(); }
+
+// src/aa_device_threshold.cu:56-163 (transposed and normal planes)
+cudaError_t psr_threshold(const float *d_snr, const uint16_t *d_harmonics, float *d_list, int nTimesamples, int nDMs,
+                          float threshold, int max_peaks, int *d_count, const float *d_msd, int dm_shift, int in_bin,
+                          bool transposed, bool greedy, cudaStream_t st)
+{
+    const int width = transposed ? nDMs : nTimesamples;
+    const int height = transposed ? nTimesamples : nDMs;
+    if (width < 1 || height < 1 || in_bin < 1)
+        return cudaErrorInvalidValue;
+    const dim3 grid((width + 255) / 256, height);
+    k_psr_threshold<<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_list, width, height, threshold, max_peaks, d_count,
+                                          d_msd, dm_shift, in_bin, transposed ? 1 : 0, greedy ? 1 : 0);
+    ++g_psr_launches;
+    return cudaGetLastError();
+}
 
 // src/aa_device_peak_find.cu:53-131: transposed planes are [nTimesamples
 // bins][nDMs] (DM trials inner), normal ones [nDMs][nTimesamples]

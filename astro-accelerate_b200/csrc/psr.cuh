@@ -34,6 +34,11 @@ cudaError_t psr_peak_find(const float *d_snr, const uint16_t *d_harmonics, float
                           float threshold, int max_peaks, int *d_count, const float *d_msd, int dm_shift, int in_bin,
                           bool transposed, bool greedy, cudaStream_t st);
 
+// Every value of the plane above the cut, recorded as psr_peak_find does
+cudaError_t psr_threshold(const float *d_snr, const uint16_t *d_harmonics, float *d_list, int nTimesamples, int nDMs,
+                          float threshold, int max_peaks, int *d_count, const float *d_msd, int dm_shift, int in_bin,
+                          bool transposed, bool greedy, cudaStream_t st);
+
 long long psr_kernel_launches();
 
 } // namespace aab200

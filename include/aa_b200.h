@@ -603,6 +603,12 @@ int aa_b200_psr_harmonic_sum_simple(const float *d_input, float *d_snr, unsigned
 int aa_b200_psr_peak_find(const float *d_snr, const unsigned short *d_harmonics, float *d_list, int nTimesamples,
                           int nDMs, float threshold, int max_peaks, int *d_count, const float *d_msd, int dm_shift,
                           int in_bin, int transposed, int greedy, void *stream);
+/* Thresholding for the periodicity search (Threshold_for_periodicity_transposed
+ * and _normal, src/aa_device_threshold.cu:56-163): every value above
+ * threshold, recorded as aa_b200_psr_peak_find records peaks. */
+int aa_b200_psr_threshold(const float *d_snr, const unsigned short *d_harmonics, float *d_list, int nTimesamples,
+                          int nDMs, float threshold, int max_peaks, int *d_count, const float *d_msd, int dm_shift,
+                          int in_bin, int transposed, int greedy, void *stream);
 long long aa_b200_psr_kernel_launches(void);
 const char *aa_b200_psr_last_error(void);
 

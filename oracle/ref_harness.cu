@@ -53,6 +53,7 @@
 #include "aa_device_power.hpp"
 #include "aa_device_harmonic_summing.hpp"
 #include "aa_device_peak_find.hpp"
+#include "aa_device_threshold.hpp"
 
 namespace astroaccelerate {
 /* defined in src/aa_device_analysis.cu without a header declaration */
@@ -465,10 +466,12 @@ int aaref_msd_profile(const float *plane, int nT, int nDMs, const int *widths, i
 /* The reference's Peak_find_for_periodicity_search
  * (src/aa_device_peak_find.cu:53-131) on a host S/N plane with its harmonic
  * counts (transposed: [nT][nDMs], else [nDMs][nT]) and msd[2*nH]: records of
- * 4 floats into list (max_peaks), their number in *count.  Returns 0 or < 0. */
+ * 4 floats into list (max_peaks), their number in *count.  mode 1 runs the
+ * periodicity thresholding (src/aa_device_threshold.cu:56-163) instead.
+ * Returns 0 or < 0. */
 int aaref_psr_peaks(const float *snr, const unsigned short *harm, int nT, int nDMs, float threshold,
                     const float *msd, int nH, int dm_shift, int in_bin, int transposed, int greedy, float *list,
-                    int max_peaks, int *count)
+                    int max_peaks, int *count, int mode)
 {
     const size_t n = (size_t)nT * (size_t)nDMs;
     float *d_snr = NULL, *d_list = NULL, *d_msd = NULL;
@@ -484,8 +487,18 @@ int aaref_psr_peaks(const float *snr, const unsigned short *harm, int nT, int nD
     cudaMemcpy(d_harm, harm, n * sizeof(unsigned short), cudaMemcpyHostToDevice);
     cudaMemcpy(d_msd, msd, 2 * (size_t)nH * sizeof(float), cudaMemcpyHostToDevice);
     cudaMemset(d_pos, 0, sizeof(int));
-    int rc = Peak_find_for_periodicity_search(d_snr, d_harm, d_list, nT, nDMs, threshold, max_peaks, d_pos, d_msd,
+    int rc;
+    if (mode == 1) {
+        if (transposed)
+            rc = Threshold_for_periodicity_transposed(d_snr, d_harm, d_list, d_pos, d_msd, threshold, nDMs, nT,
+                                                      dm_shift, in_bin, max_peaks);
+        else
+            rc = Threshold_for_periodicity_normal(d_snr, d_harm, d_list, d_pos, d_msd, threshold, nT, nDMs, dm_shift,
+                                                  in_bin, max_peaks, greedy);
+    } else {
+        rc = Peak_find_for_periodicity_search(d_snr, d_harm, d_list, nT, nDMs, threshold, max_peaks, d_pos, d_msd,
                                               dm_shift, in_bin, transposed != 0, greedy);
+    }
     if (cudaDeviceSynchronize() != cudaSuccess)
         rc = -5;
     cudaMemcpy(count, d_pos, sizeof(int), cudaMemcpyDeviceToHost);

@@ -81,10 +81,11 @@ def main():
         out["msd"][name] = {"rc": rc, "msd_bits": msd.view(np.uint32).tolist()}
         print(name, rc, flush=True)
     L.aaref_psr_peaks.argtypes = [Pf, ctypes.POINTER(ctypes.c_ushort), i, i, ctypes.c_float, Pf, i, i, i, i, i, Pf,
-                                  i, ctypes.POINTER(ctypes.c_int)]
+                                  i, ctypes.POINTER(ctypes.c_int), i]
     L.aaref_psr_peaks.restype = i
     out["peaks"] = {}
-    for name, c in P.PEAK_CASES.items():
+    out["threshold"] = {}
+    for (name, c), mode in [(kv, 0) for kv in P.PEAK_CASES.items()] + [(kv, 1) for kv in P.PEAK_CASES.items()]:
         snr, harm, msd = P.make_peak_plane(c)
         max_peaks = 1 << 20
         lst = np.zeros(4 * max_peaks, np.float32)
@@ -92,13 +93,14 @@ def main():
         rc = L.aaref_psr_peaks(np.ascontiguousarray(snr).ctypes.data_as(Pf),
                                np.ascontiguousarray(harm).ctypes.data_as(ctypes.POINTER(ctypes.c_ushort)), c["nt"],
                                c["ndms"], c["threshold"], msd.ctypes.data_as(Pf), c["nh"], c["dm_shift"], c["inbin"],
-                               c["transposed"], c["greedy"], lst.ctypes.data_as(Pf), max_peaks, ctypes.byref(cnt))
+                               c["transposed"], c["greedy"], lst.ctypes.data_as(Pf), max_peaks, ctypes.byref(cnt),
+                               mode)
         k = cnt.value
         recs = sorted(tuple(int(v) for v in r) for r in lst[:4 * k].view(np.uint32).reshape(-1, 4))
-        out["peaks"][name] = {"rc": rc, "count": k,
-                              "records_sha256": hashlib.sha256(json.dumps(recs).encode()).hexdigest(),
-                              "records_head": recs[:32]}
-        print(name, rc, k, flush=True)
+        out["threshold" if mode else "peaks"][name] = {
+            "rc": rc, "count": k, "records_sha256": hashlib.sha256(json.dumps(recs).encode()).hexdigest(),
+            "records_head": recs[:32]}
+        print(name, "threshold" if mode else "peaks", rc, k, flush=True)
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     with open(args.out, "w") as f:
         json.dump(out, f, indent=1)

@@ -107,12 +107,14 @@ def test_msd_profile_matches_reference_gpu(aa, golden, name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(P.PEAK_CASES))
-def test_periodicity_peaks_match_reference_gpu(aa, golden, name):
-    """Peak finding for the periodicity search (transposed and normal planes,
-    greedy harmonic counts): the same set of 4-float records, bit for bit."""
+@pytest.mark.parametrize("mode", ["peaks", "threshold"])
+def test_periodicity_peaks_match_reference_gpu(aa, golden, name, mode):
+    """Peak finding and thresholding for the periodicity search (transposed
+    and normal planes, greedy harmonic counts): the same set of 4-float
+    records, bit for bit."""
     import torch
     c = P.PEAK_CASES[name]
-    g = golden["peaks"][name]
+    g = golden[mode][name]
     assert g["rc"] == 0
     snr, harm, msd = P.make_peak_plane(c)
     d_snr = torch.from_numpy(np.ascontiguousarray(snr)).cuda()
@@ -121,9 +123,9 @@ def test_periodicity_peaks_match_reference_gpu(aa, golden, name):
     max_peaks = 1 << 20
     d_list = torch.zeros(4 * max_peaks, device="cuda")
     d_cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
-    assert aa.lib().aa_b200_psr_peak_find(d_snr.data_ptr(), d_harm.data_ptr(), d_list.data_ptr(), c["nt"], c["ndms"],
-                                          c["threshold"], max_peaks, d_cnt.data_ptr(), d_msd.data_ptr(),
-                                          c["dm_shift"], c["inbin"], c["transposed"], c["greedy"], None) == 0
+    fn = aa.lib().aa_b200_psr_peak_find if mode == "peaks" else aa.lib().aa_b200_psr_threshold
+    assert fn(d_snr.data_ptr(), d_harm.data_ptr(), d_list.data_ptr(), c["nt"], c["ndms"], c["threshold"], max_peaks,
+              d_cnt.data_ptr(), d_msd.data_ptr(), c["dm_shift"], c["inbin"], c["transposed"], c["greedy"], None) == 0
     torch.cuda.synchronize()
     k = int(d_cnt.item())
     assert k == g["count"]
