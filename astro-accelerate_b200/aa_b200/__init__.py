@@ -220,6 +220,7 @@ def lib():
         "aa_b200_psr_kernel_launches": ([], ll),
         "aa_b200_psr_peak_find": ([vp, vp, vp, i, i, f, i, vp, vp, i, i, i, i, vp], i),
         "aa_b200_psr_threshold": ([vp, vp, vp, i, i, f, i, vp, vp, i, i, i, i, vp], i),
+        "aa_b200_psr_harmonic_sum": ([i, vp, vp, vp, vp, i, i, i, i, vp], i),
         "aa_b200_psr_last_error": ([], ctypes.c_char_p),
         "aa_b200_spd_create": ([ll, ll], vp),
         "aa_b200_spd_destroy": ([vp], None),

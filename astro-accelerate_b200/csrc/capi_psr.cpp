@@ -60,6 +60,15 @@ int aa_b200_psr_threshold(const float *d_snr, const unsigned short *d_harmonics,
                       "periodicity thresholding");
 }
 
+int aa_b200_psr_harmonic_sum(int algorithm, const float *d_input, float *d_snr, unsigned short *d_harmonics,
+                             const float *d_msd, int nTimesamples, int nDMs, int nHarmonics, int scalloping,
+                             void *stream)
+{
+    return psr_status(psr_harmonic_sum(algorithm, d_input, d_snr, d_harmonics, d_msd, nTimesamples, nDMs, nHarmonics,
+                                       scalloping != 0, static_cast<cudaStream_t>(stream)),
+                      "harmonic sum");
+}
+
 long long aa_b200_psr_kernel_launches(void) { return psr_kernel_launches(); }
 
 const char *aa_b200_psr_last_error(void) { return g_psr_error.c_str(); }

@@ -157,9 +157,191 @@ __global__ void k_psr_threshold(const float *__restrict__ in, const uint16_t *__
     list[4 * list_pos + 2] = R * __ldg(&msd[2 * hrms + 1]) + __ldg(&msd[2 * hrms]);
 }
 
+// Harmonic sums over normal planes [nDMs][nTimesamples]
+// (src/aa_device_harmonic_summing_kernel.cu:41-268).  Each output bin is
+// independent; the expressions (float sums, the double constants and bin
+// positions of the scalloping-loss and PRESTO forms, the fast division) are
+// the reference's.
+__device__ __forceinline__ float psr_remove_scalloping_loss(float Xm2, float Xm1, float X0, float Xp1, float Xp2)
+{
+    return (X0 + (1.88494 / 2.0) * (Xm1 + Xp1) + (0.88494 / 2.0) * (Xm2 + Xp2));
+}
+
+template <bool SCAL>
+__device__ __forceinline__ void psr_bins(float *down, float *step, const float *__restrict__ d, long long pos)
+{
+    if (SCAL) {
+        const float Xm2 = d[pos - 2], Xm1 = d[pos - 1], X0 = d[pos + 0], Xp1 = d[pos + 1], Xp2 = d[pos + 2],
+                    Xp3 = d[pos + 3];
+        *down = psr_remove_scalloping_loss(Xm2, Xm1, X0, Xp1, Xp2);
+        *step = psr_remove_scalloping_loss(Xm1, X0, Xp1, Xp2, Xp3);
+    } else {
+        *down = d[pos];
+        *step = d[pos + 1];
+    }
+}
+
+template <bool SCAL>
+__device__ __forceinline__ void psr_bin_value(float *bin, const float *__restrict__ d, long long pos)
+{
+    if (SCAL) {
+        const float Xm2 = d[pos - 2], Xm1 = d[pos - 1], X0 = d[pos], Xp1 = d[pos + 1], Xp2 = d[pos + 2];
+        *bin = X0 + (1.88494 / 2.0) * (Xm1 + Xp1) + (0.88494 / 2.0) * (Xm2 + Xp2);
+    } else {
+        *bin = d[pos];
+    }
+}
+
+// greedy: at every harmonic the larger of two neighbouring bins, the chosen
+// offsets carried to the next harmonic; the harmonic count plus 100 times
+// the offsets at the best S/N
+template <bool SCAL>
+__global__ void k_hs_greedy(float *snr_out, uint16_t *harm_out, const float *__restrict__ d, const float *msd,
+                            int nT, int nH)
+{
+    const int pos0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long row = static_cast<long long>(blockIdx.y) * nT;
+    float SNR, partial_sum, maxSNR;
+    unsigned short maxHarmonics, maxdata_shift = 0;
+    int data_shift = 0;
+    float data_down = 0, data_step = 0;
+    if (pos0 > 1 && pos0 + 3 < nT)
+        psr_bins<SCAL>(&data_down, &data_step, d, row + pos0);
+    if (data_step > data_down) {
+        data_shift++;
+        partial_sum = data_step;
+    } else {
+        partial_sum = data_down;
+    }
+    maxSNR = fdividef((partial_sum - msd[0]), msd[1]);
+    maxHarmonics = 0;
+    for (int h = 1; h < nH; h++) {
+        const int pos = (h + 1) * pos0 + data_shift;
+        float dd = 0, ds = 0;
+        if (pos > 1 && pos + 3 < nT)
+            psr_bins<SCAL>(&dd, &ds, d, row + pos);
+        if (ds > dd) {
+            data_shift++;
+            partial_sum = partial_sum + ds;
+        } else {
+            partial_sum = partial_sum + dd;
+        }
+        SNR = fdividef((partial_sum - msd[2 * h]), msd[2 * h + 1]);
+        if (SNR > maxSNR) {
+            maxSNR = SNR;
+            maxHarmonics = h;
+            maxdata_shift = data_shift;
+        }
+    }
+    if (pos0 < nT) {
+        snr_out[row + pos0] = maxSNR;
+        harm_out[row + pos0] = static_cast<uint16_t>(maxHarmonics + maxdata_shift * 100);
+    }
+}
+
+// PRESTO plus: harmonic i+1 sums the bins round(f * pos / (i + 1)), f = 1..i,
+// onto the fundamental; the reported count is i - 1, as in the reference
+template <bool SCAL>
+__global__ void k_hs_presto_plus(float *snr_out, uint16_t *harm_out, const float *__restrict__ d, const float *msd,
+                                 int nT, int nH)
+{
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long row = static_cast<long long>(blockIdx.y) * nT;
+    float SNR, partial_sum, maxSNR, frequency_bin, fundamental = 0;
+    int maxHarmonics;
+    if ((pos > 1) && (pos + 2) < nT)
+        psr_bin_value<SCAL>(&fundamental, d, row + pos);
+    partial_sum = fundamental;
+    maxSNR = fdividef((partial_sum - msd[0]), msd[1]);
+    maxHarmonics = 0;
+    if (pos > 1 && (pos + 2) < nT) {
+        for (int i = 1; i < nH; i++) {
+            partial_sum = fundamental;
+            const double fundamental_fraction = ((double)pos) / ((double)(i + 1));
+            for (int f = 1; f <= i; f++) {
+                const int new_pos = (int)((((double)f) * fundamental_fraction) + 0.5);
+                frequency_bin = 0;
+                if (new_pos > 1 && (new_pos + 2) < nT)
+                    psr_bin_value<SCAL>(&frequency_bin, d, row + new_pos);
+                partial_sum = partial_sum + frequency_bin;
+            }
+            SNR = fdividef((partial_sum - msd[2 * i]), msd[2 * i + 1]);
+            if (SNR > maxSNR) {
+                maxSNR = SNR;
+                maxHarmonics = i - 1;
+            }
+        }
+    }
+    if (pos < nT) {
+        snr_out[row + pos] = maxSNR;
+        harm_out[row + pos] = static_cast<uint16_t>(maxHarmonics);
+    }
+}
+
+// PRESTO: sums of 1, 2, 4, ... 2^(factor-1) harmonics (factor =
+// floor(log2(nHarmonics)) + 1), the even multiples of a fundamental at
+// round(pos / harm)
+template <bool SCAL>
+__global__ void k_hs_presto(float *snr_out, uint16_t *harm_out, const float *__restrict__ d, const float *msd, int nT,
+                            int nHarmonicsFactor)
+{
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long row = static_cast<long long>(blockIdx.y) * nT;
+    float SNR, partial_sum, maxSNR = -10000, frequency_bin, fundamental;
+    int maxHarmonics = 0;
+    for (int i = 0; i < nHarmonicsFactor; i++) {
+        const int harm = (1 << i);
+        const float fundamental_frac = ((double)pos) * (1.0 / ((double)harm));
+        const int fundamental_pos = (int)(fundamental_frac + 0.5);
+        fundamental = 0;
+        if (fundamental_pos > 1 && (fundamental_pos + 2) < nT)
+            psr_bin_value<SCAL>(&fundamental, d, row + fundamental_pos);
+        partial_sum = fundamental;
+        for (int f = 2; f <= harm; f = f + 2) {
+            const int new_pos = (int)(((float)f) * fundamental_frac + 0.5);
+            frequency_bin = 0;
+            if (new_pos > 1 && (new_pos + 2) < nT)
+                psr_bin_value<SCAL>(&frequency_bin, d, row + new_pos);
+            partial_sum = partial_sum + frequency_bin;
+        }
+        SNR = fdividef((partial_sum - msd[2 * (harm / 2)]), msd[2 * (harm / 2) + 1]);
+        if (SNR > maxSNR) {
+            maxSNR = SNR;
+            maxHarmonics = harm - 1;
+        }
+    }
+    if (pos < nT) {
+        snr_out[row + pos] = maxSNR;
+        harm_out[row + pos] = static_cast<uint16_t>(maxHarmonics);
+    }
+}
+
 } // namespace
 
 long long psr_kernel_launches() { return g_psr_launches.load(); }
+
+// src/aa_device_harmonic_summing.cu:38-169
+cudaError_t psr_harmonic_sum(int algorithm, const float *d_input, float *d_snr, uint16_t *d_harmonics,
+                             const float *d_msd, int nTimesamples, int nDMs, int nHarmonics, bool scalloping,
+                             cudaStream_t st)
+{
+    if (nTimesamples < 1 || nDMs < 1 || nHarmonics < 1 || nHarmonics > 32)
+        return cudaErrorInvalidValue;
+    // PRESTO sums 1, 2, 4, ... harmonics: src/aa_device_harmonic_summing.cu:143
+    const int factor = static_cast<int>(std::log(static_cast<double>(nHarmonics)) / std::log(2.0)) + 1;
+    const dim3 grid((nTimesamples + 255) / 256, nDMs);
+    switch (algorithm * 2 + (scalloping ? 1 : 0)) {
+    case 2: k_hs_greedy<false><<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_input, d_msd, nTimesamples, nHarmonics); break;
+    case 3: k_hs_greedy<true><<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_input, d_msd, nTimesamples, nHarmonics); break;
+    case 4: k_hs_presto_plus<false><<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_input, d_msd, nTimesamples, nHarmonics); break;
+    case 5: k_hs_presto_plus<true><<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_input, d_msd, nTimesamples, nHarmonics); break;
+    case 6: k_hs_presto<false><<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_input, d_msd, nTimesamples, factor); break;
+    case 7: k_hs_presto<true><<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_input, d_msd, nTimesamples, factor); break;
+    default: return cudaErrorInvalidValue;
+    }
+    ++g_psr_launches;
+    return cudaGetLastError();
+}
 
 // src/aa_device_threshold.cu:56-163 (transposed and normal planes)
 cudaError_t psr_threshold(const float *d_snr, const uint16_t *d_harmonics, float *d_list, int nTimesamples, int nDMs,

@@ -39,6 +39,13 @@ cudaError_t psr_threshold(const float *d_snr, const uint16_t *d_harmonics, float
                           float threshold, int max_peaks, int *d_count, const float *d_msd, int dm_shift, int in_bin,
                           bool transposed, bool greedy, cudaStream_t st);
 
+// Harmonic sums over a normal plane [nDMs][nTimesamples]: algorithm 1
+// greedy, 2 PRESTO plus, 3 PRESTO (sums of 1, 2, 4, ... harmonics up to
+// nHarmonics); scalloping: the scalloping-loss correction of the bins.
+cudaError_t psr_harmonic_sum(int algorithm, const float *d_input, float *d_snr, uint16_t *d_harmonics,
+                             const float *d_msd, int nTimesamples, int nDMs, int nHarmonics, bool scalloping,
+                             cudaStream_t st);
+
 long long psr_kernel_launches();
 
 } // namespace aab200

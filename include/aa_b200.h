@@ -609,6 +609,15 @@ int aa_b200_psr_peak_find(const float *d_snr, const unsigned short *d_harmonics,
 int aa_b200_psr_threshold(const float *d_snr, const unsigned short *d_harmonics, float *d_list, int nTimesamples,
                           int nDMs, float threshold, int max_peaks, int *d_count, const float *d_msd, int dm_shift,
                           int in_bin, int transposed, int greedy, void *stream);
+/* The other harmonic sums of the periodicity search on a normal plane
+ * [nDMs][nTimesamples] (src/aa_device_harmonic_summing.cu:38-169): algorithm
+ * 1 greedy (counts carry 100 x the bin offsets taken), 2 PRESTO plus, 3
+ * PRESTO (sums of 1, 2, 4, ... harmonics, floor(log2 nHarmonics) + 1 of
+ * them); nHarmonics 1..32; scalloping != 0 corrects each bin for the
+ * scalloping loss.  d_msd: (mean, deviation) per harmonic count. */
+int aa_b200_psr_harmonic_sum(int algorithm, const float *d_input, float *d_snr, unsigned short *d_harmonics,
+                             const float *d_msd, int nTimesamples, int nDMs, int nHarmonics, int scalloping,
+                             void *stream);
 long long aa_b200_psr_kernel_launches(void);
 const char *aa_b200_psr_last_error(void);
 

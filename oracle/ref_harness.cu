@@ -512,6 +512,41 @@ int aaref_psr_peaks(const float *snr, const unsigned short *harm, int nT, int nD
     return rc;
 }
 
+/* The reference's greedy (algorithm 1), PRESTO plus (2) or PRESTO (3)
+ * harmonic sum (src/aa_device_harmonic_summing.cu:38-169) on a host plane
+ * [nDMs][nT] with msd[2*n_msd]: snr and harmonic counts [nDMs][nT].
+ * nH is passed as the reference's nHarmonics argument.  Returns 0 or < 0. */
+int aaref_psr_harmonics(int algorithm, const float *in, int nT, int nDMs, const float *msd, int n_msd, int nH,
+                        int scalloping, float *snr, unsigned short *harm)
+{
+    const size_t n = (size_t)nT * (size_t)nDMs;
+    float *d_in = NULL, *d_snr = NULL, *d_msd = NULL;
+    unsigned short *d_harm = NULL;
+    if (cudaMalloc((void **)&d_in, n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_snr, n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_harm, n * sizeof(unsigned short)) != cudaSuccess ||
+        cudaMalloc((void **)&d_msd, 2 * (size_t)n_msd * sizeof(float)) != cudaSuccess)
+        return -3;
+    cudaMemcpy(d_in, in, n * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_msd, msd, 2 * (size_t)n_msd * sizeof(float), cudaMemcpyHostToDevice);
+    int rc = 0;
+    if (algorithm == 1)
+        rc = periodicity_greedy_harmonic_summing(d_in, d_snr, d_harm, d_msd, nT, nDMs, nH, scalloping);
+    else if (algorithm == 2)
+        rc = periodicity_presto_plus_harmonic_summing(d_in, d_snr, d_harm, d_msd, nT, nDMs, nH, scalloping);
+    else
+        rc = periodicity_presto_harmonic_summing(d_in, d_snr, d_harm, d_msd, nT, nDMs, nH, scalloping);
+    if (cudaDeviceSynchronize() != cudaSuccess)
+        rc = -5;
+    cudaMemcpy(snr, d_snr, n * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaMemcpy(harm, d_harm, n * sizeof(unsigned short), cudaMemcpyDeviceToHost);
+    cudaFree(d_in);
+    cudaFree(d_snr);
+    cudaFree(d_harm);
+    cudaFree(d_msd);
+    return rc;
+}
+
 /* Two stages of the reference's periodicity search on given host data:
  * simple_power_and_interbin (src/aa_device_power.cu:34-52) on nDMs spectra
  * of nT/2+1 complex bins (spectra: 2*nDMs*(nT/2+1) floats) into power

@@ -101,6 +101,21 @@ def main():
             "rc": rc, "count": k, "records_sha256": hashlib.sha256(json.dumps(recs).encode()).hexdigest(),
             "records_head": recs[:32]}
         print(name, "threshold" if mode else "peaks", rc, k, flush=True)
+    L.aaref_psr_harmonics.argtypes = [i, Pf, i, i, Pf, i, i, i, Pf, ctypes.POINTER(ctypes.c_ushort)]
+    L.aaref_psr_harmonics.restype = i
+    out["harmonic_algorithms"] = {}
+    for name, c in P.HS_ALGO_CASES.items():
+        x, msd = P.make_hs_algo_input(c)
+        snr = np.zeros(x.size, np.float32)
+        hm = np.zeros(x.size, np.uint16)
+        rc = L.aaref_psr_harmonics(c["algorithm"], np.ascontiguousarray(x).ctypes.data_as(Pf), c["nt"], c["ndms"],
+                                   msd.ctypes.data_as(Pf), 32, c["nh"], c["scalloping"], snr.ctypes.data_as(Pf),
+                                   hm.ctypes.data_as(ctypes.POINTER(ctypes.c_ushort)))
+        out["harmonic_algorithms"][name] = {"rc": rc, "snr_sha256": hashlib.sha256(snr.tobytes()).hexdigest(),
+                                            "harmonics_sha256": hashlib.sha256(hm.tobytes()).hexdigest(),
+                                            "snr_head": snr[:256].view(np.uint32).tolist(),
+                                            "harmonics_head": hm[:256].tolist()}
+        print(name, rc, flush=True)
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     with open(args.out, "w") as f:
         json.dump(out, f, indent=1)

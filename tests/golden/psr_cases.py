@@ -93,3 +93,27 @@ def make_peak_plane(c):
     msd[0::2] = 2.0 * (f + 1)
     msd[1::2] = np.sqrt(f + 1) * np.float32(1.5)
     return snr, harm, msd
+
+
+# Greedy (1), PRESTO plus (2) and PRESTO (3) harmonic sums on normal power
+# planes [ndms][nt]; nh is the reference's nHarmonics argument; the msd table
+# always has 32 entries.
+HS_ALGO_CASES = {
+    "greedy_h16": dict(algorithm=1, nt=8192, ndms=6, seed=14, nh=16, scalloping=0),
+    "greedy_h8_scal": dict(algorithm=1, nt=5000, ndms=5, seed=15, nh=8, scalloping=1),
+    "presto_plus_h8": dict(algorithm=2, nt=4096, ndms=4, seed=16, nh=8, scalloping=0),
+    "presto_plus_h6_scal": dict(algorithm=2, nt=3001, ndms=3, seed=17, nh=6, scalloping=1),
+    "presto_h5": dict(algorithm=3, nt=8192, ndms=4, seed=18, nh=5, scalloping=0),
+    "presto_h4_scal": dict(algorithm=3, nt=6000, ndms=3, seed=19, nh=4, scalloping=1),
+    "presto_h32": dict(algorithm=3, nt=8192, ndms=3, seed=20, nh=32, scalloping=0),
+}
+
+
+def make_hs_algo_input(c):
+    """(plane [ndms][nt] float32 power with harmonic combs, msd [64] float32)."""
+    x = make_power_plane(dict(nt=c["nt"], ndms=c["ndms"], seed=c["seed"]))
+    f = np.arange(32, dtype=np.float32)
+    msd = np.empty(64, np.float32)
+    msd[0::2] = f + 1
+    msd[1::2] = np.sqrt(f + 1)
+    return x, msd

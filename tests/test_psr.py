@@ -132,3 +132,28 @@ def test_periodicity_peaks_match_reference_gpu(aa, golden, name, mode):
     recs = sorted(tuple(int(v) for v in r) for r in d_list[:4 * k].cpu().numpy().view(np.uint32).reshape(-1, 4))
     assert [list(r) for r in recs[:32]] == g["records_head"]
     assert hashlib.sha256(json.dumps(recs).encode()).hexdigest() == g["records_sha256"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(P.HS_ALGO_CASES))
+def test_harmonic_sum_algorithms_match_reference_gpu(aa, golden, name):
+    """Greedy, PRESTO plus and PRESTO harmonic sums (with and without the
+    scalloping-loss correction), bit for bit."""
+    import torch
+    c = P.HS_ALGO_CASES[name]
+    g = golden["harmonic_algorithms"][name]
+    assert g["rc"] == 0
+    x, msd = P.make_hs_algo_input(c)
+    dx = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    dm = torch.from_numpy(msd).cuda()
+    snr = torch.zeros(x.size, device="cuda")
+    hm = torch.zeros(x.size, dtype=torch.int16, device="cuda")
+    assert aa.lib().aa_b200_psr_harmonic_sum(c["algorithm"], dx.data_ptr(), snr.data_ptr(), hm.data_ptr(),
+                                             dm.data_ptr(), c["nt"], c["ndms"], c["nh"], c["scalloping"], None) == 0
+    torch.cuda.synchronize()
+    s_np = snr.cpu().numpy()
+    h_np = hm.cpu().numpy().view(np.uint16)
+    assert s_np[:256].view(np.uint32).tolist() == g["snr_head"]
+    assert h_np[:256].tolist() == g["harmonics_head"]
+    assert hashlib.sha256(s_np.tobytes()).hexdigest() == g["snr_sha256"]
+    assert hashlib.sha256(h_np.tobytes()).hexdigest() == g["harmonics_sha256"]
