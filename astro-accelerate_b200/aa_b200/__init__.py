@@ -222,6 +222,8 @@ def lib():
         "aa_b200_psr_threshold": ([vp, vp, vp, i, i, f, i, vp, vp, i, i, i, i, vp], i),
         "aa_b200_psr_harmonic_sum": ([i, vp, vp, vp, vp, i, i, i, i, vp], i),
         "aa_b200_psr_last_error": ([], ctypes.c_char_p),
+        "aa_b200_psr_whitening": ([vp, ctypes.c_size_t, i, vp], i),
+        "aa_b200_psr_segment_sizes": ([ctypes.c_size_t, vp, i], i),
         "aa_b200_spd_create": ([ll, ll], vp),
         "aa_b200_spd_destroy": ([vp], None),
         "aa_b200_spd_last_error": ([vp], ctypes.c_char_p),

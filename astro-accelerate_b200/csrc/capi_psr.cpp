@@ -3,6 +3,7 @@
 #include "aa_b200.h"
 
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -67,6 +68,25 @@ int aa_b200_psr_harmonic_sum(int algorithm, const float *d_input, float *d_snr, 
     return psr_status(psr_harmonic_sum(algorithm, d_input, d_snr, d_harmonics, d_msd, nTimesamples, nDMs, nHarmonics,
                                        scalloping != 0, static_cast<cudaStream_t>(stream)),
                       "harmonic sum");
+}
+
+int aa_b200_psr_whitening(void *d_spectra, size_t nSamples, int nDMs, void *stream)
+{
+    if (!d_spectra || nDMs < 1 || nSamples < 8) {
+        g_psr_error = "spectral whitening: a spectrum of at least 8 bins needed";
+        return 1;
+    }
+    return psr_status(psr_whitening(static_cast<float2 *>(d_spectra), nSamples, nDMs,
+                                    static_cast<cudaStream_t>(stream)),
+                      "spectral whitening");
+}
+
+int aa_b200_psr_segment_sizes(size_t nSamples, int *out, int cap)
+{
+    const std::vector<int> s = psr_segment_sizes(6, 250, nSamples);
+    for (int i = 0; out && i < cap && i < static_cast<int>(s.size()); ++i)
+        out[i] = s[i];
+    return static_cast<int>(s.size());
 }
 
 long long aa_b200_psr_kernel_launches(void) { return psr_kernel_launches(); }

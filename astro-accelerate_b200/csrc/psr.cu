@@ -3,6 +3,7 @@
 
 #include <atomic>
 #include <cmath>
+#include <vector>
 
 namespace aab200 {
 
@@ -316,9 +317,184 @@ __global__ void k_hs_presto(float *snr_out, uint16_t *harm_out, const float *__r
     }
 }
 
+// Spectral whitening, segment medians
+// (src/aa_device_spectral_whitening_kernel.cu:338-376): the median of the
+// powers |X|^2 of one segment (at most 256 bins), sorted in shared memory
+// with zeros padding the 256 slots; an even count averages the sorted
+// values at count/2 and count/2 + 1, as the reference does.
+constexpr int PSR_SEG_SLOTS = 256;
+
+__global__ void __launch_bounds__(PSR_SEG_SLOTS / 2) k_segment_medians(float *medians, const float2 *__restrict__ in,
+                                                                         const int *__restrict__ seg, long long nSamples,
+                                                                         int nSegments)
+{
+    __shared__ float v[PSR_SEG_SLOTS];
+    const int t = threadIdx.x;
+    const int start = seg[blockIdx.x], end = seg[blockIdx.x + 1];
+    const int range = end - start;
+    const long long row = static_cast<long long>(blockIdx.y) * nSamples;
+    for (int k = t; k < PSR_SEG_SLOTS; k += blockDim.x) {
+        float p = 0;
+        const long long pos = start + k;
+        if (k < range && pos < nSamples) {
+            const float2 value = in[row + pos];
+            p = value.x * value.x + value.y * value.y;
+        }
+        v[k] = p;
+    }
+    __syncthreads();
+    // bitonic sort, ascending
+    for (int size = 2; size <= PSR_SEG_SLOTS; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int k = t; k < PSR_SEG_SLOTS / 2; k += blockDim.x) {
+                const int lo = 2 * k - (k & (stride - 1));
+                const int hi = lo + stride;
+                const bool ascending = (lo & size) == 0;
+                const float a = v[lo], b = v[hi];
+                if ((a > b) == ascending) {
+                    v[lo] = b;
+                    v[hi] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (t == 0) {
+        const int nZeros = PSR_SEG_SLOTS - range;
+        const int median_pos = nZeros + (range >> 1);
+        float median;
+        if ((range & 1) == 0)
+            // a segment of two bins puts median_pos + 1 past the slots
+            // (the reference reads past its shared array there): the
+            // largest slot stands in
+            median = (v[median_pos] + v[min(median_pos + 1, PSR_SEG_SLOTS - 1)]) * 0.5f;
+        else
+            median = v[median_pos];
+        medians[static_cast<long long>(blockIdx.y) * nSegments + blockIdx.x] = median;
+    }
+}
+
+// Spectral whitening (src/aa_device_spectral_whitening_kernel.cu:378-427):
+// the first half segment divided by the square root of its median (scaled
+// by 1/ln 2), bin 0 set to 1; later bins by a linear interpolation of the
+// scaled medians between segment middles, in the reference's mixed
+// float/double expressions.  Block b (b >= 1) covers the bins from the
+// middle of segment b-1 to the middle of segment b; the last block also the
+// bins after the middle of the last segment, with the norms of its threads
+// (interpolation indices range - t, as the reference computes them).
+__global__ void k_whitening_sgp2(const float *__restrict__ medians, float2 *in, const int *__restrict__ seg,
+                                 long long nSamples, int nSegments)
+{
+    const long long rowm = static_cast<long long>(blockIdx.y) * nSegments;
+    if (blockIdx.x == 0) {
+        const int f0_pos = seg[0];
+        const int fp1_pos = seg[1];
+        const int current_range = fp1_pos - f0_pos;
+        const float current_mean = medians[rowm + blockIdx.x] * 1.44269504088896;
+        const float norm = 1.0 / sqrt(current_mean);
+        const long long global_pos = static_cast<long long>(blockIdx.y) * nSamples + threadIdx.x;
+        if (static_cast<int>(threadIdx.x) < (current_range >> 1)) {
+            in[global_pos].x *= norm;
+            in[global_pos].y *= norm;
+        }
+        if (threadIdx.x == 0) {
+            in[global_pos].x = 1.0;
+            in[global_pos].y = 0.0;
+        }
+    } else {
+        const int fm1_pos = seg[blockIdx.x - 1];
+        const int f0_pos = seg[blockIdx.x + 0];
+        const int fp1_pos = seg[blockIdx.x + 1];
+        const int previous_range = f0_pos - fm1_pos;
+        const int current_range = fp1_pos - f0_pos;
+        const float previous_mean = medians[rowm + blockIdx.x - 1] * 1.44269504088896;
+        const float current_mean = medians[rowm + blockIdx.x] * 1.44269504088896;
+        const int range = ((previous_range + current_range + 1) >> 1);
+        const int i = range - threadIdx.x;
+        const float slope = (current_mean - previous_mean) / ((float)range);
+        const float norm = 1.0 / sqrt(previous_mean + slope * i);
+        const int local_pos = fm1_pos + (previous_range >> 1) + i;
+        // an even previous and an odd current segment make this block's
+        // last bin the next block's first (the middle of the current
+        // segment); the reference scales it in both blocks without
+        // ordering, here only the next block scales it, once
+        const bool shared_last = blockIdx.x + 1 < gridDim.x && (previous_range & 1) == 0 && (current_range & 1) == 1;
+        if (i >= 0 && i < range - (shared_last ? 1 : 0) && local_pos < nSamples) {
+            const long long global_pos = static_cast<long long>(blockIdx.y) * nSamples + local_pos;
+            in[global_pos].x *= norm;
+            in[global_pos].y *= norm;
+        }
+        if (blockIdx.x == (gridDim.x - 1)) {
+            const int tail = fm1_pos + (previous_range >> 1) + range + threadIdx.x;
+            if (tail < nSamples) {
+                const long long global_pos = static_cast<long long>(blockIdx.y) * nSamples + tail;
+                in[global_pos].x *= norm;
+                in[global_pos].y *= norm;
+            }
+        }
+    }
+}
+
 } // namespace
 
 long long psr_kernel_launches() { return g_psr_launches.load(); }
+
+// src/aa_device_spectral_whitening.cu:17-31 (segment boundaries, a prefix sum)
+std::vector<int> psr_segment_sizes(int min_segment_length, int max_segment_length, size_t nSamples)
+{
+    std::vector<int> s;
+    s.push_back(0);
+    int seg_length = min_segment_length;
+    int seg_sum = 1 + seg_length;
+    s.push_back(seg_sum);
+    while (static_cast<size_t>(seg_sum + seg_length) < nSamples) {
+        seg_sum = seg_sum + seg_length;
+        seg_length = min_segment_length * std::log(seg_sum);
+        if (seg_length > max_segment_length)
+            seg_length = max_segment_length;
+        s.push_back(seg_sum);
+    }
+    s.push_back(static_cast<int>(nSamples));
+    return s;
+}
+
+// src/aa_device_spectral_whitening.cu:60-118 with enable_median: the
+// boundary table and the nDMs x nSegments medians live in stream-ordered
+// allocations freed on the same stream.
+cudaError_t psr_whitening(float2 *d_spectra, size_t nSamples, int nDMs, cudaStream_t st)
+{
+    if (nDMs < 1 || nSamples < 8 || nSamples > static_cast<size_t>(INT32_MAX))
+        return cudaErrorInvalidValue;
+    const std::vector<int> segments = psr_segment_sizes(6, 250, nSamples);
+    const int nSegments = static_cast<int>(segments.size());
+    int *d_seg = nullptr;
+    float *d_medians = nullptr;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&d_seg), nSegments * sizeof(int), st);
+    if (e != cudaSuccess)
+        return e;
+    e = cudaMallocAsync(reinterpret_cast<void **>(&d_medians), static_cast<size_t>(nSegments) * nDMs * sizeof(float),
+                        st);
+    if (e == cudaSuccess)
+        // pageable source: the call returns once the table is staged
+        e = cudaMemcpyAsync(d_seg, segments.data(), nSegments * sizeof(int), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        k_segment_medians<<<dim3(nSegments - 1, nDMs), PSR_SEG_SLOTS / 2, 0, st>>>(
+            d_medians, d_spectra, d_seg, static_cast<long long>(nSamples), nSegments);
+        ++g_psr_launches;
+        // blocks 0 .. nSegments-2: the reference launches one block more,
+        // which reads the boundary past the table and the median slot its
+        // median kernel never writes, and for any table value below
+        // nSamples - (last segment) writes nothing
+        k_whitening_sgp2<<<dim3(nSegments - 1, nDMs), 256, 0, st>>>(d_medians, d_spectra, d_seg,
+                                                                   static_cast<long long>(nSamples), nSegments);
+        ++g_psr_launches;
+        e = cudaGetLastError();
+    }
+    if (d_medians)
+        cudaFreeAsync(d_medians, st);
+    cudaFreeAsync(d_seg, st);
+    return e;
+}
 
 // src/aa_device_harmonic_summing.cu:38-169
 cudaError_t psr_harmonic_sum(int algorithm, const float *d_input, float *d_snr, uint16_t *d_harmonics,

@@ -7,6 +7,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -45,6 +46,16 @@ cudaError_t psr_threshold(const float *d_snr, const uint16_t *d_harmonics, float
 cudaError_t psr_harmonic_sum(int algorithm, const float *d_input, float *d_snr, uint16_t *d_harmonics,
                              const float *d_msd, int nTimesamples, int nDMs, int nHarmonics, bool scalloping,
                              cudaStream_t st);
+
+// Segment boundaries of the spectral whitening (a prefix sum from 0 to
+// nSamples; segment lengths grow as min * ln(start), capped at max)
+std::vector<int> psr_segment_sizes(int min_segment_length, int max_segment_length, size_t nSamples);
+
+// Spectral whitening (SGP2 with medians) in place: per spectrum the
+// median power of each segment, scaled by 1/ln 2, and every bin divided by
+// the square root of the medians interpolated between segment middles;
+// bin 0 set to (1, 0).  nSamples complex bins per spectrum (>= 8).
+cudaError_t psr_whitening(float2 *d_spectra, size_t nSamples, int nDMs, cudaStream_t st);
 
 long long psr_kernel_launches();
 

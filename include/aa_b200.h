@@ -618,6 +618,17 @@ int aa_b200_psr_threshold(const float *d_snr, const unsigned short *d_harmonics,
 int aa_b200_psr_harmonic_sum(int algorithm, const float *d_input, float *d_snr, unsigned short *d_harmonics,
                              const float *d_msd, int nTimesamples, int nDMs, int nHarmonics, int scalloping,
                              void *stream);
+/* Spectral whitening of the periodicity search (spectrum_whitening_SGP2
+ * with enable_median, src/aa_device_spectral_whitening.cu:60-118), in place
+ * on nDMs spectra of nSamples complex float bins (nSamples >= 8): segment
+ * medians of the power, a linear interpolation of median / ln 2 between
+ * segment middles, every bin divided by its square root; bin 0 set to
+ * (1, 0). */
+int aa_b200_psr_whitening(void *d_spectra, size_t nSamples, int nDMs, void *stream);
+/* The segment boundaries of the whitening
+ * (create_dered_segment_sizes_prefix_sum, src/aa_device_spectral_whitening.cu:17-31,
+ * lengths 6 .. 250): writes up to cap of them, returns their count. */
+int aa_b200_psr_segment_sizes(size_t nSamples, int *out, int cap);
 long long aa_b200_psr_kernel_launches(void);
 const char *aa_b200_psr_last_error(void);
 

@@ -59,3 +59,111 @@ def harmonic_sum_simple(x: np.ndarray, msd: np.ndarray, nh: int):
         snr[rows] = np.where(sel, t[np.isin(idx, rows)], snr[rows])
         harm[rows] = np.where(sel, f, harm[rows])
     return snr, harm
+
+
+# ---------------------------------------------------------------------------
+# Spectral whitening (spectrum_whitening_SGP2 with medians)
+# ---------------------------------------------------------------------------
+def segment_sizes(n_samples: int, min_len: int = 6, max_len: int = 250):
+    """create_dered_segment_sizes_prefix_sum (src/aa_device_spectral_whitening.cu:17-31):
+    0, 1 + min_len, then steps of int(min_len * ln(position)) capped at
+    max_len while the next step stays below n_samples, then n_samples."""
+    import math
+    s = [0]
+    length = min_len
+    total = 1 + length
+    s.append(total)
+    while total + length < n_samples:
+        total += length
+        length = min(int(min_len * math.log(total)), max_len)
+        s.append(total)
+    s.append(n_samples)
+    return s
+
+
+def segment_medians(power_row: np.ndarray, seg):
+    """GPU_kernel_segmented_median (src/aa_device_spectral_whitening_kernel.cu:338-376):
+    the segment's powers sorted among 256 zero-padded slots; odd counts take
+    slot zeros + n/2, even counts the mean of slots zeros + n/2 and the one
+    after (the last slot when that is past the end)."""
+    out = np.empty(len(seg) - 1, np.float32)
+    for b in range(len(seg) - 1):
+        v = np.zeros(256, np.float32)
+        r = seg[b + 1] - seg[b]
+        v[256 - r:] = np.sort(power_row[seg[b]:seg[b + 1]])
+        mp = 256 - r + (r >> 1)
+        out[b] = (v[mp] + v[min(mp + 1, 255)]) * np.float32(0.5) if r % 2 == 0 else v[mp]
+    return out
+
+
+def whitening(spectra: np.ndarray):
+    """GPU_kernel_spectrum_whitening_SGP2 (src/aa_device_spectral_whitening_kernel.cu:378-427)
+    restated on [ndms][n] complex64 spectra: bins divided by the square root
+    of median / ln 2 interpolated linearly between segment middles (the first
+    half segment by its own median, bin 0 set to 1; the bins after the middle
+    of the last segment by the last block's thread norms, index range - t).
+    A bin the reference scales in two blocks (even segment then odd one) is
+    scaled once, by the later block.  Exact float sqrt and division stand in
+    for the reference's fast-math forms: equal to about 1e-6 relative."""
+    x = spectra.astype(np.complex64).copy()
+    ndms, n = x.shape
+    seg = segment_sizes(n)
+    ns = len(seg)
+    ln2inv = 1.44269504088896
+    for d in range(ndms):
+        p = (x[d].real * x[d].real + x[d].imag * x[d].imag).astype(np.float32)
+        med = segment_medians(p, seg)
+        scale = np.ones(n, np.float32)
+        cm = np.float32(np.float64(med[0]) * ln2inv)
+        scale[:(seg[1] - seg[0]) >> 1] = np.float32(1.0 / np.float64(np.sqrt(cm)))
+        for b in range(1, ns - 1):
+            fm1, f0, fp1 = seg[b - 1], seg[b], seg[b + 1]
+            pr, cr = f0 - fm1, fp1 - f0
+            pm = np.float32(np.float64(med[b - 1]) * ln2inv)
+            cm = np.float32(np.float64(med[b]) * ln2inv)
+            rng = (pr + cr + 1) >> 1
+            slope = np.float32(np.float32(cm - pm) / np.float32(rng))
+            last = b == ns - 2
+            shared = not last and pr % 2 == 0 and cr % 2 == 1
+            for t in range(256):
+                i = rng - t
+                with np.errstate(invalid="ignore", divide="ignore"):
+                    norm = np.float32(1.0 / np.float64(np.sqrt(np.float32(pm + np.float32(slope * np.float32(i))))))
+                lp = fm1 + (pr >> 1) + i
+                if 0 <= i < rng - (1 if shared else 0) and lp < n:
+                    scale[lp] = norm
+                if last:
+                    tp = fm1 + (pr >> 1) + rng + t
+                    if tp < n:
+                        scale[tp] = norm
+        x[d] = (x[d].real * scale) + 1j * (x[d].imag * scale)
+        x[d, 0] = 1.0 + 0.0j
+    return x
+
+
+def shared_norms(spectrum: np.ndarray):
+    """For one spectrum ([n] complex64): per bin that two neighbouring
+    blocks of the reference's whitening both scale (an even segment followed
+    by an odd one), the pair (norm of the earlier block's last index, norm of
+    the later block's first index), as whitening() computes norms."""
+    n = spectrum.size
+    seg = segment_sizes(n)
+    p = (spectrum.real * spectrum.real + spectrum.imag * spectrum.imag).astype(np.float32)
+    med = segment_medians(p, seg)
+    ln2inv = 1.44269504088896
+
+    def norm(b, i):
+        pr, cr = seg[b] - seg[b - 1], seg[b + 1] - seg[b]
+        pm = np.float32(np.float64(med[b - 1]) * ln2inv)
+        cm = np.float32(np.float64(med[b]) * ln2inv)
+        rng = (pr + cr + 1) >> 1
+        slope = np.float32(np.float32(cm - pm) / np.float32(rng))
+        return np.float32(1.0 / np.float64(np.sqrt(np.float32(pm + np.float32(slope * np.float32(i))))))
+
+    out = {}
+    for b in range(1, len(seg) - 2):
+        pr, cr = seg[b] - seg[b - 1], seg[b + 1] - seg[b]
+        if pr % 2 == 0 and cr % 2 == 1:
+            rng = (pr + cr + 1) >> 1
+            out[seg[b] + (cr >> 1)] = (norm(b, rng - 1), norm(b + 1, 0))
+    return out

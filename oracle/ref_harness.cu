@@ -54,6 +54,7 @@
 #include "aa_device_harmonic_summing.hpp"
 #include "aa_device_peak_find.hpp"
 #include "aa_device_threshold.hpp"
+#include "aa_device_spectrum_whitening.hpp"
 
 namespace astroaccelerate {
 /* defined in src/aa_device_analysis.cu without a header declaration */
@@ -544,6 +545,34 @@ int aaref_psr_harmonics(int algorithm, const float *in, int nT, int nDMs, const 
     cudaFree(d_snr);
     cudaFree(d_harm);
     cudaFree(d_msd);
+    return rc;
+}
+
+/* spectrum_whitening_SGP2 with medians (src/aa_device_spectral_whitening.cu:60-118)
+ * in place on a device copy of nDMs spectra of nSamples complex bins
+ * (spectra: 2 * nDMs * nSamples floats), the result into out; segments: the
+ * boundary table of create_dered_segment_sizes_prefix_sum (min 6, max 250),
+ * up to seg_cap of them, their count in *nseg.  Returns 0 or < 0. */
+int aaref_psr_whitening(const float *spectra, long long nSamples, int nDMs, float *out, int *segments, int seg_cap,
+                        int *nseg)
+{
+    const size_t n = 2 * (size_t)nDMs * (size_t)nSamples;
+    std::vector<int> seg;
+    create_dered_segment_sizes_prefix_sum(&seg, 6, 250, (size_t)nSamples);
+    *nseg = (int)seg.size();
+    for (int i = 0; i < seg_cap && i < (int)seg.size(); ++i)
+        segments[i] = seg[i];
+    float *d = NULL;
+    if (cudaMalloc((void **)&d, n * sizeof(float)) != cudaSuccess)
+        return -3;
+    cudaMemcpy(d, spectra, n * sizeof(float), cudaMemcpyHostToDevice);
+    cudaStream_t stream = NULL;
+    spectrum_whitening_SGP2((float2 *)d, (size_t)nSamples, nDMs, true, stream);
+    int rc = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess)
+        rc = -5;
+    cudaMemcpy(out, d, n * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(d);
     return rc;
 }
 

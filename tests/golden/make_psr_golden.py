@@ -1,6 +1,8 @@
 """Generates tests/golden/psr_golden.json from the reference's own GPU
 periodicity stages (oracle/ref_harness.cu aaref_psr_blocks:
-simple_power_and_interbin and periodicity_simple_harmonic_summing) on the
+simple_power_and_interbin and periodicity_simple_harmonic_summing; the MSD
+profile, peak finding and thresholding, the harmonic sums and the spectral
+whitening of the other aaref_psr_* entries) on the
 seeded inputs of psr_cases.py: SHA-256 of every output and its first
 values.  Needs a GPU.
 
@@ -116,6 +118,35 @@ def main():
                                             "snr_head": snr[:256].view(np.uint32).tolist(),
                                             "harmonics_head": hm[:256].tolist()}
         print(name, rc, flush=True)
+    L.aaref_psr_whitening.argtypes = [Pf, ctypes.c_longlong, i, Pf, ctypes.POINTER(ctypes.c_int), i,
+                                      ctypes.POINTER(ctypes.c_int)]
+    L.aaref_psr_whitening.restype = i
+    out["whitening"] = {}
+    for name, c in P.WHITENING_CASES.items():
+        z = P.make_red_spectra(c)
+        x = np.ascontiguousarray(z.view(np.float32))
+        y = np.zeros_like(x)
+        seg = np.zeros(1 << 16, np.int32)
+        nseg = ctypes.c_int()
+        rc = L.aaref_psr_whitening(x.ctypes.data_as(Pf), c["n"], c["ndms"], y.ctypes.data_as(Pf),
+                                   seg.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), seg.size, ctypes.byref(nseg))
+        seg = seg[:nseg.value].tolist()
+        yc = y.view(np.complex64).reshape(c["ndms"], c["n"])
+        shared = P.shared_bins(seg)
+        stale = P.stale_bins(seg)
+        masked = yc.copy()
+        masked[:, shared] = 0
+        masked[:, stale] = 0
+        out["whitening"][name] = {
+            "rc": rc, "segments": seg, "out_sha256": hashlib.sha256(y.tobytes()).hexdigest(),
+            "masked_sha256": hashlib.sha256(masked.tobytes()).hexdigest(),
+            "shared": [[d, b, int(yc[d, b:b + 1].view(np.uint32)[0]), int(yc[d, b:b + 1].view(np.uint32)[1])]
+                       for d in range(c["ndms"]) for b in shared],
+            "stale": [[d, b, int(yc[d, b:b + 1].view(np.uint32)[0]), int(yc[d, b:b + 1].view(np.uint32)[1])]
+                      for d in range(c["ndms"]) for b in stale],
+            "head": y.reshape(c["ndms"], -1)[0, :256].view(np.uint32).tolist(),
+            "tail": y.reshape(c["ndms"], -1)[-1, -256:].view(np.uint32).tolist()}
+        print(name, rc, len(seg), flush=True)
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     with open(args.out, "w") as f:
         json.dump(out, f, indent=1)

@@ -117,3 +117,48 @@ def make_hs_algo_input(c):
     msd[0::2] = f + 1
     msd[1::2] = np.sqrt(f + 1)
     return x, msd
+
+
+# Spectral whitening (SGP2 with medians) on red-noise spectra of n complex
+# bins: the periodicity search's nT/2 + 1 bins, an odd and an even size
+WHITENING_CASES = {
+    "white_4097x8": dict(n=4097, ndms=8, seed=21),
+    "white_65537x3": dict(n=65537, ndms=3, seed=22),
+    "white_16384x4": dict(n=16384, ndms=4, seed=23),
+    "white_1000x5": dict(n=1000, ndms=5, seed=24),
+}
+
+
+def make_red_spectra(c) -> np.ndarray:
+    """[ndms][n] complex64: complex Gaussian bins whose power falls as a red
+    spectrum 1 + 300 / (1 + k / 20)^2 over a floor of n, with a few lines."""
+    rng = np.random.Generator(np.random.PCG64(c["seed"]))
+    k = np.arange(c["n"], dtype=np.float64)
+    amp = np.sqrt(c["n"] * (1.0 + 300.0 / (1.0 + k / 20.0) ** 2) / 2.0)
+    z = (rng.normal(0, 1, (c["ndms"], c["n"])) + 1j * rng.normal(0, 1, (c["ndms"], c["n"]))) * amp
+    for d in range(c["ndms"]):
+        f = int(rng.integers(30, c["n"] // 10))
+        for h in range(1, 5):
+            if h * f < c["n"]:
+                z[d, h * f] += 10.0 * np.sqrt(c["n"]) / h
+    return np.ascontiguousarray(z.astype(np.complex64))
+
+
+def shared_bins(seg):
+    """Bins the reference's whitening scales in two neighbouring blocks:
+    where an even segment is followed by an odd one (not the last pair),
+    the middle of the odd one."""
+    out = []
+    for b in range(1, len(seg) - 2):
+        pr, cr = seg[b] - seg[b - 1], seg[b + 1] - seg[b]
+        if pr % 2 == 0 and cr % 2 == 1:
+            out.append(seg[b] + (cr >> 1))
+    return out
+
+
+def stale_bins(seg):
+    """Bins from the middle of the last segment to the end: the reference's
+    whitening launches one block past its segments, which reads the boundary
+    after its table (device memory it never wrote) and, when that word holds
+    a boundary a little past the end, scales these bins a second time."""
+    return list(range(seg[-2] + ((seg[-1] - seg[-2]) >> 1), seg[-1]))
