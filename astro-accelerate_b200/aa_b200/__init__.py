@@ -224,6 +224,16 @@ def lib():
         "aa_b200_psr_last_error": ([], ctypes.c_char_p),
         "aa_b200_psr_whitening": ([vp, ctypes.c_size_t, i, vp], i),
         "aa_b200_psr_segment_sizes": ([ctypes.c_size_t, vp, i], i),
+        "aa_b200_psr_candidates_process": ([vp, ctypes.c_size_t, vp, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_size_t, f, i], i),
+        "aa_b200_psr_candidates_create": ([], vp),
+        "aa_b200_psr_candidates_destroy": ([vp], None),
+        "aa_b200_psr_candidates_add": ([vp, vp, ctypes.c_size_t, i, i, vp, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_size_t, f, i], i),
+        "aa_b200_psr_candidates_count": ([vp], ctypes.c_size_t),
+        "aa_b200_psr_candidates_copy": ([vp, vp], i),
+        "aa_b200_psr_candidates_export": ([vp, ctypes.c_char_p], i),
+        "aa_b200_psr_candidates_last_error": ([], ctypes.c_char_p),
         "aa_b200_spd_create": ([ll, ll], vp),
         "aa_b200_spd_destroy": ([vp], None),
         "aa_b200_spd_last_error": ([vp], ctypes.c_char_p),

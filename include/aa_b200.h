@@ -632,6 +632,33 @@ int aa_b200_psr_segment_sizes(size_t nSamples, int *out, int cap);
 long long aa_b200_psr_kernel_launches(void);
 const char *aa_b200_psr_last_error(void);
 
+/* ---------------------------------------------------------------------------
+ * Periodicity candidate lists (aa_periodicity_candidates,
+ * include/aa_periodicity_candidates.hpp:14-202), host side.  Records of 4
+ * floats (DM trial, bin, power, harmonic count) as the periodicity peak
+ * finding writes them become (DM = trial * dm_step + dm_low, frequency =
+ * bin / (sampling_time * nTimesamples * mod), S/N = (power - msd[2h]) /
+ * msd[2h+1], h); with greedy the hundreds of the harmonic count are a bin
+ * offset that adds offset / h bin widths to the frequency.  mod is 1 for
+ * power lists and 2 for interbin lists (src/aa_device_periods.cu:655-660).
+ * --------------------------------------------------------------------------- */
+/* In place on host records */
+int aa_b200_psr_candidates_process(float *records, size_t n, const float *msd, double dm_low, double dm_step,
+                                   double sampling_time, size_t nTimesamples, float mod, int greedy);
+void *aa_b200_psr_candidates_create(void);
+void aa_b200_psr_candidates_destroy(void *list);
+/* Add_Candidates: copies n records (from device memory when on_device) and
+ * converts them; lists keep the order they were added in. */
+int aa_b200_psr_candidates_add(void *list, const float *records, size_t n, int on_device, int range_id,
+                               const float *msd, double dm_low, double dm_step, double sampling_time,
+                               size_t nTimesamples, float mod, int greedy);
+size_t aa_b200_psr_candidates_count(const void *list);
+/* Copy_candidates: every record, list after list, into out (4 * count floats) */
+int aa_b200_psr_candidates_copy(const void *list, float *out);
+/* Export_candidates_to_file: the same records as raw floats */
+int aa_b200_psr_candidates_export(const void *list, const char *filename);
+const char *aa_b200_psr_candidates_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -167,3 +167,28 @@ def shared_norms(spectrum: np.ndarray):
             rng = (pr + cr + 1) >> 1
             out[seg[b] + (cr >> 1)] = (norm(b, rng - 1), norm(b + 1, 0))
     return out
+
+
+def candidates_process(rec, msd, dm_low, dm_step, tsamp, nt, mod, greedy):
+    """aa_periodicity_candidates_data::Process (include/aa_periodicity_candidates.hpp:81-105)
+    on records [n][4] float32, in its float/double expressions: the bin width
+    (1/tsamp) / float(nt * mod) with nt rounded to float, fraction offset/h
+    in double stored as float, DM and frequency in double stored as float,
+    S/N in float."""
+    r = np.array(rec, np.float32).reshape(-1, 4).copy()
+    h = r[:, 3].astype(np.int64)
+    fc = np.zeros(len(r), np.float32)
+    if greedy:
+        ds = (r[:, 3].astype(np.float64) / 100.0).astype(np.int64)
+        h = h - ds * 100
+        bw = np.float32((1.0 / tsamp) / np.float64(np.float32(np.float32(nt) * np.float32(mod))))
+        pos = h > 0
+        frac = (ds[pos].astype(np.float64) / h[pos].astype(np.float64)).astype(np.float32)
+        fc[pos] = (bw * frac).astype(np.float32)
+    m = np.asarray(msd, np.float32)
+    r[:, 0] = (r[:, 0].astype(np.float64) * dm_step + dm_low).astype(np.float32)
+    r[:, 1] = (r[:, 1].astype(np.float64) * (1.0 / (tsamp * np.float64(nt) * np.float64(np.float32(mod))))
+               + fc.astype(np.float64)).astype(np.float32)
+    r[:, 2] = ((r[:, 2] - m[2 * h]) / m[2 * h + 1]).astype(np.float32)
+    r[:, 3] = h.astype(np.float32)
+    return r

@@ -162,3 +162,37 @@ def stale_bins(seg):
     after its table (device memory it never wrote) and, when that word holds
     a boundary a little past the end, scales these bins a second time."""
     return list(range(seg[-2] + ((seg[-1] - seg[-2]) >> 1), seg[-1]))
+
+
+# Periodicity candidate records (DM trial, bin, power, harmonic count) as the
+# peak finding writes them, converted by the host lists: power lists (mod 1),
+# interbin lists (mod 2), greedy lists (bin offsets in the hundreds)
+CANDIDATE_CASES = {
+    "cands_power": dict(n=3000, ndms=512, nt=1 << 20, nh=32, mod=1.0, greedy=0, dm_low=0.0, dm_step=0.1,
+                        tsamp=6.4e-5, seed=31),
+    "cands_interbin": dict(n=2500, ndms=1024, nt=1 << 18, nh=16, mod=2.0, greedy=0, dm_low=150.0, dm_step=0.25,
+                           tsamp=1.28e-4, seed=32),
+    "cands_greedy": dict(n=4000, ndms=300, nt=(1 << 19) + 3, nh=8, mod=1.0, greedy=1, dm_low=12.5, dm_step=0.05,
+                         tsamp=6.5536e-5, seed=33),
+    "cands_greedy_interbin": dict(n=1500, ndms=77, nt=1 << 16, nh=32, mod=2.0, greedy=1, dm_low=1000.0,
+                                  dm_step=3.0, tsamp=2.56e-4, seed=34),
+}
+
+
+def make_candidate_records(c):
+    """(records [n][4] float32, msd [2*nh] float32)."""
+    rng = np.random.Generator(np.random.PCG64(c["seed"]))
+    n = c["n"]
+    rec = np.empty((n, 4), np.float32)
+    rec[:, 0] = rng.integers(0, c["ndms"], n)
+    rec[:, 1] = rng.integers(1, c["nt"] // 2 * (2 if c["mod"] == 2.0 else 1), n)
+    rec[:, 2] = rng.uniform(5.0, 200.0, n).astype(np.float32)
+    h = rng.integers(0, c["nh"], n)
+    if c["greedy"]:
+        h = h + 100 * rng.integers(0, 4, n)
+    rec[:, 3] = h
+    f = np.arange(c["nh"], dtype=np.float32)
+    msd = np.empty(2 * c["nh"], np.float32)
+    msd[0::2] = np.float32(1.7) * (f + 1)
+    msd[1::2] = np.sqrt(f + 1) * np.float32(1.3)
+    return np.ascontiguousarray(rec), msd
