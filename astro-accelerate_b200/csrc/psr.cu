@@ -332,8 +332,13 @@ __global__ void __launch_bounds__(PSR_SEG_SLOTS / 2) k_segment_medians(float *me
     const int t = threadIdx.x;
     const int start = seg[blockIdx.x], end = seg[blockIdx.x + 1];
     const int range = end - start;
+    // Powers are >= 0 and the pads are zeros, so the sorted slots hold the
+    // pads first and slot pads + k is the k-th smallest power for any pad
+    // count: the smallest power of two (64 .. 256) above the segment sorts
+    // to the same median as the reference's 256 slots.
+    const int slots = range <= 64 ? 64 : (range <= 128 ? 128 : PSR_SEG_SLOTS);
     const long long row = static_cast<long long>(blockIdx.y) * nSamples;
-    for (int k = t; k < PSR_SEG_SLOTS; k += blockDim.x) {
+    for (int k = t; k < slots; k += blockDim.x) {
         float p = 0;
         const long long pos = start + k;
         if (k < range && pos < nSamples) {
@@ -343,10 +348,10 @@ __global__ void __launch_bounds__(PSR_SEG_SLOTS / 2) k_segment_medians(float *me
         v[k] = p;
     }
     __syncthreads();
-    // bitonic sort, ascending
-    for (int size = 2; size <= PSR_SEG_SLOTS; size <<= 1) {
+    // bitonic sort, ascending (slots is block-uniform)
+    for (int size = 2; size <= slots; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int k = t; k < PSR_SEG_SLOTS / 2; k += blockDim.x) {
+            for (int k = t; k < slots / 2; k += blockDim.x) {
                 const int lo = 2 * k - (k & (stride - 1));
                 const int hi = lo + stride;
                 const bool ascending = (lo & size) == 0;
@@ -360,14 +365,14 @@ __global__ void __launch_bounds__(PSR_SEG_SLOTS / 2) k_segment_medians(float *me
         }
     }
     if (t == 0) {
-        const int nZeros = PSR_SEG_SLOTS - range;
+        const int nZeros = slots - range;
         const int median_pos = nZeros + (range >> 1);
         float median;
         if ((range & 1) == 0)
             // a segment of two bins puts median_pos + 1 past the slots
             // (the reference reads past its shared array there): the
             // largest slot stands in
-            median = (v[median_pos] + v[min(median_pos + 1, PSR_SEG_SLOTS - 1)]) * 0.5f;
+            median = (v[median_pos] + v[min(median_pos + 1, slots - 1)]) * 0.5f;
         else
             median = v[median_pos];
         medians[static_cast<long long>(blockIdx.y) * nSegments + blockIdx.x] = median;

@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="survey", choices=["survey", "mid", "small", "batched", "refine", "e2e", "spd"])
+    ap.add_argument("--config", default="survey", choices=["survey", "mid", "small", "batched", "refine", "e2e", "spd", "whitening"])
     ap.add_argument("--beams", type=int, default=48, help="beams of the multi-beam draw (batched config)")
     ap.add_argument("--snippets", type=int, default=256, help="snippets per step (refine config)")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -812,6 +812,109 @@ def run_spd(args, rank, world, local):
     return 0
 
 
+WHITENING_WORKLOAD = dict(ndms=512, nbins=(1 << 20) // 2 + 1, seed=41)
+
+
+def run_whitening(args, rank, world, local):
+    """Spectral whitening of the periodicity search (the reference's
+    spectrum_whitening_SGP2 with medians, bit-exact outside its raced bins)
+    on 512 spectra of 2^19 + 1 complex bins (the spectra of 2^20-sample
+    series, 2.1 GB, above L2), resident in HBM: one step = segment medians
+    and the interpolated normalisation, in place; the spectra are restored
+    from a pristine copy outside the timed region.  Algorithmic bytes: 8 per
+    bin read by the median kernel, 8 read and 8 written by the
+    normalisation.  e2e: pinned host spectra in, whitened spectra out,
+    through aa_b200_psr_whitening."""
+    import numpy as np
+    import torch
+    import aa_b200 as aa
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    w = WHITENING_WORKLOAD
+    nb, nd = w["nbins"], w["ndms"]
+    g = torch.Generator(device=device)
+    g.manual_seed(w["seed"] + rank)
+    k = torch.arange(nb, device=device, dtype=torch.float32)
+    amp = torch.sqrt(nb * (1.0 + 300.0 / (1.0 + k / 20.0) ** 2) / 2.0)
+    pristine = (torch.randn((nd, nb, 2), device=device, generator=g) * amp[None, :, None]).contiguous()
+    spec = torch.empty_like(pristine)
+    L = aa.lib()
+    stream = torch.cuda.current_stream(device).cuda_stream
+
+    def one():
+        if L.aa_b200_psr_whitening(spec.data_ptr(), nb, nd, stream) != 0:
+            raise RuntimeError(L.aa_b200_psr_last_error().decode())
+
+    for _ in range(max(3, args.warmup)):
+        spec.copy_(pristine)
+        one()
+    torch.cuda.synchronize()
+    launches0 = L.aa_b200_psr_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            spec.copy_(pristine)
+            torch.cuda.synchronize()
+            e0.record()
+            one()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    launches = (L.aa_b200_psr_kernel_launches() - launches0) // max(1, args.steps)
+    step_ms = statistics.median(ms)
+    host = torch.empty_like(pristine, device="cpu").pin_memory()
+    host.copy_(pristine)
+    out = torch.empty_like(host).pin_memory()
+    e2e_ms = []
+    for _ in range(max(1, args.e2e_steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        spec.copy_(host, non_blocking=True)
+        one()
+        out.copy_(spec, non_blocking=True)
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e = statistics.median(e2e_ms)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    bins = nd * nb
+    achieved = 24.0 * bins / (step_ms / 1e3) / 1e9
+    cpu = None
+    if rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import psr_oracle as O
+        sample = pristine[0].cpu().numpy().astype(np.float32)
+        z = (sample[:, 0] + 1j * sample[:, 1]).astype(np.complex64)[None, :]
+        t0 = time.perf_counter()
+        O.whitening(z)
+        dt = time.perf_counter() - t0
+        cpu = {"value": z.size / dt, "unit": "bins/s", "cores": 1, "kind": "port",
+               "sample": f"oracle on 1 spectrum of {z.size} bins, {dt:.1f} s"}
+    line = {"metric": "spectrum bins/s whitened (periodicity spectral whitening, reference rules)",
+            "value": bins / (step_ms / 1e3), "unit": "bins/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"spectral whitening: {nd} spectra x {nb} complex bins f32 "
+                                   f"({bins * 8 / 1e9:.1f} GB), segment medians and SGP2 normalisation",
+                       "l2": "inputs larger than L2"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "k_segment_medians + k_whitening_sgp2", "achieved": achieved,
+                         "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                         "algorithmic_bytes": 24 * bins},
+            "e2e": {"value": bins / (e2e / 1e3), "unit": "bins/s", "h2d_bytes_per_step": bins * 8,
+                    "d2h_bytes_per_step": bins * 8},
+            "cpu_baseline": cpu, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -825,8 +928,10 @@ def main():
         return run_e2e(args, rank, world, local)
     if args.config == "spd" and args.impl != "reference":
         return run_spd(args, rank, world, local)
+    if args.config == "whitening" and args.impl != "reference":
+        return run_whitening(args, rank, world, local)
     cfg = {"survey": SURVEY, "mid": MID, "small": SMALL, "batched": SURVEY, "refine": SURVEY,
-           "e2e": SURVEY, "spd": SURVEY}[args.config]
+           "e2e": SURVEY, "spd": SURVEY, "whitening": SURVEY}[args.config]
     if args.nbits:
         cfg = dict(cfg, nbits=args.nbits)
     if args.impl == "reference":
