@@ -152,6 +152,8 @@ def lib():
         "aa_b200_selftest_bounded_wait": ([i, P(i)], i),
         "aa_b200_debug_fail_after": ([ll], None),
         "aa_b200_debug_fail_countdown": ([], ll),
+        "aa_b200_smem_load_rate": ([i, vp, P(d), P(f)], i),
+        "aa_b200_binary_version": ([P(i)], i),
         "aa_b200_pipeline_set_export_base": ([vp, ctypes.c_char_p], b),
         "aa_b200_export_dd_data": ([i, PPPFLOAT, sz, P(i), P(i), ctypes.c_char_p, P(i), i], i),
         "aa_b200_sd_per_file_from_file_size": ([sz, sz, sz], sz),
@@ -264,6 +266,16 @@ def declared_symbols() -> list:
     hdr = os.path.join(os.path.dirname(PKG_ROOT), "include", "aa_b200.h")
     text = open(hdr).read()
     return sorted(set(re.findall(r"\b(aa_(?:py|b200)_\w+)\s*\(", text)))
+
+
+def smem_load_rate(iters: int = 4096, stream=None) -> dict:
+    """Measured 32-bit shared-memory loads per second of this GPU (see
+    aa_b200_smem_load_rate) and the adds/s bound it sets for the
+    channel-quad kernel (four channel adds per load)."""
+    rate, ms = ctypes.c_double(), ctypes.c_float()
+    if lib().aa_b200_smem_load_rate(iters, stream, ctypes.byref(rate), ctypes.byref(ms)) != 0:
+        raise RuntimeError("shared-memory load-rate measurement failed")
+    return {"loads_per_s": rate.value, "adds_per_s": 4.0 * rate.value, "ms": ms.value, "iters": iters}
 
 
 def last_error() -> str:

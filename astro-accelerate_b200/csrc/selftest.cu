@@ -77,6 +77,17 @@ int aa_b200_selftest_bounded_wait(int limit, int *status)
     return rc;
 }
 
+int aa_b200_binary_version(int *version)
+{
+    if (!version)
+        return 1;
+    cudaFuncAttributes a{};
+    if (cudaFuncGetAttributes(&a, aab200::k_wait_probe) != cudaSuccess)
+        return 1;
+    *version = a.binaryVersion;
+    return 0;
+}
+
 void aa_b200_debug_fail_after(long long n) { aab200::arm_injected_failure(n); }
 
 long long aa_b200_debug_fail_countdown(void) { return aab200::injected_failure_countdown(); }

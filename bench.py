@@ -8,17 +8,27 @@ strategy -- over one synthetic filterbank of the survey-scale configuration:
 Gaussian noise N(127.5, 16) plus 8 dispersed boxcar pulses (DM U[50, 2900],
 width log-U[0.25, 8] ms, 3-10 sigma).
 
-  value  DM-trial.samples/s with the input resident in HBM ([t][c] uint16) and
-         the output kept in HBM; corner turn, binning and dedispersion of all
-         chunks and ranges are timed with CUDA events on the library's stream.
-  e2e    the same metric through the reference-facing C ABI
-         (aa_py_pipeline_api / run loop) from a pinned host input to the
-         pinned host float*** output, host<->device copies inside the timed
-         region (wall clock between device synchronisations).
+  value     DM-trial.samples/s with the input resident in HBM ([t][c] uint16)
+            and the output kept in HBM; corner turn, binning and dedispersion
+            of all chunks and ranges are timed with CUDA events on the
+            library's stream.
+  parity    the timed run's output compared bit for bit with the oracle on
+            windows it computes in seconds (chunk 0 range 0, the first binned
+            range, every range of the last chunk); a mismatch fails the run.
+  e2e       the same metric through the reference-facing C ABI
+            (aa_py_pipeline_api / run loop) from a pinned host input to the
+            pinned host float*** output, host<->device copies inside the timed
+            region (wall clock between device synchronisations).
+  roofline  the dedispersion kernel's channel adds/s against the shared-memory
+            load rate measured on the same GPU (4 adds per 32-bit load), with
+            the HBM figure beside it.
+  batched_vs_plain  the first 8 beams of the seeded multi-beam draw, batched
+            (one graph, one persistent kernel) and beam by beam, bit-exact.
 
 `--impl reference` times the reference path's CPU restatement (the oracle;
 the reference ships no CPU DDTR) on the host's cores on a bounded sample
-of the same workload.  Under torchrun every rank runs its own beam (weak
+of the same workload, and the reference's own GPU pipeline (built from its
+sources) at 2^18 samples.  Under torchrun every rank runs its own beam (weak
 scaling, no collective on the data path); rank 0 prints one JSON line.
 """
 from __future__ import annotations
@@ -45,6 +55,14 @@ MID = dict(SURVEY, nsamp=1 << 18)
 SMALL = dict(nchans=1024, nbits=8, fch1=1550.0, foff=-0.390625, tsamp=64e-6, nsamp=1 << 18,
              plan=[(0, 500, 0.5, 1, 1)], npulses=1, seed=1)
 METRIC = "DM-trial*samples/s (plain DDTR, 1 beam per GPU, bit-exact)"
+METRIC_UNCHECKED = "DM-trial*samples/s (plain DDTR, 1 beam per GPU)"
+# DRAM bytes per algorithmic byte of the dedispersion kernel, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum of one launch); the
+# roofline's traffic is this ratio times a launch's algorithmic bytes
+TRAFFIC_PER_ALG_BYTE = 2.31 / 2.46
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_ddtr_quad launch (range 0, 4096 ch x "
+                  "2^18 samples: 0.96 + 1.35 GB against 2.46 GB algorithmic), scaled by the algorithmic bytes of "
+                  "an average launch of this workload; profiles/k_ddtr_quad_mid_8bit_4096ch_2e18_range0.md")
 PUBLISHED_REALTIME = 6.28  # reference wiki, 8-range "b2" plan, unnamed GPU
 
 
@@ -59,6 +77,9 @@ def parse():
     ap.add_argument("--snippets", type=int, default=256, help="snippets per step (refine config)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the timed output")
+    ap.add_argument("--multibeam-beams", type=int, default=8,
+                    help="beams of the reduced multi-beam draw timed batched vs plain in the default line (0: off)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--tile-words", type=int, default=0)
     ap.add_argument("--group-dms", type=int, default=0)
@@ -167,28 +188,26 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline(cfg, x_host_tc, strat, seconds):
+def cpu_baseline(cfg, x_host_tc, seconds):
     """The oracle on a bounded sample: range 0, 64-trial DM blocks over a
     131040-sample window of chunk 0, repeated over DM blocks until `seconds`
-    of CPU work.  Returns (DM-trial.samples/s, threads, description)."""
+    of CPU work (strategy from the oracle too).  Returns (DM-trial.samples/s,
+    threads, description)."""
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.build()
+    ost = O.strategy(cfg["plan"], cfg["nchans"], cfg["nsamp"], cfg["fch1"], cfg["foff"], cfg["tsamp"], cfg["nbits"])
     nch = cfg["nchans"]
-    tp = min(131040, strat["t_processed"][0][0])
-    L = tp + strat["maxshift"]
+    tp = min(131040, ost.t_processed[0][0])
+    L = tp + ost.maxshift
     flat = O.corner_turn(np.ascontiguousarray(x_host_tc[:L]), nch, L)
-    d = strat["dm"][0]
-    tsr = np.float32(cfg["tsamp"]) * np.float32(d[3])
-    kind = O.select_kernel(cfg["nbits"], d[2], tsr, strat["dmshifts"][-1])
-    m0 = np.float32(np.float32(d[0]) / tsr)
-    ms = np.float32(np.float32(d[2]) / tsr)
+    d = ost.dm[0]
+    kind, m0, ms = _range_delay_params(O, cfg, d, ost.dmshifts[-1])
     done, t_total, blocks = 0, 0.0, 0
-    while t_total < seconds and blocks * 64 < strat["ndms"][0]:
-        start = np.float32(m0 + np.float32(blocks * 64) * ms)
+    while t_total < seconds and blocks * 64 < ost.ndms[0]:
         t0 = time.perf_counter()
-        O.dedisperse(kind, O.FMA_ALL, flat, L, nch, tp, 64, strat["dmshifts"], start, ms, d[3])
+        O.dedisperse_window(kind, O.FMA_ALL, flat, L, nch, 64 * blocks, 64, 0, tp, ost.dmshifts, m0, ms, d[3])
         t_total += time.perf_counter() - t0
         done += 64 * tp
         blocks += 1
@@ -197,32 +216,233 @@ def cpu_baseline(cfg, x_host_tc, strat, seconds):
 
 
 # ---------------------------------------------------------------------------
-def run_reference_arm(args, cfg, rank, world):
+PARITY_T = 65536  # outputs per DM trial of the windowed chunk-0 checks
+
+
+def _range_delay_params(O, cfg, d, dmshift_last):
+    """Kernel kind, mstartdm and mdmstep of one range as the reference runner
+    computes them (include/aa_permitted_pipelines_generic.hpp:778,
+    src/aa_dedisperse.cpp:18-30): float arithmetic throughout."""
     import numpy as np
-    import aa_b200 as aa
-    strat = aa.strategy(cfg["plan"], cfg["nchans"], cfg["nsamp"], cfg["fch1"], cfg["foff"], cfg["tsamp"],
-                        cfg["nbits"])
+    tsr = np.float32(cfg["tsamp"]) * np.float32(d[3])
+    kind = O.select_kernel(cfg["nbits"], d[2], tsr, dmshift_last)
+    return kind, np.float32(np.float32(d[0]) / tsr), np.float32(np.float32(d[2]) / tsr)
+
+
+def parity_checks(cfg, ost, host_rows, device_rows, log=None):
+    """Bit-for-bit comparison of the timed run's device output with the oracle
+    on windows the oracle finishes in seconds:
+
+      * chunk 0, range 0: the last 64-trial DM block, outputs [0, PARITY_T);
+      * chunk 0, the first x2-binned range: its last DM block over PARITY_T
+        binned outputs (the oracle bins a window of the corner-turned chunk
+        as the reference's first binning step does);
+      * the last chunk (whose input starts beyond 2^31 elements for the
+        survey size): a replay of the reference runner's flat buffer for that
+        chunk -- corner turn, every x2 binning with the runner's lengths
+        (including the mis-strided second and third steps) -- and the last
+        DM block of every range over all its outputs.
+
+    host_rows(a, b) returns input rows [a, b) as [t][c] uint16;
+    device_rows(r, dm0, ndm, col0, ncol) the timed output.  Returns the
+    summary dict for the bench line."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    nch, nr = cfg["nchans"], len(ost.ndms)
+    last = ost.dmshifts[-1]
+    checks, compared, bad = [], 0, 0
+    t_start = time.perf_counter()
+
+    def compare(label, want, r, dm0, col0):
+        nonlocal compared, bad
+        got = device_rows(r, dm0, want.shape[0], col0, want.shape[1])
+        nbad = int(np.count_nonzero(got.view(np.uint32) != want.view(np.uint32)))
+        compared += want.size
+        bad += nbad
+        checks.append({"check": label, "range": r, "dm_trials": [dm0, dm0 + want.shape[0]],
+                       "outputs": [col0, col0 + want.shape[1]], "mismatching": nbad})
+        if log:
+            log(f"parity {label}: {want.size} outputs, {nbad} mismatching")
+
+    def last_block(r):
+        return 64 * (ost.ndms[r] // 64 - 1)
+
+    # chunk 0, range 0
+    d = ost.dm[0]
+    kind, m0, ms = _range_delay_params(O, cfg, d, last)
+    T = min(PARITY_T, ost.t_processed[0][0])
+    L = T + ost.maxshift // d[3]
+    flat = O.corner_turn(host_rows(0, L), nch, L)
+    dm0 = last_block(0)
+    want = O.dedisperse_window(kind, O.FMA_ALL, flat, L, nch, dm0, 64, 0, T, ost.dmshifts, m0, ms, d[3])
+    compare("chunk 0 range 0", want, 0, dm0, 0)
+    # chunk 0, first binned range (a single x2 step from unbinned data)
+    r1 = next((r for r in range(1, nr) if ost.dm[r][3] == 2 and ost.dm[r - 1][3] == 1), None)
+    if r1 is not None and nch % 32 == 0:
+        d = ost.dm[r1]
+        kind, m0, ms = _range_delay_params(O, cfg, d, last)
+        msr = ost.maxshift // 2
+        T = min(PARITY_T, ost.t_processed[r1][0])
+        W = T + msr
+        W += (-W) % 8  # the binning kernel's grid covers whole 16-sample groups
+        flat = O.bin_flat(O.corner_turn(host_rows(0, 2 * W), nch, 2 * W), nch, 2 * W)
+        dm0 = last_block(r1)
+        want = O.dedisperse_window(kind, O.FMA_ALL, flat, W, nch, dm0, 64, 0, T, ost.dmshifts, m0, ms, 2)
+        compare(f"chunk 0 range {r1} (binned x2)", want, r1, dm0, 0)
+    # last chunk: replay of the runner's flat buffer
+    k = ost.num_tchunks - 1
+    if k > 0:
+        inc = sum(ost.t_processed[0][:k])
+        L = ost.t_processed[0][k] + ost.maxshift
+        buf = O.corner_turn(host_rows(inc, inc + L), nch, L)
+        old = 1
+        for r in range(nr):
+            d = ost.dm[r]
+            msr = ost.maxshift // d[3]
+            if d[3] > old:
+                nsb = ost.t_processed[r - 1][k] + msr * d[3]
+                if nsb > L:
+                    # the reference would bin data of an earlier chunk left in its buffer
+                    break
+                buf = O.bin_flat(buf, nch, nsb)
+            old = d[3]
+            tp = ost.t_processed[r][k]
+            kind, m0, ms = _range_delay_params(O, cfg, d, last)
+            dm0 = last_block(r)
+            want = O.dedisperse_window(kind, O.FMA_ALL, buf, tp + msr, nch, dm0, 64, 0, tp, ost.dmshifts, m0, ms,
+                                       d[3])
+            compare(f"chunk {k} range {r}", want, r, dm0, inc // d[3])
+    return {"outputs_compared": compared, "mismatching": bad, "checks": checks, "oracle": "oracle/aa_oracle.c",
+            "oracle_threads": O.num_threads(), "seconds": time.perf_counter() - t_start}
+
+
+# ---------------------------------------------------------------------------
+REF_SAMPLE_T = 16384  # outputs per DM trial of each timed reference block
+
+
+def reference_gpu_mid(cfg_mid, repeats=2):
+    """The reference's own GPU pipeline (AstroAccelerate built from its
+    sources into oracle/_ref/libaaref.so) on the 2^18-sample configuration,
+    where its 32-bit kernel indices stay in range (at 2^21 samples its chunks
+    pass 2^31 elements and the harness refuses them).  Host [t][c] input,
+    DM-time rows copied to the host, the runner's run(status) loop timed by
+    the harness after set-up.  Returns a dict, or a dict with "unavailable"."""
+    import ctypes
+    import numpy as np
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libaaref.so")
+    if not os.path.exists(lib_path):
+        return {"unavailable": "oracle/_ref/libaaref.so is not built (the reference sources were absent at build)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU"}
+        x, _ = synth_input_device(cfg_mid, cfg_mid["seed"], torch.device("cuda", 0))
+        host = x.cpu().numpy().view(np.uint16)
+        del x
+        torch.cuda.empty_cache()
+    except Exception as e:  # noqa: BLE001 - reported in the line
+        return {"unavailable": f"input synthesis failed: {e}"}
+
+    class DM(ctypes.Structure):
+        _fields_ = [("low", ctypes.c_float), ("high", ctypes.c_float), ("step", ctypes.c_float),
+                    ("inBin", ctypes.c_int), ("outBin", ctypes.c_int)]
+
+    L = ctypes.CDLL(lib_path)
+    L.aaref_time_ddtr.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_int, ctypes.POINTER(DM), ctypes.c_int, ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
+    L.aaref_time_ddtr.restype = ctypes.c_int
+    plan = (DM * len(cfg_mid["plan"]))()
+    for k, (lo, hi, st, ib, ob) in enumerate(cfg_mid["plan"]):
+        plan[k].low, plan[k].high, plan[k].step, plan[k].inBin, plan[k].outBin = lo, hi, st, ib, ob
+    secs = []
+    for _ in range(repeats):
+        sec, nt = ctypes.c_double(), ctypes.c_int()
+        rc = L.aaref_time_ddtr(host.ctypes.data, cfg_mid["nchans"], cfg_mid["nsamp"], cfg_mid["tsamp"],
+                               cfg_mid["fch1"], cfg_mid["foff"], cfg_mid["nbits"], plan, len(cfg_mid["plan"]), 1,
+                               ctypes.byref(sec), ctypes.byref(nt))
+        if rc != 0:
+            return {"unavailable": f"reference pipeline returned {rc}"}
+        secs.append(sec.value)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ost = O.strategy(cfg_mid["plan"], cfg_mid["nchans"], cfg_mid["nsamp"], cfg_mid["fch1"], cfg_mid["foff"],
+                     cfg_mid["tsamp"], cfg_mid["nbits"])
+    units = sum(ost.ndms[r] * ost.total_samps(r) for r in range(len(ost.ndms)))
+    sec = min(secs)
+    return {"workload": f"{cfg_mid['nchans']} ch x {cfg_mid['nsamp']} samples, {cfg_mid['nbits']}-bit, "
+                        f"{len(cfg_mid['plan'])}-range survey plan",
+            "value": units / sec, "unit": "DM-trial*samples/s", "ms_per_step": sec * 1e3,
+            "realtime_x": ost.total_samps(0) * cfg_mid["tsamp"] / sec, "runs": len(secs),
+            "timing": "the reference runner's run(status) loop after set-up, host [t][c] input, rows copied to "
+                      "the host (wall clock inside oracle/ref_harness.cu), best of the runs"}
+
+
+def reference_cpu_step(O, cfg, ost, x_window, step):
+    """One timed step of the reference arm: for every range, one 64-trial DM
+    block (a different block each step) over REF_SAMPLE_T outputs of a
+    corner-turned window of chunk 0, with that range's delay arithmetic and
+    row length.  Returns the per-range outputs/s."""
+    import numpy as np
+    nch = cfg["nchans"]
+    rates = []
+    for r, d in enumerate(ost.dm):
+        kind, m0, ms = _range_delay_params(O, cfg, d, ost.dmshifts[-1])
+        T = min(REF_SAMPLE_T, ost.t_processed[r][0])
+        nblocks = max(1, ost.ndms[r] // 64)
+        dm0 = 64 * ((7 * step + 3 * r) % nblocks)
+        t0 = time.perf_counter()
+        # the window's row length stands in for the range's (the work per
+        # output does not depend on the row length or the sample values)
+        O.dedisperse_window(kind, O.FMA_ALL, x_window, x_window.shape[1], nch, dm0, 64, 0, T, ost.dmshifts, m0, ms,
+                            d[3])
+        rates.append(64 * T / (time.perf_counter() - t0))
+    return rates
+
+
+def run_reference_arm(args, cfg, rank, world):
+    """The reference arm: the reference ships no CPU dedispersion, so its CPU
+    path is the oracle's restatement of the reference kernels (OpenMP over all
+    host threads), timed on a bounded sample of the same workload and
+    extrapolated per range to a whole step; plus, on the 2^18-sample
+    configuration, the reference's own GPU pipeline built from its sources."""
+    import numpy as np
     if rank != 0:
         return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    ost = O.strategy(cfg["plan"], cfg["nchans"], cfg["nsamp"], cfg["fch1"], cfg["foff"], cfg["tsamp"], cfg["nbits"])
+    nch = cfg["nchans"]
     rng = np.random.Generator(np.random.PCG64(cfg["seed"]))
-    L = min(131040, strat["t_processed"][0][0]) + strat["maxshift"]
-    x = np.clip(np.rint(rng.normal(127.5, 16.0, size=(L, cfg["nchans"]))), 0, 255).astype(np.uint16)
-    per_step = max(2.0, 30.0 / max(1, args.steps + args.warmup))
-    for _ in range(args.warmup):
-        cpu_baseline(cfg, x, strat, 0.5)
-    vals = []
-    desc, threads = "", 1
-    for _ in range(args.steps):
-        v, threads, desc = cpu_baseline(cfg, x, strat, per_step)
-        vals.append(v)
-    value = statistics.median(vals)
+    Wmax = max(min(REF_SAMPLE_T, ost.t_processed[r][0]) + ost.maxshift // ost.dm[r][3] for r in range(len(ost.dm)))
+    vmax = (1 << min(cfg["nbits"], 16)) - 1
+    xt = np.clip(np.rint(rng.normal((vmax + 1) / 2 - 0.5, (vmax + 1) / 16.0, size=(Wmax, nch))), 0, vmax)
+    x_window = O.corner_turn(xt.astype(np.uint16), nch, Wmax).reshape(nch, Wmax)
+    units_r = [ost.ndms[r] * ost.total_samps(r) for r in range(len(ost.dm))]
+    for w in range(args.warmup):
+        reference_cpu_step(O, cfg, ost, x_window, 1000 + w)
+    step_s = []
+    for k in range(args.steps):
+        rates = reference_cpu_step(O, cfg, ost, x_window, k)
+        step_s.append(sum(u / v for u, v in zip(units_r, rates)))
+    sec = statistics.median(step_s)
+    value = sum(units_r) / sec
+    desc = (f"oracle (OpenMP restatement of the reference kernels) per step: one 64-trial DM block of each of the "
+            f"{len(ost.dm)} ranges over {REF_SAMPLE_T} outputs of chunk 0 ({nch} channels); each range's "
+            f"outputs/s scaled to its whole output count, summed to the step time "
+            f"{sec:.0f} s (median of {args.steps} steps); corner turn and binning not timed (<2% of the step on "
+            f"the GPU)")
     line = {"metric": METRIC, "value": value, "unit": "DM-trial*samples/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": units_per_step(strat) / value * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8" if cfg["nbits"] <= 8 else "f32", "data": "synthetic",
             "config": workload_config(cfg), "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": "DM-trial*samples/s", "cores": threads, "kind": "port",
+            "cpu_baseline": {"value": value, "unit": "DM-trial*samples/s", "cores": O.num_threads(), "kind": "port",
                              "sample": desc},
-            "e2e": {"value": value, "unit": "DM-trial*samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": "DM-trial*samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_gpu": reference_gpu_mid(MID) if cfg["nsamp"] >= MID["nsamp"] else None}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -246,27 +466,14 @@ def dev_rows(aa, ptr, shape):
     return torch.as_tensor(aa._DeviceRows(ptr, shape), device="cuda")
 
 
-def run_batched(args, rank, world, local):
-    """Multi-beam workload: the seeded 48-beam draw (aa_b200.workloads), run
-    (a) as batches -- one CUDA graph with one persistent dedispersion kernel
-    per batch, batches sized to device memory -- and (b) beam by beam through
-    the plain pipeline, both with the input resident in HBM and the output
-    kept in HBM, both timed with CUDA events on the same stream.  Every
-    beam's batched output is compared with its plain output bit for bit."""
-    import numpy as np
+def measure_multibeam(aa, WL, beams, steps, warmup, device, stream, clk=None):
+    """Times a multi-beam draw (a) as batches -- one CUDA graph with one
+    persistent dedispersion kernel per batch, batches sized to device memory
+    -- and (b) beam by beam through the plain pipeline, both with the input
+    resident in HBM and the output kept in HBM, both timed with CUDA events on
+    the same stream (median over `steps` runs after `warmup`).  Every beam's
+    batched output is compared with its plain output bit for bit."""
     import torch
-    import torch.distributed as dist
-    import aa_b200 as aa
-    from aa_b200 import workloads as WL
-
-    torch.cuda.set_device(local)
-    device = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
-    beams = WL.multibeam_draw(seed=3 + 1000 * rank, nbeams=args.beams)
-    stream = torch.cuda.Stream(device)
-    stream.wait_stream(torch.cuda.current_stream(device))
     mds, plans, sizes, units_b = [], [], [], []
     for b in beams:
         md = aa.filterbank_metadata_struct(0.0, b["tsamp"], b["fch1"], b["foff"], b["nbits"], b["nsamp"],
@@ -287,80 +494,106 @@ def run_batched(args, rank, world, local):
     tot = dict(batched_ms=0.0, plain_ms=0.0, plain_fresh_s=0.0, setup_s=0.0, units=0, launches=0, items=0)
     bit_exact, mismatches, n_cmp = True, [], 0
     wave_info = []
-    with ClockSampler(local) as clk:
-        for w in waves:
-            xs = {i: WL.synth_beam_device(beams[i], device) for i in w}
-            torch.cuda.synchronize(device)
-            B = aa.batch(free_memory=MULTIBEAM_FREE_MEMORY, stream=stream.cuda_stream)
+    for w in waves:
+        xs = {i: WL.synth_beam_device(beams[i], device) for i in w}
+        torch.cuda.synchronize(device)
+        B = aa.batch(free_memory=MULTIBEAM_FREE_MEMORY, stream=stream.cuda_stream)
+        t0 = time.perf_counter()
+        for i in w:
+            B.add_beam(mds[i], plans[i], xs[i])
+        B.setup()
+        tot["setup_s"] += time.perf_counter() - t0
+        for _ in range(max(1, warmup)):
+            B.run()
+            B.synchronize()
+        ms = []
+        for _ in range(steps):
+            ev0.record(stream)
+            B.run()
+            ev1.record(stream)
+            B.synchronize()
+            ms.append(ev0.elapsed_time(ev1))
+        info = B.info()
+        tot["batched_ms"] += statistics.median(ms)
+        tot["launches"] += info["launches_per_run"]
+        tot["items"] += info["work_items"]
+        wave_info.append({"beams": len(w), "ms": statistics.median(ms), "work_items": info["work_items"],
+                          "persistent_jobs": info["persistent_jobs"], "other_jobs": info["other_jobs"],
+                          "grid": info["grid"], "smem_bytes": info["smem_bytes"]})
+        # plain arm, beam by beam on the same stream
+        for j, i in enumerate(w):
+            b = beams[i]
             t0 = time.perf_counter()
-            for i in w:
-                B.add_beam(mds[i], plans[i], xs[i])
-            B.setup()
-            tot["setup_s"] += time.perf_counter() - t0
-            for _ in range(max(1, args.warmup)):
-                B.run()
-                B.synchronize()
-            ms = []
-            for _ in range(args.steps):
-                ev0.record(stream)
-                B.run()
-                ev1.record(stream)
-                B.synchronize()
-                ms.append(ev0.elapsed_time(ev1))
-            info = B.info()
-            tot["batched_ms"] += statistics.median(ms)
-            tot["launches"] += info["launches_per_run"]
-            tot["items"] += info["work_items"]
-            wave_info.append({"beams": len(w), "ms": statistics.median(ms), "work_items": info["work_items"],
-                              "persistent_jobs": info["persistent_jobs"], "other_jobs": info["other_jobs"],
-                              "grid": info["grid"], "smem_bytes": info["smem_bytes"]})
-            # plain arm, beam by beam on the same stream
-            for j, i in enumerate(w):
-                b = beams[i]
-                t0 = time.perf_counter()
-                pipe = aa.create_pipeline(mds[i], xs[i].data_ptr(), device_input=True, device_output=True,
-                                          copy_to_host=False, stream=stream.cuda_stream, card_number=local)
-                pipe.set_options(free_memory=MULTIBEAM_FREE_MEMORY)
-                if not pipe.bind_ddtr_plan(plans[i]) or not (pipe.run_all() and pipe.synchronize()):
+            pipe = aa.create_pipeline(mds[i], xs[i].data_ptr(), device_input=True, device_output=True,
+                                      copy_to_host=False, stream=stream.cuda_stream, card_number=device.index or 0)
+            pipe.set_options(free_memory=MULTIBEAM_FREE_MEMORY)
+            if not pipe.bind_ddtr_plan(plans[i]) or not (pipe.run_all() and pipe.synchronize()):
+                raise RuntimeError(pipe.last_error())
+            tot["plain_fresh_s"] += time.perf_counter() - t0
+            for _ in range(max(0, warmup - 1)):
+                pipe.rewind()
+                if not (pipe.run_all() and pipe.synchronize()):
                     raise RuntimeError(pipe.last_error())
-                tot["plain_fresh_s"] += time.perf_counter() - t0
-                pms = []
-                for _ in range(args.steps):
-                    pipe.rewind()
-                    ev0.record(stream)
-                    if not pipe.run_all():
-                        raise RuntimeError(pipe.last_error())
-                    ev1.record(stream)
-                    if not pipe.synchronize():
-                        raise RuntimeError(pipe.last_error())
-                    pms.append(ev0.elapsed_time(ev1))
-                tot["plain_ms"] += statistics.median(pms)
-                for r in range(len(b["plan"])):
-                    ndms, total, _ = B.range_shape(j, r)
-                    a = B.output(j, r).view(torch.int32)
-                    p = dev_rows(aa, pipe.device_output(r), (ndms, total)).view(torch.int32)
-                    n_cmp += 1
-                    if not torch.equal(a, p):
-                        bit_exact = False
-                        mismatches.append([i, r])
-                pipe.cleanUp()
-                pipe.delete()
-                tot["units"] += units_b[i]
-            B.delete()
-            del xs
-            torch.cuda.synchronize(device)
-            torch.cuda.empty_cache()
+            pms = []
+            for _ in range(steps):
+                pipe.rewind()
+                ev0.record(stream)
+                if not pipe.run_all():
+                    raise RuntimeError(pipe.last_error())
+                ev1.record(stream)
+                if not pipe.synchronize():
+                    raise RuntimeError(pipe.last_error())
+                pms.append(ev0.elapsed_time(ev1))
+            tot["plain_ms"] += statistics.median(pms)
+            for r in range(len(b["plan"])):
+                ndms, total, _ = B.range_shape(j, r)
+                a = B.output(j, r).view(torch.int32)
+                p = dev_rows(aa, pipe.device_output(r), (ndms, total)).view(torch.int32)
+                n_cmp += 1
+                if not torch.equal(a, p):
+                    bit_exact = False
+                    mismatches.append([i, r])
+            pipe.cleanUp()
+            pipe.delete()
+            tot["units"] += units_b[i]
+        B.delete()
+        del xs
+        torch.cuda.synchronize(device)
+        torch.cuda.empty_cache()
     for p in plans:
         p.delete()
-    batched_s = tot["batched_ms"] / 1e3
-    plain_s = tot["plain_ms"] / 1e3
+    obs_s = sum(b["nsamp"] * b["tsamp"] for b in beams)
+    return {"units": tot["units"], "batched_s": tot["batched_ms"] / 1e3, "plain_s": tot["plain_ms"] / 1e3,
+            "obs_s": obs_s, "waves": wave_info, "launches": tot["launches"], "work_items": tot["items"],
+            "setup_s": tot["setup_s"], "plain_fresh_s": tot["plain_fresh_s"], "bit_exact": bit_exact,
+            "compared_ranges": n_cmp, "mismatches": mismatches[:10],
+            "nbits_count": {n: sum(1 for b in beams if b["nbits"] == n) for n in (4, 8, 16)}}
+
+
+def run_batched(args, rank, world, local):
+    """Multi-beam workload: the seeded 48-beam draw (aa_b200.workloads), run
+    as batches and beam by beam (measure_multibeam)."""
+    import torch
+    import torch.distributed as dist
+    import aa_b200 as aa
+    from aa_b200 import workloads as WL
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    beams = WL.multibeam_draw(seed=3 + 1000 * rank, nbeams=args.beams)
+    stream = torch.cuda.Stream(device)
+    stream.wait_stream(torch.cuda.current_stream(device))
+    with ClockSampler(local) as clk:
+        m = measure_multibeam(aa, WL, beams, args.steps, args.warmup, device, stream)
+    batched_s, plain_s = m["batched_s"], m["plain_s"]
     if world > 1:
         t = torch.tensor([batched_s, plain_s], device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         batched_s, plain_s = float(t[0]), float(t[1])
-    value = tot["units"] * world / batched_s
-    obs_s = sum(b["nsamp"] * b["tsamp"] for b in beams)
-    nbits_count = {n: sum(1 for b in beams if b["nbits"] == n) for n in (4, 8, 16)}
+    value = m["units"] * world / batched_s
     if rank == 0:
         line = {
             "metric": "DM-trial*samples/s (batched multi-beam DDTR, bit-exact vs plain per-beam launch)",
@@ -369,27 +602,26 @@ def run_batched(args, rank, world, local):
             "scaling": "weak", "vs_baseline": None, "dtype": "u8+u16", "data": "synthetic",
             "config": {"workload": f"multi-beam DDTR: {len(beams)} beams, 2048-4096 ch, 4/8/16-bit, 2^16-2^21 "
                                    f"samples, 2-6-range prefixes of the survey plan cut at DM 500-3000",
-                       "beams": len(beams), "nbits_count": nbits_count, "seed": 3,
-                       "strategy_free_memory": MULTIBEAM_FREE_MEMORY, "waves": len(waves),
+                       "beams": len(beams), "nbits_count": m["nbits_count"], "seed": 3,
+                       "strategy_free_memory": MULTIBEAM_FREE_MEMORY, "waves": len(m["waves"]),
                        "l2_policy": "inputs larger than L2", "parallelism": "beams per GPU, batched"},
-            "realtime_x": obs_s / batched_s,
-            "plain": {"value": tot["units"] * world / plain_s, "ms_per_step": plain_s * 1e3,
-                      "realtime_x": obs_s / plain_s,
-                      "fresh_pipeline_s": tot["plain_fresh_s"],
+            "realtime_x": m["obs_s"] / batched_s,
+            "plain": {"value": m["units"] * world / plain_s, "ms_per_step": plain_s * 1e3,
+                      "realtime_x": m["obs_s"] / plain_s,
+                      "fresh_pipeline_s": m["plain_fresh_s"],
                       "note": "beam by beam through the plain pipeline (device input/output), set-up excluded; "
                               "fresh_pipeline_s = wall time of create+bind+first run per beam, summed"},
             "batched_over_plain": plain_s / batched_s,
-            "bit_exact": bit_exact, "compared_ranges": n_cmp, "mismatches": mismatches[:10],
-            "batched": {"setup_s": tot["setup_s"], "work_items": tot["items"],
-                        "waves": wave_info},
-            "gpu_launches": tot["launches"] * args.steps,
+            "bit_exact": m["bit_exact"], "compared_ranges": m["compared_ranges"], "mismatches": m["mismatches"],
+            "batched": {"setup_s": m["setup_s"], "work_items": m["work_items"], "waves": m["waves"]},
+            "gpu_launches": m["launches"] * args.steps,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
-    return 0 if bit_exact else 1
+    return 0 if m["bit_exact"] else 1
 
 
 def _search_and_refine(aa, SR, R, x, kc, outputs, strat, k=64, steps=50):
@@ -920,6 +1152,14 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference" and args.config not in ("survey", "mid", "small"):
+        # only the plain DDTR configurations have a reference arm; print no
+        # line that would stand for one
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "config": args.config,
+                              "unavailable": f"no reference arm for --config {args.config}: the reference arm times "
+                                             "the plain DDTR path (survey, mid, small)"}), flush=True)
+        return 0
     if args.config == "batched" and args.impl != "reference":
         return run_batched(args, rank, world, local)
     if args.config == "refine" and args.impl != "reference":
@@ -958,6 +1198,9 @@ def main():
     stream = torch.cuda.Stream(device)
     stream.wait_stream(torch.cuda.current_stream(device))
     md = metadata_struct(aa, cfg)
+
+    # ---------------- measured shared-memory roof of this GPU ----------------
+    smem = aa.smem_load_rate(8192, stream.cuda_stream)
 
     # ---------------- device-resident value ----------------
     pipe = aa.create_pipeline(md, x.data_ptr(), device_input=True, device_output=True, copy_to_host=False,
@@ -999,6 +1242,27 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_step = float(t.item())
     value = units * world / (ms_step / 1e3)
+
+    # ---------------- parity of the timed output (the oracle as checker) ----------------
+    parity = None
+    if rank == 0 and not args.no_parity:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        ost = O.strategy(cfg["plan"], cfg["nchans"], cfg["nsamp"], cfg["fch1"], cfg["foff"], cfg["tsamp"],
+                         cfg["nbits"])
+        same_strategy = (ost.ndms == list(strat["ndms"]) and ost.maxshift == strat["maxshift"] and
+                         ost.t_processed == [list(v) for v in strat["t_processed"]])
+
+        def host_rows(a, b):
+            return x[a:b].cpu().numpy().view(np.uint16)
+
+        def device_rows(r, dm0, ndm, col0, ncol):
+            nd, tot = strat["ndms"][r], sum(strat["t_processed"][r])
+            rows = dev_rows(aa, pipe.device_output(r), (nd, tot))
+            return rows[dm0:dm0 + ndm, col0:col0 + ncol].cpu().numpy()
+
+        parity = parity_checks(cfg, ost, host_rows, device_rows)
+        parity["strategy_identical_to_oracle"] = same_strategy
     pipe.cleanUp()
     pipe.delete()
 
@@ -1009,111 +1273,49 @@ def main():
         xh.copy_(x)
         del x
         torch.cuda.empty_cache()
-        comps = aa.aa_py_pipeline_components(True, False, False, False)
-        opts = aa.aa_py_pipeline_component_options()
-        opts.copy_ddtr_data_to_host = True
-        api = aa.aa_py_pipeline(comps, opts, md, ctypes_ushort_ptr(xh), local)
-        if not api.bind_ddtr_plan(plan):
-            raise RuntimeError(api.last_error())
-        walls = []
-        for step in range(1 + args.e2e_steps):
-            torch.cuda.synchronize(device)
-            barrier()
-            t0 = time.perf_counter()
-            api.rewind()
-            while api.run():
-                pass
-            if api.status_code() == aa.STATUS_ERROR:
-                raise RuntimeError(api.last_error())
-            torch.cuda.synchronize(device)
-            walls.append(time.perf_counter() - t0)
-        wall = statistics.median(walls[1:])  # the first run also allocates
-        if world > 1:
-            t = torch.tensor([wall], device=device)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wall = float(t.item())
-        h2d = sum((strat["t_processed"][0][k] + strat["maxshift"]) * cfg["nchans"] * 2
-                  for k in range(strat["num_tchunks"]))
-        e2e = {"value": units * world / wall, "unit": "DM-trial*samples/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": units * 4, "ms_per_step": wall * 1e3,
-               "realtime_x": sum(strat["t_processed"][0]) * cfg["tsamp"] / wall}
+        e2e = measure_e2e(aa, cfg, md, plan, xh, strat, units, args.e2e_steps, local, device, barrier, world)
         x_host = xh.numpy().view(np.uint16)
-        api.cleanUp()
-        api.delete()
         if args.with_analysis:
-            # the same run with the analysis component (single-pulse detection
-            # of every step's rows and its candidate files), as the reference
-            # runner does it
-            import tempfile
-            a = ANALYSIS
-            comps_a = aa.aa_py_pipeline_components(True, True, False, False)
-            api = aa.aa_py_pipeline(comps_a, opts, md, ctypes_ushort_ptr(xh), local)
-            if not api.bind_ddtr_plan(plan):
-                raise RuntimeError(api.last_error())
-            if not api.bind_analysis_plan(aa.aa_py_analysis_plan(a["sigma_cutoff"], a["sigma_constant"],
-                                                                 a["max_width_s"], a["algorithm"],
-                                                                 bool(a["baseline_noise"]))):
-                raise RuntimeError(api.last_error())
-            api.set_candidate_output(True, tempfile.mkdtemp(prefix="spd_cands_"))
-            walls, ncand = [], 0
-            for step in range(1 + args.e2e_steps):
-                torch.cuda.synchronize(device)
-                t0 = time.perf_counter()
-                api.rewind()
-                ncand = 0
-                while api.run():
-                    if api.status_code() == aa.STATUS_HAS_MORE:
-                        ncand += lib_spd_count(aa, api)
-                if api.status_code() == aa.STATUS_ERROR:
-                    raise RuntimeError(api.last_error())
-                torch.cuda.synchronize(device)
-                walls.append(time.perf_counter() - t0)
-            wall = statistics.median(walls[1:])
-            e2e["with_analysis"] = {"value": units * world / wall, "unit": "DM-trial*samples/s",
-                                    "ms_per_step": wall * 1e3, "candidates": ncand, "settings": a}
-            api.cleanUp()
-            api.delete()
+            e2e["with_analysis"] = measure_e2e_analysis(aa, md, plan, xh, units, args.e2e_steps, local, device, world)
         # the same run fed the samples as a SIGPROC file stores them
         # (aa_b200_pipeline_set_packed_input): nbits/16 of the H2D bytes
         if cfg["nbits"] <= 8:
-            from aa_b200.sigproc import pack
-            if cfg["nbits"] == 8:
-                xp = torch.empty((xh.shape[0], xh.shape[1]), dtype=torch.uint8, pin_memory=True)
-                xp.copy_(xh.to(torch.uint8))
-            else:
-                xp = torch.from_numpy(pack(x_host, cfg["nbits"])).pin_memory()
-            api = aa.aa_py_pipeline(comps, opts, md, None, local)
-            api.set_packed_input(xp.data_ptr())
-            if not api.bind_ddtr_plan(plan):
-                raise RuntimeError(api.last_error())
-            walls = []
-            for step in range(1 + args.e2e_steps):
-                torch.cuda.synchronize(device)
-                barrier()
-                t0 = time.perf_counter()
-                api.rewind()
-                while api.run():
-                    pass
-                if api.status_code() == aa.STATUS_ERROR:
-                    raise RuntimeError(api.last_error())
-                torch.cuda.synchronize(device)
-                walls.append(time.perf_counter() - t0)
-            wall = statistics.median(walls[1:])
-            if world > 1:
-                t = torch.tensor([wall], device=device)
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-                wall = float(t.item())
-            e2e["packed_input"] = {
-                "value": units * world / wall, "unit": "DM-trial*samples/s", "ms_per_step": wall * 1e3,
-                "h2d_bytes_per_step": sum((strat["t_processed"][0][k] + strat["maxshift"]) * cfg["nchans"] *
-                                          cfg["nbits"] // 8 for k in range(strat["num_tchunks"])),
-                "d2h_bytes_per_step": units * 4, "api": "aa_b200_pipeline_set_packed_input"}
-            api.cleanUp()
-            api.delete()
-            del xp
+            e2e["packed_input"] = measure_e2e_packed(aa, cfg, md, plan, xh, x_host, strat, units, args.e2e_steps,
+                                                     local, device, barrier, world)
+        del xh
     else:
         x_host = x[:min(131040, strat["t_processed"][0][0]) + strat["maxshift"]].cpu().numpy().view(np.uint16)
+        del x
     plan.delete()
+    torch.cuda.empty_cache()
+
+    # ---------------- the 2^18-sample configuration end to end ----------------
+    # (the size at which the reference's own GPU pipeline runs; its arm
+    # reports reference_gpu on the same input)
+    mid_e2e = None
+    if rank == 0 and cfg is SURVEY and not args.no_e2e:
+        mid_e2e = measure_mid_e2e(aa, local, device, args.e2e_steps)
+
+    # ---------------- batched vs plain on a reduced multi-beam draw ----------------
+    multibeam = None
+    if args.multibeam_beams > 0 and cfg is SURVEY:
+        from aa_b200 import workloads as WL
+        beams = WL.multibeam_draw(seed=3 + 1000 * rank, nbeams=48)[:args.multibeam_beams]
+        m = measure_multibeam(aa, WL, beams, 2, 1, device, stream)
+        bs, ps = m["batched_s"], m["plain_s"]
+        if world > 1:
+            t = torch.tensor([bs, ps], device=device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            bs, ps = float(t[0]), float(t[1])
+        multibeam = {
+            "workload": f"the first {len(beams)} beams of the seeded 48-beam multi-beam draw (seed 3): "
+                        f"2048-4096 ch, 4/8/16-bit ({m['nbits_count']}), 2^16-2^21 samples, 2-6-range prefixes of "
+                        f"the survey plan; input and output resident in HBM",
+            "batched": {"value": m["units"] * world / bs, "ms_per_step": bs * 1e3, "realtime_x": m["obs_s"] / bs},
+            "plain": {"value": m["units"] * world / ps, "ms_per_step": ps * 1e3, "realtime_x": m["obs_s"] / ps},
+            "batched_over_plain": ps / bs, "bit_exact": m["bit_exact"], "compared_ranges": m["compared_ranges"],
+            "mismatches": m["mismatches"], "waves": len(m["waves"]), "steps": 2, "warmup": 1,
+            "timing": "CUDA events on one stream, median of 2 runs per arm after 1 warm-up"}
 
     # ---------------- roofline of the dominant kernel ----------------
     dd_ms, dd_n = kern["dedisperse"]
@@ -1123,11 +1325,11 @@ def main():
         for k in range(strat["num_tchunks"]):
             tp = strat["t_processed"][r][k]
             ms_r = strat["maxshift"] // cfg["plan"][r][3]
-            alg_bytes += nch * (tp + ms_r) + strat["ndms"][r] * tp * 4
+            alg_bytes += nch * (tp + ms_r) * (1 if cfg["nbits"] <= 8 else 2) + strat["ndms"][r] * tp * 4
             alg_adds += strat["ndms"][r] * tp * nch
     launches_per_step = len(cfg["plan"]) * strat["num_tchunks"]
-    avg_launch_s = dd_ms / 1e3 / max(1, dd_n)
-    achieved = alg_bytes / launches_per_step / avg_launch_s / 1e9
+    dd_s_per_step = dd_ms / 1e3 / (dd_n / launches_per_step)
+    adds_rate = alg_adds / dd_s_per_step
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -1138,25 +1340,38 @@ def main():
     kernel_names = {"quad": "k_ddtr_quad", "phase": "k_ddtr_u8", "f32": "k_ddtr_f32", "gather": "k_ddtr_u16",
                     "sub": "k_ddtr_sub", "quadws": "k_ddtr_quadws"}
     used = sorted({kernel_names[ri["kernel"]] for ri in ranges})
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": None, "kernel": "+".join(used),
-                "peak_source": "MEASURED_PEAKS.json (measured)" if "hbm_gbs" in peaks else "fallback",
-                "note": "the DDTR kernel is integer/shared-memory bound, not HBM bound; see integer_rate"}
-    integer_rate = {"channel_adds_per_s": alg_adds / (dd_ms / 1e3 / (dd_n / launches_per_step)),
-                    "kernel_share_of_step": dd_ms / max(1e-9, ms_total)}
+    hbm_achieved = alg_bytes / dd_s_per_step / 1e9
+    roofline = {
+        "bound": "shared-memory", "kernel": "+".join(used), "unit": "adds/s",
+        "achieved": adds_rate, "peak": smem["adds_per_s"], "frac": adds_rate / smem["adds_per_s"],
+        "traffic": TRAFFIC_PER_ALG_BYTE * alg_bytes / launches_per_step,
+        "algorithmic": {"adds_per_launch": alg_adds / launches_per_step,
+                        "bytes_per_launch": alg_bytes / launches_per_step,
+                        "per_unit": f"{nch} channel adds and, per step, the packed input once per (chunk, range) "
+                                    f"plus 4 B per output"},
+        "peak_source": f"measured on this GPU by aa_b200_smem_load_rate: {smem['loads_per_s']:.4g} 32-bit shared "
+                       f"loads/s x 4 adds per load (the channel-quad kernel's bound)",
+        "traffic_source": TRAFFIC_SOURCE,
+        "hbm": {"achieved": hbm_achieved, "peak": hbm, "unit": "GB/s", "frac": hbm_achieved / hbm,
+                "peak_source": "MEASURED_PEAKS.json (measured)" if "hbm_gbs" in peaks else "fallback"},
+    }
 
     result = None
     if rank == 0:
-        cb_value, cb_threads, cb_desc = cpu_baseline(cfg, x_host, strat, args.cpu_seconds) if world == 1 else (
+        cb_value, cb_threads, cb_desc = cpu_baseline(cfg, x_host, args.cpu_seconds) if world == 1 else (
             None, None, None)
         result = {
-            "metric": METRIC, "value": value, "unit": "DM-trial*samples/s", "n_gpus": world, "steps": args.steps,
+            "metric": METRIC if parity is not None else METRIC_UNCHECKED, "value": value,
+            "unit": "DM-trial*samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u8" if cfg["nbits"] <= 8 else "f32", "data": "synthetic", "config": workload_config(cfg),
+            "vs_baseline": None, "dtype": "u8" if cfg["nbits"] <= 8 else "f32", "data": "synthetic",
+            "config": workload_config(cfg),
             "realtime_x": sum(strat["t_processed"][0]) * cfg["tsamp"] / (ms_step / 1e3),
             "published_realtime_x": PUBLISHED_REALTIME,
-            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "integer_rate": integer_rate,
+            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "parity": parity,
+            "batched_vs_plain": multibeam, "mid_e2e": mid_e2e,
             "kernels_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()},
+            "kernel_share_of_step": dd_ms / max(1e-9, ms_total),
             "kernel_launches_per_step": {k: v[1] / args.steps for k, v in kern.items()},
             "ranges": ranges, "pulses": len(pulses), "clocks": clk.summary(),
             "cpu_baseline": None if cb_value is None else {"value": cb_value, "unit": "DM-trial*samples/s",
@@ -1165,7 +1380,151 @@ def main():
         print(json.dumps(result), flush=True)
     if world > 1:
         dist.destroy_process_group()
-    return 0
+    ok = parity is None or parity["mismatching"] == 0
+    return 0 if ok else 1
+
+
+def measure_e2e(aa, cfg, md, plan, xh, strat, units, e2e_steps, local, device, barrier, world):
+    """The metric through aa_py_pipeline_api / run loop from the pinned host
+    [t][c] input to the pinned host float*** rows (copies inside the timed
+    region; wall clock between device synchronisations; the first run, which
+    also allocates, is not counted)."""
+    import torch
+    import torch.distributed as dist
+    comps = aa.aa_py_pipeline_components(True, False, False, False)
+    opts = aa.aa_py_pipeline_component_options()
+    opts.copy_ddtr_data_to_host = True
+    api = aa.aa_py_pipeline(comps, opts, md, ctypes_ushort_ptr(xh), local)
+    if not api.bind_ddtr_plan(plan):
+        raise RuntimeError(api.last_error())
+    walls = []
+    for step in range(1 + e2e_steps):
+        torch.cuda.synchronize(device)
+        barrier()
+        t0 = time.perf_counter()
+        api.rewind()
+        while api.run():
+            pass
+        if api.status_code() == aa.STATUS_ERROR:
+            raise RuntimeError(api.last_error())
+        torch.cuda.synchronize(device)
+        walls.append(time.perf_counter() - t0)
+    wall = statistics.median(walls[1:])
+    if world > 1:
+        t = torch.tensor([wall], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        wall = float(t.item())
+    h2d = sum((strat["t_processed"][0][k] + strat["maxshift"]) * cfg["nchans"] * 2
+              for k in range(strat["num_tchunks"]))
+    api.cleanUp()
+    api.delete()
+    return {"value": units * world / wall, "unit": "DM-trial*samples/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": units * 4, "ms_per_step": wall * 1e3,
+            "realtime_x": sum(strat["t_processed"][0]) * cfg["tsamp"] / wall}
+
+
+def measure_e2e_analysis(aa, md, plan, xh, units, e2e_steps, local, device, world):
+    """The e2e run with the analysis component (single-pulse detection of
+    every step's rows and its candidate files), as the reference runner does
+    it."""
+    import tempfile
+    import torch
+    a = ANALYSIS
+    comps_a = aa.aa_py_pipeline_components(True, True, False, False)
+    opts = aa.aa_py_pipeline_component_options()
+    opts.copy_ddtr_data_to_host = True
+    api = aa.aa_py_pipeline(comps_a, opts, md, ctypes_ushort_ptr(xh), local)
+    if not api.bind_ddtr_plan(plan):
+        raise RuntimeError(api.last_error())
+    if not api.bind_analysis_plan(aa.aa_py_analysis_plan(a["sigma_cutoff"], a["sigma_constant"], a["max_width_s"],
+                                                         a["algorithm"], bool(a["baseline_noise"]))):
+        raise RuntimeError(api.last_error())
+    api.set_candidate_output(True, tempfile.mkdtemp(prefix="spd_cands_"))
+    walls, ncand = [], 0
+    for step in range(1 + e2e_steps):
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        api.rewind()
+        ncand = 0
+        while api.run():
+            if api.status_code() == aa.STATUS_HAS_MORE:
+                ncand += lib_spd_count(aa, api)
+        if api.status_code() == aa.STATUS_ERROR:
+            raise RuntimeError(api.last_error())
+        torch.cuda.synchronize(device)
+        walls.append(time.perf_counter() - t0)
+    wall = statistics.median(walls[1:])
+    api.cleanUp()
+    api.delete()
+    return {"value": units * world / wall, "unit": "DM-trial*samples/s", "ms_per_step": wall * 1e3,
+            "candidates": ncand, "settings": a}
+
+
+def measure_e2e_packed(aa, cfg, md, plan, xh, x_host, strat, units, e2e_steps, local, device, barrier, world):
+    """The e2e run fed the samples as a SIGPROC file stores them
+    (aa_b200_pipeline_set_packed_input): nbits/16 of the H2D bytes."""
+    import torch
+    import torch.distributed as dist
+    from aa_b200.sigproc import pack
+    if cfg["nbits"] == 8:
+        xp = torch.empty((xh.shape[0], xh.shape[1]), dtype=torch.uint8, pin_memory=True)
+        xp.copy_(xh.to(torch.uint8))
+    else:
+        xp = torch.from_numpy(pack(x_host, cfg["nbits"])).pin_memory()
+    comps = aa.aa_py_pipeline_components(True, False, False, False)
+    opts = aa.aa_py_pipeline_component_options()
+    opts.copy_ddtr_data_to_host = True
+    api = aa.aa_py_pipeline(comps, opts, md, None, local)
+    api.set_packed_input(xp.data_ptr())
+    if not api.bind_ddtr_plan(plan):
+        raise RuntimeError(api.last_error())
+    walls = []
+    for step in range(1 + e2e_steps):
+        torch.cuda.synchronize(device)
+        barrier()
+        t0 = time.perf_counter()
+        api.rewind()
+        while api.run():
+            pass
+        if api.status_code() == aa.STATUS_ERROR:
+            raise RuntimeError(api.last_error())
+        torch.cuda.synchronize(device)
+        walls.append(time.perf_counter() - t0)
+    wall = statistics.median(walls[1:])
+    if world > 1:
+        t = torch.tensor([wall], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        wall = float(t.item())
+    api.cleanUp()
+    api.delete()
+    del xp
+    return {"value": units * world / wall, "unit": "DM-trial*samples/s", "ms_per_step": wall * 1e3,
+            "h2d_bytes_per_step": sum((strat["t_processed"][0][k] + strat["maxshift"]) * cfg["nchans"] *
+                                      cfg["nbits"] // 8 for k in range(strat["num_tchunks"])),
+            "d2h_bytes_per_step": units * 4, "api": "aa_b200_pipeline_set_packed_input"}
+
+
+def measure_mid_e2e(aa, local, device, e2e_steps):
+    """The 2^18-sample configuration (bench's MID: the survey plan, 4096
+    channels) end to end through the C ABI, on the input the reference arm's
+    reference_gpu figure uses (the same generator and seed)."""
+    import torch
+    cfg = MID
+    x, _ = synth_input_device(cfg, cfg["seed"], device)
+    xh = torch.empty(x.shape, dtype=torch.int16, pin_memory=True)
+    xh.copy_(x)
+    del x
+    torch.cuda.empty_cache()
+    md = metadata_struct(aa, cfg)
+    plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in cfg["plan"]])
+    strat = aa.strategy(cfg["plan"], cfg["nchans"], cfg["nsamp"], cfg["fch1"], cfg["foff"], cfg["tsamp"],
+                        cfg["nbits"])
+    units = units_per_step(strat)
+    r = measure_e2e(aa, cfg, md, plan, xh, strat, units, max(3, e2e_steps), local, device, lambda: None, 1)
+    plan.delete()
+    r["workload"] = (f"{cfg['nchans']} ch x {cfg['nsamp']} samples, {cfg['nbits']}-bit, {len(cfg['plan'])}-range "
+                     f"survey plan, host [t][c] input, rows copied to the host")
+    return r
 
 
 def lib_spd_count(aa, api) -> int:

@@ -238,11 +238,16 @@ int aa_b200_dedisperse(int i, int t_processed, const int *inBin, const float *dm
  * image, which every GPU that loads the library holds until the process
  * exits.  Limits: nchans <= AA_B200_NOALLOC_MAX_CHANS and
  * nchans * ndms[i] <= AA_B200_NOALLOC_MAX_ENTRIES; larger calls are refused
- * (return 1, message in aa_b200_noalloc_last_error).  The first call on each
- * device looks up the array's device address (cudaGetSymbolAddress), so make
- * that first call before any stream capture.  All calls share the array:
- * calls that overlap on the GPU (other threads, other streams) race and must
- * be serialised by the caller.  Each call clears what must start at zero. */
+ * (return 1, message in aa_b200_noalloc_last_error).  It runs the generic
+ * one-byte kernel (k_ddtr_u8) or the two-byte gather kernel (k_ddtr_u16), not
+ * the faster channel-quad kernel, whose pattern tables would not fit the
+ * array.  Each call waits on `stream` (cudaStreamSynchronize) to read the
+ * device's error flags back, so it blocks the calling thread until its work
+ * is done.  The first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * threads, other streams) race and must be serialised by the caller.  Each
+ * call clears what must start at zero. */
 #define AA_B200_NOALLOC_SCRATCH_BYTES (16u << 20)
 #define AA_B200_NOALLOC_MAX_CHANS 16384
 #define AA_B200_NOALLOC_MAX_ENTRIES (1u << 20)
@@ -269,11 +274,26 @@ const char *aa_b200_version(void);
  * device error flags (8 = the wait ran out, as the staged kernels report an
  * overdue copy).  Returns 0 when the kernel ran and the flags were read. */
 int aa_b200_selftest_bounded_wait(int limit, int *status);
+/* The compute capability the library's device code was compiled for, as the
+ * CUDA runtime reports it for one of its kernels (major*10 + minor; 100 for
+ * the sm_100a build).  Needs a GPU.  Returns 0 on success. */
+int aa_b200_binary_version(int *version);
 /* Host-side failure injection: the n-th CUDA result checked by any pipeline
  * or batch engine after this call reads as a failure ("injected failure" in
  * the error message); n <= 0 disarms.  For tests of the error paths. */
 void aa_b200_debug_fail_after(long long n);
 long long aa_b200_debug_fail_countdown(void);
+
+/* ---------------------------------------------------------------------------
+ * Measured roof (no reference counterpart): 32-bit shared-memory loads per
+ * second over the whole GPU, from conflict-free warp-wide loads (two
+ * 1024-thread CTAs per SM, iters x 16 loads per thread), timed with CUDA
+ * events on `stream` (a cudaStream_t, NULL = legacy default stream).  The
+ * channel-quad dedispersion kernel adds four channel samples per such load,
+ * so 4 x *loads_per_s is its shared-memory bound in adds/s.  Returns 0 on
+ * success; *ms_out (may be NULL) receives the timed kernel's duration.
+ * ------------------------------------------------------------------------- */
+int aa_b200_smem_load_rate(int iters, void *stream, double *loads_per_s, float *ms_out);
 
 /* ---------------------------------------------------------------------------
  * SIGPROC filterbank input (src/aa_py_sigproc_input.cpp:7-33, reader

@@ -358,36 +358,52 @@ int aao_dedisperse(int kernel, int fma_mode, const uint16_t *in, size_t in_len,
                    const float *dmshifts, float mstartdm, float mdmstep,
                    int bin, float *out, double *sums)
 {
-    int dm;
+    return aao_dedisperse_window(kernel, fma_mode, in, in_len, i_nsamp, nchans, 0, ndms, 0,
+                                 t_processed, 0, dmshifts, mstartdm, mdmstep, bin, out, sums);
+}
+
+/* The same kernels for DM trials dm_first .. dm_first+ndm-1 of the range
+ * (delays from the absolute trial index, so the block decomposition of
+ * :196-197 is kept) and outputs t_first .. t_first+nt-1; output t reads
+ * in[c*i_nsamp + t - t_shift + delay], so a caller may pass a buffer that
+ * starts t_shift samples into the channel rows.  out/sums are [ndm][nt]. */
+int aao_dedisperse_window(int kernel, int fma_mode, const uint16_t *in, size_t in_len,
+                          int i_nsamp, int nchans, int dm_first, int ndm, long long t_first,
+                          int nt, long long t_shift, const float *dmshifts, float mstartdm,
+                          float mdmstep, int bin, float *out, double *sums)
+{
+    int j;
     int err = 0;
     /* 4-bit wide-band kernel drops the channels beyond 4096*floor(nchans/4096)
      * (call wrapper :520 uses integer division inside ceil). */
     int nch_used = nchans;
     if (kernel == AAO_K_SHARED4 && nchans > 4096)
         nch_used = 4096 * (nchans / 4096);
-    if (t_processed <= 0 || ndms <= 0)
+    if (nt <= 0 || ndm <= 0)
         return 0;
 
 #pragma omp parallel for schedule(dynamic, 1) reduction(| : err)
-    for (dm = 0; dm < ndms; dm++) {
+    for (j = 0; j < ndm; j++) {
         int t, c, k;
+        const int dm = dm_first + j;
         int *dl = (int *)malloc(sizeof(int) * 8 * (size_t)nchans);
         int64_t *isum = NULL;
         float *fsum = NULL;
         int integer = (kernel == AAO_K_SHARED8 || kernel == AAO_K_SHARED4);
         if (integer)
-            isum = (int64_t *)calloc((size_t)t_processed, sizeof(int64_t));
+            isum = (int64_t *)calloc((size_t)nt, sizeof(int64_t));
         else
-            fsum = (float *)calloc((size_t)t_processed, sizeof(float));
+            fsum = (float *)calloc((size_t)nt, sizeof(float));
         for (c = 0; c < nchans; c++)
             for (k = 0; k < 8; k++)
                 dl[c * 8 + k] = aao_delay(kernel, fma_mode, dmshifts[c], dm, k, mstartdm, mdmstep);
         for (c = 0; c < nch_used; c++) {
-            const size_t row = (size_t)c * (size_t)i_nsamp;
+            const long long row = (long long)c * (long long)i_nsamp - t_shift;
             const int *d = dl + c * 8;
-            for (t = 0; t < t_processed; t++) {
-                int delay = (kernel == AAO_K_CACHE) ? d[0] : d[class_of(kernel, t)];
-                long long idx = (long long)row + t + delay;
+            for (t = 0; t < nt; t++) {
+                const long long ta = t_first + t;
+                int delay = (kernel == AAO_K_CACHE) ? d[0] : d[class_of(kernel, (int)(ta & 31))];
+                long long idx = row + ta + delay;
                 unsigned v;
                 if (idx < 0 || (size_t)idx >= in_len) {
                     err |= 1;
@@ -402,9 +418,9 @@ int aao_dedisperse(int kernel, int fma_mode, const uint16_t *in, size_t in_len,
                     fsum[t] = fsum[t] + (float)v;
             }
         }
-        for (t = 0; t < t_processed; t++) {
+        for (t = 0; t < nt; t++) {
             float o;
-            size_t oi = (size_t)dm * (size_t)t_processed + t;
+            size_t oi = (size_t)j * (size_t)nt + t;
             if (integer) {
                 float s = (float)isum[t];
                 if (kernel == AAO_K_SHARED4)

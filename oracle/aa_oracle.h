@@ -70,6 +70,11 @@ int aao_dedisperse(int kernel, int fma_mode, const uint16_t *in, size_t in_len,
                    const float *dmshifts, float mstartdm, float mdmstep,
                    int bin, float *out, double *sums);
 
+int aao_dedisperse_window(int kernel, int fma_mode, const uint16_t *in, size_t in_len,
+                          int i_nsamp, int nchans, int dm_first, int ndm, long long t_first,
+                          int nt, long long t_shift, const float *dmshifts, float mstartdm,
+                          float mdmstep, int bin, float *out, double *sums);
+
 void aao_corner_turn(const uint16_t *in_tc, uint16_t *out_ct, int nchans, int nsamp);
 
 int aao_bin_flat(uint16_t *buf, size_t buf_len, int nchans, int nsamp);

@@ -75,6 +75,12 @@ def lib():
                                      ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_int,
                                      ctypes.c_void_p, ctypes.c_void_p]
         L.aao_dedisperse.restype = ctypes.c_int
+        L.aao_dedisperse_window.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+                                            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_longlong, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p,
+                                            ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.c_void_p]
+        L.aao_dedisperse_window.restype = ctypes.c_int
         L.aao_corner_turn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.aao_corner_turn.restype = None
         L.aao_bin_flat.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_int]
@@ -167,6 +173,23 @@ def dedisperse(kernel, fma_mode, flat: np.ndarray, i_nsamp, nchans, t_processed,
     rc = lib().aao_dedisperse(kernel, fma_mode, _ptr(flat), flat.size, i_nsamp, nchans, t_processed,
                               ndms, _ptr(dmshifts), mstartdm, mdmstep, bin_, _ptr(out),
                               _ptr(sums) if want_sums else None)
+    if rc != 0:
+        raise ValueError(f"oracle dedisperse failed (code {rc})")
+    return (out, sums) if want_sums else out
+
+
+def dedisperse_window(kernel, fma_mode, flat: np.ndarray, i_nsamp, nchans, dm_first, ndm, t_first, nt,
+                      dmshifts, mstartdm, mdmstep, bin_, t_shift=0, want_sums=False):
+    """DM trials dm_first.. and outputs t_first.. of one (chunk, range);
+    output t reads flat[c*i_nsamp + t - t_shift + delay] (a buffer that starts
+    t_shift samples into the channel rows).  Returns [ndm][nt]."""
+    flat = np.ascontiguousarray(flat, dtype=np.uint16)
+    dmshifts = np.ascontiguousarray(dmshifts, dtype=np.float32)
+    out = np.zeros((ndm, nt), np.float32)
+    sums = np.zeros((ndm, nt), np.float64) if want_sums else None
+    rc = lib().aao_dedisperse_window(kernel, fma_mode, _ptr(flat), flat.size, i_nsamp, nchans, dm_first, ndm,
+                                     t_first, nt, t_shift, _ptr(dmshifts), mstartdm, mdmstep, bin_, _ptr(out),
+                                     _ptr(sums) if want_sums else None)
     if rc != 0:
         raise ValueError(f"oracle dedisperse failed (code {rc})")
     return (out, sums) if want_sums else out

@@ -121,3 +121,33 @@ def test_oracle_matches_reference_gpu(oracle_mod, golden_ddtr, name):
                 if abs(float(ref) * div) < 2**24:  # integer sums; fp32 sums of 16-bit data above 2^24 are rounded
                     assert np.rint(float(outs[r][i, j]) * div) == np.rint(float(ref) * div)
                 assert abs(int(outs[r][i, j].view(np.int32)) - int(np.int32(bits))) <= 2
+
+
+@pytest.mark.parametrize("name", ["shared8_binned", "shared4", "cache16"])
+def test_windowed_dedispersion_equals_whole_range(oracle_mod, name):
+    """aao_dedisperse_window (the bench's in-run parity check) gives the same
+    bits as the whole-range oracle for a DM block and a time window, on the
+    whole buffer and on a buffer that starts inside the channel rows."""
+    O = oracle_mod
+    case = C.CASES[name]
+    x = C.make_input(case)
+    s = O.strategy(case["plan"], case["nchans"], case["nsamp"], case["fch1"], case["foff"], case["tsamp"],
+                   case["nbits"], C.strategy_free_memory(case))
+    d = s.dm[0]
+    tsr = np.float32(case["tsamp"]) * np.float32(d[3])
+    kind = O.select_kernel(case["nbits"], d[2], tsr, s.dmshifts[-1])
+    m0, ms = np.float32(np.float32(d[0]) / tsr), np.float32(np.float32(d[2]) / tsr)
+    tp = s.t_processed[0][0]
+    L = tp + s.maxshift
+    nch = case["nchans"]
+    full = O.dedisperse(kind, O.FMA_ALL, O.corner_turn(x[:L], nch, L), L, nch, tp, s.ndms[0], s.dmshifts, m0, ms,
+                        d[3])
+    dm0 = 64 * (s.ndms[0] // 64 - 1)
+    t0, nt = 96, tp - 96 - 64
+    w = O.dedisperse_window(kind, O.FMA_ALL, O.corner_turn(x[:L], nch, L), L, nch, dm0, 64, t0, nt, s.dmshifts, m0,
+                            ms, d[3])
+    assert np.array_equal(w.view(np.uint32), full[dm0:dm0 + 64, t0:t0 + nt].view(np.uint32))
+    sh = 64
+    w2 = O.dedisperse_window(kind, O.FMA_ALL, O.corner_turn(x[sh:L], nch, L - sh), L - sh, nch, dm0, 64, t0, nt,
+                             s.dmshifts, m0, ms, d[3], t_shift=sh)
+    assert np.array_equal(w2.view(np.uint32), full[dm0:dm0 + 64, t0:t0 + nt].view(np.uint32))

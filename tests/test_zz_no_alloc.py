@@ -7,8 +7,9 @@ reserve all device memory at start-up cannot let the library call cudaMalloc.
 The entry point keeps its delay, window and offset tables in a fixed array of
 the library's device image instead.  This test calls it through the C ABI
 twice in a row and checks both results against aa_b200_dedisperse (which
-allocates its scratch) bit for bit -- the tolerance of every other parity test
-here -- and that the second call changes nothing in the device's free memory.
+allocates its scratch) and against the CPU oracle, bit for bit -- the
+tolerance of every other parity test here -- and that the second call changes
+nothing in the device's free memory.
 The file is named to be collected last, so a run that stops at the first
 failure has run every other test before it.
 """
@@ -41,12 +42,12 @@ def _inputs(aa, name):
     args = dict(i=0, t_processed=tp, inBin=[d[3] for d in s["dm"]], dmshifts=s["dmshifts"], d_input=d_ct,
                 i_nsamp=L, d_input_elems=d_ct.numel(), out_pitch=tp, nchans=nch, tsamp=tsr,
                 dm_low=[d[0] for d in s["dm"]], dm_step=[d[2] for d in s["dm"]], ndms=s["ndms"], nbits=nbits)
-    return torch, s, tp, args
+    return torch, s, tp, args, case, x
 
 
 @pytest.mark.parametrize("name", ["shared8_binned", "fma_probe", "cache16"])
-def test_noalloc_matches_allocating_entry_point(aa, cuda_device, name):
-    torch, s, tp, args = _inputs(aa, name)
+def test_noalloc_matches_allocating_entry_point(aa, oracle_mod, cuda_device, name):
+    torch, s, tp, args, case, x = _inputs(aa, name)
     n = s["ndms"][0] * tp
     ref = torch.zeros(n, dtype=torch.float32, device="cuda")
     aa.dedisperse(d_output=ref, **args)
@@ -63,6 +64,17 @@ def test_noalloc_matches_allocating_entry_point(aa, cuda_device, name):
     want = ref.cpu().numpy()
     for got in outs:
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    # and directly against the oracle: range 0 of chunk 0 on the corner-turned input
+    O = oracle_mod
+    L = args["i_nsamp"]
+    d = s["dm"][0]
+    tsr = np.float32(case["tsamp"]) * np.float32(d[3])
+    kind = O.select_kernel(case["nbits"], d[2], tsr, s["dmshifts"][-1])
+    flat = O.corner_turn(x[:L], case["nchans"], L)
+    m0, ms = np.float32(np.float32(d[0]) / tsr), np.float32(np.float32(d[2]) / tsr)
+    oracle_out = O.dedisperse(kind, O.FMA_ALL, flat, L, case["nchans"], tp, s["ndms"][0], s["dmshifts"], m0, ms, d[3])
+    for got in outs:
+        assert np.array_equal(got.view(np.uint32), oracle_out.reshape(-1).view(np.uint32))
 
 
 def test_noalloc_refuses_sizes_beyond_its_scratch(aa, cuda_device):
