@@ -538,7 +538,8 @@ class aa_py_pipeline:
     def set_kernel_variant(self, variant: int):
         """Kernel family per range (before bind): 0 auto (timed per range), 1
         generic kernels, 2 channel-quad / fp32, 3 subband / fp32, 4
-        warp-specialised channel-quad / fp32."""
+        warp-specialised channel-quad / fp32, 5 split-phase channel-quad /
+        fp32."""
         if not lib().aa_b200_pipeline_set_kernel_variant(self.m_obj, variant):
             raise ValueError(self.last_error())
         return True
@@ -570,7 +571,8 @@ class aa_py_pipeline:
                                               ctypes.byref(t)):
             raise RuntimeError(self.last_error())
         return {"kind": KIND_NAMES[k.value & 0xFF], "kernel": ("quad" if k.value & 0x100 else "f32" if k.value & 0x200 else
-                           "gather" if k.value & 0x400 else "sub" if k.value & 0x800 else "quadws" if k.value & 0x1000 else "phase"),
+                           "gather" if k.value & 0x400 else "sub" if k.value & 0x800 else "quadws" if k.value & 0x1000
+                           else "quadsp" if k.value & 0x2000 else "phase"),
                 "stage_depth": lib().aa_b200_pipeline_stage_depth(self.m_obj, r),
                 "group_dms": g.value, "span": s.value, "tile_words": t.value}
 

@@ -8,7 +8,7 @@ namespace aab200 {
 
 bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache &cache, std::string &err)
 {
-    const bool quad = (job.variant == 2 || job.variant == 5);
+    const bool quad = (job.variant == 2 || job.variant == 5 || job.variant == 6);
     const auto key = std::make_tuple(job.variant, job.p.nch_used, quad ? job.q.W : job.f.W,
                                      quad ? job.q.raww : job.f.rawh, quad ? job.q.npool / std::max(1, job.q.qs) : 0,
                                      job.p.kind, static_cast<long long>(job.groups));
@@ -40,6 +40,12 @@ bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache 
                 t.q.npool = c * maxcnt;
                 if (job.variant == 5) {
                     bytes = quadws_smem_bytes(t.q);
+                } else if (job.variant == 6) {
+                    BatchJobDev d{};
+                    d.p = t.p;
+                    d.q = t.q;
+                    d.variant = 6;
+                    bytes = std::max(quadsp_smem_bytes(t.q), persistent_job_smem(d));
                 } else {
                     BatchJobDev d{};
                     d.p = t.p;

@@ -149,8 +149,8 @@ bool BatchDdtr::build_jobs()
             if (!P.make_job(op, b.level_ptr[op.chunk][op.src_level], b.level_elems[op.chunk][op.src_level], out,
                             P.strategy().total_samps(op.range), job))
                 return fail("beam " + std::to_string(bi) + ": " + P.last_error());
-            const bool stageable =
-                (job.variant == 2 && job.q.M == 16) || (job.variant == 3 && job.tile_samples == 512);
+            const bool quadlike = (job.variant == 2 || job.variant == 6);
+            const bool stageable = (quadlike && job.q.M == 16) || (job.variant == 3 && job.tile_samples == 512);
             if (!stageable || !opt_.persistent) {
                 if (stageable && opt_.autotune && !tune_job(job))
                     return false;
@@ -172,7 +172,7 @@ bool BatchDdtr::build_jobs()
                     d.variant = job.variant;
                     const int maxcnt = std::max(1, job.q.npool / std::max(1, job.q.qs));
                     while (persistent_job_smem(d) > 227 * 1024) {
-                        if (job.variant == 2 && d.q.qs > 1) {
+                        if (quadlike && d.q.qs > 1) {
                             d.q.qs /= 2;
                             d.q.npool = d.q.qs * maxcnt;
                         } else if (job.variant == 3 && d.f.cs > 4) {
@@ -184,9 +184,9 @@ bool BatchDdtr::build_jobs()
                     job.q = d.q;
                     job.f = d.f;
                 }
-                tuned[key] = std::make_pair(job.variant == 2 ? job.q.qs : job.f.cs, job.q.npool);
+                tuned[key] = std::make_pair(quadlike ? job.q.qs : job.f.cs, job.q.npool);
             } else {
-                if (job.variant == 2) {
+                if (quadlike) {
                     job.q.qs = it->second.first;
                     job.q.npool = it->second.second;
                 } else {

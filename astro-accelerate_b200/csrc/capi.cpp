@@ -777,9 +777,10 @@ bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant)
     Api *a = as_api(obj);
     if (a->pipe)
         return api_fail(a, "the kernel variant must be set before the plan is bound");
-    if (variant < 0 || variant > 4)
+    if (variant < 0 || variant > 5)
         return api_fail(a, "kernel variant must be 0 (auto), 1 (generic kernels), 2 (channel-quad / fp32 kernels), "
-                           "3 (subband / fp32 kernels) or 4 (warp-specialised channel-quad / fp32 kernels)");
+                           "3 (subband / fp32 kernels), 4 (warp-specialised channel-quad / fp32 kernels) or 5 "
+                           "(split-phase channel-quad / fp32 kernels)");
     a->popt.kernel_variant = variant;
     return true;
 }
@@ -890,6 +891,10 @@ int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms,
         *tile_words = 4;
     } else if (rc.variant == 5) {
         *kind |= 0x1000;
+        *span = rc.quad_span;
+        *tile_words = rc.quad.M / 4;
+    } else if (rc.variant == 6) {
+        *kind |= 0x2000;
         *span = rc.quad_span;
         *tile_words = rc.quad.M / 4;
     } else if (rc.variant == 4) {

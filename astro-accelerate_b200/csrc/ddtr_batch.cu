@@ -11,8 +11,9 @@
 // output is bit-identical to its plain run.
 //
 // Shared memory: [mbarriers][job descriptor][body area], the body area sized
-// for the largest job.  The mbarriers are initialised once; a running stage
-// counter carries their phases from item to item.
+// for the largest job.  The mbarriers are initialised once; running stage
+// counters carry their phases from item to item (one for the TMA rings of
+// the quad and fp32 bodies, one for the split-phase quad body's barriers).
 #include "ddtr_bodies.cuh"
 
 namespace aab200 {
@@ -40,7 +41,8 @@ __global__ void __launch_bounds__(body::NTHREADS, 1)
     const BatchJobDev &jd = *reinterpret_cast<const BatchJobDev *>(jd_words);
     uint32_t *area = sm + body::BAR_WORDS + JD_WORDS;
     body::init_barriers(bar0);
-    unsigned stage_ctr = 0;
+    unsigned stage_ctr = 0; // phases of the TMA ring barriers (quad and fp32 bodies)
+    unsigned sp_ctr = 0;    // phases of the split-phase quad body's barriers
     int jcur = 0; // thread 0: job of the last item (items arrive in increasing order)
     for (;;) {
         if (tid == 0) {
@@ -65,6 +67,8 @@ __global__ void __launch_bounds__(body::NTHREADS, 1)
         bool ok;
         if (jd.variant == 2)
             ok = body::quad_body<BATCH_M, 4>(jd.p, jd.q, g, t0, area, bar0, stage_ctr);
+        else if (jd.variant == 6)
+            ok = body::quad_sp_body<BATCH_M>(jd.p, jd.q, g, t0, area, bar0, sp_ctr);
         else
             ok = body::f32_body<BATCH_M>(jd.p, jd.f, g, t0, area, bar0, stage_ctr);
         fence_proxy_async();
@@ -82,6 +86,8 @@ size_t persistent_job_smem(const BatchJobDev &j)
     size_t words;
     if (j.variant == 2)
         words = body::quad_body_words(j.q.qs, j.p.group_dms, j.q.raww, j.q.nq_pad, j.q.npool, j.q.W);
+    else if (j.variant == 6)
+        words = body::quad_sp_body_words(j.q.qs, j.q.raww, j.q.nq_pad, j.q.npool, j.q.W);
     else
         words = body::f32_body_words(j.f.cs, j.p.group_dms, j.f.rawh, j.f.nch_pad, j.f.W);
     return 4 * (body::BAR_WORDS + JD_WORDS + words);

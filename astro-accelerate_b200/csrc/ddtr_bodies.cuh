@@ -31,10 +31,22 @@ constexpr int SUB_SLOTS = 6; // TMA ring depth of the subband body
 constexpr int QDMW = 4;    // DM trials per warp
 constexpr int NTHREADS = 512;
 
-// Words of the caller-owned barrier area (QNSTAGE 8-byte mbarriers), rounded
-// up to 16 bytes: the body area behind it holds TMA destinations and 16-byte
-// vector accesses.
-constexpr int BAR_WORDS = ((2 * (QNSTAGE > SUB_SLOTS ? QNSTAGE : SUB_SLOTS) + 2) + 3) & ~3;
+// The caller-owned barrier area: RING_BARS one-arrival mbarriers for the TMA
+// rings of the quad, fp32 and subband bodies (phases carried by stage_ctr),
+// then the split-phase quad body's own barriers (phases carried by its own
+// counter): SP_QN TMA barriers, SP_NB "rows built" and SP_NB "rows consumed"
+// barriers with one arrival per warp.  Rounded up to 16 bytes: the body area
+// behind it holds TMA destinations and 16-byte vector accesses.
+constexpr int RING_BARS = 8;
+static_assert(RING_BARS >= QNSTAGE && RING_BARS >= SUB_SLOTS, "one ring barrier per TMA slot");
+constexpr int SP_QN = 4;      // TMA ring depth of the split-phase quad body
+constexpr int SP_NB = 3;      // pattern-row buffers of the split-phase quad body
+constexpr int SP_WARPS = 16;  // warps of the split-phase quad body (arrivals per phase)
+constexpr int SP_BAR_T = RING_BARS;
+constexpr int SP_BAR_FULL = SP_BAR_T + SP_QN;
+constexpr int SP_BAR_EMPTY = SP_BAR_FULL + SP_NB;
+constexpr int NBARS = SP_BAR_EMPTY + SP_NB; // mbarriers in the area
+constexpr int BAR_WORDS = (2 * NBARS + 3) & ~3;
 static_assert(BAR_WORDS % 4 == 0, "the body area must start on a 16-byte boundary");
 
 __device__ __forceinline__ int output_class(int kind, long long t)
@@ -42,13 +54,11 @@ __device__ __forceinline__ int output_class(int kind, long long t)
     return (kind == KIND_SHARED4) ? static_cast<int>((t & 31) >> 2) : static_cast<int>((t & 15) >> 1);
 }
 
-constexpr int NBARS = BAR_WORDS / 2; // mbarriers in the area
-
 __device__ __forceinline__ void init_barriers(unsigned bar0)
 {
     if (threadIdx.x == 0)
         for (int i = 0; i < NBARS; ++i)
-            mbar_init(bar0 + 8 * i, 1);
+            mbar_init(bar0 + 8 * i, (i >= SP_BAR_FULL) ? SP_WARPS : 1);
     mbar_init_fence();
 }
 
@@ -384,6 +394,289 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
         issue(s + QNSTAGE);
     }
     stage_ctr = sbase + static_cast<unsigned>(nstages);
+    if (!ok)
+        return false;
+
+    // (float)S / nchans / bin, the reference's expression (4-bit: / nchans)
+#pragma unroll
+    for (int j = 0; j < DW; ++j) {
+        const int dm = dm0 + warp * DW + j;
+        if (dm >= p.ndms)
+            continue;
+        float *orow = p.out + static_cast<long long>(dm) * p.out_pitch;
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            const long long t = t0 + lane + 32 * m;
+            if (t < p.tp) {
+                const float v = static_cast<float>(static_cast<int>(acc[j][m]));
+                orow[t] = p.divide_by_bin ? (v / p.nchans_f / p.bin_f) : (v / p.nchans_f);
+            }
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Split-phase channel-quad body: the sums of quad_body with the CTA barrier
+// of every stage replaced by mbarrier hand-offs, so that a warp that is done
+// early goes on to the next stage instead of waiting for the slowest one.
+//
+// Per stage s (all 16 warps alike; warp 0 also issues the copies):
+//   build(s+1): wait "consumed" of stage s+1-SP_NB (its row buffer is free)
+//               and the stage's copies, build this warp's share of its
+//               pre-skewed rows, arrive on "built" of stage s+1;
+//   sum(s):     wait "built" of stage s, add, arrive on "consumed" of s;
+//   warp 0:     wait "consumed" of stage s-1 (its TMA slot is free) and
+//               issue the copies of stage s+SP_QN-1.
+// So warps may drift up to a stage apart and the builds of stage s+1 overlap
+// the sums of stage s across the CTA.  One lane per warp arrives, after a
+// __syncwarp, so each arrival (release) covers the whole warp's shared-memory
+// accesses; the waits acquire.  The raw-row byte shifts written by warp 0 are
+// published by its expect_tx arrival on the stage's TMA barrier.  Barrier
+// phases follow the caller's split-phase counter sp_ctr, so a persistent CTA
+// carries them from tile to tile; a CTA barrier at the start of a tile keeps
+// tiles apart (the window table and every buffer are free there).
+//
+// Only for ranges without per-byte entries (every (quad, DM trial) has a
+// pre-skewed row); an entry of -1 sets DERR_WINDOW.  Every wait is bounded: a
+// warp whose wait gives up sets DERR_TIMEOUT and leaves the stage loop; warp 0
+// then waits, with the same bound, for the copies it issued.
+//
+// Shared memory (words from sm): qwin[nq_pad] | raw[SP_QN][QS*4][RAWW] |
+// ent[SP_QN][QS][64] | pat[SP_QN][QS][16] | rsh[SP_QN][QS*4] |
+// P[SP_NB][npool][W].
+// ---------------------------------------------------------------------------
+__host__ __device__ inline size_t quad_sp_body_words(int qs, int raww, int nq_pad, int npool, int W)
+{
+    size_t o = static_cast<size_t>(nq_pad);
+    o += static_cast<size_t>(SP_QN) * qs * 4 * raww;
+    o += static_cast<size_t>(SP_QN) * qs * 64;
+    o += static_cast<size_t>(SP_QN) * qs * 16;
+    o += static_cast<size_t>(SP_QN) * qs * 4;
+    o = (o + 3) & ~static_cast<size_t>(3);
+    o += static_cast<size_t>(SP_NB) * npool * W;
+    return o;
+}
+
+__device__ __forceinline__ void mbar_arrive_one(unsigned bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+
+template <int M>
+__device__ bool quad_sp_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long long t0, uint32_t *sm,
+                             unsigned bar0, unsigned &sp_ctr)
+{
+    constexpr int DW = 4;
+    constexpr int NT = 32 * SP_WARPS;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int GD = 64;
+    const int dm0 = g * GD;
+    const int W = Q.W, RAWW = Q.raww, QS = Q.qs;
+    const unsigned char *in = static_cast<const unsigned char *>(p.in);
+    const int nstages = (Q.nquads + QS - 1) / QS;
+    const unsigned sbase = sp_ctr;
+
+    const int o_qw = 0;
+    const int o_raw = o_qw + Q.nq_pad;
+    const int o_ent = o_raw + SP_QN * QS * 4 * RAWW;
+    const int o_pat = o_ent + SP_QN * QS * GD;
+    const int o_rsh = o_pat + SP_QN * QS * 16;
+    const int o_P = ((o_rsh + SP_QN * QS * 4) + 3) & ~3;
+
+    auto tbar = [&](int s) { return bar0 + 8u * (SP_BAR_T + (sbase + static_cast<unsigned>(s)) % SP_QN); };
+    auto tpar = [&](int s) { return ((sbase + static_cast<unsigned>(s)) / SP_QN) & 1u; };
+    auto fbar = [&](int s) { return bar0 + 8u * (SP_BAR_FULL + (sbase + static_cast<unsigned>(s)) % SP_NB); };
+    auto ebar = [&](int s) { return bar0 + 8u * (SP_BAR_EMPTY + (sbase + static_cast<unsigned>(s)) % SP_NB); };
+    auto bpar = [&](int s) { return ((sbase + static_cast<unsigned>(s)) / SP_NB) & 1u; };
+    auto slot_of = [&](int s) { return static_cast<int>((sbase + static_cast<unsigned>(s)) % SP_QN); };
+    auto buf_of = [&](int s) { return static_cast<int>((sbase + static_cast<unsigned>(s)) % SP_NB); };
+
+    __syncthreads(); // the previous tile of a persistent CTA is done with every buffer
+    for (int i = tid; i < (Q.nq_pad >> 2); i += NT)
+        cp_async16(&sm[o_qw + 4 * i], Q.qwin + static_cast<size_t>(g) * Q.nq_pad + 4 * i);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+
+    bool ok = true;
+    auto wait = [&](unsigned bar, unsigned parity) {
+        if (ok && !mbar_wait_bounded(bar, parity)) {
+            atomicOr(p.err, DERR_TIMEOUT);
+            ok = false;
+        }
+    };
+
+    // warp 0: the stage's raw rows, DM offsets and patterns into its TMA slot
+    int issued = 0;
+    auto issue = [&](int s) {
+        const int slot = slot_of(s);
+        const int q0 = s * QS;
+        const int nq = min(QS, Q.nquads - q0);
+        const int c0 = 4 * q0;
+        const int nrows = max(0, min(4 * nq, p.nch_used - c0));
+        const unsigned bar = tbar(s);
+        uintptr_t a = 0;
+        if (lane < 4 * nq) {
+            if (lane < nrows) {
+                const int w0 = static_cast<int>(sm[o_qw + q0 + (lane >> 2)]);
+                a = reinterpret_cast<uintptr_t>(in + static_cast<long long>(c0 + lane) * p.stride + t0 + w0);
+                sm[o_rsh + slot * QS * 4 + lane] = static_cast<uint32_t>(a & 15);
+            } else {
+                sm[o_rsh + slot * QS * 4 + lane] = 0xFFFFFFFFu; // channel contributes nothing
+            }
+        }
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0)
+            mbar_expect_tx(bar, static_cast<unsigned>(nrows * RAWW * 4 + nq * GD * 4 + nq * 64));
+        __syncwarp();
+        if (lane < nrows)
+            tma_load_1d(smem_addr(&sm[o_raw + (slot * QS * 4 + lane) * RAWW]),
+                        reinterpret_cast<const void *>(a & ~static_cast<uintptr_t>(15)),
+                        static_cast<unsigned>(RAWW * 4), bar);
+        if (lane < nq)
+            tma_load_1d(smem_addr(&sm[o_ent + (slot * QS + lane) * GD]),
+                        Q.qoff + static_cast<size_t>(q0 + lane) * p.ndms + dm0, static_cast<unsigned>(GD * 4), bar);
+        if (lane == 0)
+            tma_load_1d(smem_addr(&sm[o_pat + slot * QS * 16]), Q.qpat + (static_cast<size_t>(g) * Q.nquads + q0) * 16,
+                        static_cast<unsigned>(nq * 64), bar);
+        issued = s + 1;
+    };
+
+    // this warp's share of the pre-skewed rows of stage s (one warp per row)
+    auto build = [&](int s) {
+        const int slot = slot_of(s);
+        const int b = buf_of(s);
+        const int q0 = s * QS;
+        const int nq = min(QS, Q.nquads - q0);
+        int total = 0;
+        for (int q = 0; q < nq; ++q)
+            total += static_cast<int>(sm[o_pat + (slot * QS + q) * 16 + 15]);
+        total = min(total, Q.npool);
+        const int n4 = W >> 2;
+        int q = 0, base = 0;
+        int cnt_q = (nq > 0) ? static_cast<int>(sm[o_pat + (slot * QS) * 16 + 15]) : 0;
+        for (int r = warp; r < total; r += SP_WARPS) {
+            while (r >= base + cnt_q && q + 1 < nq) {
+                base += cnt_q;
+                ++q;
+                cnt_q = static_cast<int>(sm[o_pat + (slot * QS + q) * 16 + 15]);
+            }
+            const unsigned pw = sm[o_pat + (slot * QS + q) * 16 + (r - base)];
+            int d[4], rs[4], rb[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                d[i] = (i == 0) ? 0 : static_cast<int>((pw >> (8 * (i - 1))) & 255u);
+                rs[i] = static_cast<int>(sm[o_rsh + slot * QS * 4 + 4 * q + i]);
+                rb[i] = o_raw + (slot * QS * 4 + 4 * q + i) * RAWW;
+            }
+            const int prow = o_P + (b * Q.npool + r) * W;
+            for (int t4 = lane; t4 < n4; t4 += 32) {
+                const int tau = 4 * t4;
+                uint32_t a[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if (rs[i] < 0) {
+                        a[i] = 0u;
+                    } else {
+                        const int bb = rs[i] + tau + d[i];
+                        const int wi = rb[i] + (bb >> 2);
+                        a[i] = __funnelshift_r(sm[wi], sm[wi + 1], 8u * static_cast<unsigned>(bb & 3));
+                    }
+                }
+                // 4x4 byte transpose: word k of the result holds sample tau+k of the four channels
+                const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), hi01 = __byte_perm(a[0], a[1], 0x7362);
+                const uint32_t lo23 = __byte_perm(a[2], a[3], 0x5140), hi23 = __byte_perm(a[2], a[3], 0x7362);
+                uint4 v;
+                v.x = __byte_perm(lo01, lo23, 0x5410);
+                v.y = __byte_perm(lo01, lo23, 0x7632);
+                v.z = __byte_perm(hi01, hi23, 0x5410);
+                v.w = __byte_perm(hi01, hi23, 0x7632);
+                *reinterpret_cast<uint4 *>(&sm[prow + tau]) = v;
+            }
+        }
+    };
+
+    uint32_t acc[DW][M];
+#pragma unroll
+    for (int j = 0; j < DW; ++j)
+#pragma unroll
+        for (int m = 0; m < M; ++m)
+            acc[j][m] = 0u;
+
+    if (warp == 0)
+        for (int s = 0; s < SP_QN - 1 && s < nstages; ++s)
+            issue(s);
+    if (nstages > 0) {
+        wait(tbar(0), tpar(0));
+        if (ok)
+            build(0);
+        __syncwarp();
+        if (lane == 0)
+            mbar_arrive_one(fbar(0));
+    }
+    int s = 0;
+    for (; s < nstages && ok; ++s) {
+        if (s + 1 < nstages) {
+            if (s + 1 >= SP_NB)
+                wait(ebar(s + 1 - SP_NB), bpar(s + 1 - SP_NB));
+            wait(tbar(s + 1), tpar(s + 1));
+            if (!ok)
+                break;
+            build(s + 1);
+            __syncwarp();
+            if (lane == 0)
+                mbar_arrive_one(fbar(s + 1));
+        }
+        wait(fbar(s), bpar(s));
+        if (!ok)
+            break;
+        const int slot = slot_of(s);
+        const int b = buf_of(s);
+        const int q0 = s * QS;
+        const int nq = min(QS, Q.nquads - q0);
+        int rbase = 0;
+        for (int q = 0; q < nq; ++q) {
+            const int prow = o_P + (b * Q.npool + rbase) * W + lane;
+            const int4 e4 = *reinterpret_cast<const int4 *>(&sm[o_ent + (slot * QS + q) * GD + warp * DW]);
+            const int ej[DW] = {e4.x, e4.y, e4.z, e4.w};
+            if ((e4.x | e4.y | e4.z | e4.w) < 0)
+                atomicOr(p.err, DERR_WINDOW);
+            // neighbouring DM trials often share the quad's offset: their
+            // words are already in registers (warp-uniform test)
+            uint32_t w[M];
+#pragma unroll
+            for (int j = 0; j < DW; ++j) {
+                if (j == 0 || ej[j] != ej[j - 1]) {
+                    const int e = prow + max(ej[j], 0);
+#pragma unroll
+                    for (int m = 0; m < M; ++m)
+                        w[m] = sm[e + 32 * m];
+                }
+#pragma unroll
+                for (int m = 0; m < M; ++m)
+                    acc[j][m] = __dp4a(w[m], 0x01010101u, acc[j][m]);
+            }
+            rbase += static_cast<int>(sm[o_pat + (slot * QS + q) * 16 + 15]);
+        }
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0)
+            mbar_arrive_one(ebar(s));
+        if (warp == 0 && s + SP_QN - 1 < nstages) {
+            if (s >= 1)
+                wait(ebar(s - 1), bpar(s - 1));
+            if (!ok)
+                break;
+            issue(s + SP_QN - 1);
+        }
+    }
+    if (!ok && warp == 0) // copies this warp issued may still be landing: wait for them
+        for (int k = max(0, issued - (SP_QN - 1)); k < issued; ++k)
+            mbar_wait_bounded(tbar(k), tpar(k));
+    sp_ctr = sbase + static_cast<unsigned>(nstages);
     if (!ok)
         return false;
 

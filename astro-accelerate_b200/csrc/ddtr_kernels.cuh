@@ -121,6 +121,11 @@ cudaError_t launch_ddtr_quad(const DdtrLaunch &p, const QuadLaunch &q, cudaStrea
 // Runs only ranges without per-byte entries (stats[3] of the pattern kernel = 0).
 cudaError_t launch_ddtr_quadws(const DdtrLaunch &p, const QuadLaunch &q, cudaStream_t st);
 size_t quadws_smem_bytes(const QuadLaunch &q);
+// Split-phase channel-quad kernel (M = 16 only): the quad kernel's sums with
+// mbarrier hand-offs between the row builds and the sums instead of a CTA
+// barrier per stage.  Runs only ranges without per-byte entries.
+cudaError_t launch_ddtr_quadsp(const DdtrLaunch &p, const QuadLaunch &q, cudaStream_t st);
+size_t quadsp_smem_bytes(const QuadLaunch &q);
 
 // Subband kernel (ddtr_sub.cu): 16-channel partial sums per skew pattern.
 constexpr int SUB_BLK_WORDS = 128; // pattern block per (subband, DM group)
@@ -182,7 +187,7 @@ struct BatchJobDev {
     DdtrLaunch p;
     QuadLaunch q;
     F32Launch f;
-    int variant; // 2 channel-quad, 3 staged fp32
+    int variant; // 2 channel-quad, 3 staged fp32, 6 split-phase channel-quad
     int groups;
     long long item0;
 };

@@ -129,7 +129,41 @@ __global__ void __launch_bounds__(body::WS_THREADS, 1) k_ddtr_quadws(const DdtrL
                        stage_ctr);
 }
 
+// Split-phase channel-quad kernel (body::quad_sp_body): 16 warps x 4 DM
+// trials x 512 samples, one CTA per SM.
+__global__ void __launch_bounds__(32 * body::SP_WARPS, 1) k_ddtr_quadsp(const DdtrLaunch p, const QuadLaunch Q)
+{
+    extern __shared__ __align__(16) uint32_t sm[];
+    const unsigned bar0 = smem_addr(sm);
+    body::init_barriers(bar0);
+    __syncthreads();
+    unsigned sp_ctr = 0;
+    body::quad_sp_body<16>(p, Q, blockIdx.x, static_cast<long long>(blockIdx.y) * 512, sm + body::BAR_WORDS, bar0,
+                           sp_ctr);
+}
+
 } // namespace
+
+size_t quadsp_smem_bytes(const QuadLaunch &q)
+{
+    return 4 * (body::BAR_WORDS + body::quad_sp_body_words(q.qs, q.raww, q.nq_pad, q.npool, q.W));
+}
+
+cudaError_t launch_ddtr_quadsp(const DdtrLaunch &p, const QuadLaunch &q, cudaStream_t st)
+{
+    if (p.group_dms != 64 || q.qs < 1 || q.qs > 8 || q.M != 16)
+        return cudaErrorInvalidValue;
+    const size_t smem = quadsp_smem_bytes(q);
+    if (smem > 227 * 1024)
+        return cudaErrorInvalidValue;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_ddtr_quadsp, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess)
+        return e;
+    dim3 grid(p.ndms / p.group_dms, static_cast<unsigned>((p.tp + 511) / 512));
+    k_ddtr_quadsp<<<grid, 32 * body::SP_WARPS, smem, st>>>(p, q);
+    return cudaGetLastError();
+}
 
 size_t quadws_smem_bytes(const QuadLaunch &q)
 {

@@ -133,7 +133,9 @@ bool DdtrPipeline::build_range(int r)
         if (!build_sub_tables(r))
             return false;
     }
-    if (elem_bytes_ == 1 && (opt_.kernel_variant == 0 || opt_.kernel_variant == 2 || opt_.kernel_variant == 4) &&
+    if (elem_bytes_ == 1 &&
+        (opt_.kernel_variant == 0 || opt_.kernel_variant == 2 || opt_.kernel_variant == 4 ||
+         opt_.kernel_variant == 5) &&
         rc.group_dms == 64) {
         if (!build_quad_tables(r))
             return false;
@@ -149,6 +151,15 @@ bool DdtrPipeline::build_range(int r)
             return fail("the warp-specialised channel-quad kernel cannot run range " + std::to_string(r) +
                         " (entries on the per-byte path, or its stage does not fit shared memory)");
         rc.variant = 5;
+    }
+    if (elem_bytes_ == 1 && opt_.kernel_variant == 5) {
+        const int qs = quad_sp_depth(rc);
+        if (qs == 0)
+            return fail("the split-phase channel-quad kernel cannot run range " + std::to_string(r) +
+                        " (entries on the per-byte path, or its stage does not fit shared memory)");
+        rc.quad.npool = qs * std::max(1, rc.quad.npool / std::max(1, rc.quad.qs));
+        rc.quad.qs = qs;
+        rc.variant = 6;
     }
     if (elem_bytes_ == 2 && opt_.kernel_variant != 1 && rc.group_dms == 64 && nchans <= 16384) {
         const F32Geometry G = f32_geometry(rc.span, rc.group_dms, nchans, 0);
@@ -304,6 +315,27 @@ bool DdtrPipeline::quad_ws_fits(const RangeConfig &rc) const
     q.npool = rc.quad.npool;
     q.W = rc.quad.W;
     return quadws_smem_bytes(q) <= kStagedSmemLimit;
+}
+
+// The split-phase channel-quad kernel needs the same (512-sample tiles, no
+// per-byte entries) and its deeper rings in shared memory: the largest stage
+// depth up to the range's whose rings fit, 0 if none does.
+int DdtrPipeline::quad_sp_depth(const RangeConfig &rc) const
+{
+    if (!rc.has_quad || !rc.quad_ws_ok || rc.quad.M != 16)
+        return 0;
+    QuadLaunch q{};
+    q.raww = rc.quad.raww;
+    q.nq_pad = rc.quad.nq_pad;
+    q.W = rc.quad.W;
+    const int maxcnt = std::max(1, rc.quad.npool / std::max(1, rc.quad.qs));
+    for (int qs = rc.quad.qs; qs >= 1; qs /= 2) {
+        q.qs = qs;
+        q.npool = qs * maxcnt;
+        if (quadsp_smem_bytes(q) <= kStagedSmemLimit)
+            return qs;
+    }
+    return 0;
 }
 
 // Optional processing of the reference runner: the bandpass normalisation
@@ -581,7 +613,7 @@ bool DdtrPipeline::tune_ranges()
     StageTuneCache cache;
     for (size_t r = 0; r < ranges_.size(); ++r) {
         RangeConfig &rc = ranges_[r];
-        if (rc.variant != 2 && rc.variant != 3 && rc.variant != 5)
+        if (rc.variant != 2 && rc.variant != 3 && rc.variant != 5 && rc.variant != 6)
             continue;
         const DdtrOp *op = nullptr;
         for (const DdtrOp &o : ops_)
@@ -599,11 +631,37 @@ bool DdtrPipeline::tune_ranges()
         std::string err;
         if (!tune_stage_depth(job, st_, device_, cache, err))
             return fail(err);
-        if (rc.variant == 2 || rc.variant == 5) {
+        if (rc.variant == 2 || rc.variant == 5 || rc.variant == 6) {
             rc.quad.qs = job.q.qs;
             rc.quad.npool = job.q.npool;
         } else {
             rc.f32.cs = job.f.cs;
+        }
+        if (rc.variant == 2 && opt_.kernel_variant == 0 && quad_sp_depth(rc) > 0) {
+            // the split-phase kernel (its own stage depth) against the tuned
+            // channel-quad kernel
+            const float t_quad = time_job_slice(job, st_, device_, err);
+            if (t_quad < 0.f)
+                return fail(err);
+            const QuadGeometry keep = rc.quad;
+            const int qs = quad_sp_depth(rc);
+            rc.quad.npool = qs * std::max(1, rc.quad.npool / std::max(1, rc.quad.qs));
+            rc.quad.qs = qs;
+            rc.variant = 6;
+            DdtrJob jsp;
+            bool made = make_job(*op, d_flat_[op->src_level & 1], flat_elems_, out, pitch, jsp);
+            if (made && !tune_stage_depth(jsp, st_, device_, cache, err))
+                return fail(err);
+            const float t_sp = made ? time_job_slice(jsp, st_, device_, err) : -1.f;
+            if (made && t_sp < 0.f)
+                return fail(err);
+            if (made && t_sp < t_quad) {
+                rc.quad.qs = jsp.q.qs;
+                rc.quad.npool = jsp.q.npool;
+            } else {
+                rc.variant = 2;
+                rc.quad = keep;
+            }
         }
         if (rc.variant == 2 && rc.has_sub) {
             // the subband kernel against the tuned channel-quad kernel
@@ -725,16 +783,17 @@ bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, f
                   : (elem_bytes_ == 2 && rc.variant == 3) ? 3
                   : (elem_bytes_ == 1 && rc.variant == 4) ? 4
                   : (elem_bytes_ == 1 && rc.variant == 5) ? 5
+                  : (elem_bytes_ == 1 && rc.variant == 6) ? 6
                                                           : 1;
     job.elem_bytes = elem_bytes_;
     job.tile_words = rc.tile_words;
     job.offtab = rc.d_offtab;
-    const int tile = (job.variant == 2 || job.variant == 5)
+    const int tile = (job.variant == 2 || job.variant == 5 || job.variant == 6)
                          ? 32 * rc.quad.M
                          : ((job.variant == 3 || job.variant == 4) ? 512 : 128 * rc.tile_words);
     const long long ntiles = (tp + tile - 1) / tile;
     long long need;
-    if (elem_bytes_ == 1 && (job.variant == 2 || job.variant == 5))
+    if (elem_bytes_ == 1 && (job.variant == 2 || job.variant == 5 || job.variant == 6))
         need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ntiles * tile + rc.delay_max + 4LL * rc.quad.raww + 64;
     else if (job.variant == 4)
         need = static_cast<long long>(rc.nch_used - 1) * i_nsamp + ntiles * tile + rc.delay_max + 4LL * rc.sub.raww + 64;
@@ -769,7 +828,7 @@ bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, f
     if (job.variant == 1 && elem_bytes_ == 1 &&
         ((reinterpret_cast<uintptr_t>(p.out) & 15) || (p.out_pitch & 3) || (tp & 3)))
         return fail("output rows are not 16-byte aligned");
-    if (job.variant == 2 || job.variant == 5) {
+    if (job.variant == 2 || job.variant == 5 || job.variant == 6) {
         QuadLaunch &q = job.q;
         q.qpat = rc.d_qpat;
         q.qwin = rc.d_qwin;
@@ -812,6 +871,8 @@ cudaError_t launch_job(const DdtrJob &job, cudaStream_t st)
         return launch_ddtr_sub(job.p, job.s, st);
     if (job.variant == 5)
         return launch_ddtr_quadws(job.p, job.q, st);
+    if (job.variant == 6)
+        return launch_ddtr_quadsp(job.p, job.q, st);
     return (job.elem_bytes == 1) ? launch_ddtr_u8(job.p, job.offtab, job.tile_words, st) : launch_ddtr_u16(job.p, st);
 }
 

@@ -42,7 +42,7 @@ struct PipelineOptions {
     int tile_words = 0;         // 0: autotune
     int kernel_variant = 0;     // 0: choose per range, 1: generic kernels, 2: channel-quad / fp32 kernels,
                                 // 3: subband / fp32 kernels, 4: warp-specialised channel-quad
-                                // / fp32 kernels
+                                // / fp32 kernels, 5: split-phase channel-quad / fp32 kernels
     int group_dms = 0;          // 0: autotune
     bool device_input = false;  // the input pointer is device memory ([t][c] uint16)
     // the input holds the SIGPROC data section as stored ([t][nchans*nbits/8]
@@ -92,7 +92,8 @@ struct DdtrOp {
 
 // A dedispersion launch, ready for a stream (launch_job) or a batch queue.
 struct DdtrJob {
-    int variant = 1; // 1 generic, 2 channel-quad, 3 staged fp32, 4 subband, 5 warp-specialised quad
+    int variant = 1; // 1 generic, 2 channel-quad, 3 staged fp32, 4 subband, 5 warp-specialised quad,
+                     // 6 split-phase quad
     int elem_bytes = 1;
     int tile_words = 4;
     const int32_t *offtab = nullptr;
@@ -128,7 +129,8 @@ struct RangeConfig {
     // 1: generic kernel (k_ddtr_u8 byte-phase / k_ddtr_u16 gather), 2: channel-quad
     // kernel (k_ddtr_quad, one-byte data), 3: staged fp32 kernel (k_ddtr_f32, two-byte data),
     // 4: subband kernel (k_ddtr_sub, one-byte data), 5: warp-specialised channel-quad
-    // kernel (k_ddtr_quadws, one-byte data)
+    // kernel (k_ddtr_quadws, one-byte data), 6: split-phase channel-quad kernel
+    // (k_ddtr_quadsp, one-byte data)
     int variant = 1;
     QuadGeometry quad{};
     int quad_span = 0, quad_dmax = 0, quad_maxcnt = 0, nquads = 0;
@@ -214,6 +216,7 @@ private:
     bool build_range(int r);
     bool setup_processing(long long L0);
     bool quad_ws_fits(const RangeConfig &rc) const;
+    int quad_sp_depth(const RangeConfig &rc) const;
     bool build_quad_tables(int r);
     bool build_sub_tables(int r);
     bool tune_ranges();

@@ -84,8 +84,8 @@ def parse():
     ap.add_argument("--tile-words", type=int, default=0)
     ap.add_argument("--group-dms", type=int, default=0)
     ap.add_argument("--variant", type=int, default=0,
-                    help="0 auto, 1 generic kernels, 2 channel-quad, 3 subband, 4 warp-specialised channel-quad "
-                         "(2-4 run the staged fp32 kernel on two-byte data)")
+                    help="0 auto, 1 generic kernels, 2 channel-quad, 3 subband, 4 warp-specialised channel-quad, "
+                         "5 split-phase channel-quad (2-5 run the staged fp32 kernel on two-byte data)")
     ap.add_argument("--with-analysis", action="store_true",
                     help="add an e2e run through the C ABI with the analysis component after every step")
     ap.add_argument("--spd-nt", type=int, default=0, help="samples per DM trial of the spd config (default 2^19)")
@@ -1338,7 +1338,7 @@ def main():
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     kernel_names = {"quad": "k_ddtr_quad", "phase": "k_ddtr_u8", "f32": "k_ddtr_f32", "gather": "k_ddtr_u16",
-                    "sub": "k_ddtr_sub", "quadws": "k_ddtr_quadws"}
+                    "sub": "k_ddtr_sub", "quadws": "k_ddtr_quadws", "quadsp": "k_ddtr_quadsp"}
     used = sorted({kernel_names[ri["kernel"]] for ri in ranges})
     hbm_achieved = alg_bytes / dd_s_per_step / 1e9
     roofline = {

@@ -356,6 +356,12 @@ bool aa_b200_pipeline_set_options(void *obj, int stride_mode, int fma_mode, int 
  * and is unpacked on the GPU in the corner-turn kernel; outputs are
  * identical to the unsigned-short input of the same samples. */
 bool aa_b200_pipeline_set_packed_input(void *obj, const void *packed);
+/* Before bind: the kernel family per range.  0 chooses per range (the
+ * autotuner times the candidates), 1 the generic kernels, 2 the channel-quad
+ * kernel (one-byte data) / staged fp32 kernel (two-byte data), 3 the subband
+ * kernel / fp32, 4 the warp-specialised channel-quad kernel / fp32, 5 the
+ * split-phase channel-quad kernel / fp32.  A forced family that cannot run a
+ * range makes the bind fail with the reason. */
 bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant);
 /* output_dmt (pipeline_component_option_struct): when the run finishes, the
  * DM-time output of every range is written in the reference's

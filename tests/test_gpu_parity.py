@@ -131,9 +131,10 @@ def test_tile_shapes_agree(aa, oracle_mod, cuda_device, tile_words, group_dms, v
     assert_matches_oracle(case, s, got, want, kern)
 
 
-@pytest.mark.parametrize("name,variant,kernel", [("shared8_binned", 0, "quad"), ("shared8_binned", 1, "phase"),
-                                                 ("shared8_binned", 2, "quad"), ("shared8_nch3000", 0, "sub|quad"),
-                                                 ("shared8_nch3000", 4, "quadws"),
+@pytest.mark.parametrize("name,variant,kernel", [("shared8_binned", 0, "quad|quadsp"), ("shared8_binned", 1, "phase"),
+                                                 ("shared8_binned", 2, "quad"),
+                                                 ("shared8_nch3000", 0, "sub|quad|quadsp"),
+                                                 ("shared8_nch3000", 4, "quadws"), ("shared8_nch3000", 5, "quadsp"),
                                                  ("shared8_nch3000", 3, "sub"), ("shared8_nch3000", 2, "quad"),
                                                  ("shared16", 0, "f32"), ("shared16", 1, "gather"),
                                                  ("cache16", 2, "f32")])
@@ -184,6 +185,42 @@ def test_warp_specialised_quad_runs_the_plain_cases(aa, cuda_device):
         except AssertionError as e:
             assert WS_REFUSED in str(e), str(e)
     assert ran, "the warp-specialised kernel ran none of the cases"
+
+
+SP_REFUSED = "split-phase channel-quad kernel cannot run"
+
+
+@pytest.mark.parametrize("name", WS_CASES)
+def test_split_phase_quad_matches_oracle(aa, oracle_mod, golden_ddtr, cuda_device, name):
+    """Variant 5 forces the split-phase channel-quad kernel (k_ddtr_quadsp) on
+    one-byte data: bit-identical to the oracle and to the reference GPU
+    output.  Ranges with (quad, DM) entries on the per-byte path are refused."""
+    case = C.CASES[name]
+    x = C.make_input(case)
+    try:
+        got, info, _, _ = run_pipeline(aa, case, x, variant=5)
+    except AssertionError as e:
+        assert SP_REFUSED in str(e), str(e)
+        pytest.skip(f"refused: {e}")
+    assert all(i["kernel"] == "quadsp" for i in info), [i["kernel"] for i in info]
+    s, want, kern = oracle_run(oracle_mod, case, x)
+    assert_matches_oracle(case, s, got, want, kern)
+    for r, rr in enumerate(golden_ddtr.get(name, {}).get("ranges", [])):
+        assert hashlib.sha256(got[r].tobytes()).hexdigest() == rr["sha256"], f"range {r} differs from the reference GPU"
+
+
+def test_split_phase_quad_runs_the_plain_cases(aa, cuda_device):
+    """The split-phase kernel takes the cases whose every entry has a
+    pre-skewed row."""
+    ran = []
+    for name in ("cache8", "shared8_nch3000", "fma_probe"):
+        case = C.CASES[name]
+        try:
+            _, info, _, _ = run_pipeline(aa, case, C.make_input(case), variant=5)
+            ran.append(name)
+        except AssertionError as e:
+            assert SP_REFUSED in str(e), str(e)
+    assert ran, "the split-phase kernel ran none of the cases"
 
 
 def test_subband_kernel_refused_where_patterns_do_not_fit(aa, cuda_device):
