@@ -148,6 +148,7 @@ def lib():
         "aa_b200_pipeline_set_options": ([vp, i, i, i, sz, i, i], b),
         "aa_b200_pipeline_create": ([filterbank_metadata_struct, vp, i, i, i, vp, i], vp),
         "aa_b200_pipeline_set_kernel_variant": ([vp, i], b),
+        "aa_b200_pipeline_set_autotune": ([vp, i], b),
         "aa_b200_pipeline_set_packed_input": ([vp, vp], b),
         "aa_b200_selftest_bounded_wait": ([i, P(i)], i),
         "aa_b200_debug_fail_after": ([ll], None),
@@ -539,8 +540,15 @@ class aa_py_pipeline:
         """Kernel family per range (before bind): 0 auto (timed per range), 1
         generic kernels, 2 channel-quad / fp32, 3 subband / fp32, 4
         warp-specialised channel-quad / fp32, 5 split-phase channel-quad /
-        fp32."""
+        fp32, 6 channel-quad with reuse by offset pattern / fp32, 7
+        channel-quad on 256-sample tiles, two CTAs per SM / fp32."""
         if not lib().aa_b200_pipeline_set_kernel_variant(self.m_obj, variant):
+            raise ValueError(self.last_error())
+        return True
+
+    def set_autotune(self, enable: bool):
+        """Time the staged kernels per range at set-up (default on)."""
+        if not lib().aa_b200_pipeline_set_autotune(self.m_obj, int(bool(enable))):
             raise ValueError(self.last_error())
         return True
 

@@ -185,6 +185,11 @@ bool run_analysis(Api *a)
 
 } // namespace
 
+namespace aab200 {
+// the message aa_b200_last_error() returns, for the library's other C-ABI files
+void set_last_error(const std::string &m) { set_error(m); }
+} // namespace aab200
+
 extern "C" {
 
 // ---------------------------------------------------------------------------
@@ -772,15 +777,25 @@ bool aa_b200_pipeline_set_packed_input(void *obj, const void *packed)
     return true;
 }
 
+bool aa_b200_pipeline_set_autotune(void *obj, int enable)
+{
+    Api *a = as_api(obj);
+    if (a->pipe)
+        return api_fail(a, "autotuning must be chosen before the plan is bound");
+    a->popt.autotune = enable != 0;
+    return true;
+}
+
 bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant)
 {
     Api *a = as_api(obj);
     if (a->pipe)
         return api_fail(a, "the kernel variant must be set before the plan is bound");
-    if (variant < 0 || variant > 5)
+    if (variant < 0 || variant > 7)
         return api_fail(a, "kernel variant must be 0 (auto), 1 (generic kernels), 2 (channel-quad / fp32 kernels), "
-                           "3 (subband / fp32 kernels), 4 (warp-specialised channel-quad / fp32 kernels) or 5 "
-                           "(split-phase channel-quad / fp32 kernels)");
+                           "3 (subband / fp32 kernels), 4 (warp-specialised channel-quad / fp32 kernels), 5 "
+                           "(split-phase channel-quad / fp32 kernels), 6 (channel-quad with reuse by offset "
+                           "pattern / fp32) or 7 (channel-quad, 256-sample tiles, two CTAs per SM / fp32)");
     a->popt.kernel_variant = variant;
     return true;
 }

@@ -161,7 +161,46 @@ __host__ __device__ inline size_t quad_body_words(int qs, int group_dms, int raw
     return o;
 }
 
-template <int M, int DW>
+// Sums of one quad for a warp's four DM trials whose offsets are ej.  Bit j-1
+// of MASK is set when trial j's offset differs from trial j-1's: only then
+// are its words loaded, the others reuse the registers.  One straight-line
+// instance per mask, so that no load is issued for a trial that reuses.
+template <int MASK, int M>
+__device__ __forceinline__ void quad_sum4(uint32_t (&acc)[4][M], const uint32_t *sm, const int (&ej)[4], int prow)
+{
+    uint32_t w[M];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (j == 0 || ((MASK >> (j - 1)) & 1)) {
+#pragma unroll
+            for (int m = 0; m < M; ++m)
+                w[m] = sm[prow + ej[j] + 32 * m];
+        }
+#pragma unroll
+        for (int m = 0; m < M; ++m)
+            acc[j][m] = __dp4a(w[m], 0x01010101u, acc[j][m]);
+    }
+}
+
+template <int M>
+__device__ __forceinline__ void quad_sum4_dispatch(uint32_t (&acc)[4][M], const uint32_t *sm, const int (&ej)[4],
+                                                   int prow)
+{
+    const int mask = (ej[1] != ej[0] ? 1 : 0) | (ej[2] != ej[1] ? 2 : 0) | (ej[3] != ej[2] ? 4 : 0);
+    switch (mask) {
+    case 0: quad_sum4<0, M>(acc, sm, ej, prow); break;
+    case 1: quad_sum4<1, M>(acc, sm, ej, prow); break;
+    case 2: quad_sum4<2, M>(acc, sm, ej, prow); break;
+    case 3: quad_sum4<3, M>(acc, sm, ej, prow); break;
+    case 4: quad_sum4<4, M>(acc, sm, ej, prow); break;
+    case 5: quad_sum4<5, M>(acc, sm, ej, prow); break;
+    case 6: quad_sum4<6, M>(acc, sm, ej, prow); break;
+    default: quad_sum4<7, M>(acc, sm, ej, prow); break;
+    }
+}
+
+// SWITCH: the four trials of a warp (DW = 4) take quad_sum4_dispatch
+template <int M, int DW, bool SWITCH = false>
 __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long long t0, uint32_t *sm, unsigned bar0,
                           unsigned &stage_ctr)
 {
@@ -359,7 +398,10 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
                     ej[4 * h + 3] = e4.w;
                     any_neg |= e4.x | e4.y | e4.z | e4.w;
                 }
-                if (any_neg >= 0) {
+                if (SWITCH && DW == 4 && any_neg >= 0) {
+                    quad_sum4_dispatch<M>(reinterpret_cast<uint32_t(&)[4][M]>(acc), sm,
+                                          reinterpret_cast<const int(&)[4]>(ej), prow);
+                } else if (any_neg >= 0) {
                     // neighbouring DM trials often share the quad's offset:
                     // their words are already in registers (warp-uniform test)
                     uint32_t w[M];

@@ -104,6 +104,8 @@ struct QuadLaunch {
     int qs;    // channel quads per stage
     int npool; // pre-skewed rows per stage buffer
     int M;     // outputs per lane per DM trial (tile = 32*M)
+    int flavour; // 0: per-trial reuse test; 1: reuse by a switch over the warp's offset pattern
+                 // (M = 16); 2: M = 8 with 16 warps and two CTAs per SM
 };
 
 struct QuadGeometry {

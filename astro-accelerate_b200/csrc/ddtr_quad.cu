@@ -104,16 +104,16 @@ __global__ void k_quad_offsets(const int32_t *__restrict__ qtmp, size_t n, int W
 // M = 16: 16 warps x 4 DM trials, one CTA per SM (127 registers);
 // M = 8: 8 warps x 8 DM trials, two CTAs per SM, so that one CTA issues
 // while the other waits at its stage barrier.
-template <int M, int DW>
-__global__ void __launch_bounds__(32 * 64 / DW, (DW == 8) ? 2 : 1) k_ddtr_quad(const DdtrLaunch p, const QuadLaunch Q)
+template <int M, int DW, bool SWITCH, int MINB>
+__global__ void __launch_bounds__(32 * 64 / DW, MINB) k_ddtr_quad(const DdtrLaunch p, const QuadLaunch Q)
 {
     extern __shared__ __align__(16) uint32_t sm[];
     const unsigned bar0 = smem_addr(sm);
     body::init_barriers(bar0);
     __syncthreads();
     unsigned stage_ctr = 0;
-    body::quad_body<M, DW>(p, Q, blockIdx.x, static_cast<long long>(blockIdx.y) * (32 * M), sm + body::BAR_WORDS,
-                           bar0, stage_ctr);
+    body::quad_body<M, DW, SWITCH>(p, Q, blockIdx.x, static_cast<long long>(blockIdx.y) * (32 * M),
+                                   sm + body::BAR_WORDS, bar0, stage_ctr);
 }
 
 // 16 consumer + WS_PROD producer warps (body::quad_ws_body); five warps per
@@ -213,32 +213,33 @@ QuadGeometry quad_geometry(int span, int dmax, int maxcnt, int group_dms, int nq
     return G;
 }
 
+template <typename K>
+static cudaError_t launch_quad_instance(K kernel, int threads, const DdtrLaunch &p, const QuadLaunch &q, size_t smem,
+                                        cudaStream_t st)
+{
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess)
+        return e;
+    const long long tile = 32LL * q.M;
+    dim3 grid(p.ndms / p.group_dms, static_cast<unsigned>((p.tp + tile - 1) / tile));
+    kernel<<<grid, threads, smem, st>>>(p, q);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_ddtr_quad(const DdtrLaunch &p, const QuadLaunch &q, cudaStream_t st)
 {
     if (p.group_dms != 64 || q.qs < 1 || q.qs > 8)
         return cudaErrorInvalidValue;
     const size_t smem = 4 * (body::BAR_WORDS + body::quad_body_words(q.qs, p.group_dms, q.raww, q.nq_pad, q.npool, q.W));
-    const long long tile = 32LL * q.M;
-    dim3 grid(p.ndms / p.group_dms, static_cast<unsigned>((p.tp + tile - 1) / tile));
-    cudaError_t e;
-    switch (q.M) {
-    case 8:
-        e = cudaFuncSetAttribute(k_ddtr_quad<8, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        if (e != cudaSuccess)
-            return e;
-        k_ddtr_quad<8, 8><<<grid, 256, smem, st>>>(p, q);
-        break;
-    case 16:
-        e = cudaFuncSetAttribute(k_ddtr_quad<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem));
-        if (e != cudaSuccess)
-            return e;
-        k_ddtr_quad<16, 4><<<grid, 512, smem, st>>>(p, q);
-        break;
-    default:
-        return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+    if (q.M == 8 && q.flavour == 2)
+        return launch_quad_instance(k_ddtr_quad<8, 4, true, 2>, 512, p, q, smem, st);
+    if (q.M == 8)
+        return launch_quad_instance(k_ddtr_quad<8, 8, false, 2>, 256, p, q, smem, st);
+    if (q.M == 16 && q.flavour == 1)
+        return launch_quad_instance(k_ddtr_quad<16, 4, true, 1>, 512, p, q, smem, st);
+    if (q.M == 16)
+        return launch_quad_instance(k_ddtr_quad<16, 4, false, 1>, 512, p, q, smem, st);
+    return cudaErrorInvalidValue;
 }
 
 } // namespace aab200

@@ -26,8 +26,10 @@ template <int U> struct LoadPass {
     static __device__ __forceinline__ void run(unsigned a, unsigned &acc0, unsigned &acc1)
     {
         unsigned v0, v1;
-        asm volatile("ld.shared.b32 %0, [%1+%2];" : "=r"(v0) : "r"(a), "n"(512 * U));
-        asm volatile("ld.shared.b32 %0, [%1+%2];" : "=r"(v1) : "r"(a), "n"(512 * (U + 1)));
+        // volatile: every pass loads again (a plain load of an unchanged
+        // address would be hoisted out of the loop)
+        asm volatile("ld.volatile.shared.b32 %0, [%1+%2];" : "=r"(v0) : "r"(a), "n"(512 * U));
+        asm volatile("ld.volatile.shared.b32 %0, [%1+%2];" : "=r"(v1) : "r"(a), "n"(512 * (U + 1)));
         acc0 += v0;
         acc1 += v1;
         LoadPass<U + 2>::run(a, acc0, acc1);

@@ -135,7 +135,7 @@ bool DdtrPipeline::build_range(int r)
     }
     if (elem_bytes_ == 1 &&
         (opt_.kernel_variant == 0 || opt_.kernel_variant == 2 || opt_.kernel_variant == 4 ||
-         opt_.kernel_variant == 5) &&
+         opt_.kernel_variant == 5 || opt_.kernel_variant == 6 || opt_.kernel_variant == 7) &&
         rc.group_dms == 64) {
         if (!build_quad_tables(r))
             return false;
@@ -215,7 +215,7 @@ bool DdtrPipeline::build_quad_tables(int r)
         rc.quad_dmax = hs[1];
         rc.quad_maxcnt = hs[2];
         rc.nquads = nquads;
-        const int M = (opt_.tile_words == 2) ? 8 : 16;
+        const int M = (opt_.tile_words == 2 || opt_.kernel_variant == 7) ? 8 : 16;
         int qs = 4;
         QuadGeometry G = quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, nquads, M, qs);
         while (G.smem_bytes > kStagedSmemLimit && qs > 1) {
@@ -840,6 +840,7 @@ bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, f
         q.qs = rc.quad.qs;
         q.npool = rc.quad.npool;
         q.M = rc.quad.M;
+        q.flavour = (opt_.kernel_variant == 6 && q.M == 16) ? 1 : (opt_.kernel_variant == 7 && q.M == 8) ? 2 : 0;
     } else if (job.variant == 3) {
         job.f = rc.f32;
     } else if (job.variant == 4) {

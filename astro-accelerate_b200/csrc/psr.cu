@@ -3,6 +3,8 @@
 
 #include <atomic>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <vector>
 
 namespace aab200 {
@@ -11,64 +13,139 @@ namespace {
 
 std::atomic<long long> g_psr_launches{0};
 
-constexpr int PSR_PAI_THREADS = 512; // PAI_NTHREADS
-constexpr int PSR_PHS_THREADS = 64;  // PHS_NTHREADS
+// ---------------------------------------------------------------------------
+// Power and interbin spectra.  One thread per pair of bins (2i, 2i+1) of one
+// spectrum; the pair's right neighbour (bin 2i+2, needed by the interbin
+// value of bin 2i+1) is the next lane's first bin, passed by a shuffle (the
+// last lane of a warp loads it).  Per bin the values follow
+// src/aa_device_power_kernel.cu:19-41: X / norm component-wise (the fast
+// division), |X|^2, and 0.616850275 |X_k - X_{k+1}|^2; bin 0 and the bins
+// at and above nT/2 give zeros.  Four consecutive interbin entries are one
+// 16-byte store when the row length allows it.
+// ---------------------------------------------------------------------------
+constexpr int PSR_PAIR_THREADS = 256;
 
-// src/aa_device_power_kernel.cu:19-41
-__global__ void __launch_bounds__(PSR_PAI_THREADS) k_power_interbin(const float2 *__restrict__ in, float *power,
-                                                                    float *interbin, int nT, float norm)
+__device__ __forceinline__ float2 psr_scaled(float2 a, float norm) { return make_float2(a.x / norm, a.y / norm); }
+__device__ __forceinline__ float psr_power(float2 a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ float psr_interbin(float2 a, float2 b)
 {
-    const int pos_x = blockIdx.x * blockDim.x + threadIdx.x;
-    const long long pos_y = static_cast<long long>(blockIdx.y) * ((nT >> 1) + 1);
-    float2 A, B;
-    A.x = 0;
-    A.y = 0;
-    B.x = 0;
-    B.y = 0;
-    if ((pos_x < (nT >> 1)) && (pos_x > 0)) {
-        A = in[pos_y + pos_x];
-        B = in[pos_y + pos_x + 1];
-        A.x = A.x / norm;
-        A.y = A.y / norm;
-        B.x = B.x / norm;
-        B.y = B.y / norm;
-    }
-    if (pos_x < (nT >> 1)) {
-        const long long row = blockIdx.y;
-        power[row * (nT >> 1) + pos_x] = A.x * A.x + A.y * A.y;
-        interbin[row * nT + 2 * pos_x] = A.x * A.x + A.y * A.y;
-        interbin[row * nT + 2 * pos_x + 1] = 0.616850275f * ((A.x - B.x) * (A.x - B.x) + (A.y - B.y) * (A.y - B.y));
+    return 0.616850275f * ((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
+}
+
+template <bool VEC4>
+__global__ void __launch_bounds__(PSR_PAIR_THREADS) k_power_pairs(const float2 *__restrict__ in, float *power,
+                                                                  float *interbin, int nT, float norm)
+{
+    const int half = nT >> 1;
+    const long long r = blockIdx.y;
+    const float2 *spec = in + r * (half + 1);
+    const int k0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const float2 zero = make_float2(0.f, 0.f);
+    const float2 x0 = (k0 <= half) ? spec[k0] : zero;
+    const float2 x1 = (k0 + 1 <= half) ? spec[k0 + 1] : zero;
+    float2 x2;
+    x2.x = __shfl_down_sync(0xffffffffu, x0.x, 1);
+    x2.y = __shfl_down_sync(0xffffffffu, x0.y, 1);
+    if ((threadIdx.x & 31) == 31)
+        x2 = (k0 + 2 <= half) ? spec[k0 + 2] : zero;
+    // bin k0 (zero at k0 = 0) and bin k0 + 1
+    const float2 a = (k0 > 0) ? psr_scaled(x0, norm) : zero;
+    const float2 b = (k0 > 0) ? psr_scaled(x1, norm) : zero;
+    const float2 c = psr_scaled(x1, norm);
+    const float2 d = psr_scaled(x2, norm);
+    const float pa = psr_power(a), pc = psr_power(c);
+    const float ia = psr_interbin(a, b), ic = psr_interbin(c, d);
+    float *prow = power + r * half;
+    float *irow = interbin + r * nT;
+    if (VEC4 && k0 + 1 < half) {
+        prow[k0] = pa;
+        prow[k0 + 1] = pc;
+        *reinterpret_cast<float4 *>(irow + 2 * k0) = make_float4(pa, ia, pc, ic);
+    } else {
+        if (k0 < half) {
+            prow[k0] = pa;
+            irow[2 * k0] = pa;
+            irow[2 * k0 + 1] = ia;
+        }
+        if (k0 + 1 < half) {
+            prow[k0 + 1] = pc;
+            irow[2 * k0 + 2] = pc;
+            irow[2 * k0 + 3] = ic;
+        }
     }
 }
 
-// src/aa_device_harmonic_summing_kernel.cu:8-39
-__global__ void __launch_bounds__(PSR_PHS_THREADS) k_harmonic_sum_simple(const float *__restrict__ in, float *snr_out,
-                                                                         uint16_t *harm_out,
-                                                                         const float *__restrict__ msd, int nBins,
-                                                                         int nSpectra, int nHarmonics)
+// ---------------------------------------------------------------------------
+// Simple harmonic sum over corner-turned power spectra [bin][spectrum]: four
+// neighbouring spectra per thread (one 16-byte load per harmonic when the
+// spectrum count allows it), the (mean, deviation) table of the harmonic
+// counts staged once per block in shared memory.  Per spectrum and bin b the
+// running sum over bins b, 2b, ... (below nBins) and the best
+// (sum - mean_f) / sd_f with its f, as src/aa_device_harmonic_summing_kernel.cu:8-39
+// defines them (the fast division; a later f must be strictly better).
+// ---------------------------------------------------------------------------
+constexpr int PSR_HS_THREADS = 128;
+constexpr int PSR_MAX_HARMONICS = 32;
+
+template <int V>
+__global__ void __launch_bounds__(PSR_HS_THREADS) k_harmonic_columns(const float *__restrict__ in, float *snr_out,
+                                                                     uint16_t *harm_out, const float *__restrict__ msd,
+                                                                     int nBins, int nSpectra, int nHarmonics)
 {
-    const int s = blockIdx.y * blockDim.x + threadIdx.x;
-    if (s >= nSpectra)
+    __shared__ float s_msd[2 * PSR_MAX_HARMONICS];
+    for (int i = threadIdx.x; i < 2 * nHarmonics; i += blockDim.x)
+        s_msd[i] = msd[i];
+    __syncthreads();
+    const int s0 = V * (blockIdx.y * blockDim.x + threadIdx.x);
+    if (s0 >= nSpectra)
         return;
     const long long b = blockIdx.x;
-    float HS_value = __ldg(in + b * nSpectra + s);
-    float SNR = (HS_value - __ldg(msd)) / (__ldg(msd + 1));
-    uint16_t best = 0;
+    float acc[V], best[V];
+    uint16_t hbest[V];
+    auto load = [&](long long bin, float *v) {
+        const float *p = in + bin * nSpectra + s0;
+        if (V == 4) {
+            const float4 q = __ldg(reinterpret_cast<const float4 *>(p));
+            v[0] = q.x;
+            v[1] = q.y;
+            v[2] = q.z;
+            v[3] = q.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < V; ++k)
+                v[k] = __ldg(p + k);
+        }
+    };
+    load(b, acc);
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        best[k] = (acc[k] - s_msd[0]) / s_msd[1];
+        hbest[k] = 0;
+    }
     if (b > 0) {
-        for (int f = 1; f < nHarmonics; f++) {
-            const long long bin = b + f * b;
-            if (bin < nBins) {
-                HS_value = HS_value + __ldg(in + bin * nSpectra + s);
-                const float temp_SNR = (HS_value - __ldg(msd + 2 * f)) / (__ldg(msd + 2 * f + 1));
-                if (temp_SNR > SNR) {
-                    SNR = temp_SNR;
-                    best = static_cast<uint16_t>(f);
+        for (int f = 1; f < nHarmonics; ++f) {
+            const long long bin = (f + 1) * b;
+            if (bin >= nBins)
+                break; // the bins of later harmonics are further out
+            float v[V];
+            load(bin, v);
+            const float m = s_msd[2 * f], sd = s_msd[2 * f + 1];
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                acc[k] = acc[k] + v[k];
+                const float t = (acc[k] - m) / sd;
+                if (t > best[k]) {
+                    best[k] = t;
+                    hbest[k] = static_cast<uint16_t>(f);
                 }
             }
         }
     }
-    snr_out[b * nSpectra + s] = SNR;
-    harm_out[b * nSpectra + s] = best;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        snr_out[b * nSpectra + s0 + k] = best[k];
+        harm_out[b * nSpectra + s0 + k] = hbest[k];
+    }
 }
 
 // Peak finding for the periodicity search
@@ -158,283 +235,302 @@ __global__ void k_psr_threshold(const float *__restrict__ in, const uint16_t *__
     list[4 * list_pos + 2] = R * __ldg(&msd[2 * hrms + 1]) + __ldg(&msd[2 * hrms]);
 }
 
+// ---------------------------------------------------------------------------
 // Harmonic sums over normal planes [nDMs][nTimesamples]
-// (src/aa_device_harmonic_summing_kernel.cu:41-268).  Each output bin is
-// independent; the expressions (float sums, the double constants and bin
-// positions of the scalloping-loss and PRESTO forms, the fast division) are
-// the reference's.
-__device__ __forceinline__ float psr_remove_scalloping_loss(float Xm2, float Xm1, float X0, float Xp1, float Xp2)
+// (src/aa_device_harmonic_summing_kernel.cu:41-268 define the three
+// algorithms).  With the scalloping-loss correction every bin the sums read
+// is the same five-bin combination of its neighbours, so it is computed once
+// per bin by k_scalloping_corrected into a scratch plane and the sum kernels
+// read one value per bin from it; without the correction they read the input.
+// One thread per output bin, rows along the grid's y; the (mean, deviation)
+// table of the harmonic counts is staged once per block in shared memory.
+// ---------------------------------------------------------------------------
+// X0 + 0.94247 (X-1 + X+1) + 0.44247 (X-2 + X+2), evaluated in double with
+// the reference's constants and order, rounded to float
+__device__ __forceinline__ float psr_corrected(float Xm2, float Xm1, float X0, float Xp1, float Xp2)
 {
     return (X0 + (1.88494 / 2.0) * (Xm1 + Xp1) + (0.88494 / 2.0) * (Xm2 + Xp2));
 }
 
-template <bool SCAL>
-__device__ __forceinline__ void psr_bins(float *down, float *step, const float *__restrict__ d, long long pos)
-{
-    if (SCAL) {
-        const float Xm2 = d[pos - 2], Xm1 = d[pos - 1], X0 = d[pos + 0], Xp1 = d[pos + 1], Xp2 = d[pos + 2],
-                    Xp3 = d[pos + 3];
-        *down = psr_remove_scalloping_loss(Xm2, Xm1, X0, Xp1, Xp2);
-        *step = psr_remove_scalloping_loss(Xm1, X0, Xp1, Xp2, Xp3);
-    } else {
-        *down = d[pos];
-        *step = d[pos + 1];
-    }
-}
+constexpr int PSR_COR_TILE = 256;
 
-template <bool SCAL>
-__device__ __forceinline__ void psr_bin_value(float *bin, const float *__restrict__ d, long long pos)
+// out[k] for 2 <= k <= nT-3 (the bins whose five-bin window lies in the row);
+// each block stages its tile with a two-bin halo on each side
+__global__ void __launch_bounds__(PSR_COR_TILE) k_scalloping_corrected(const float *__restrict__ in, float *out,
+                                                                       int nT)
 {
-    if (SCAL) {
-        const float Xm2 = d[pos - 2], Xm1 = d[pos - 1], X0 = d[pos], Xp1 = d[pos + 1], Xp2 = d[pos + 2];
-        *bin = X0 + (1.88494 / 2.0) * (Xm1 + Xp1) + (0.88494 / 2.0) * (Xm2 + Xp2);
-    } else {
-        *bin = d[pos];
-    }
-}
-
-// greedy: at every harmonic the larger of two neighbouring bins, the chosen
-// offsets carried to the next harmonic; the harmonic count plus 100 times
-// the offsets at the best S/N
-template <bool SCAL>
-__global__ void k_hs_greedy(float *snr_out, uint16_t *harm_out, const float *__restrict__ d, const float *msd,
-                            int nT, int nH)
-{
-    const int pos0 = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ float t[PSR_COR_TILE + 4];
     const long long row = static_cast<long long>(blockIdx.y) * nT;
-    float SNR, partial_sum, maxSNR;
-    unsigned short maxHarmonics, maxdata_shift = 0;
-    int data_shift = 0;
-    float data_down = 0, data_step = 0;
-    if (pos0 > 1 && pos0 + 3 < nT)
-        psr_bins<SCAL>(&data_down, &data_step, d, row + pos0);
-    if (data_step > data_down) {
-        data_shift++;
-        partial_sum = data_step;
-    } else {
-        partial_sum = data_down;
-    }
-    maxSNR = fdividef((partial_sum - msd[0]), msd[1]);
-    maxHarmonics = 0;
-    for (int h = 1; h < nH; h++) {
-        const int pos = (h + 1) * pos0 + data_shift;
-        float dd = 0, ds = 0;
-        if (pos > 1 && pos + 3 < nT)
-            psr_bins<SCAL>(&dd, &ds, d, row + pos);
-        if (ds > dd) {
-            data_shift++;
-            partial_sum = partial_sum + ds;
-        } else {
-            partial_sum = partial_sum + dd;
-        }
-        SNR = fdividef((partial_sum - msd[2 * h]), msd[2 * h + 1]);
-        if (SNR > maxSNR) {
-            maxSNR = SNR;
-            maxHarmonics = h;
-            maxdata_shift = data_shift;
-        }
-    }
-    if (pos0 < nT) {
-        snr_out[row + pos0] = maxSNR;
-        harm_out[row + pos0] = static_cast<uint16_t>(maxHarmonics + maxdata_shift * 100);
-    }
-}
-
-// PRESTO plus: harmonic i+1 sums the bins round(f * pos / (i + 1)), f = 1..i,
-// onto the fundamental; the reported count is i - 1, as in the reference
-template <bool SCAL>
-__global__ void k_hs_presto_plus(float *snr_out, uint16_t *harm_out, const float *__restrict__ d, const float *msd,
-                                 int nT, int nH)
-{
-    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
-    const long long row = static_cast<long long>(blockIdx.y) * nT;
-    float SNR, partial_sum, maxSNR, frequency_bin, fundamental = 0;
-    int maxHarmonics;
-    if ((pos > 1) && (pos + 2) < nT)
-        psr_bin_value<SCAL>(&fundamental, d, row + pos);
-    partial_sum = fundamental;
-    maxSNR = fdividef((partial_sum - msd[0]), msd[1]);
-    maxHarmonics = 0;
-    if (pos > 1 && (pos + 2) < nT) {
-        for (int i = 1; i < nH; i++) {
-            partial_sum = fundamental;
-            const double fundamental_fraction = ((double)pos) / ((double)(i + 1));
-            for (int f = 1; f <= i; f++) {
-                const int new_pos = (int)((((double)f) * fundamental_fraction) + 0.5);
-                frequency_bin = 0;
-                if (new_pos > 1 && (new_pos + 2) < nT)
-                    psr_bin_value<SCAL>(&frequency_bin, d, row + new_pos);
-                partial_sum = partial_sum + frequency_bin;
-            }
-            SNR = fdividef((partial_sum - msd[2 * i]), msd[2 * i + 1]);
-            if (SNR > maxSNR) {
-                maxSNR = SNR;
-                maxHarmonics = i - 1;
-            }
-        }
-    }
-    if (pos < nT) {
-        snr_out[row + pos] = maxSNR;
-        harm_out[row + pos] = static_cast<uint16_t>(maxHarmonics);
-    }
-}
-
-// PRESTO: sums of 1, 2, 4, ... 2^(factor-1) harmonics (factor =
-// floor(log2(nHarmonics)) + 1), the even multiples of a fundamental at
-// round(pos / harm)
-template <bool SCAL>
-__global__ void k_hs_presto(float *snr_out, uint16_t *harm_out, const float *__restrict__ d, const float *msd, int nT,
-                            int nHarmonicsFactor)
-{
-    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
-    const long long row = static_cast<long long>(blockIdx.y) * nT;
-    float SNR, partial_sum, maxSNR = -10000, frequency_bin, fundamental;
-    int maxHarmonics = 0;
-    for (int i = 0; i < nHarmonicsFactor; i++) {
-        const int harm = (1 << i);
-        const float fundamental_frac = ((double)pos) * (1.0 / ((double)harm));
-        const int fundamental_pos = (int)(fundamental_frac + 0.5);
-        fundamental = 0;
-        if (fundamental_pos > 1 && (fundamental_pos + 2) < nT)
-            psr_bin_value<SCAL>(&fundamental, d, row + fundamental_pos);
-        partial_sum = fundamental;
-        for (int f = 2; f <= harm; f = f + 2) {
-            const int new_pos = (int)(((float)f) * fundamental_frac + 0.5);
-            frequency_bin = 0;
-            if (new_pos > 1 && (new_pos + 2) < nT)
-                psr_bin_value<SCAL>(&frequency_bin, d, row + new_pos);
-            partial_sum = partial_sum + frequency_bin;
-        }
-        SNR = fdividef((partial_sum - msd[2 * (harm / 2)]), msd[2 * (harm / 2) + 1]);
-        if (SNR > maxSNR) {
-            maxSNR = SNR;
-            maxHarmonics = harm - 1;
-        }
-    }
-    if (pos < nT) {
-        snr_out[row + pos] = maxSNR;
-        harm_out[row + pos] = static_cast<uint16_t>(maxHarmonics);
-    }
-}
-
-// Spectral whitening, segment medians
-// (src/aa_device_spectral_whitening_kernel.cu:338-376): the median of the
-// powers |X|^2 of one segment (at most 256 bins), sorted in shared memory
-// with zeros padding the 256 slots; an even count averages the sorted
-// values at count/2 and count/2 + 1, as the reference does.
-constexpr int PSR_SEG_SLOTS = 256;
-
-__global__ void __launch_bounds__(PSR_SEG_SLOTS / 2) k_segment_medians(float *medians, const float2 *__restrict__ in,
-                                                                         const int *__restrict__ seg, long long nSamples,
-                                                                         int nSegments)
-{
-    __shared__ float v[PSR_SEG_SLOTS];
-    const int t = threadIdx.x;
-    const int start = seg[blockIdx.x], end = seg[blockIdx.x + 1];
-    const int range = end - start;
-    // Powers are >= 0 and the pads are zeros, so the sorted slots hold the
-    // pads first and slot pads + k is the k-th smallest power for any pad
-    // count: the smallest power of two (64 .. 256) above the segment sorts
-    // to the same median as the reference's 256 slots.
-    const int slots = range <= 64 ? 64 : (range <= 128 ? 128 : PSR_SEG_SLOTS);
-    const long long row = static_cast<long long>(blockIdx.y) * nSamples;
-    for (int k = t; k < slots; k += blockDim.x) {
-        float p = 0;
-        const long long pos = start + k;
-        if (k < range && pos < nSamples) {
-            const float2 value = in[row + pos];
-            p = value.x * value.x + value.y * value.y;
-        }
-        v[k] = p;
+    const int k0 = blockIdx.x * PSR_COR_TILE;
+    for (int i = threadIdx.x; i < PSR_COR_TILE + 4; i += blockDim.x) {
+        const int k = k0 - 2 + i;
+        t[i] = (k >= 0 && k < nT) ? in[row + k] : 0.f;
     }
     __syncthreads();
-    // bitonic sort, ascending (slots is block-uniform)
-    for (int size = 2; size <= slots; size <<= 1) {
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int k = t; k < slots / 2; k += blockDim.x) {
-                const int lo = 2 * k - (k & (stride - 1));
-                const int hi = lo + stride;
-                const bool ascending = (lo & size) == 0;
-                const float a = v[lo], b = v[hi];
-                if ((a > b) == ascending) {
-                    v[lo] = b;
-                    v[hi] = a;
-                }
-            }
-            __syncthreads();
-        }
-    }
-    if (t == 0) {
-        const int nZeros = slots - range;
-        const int median_pos = nZeros + (range >> 1);
-        float median;
-        if ((range & 1) == 0)
-            // a segment of two bins puts median_pos + 1 past the slots
-            // (the reference reads past its shared array there): the
-            // largest slot stands in
-            median = (v[median_pos] + v[min(median_pos + 1, slots - 1)]) * 0.5f;
-        else
-            median = v[median_pos];
-        medians[static_cast<long long>(blockIdx.y) * nSegments + blockIdx.x] = median;
-    }
+    const int k = k0 + threadIdx.x;
+    if (k >= nT)
+        return;
+    const float *w = t + threadIdx.x; // w[2] is bin k
+    out[row + k] = (k >= 2 && k + 2 < nT) ? psr_corrected(w[0], w[1], w[2], w[3], w[4]) : 0.f;
 }
 
-// Spectral whitening (src/aa_device_spectral_whitening_kernel.cu:378-427):
-// the first half segment divided by the square root of its median (scaled
-// by 1/ln 2), bin 0 set to 1; later bins by a linear interpolation of the
-// scaled medians between segment middles, in the reference's mixed
-// float/double expressions.  Block b (b >= 1) covers the bins from the
-// middle of segment b-1 to the middle of segment b; the last block also the
-// bins after the middle of the last segment, with the norms of its threads
-// (interpolation indices range - t, as the reference computes them).
-__global__ void k_whitening_sgp2(const float *__restrict__ medians, float2 *in, const int *__restrict__ seg,
-                                 long long nSamples, int nSegments)
+// nH: harmonics (greedy, PRESTO plus) or powers of two (PRESTO); n_msd:
+// entries of the (mean, deviation) table, at most 2 * PSR_MAX_HARMONICS
+template <int ALG>
+__global__ void __launch_bounds__(256) k_harmonic_rows(const float *__restrict__ v, float *snr_out,
+                                                       uint16_t *harm_out, const float *__restrict__ msd, int nT,
+                                                       int nH, int n_msd)
 {
-    const long long rowm = static_cast<long long>(blockIdx.y) * nSegments;
-    if (blockIdx.x == 0) {
-        const int f0_pos = seg[0];
-        const int fp1_pos = seg[1];
-        const int current_range = fp1_pos - f0_pos;
-        const float current_mean = medians[rowm + blockIdx.x] * 1.44269504088896;
-        const float norm = 1.0 / sqrt(current_mean);
-        const long long global_pos = static_cast<long long>(blockIdx.y) * nSamples + threadIdx.x;
-        if (static_cast<int>(threadIdx.x) < (current_range >> 1)) {
-            in[global_pos].x *= norm;
-            in[global_pos].y *= norm;
+    __shared__ float s_msd[2 * PSR_MAX_HARMONICS];
+    for (int i = threadIdx.x; i < n_msd; i += blockDim.x)
+        s_msd[i] = msd[i];
+    __syncthreads();
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= nT)
+        return;
+    const float *rv = v + static_cast<long long>(blockIdx.y) * nT;
+    auto bin = [&](int k, int hi) -> float { return (k > 1 && k + hi < nT) ? __ldg(rv + k) : 0.f; };
+    float best;
+    int out_h;
+    if (ALG == 1) {
+        // greedy: at each harmonic the larger of bins p and p+1, p = (h+1) pos
+        // + the steps taken so far; the count plus 100 x the steps at the best
+        int steps = 0, best_h = 0, best_steps = 0;
+        float lo = 0.f, hi = 0.f;
+        if (pos > 1 && pos + 3 < nT) {
+            lo = __ldg(rv + pos);
+            hi = __ldg(rv + pos + 1);
         }
-        if (threadIdx.x == 0) {
-            in[global_pos].x = 1.0;
-            in[global_pos].y = 0.0;
+        float sum;
+        if (hi > lo) {
+            ++steps;
+            sum = hi;
+        } else {
+            sum = lo;
+        }
+        best = fdividef((sum - s_msd[0]), s_msd[1]);
+        for (int h = 1; h < nH; ++h) {
+            const int p = (h + 1) * pos + steps;
+            lo = hi = 0.f;
+            if (p > 1 && p + 3 < nT) {
+                lo = __ldg(rv + p);
+                hi = __ldg(rv + p + 1);
+            }
+            if (hi > lo) {
+                ++steps;
+                sum = sum + hi;
+            } else {
+                sum = sum + lo;
+            }
+            const float snr = fdividef((sum - s_msd[2 * h]), s_msd[2 * h + 1]);
+            if (snr > best) {
+                best = snr;
+                best_h = h;
+                best_steps = steps;
+            }
+        }
+        out_h = best_h + 100 * best_steps;
+    } else if (ALG == 2) {
+        // PRESTO plus: count i sums the fundamental and bins round(f pos / (i+1)),
+        // f = 1..i; reported as i - 1
+        const float fund = bin(pos, 2);
+        best = fdividef((fund - s_msd[0]), s_msd[1]);
+        out_h = 0;
+        if (pos > 1 && pos + 2 < nT) {
+            for (int i = 1; i < nH; ++i) {
+                float sum = fund;
+                const double frac = ((double)pos) / ((double)(i + 1));
+                for (int f = 1; f <= i; ++f)
+                    sum = sum + bin((int)((((double)f) * frac) + 0.5), 2);
+                const float snr = fdividef((sum - s_msd[2 * i]), s_msd[2 * i + 1]);
+                if (snr > best) {
+                    best = snr;
+                    out_h = i - 1;
+                }
+            }
         }
     } else {
-        const int fm1_pos = seg[blockIdx.x - 1];
-        const int f0_pos = seg[blockIdx.x + 0];
-        const int fp1_pos = seg[blockIdx.x + 1];
-        const int previous_range = f0_pos - fm1_pos;
-        const int current_range = fp1_pos - f0_pos;
-        const float previous_mean = medians[rowm + blockIdx.x - 1] * 1.44269504088896;
-        const float current_mean = medians[rowm + blockIdx.x] * 1.44269504088896;
-        const int range = ((previous_range + current_range + 1) >> 1);
-        const int i = range - threadIdx.x;
-        const float slope = (current_mean - previous_mean) / ((float)range);
-        const float norm = 1.0 / sqrt(previous_mean + slope * i);
-        const int local_pos = fm1_pos + (previous_range >> 1) + i;
-        // an even previous and an odd current segment make this block's
-        // last bin the next block's first (the middle of the current
-        // segment); the reference scales it in both blocks without
-        // ordering, here only the next block scales it, once
-        const bool shared_last = blockIdx.x + 1 < gridDim.x && (previous_range & 1) == 0 && (current_range & 1) == 1;
-        if (i >= 0 && i < range - (shared_last ? 1 : 0) && local_pos < nSamples) {
-            const long long global_pos = static_cast<long long>(blockIdx.y) * nSamples + local_pos;
-            in[global_pos].x *= norm;
-            in[global_pos].y *= norm;
+        // PRESTO: for 1, 2, 4, ... harmonics (nH here is the count of
+        // powers of two) the fundamental at round(pos / n) plus its even
+        // multiples
+        best = -10000;
+        out_h = 0;
+        for (int i = 0; i < nH; ++i) {
+            const int n = 1 << i;
+            const float frac = ((double)pos) * (1.0 / ((double)n));
+            float sum = bin((int)(frac + 0.5), 2);
+            for (int f = 2; f <= n; f += 2)
+                sum = sum + bin((int)(((float)f) * frac + 0.5), 2);
+            const float snr = fdividef((sum - s_msd[2 * (n / 2)]), s_msd[2 * (n / 2) + 1]);
+            if (snr > best) {
+                best = snr;
+                out_h = n - 1;
+            }
         }
-        if (blockIdx.x == (gridDim.x - 1)) {
-            const int tail = fm1_pos + (previous_range >> 1) + range + threadIdx.x;
+    }
+    const long long o = static_cast<long long>(blockIdx.y) * nT + pos;
+    snr_out[o] = best;
+    harm_out[o] = static_cast<uint16_t>(out_h);
+}
+
+// ---------------------------------------------------------------------------
+// Spectral whitening (src/aa_device_spectral_whitening_kernel.cu:338-427
+// defines the medians and the SGP2 normalisation).
+//
+// Medians: one warp per (segment, spectrum).  The segment's powers |X|^2 (at
+// most 256 bins) fill 32 x V registers of the warp (element e = 32 v + lane,
+// slots past the segment hold +inf) and a bitonic network sorts them: pairs
+// 32 or more elements apart exchange inside a lane's registers, nearer pairs
+// across lanes by shuffles.  The median is the sorted power at range/2 (odd
+// range) or the mean of those at range/2 and range/2 + 1 (even range; a
+// two-bin segment takes its largest power for the second), which is the
+// reference's choice on its zero-padded 256-slot sort.
+// ---------------------------------------------------------------------------
+constexpr int PSR_WARPS_PER_BLOCK = 8;
+constexpr int PSR_MAX_SEGMENT = 256;
+
+template <int V>
+__device__ float psr_segment_median(const float2 *__restrict__ spec, int start, int range, long long nSamples)
+{
+    const int lane = threadIdx.x & 31;
+    float x[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const int e = 32 * v + lane;
+        x[v] = INFINITY;
+        if (e < range && start + e < nSamples) {
+            const float2 q = spec[start + e];
+            x[v] = q.x * q.x + q.y * q.y;
+        }
+    }
+#pragma unroll
+    for (int size = 2; size <= 32 * V; size <<= 1) {
+#pragma unroll
+        for (int j = size >> 1; j > 0; j >>= 1) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const int e = 32 * v + lane;
+                const bool keep_min = ((e & j) == 0) == ((e & size) == 0);
+                float other;
+                if (j >= 32) {
+                    const int pv = v ^ (j >> 5);
+                    if (pv < v)
+                        continue; // the pair (pv, v) was handled at pv
+                    other = x[pv];
+                    const float lo = fminf(x[v], other), hi = fmaxf(x[v], other);
+                    x[v] = keep_min ? lo : hi;
+                    x[pv] = keep_min ? hi : lo;
+                } else {
+                    other = __shfl_xor_sync(0xffffffffu, x[v], j);
+                    x[v] = keep_min ? fminf(x[v], other) : fmaxf(x[v], other);
+                }
+            }
+        }
+    }
+    auto rank = [&](int r) {
+        float t = x[0];
+#pragma unroll
+        for (int v = 1; v < V; ++v)
+            if ((r >> 5) == v)
+                t = x[v];
+        return __shfl_sync(0xffffffffu, t, r & 31);
+    };
+    const int mid = range >> 1;
+    if (range & 1)
+        return rank(mid);
+    return (rank(mid) + rank(min(mid + 1, range - 1))) * 0.5f;
+}
+
+// segments of at most PSR_MAX_SEGMENT bins (psr_whitening checks the table)
+__global__ void __launch_bounds__(32 * PSR_WARPS_PER_BLOCK) k_segment_medians_warp(float *medians,
+                                                                                 const float2 *__restrict__ in,
+                                                                                 const int *__restrict__ seg,
+                                                                                 long long nSamples, int nSegments)
+{
+    const int m = blockIdx.x * PSR_WARPS_PER_BLOCK + (threadIdx.x >> 5);
+    if (m >= nSegments - 1)
+        return;
+    const int start = seg[m], range = seg[m + 1] - start;
+    const float2 *spec = in + static_cast<long long>(blockIdx.y) * nSamples;
+    float med;
+    if (range <= 32)
+        med = psr_segment_median<1>(spec, start, range, nSamples);
+    else if (range <= 64)
+        med = psr_segment_median<2>(spec, start, range, nSamples);
+    else if (range <= 128)
+        med = psr_segment_median<4>(spec, start, range, nSamples);
+    else
+        med = psr_segment_median<8>(spec, start, range, nSamples);
+    if ((threadIdx.x & 31) == 0)
+        medians[static_cast<long long>(blockIdx.y) * nSegments + m] = med;
+}
+
+// ---------------------------------------------------------------------------
+// SGP2 normalisation: one warp per interpolation span b of one spectrum.
+// Span 0 scales the first half of segment 0 by 1/sqrt(its median / ln 2)
+// and sets bin 0 to (1, 0); span b >= 1 covers the bins from the middle of
+// segment b-1 to the middle of segment b, each scaled by 1/sqrt of the
+// medians interpolated linearly at its offset i, in the reference's mixed
+// float/double expressions.  The last span also scales the 256 bins after
+// the last middle with the norms at offsets range - t (t = 0..255), as the
+// reference's last block does with its 256 threads.  When an even segment
+// meets an odd one, the span's last bin is the next span's first: only the
+// next span scales it (the reference scales it in both, unordered).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float psr_scaled_median(float m) { return m * 1.44269504088896; }
+
+__global__ void __launch_bounds__(32 * PSR_WARPS_PER_BLOCK) k_sgp2_spans(const float *__restrict__ medians, float2 *in,
+                                                                       const int *__restrict__ seg,
+                                                                       long long nSamples, int nSegments)
+{
+    const int b = blockIdx.x * PSR_WARPS_PER_BLOCK + (threadIdx.x >> 5);
+    const int nspans = nSegments - 1;
+    if (b >= nspans)
+        return;
+    const int lane = threadIdx.x & 31;
+    const float *med = medians + static_cast<long long>(blockIdx.y) * nSegments;
+    float2 *spec = in + static_cast<long long>(blockIdx.y) * nSamples;
+    auto scale = [&](long long pos, float norm) {
+        float2 q = spec[pos];
+        q.x *= norm;
+        q.y *= norm;
+        spec[pos] = q;
+    };
+    if (b == 0) {
+        const int current_range = seg[1] - seg[0];
+        const float current_mean = psr_scaled_median(med[0]);
+        const float norm = 1.0 / sqrt(current_mean);
+        for (int t = lane; t < (current_range >> 1); t += 32)
+            scale(t, norm);
+        __syncwarp();
+        if (lane == 0)
+            spec[0] = make_float2(1.0f, 0.0f);
+        return;
+    }
+    const int fm1_pos = seg[b - 1], f0_pos = seg[b], fp1_pos = seg[b + 1];
+    const int previous_range = f0_pos - fm1_pos;
+    const int current_range = fp1_pos - f0_pos;
+    const float previous_mean = psr_scaled_median(med[b - 1]);
+    const float current_mean = psr_scaled_median(med[b]);
+    const int range = ((previous_range + current_range + 1) >> 1);
+    const float slope = (current_mean - previous_mean) / ((float)range);
+    const int first = fm1_pos + (previous_range >> 1);
+    const bool shared_last = b + 1 < nspans && (previous_range & 1) == 0 && (current_range & 1) == 1;
+    const int n = range - (shared_last ? 1 : 0);
+    for (int i = lane; i < n; i += 32) {
+        const int local_pos = first + i;
+        if (local_pos < nSamples) {
+            const float norm = 1.0 / sqrt(previous_mean + slope * i);
+            scale(local_pos, norm);
+        }
+    }
+    if (b == nspans - 1) {
+        for (int t = lane; t < 256; t += 32) {
+            const int tail = first + range + t;
             if (tail < nSamples) {
-                const long long global_pos = static_cast<long long>(blockIdx.y) * nSamples + tail;
-                in[global_pos].x *= norm;
-                in[global_pos].y *= norm;
+                const int i = range - t;
+                const float norm = 1.0 / sqrt(previous_mean + slope * i);
+                scale(tail, norm);
             }
         }
     }
@@ -463,65 +559,118 @@ std::vector<int> psr_segment_sizes(int min_segment_length, int max_segment_lengt
     return s;
 }
 
-// src/aa_device_spectral_whitening.cu:60-118 with enable_median: the
-// boundary table and the nDMs x nSegments medians live in stream-ordered
-// allocations freed on the same stream.
+// The boundary table of a spectrum length, copied to the device once per
+// (device, length) and kept for the process.
+namespace {
+struct SegTable {
+    int *d = nullptr;
+    int n = 0;
+};
+std::mutex g_seg_mutex;
+std::map<std::pair<int, size_t>, SegTable> g_seg_tables;
+} // namespace
+
+// src/aa_device_spectral_whitening.cu:60-118 with enable_median.  The
+// medians live in a stream-ordered scratch allocation freed on the same
+// stream; a boundary table not yet on the device is copied synchronously,
+// which a capturing stream refuses (cudaErrorStreamCaptureUnsupported).
 cudaError_t psr_whitening(float2 *d_spectra, size_t nSamples, int nDMs, cudaStream_t st)
 {
     if (nDMs < 1 || nSamples < 8 || nSamples > static_cast<size_t>(INT32_MAX))
         return cudaErrorInvalidValue;
-    const std::vector<int> segments = psr_segment_sizes(6, 250, nSamples);
-    const int nSegments = static_cast<int>(segments.size());
-    int *d_seg = nullptr;
-    float *d_medians = nullptr;
-    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&d_seg), nSegments * sizeof(int), st);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess)
         return e;
+    SegTable tab;
+    {
+        std::lock_guard<std::mutex> lock(g_seg_mutex);
+        auto it = g_seg_tables.find(std::make_pair(dev, nSamples));
+        if (it != g_seg_tables.end()) {
+            tab = it->second;
+        } else {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            e = cudaStreamIsCapturing(st, &cs);
+            if (e != cudaSuccess)
+                return e;
+            if (cs != cudaStreamCaptureStatusNone)
+                return cudaErrorStreamCaptureUnsupported;
+            const std::vector<int> segments = psr_segment_sizes(6, 250, nSamples);
+            for (size_t i = 0; i + 1 < segments.size(); ++i)
+                if (segments[i + 1] - segments[i] > PSR_MAX_SEGMENT || segments[i + 1] <= segments[i])
+                    return cudaErrorInvalidValue;
+            tab.n = static_cast<int>(segments.size());
+            e = cudaMalloc(reinterpret_cast<void **>(&tab.d), tab.n * sizeof(int));
+            if (e == cudaSuccess)
+                e = cudaMemcpy(tab.d, segments.data(), tab.n * sizeof(int), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                cudaFree(tab.d);
+                return e;
+            }
+            g_seg_tables[std::make_pair(dev, nSamples)] = tab;
+        }
+    }
+    const int nSegments = tab.n;
+    float *d_medians = nullptr;
     e = cudaMallocAsync(reinterpret_cast<void **>(&d_medians), static_cast<size_t>(nSegments) * nDMs * sizeof(float),
                         st);
-    if (e == cudaSuccess)
-        // pageable source: the call returns once the table is staged
-        e = cudaMemcpyAsync(d_seg, segments.data(), nSegments * sizeof(int), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) {
-        k_segment_medians<<<dim3(nSegments - 1, nDMs), PSR_SEG_SLOTS / 2, 0, st>>>(
-            d_medians, d_spectra, d_seg, static_cast<long long>(nSamples), nSegments);
+    if (e != cudaSuccess)
+        return e;
+    const dim3 grid((nSegments - 1 + PSR_WARPS_PER_BLOCK - 1) / PSR_WARPS_PER_BLOCK, nDMs);
+    {
+        k_segment_medians_warp<<<grid, 32 * PSR_WARPS_PER_BLOCK, 0, st>>>(
+            d_medians, d_spectra, tab.d, static_cast<long long>(nSamples), nSegments);
         ++g_psr_launches;
-        // blocks 0 .. nSegments-2: the reference launches one block more,
+        // spans 0 .. nSegments-2: the reference launches one block more,
         // which reads the boundary past the table and the median slot its
         // median kernel never writes, and for any table value below
         // nSamples - (last segment) writes nothing
-        k_whitening_sgp2<<<dim3(nSegments - 1, nDMs), 256, 0, st>>>(d_medians, d_spectra, d_seg,
-                                                                   static_cast<long long>(nSamples), nSegments);
+        k_sgp2_spans<<<grid, 32 * PSR_WARPS_PER_BLOCK, 0, st>>>(d_medians, d_spectra, tab.d,
+                                                                static_cast<long long>(nSamples), nSegments);
         ++g_psr_launches;
         e = cudaGetLastError();
     }
-    if (d_medians)
-        cudaFreeAsync(d_medians, st);
-    cudaFreeAsync(d_seg, st);
+    cudaFreeAsync(d_medians, st);
     return e;
 }
 
-// src/aa_device_harmonic_summing.cu:38-169
+// src/aa_device_harmonic_summing.cu:38-169: which algorithm, the PRESTO
+// count of powers of two; the scalloping-corrected plane is a stream-ordered
+// scratch allocation freed on the same stream
 cudaError_t psr_harmonic_sum(int algorithm, const float *d_input, float *d_snr, uint16_t *d_harmonics,
                              const float *d_msd, int nTimesamples, int nDMs, int nHarmonics, bool scalloping,
                              cudaStream_t st)
 {
-    if (nTimesamples < 1 || nDMs < 1 || nHarmonics < 1 || nHarmonics > 32)
+    if (nTimesamples < 1 || nDMs < 1 || nHarmonics < 1 || nHarmonics > PSR_MAX_HARMONICS || algorithm < 1 ||
+        algorithm > 3)
         return cudaErrorInvalidValue;
     // PRESTO sums 1, 2, 4, ... harmonics: src/aa_device_harmonic_summing.cu:143
     const int factor = static_cast<int>(std::log(static_cast<double>(nHarmonics)) / std::log(2.0)) + 1;
+    const float *src = d_input;
+    float *d_cor = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (scalloping) {
+        e = cudaMallocAsync(reinterpret_cast<void **>(&d_cor),
+                            static_cast<size_t>(nTimesamples) * static_cast<size_t>(nDMs) * sizeof(float), st);
+        if (e != cudaSuccess)
+            return e;
+        k_scalloping_corrected<<<dim3((nTimesamples + PSR_COR_TILE - 1) / PSR_COR_TILE, nDMs), PSR_COR_TILE, 0, st>>>(
+            d_input, d_cor, nTimesamples);
+        ++g_psr_launches;
+        src = d_cor;
+    }
     const dim3 grid((nTimesamples + 255) / 256, nDMs);
-    switch (algorithm * 2 + (scalloping ? 1 : 0)) {
-    case 2: k_hs_greedy<false><<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_input, d_msd, nTimesamples, nHarmonics); break;
-    case 3: k_hs_greedy<true><<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_input, d_msd, nTimesamples, nHarmonics); break;
-    case 4: k_hs_presto_plus<false><<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_input, d_msd, nTimesamples, nHarmonics); break;
-    case 5: k_hs_presto_plus<true><<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_input, d_msd, nTimesamples, nHarmonics); break;
-    case 6: k_hs_presto<false><<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_input, d_msd, nTimesamples, factor); break;
-    case 7: k_hs_presto<true><<<grid, 256, 0, st>>>(d_snr, d_harmonics, d_input, d_msd, nTimesamples, factor); break;
-    default: return cudaErrorInvalidValue;
+    const int nh = (algorithm == 3) ? factor : nHarmonics;
+    switch (algorithm) {
+    case 1: k_harmonic_rows<1><<<grid, 256, 0, st>>>(src, d_snr, d_harmonics, d_msd, nTimesamples, nh, 2 * nHarmonics); break;
+    case 2: k_harmonic_rows<2><<<grid, 256, 0, st>>>(src, d_snr, d_harmonics, d_msd, nTimesamples, nh, 2 * nHarmonics); break;
+    default: k_harmonic_rows<3><<<grid, 256, 0, st>>>(src, d_snr, d_harmonics, d_msd, nTimesamples, nh, 2 * nHarmonics); break;
     }
     ++g_psr_launches;
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    if (d_cor)
+        cudaFreeAsync(d_cor, st);
+    return e;
 }
 
 // src/aa_device_threshold.cu:56-163 (transposed and normal planes)
@@ -565,9 +714,14 @@ cudaError_t psr_power_interbin(const float2 *d_in, float *d_power, float *d_inte
     const int half = nTimesamples >> 1;
     if (half < 1 || nDMs < 1)
         return cudaErrorInvalidValue;
-    const dim3 grid((half + PSR_PAI_THREADS - 1) / PSR_PAI_THREADS, nDMs);
+    const int pairs = (half + 1) / 2;
+    const dim3 grid((pairs + PSR_PAIR_THREADS - 1) / PSR_PAIR_THREADS, nDMs);
     const float norm = static_cast<float>(std::sqrt(static_cast<double>(nTimesamples)));
-    k_power_interbin<<<grid, PSR_PAI_THREADS, 0, st>>>(d_in, d_power, d_interbin, nTimesamples, norm);
+    const bool vec4 = (nTimesamples % 4) == 0 && (reinterpret_cast<uintptr_t>(d_interbin) & 15) == 0;
+    if (vec4)
+        k_power_pairs<true><<<grid, PSR_PAIR_THREADS, 0, st>>>(d_in, d_power, d_interbin, nTimesamples, norm);
+    else
+        k_power_pairs<false><<<grid, PSR_PAIR_THREADS, 0, st>>>(d_in, d_power, d_interbin, nTimesamples, norm);
     ++g_psr_launches;
     return cudaGetLastError();
 }
@@ -576,11 +730,17 @@ cudaError_t psr_power_interbin(const float2 *d_in, float *d_power, float *d_inte
 cudaError_t psr_harmonic_sum_simple(const float *d_in, float *d_snr, uint16_t *d_harmonics, const float *d_msd,
                                     int nBins, int nSpectra, int nHarmonics, cudaStream_t st)
 {
-    if (nBins < 1 || nSpectra < 1 || nHarmonics < 1)
+    if (nBins < 1 || nSpectra < 1 || nHarmonics < 1 || nHarmonics > PSR_MAX_HARMONICS)
         return cudaErrorInvalidValue;
-    const dim3 grid(nBins, (nSpectra + PSR_PHS_THREADS - 1) / PSR_PHS_THREADS);
-    k_harmonic_sum_simple<<<grid, PSR_PHS_THREADS, 0, st>>>(d_in, d_snr, d_harmonics, d_msd, nBins, nSpectra,
-                                                            nHarmonics);
+    const bool vec4 = (nSpectra % 4) == 0 && (reinterpret_cast<uintptr_t>(d_in) & 15) == 0;
+    const int per = vec4 ? 4 : 1;
+    const dim3 grid(nBins, (nSpectra / per + PSR_HS_THREADS - 1) / PSR_HS_THREADS);
+    if (vec4)
+        k_harmonic_columns<4><<<grid, PSR_HS_THREADS, 0, st>>>(d_in, d_snr, d_harmonics, d_msd, nBins, nSpectra,
+                                                              nHarmonics);
+    else
+        k_harmonic_columns<1><<<grid, PSR_HS_THREADS, 0, st>>>(d_in, d_snr, d_harmonics, d_msd, nBins, nSpectra,
+                                                              nHarmonics);
     ++g_psr_launches;
     return cudaGetLastError();
 }

@@ -496,244 +496,166 @@ __global__ void k_msd_interpolate(const float *__restrict__ dit, float *__restri
 }
 
 // ---------------------------------------------------------------------------
-// Boxcar S/N planes (src/aa_device_SPS_long_kernel.cu:42-168 and :170-283).
-// A block of 512 threads covers 2*512 - nBoxcars samples of one DM trial,
-// two per thread.  Thread t holds the sums of 1..4 samples starting at its
-// two samples (Bw[0..3] from sample 2t, Bw[4..7] from 2t+1); a boxcar of
-// width d+1..d+4 adds the 4-sample sum of thread t + d/2 - ... exchanged
-// through shared memory, so thread t at step d updates the best S/N of
-// thread t - d/2.  S/N = (sum - mean_w) / sd_w with the fast division; the
-// width of the best S/N is kept with it.  Each plane also writes the
-// 2-sample sums (the next iteration's input at half resolution) and the
-// 4-sample sums at half resolution (the running boxcar values).
+// Boxcar S/N planes: for every start sample u of a DM trial and every width
+// w = 1..nBoxcars the boxcar sum B(u, w), its S/N and the best S/N over w with
+// its width; plus the half-resolution pair sums (the next iteration's input)
+// and the full-width boxcar values at even starts (the next iteration's
+// running values).  src/aa_device_SPS_long_kernel.cu:42-283 defines what is
+// computed; the association of every sum and the order of every comparison
+// below reproduce its values bit for bit:
+//   * w = 4q + k + 1 (k = 0..3): B(u, w) = P_k(u + 4q) + S4(u + 4q - 4) + ...
+//     + S4(u), added left to right, where P_k(v) = ((x[v] + x[v+1]) + x[v+2])
+//     + x[v+3] truncated to k+1 terms and S4 = P_3; a pair of samples (2p,
+//     2p+1) whose even sample has fewer than 4 samples after it counts as
+//     zeros;
+//   * S/N = (B - mean_w) / sd_w (later iterations: (bv(u) + (B - mean_w)) /
+//     sd_w with the running value bv at the start) by the fast division;
+//   * per q the best of its four widths (a later width only when strictly
+//     better, the pair of pairs likewise), at q = 0 the second pair on a
+//     tie; over q a later group only when strictly better.
+//
+// Design: one warp per window of 128 consecutive positions v of one DM
+// trial, four consecutive positions per lane.  The sum for start u and group
+// q is built by the lane holding v = u + 4q: it starts from P_k(v) and adds
+// S4(v - 4), S4(v - 8), ... one group per step, the S4 of the lane q places
+// below arriving by a shuffle; the group's best S/N then moves down q lanes
+// by a shuffle to the lane that owns u, which folds it into its running
+// best.  No shared memory and no block barrier; a window yields 128 - 4(Q-1)
+// starts (Q = nBoxcars / 4), its last Q-1 lanes only feed the others.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float snr_of(float bw, float2 st) { return __fdividef(bw - st.x, st.y); }
+constexpr int SNR_WARPS = 8;
 
-__device__ __forceinline__ float snr_of_bv(float bv, float bw, float2 st) { return __fdividef(bv + (bw - st.x), st.y); }
-
-template <int nBoxcars>
-__global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_first(const float *__restrict__ in, float *bv_out, float *dec,
-                                                             float *snr_out, uint16_t *taps_out, const SnrMsd msd,
-                                                             int nT, int dtm)
+template <int NB, bool NTH>
+__global__ void __launch_bounds__(32 * SNR_WARPS) k_boxcar_snr(const float *__restrict__ in,
+                                                               const float *__restrict__ bv_in, float *bv_out,
+                                                               float *dec, float *snr_out, uint16_t *taps_out,
+                                                               const SnrMsd msd, int nT, int startTaps,
+                                                               int dit_value, int dtm)
 {
-    __shared__ float2 s_in[SPD_NTHREADS];
-    __shared__ float2 s_snr[SPD_NTHREADS];
-    __shared__ ushort2 s_taps[SPD_NTHREADS];
-    const int t = threadIdx.x;
-    float Bw[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    float2 f1, f2, f3, SNR = make_float2(0, 0);
-    ushort2 taps, taps1, taps2;
-    int spos = blockIdx.x * (2 * SPD_NTHREADS - nBoxcars) + 2 * t;
+    constexpr int Q = NB / 4;
+    constexpr int OUT = 128 - 4 * (Q - 1); // starts per window
+    const int lane = threadIdx.x & 31;
+    const long long window = static_cast<long long>(blockIdx.x) * SNR_WARPS + (threadIdx.x >> 5);
+    const long long wbase = window * OUT;
+    if (wbase >= nT)
+        return;
     const long long row = static_cast<long long>(blockIdx.y) * nT;
-    if ((spos + 4) < nT) {
-        const long long g = row + spos;
-        f1.x = in[g];
-        f1.y = in[g + 1];
-        f2.x = in[g + 2];
-        f2.y = in[g + 3];
-        f3.x = in[g + 4];
-        Bw[0] = f1.x;
-        Bw[4] = f1.y;
-        Bw[1] = f1.x + f1.y;
-        Bw[5] = f1.y + f2.x;
-        Bw[2] = Bw[1] + f2.x;
-        Bw[6] = Bw[5] + f2.y;
-        Bw[3] = Bw[1] + f2.x + f2.y;
-        Bw[7] = Bw[5] + f2.y + f3.x;
-    }
-    spos = blockIdx.x * (SPD_NTHREADS - (nBoxcars >> 1)) + t;
-    if (t < (SPD_NTHREADS - (nBoxcars >> 1)) && spos < dtm)
-        dec[static_cast<long long>(blockIdx.y) * dtm + spos] = Bw[1];
-    s_in[t].x = Bw[3];
-    s_in[t].y = Bw[7];
-    __syncthreads();
-    float2 st = msd.v[0];
-    f1.x = snr_of(Bw[0], st);
-    f1.y = snr_of(Bw[4], st);
-    st = msd.v[1];
-    f2.x = snr_of(Bw[1], st);
-    f2.y = snr_of(Bw[5], st);
-    if (f2.x > f1.x) { f1.x = f2.x; taps1.x = 2; } else taps1.x = 1;
-    if (f2.y > f1.y) { f1.y = f2.y; taps1.y = 2; } else taps1.y = 1;
-    st = msd.v[2];
-    f2.x = snr_of(Bw[2], st);
-    f2.y = snr_of(Bw[6], st);
-    st = msd.v[3];
-    f3.x = snr_of(Bw[3], st);
-    f3.y = snr_of(Bw[7], st);
-    if (f3.x > f2.x) { f2.x = f3.x; taps2.x = 4; } else taps2.x = 3;
-    if (f3.y > f2.y) { f2.y = f3.y; taps2.y = 4; } else taps2.y = 3;
-    if (f1.x > f2.x) { SNR.x = f1.x; taps.x = taps1.x; } else { SNR.x = f2.x; taps.x = taps2.x; }
-    if (f1.y > f2.y) { SNR.y = f1.y; taps.y = taps1.y; } else { SNR.y = f2.y; taps.y = taps2.y; }
-    s_snr[t] = SNR;
-    s_taps[t] = taps;
+    const float *x = in + row;
+    const long long v0 = wbase + 4 * lane; // this lane's first position
+
+    // samples v0 .. v0+6 (the last three from the next lane)
+    float xs[7];
 #pragma unroll
-    for (int d = 4; d < nBoxcars; d += 4) {
-        __syncthreads();
-        spos = t - (d >> 1);
-        if (spos >= 0) {
-            f1 = s_in[spos];
-            SNR = s_snr[spos];
-            taps = s_taps[spos];
-            Bw[0] = Bw[0] + f1.x; Bw[4] = Bw[4] + f1.y;
-            Bw[1] = Bw[1] + f1.x; Bw[5] = Bw[5] + f1.y;
-            Bw[2] = Bw[2] + f1.x; Bw[6] = Bw[6] + f1.y;
-            Bw[3] = Bw[3] + f1.x; Bw[7] = Bw[7] + f1.y;
-            st = msd.v[d];
-            f1.x = snr_of(Bw[0], st);
-            f1.y = snr_of(Bw[4], st);
-            st = msd.v[d + 1];
-            f2.x = snr_of(Bw[1], st);
-            f2.y = snr_of(Bw[5], st);
-            if (f2.x > f1.x) { f1.x = f2.x; taps1.x = d + 2; } else taps1.x = d + 1;
-            if (f2.y > f1.y) { f1.y = f2.y; taps1.y = d + 2; } else taps1.y = d + 1;
-            st = msd.v[d + 2];
-            f2.x = snr_of(Bw[2], st);
-            f2.y = snr_of(Bw[6], st);
-            st = msd.v[d + 3];
-            f3.x = snr_of(Bw[3], st);
-            f3.y = snr_of(Bw[7], st);
-            if (f3.x > f2.x) { f2.x = f3.x; taps2.x = d + 4; } else taps2.x = d + 3;
-            if (f3.y > f2.y) { f2.y = f3.y; taps2.y = d + 4; } else taps2.y = d + 3;
-            if (f2.x > f1.x) { f1.x = f2.x; taps1.x = taps2.x; }
-            if (f2.y > f1.y) { f1.y = f2.y; taps1.y = taps2.y; }
-            if (f1.x > SNR.x) { SNR.x = f1.x; taps.x = taps1.x; }
-            if (f1.y > SNR.y) { SNR.y = f1.y; taps.y = taps1.y; }
-            s_snr[spos] = SNR;
-            s_taps[spos] = taps;
+    for (int j = 0; j < 4; ++j)
+        xs[j] = (v0 + j < nT) ? __ldg(x + v0 + j) : 0.f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const float nx = __shfl_down_sync(0xffffffffu, xs[j], 1);
+        xs[4 + j] = (lane == 31) ? ((v0 + 4 + j < nT) ? __ldg(x + v0 + 4 + j) : 0.f) : nx;
+    }
+    // partial sums P_k(v) of the four positions; zeros for pairs without
+    // four samples after their even sample
+    float acc[4][4], s4[4], bv[4], pair[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const long long v = v0 + p;
+        const bool ok = ((v & ~1LL) + 4) < nT;
+        const float a1 = xs[p] + xs[p + 1];
+        const float a2 = a1 + xs[p + 2];
+        const float a3 = a2 + xs[p + 3];
+        acc[p][0] = ok ? xs[p] : 0.f;
+        acc[p][1] = ok ? a1 : 0.f;
+        acc[p][2] = ok ? a2 : 0.f;
+        acc[p][3] = ok ? a3 : 0.f;
+        s4[p] = acc[p][3];
+        pair[p] = acc[p][1];
+        bv[p] = 0.f;
+        if (NTH && ok)
+            bv[p] = __ldg(bv_in + row + v);
+    }
+    auto snr = [&](float b, float bvu, int w) -> float {
+        const float2 st = msd.v[w];
+        return NTH ? __fdividef(bvu + (b - st.x), st.y) : __fdividef(b - st.x, st.y);
+    };
+    float best[4];
+    int taps[4];
+    float full[4]; // B(u, NB) of this lane's starts (bv_out at even starts)
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        float bvq[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            if (q > 0) {
+                const float sv = __shfl_up_sync(0xffffffffu, s4[p], q);
+                acc[p][0] = acc[p][0] + sv;
+                acc[p][1] = acc[p][1] + sv;
+                acc[p][2] = acc[p][2] + sv;
+                acc[p][3] = acc[p][3] + sv;
+            }
+            bvq[p] = NTH ? ((q > 0) ? __shfl_up_sync(0xffffffffu, bv[p], q) : bv[p]) : 0.f;
+        }
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const int d = 4 * q;
+            float f1 = snr(acc[p][0], bvq[p], d);
+            float f2 = snr(acc[p][1], bvq[p], d + 1);
+            int t1, t2;
+            if (f2 > f1) {
+                f1 = f2;
+                t1 = d + 2;
+            } else {
+                t1 = d + 1;
+            }
+            f2 = snr(acc[p][2], bvq[p], d + 2);
+            const float f3 = snr(acc[p][3], bvq[p], d + 3);
+            if (f3 > f2) {
+                f2 = f3;
+                t2 = d + 4;
+            } else {
+                t2 = d + 3;
+            }
+            float c;
+            int ct;
+            if (q == 0) {
+                if (f1 > f2) {
+                    c = f1;
+                    ct = t1;
+                } else {
+                    c = f2;
+                    ct = t2;
+                }
+                best[p] = c;
+                taps[p] = ct;
+            } else {
+                if (f2 > f1) {
+                    f1 = f2;
+                    t1 = t2;
+                }
+                c = __shfl_down_sync(0xffffffffu, f1, q);
+                ct = __shfl_down_sync(0xffffffffu, t1, q);
+                if (c > best[p]) {
+                    best[p] = c;
+                    taps[p] = ct;
+                }
+            }
+            if (q == Q - 1)
+                full[p] = (Q > 1) ? __shfl_down_sync(0xffffffffu, acc[p][3], Q - 1) : acc[p][3];
         }
     }
-    if (spos >= 0)
-        s_in[spos].x = Bw[3];
-    __syncthreads();
-    spos = blockIdx.x * (2 * SPD_NTHREADS - nBoxcars) + 2 * t;
-    if (t < (SPD_NTHREADS - (nBoxcars >> 1)) && spos < nT) {
-        const long long g = row + spos;
-        snr_out[g] = s_snr[t].x;
-        snr_out[g + 1] = s_snr[t].y;
-        taps_out[g] = s_taps[t].x;
-        taps_out[g + 1] = s_taps[t].y;
-        spos = blockIdx.x * (SPD_NTHREADS - (nBoxcars >> 1)) + t;
-        if (spos < dtm)
-            bv_out[static_cast<long long>(blockIdx.y) * dtm + spos] = s_in[t].x;
-    }
-}
-
-// Later iterations: the input is the previous iteration's 2-sample sums, and
-// the running boxcar values of the previous widths (bv_in) are added in front.
-template <int nBoxcars>
-__global__ void __launch_bounds__(SPD_NTHREADS) k_spdt_nth(const float *__restrict__ in, const float *bv_in,
-                                                           float *bv_out, float *dec, float *snr_out,
-                                                           uint16_t *taps_out, const SnrMsd msd, int nT,
-                                                           int startTaps, int dit_value, int dtm)
-{
-    __shared__ float2 s_in[SPD_NTHREADS];
-    __shared__ float2 s_bv[SPD_NTHREADS];
-    __shared__ float2 s_snr[SPD_NTHREADS];
-    __shared__ ushort2 s_taps[SPD_NTHREADS];
-    const int t = threadIdx.x;
-    float Bw[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    float2 f1, f2, f3, SNR;
-    ushort2 taps, taps1, taps2;
-    s_bv[t].x = 0;
-    s_bv[t].y = 0;
-    int spos = blockIdx.x * (2 * SPD_NTHREADS - nBoxcars) + 2 * t;
-    const long long row = static_cast<long long>(blockIdx.y) * nT;
-    if ((spos + 4) < nT) {
-        const long long g = row + spos;
-        f1.x = in[g];
-        f1.y = in[g + 1];
-        f2.x = in[g + 2];
-        f2.y = in[g + 3];
-        f3.x = in[g + 4];
-        Bw[0] = f1.x;
-        Bw[4] = f1.y;
-        Bw[1] = f1.x + f1.y;
-        Bw[5] = f1.y + f2.x;
-        Bw[2] = Bw[1] + f2.x;
-        Bw[6] = Bw[5] + f2.y;
-        Bw[3] = Bw[1] + f2.x + f2.y;
-        Bw[7] = Bw[5] + f2.y + f3.x;
-        s_bv[t].x = bv_in[g];
-        s_bv[t].y = bv_in[g + 1];
-    }
-    spos = blockIdx.x * (SPD_NTHREADS - (nBoxcars >> 1)) + t;
-    if (t < (SPD_NTHREADS - (nBoxcars >> 1)) && spos < dtm)
-        dec[static_cast<long long>(blockIdx.y) * dtm + spos] = Bw[1];
-    s_in[t].x = Bw[3];
-    s_in[t].y = Bw[7];
-    SNR.x = 0;
-    SNR.y = 0;
-    __syncthreads();
-    float2 st = msd.v[0];
-    f1.x = snr_of_bv(s_bv[t].x, Bw[0], st);
-    f1.y = snr_of_bv(s_bv[t].y, Bw[4], st);
-    st = msd.v[1];
-    f2.x = snr_of_bv(s_bv[t].x, Bw[1], st);
-    f2.y = snr_of_bv(s_bv[t].y, Bw[5], st);
-    if (f2.x > f1.x) { f1.x = f2.x; taps1.x = 2; } else taps1.x = 1;
-    if (f2.y > f1.y) { f1.y = f2.y; taps1.y = 2; } else taps1.y = 1;
-    st = msd.v[2];
-    f2.x = snr_of_bv(s_bv[t].x, Bw[2], st);
-    f2.y = snr_of_bv(s_bv[t].y, Bw[6], st);
-    st = msd.v[3];
-    f3.x = snr_of_bv(s_bv[t].x, Bw[3], st);
-    f3.y = snr_of_bv(s_bv[t].y, Bw[7], st);
-    if (f3.x > f2.x) { f2.x = f3.x; taps2.x = 4; } else taps2.x = 3;
-    if (f3.y > f2.y) { f2.y = f3.y; taps2.y = 4; } else taps2.y = 3;
-    if (f1.x > f2.x) { SNR.x = f1.x; taps.x = taps1.x; } else { SNR.x = f2.x; taps.x = taps2.x; }
-    if (f1.y > f2.y) { SNR.y = f1.y; taps.y = taps1.y; } else { SNR.y = f2.y; taps.y = taps2.y; }
-    s_snr[t] = SNR;
-    s_taps[t] = taps;
+    if (lane >= 32 - (Q - 1))
+        return;
 #pragma unroll
-    for (int d = 4; d < nBoxcars; d += 4) {
-        __syncthreads();
-        spos = t - (d >> 1);
-        if (spos >= 0) {
-            f1 = s_in[spos];
-            SNR = s_snr[spos];
-            taps = s_taps[spos];
-            Bw[0] = Bw[0] + f1.x; Bw[4] = Bw[4] + f1.y;
-            Bw[1] = Bw[1] + f1.x; Bw[5] = Bw[5] + f1.y;
-            Bw[2] = Bw[2] + f1.x; Bw[6] = Bw[6] + f1.y;
-            Bw[3] = Bw[3] + f1.x; Bw[7] = Bw[7] + f1.y;
-            st = msd.v[d];
-            f1.x = snr_of_bv(s_bv[spos].x, Bw[0], st);
-            f1.y = snr_of_bv(s_bv[spos].y, Bw[4], st);
-            st = msd.v[d + 1];
-            f2.x = snr_of_bv(s_bv[spos].x, Bw[1], st);
-            f2.y = snr_of_bv(s_bv[spos].y, Bw[5], st);
-            if (f2.x > f1.x) { f1.x = f2.x; taps1.x = d + 2; } else taps1.x = d + 1;
-            if (f2.y > f1.y) { f1.y = f2.y; taps1.y = d + 2; } else taps1.y = d + 1;
-            st = msd.v[d + 2];
-            f2.x = snr_of_bv(s_bv[spos].x, Bw[2], st);
-            f2.y = snr_of_bv(s_bv[spos].y, Bw[6], st);
-            st = msd.v[d + 3];
-            f3.x = snr_of_bv(s_bv[spos].x, Bw[3], st);
-            f3.y = snr_of_bv(s_bv[spos].y, Bw[7], st);
-            if (f3.x > f2.x) { f2.x = f3.x; taps2.x = d + 4; } else taps2.x = d + 3;
-            if (f3.y > f2.y) { f2.y = f3.y; taps2.y = d + 4; } else taps2.y = d + 3;
-            if (f2.x > f1.x) { f1.x = f2.x; taps1.x = taps2.x; }
-            if (f2.y > f1.y) { f1.y = f2.y; taps1.y = taps2.y; }
-            if (f1.x > SNR.x) { SNR.x = f1.x; taps.x = taps1.x; }
-            if (f1.y > SNR.y) { SNR.y = f1.y; taps.y = taps1.y; }
-            s_snr[spos] = SNR;
-            s_taps[spos] = taps;
+    for (int p = 0; p < 4; ++p) {
+        const long long u = v0 + p;
+        if (u >= nT)
+            break;
+        snr_out[row + u] = best[p];
+        taps_out[row + u] = static_cast<uint16_t>(NTH ? startTaps + taps[p] * dit_value : taps[p]);
+        if ((p & 1) == 0 && (u >> 1) < dtm) {
+            const long long o = static_cast<long long>(blockIdx.y) * dtm + (u >> 1);
+            dec[o] = pair[p];
+            bv_out[o] = NTH ? bv[p] + full[p] : full[p];
         }
-    }
-    if (spos >= 0)
-        s_in[spos].x = s_bv[spos].x + Bw[3];
-    __syncthreads();
-    spos = blockIdx.x * (2 * SPD_NTHREADS - nBoxcars) + 2 * t;
-    if (t < (SPD_NTHREADS - (nBoxcars >> 1)) && spos < nT) {
-        const long long g = row + spos;
-        snr_out[g] = s_snr[t].x;
-        snr_out[g + 1] = s_snr[t].y;
-        taps_out[g] = startTaps + s_taps[t].x * dit_value;
-        taps_out[g + 1] = startTaps + s_taps[t].y * dit_value;
-        spos = blockIdx.x * (SPD_NTHREADS - (nBoxcars >> 1)) + t;
-        if (spos < dtm)
-            bv_out[static_cast<long long>(blockIdx.y) * dtm + spos] = s_in[t].x;
     }
 }
 
@@ -1110,25 +1032,31 @@ cudaError_t msd_interpolate(const float *d_msd_dit, float *d_msd_interp, const i
     return cudaGetLastError();
 }
 
-cudaError_t spdt_first_plane(const float *d_input, float *d_bv_out, float *d_decimated, float *d_snr, uint16_t *d_taps,
-                             const SnrMsd &msd, int nTimesamples, int nBoxcars, int dtm, int nBlocks, int nDMs,
-                             cudaStream_t st)
+// nBlocks: the plan's count of the reference's 512-thread blocks, 0 when the
+// plane is too short to be searched at this iteration (then nothing is
+// written); otherwise every start sample of every DM trial is covered
+template <bool NTH>
+static cudaError_t launch_boxcar_snr(const float *in, const float *bv_in, float *bv_out, float *dec, float *snr,
+                                     uint16_t *taps, const SnrMsd &msd, int nT, int nBoxcars, int startTaps,
+                                     int dit_value, int dtm, int nBlocks, int nDMs, cudaStream_t st)
 {
-    if (nBlocks <= 0)
+    if (nBlocks <= 0 || nT <= 0)
         return cudaSuccess;
-    const dim3 grid(nBlocks, nDMs);
+    const int out = 128 - 4 * (nBoxcars / 4 - 1);
+    const long long windows = (static_cast<long long>(nT) + out - 1) / out;
+    const dim3 grid(static_cast<unsigned>((windows + SNR_WARPS - 1) / SNR_WARPS), nDMs);
     switch (nBoxcars) {
     case 32:
-        k_spdt_first<32><<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_bv_out, d_decimated, d_snr, d_taps, msd,
-                                                        nTimesamples, dtm);
+        k_boxcar_snr<32, NTH><<<grid, 32 * SNR_WARPS, 0, st>>>(in, bv_in, bv_out, dec, snr, taps, msd, nT, startTaps,
+                                                              dit_value, dtm);
         break;
     case 16:
-        k_spdt_first<16><<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_bv_out, d_decimated, d_snr, d_taps, msd,
-                                                        nTimesamples, dtm);
+        k_boxcar_snr<16, NTH><<<grid, 32 * SNR_WARPS, 0, st>>>(in, bv_in, bv_out, dec, snr, taps, msd, nT, startTaps,
+                                                              dit_value, dtm);
         break;
     case 8:
-        k_spdt_first<8><<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_bv_out, d_decimated, d_snr, d_taps, msd,
-                                                       nTimesamples, dtm);
+        k_boxcar_snr<8, NTH><<<grid, 32 * SNR_WARPS, 0, st>>>(in, bv_in, bv_out, dec, snr, taps, msd, nT, startTaps,
+                                                             dit_value, dtm);
         break;
     default:
         return cudaErrorInvalidValue;
@@ -1137,31 +1065,20 @@ cudaError_t spdt_first_plane(const float *d_input, float *d_bv_out, float *d_dec
     return cudaGetLastError();
 }
 
+cudaError_t spdt_first_plane(const float *d_input, float *d_bv_out, float *d_decimated, float *d_snr, uint16_t *d_taps,
+                             const SnrMsd &msd, int nTimesamples, int nBoxcars, int dtm, int nBlocks, int nDMs,
+                             cudaStream_t st)
+{
+    return launch_boxcar_snr<false>(d_input, nullptr, d_bv_out, d_decimated, d_snr, d_taps, msd, nTimesamples,
+                                    nBoxcars, 0, 1, dtm, nBlocks, nDMs, st);
+}
+
 cudaError_t spdt_nth_plane(const float *d_input, const float *d_bv_in, float *d_bv_out, float *d_decimated,
                            float *d_snr, uint16_t *d_taps, const SnrMsd &msd, int nTimesamples, int nBoxcars,
                            int startTaps, int dit_value, int dtm, int nBlocks, int nDMs, cudaStream_t st)
 {
-    if (nBlocks <= 0)
-        return cudaSuccess;
-    const dim3 grid(nBlocks, nDMs);
-    switch (nBoxcars) {
-    case 32:
-        k_spdt_nth<32><<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_bv_in, d_bv_out, d_decimated, d_snr, d_taps, msd,
-                                                      nTimesamples, startTaps, dit_value, dtm);
-        break;
-    case 16:
-        k_spdt_nth<16><<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_bv_in, d_bv_out, d_decimated, d_snr, d_taps, msd,
-                                                      nTimesamples, startTaps, dit_value, dtm);
-        break;
-    case 8:
-        k_spdt_nth<8><<<grid, SPD_NTHREADS, 0, st>>>(d_input, d_bv_in, d_bv_out, d_decimated, d_snr, d_taps, msd,
-                                                     nTimesamples, startTaps, dit_value, dtm);
-        break;
-    default:
-        return cudaErrorInvalidValue;
-    }
-    ++g_spd_launches;
-    return cudaGetLastError();
+    return launch_boxcar_snr<true>(d_input, d_bv_in, d_bv_out, d_decimated, d_snr, d_taps, msd, nTimesamples,
+                                   nBoxcars, startTaps, dit_value, dtm, nBlocks, nDMs, st);
 }
 
 cudaError_t spd_peak_find(const float *d_snr, const uint16_t *d_taps, unsigned *d_dm, unsigned *d_ts, float *d_csnr,

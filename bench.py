@@ -78,6 +78,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the timed output")
+    ap.add_argument("--no-autotune", action="store_true", help="no per-range kernel timing at set-up")
     ap.add_argument("--multibeam-beams", type=int, default=8,
                     help="beams of the reduced multi-beam draw timed batched vs plain in the default line (0: off)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -85,7 +86,8 @@ def parse():
     ap.add_argument("--group-dms", type=int, default=0)
     ap.add_argument("--variant", type=int, default=0,
                     help="0 auto, 1 generic kernels, 2 channel-quad, 3 subband, 4 warp-specialised channel-quad, "
-                         "5 split-phase channel-quad (2-5 run the staged fp32 kernel on two-byte data)")
+                         "5 split-phase channel-quad, 6 channel-quad with reuse by offset pattern, 7 channel-quad on "
+                         "256-sample tiles (2-7 run the staged fp32 kernel on two-byte data)")
     ap.add_argument("--with-analysis", action="store_true",
                     help="add an e2e run through the C ABI with the analysis component after every step")
     ap.add_argument("--spd-nt", type=int, default=0, help="samples per DM trial of the spd config (default 2^19)")
@@ -1207,6 +1209,8 @@ def main():
                               stream=stream.cuda_stream, card_number=local)
     pipe.set_options(tile_words=args.tile_words, group_dms=args.group_dms)
     pipe.set_kernel_variant(args.variant)
+    if args.no_autotune:
+        pipe.set_autotune(False)
     plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in cfg["plan"]])
     if not pipe.bind_ddtr_plan(plan):
         raise RuntimeError(pipe.last_error())

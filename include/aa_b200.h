@@ -259,6 +259,44 @@ int aa_b200_dedisperse_noalloc(int i, int t_processed, const int *inBin, const f
  * this thread ("" if the last call succeeded). */
 const char *aa_b200_noalloc_last_error(void);
 
+/* ---------------------------------------------------------------------------
+ * The reference's dedispersion seam with its own argument lists (C twins of
+ * the C++ functions of namespace astroaccelerate declared in
+ * aa_b200_seam.hpp, which link unchanged against code written for the
+ * reference's runner).  Reference buffers: one unsigned short per sample,
+ * [t][c] as loaded, [c][t] after the corner turn; float rows out.  All on
+ * the legacy default stream.
+ * ------------------------------------------------------------------------- */
+/* load_chunk_data (src/aa_device_load_data.cu:39-56): H2D of
+ * (t_processed + maxshift) * nchans samples, the delay table to d_dm_shifts
+ * where the reference does that, and set_dedispersion_constants. */
+void aa_b200_seam_load_chunk_data(unsigned short *device_pointer, const unsigned short *host_pointer, int t_processed,
+                                  int maxshift, int nchans, float *dmshifts, float *d_dm_shifts, int nbits);
+/* set_dedispersion_constants (src/aa_device_load_data.cu:58-61): row length
+ * t_processed + maxshift and t_processed for the next aa_b200_seam_dedisperse
+ * of this thread (per thread; the reference's are process-wide constants). */
+void aa_b200_seam_set_dedispersion_constants(int t_processed, int maxshift);
+/* corner_turn_SM_inplace (src/aa_corner_turn.cpp:118-121): [secondary][primary]
+ * to [primary][secondary] in place, through d_temporary. */
+void aa_b200_seam_corner_turn_SM_inplace(unsigned short *d_input, unsigned short *d_temporary, size_t primary_size,
+                                         size_t secondary_size);
+/* bin_gpu (src/aa_bin_gpu.cpp:8-44): the x2 binning of the flat buffer in
+ * place, d_output as scratch. */
+void aa_b200_seam_bin_gpu(unsigned short *d_input, float *d_output, int nchans, int nsamp);
+/* dedisperse (src/aa_dedisperse.cpp:5-163): DM range i of d_input
+ * [nchans][row length of set_dedispersion_constants] into d_output
+ * [ndms[i]][t_processed].  Tables per range are built on the first call and
+ * kept per thread; the rows are staged into a padded buffer of the library.
+ * Returns 0, or 1 with the reason in aa_b200_last_error(); the device work
+ * is complete when it returns. */
+int aa_b200_seam_dedisperse(int i, int t_processed, int *inBin, float *dmshifts, unsigned short *d_input,
+                            float *d_output, float *d_dm_shifts, int nchans, float *tsamp, float *dm_low,
+                            float *dm_step, const int *ndms, int nbits, int failsafe);
+/* save_data_offset_stream (src/aa_device_save_data.cu:19-62): the chunk's DM
+ * rows of range dm_range to output_buffer[dm_range][dm] + inc/inBin. */
+void aa_b200_seam_save_data_offset_stream(int dm_range, int current_time_chunk, int **t_processed, long inc,
+                                          int *inBin, const int *ndms, float *d_DDTR_output, float ***output_buffer);
+
 /* Message of the last failure of this thread ("" if none). */
 const char *aa_b200_last_error(void);
 /* Kernels this library has launched in this process. */
@@ -360,9 +398,15 @@ bool aa_b200_pipeline_set_packed_input(void *obj, const void *packed);
  * autotuner times the candidates), 1 the generic kernels, 2 the channel-quad
  * kernel (one-byte data) / staged fp32 kernel (two-byte data), 3 the subband
  * kernel / fp32, 4 the warp-specialised channel-quad kernel / fp32, 5 the
- * split-phase channel-quad kernel / fp32.  A forced family that cannot run a
- * range makes the bind fail with the reason. */
+ * split-phase channel-quad kernel / fp32, 6 the channel-quad kernel with its
+ * register reuse chosen per warp by the pattern of equal offsets / fp32, 7
+ * the channel-quad kernel on 256-sample tiles, two CTAs per SM / fp32.  A
+ * forced family that cannot run a range makes the bind fail with the reason. */
 bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant);
+/* Before bind: whether the set-up times the staged kernels' stage depth (and,
+ * for variant 0, the candidate kernels) per range on a slice of the first
+ * chunk (default 1).  0 keeps the largest stage that fits shared memory. */
+bool aa_b200_pipeline_set_autotune(void *obj, int enable);
 /* output_dmt (pipeline_component_option_struct): when the run finishes, the
  * DM-time output of every range is written in the reference's
  * Export_DD_data files (include/aa_pipeline_runner.hpp:165-216), DM rows per

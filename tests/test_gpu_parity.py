@@ -135,6 +135,8 @@ def test_tile_shapes_agree(aa, oracle_mod, cuda_device, tile_words, group_dms, v
                                                  ("shared8_binned", 2, "quad"),
                                                  ("shared8_nch3000", 0, "sub|quad|quadsp"),
                                                  ("shared8_nch3000", 4, "quadws"), ("shared8_nch3000", 5, "quadsp"),
+                                                 ("shared8_binned", 6, "quad"), ("shared8_binned", 7, "quad"),
+                                                 ("shared8_nch3000", 6, "quad"), ("shared8_nch3000", 7, "quad"),
                                                  ("shared8_nch3000", 3, "sub"), ("shared8_nch3000", 2, "quad"),
                                                  ("shared16", 0, "f32"), ("shared16", 1, "gather"),
                                                  ("cache16", 2, "f32")])
