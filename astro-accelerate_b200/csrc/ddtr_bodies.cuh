@@ -172,9 +172,10 @@ __device__ __forceinline__ void quad_sum4(uint32_t (&acc)[4][M], const uint32_t 
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         if (j == 0 || ((MASK >> (j - 1)) & 1)) {
+            const uint32_t *src = sm + (prow + ej[j]); // constant offsets fold into the loads
 #pragma unroll
             for (int m = 0; m < M; ++m)
-                w[m] = sm[prow + ej[j] + 32 * m];
+                w[m] = src[32 * m];
         }
 #pragma unroll
         for (int m = 0; m < M; ++m)
@@ -199,8 +200,11 @@ __device__ __forceinline__ void quad_sum4_dispatch(uint32_t (&acc)[4][M], const 
     }
 }
 
-// SWITCH: the four trials of a warp (DW = 4) take quad_sum4_dispatch
-template <int M, int DW, bool SWITCH = false>
+// SWITCH: the four trials of a warp (DW = 4) take quad_sum4_dispatch.
+// LOADALL: every trial loads its own words (no register reuse between trials
+// that share an offset): more shared loads, but no data-dependent branch and
+// no register copies in the sum loop.
+template <int M, int DW, bool SWITCH = false, bool LOADALL = false>
 __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long long t0, uint32_t *sm, unsigned bar0,
                           unsigned &stage_ctr)
 {
@@ -398,7 +402,15 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
                     ej[4 * h + 3] = e4.w;
                     any_neg |= e4.x | e4.y | e4.z | e4.w;
                 }
-                if (SWITCH && DW == 4 && any_neg >= 0) {
+                if (LOADALL && any_neg >= 0) {
+#pragma unroll
+                    for (int j = 0; j < DW; ++j) {
+                        const uint32_t *src = sm + (prow + ej[j]);
+#pragma unroll
+                        for (int m = 0; m < M; ++m)
+                            acc[j][m] = __dp4a(src[32 * m], 0x01010101u, acc[j][m]);
+                    }
+                } else if (SWITCH && DW == 4 && any_neg >= 0) {
                     quad_sum4_dispatch<M>(reinterpret_cast<uint32_t(&)[4][M]>(acc), sm,
                                           reinterpret_cast<const int(&)[4]>(ej), prow);
                 } else if (any_neg >= 0) {
@@ -408,9 +420,10 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
 #pragma unroll
                     for (int j = 0; j < DW; ++j) {
                         if (j == 0 || ej[j] != ej[j - 1]) {
+                            const uint32_t *src = sm + (prow + ej[j]); // constant offsets fold into the loads
 #pragma unroll
                             for (int m = 0; m < M; ++m)
-                                w[m] = sm[prow + ej[j] + 32 * m];
+                                w[m] = src[32 * m];
                         }
 #pragma unroll
                         for (int m = 0; m < M; ++m)
@@ -420,9 +433,10 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
 #pragma unroll
                     for (int j = 0; j < DW; ++j) {
                         if (ej[j] >= 0) {
+                            const uint32_t *src = sm + (prow + ej[j]);
 #pragma unroll
                             for (int m = 0; m < M; ++m)
-                                acc[j][m] = __dp4a(sm[prow + ej[j] + 32 * m], 0x01010101u, acc[j][m]);
+                                acc[j][m] = __dp4a(src[32 * m], 0x01010101u, acc[j][m]);
                         } else {
                             slow(j, slot, q0, q);
                         }
@@ -453,6 +467,266 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
                 const float v = static_cast<float>(static_cast<int>(acc[j][m]));
                 orow[t] = p.divide_by_bin ? (v / p.nchans_f / p.bin_f) : (v / p.nchans_f);
             }
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Channel-quad pair body (one-byte samples, exact integer sums): the staging
+// and pattern tables of quad_body, but each pre-skewed pattern row is stored
+// already summed over its four channels, as pairs of 16-bit sums:
+//   E[k] = (S[2k], S[2k+1]),  O[k] = (S[2k+1], S[2k+2]),
+//   S[tau] = x[c][tau] + x[c+1][tau+d1] + x[c+2][tau+d2] + x[c+3][tau+d3]
+// (each at most 4 x 255).  A DM trial whose quad offset is tau adds, for the
+// output pair (2k, 2k+1), the word E[k + tau/2] (tau even) or O[k +
+// (tau-1)/2] (tau odd): one 32-bit load and one add for two outputs of four
+// channels, into 16-bit lanes that are moved into 32-bit sums every 64
+// quads (64 x 1020 < 2^16).  Lanes own output pairs 2(lane + 32m), m < MP, so
+// the loads are conflict-free.  The offsets come from the pair table
+// (k_quad_offsets in pair mode): slot*W + (tau&1)*W/2 + tau/2.
+//
+// Runs ranges without per-byte entries only (an entry of -1 sets
+// DERR_WINDOW).  Shared memory as quad_body, the P buffers holding the E and
+// O halves of each row.
+// ---------------------------------------------------------------------------
+template <int MP>
+__device__ bool quad_pair_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long long t0, uint32_t *sm,
+                               unsigned bar0, unsigned &stage_ctr)
+{
+    constexpr int DW = 4;
+    constexpr int NW = 16;
+    constexpr int NT = 32 * NW;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int GD = 64;
+    const int dm0 = g * GD;
+    const int W = Q.W, RAWW = Q.raww, QS = Q.qs, HW = Q.W >> 1;
+    const unsigned char *in = static_cast<const unsigned char *>(p.in);
+    const int nstages = (Q.nquads + QS - 1) / QS;
+    const unsigned sbase = stage_ctr;
+
+    const int o_qw = 0;
+    const int o_raw = o_qw + Q.nq_pad;
+    const int o_ent = o_raw + QNSTAGE * QS * 4 * RAWW;
+    const int o_pat = o_ent + QNSTAGE * QS * GD;
+    const int o_rsh = o_pat + QNSTAGE * QS * 16;
+    const int o_P = ((o_rsh + QNSTAGE * QS * 4) + 3) & ~3;
+
+    for (int i = tid; i < (Q.nq_pad >> 2); i += NT)
+        cp_async16(&sm[o_qw + 4 * i], Q.qwin + static_cast<size_t>(g) * Q.nq_pad + 4 * i);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+
+    auto issue = [&](int s) {
+        if (warp != 0 || s >= nstages)
+            return;
+        const unsigned gs = sbase + static_cast<unsigned>(s);
+        const int slot = static_cast<int>(gs % QNSTAGE);
+        const int q0 = s * QS;
+        const int nq = min(QS, Q.nquads - q0);
+        const int c0 = 4 * q0;
+        const int nrows = max(0, min(4 * nq, p.nch_used - c0));
+        const unsigned bar = bar0 + 8 * slot;
+        fence_proxy_async();
+        if (lane == 0)
+            mbar_expect_tx(bar, static_cast<unsigned>(nrows * RAWW * 4 + nq * GD * 4 + nq * 64));
+        __syncwarp();
+        if (lane < 4 * nq) {
+            const int c = c0 + lane;
+            if (lane < nrows) {
+                const int w0 = static_cast<int>(sm[o_qw + q0 + (lane >> 2)]);
+                const uintptr_t a = reinterpret_cast<uintptr_t>(in + static_cast<long long>(c) * p.stride + t0 + w0);
+                sm[o_rsh + slot * QS * 4 + lane] = static_cast<uint32_t>(a & 15);
+                tma_load_1d(smem_addr(&sm[o_raw + (slot * QS * 4 + lane) * RAWW]),
+                            reinterpret_cast<const void *>(a & ~static_cast<uintptr_t>(15)),
+                            static_cast<unsigned>(RAWW * 4), bar);
+            } else {
+                sm[o_rsh + slot * QS * 4 + lane] = 0xFFFFFFFFu; // channel contributes nothing
+            }
+        }
+        if (lane < nq)
+            tma_load_1d(smem_addr(&sm[o_ent + (slot * QS + lane) * GD]),
+                        Q.qoff + static_cast<size_t>(q0 + lane) * p.ndms + dm0, static_cast<unsigned>(GD * 4), bar);
+        if (lane == 0)
+            tma_load_1d(smem_addr(&sm[o_pat + slot * QS * 16]), Q.qpat + (static_cast<size_t>(g) * Q.nquads + q0) * 16,
+                        static_cast<unsigned>(nq * 64), bar);
+    };
+
+    bool ok = true;
+    auto wait_stage = [&](int s) -> int {
+        const unsigned gs = sbase + static_cast<unsigned>(s);
+        const int slot = static_cast<int>(gs % QNSTAGE);
+        if (!mbar_wait_bounded(bar0 + 8 * slot, (gs / QNSTAGE) & 1u)) {
+            if (ok)
+                atomicOr(p.err, DERR_TIMEOUT);
+            ok = false;
+        }
+        return slot;
+    };
+
+    // the summed pair rows of stage s into buffer b: work items are (row,
+    // 4-sample column), spread over all warps; the pair (S[tau+3],
+    // S[tau+4]) takes S[tau+4] from the next lane (the last lane of a warp
+    // computes it)
+    auto build = [&](int s, int b) {
+        const int slot = wait_stage(s);
+        const int q0 = s * QS;
+        const int nq = min(QS, Q.nquads - q0);
+        int total = 0;
+        for (int q = 0; q < nq; ++q)
+            total += static_cast<int>(sm[o_pat + (slot * QS + q) * 16 + 15]);
+        total = min(total, Q.npool);
+        const int n4 = W >> 2;
+        int q = 0, base = 0;
+        int cnt_q = (nq > 0) ? static_cast<int>(sm[o_pat + (slot * QS) * 16 + 15]) : 0;
+        for (int r = warp; r < total; r += NW) {
+            while (r >= base + cnt_q && q + 1 < nq) {
+                base += cnt_q;
+                ++q;
+                cnt_q = static_cast<int>(sm[o_pat + (slot * QS + q) * 16 + 15]);
+            }
+            const unsigned pw = sm[o_pat + (slot * QS + q) * 16 + (r - base)];
+            int d[4], rs[4], rb[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                d[i] = (i == 0) ? 0 : static_cast<int>((pw >> (8 * (i - 1))) & 255u);
+                rs[i] = static_cast<int>(sm[o_rsh + slot * QS * 4 + 4 * q + i]);
+                rb[i] = o_raw + (slot * QS * 4 + 4 * q + i) * RAWW;
+            }
+            const int erow = o_P + (b * Q.npool + r) * W;
+            const int orow = erow + HW;
+            for (int c4 = 0; c4 < n4; c4 += 32) {
+                const int t4 = c4 + lane;
+                const bool live = t4 < n4;
+                const int tau = 4 * t4;
+                uint32_t a[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if (rs[i] < 0 || !live) {
+                        a[i] = 0u;
+                    } else {
+                        const int bb = rs[i] + tau + d[i];
+                        const int wi = rb[i] + (bb >> 2);
+                        a[i] = __funnelshift_r(sm[wi], sm[wi + 1], 8u * static_cast<unsigned>(bb & 3));
+                    }
+                }
+                // 4x4 byte transpose, then the four channels of each sample summed
+                const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), hi01 = __byte_perm(a[0], a[1], 0x7362);
+                const uint32_t lo23 = __byte_perm(a[2], a[3], 0x5140), hi23 = __byte_perm(a[2], a[3], 0x7362);
+                const uint32_t s0 = __dp4a(__byte_perm(lo01, lo23, 0x5410), 0x01010101u, 0u);
+                const uint32_t s1 = __dp4a(__byte_perm(lo01, lo23, 0x7632), 0x01010101u, 0u);
+                const uint32_t s2 = __dp4a(__byte_perm(hi01, hi23, 0x5410), 0x01010101u, 0u);
+                const uint32_t s3 = __dp4a(__byte_perm(hi01, hi23, 0x7632), 0x01010101u, 0u);
+                uint32_t s4 = __shfl_down_sync(0xffffffffu, s0, 1);
+                if (live && (lane == 31 || t4 + 1 == n4)) {
+                    // S[tau+4]: the four channels' bytes at tau+4
+                    s4 = 0u;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (rs[i] >= 0) {
+                            const int bb = rs[i] + tau + 4 + d[i];
+                            s4 += (sm[rb[i] + (bb >> 2)] >> (8u * static_cast<unsigned>(bb & 3))) & 255u;
+                        }
+                }
+                if (live) {
+                    *reinterpret_cast<uint2 *>(&sm[erow + 2 * t4]) =
+                        make_uint2(__byte_perm(s0, s1, 0x5410), __byte_perm(s2, s3, 0x5410));
+                    *reinterpret_cast<uint2 *>(&sm[orow + 2 * t4]) =
+                        make_uint2(__byte_perm(s1, s2, 0x5410), __byte_perm(s3, s4, 0x5410));
+                }
+            }
+        }
+    };
+
+    uint32_t acc[DW][2 * MP];
+    uint32_t a16[DW][MP];
+#pragma unroll
+    for (int j = 0; j < DW; ++j) {
+#pragma unroll
+        for (int m = 0; m < 2 * MP; ++m)
+            acc[j][m] = 0u;
+#pragma unroll
+        for (int m = 0; m < MP; ++m)
+            a16[j][m] = 0u;
+    }
+    auto flush = [&]() {
+#pragma unroll
+        for (int j = 0; j < DW; ++j)
+#pragma unroll
+            for (int m = 0; m < MP; ++m) {
+                acc[j][2 * m] += a16[j][m] & 0xFFFFu;
+                acc[j][2 * m + 1] += a16[j][m] >> 16;
+                a16[j][m] = 0u;
+            }
+    };
+
+#pragma unroll
+    for (int s = 0; s < QNSTAGE - 1; ++s)
+        issue(s);
+    __syncthreads(); // raw-row shifts written by warp 0 become visible
+    if (nstages > 0)
+        build(0, 0);
+    fence_proxy_async();
+    __syncthreads();
+    issue(QNSTAGE - 1);
+
+    int quads_since_flush = 0;
+    for (int s = 0; s < nstages; ++s) {
+        if (s + 1 < nstages)
+            build(s + 1, (s + 1) & 1);
+        const int slot = static_cast<int>((sbase + static_cast<unsigned>(s)) % QNSTAGE);
+        const int q0 = s * QS;
+        const int nq = min(QS, Q.nquads - q0);
+        if (ok) {
+            int rbase = 0;
+            for (int q = 0; q < nq; ++q) {
+                const int prow = o_P + ((s & 1) * Q.npool + rbase) * W + lane;
+                const int4 e4 = *reinterpret_cast<const int4 *>(&sm[o_ent + (slot * QS + q) * GD + warp * DW]);
+                const int ej[DW] = {e4.x, e4.y, e4.z, e4.w};
+                if ((e4.x | e4.y | e4.z | e4.w) < 0)
+                    atomicOr(p.err, DERR_WINDOW);
+                // every trial loads its own words: no data-dependent branch
+#pragma unroll
+                for (int j = 0; j < DW; ++j) {
+                    const uint32_t *src = sm + (prow + max(ej[j], 0)); // constant offsets fold into the loads
+#pragma unroll
+                    for (int m = 0; m < MP; ++m)
+                        a16[j][m] += src[32 * m];
+                }
+                rbase += static_cast<int>(sm[o_pat + (slot * QS + q) * 16 + 15]);
+                if (++quads_since_flush == 64) {
+                    flush();
+                    quads_since_flush = 0;
+                }
+            }
+        }
+        fence_proxy_async();
+        __syncthreads();
+        issue(s + QNSTAGE);
+    }
+    flush();
+    stage_ctr = sbase + static_cast<unsigned>(nstages);
+    if (!ok)
+        return false;
+
+    // (float)S / nchans / bin, the reference's expression (4-bit: / nchans)
+#pragma unroll
+    for (int j = 0; j < DW; ++j) {
+        const int dm = dm0 + warp * DW + j;
+        if (dm >= p.ndms)
+            continue;
+        float *orow = p.out + static_cast<long long>(dm) * p.out_pitch;
+#pragma unroll
+        for (int m = 0; m < MP; ++m) {
+            const long long t = t0 + 2 * (lane + 32 * m);
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (t + h < p.tp) {
+                    const float v = static_cast<float>(static_cast<int>(acc[j][2 * m + h]));
+                    orow[t + h] = p.divide_by_bin ? (v / p.nchans_f / p.bin_f) : (v / p.nchans_f);
+                }
         }
     }
     return true;
@@ -692,10 +966,10 @@ __device__ bool quad_sp_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, lo
 #pragma unroll
             for (int j = 0; j < DW; ++j) {
                 if (j == 0 || ej[j] != ej[j - 1]) {
-                    const int e = prow + max(ej[j], 0);
+                    const uint32_t *src = sm + (prow + max(ej[j], 0)); // constant offsets fold into the loads
 #pragma unroll
                     for (int m = 0; m < M; ++m)
-                        w[m] = sm[e + 32 * m];
+                        w[m] = src[32 * m];
                 }
 #pragma unroll
                 for (int m = 0; m < M; ++m)

@@ -105,7 +105,9 @@ struct QuadLaunch {
     int npool; // pre-skewed rows per stage buffer
     int M;     // outputs per lane per DM trial (tile = 32*M)
     int flavour; // 0: per-trial reuse test; 1: reuse by a switch over the warp's offset pattern
-                 // (M = 16); 2: M = 8 with 16 warps and two CTAs per SM
+                 // (M = 16); 2: M = 8 with 16 warps and two CTAs per SM; 3: the pair body
+                 // (rows summed over the quad, 16-bit pairs; pair-mode offsets; M = 16);
+                 // 4: every DM trial loads its own words (M = 16)
 };
 
 struct QuadGeometry {
@@ -116,7 +118,8 @@ struct QuadGeometry {
 QuadGeometry quad_geometry(int span, int dmax, int maxcnt, int group_dms, int nquads, int out_words, int qs);
 cudaError_t launch_quad_patterns(const int32_t *table, int nch_used, int ndms, int group_dms, int nquads, int nq_pad,
                                  int32_t *qpat, int32_t *qwin, int32_t *qtmp, int *stats, cudaStream_t st);
-cudaError_t launch_quad_offsets(const int32_t *qtmp, size_t n, int W, int32_t *qoff, cudaStream_t st);
+cudaError_t launch_quad_offsets(const int32_t *qtmp, size_t n, int W, int32_t *qoff, cudaStream_t st,
+                                int pairs = 0);
 cudaError_t launch_ddtr_quad(const DdtrLaunch &p, const QuadLaunch &q, cudaStream_t st);
 // Warp-specialised channel-quad kernel (M = 16 only): producer warps build the
 // pre-skewed rows of the next stage while consumer warps sum the current one.

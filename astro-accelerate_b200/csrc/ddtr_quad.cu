@@ -92,19 +92,24 @@ __global__ void k_quad_patterns(const int32_t *__restrict__ table, int nch_used,
         atomicAdd(stats + 3, nbyte); // (quad, DM) entries that need the per-byte path
 }
 
-__global__ void k_quad_offsets(const int32_t *__restrict__ qtmp, size_t n, int W, int32_t *__restrict__ qoff)
+// pairs = 0: slot*W + tau (words of a pre-skewed row); pairs = 1: the pair
+// body's offsets slot*W + (tau&1)*W/2 + tau/2 (E half for even tau, O half
+// for odd tau)
+__global__ void k_quad_offsets(const int32_t *__restrict__ qtmp, size_t n, int W, int pairs,
+                               int32_t *__restrict__ qoff)
 {
     const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
     const int v = qtmp[i];
-    qoff[i] = (v < 0) ? -1 : ((v >> 24) * W + (v & 0xFFFFFF));
+    const int tau = v & 0xFFFFFF;
+    qoff[i] = (v < 0) ? -1 : ((v >> 24) * W + (pairs ? (tau & 1) * (W >> 1) + (tau >> 1) : tau));
 }
 
 // M = 16: 16 warps x 4 DM trials, one CTA per SM (127 registers);
 // M = 8: 8 warps x 8 DM trials, two CTAs per SM, so that one CTA issues
 // while the other waits at its stage barrier.
-template <int M, int DW, bool SWITCH, int MINB>
+template <int M, int DW, bool SWITCH, int MINB, bool LOADALL = false>
 __global__ void __launch_bounds__(32 * 64 / DW, MINB) k_ddtr_quad(const DdtrLaunch p, const QuadLaunch Q)
 {
     extern __shared__ __align__(16) uint32_t sm[];
@@ -112,8 +117,8 @@ __global__ void __launch_bounds__(32 * 64 / DW, MINB) k_ddtr_quad(const DdtrLaun
     body::init_barriers(bar0);
     __syncthreads();
     unsigned stage_ctr = 0;
-    body::quad_body<M, DW, SWITCH>(p, Q, blockIdx.x, static_cast<long long>(blockIdx.y) * (32 * M),
-                                   sm + body::BAR_WORDS, bar0, stage_ctr);
+    body::quad_body<M, DW, SWITCH, LOADALL>(p, Q, blockIdx.x, static_cast<long long>(blockIdx.y) * (32 * M),
+                                            sm + body::BAR_WORDS, bar0, stage_ctr);
 }
 
 // 16 consumer + WS_PROD producer warps (body::quad_ws_body); five warps per
@@ -127,6 +132,19 @@ __global__ void __launch_bounds__(body::WS_THREADS, 1) k_ddtr_quadws(const DdtrL
     unsigned stage_ctr = 0;
     body::quad_ws_body(p, Q, blockIdx.x, static_cast<long long>(blockIdx.y) * 512, sm + body::BAR_WORDS, bar0,
                        stage_ctr);
+}
+
+// Channel-quad pair kernel (body::quad_pair_body): 16 warps x 4 DM trials x
+// 256 output pairs, one CTA per SM.
+__global__ void __launch_bounds__(512, 1) k_ddtr_quadpair(const DdtrLaunch p, const QuadLaunch Q)
+{
+    extern __shared__ __align__(16) uint32_t sm[];
+    const unsigned bar0 = smem_addr(sm);
+    body::init_barriers(bar0);
+    __syncthreads();
+    unsigned stage_ctr = 0;
+    body::quad_pair_body<8>(p, Q, blockIdx.x, static_cast<long long>(blockIdx.y) * 512, sm + body::BAR_WORDS, bar0,
+                            stage_ctr);
 }
 
 // Split-phase channel-quad kernel (body::quad_sp_body): 16 warps x 4 DM
@@ -194,9 +212,9 @@ cudaError_t launch_quad_patterns(const int32_t *table, int nch_used, int ndms, i
     return cudaGetLastError();
 }
 
-cudaError_t launch_quad_offsets(const int32_t *qtmp, size_t n, int W, int32_t *qoff, cudaStream_t st)
+cudaError_t launch_quad_offsets(const int32_t *qtmp, size_t n, int W, int32_t *qoff, cudaStream_t st, int pairs)
 {
-    k_quad_offsets<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(qtmp, n, W, qoff);
+    k_quad_offsets<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(qtmp, n, W, pairs, qoff);
     return cudaGetLastError();
 }
 
@@ -231,6 +249,10 @@ cudaError_t launch_ddtr_quad(const DdtrLaunch &p, const QuadLaunch &q, cudaStrea
     if (p.group_dms != 64 || q.qs < 1 || q.qs > 8)
         return cudaErrorInvalidValue;
     const size_t smem = 4 * (body::BAR_WORDS + body::quad_body_words(q.qs, p.group_dms, q.raww, q.nq_pad, q.npool, q.W));
+    if (q.M == 16 && q.flavour == 3)
+        return launch_quad_instance(k_ddtr_quadpair, 512, p, q, smem, st);
+    if (q.M == 16 && q.flavour == 4)
+        return launch_quad_instance(k_ddtr_quad<16, 4, false, 1, true>, 512, p, q, smem, st);
     if (q.M == 8 && q.flavour == 2)
         return launch_quad_instance(k_ddtr_quad<8, 4, true, 2>, 512, p, q, smem, st);
     if (q.M == 8)

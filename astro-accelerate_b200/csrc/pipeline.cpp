@@ -135,7 +135,8 @@ bool DdtrPipeline::build_range(int r)
     }
     if (elem_bytes_ == 1 &&
         (opt_.kernel_variant == 0 || opt_.kernel_variant == 2 || opt_.kernel_variant == 4 ||
-         opt_.kernel_variant == 5 || opt_.kernel_variant == 6 || opt_.kernel_variant == 7) &&
+         opt_.kernel_variant == 5 || opt_.kernel_variant == 6 || opt_.kernel_variant == 7 ||
+         opt_.kernel_variant == 8 || opt_.kernel_variant == 9) &&
         rc.group_dms == 64) {
         if (!build_quad_tables(r))
             return false;
@@ -226,7 +227,9 @@ bool DdtrPipeline::build_quad_tables(int r)
             rc.quad = G;
             rc.variant = 2;
             rc.has_quad = true;
-            ok = check_cuda(launch_quad_offsets(d_qtmp, nq_ent, G.W, rc.d_qoff, st_), "quad offsets");
+            const bool pairs = (opt_.kernel_variant == 8) && hs[3] == 0 && M == 16;
+            rc.quad_pairs = pairs;
+            ok = check_cuda(launch_quad_offsets(d_qtmp, nq_ent, G.W, rc.d_qoff, st_, pairs ? 1 : 0), "quad offsets");
             ++launches_;
         }
     }
@@ -840,7 +843,11 @@ bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, f
         q.qs = rc.quad.qs;
         q.npool = rc.quad.npool;
         q.M = rc.quad.M;
-        q.flavour = (opt_.kernel_variant == 6 && q.M == 16) ? 1 : (opt_.kernel_variant == 7 && q.M == 8) ? 2 : 0;
+        q.flavour = rc.quad_pairs                                ? 3
+                    : (opt_.kernel_variant == 9 && q.M == 16) ? 4
+                    : (opt_.kernel_variant == 6 && q.M == 16) ? 1
+                    : (opt_.kernel_variant == 7 && q.M == 8)  ? 2
+                                                              : 0;
     } else if (job.variant == 3) {
         job.f = rc.f32;
     } else if (job.variant == 4) {

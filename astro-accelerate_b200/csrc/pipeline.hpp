@@ -143,6 +143,7 @@ struct RangeConfig {
     // subband and the channel-quad tables may exist until the autotuner picks
     bool has_sub = false, has_quad = false;
     bool quad_ws_ok = false; // no per-byte entries: the warp-specialised quad kernel may run it
+    bool quad_pairs = false; // the offset table is in pair mode (the pair body runs the range)
     SubGeometry sub{};
     int nsub = 0;
     int32_t *d_sblk = nullptr;

@@ -25,11 +25,63 @@ std::atomic<long long> g_psr_launches{0};
 // ---------------------------------------------------------------------------
 constexpr int PSR_PAIR_THREADS = 256;
 
-__device__ __forceinline__ float2 psr_scaled(float2 a, float norm) { return make_float2(a.x / norm, a.y / norm); }
-__device__ __forceinline__ float psr_power(float2 a) { return a.x * a.x + a.y * a.y; }
+// How the contractible expressions below are evaluated.  The values must
+// round exactly as the reference build's (nvcc with --use_fast_math, which
+// fuses a multiply into a following add); each form is spelled out with
+// intrinsics so that the result does not depend on the compiler's choice in
+// this file's context.  Form 0 leaves the choice to the compiler.
+// The forms used are those that give the reference's bits on the golden
+// spectra (tests/golden/psr_golden.json).
+#ifndef PSR_POWER_FORM
+#define PSR_POWER_FORM 1 // x*x + y*y: 1 fma(x,x,y*y), 2 fma(y,y,x*x), 3 unfused, 0 compiler's choice
+#endif
+#ifndef PSR_INTERP_FORM
+#define PSR_INTERP_FORM 1 // mean + slope*i: 1 fma, 2 unfused, 0 compiler's choice
+#endif
+#ifndef PSR_SCAL_FORM
+#define PSR_SCAL_FORM 1 // scalloping correction in double: 1 nested fma, 2 unfused, 0 compiler's choice
+#endif
+#ifndef PSR_PP_FORM
+#define PSR_PP_FORM 1 // PRESTO-plus bin f*frac + 0.5 in double: 1 fma, 2 unfused, 0 compiler's choice
+#endif
+#ifndef PSR_DIV_FORM
+#define PSR_DIV_FORM 0 // X / norm of the power spectra: 1 __fdividef, 2 x * (1/norm), 3 IEEE, 4 x * rcp_rn(norm),
+                       // 0 the division operator (fast-math build)
+#endif
+
+__device__ __forceinline__ float psr_sq2(float x, float y)
+{
+#if PSR_POWER_FORM == 1
+    return fmaf(x, x, __fmul_rn(y, y));
+#elif PSR_POWER_FORM == 2
+    return fmaf(y, y, __fmul_rn(x, x));
+#elif PSR_POWER_FORM == 3
+    return __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y));
+#else
+    return x * x + y * y;
+#endif
+}
+
+__device__ __forceinline__ float psr_div(float x, float norm)
+{
+#if PSR_DIV_FORM == 1
+    return __fdividef(x, norm);
+#elif PSR_DIV_FORM == 2
+    return x * (1.0f / norm);
+#elif PSR_DIV_FORM == 3
+    return __fdiv_rn(x, norm);
+#elif PSR_DIV_FORM == 4
+    return __fmul_rn(x, __frcp_rn(norm));
+#else
+    return x / norm;
+#endif
+}
+
+__device__ __forceinline__ float2 psr_scaled(float2 a, float norm) { return make_float2(psr_div(a.x, norm), psr_div(a.y, norm)); }
+__device__ __forceinline__ float psr_power(float2 a) { return psr_sq2(a.x, a.y); }
 __device__ __forceinline__ float psr_interbin(float2 a, float2 b)
 {
-    return 0.616850275f * ((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
+    return 0.616850275f * psr_sq2(a.x - b.x, a.y - b.y);
 }
 
 template <bool VEC4>
@@ -249,7 +301,25 @@ __global__ void k_psr_threshold(const float *__restrict__ in, const uint16_t *__
 // the reference's constants and order, rounded to float
 __device__ __forceinline__ float psr_corrected(float Xm2, float Xm1, float X0, float Xp1, float Xp2)
 {
+#if PSR_SCAL_FORM == 1
+    return (float)fma((0.88494 / 2.0), (double)(Xm2 + Xp2), fma((1.88494 / 2.0), (double)(Xm1 + Xp1), (double)X0));
+#elif PSR_SCAL_FORM == 2
+    return (float)__dadd_rn(__dadd_rn((double)X0, __dmul_rn((1.88494 / 2.0), (double)(Xm1 + Xp1))),
+                            __dmul_rn((0.88494 / 2.0), (double)(Xm2 + Xp2)));
+#else
     return (X0 + (1.88494 / 2.0) * (Xm1 + Xp1) + (0.88494 / 2.0) * (Xm2 + Xp2));
+#endif
+}
+
+__device__ __forceinline__ int psr_pp_bin(int f, double frac)
+{
+#if PSR_PP_FORM == 1
+    return (int)fma((double)f, frac, 0.5);
+#elif PSR_PP_FORM == 2
+    return (int)__dadd_rn(__dmul_rn((double)f, frac), 0.5);
+#else
+    return (int)((((double)f) * frac) + 0.5);
+#endif
 }
 
 constexpr int PSR_COR_TILE = 256;
@@ -341,7 +411,7 @@ __global__ void __launch_bounds__(256) k_harmonic_rows(const float *__restrict__
                 float sum = fund;
                 const double frac = ((double)pos) / ((double)(i + 1));
                 for (int f = 1; f <= i; ++f)
-                    sum = sum + bin((int)((((double)f) * frac) + 0.5), 2);
+                    sum = sum + bin(psr_pp_bin(f, frac), 2);
                 const float snr = fdividef((sum - s_msd[2 * i]), s_msd[2 * i + 1]);
                 if (snr > best) {
                     best = snr;
@@ -400,7 +470,7 @@ __device__ float psr_segment_median(const float2 *__restrict__ spec, int start, 
         x[v] = INFINITY;
         if (e < range && start + e < nSamples) {
             const float2 q = spec[start + e];
-            x[v] = q.x * q.x + q.y * q.y;
+            x[v] = psr_sq2(q.x, q.y);
         }
     }
 #pragma unroll
@@ -479,6 +549,17 @@ __global__ void __launch_bounds__(32 * PSR_WARPS_PER_BLOCK) k_segment_medians_wa
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float psr_scaled_median(float m) { return m * 1.44269504088896; }
 
+__device__ __forceinline__ float psr_interp(float mean, float slope, int i)
+{
+#if PSR_INTERP_FORM == 1
+    return fmaf(slope, (float)i, mean);
+#elif PSR_INTERP_FORM == 2
+    return __fadd_rn(mean, __fmul_rn(slope, (float)i));
+#else
+    return mean + slope * i;
+#endif
+}
+
 __global__ void __launch_bounds__(32 * PSR_WARPS_PER_BLOCK) k_sgp2_spans(const float *__restrict__ medians, float2 *in,
                                                                        const int *__restrict__ seg,
                                                                        long long nSamples, int nSegments)
@@ -520,7 +601,7 @@ __global__ void __launch_bounds__(32 * PSR_WARPS_PER_BLOCK) k_sgp2_spans(const f
     for (int i = lane; i < n; i += 32) {
         const int local_pos = first + i;
         if (local_pos < nSamples) {
-            const float norm = 1.0 / sqrt(previous_mean + slope * i);
+            const float norm = 1.0 / sqrt(psr_interp(previous_mean, slope, i));
             scale(local_pos, norm);
         }
     }
@@ -529,7 +610,7 @@ __global__ void __launch_bounds__(32 * PSR_WARPS_PER_BLOCK) k_sgp2_spans(const f
             const int tail = first + range + t;
             if (tail < nSamples) {
                 const int i = range - t;
-                const float norm = 1.0 / sqrt(previous_mean + slope * i);
+                const float norm = 1.0 / sqrt(psr_interp(previous_mean, slope, i));
                 scale(tail, norm);
             }
         }

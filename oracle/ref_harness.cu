@@ -633,6 +633,12 @@ int aaref_spd(const float *plane, int nDMs, int nT, float tsamp, int inBin, floa
     const size_t n = (size_t)nDMs * (size_t)nT;
     if ((long long)(2 * n) > plane_cap)
         return -1;
+    /* the S/N planes of all iterations hold up to 2 * nDMs * nT values, which
+     * the reference addresses with int offsets (nDMs * output_shift,
+     * src/aa_device_SPS_long.cu:69,73): refuse planes where they could pass
+     * 2^31, where its search faulted */
+    if ((long long)(2 * n) >= (1LL << 31))
+        return -6;
     /* max_ts: analysis_GPU's maxTimeSamples (0 = the plane).  Below the plane
      * the search runs in batches and the whole-plane S/N stage is skipped. */
     const bool whole = (max_ts <= 0 || (size_t)max_ts >= n);
@@ -736,6 +742,8 @@ int aaref_time_spd(const float *d_src, int nDMs, int nT, float tsamp, int inBin,
                    long long max_ts, int reps, float *ms, long long *ncands)
 {
     const size_t n = (size_t)nDMs * (size_t)nT;
+    if ((long long)(2 * n) >= (1LL << 31))
+        return -6; /* int S/N-plane offsets of the reference, as in aaref_spd */
     unsigned long int maxTS = (max_ts <= 0) ? (unsigned long int)n : (unsigned long int)max_ts;
     int max_boxcar_width = (int)(max_boxcar_width_in_sec / tsamp);
     int mwp = 0;

@@ -65,6 +65,21 @@ CASES = {
     # outputs, so this case pins the contraction the reference build uses
     "fma_probe": dict(nchans=512, nbits=8, fch1=1662.862, foff=-0.526171875, tsamp=9.0443e-05, nsamp=1 << 14,
                       plan=[(10.36, 20.05, 0.0763, 1, 1)], free_memory=0, seed=21, pulses=[(14.0, 8, 5.0)]),
+    # 1024 channels x 2^18 samples, 8-bit, 0-500 in steps of 0.5 (1024 trials after rounding), one pulse
+    # of 1 ms at DM 300 and 5 sigma: the plain small configuration at its full size (cache kernel)
+    "plain1024_full": dict(nchans=1024, nbits=8, fch1=1550.0, foff=-0.390625, tsamp=64e-6, nsamp=1 << 18,
+                           plan=[(0, 500, 0.5, 1, 1)], free_memory=0, seed=1, pulses=[(300.0, 16, 5.0)], heavy=True),
+    # more than 8192 channels: the reference reads the delay table from global memory
+    # (shared_dedisperse_kernel_nchan8192p, src/aa_device_dedispersion_kernel.cu:243-301)
+    "wide8": dict(nchans=8320, nbits=8, fch1=1670.0, foff=-300.0 / 8320, tsamp=64e-6, nsamp=1 << 13,
+                  plan=[(0, 25.5, 0.1, 1, 1)], free_memory=0, seed=23, pulses=[(12.0, 8, 4.0)]),
+    # the same band with 16-bit samples: above 8192 channels the reference launches its
+    # constant-memory kernel without filling the table past 8192 entries
+    # (src/aa_device_dedispersion_kernel.cu:540-543); this library computes the intended
+    # delays, so the case is checked against the oracle only
+    "wide16": dict(nchans=8320, nbits=16, fch1=1670.0, foff=-300.0 / 8320, tsamp=64e-6, nsamp=1 << 13,
+                   plan=[(0, 25.5, 0.1, 1, 1)], free_memory=0, seed=24, pulses=[(12.0, 8, 3.0)],
+                   no_reference=True),
     # the survey plan on a short 4096-channel block (every range is shared-kernel)
     "survey_plan": dict(nchans=4096, nbits=8, fch1=1670.0, foff=-0.0732421875, tsamp=64e-6, nsamp=45000,
                         plan=SURVEY_PLAN, free_memory=0, seed=20, pulses=[(400.0, 16, 5.0), (1700.0, 40, 4.0)],

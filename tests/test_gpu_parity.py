@@ -137,6 +137,8 @@ def test_tile_shapes_agree(aa, oracle_mod, cuda_device, tile_words, group_dms, v
                                                  ("shared8_nch3000", 4, "quadws"), ("shared8_nch3000", 5, "quadsp"),
                                                  ("shared8_binned", 6, "quad"), ("shared8_binned", 7, "quad"),
                                                  ("shared8_nch3000", 6, "quad"), ("shared8_nch3000", 7, "quad"),
+                                                 ("shared8_nch3000", 8, "quad"), ("shared8_binned", 8, "quad"),
+                                                 ("shared8_nch3000", 9, "quad"), ("shared8_binned", 9, "quad"),
                                                  ("shared8_nch3000", 3, "sub"), ("shared8_nch3000", 2, "quad"),
                                                  ("shared16", 0, "f32"), ("shared16", 1, "gather"),
                                                  ("cache16", 2, "f32")])
@@ -205,6 +207,21 @@ def test_split_phase_quad_matches_oracle(aa, oracle_mod, golden_ddtr, cuda_devic
         assert SP_REFUSED in str(e), str(e)
         pytest.skip(f"refused: {e}")
     assert all(i["kernel"] == "quadsp" for i in info), [i["kernel"] for i in info]
+    s, want, kern = oracle_run(oracle_mod, case, x)
+    assert_matches_oracle(case, s, got, want, kern)
+    for r, rr in enumerate(golden_ddtr.get(name, {}).get("ranges", [])):
+        assert hashlib.sha256(got[r].tobytes()).hexdigest() == rr["sha256"], f"range {r} differs from the reference GPU"
+
+
+@pytest.mark.parametrize("name", WS_CASES)
+def test_quad_pair_rows_match_oracle(aa, oracle_mod, golden_ddtr, cuda_device, name):
+    """Variant 8 runs the channel-quad pair body (rows summed over the quad,
+    16-bit pairs) on every range without per-byte entries and the channel-quad
+    kernel on the others: bit-identical to the oracle and to the reference GPU."""
+    case = C.CASES[name]
+    x = C.make_input(case)
+    got, info, _, _ = run_pipeline(aa, case, x, variant=8)
+    assert all(i["kernel"] == "quad" for i in info), [i["kernel"] for i in info]
     s, want, kern = oracle_run(oracle_mod, case, x)
     assert_matches_oracle(case, s, got, want, kern)
     for r, rr in enumerate(golden_ddtr.get(name, {}).get("ranges", [])):

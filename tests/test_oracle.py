@@ -151,3 +151,36 @@ def test_windowed_dedispersion_equals_whole_range(oracle_mod, name):
     w2 = O.dedisperse_window(kind, O.FMA_ALL, O.corner_turn(x[sh:L], nch, L - sh), L - sh, nch, dm0, 64, t0, nt,
                              s.dmshifts, m0, ms, d[3], t_shift=sh)
     assert np.array_equal(w2.view(np.uint32), full[dm0:dm0 + 64, t0:t0 + nt].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", [n for n, c in C.CASES.items() if c.get("heavy")])
+def test_oracle_matches_reference_gpu_samples_of_heavy_cases(oracle_mod, golden_ddtr, name):
+    """The cases too large for a whole oracle run here: the oracle's value at
+    each of the golden file's sampled outputs (DM trial, sample) of the
+    single-chunk, unbinned ranges equals the reference GPU's bit for bit."""
+    if name not in golden_ddtr:
+        pytest.skip("case not in the golden file")
+    case = C.CASES[name]
+    rec = golden_ddtr[name]
+    x = C.make_input(case)
+    s = oracle_mod.strategy(case["plan"], case["nchans"], case["nsamp"], case["fch1"], case["foff"], case["tsamp"],
+                            case["nbits"], C.strategy_free_memory(case))
+    assert s.t_processed == rec["strategy"]["t_processed"]
+    if s.num_tchunks != 1:
+        pytest.skip("sampled check covers single-chunk cases")
+    L = s.t_processed[0][0] + s.maxshift
+    flat = oracle_mod.corner_turn(x[:L], case["nchans"], L)
+    checked = 0
+    for r, rr in enumerate(rec["ranges"]):
+        d = s.dm[r]
+        if d[3] != 1:
+            continue
+        tsr = np.float32(case["tsamp"]) * np.float32(d[3])
+        kind = oracle_mod.select_kernel(case["nbits"], d[2], tsr, s.dmshifts[-1])
+        m0, ms = np.float32(np.float32(d[0]) / tsr), np.float32(np.float32(d[2]) / tsr)
+        for i, j, bits in rr["samples"]:
+            v = oracle_mod.dedisperse_window(kind, oracle_mod.FMA_ALL, flat, L, case["nchans"], i, 1, j, 1,
+                                             s.dmshifts, m0, ms, d[3])
+            assert int(v[0, 0].view(np.uint32)) == bits, (r, i, j)
+            checked += 1
+    assert checked > 0

@@ -60,7 +60,7 @@ def write_plan(path, case, s):
         f.write(f"{case['nchans']} {case['nsamp']} {case['nbits']} {case['tsamp']!r} {s.maxshift} {len(s.ndms)} "
                 f"{s.num_tchunks}\n")
         for r, d in enumerate(s.dm):
-            f.write(f"{np.float32(d[0])!r} {np.float32(d[2])!r} {d[3]} {s.ndms[r]}\n")
+            f.write(f"{float(np.float32(d[0]))!r} {float(np.float32(d[2]))!r} {d[3]} {s.ndms[r]}\n")
         for r in range(len(s.ndms)):
             f.write(" ".join(str(v) for v in s.t_processed[r]) + "\n")
         f.write(" ".join(repr(float(v)) for v in s.dmshifts) + "\n")
