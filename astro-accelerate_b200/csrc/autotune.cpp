@@ -10,7 +10,7 @@ bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache 
 {
     const bool quad = (job.variant == 2 || job.variant == 5 || job.variant == 6);
     const auto key = std::make_tuple(job.variant, job.p.nch_used, quad ? job.q.W : job.f.W,
-                                     quad ? job.q.raww : job.f.rawh, quad ? job.q.npool / std::max(1, job.q.qs) : 0,
+                                     quad ? job.q.raww : job.f.rawh, quad ? job.q.maxpat * 1000 + job.q.flavour : 0,
                                      job.p.kind, static_cast<long long>(job.groups));
     int best = -1;
     auto it = cache.best.find(key);
@@ -29,7 +29,6 @@ bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache 
             return false;
         }
         float best_ms = 1e30f;
-        const int maxcnt = quad ? std::max(1, job.q.npool / std::max(1, job.q.qs)) : 0;
         for (int c : cands) {
             DdtrJob t = slice;
             size_t bytes;
@@ -37,7 +36,7 @@ bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache 
                 if (c > 8)
                     continue;
                 t.q.qs = c;
-                t.q.npool = c * maxcnt;
+                t.q.npool = quad_npool(t.q, c);
                 if (job.variant == 5) {
                     bytes = quadws_smem_bytes(t.q);
                 } else if (job.variant == 6) {
@@ -100,9 +99,8 @@ bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache 
         cache.best[key] = best;
     }
     if (quad) {
-        const int maxcnt = std::max(1, job.q.npool / std::max(1, job.q.qs));
         job.q.qs = best;
-        job.q.npool = best * maxcnt;
+        job.q.npool = quad_npool(job.q, best);
     } else {
         job.f.cs = best;
     }

@@ -170,11 +170,10 @@ bool BatchDdtr::build_jobs()
                     d.q = job.q;
                     d.f = job.f;
                     d.variant = job.variant;
-                    const int maxcnt = std::max(1, job.q.npool / std::max(1, job.q.qs));
                     while (persistent_job_smem(d) > 227 * 1024) {
                         if (quadlike && d.q.qs > 1) {
                             d.q.qs /= 2;
-                            d.q.npool = d.q.qs * maxcnt;
+                            d.q.npool = quad_npool(d.q, d.q.qs);
                         } else if (job.variant == 3 && d.f.cs > 4) {
                             d.f.cs /= 2;
                         } else {

@@ -791,12 +791,14 @@ bool aa_b200_pipeline_set_kernel_variant(void *obj, int variant)
     Api *a = as_api(obj);
     if (a->pipe)
         return api_fail(a, "the kernel variant must be set before the plan is bound");
-    if (variant < 0 || variant > 9)
+    if (variant < 0 || variant > 12)
         return api_fail(a, "kernel variant must be 0 (auto), 1 (generic kernels), 2 (channel-quad / fp32 kernels), "
                            "3 (subband / fp32 kernels), 4 (warp-specialised channel-quad / fp32 kernels), 5 "
                            "(split-phase channel-quad / fp32 kernels), 6 (channel-quad with reuse by offset "
                            "pattern / fp32), 7 (channel-quad, 256-sample tiles, two CTAs per SM / fp32), 8 (channel-quad "
-                           "pair rows / fp32) or 9 (channel-quad without register reuse / fp32)");
+                           "pair rows / fp32), 9 (channel-quad without register reuse / fp32), 10 (channel-quad without the "
+                           "per-byte path where a range has none / fp32), 11 (9 and 10) or 12 (11 with 32-bit shared "
+                           "addresses)");
     a->popt.kernel_variant = variant;
     return true;
 }

@@ -200,14 +200,35 @@ __device__ __forceinline__ void quad_sum4_dispatch(uint32_t (&acc)[4][M], const 
     }
 }
 
+// One DM trial's words of a quad row: M 32-bit shared loads at a 32-bit
+// shared address plus immediate offsets (128 bytes apart: the lanes of a warp
+// read 32 consecutive words), each added into the trial's accumulators.
+template <int M, int K = 0> struct QuadRowSum {
+    static __device__ __forceinline__ void add(uint32_t (&acc)[M], unsigned a)
+    {
+        if constexpr (K < M) {
+            uint32_t v;
+            asm volatile("ld.shared.b32 %0, [%1+%2];" : "=r"(v) : "r"(a), "n"(128 * K));
+            acc[K] = __dp4a(v, 0x01010101u, acc[K]);
+            QuadRowSum<M, K + 1>::add(acc, a);
+        }
+    }
+};
+
 // SWITCH: the four trials of a warp (DW = 4) take quad_sum4_dispatch.
 // LOADALL: every trial loads its own words (no register reuse between trials
 // that share an offset): more shared loads, but no data-dependent branch and
 // no register copies in the sum loop.
-template <int M, int DW, bool SWITCH = false, bool LOADALL = false>
+// NOSLOW: no per-byte path (the range has none; an entry of -1 sets
+// DERR_WINDOW), so the sum loop has a single path and the accumulators keep
+// their registers across it.
+// ASM (with NOSLOW and LOADALL): the loads as 32-bit shared addresses with
+// immediate offsets (QuadRowSum).
+template <int M, int DW, bool SWITCH = false, bool LOADALL = false, bool NOSLOW = false, bool ASM = false>
 __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long long t0, uint32_t *sm, unsigned bar0,
                           unsigned &stage_ctr)
 {
+    const unsigned sm_base = smem_addr(sm);
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     constexpr int NW = 64 / DW; // warps (64 DM trials per CTA)
@@ -402,7 +423,37 @@ __device__ bool quad_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, long 
                     ej[4 * h + 3] = e4.w;
                     any_neg |= e4.x | e4.y | e4.z | e4.w;
                 }
-                if (LOADALL && any_neg >= 0) {
+                if (NOSLOW) {
+                    if (any_neg < 0)
+                        atomicOr(p.err, DERR_WINDOW);
+                    if (LOADALL && ASM) {
+#pragma unroll
+                        for (int j = 0; j < DW; ++j)
+                            QuadRowSum<M>::add(acc[j], sm_base + 4u * static_cast<unsigned>(prow + max(ej[j], 0)));
+                    } else if (LOADALL) {
+#pragma unroll
+                        for (int j = 0; j < DW; ++j) {
+                            const uint32_t *src = sm + (prow + max(ej[j], 0));
+#pragma unroll
+                            for (int m = 0; m < M; ++m)
+                                acc[j][m] = __dp4a(src[32 * m], 0x01010101u, acc[j][m]);
+                        }
+                    } else {
+                        uint32_t w[M];
+#pragma unroll
+                        for (int j = 0; j < DW; ++j) {
+                            if (j == 0 || ej[j] != ej[j - 1]) {
+                                const uint32_t *src = sm + (prow + max(ej[j], 0));
+#pragma unroll
+                                for (int m = 0; m < M; ++m)
+                                    w[m] = src[32 * m];
+                            }
+#pragma unroll
+                            for (int m = 0; m < M; ++m)
+                                acc[j][m] = __dp4a(w[m], 0x01010101u, acc[j][m]);
+                        }
+                    }
+                } else if (LOADALL && any_neg >= 0) {
 #pragma unroll
                     for (int j = 0; j < DW; ++j) {
                         const uint32_t *src = sm + (prow + ej[j]);
@@ -672,7 +723,8 @@ __device__ bool quad_pair_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, 
     __syncthreads();
     issue(QNSTAGE - 1);
 
-    int quads_since_flush = 0;
+    // at most 64 quads between two moves of the 16-bit sums (QS <= 8)
+    const int stages_per_flush = 64 / QS;
     for (int s = 0; s < nstages; ++s) {
         if (s + 1 < nstages)
             build(s + 1, (s + 1) & 1);
@@ -696,12 +748,10 @@ __device__ bool quad_pair_body(const DdtrLaunch &p, const QuadLaunch &Q, int g, 
                         a16[j][m] += src[32 * m];
                 }
                 rbase += static_cast<int>(sm[o_pat + (slot * QS + q) * 16 + 15]);
-                if (++quads_since_flush == 64) {
-                    flush();
-                    quads_since_flush = 0;
-                }
             }
         }
+        if ((s + 1) % stages_per_flush == 0)
+            flush();
         fence_proxy_async();
         __syncthreads();
         issue(s + QNSTAGE);

@@ -104,10 +104,13 @@ struct QuadLaunch {
     int qs;    // channel quads per stage
     int npool; // pre-skewed rows per stage buffer
     int M;     // outputs per lane per DM trial (tile = 32*M)
+    int maxpat;      // most patterns of one quad in a DM group
+    int npool_qs[4]; // pre-skewed rows a stage of 1, 2, 4, 8 quads needs at most (0: qs x maxpat)
     int flavour; // 0: per-trial reuse test; 1: reuse by a switch over the warp's offset pattern
                  // (M = 16); 2: M = 8 with 16 warps and two CTAs per SM; 3: the pair body
                  // (rows summed over the quad, 16-bit pairs; pair-mode offsets; M = 16);
-                 // 4: every DM trial loads its own words (M = 16)
+                 // 4: every DM trial loads its own words (M = 16); 5: no per-byte path
+                 // (M = 16, ranges without per-byte entries); 6: 4 and 5
 };
 
 struct QuadGeometry {
@@ -115,7 +118,15 @@ struct QuadGeometry {
     size_t smem_bytes;
 };
 
-QuadGeometry quad_geometry(int span, int dmax, int maxcnt, int group_dms, int nquads, int out_words, int qs);
+QuadGeometry quad_geometry(int span, int dmax, int maxcnt, int group_dms, int nquads, int out_words, int qs,
+                           int npool = 0);
+// Rows a stage of qs quads needs: the table of the range when it has one,
+// else qs x the most patterns of a quad.
+inline int quad_npool(const QuadLaunch &q, int qs)
+{
+    const int k = (qs == 1) ? 0 : (qs == 2) ? 1 : (qs == 4) ? 2 : (qs == 8) ? 3 : -1;
+    return (k >= 0 && q.npool_qs[k] > 0) ? q.npool_qs[k] : qs * (q.maxpat > 0 ? q.maxpat : 1);
+}
 cudaError_t launch_quad_patterns(const int32_t *table, int nch_used, int ndms, int group_dms, int nquads, int nq_pad,
                                  int32_t *qpat, int32_t *qwin, int32_t *qtmp, int *stats, cudaStream_t st);
 cudaError_t launch_quad_offsets(const int32_t *qtmp, size_t n, int W, int32_t *qoff, cudaStream_t st,

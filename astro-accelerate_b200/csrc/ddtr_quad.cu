@@ -109,7 +109,7 @@ __global__ void k_quad_offsets(const int32_t *__restrict__ qtmp, size_t n, int W
 // M = 16: 16 warps x 4 DM trials, one CTA per SM (127 registers);
 // M = 8: 8 warps x 8 DM trials, two CTAs per SM, so that one CTA issues
 // while the other waits at its stage barrier.
-template <int M, int DW, bool SWITCH, int MINB, bool LOADALL = false>
+template <int M, int DW, bool SWITCH, int MINB, bool LOADALL = false, bool NOSLOW = false, bool ASM = false>
 __global__ void __launch_bounds__(32 * 64 / DW, MINB) k_ddtr_quad(const DdtrLaunch p, const QuadLaunch Q)
 {
     extern __shared__ __align__(16) uint32_t sm[];
@@ -117,8 +117,9 @@ __global__ void __launch_bounds__(32 * 64 / DW, MINB) k_ddtr_quad(const DdtrLaun
     body::init_barriers(bar0);
     __syncthreads();
     unsigned stage_ctr = 0;
-    body::quad_body<M, DW, SWITCH, LOADALL>(p, Q, blockIdx.x, static_cast<long long>(blockIdx.y) * (32 * M),
-                                            sm + body::BAR_WORDS, bar0, stage_ctr);
+    body::quad_body<M, DW, SWITCH, LOADALL, NOSLOW, ASM>(p, Q, blockIdx.x,
+                                                         static_cast<long long>(blockIdx.y) * (32 * M),
+                                                         sm + body::BAR_WORDS, bar0, stage_ctr);
 }
 
 // 16 consumer + WS_PROD producer warps (body::quad_ws_body); five warps per
@@ -218,14 +219,14 @@ cudaError_t launch_quad_offsets(const int32_t *qtmp, size_t n, int W, int32_t *q
     return cudaGetLastError();
 }
 
-QuadGeometry quad_geometry(int span, int dmax, int maxcnt, int group_dms, int nquads, int out_words, int qs)
+QuadGeometry quad_geometry(int span, int dmax, int maxcnt, int group_dms, int nquads, int out_words, int qs, int npool)
 {
     QuadGeometry G;
     G.M = out_words;
     G.W = ((span + 32 * out_words) + 3) & ~3;
     G.raww = ((((15 + G.W + dmax + 3) >> 2) + 2) + 3) & ~3;
     G.qs = qs;
-    G.npool = qs * (maxcnt > 0 ? maxcnt : 1);
+    G.npool = npool > 0 ? npool : qs * (maxcnt > 0 ? maxcnt : 1);
     G.nq_pad = (nquads + 3) & ~3;
     G.smem_bytes = 4 * (body::BAR_WORDS + body::quad_body_words(qs, group_dms, G.raww, G.nq_pad, G.npool, G.W));
     return G;
@@ -253,6 +254,12 @@ cudaError_t launch_ddtr_quad(const DdtrLaunch &p, const QuadLaunch &q, cudaStrea
         return launch_quad_instance(k_ddtr_quadpair, 512, p, q, smem, st);
     if (q.M == 16 && q.flavour == 4)
         return launch_quad_instance(k_ddtr_quad<16, 4, false, 1, true>, 512, p, q, smem, st);
+    if (q.M == 16 && q.flavour == 5)
+        return launch_quad_instance(k_ddtr_quad<16, 4, false, 1, false, true>, 512, p, q, smem, st);
+    if (q.M == 16 && q.flavour == 6)
+        return launch_quad_instance(k_ddtr_quad<16, 4, false, 1, true, true>, 512, p, q, smem, st);
+    if (q.M == 16 && q.flavour == 7)
+        return launch_quad_instance(k_ddtr_quad<16, 4, false, 1, true, true, true>, 512, p, q, smem, st);
     if (q.M == 8 && q.flavour == 2)
         return launch_quad_instance(k_ddtr_quad<8, 4, true, 2>, 512, p, q, smem, st);
     if (q.M == 8)

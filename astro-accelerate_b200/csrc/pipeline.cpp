@@ -12,6 +12,14 @@
 
 namespace aab200 {
 
+// Rows a stage of qs channel quads of the range needs.
+static int rc_npool(const RangeConfig &rc, int qs)
+{
+    const int k = (qs == 1) ? 0 : (qs == 2) ? 1 : (qs == 4) ? 2 : (qs == 8) ? 3 : -1;
+    return (k >= 0 && rc.quad_npool_qs[k] > 0) ? rc.quad_npool_qs[k] : qs * std::max(1, rc.quad_maxcnt);
+}
+
+
 namespace {
 constexpr int kMaxSmemOptin = 227 * 1024;
 }
@@ -136,7 +144,8 @@ bool DdtrPipeline::build_range(int r)
     if (elem_bytes_ == 1 &&
         (opt_.kernel_variant == 0 || opt_.kernel_variant == 2 || opt_.kernel_variant == 4 ||
          opt_.kernel_variant == 5 || opt_.kernel_variant == 6 || opt_.kernel_variant == 7 ||
-         opt_.kernel_variant == 8 || opt_.kernel_variant == 9) &&
+         opt_.kernel_variant == 8 || opt_.kernel_variant == 9 || opt_.kernel_variant == 10 ||
+         opt_.kernel_variant == 11 || opt_.kernel_variant == 12) &&
         rc.group_dms == 64) {
         if (!build_quad_tables(r))
             return false;
@@ -158,7 +167,7 @@ bool DdtrPipeline::build_range(int r)
         if (qs == 0)
             return fail("the split-phase channel-quad kernel cannot run range " + std::to_string(r) +
                         " (entries on the per-byte path, or its stage does not fit shared memory)");
-        rc.quad.npool = qs * std::max(1, rc.quad.npool / std::max(1, rc.quad.qs));
+        rc.quad.npool = rc_npool(rc, qs);
         rc.quad.qs = qs;
         rc.variant = 6;
     }
@@ -210,18 +219,40 @@ bool DdtrPipeline::build_quad_tables(int r)
               check_cuda(cudaMemcpyAsync(hs, d_stats, 4 * sizeof(int), cudaMemcpyDeviceToHost, st_), "D2H") &&
               check_cuda(cudaStreamSynchronize(st_), "sync");
     ++launches_;
+    std::vector<int> counts(static_cast<size_t>(ngroups) * nquads);
+    if (ok)
+        // the pattern count (word 15) of every (group, quad)
+        ok = check_cuda(cudaMemcpy2D(counts.data(), sizeof(int), rc.d_qpat + 15, 16 * sizeof(int32_t), sizeof(int),
+                                     counts.size(), cudaMemcpyDeviceToHost),
+                        "D2H");
     if (ok) {
         rc.quad_ws_ok = (hs[3] == 0);
         rc.quad_span = hs[0];
         rc.quad_dmax = hs[1];
         rc.quad_maxcnt = hs[2];
         rc.nquads = nquads;
+        // rows a stage really needs: the largest sum of pattern counts over
+        // the quads of a stage, for each stage depth
+        for (int k = 0; k < 4; ++k) {
+            const int qs_k = 1 << k;
+            int most = 0;
+            for (int g = 0; g < ngroups; ++g)
+                for (int q0 = 0; q0 < nquads; q0 += qs_k) {
+                    int tot = 0;
+                    for (int q = q0; q < std::min(nquads, q0 + qs_k); ++q)
+                        tot += counts[static_cast<size_t>(g) * nquads + q];
+                    most = std::max(most, tot);
+                }
+            rc.quad_npool_qs[k] = std::max(1, most);
+        }
+        auto npool_for = [&](int qs_) { return rc.quad_npool_qs[qs_ == 1 ? 0 : qs_ == 2 ? 1 : qs_ == 4 ? 2 : 3]; };
         const int M = (opt_.tile_words == 2 || opt_.kernel_variant == 7) ? 8 : 16;
-        int qs = 4;
-        QuadGeometry G = quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, nquads, M, qs);
+        int qs = 8;
+        QuadGeometry G =
+            quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, nquads, M, qs, npool_for(qs));
         while (G.smem_bytes > kStagedSmemLimit && qs > 1) {
             qs /= 2;
-            G = quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, nquads, M, qs);
+            G = quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, nquads, M, qs, npool_for(qs));
         }
         if (G.smem_bytes <= kStagedSmemLimit && rc.quad_dmax <= 255) {
             rc.quad = G;
@@ -331,10 +362,9 @@ int DdtrPipeline::quad_sp_depth(const RangeConfig &rc) const
     q.raww = rc.quad.raww;
     q.nq_pad = rc.quad.nq_pad;
     q.W = rc.quad.W;
-    const int maxcnt = std::max(1, rc.quad.npool / std::max(1, rc.quad.qs));
     for (int qs = rc.quad.qs; qs >= 1; qs /= 2) {
         q.qs = qs;
-        q.npool = qs * maxcnt;
+        q.npool = rc_npool(rc, qs);
         if (quadsp_smem_bytes(q) <= kStagedSmemLimit)
             return qs;
     }
@@ -648,7 +678,7 @@ bool DdtrPipeline::tune_ranges()
                 return fail(err);
             const QuadGeometry keep = rc.quad;
             const int qs = quad_sp_depth(rc);
-            rc.quad.npool = qs * std::max(1, rc.quad.npool / std::max(1, rc.quad.qs));
+            rc.quad.npool = rc_npool(rc, qs);
             rc.quad.qs = qs;
             rc.variant = 6;
             DdtrJob jsp;
@@ -843,8 +873,14 @@ bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, f
         q.qs = rc.quad.qs;
         q.npool = rc.quad.npool;
         q.M = rc.quad.M;
-        q.flavour = rc.quad_pairs                                ? 3
-                    : (opt_.kernel_variant == 9 && q.M == 16) ? 4
+        q.maxpat = rc.quad_maxcnt;
+        for (int k = 0; k < 4; ++k)
+            q.npool_qs[k] = rc.quad_npool_qs[k];
+        q.flavour = rc.quad_pairs                                              ? 3
+                    : (opt_.kernel_variant == 10 && q.M == 16 && rc.quad_ws_ok) ? 5
+                    : (opt_.kernel_variant == 11 && q.M == 16 && rc.quad_ws_ok) ? 6
+                    : (opt_.kernel_variant == 12 && q.M == 16 && rc.quad_ws_ok) ? 7
+                    : (opt_.kernel_variant == 9 && q.M == 16)               ? 4
                     : (opt_.kernel_variant == 6 && q.M == 16) ? 1
                     : (opt_.kernel_variant == 7 && q.M == 8)  ? 2
                                                               : 0;

@@ -134,6 +134,7 @@ struct RangeConfig {
     int variant = 1;
     QuadGeometry quad{};
     int quad_span = 0, quad_dmax = 0, quad_maxcnt = 0, nquads = 0;
+    int quad_npool_qs[4] = {0, 0, 0, 0}; // rows a stage of 1, 2, 4, 8 quads needs (largest over groups and stages)
     int32_t *d_qpat = nullptr;
     int32_t *d_qwin = nullptr;
     int32_t *d_qoff = nullptr;

@@ -33,7 +33,10 @@ constexpr int PSR_PAIR_THREADS = 256;
 // The forms used are those that give the reference's bits on the golden
 // spectra (tests/golden/psr_golden.json).
 #ifndef PSR_POWER_FORM
-#define PSR_POWER_FORM 1 // x*x + y*y: 1 fma(x,x,y*y), 2 fma(y,y,x*x), 3 unfused, 0 compiler's choice
+#define PSR_POWER_FORM 2 // power spectra x*x + y*y: 1 fma(x,x,y*y), 2 fma(y,y,x*x), 3 unfused, 0 compiler's choice
+#endif
+#ifndef PSR_MEDIAN_POWER_FORM
+#define PSR_MEDIAN_POWER_FORM 1 // powers of the whitening medians, the same choices
 #endif
 #ifndef PSR_INTERP_FORM
 #define PSR_INTERP_FORM 1 // mean + slope*i: 1 fma, 2 unfused, 0 compiler's choice
@@ -45,21 +48,19 @@ constexpr int PSR_PAIR_THREADS = 256;
 #define PSR_PP_FORM 1 // PRESTO-plus bin f*frac + 0.5 in double: 1 fma, 2 unfused, 0 compiler's choice
 #endif
 #ifndef PSR_DIV_FORM
-#define PSR_DIV_FORM 0 // X / norm of the power spectra: 1 __fdividef, 2 x * (1/norm), 3 IEEE, 4 x * rcp_rn(norm),
+#define PSR_DIV_FORM 4 // X / norm of the power spectra: 1 __fdividef, 2 x * (1/norm), 3 IEEE, 4 x * rcp_rn(norm),
                        // 0 the division operator (fast-math build)
 #endif
 
-__device__ __forceinline__ float psr_sq2(float x, float y)
+template <int FORM> __device__ __forceinline__ float psr_sq2(float x, float y)
 {
-#if PSR_POWER_FORM == 1
-    return fmaf(x, x, __fmul_rn(y, y));
-#elif PSR_POWER_FORM == 2
-    return fmaf(y, y, __fmul_rn(x, x));
-#elif PSR_POWER_FORM == 3
-    return __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y));
-#else
+    if (FORM == 1)
+        return fmaf(x, x, __fmul_rn(y, y));
+    if (FORM == 2)
+        return fmaf(y, y, __fmul_rn(x, x));
+    if (FORM == 3)
+        return __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y));
     return x * x + y * y;
-#endif
 }
 
 __device__ __forceinline__ float psr_div(float x, float norm)
@@ -78,10 +79,10 @@ __device__ __forceinline__ float psr_div(float x, float norm)
 }
 
 __device__ __forceinline__ float2 psr_scaled(float2 a, float norm) { return make_float2(psr_div(a.x, norm), psr_div(a.y, norm)); }
-__device__ __forceinline__ float psr_power(float2 a) { return psr_sq2(a.x, a.y); }
+__device__ __forceinline__ float psr_power(float2 a) { return psr_sq2<PSR_POWER_FORM>(a.x, a.y); }
 __device__ __forceinline__ float psr_interbin(float2 a, float2 b)
 {
-    return 0.616850275f * psr_sq2(a.x - b.x, a.y - b.y);
+    return 0.616850275f * psr_sq2<PSR_POWER_FORM>(a.x - b.x, a.y - b.y);
 }
 
 template <bool VEC4>
@@ -470,7 +471,7 @@ __device__ float psr_segment_median(const float2 *__restrict__ spec, int start, 
         x[v] = INFINITY;
         if (e < range && start + e < nSamples) {
             const float2 q = spec[start + e];
-            x[v] = psr_sq2(q.x, q.y);
+            x[v] = psr_sq2<PSR_MEDIAN_POWER_FORM>(q.x, q.y);
         }
     }
 #pragma unroll

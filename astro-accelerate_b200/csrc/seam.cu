@@ -63,7 +63,7 @@ struct SeamRange {
     bool quad = false, f32 = false;
     QuadGeometry qg{};
     F32Launch fl{};
-    int nquads = 0;
+    int nquads = 0, maxpat = 0;
     int32_t *d_table = nullptr, *d_wmin = nullptr, *d_qpat = nullptr, *d_qwin = nullptr, *d_qoff = nullptr;
     ~SeamRange()
     {
@@ -194,6 +194,7 @@ bool build_range(SeamRange &R, const float *dmshifts, std::string &err)
                  check(cudaStreamSynchronize(st), err, "sync");
             R.qg = G;
             R.nquads = nquads;
+            R.maxpat = hs[2];
             R.quad = ok;
         } else {
             err = "the delay span of this range does not fit the channel-quad kernel";
@@ -354,6 +355,7 @@ int aa_b200_seam_dedisperse(int i, int t_processed, int *inBin, float *dmshifts,
             q.qs = R->qg.qs;
             q.npool = R->qg.npool;
             q.M = R->qg.M;
+            q.maxpat = R->maxpat;
             q.flavour = 0;
             e = launch_ddtr_quad(p, q, st);
         } else {

@@ -139,6 +139,9 @@ def test_tile_shapes_agree(aa, oracle_mod, cuda_device, tile_words, group_dms, v
                                                  ("shared8_nch3000", 6, "quad"), ("shared8_nch3000", 7, "quad"),
                                                  ("shared8_nch3000", 8, "quad"), ("shared8_binned", 8, "quad"),
                                                  ("shared8_nch3000", 9, "quad"), ("shared8_binned", 9, "quad"),
+                                                 ("shared8_nch3000", 10, "quad"), ("shared8_binned", 10, "quad"),
+                                                 ("shared8_nch3000", 11, "quad"), ("shared8_binned", 11, "quad"),
+                                                 ("shared8_nch3000", 12, "quad"), ("shared8_binned", 12, "quad"),
                                                  ("shared8_nch3000", 3, "sub"), ("shared8_nch3000", 2, "quad"),
                                                  ("shared16", 0, "f32"), ("shared16", 1, "gather"),
                                                  ("cache16", 2, "f32")])
