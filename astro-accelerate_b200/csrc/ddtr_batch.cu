@@ -65,7 +65,9 @@ __global__ void __launch_bounds__(body::NTHREADS, 1)
         const int g = static_cast<int>(li % jd.groups);
         const long long t0 = (li / jd.groups) * (32 * BATCH_M);
         bool ok;
-        if (jd.variant == 2)
+        if (jd.variant == 2 && jd.q.flavour == 7)
+            ok = body::quad_body<BATCH_M, 4, false, true, true, true>(jd.p, jd.q, g, t0, area, bar0, stage_ctr);
+        else if (jd.variant == 2)
             ok = body::quad_body<BATCH_M, 4>(jd.p, jd.q, g, t0, area, bar0, stage_ctr);
         else if (jd.variant == 6)
             ok = body::quad_sp_body<BATCH_M>(jd.p, jd.q, g, t0, area, bar0, sp_ctr);

@@ -876,14 +876,18 @@ bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, f
         q.maxpat = rc.quad_maxcnt;
         for (int k = 0; k < 4; ++k)
             q.npool_qs[k] = rc.quad_npool_qs[k];
+        // the default on a range without per-byte entries: one load per DM
+        // trial and no per-byte path in the sum loop (flavour 7); with
+        // per-byte entries the kernel that has that path (flavour 0)
+        const bool plain = opt_.kernel_variant == 0 || opt_.kernel_variant == 2 || opt_.kernel_variant == 12;
         q.flavour = rc.quad_pairs                                              ? 3
                     : (opt_.kernel_variant == 10 && q.M == 16 && rc.quad_ws_ok) ? 5
                     : (opt_.kernel_variant == 11 && q.M == 16 && rc.quad_ws_ok) ? 6
-                    : (opt_.kernel_variant == 12 && q.M == 16 && rc.quad_ws_ok) ? 7
-                    : (opt_.kernel_variant == 9 && q.M == 16)               ? 4
-                    : (opt_.kernel_variant == 6 && q.M == 16) ? 1
-                    : (opt_.kernel_variant == 7 && q.M == 8)  ? 2
-                                                              : 0;
+                    : (plain && q.M == 16 && rc.quad_ws_ok)                     ? 7
+                    : (opt_.kernel_variant == 9 && q.M == 16)                   ? 4
+                    : (opt_.kernel_variant == 6 && q.M == 16)                   ? 1
+                    : (opt_.kernel_variant == 7 && q.M == 8)                    ? 2
+                                                                                : 0;
     } else if (job.variant == 3) {
         job.f = rc.f32;
     } else if (job.variant == 4) {
