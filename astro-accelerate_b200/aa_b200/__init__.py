@@ -175,6 +175,7 @@ def lib():
         "aa_b200_pipeline_range_info": ([vp, i, P(i), P(i), P(i), P(i)], i),
         "aa_b200_pipeline_kernel_launches": ([vp], ll),
         "aa_b200_pipeline_stage_depth": ([vp, i], i),
+        "aa_b200_pipeline_range_kernel": ([vp, i, P(i), P(i), P(i), P(i)], i),
         "aa_b200_pipeline_last_error": ([vp], ctypes.c_char_p),
         "aa_b200_pipeline_num_tchunks": ([vp], i),
         "aa_b200_pipeline_maxshift": ([vp], i),
@@ -227,6 +228,7 @@ def lib():
         "aa_b200_psr_last_error": ([], ctypes.c_char_p),
         "aa_b200_psr_whitening": ([vp, ctypes.c_size_t, i, vp], i),
         "aa_b200_psr_segment_sizes": ([ctypes.c_size_t, vp, i], i),
+        "aa_b200_psr_segment_medians": ([vp, ctypes.c_size_t, i, vp, i, vp, vp], i),
         "aa_b200_psr_candidates_process": ([vp, ctypes.c_size_t, vp, ctypes.c_double, ctypes.c_double,
                                             ctypes.c_double, ctypes.c_size_t, f, i], i),
         "aa_b200_psr_candidates_create": ([], vp),
@@ -582,7 +584,17 @@ class aa_py_pipeline:
                            "gather" if k.value & 0x400 else "sub" if k.value & 0x800 else "quadws" if k.value & 0x1000
                            else "quadsp" if k.value & 0x2000 else "phase"),
                 "stage_depth": lib().aa_b200_pipeline_stage_depth(self.m_obj, r),
-                "group_dms": g.value, "span": s.value, "tile_words": t.value}
+                "group_dms": g.value, "span": s.value, "tile_words": t.value, **self.range_kernel(r)}
+
+    def range_kernel(self, r: int) -> dict:
+        """The kernel shape range r runs after set-up: channel-quad flavour
+        (-1 for other kernels), output tile (DM trials x samples per CTA) and
+        DM trials per warp."""
+        f, d, t, w = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        if lib().aa_b200_pipeline_range_kernel(self.m_obj, r, ctypes.byref(f), ctypes.byref(d), ctypes.byref(t),
+                                               ctypes.byref(w)):
+            raise RuntimeError(self.last_error())
+        return {"flavour": f.value, "tile": [d.value, t.value], "dms_per_warp": w.value}
 
     def time_kernels(self, on: bool = True):
         return bool(lib().aa_b200_pipeline_time_kernels(self.m_obj, int(on)))

@@ -9,6 +9,14 @@
 // on a slice of the job -- about two CTAs per SM -- with CUDA events, keeps
 // the fastest, and caches it by the job's shape.  The slice writes into the
 // job's own output rows, which the real run overwrites.
+//
+// The plain pipeline (DdtrPipeline::tune_ranges) searches further per range
+// with the same slice timing: the channel-quad output tile (64 DM trials x
+// 512 samples, or x 256 samples with 8 or 4 DM trials per warp), the sum-loop
+// flavour, each at its own tuned depth; then the split-phase and subband
+// kernels against the winner.  The DM-group size (64) is fixed by the staged
+// kernels' tables; the generic kernels take tile words and group sizes from
+// the options.
 #pragma once
 #include <map>
 #include <string>

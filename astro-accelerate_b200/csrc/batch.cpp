@@ -201,6 +201,7 @@ bool BatchDdtr::build_jobs()
     pjobs_.clear();
     total_items_ = 0;
     smem_ = 0;
+    split_phase_ = false;
     for (const Staged &s : staged) {
         BatchJobDev d{};
         d.p = s.job.p;
@@ -211,12 +212,13 @@ bool BatchDdtr::build_jobs()
         d.item0 = total_items_;
         total_items_ += static_cast<long long>(s.job.groups) * s.job.tiles;
         smem_ = std::max(smem_, persistent_job_smem(d));
+        split_phase_ = split_phase_ || d.variant == 6;
         pjobs_.push_back(d);
     }
     if (!pjobs_.empty()) {
         if (smem_ > 227 * 1024)
             return fail("persistent kernel shared memory above the per-CTA limit");
-        const int per_sm = persistent_blocks_per_sm(smem_);
+        const int per_sm = persistent_blocks_per_sm(smem_, split_phase_);
         if (per_sm < 1)
             return fail("the persistent kernel does not fit an SM");
         int nsm = 148;
@@ -275,7 +277,7 @@ bool BatchDdtr::issue_work(cudaStream_t st)
     if (!pjobs_.empty()) {
         if (!check_cuda(cudaMemsetAsync(d_counter_, 0, sizeof(unsigned long long), st), "memset") ||
             !check_cuda(launch_ddtr_persistent(d_jobs_, static_cast<int>(pjobs_.size()), total_items_, d_counter_, smem_,
-                                               grid_, st),
+                                               grid_, split_phase_, st),
                         "persistent dedispersion"))
             return false;
         ++launches;

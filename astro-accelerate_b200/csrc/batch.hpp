@@ -120,6 +120,7 @@ private:
     long long total_items_ = 0;
     size_t smem_ = 0;
     int grid_ = 0;
+    bool split_phase_ = false; // a split-phase job among the persistent ones
     size_t level_bytes_ = 0;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;

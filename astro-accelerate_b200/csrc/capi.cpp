@@ -931,7 +931,25 @@ int aa_b200_pipeline_stage_depth(void *obj, int range)
     if (!a->pipe || !a->pipe->setup() || range < 0 || range >= static_cast<int>(a->pipe->strategy().nranges()))
         return 0;
     const RangeConfig &rc = a->pipe->range_config(range);
-    return (rc.variant == 2 || rc.variant == 5) ? rc.quad.qs : (rc.variant == 3 ? rc.f32.cs : (rc.variant == 4 ? 1 : 0));
+    return (rc.variant == 2 || rc.variant == 5 || rc.variant == 6) ? rc.quad.qs
+                                                                   : (rc.variant == 3 ? rc.f32.cs : (rc.variant == 4 ? 1 : 0));
+}
+
+int aa_b200_pipeline_range_kernel(void *obj, int range, int *flavour, int *tile_dms, int *tile_samples,
+                                  int *dms_per_warp)
+{
+    Api *a = as_api(obj);
+    if (!a->pipe || !a->pipe->setup() || range < 0 || range >= static_cast<int>(a->pipe->strategy().nranges()))
+        return 1;
+    const RangeConfig &rc = a->pipe->range_config(range);
+    const bool quadlike = rc.variant == 2 || rc.variant == 5 || rc.variant == 6;
+    *flavour = (rc.variant == 2) ? a->pipe->quad_flavour_of(rc) : -1;
+    *tile_dms = rc.group_dms;
+    *tile_samples = quadlike ? 32 * rc.quad.M : ((rc.variant == 3 || rc.variant == 4) ? 512 : 128 * rc.tile_words);
+    // M = 8 with flavour 0 runs 8 warps of 8 DM trials; every other staged
+    // channel-quad form 16 warps of 4
+    *dms_per_warp = quadlike ? ((rc.quad.M == 8 && *flavour != 2) ? 8 : 4) : 0;
+    return 0;
 }
 
 long long aa_b200_pipeline_kernel_launches(void *obj)

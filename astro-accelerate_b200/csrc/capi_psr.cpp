@@ -81,6 +81,18 @@ int aa_b200_psr_whitening(void *d_spectra, size_t nSamples, int nDMs, void *stre
                       "spectral whitening");
 }
 
+int aa_b200_psr_segment_medians(const void *d_spectra, size_t nSamples, int nDMs, const int *segments,
+                                int nSegments, float *d_medians, void *stream)
+{
+    if (!d_spectra || !segments || !d_medians) {
+        g_psr_error = "segment medians: null pointer";
+        return 1;
+    }
+    return psr_status(psr_segment_medians(static_cast<const float2 *>(d_spectra), nSamples, nDMs, segments,
+                                          nSegments, d_medians, static_cast<cudaStream_t>(stream)),
+                      "segment medians");
+}
+
 int aa_b200_psr_segment_sizes(size_t nSamples, int *out, int cap)
 {
     const std::vector<int> s = psr_segment_sizes(6, 250, nSamples);

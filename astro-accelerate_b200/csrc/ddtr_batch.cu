@@ -28,6 +28,10 @@ static_assert(sizeof(BatchJobDev) % 4 == 0, "job descriptor is copied word by wo
 static_assert((body::BAR_WORDS + JD_WORDS) % 4 == 0, "the body area must start on a 16-byte boundary");
 constexpr int BATCH_M = 16;
 
+// SP: the instance that also holds the split-phase body (jobs of variant 6);
+// without it the other bodies fit the 128 registers a thread has at 512
+// threads without spilling.
+template <bool SP>
 __global__ void __launch_bounds__(body::NTHREADS, 1)
     k_ddtr_persistent(const BatchJobDev *__restrict__ jobs, int njobs, long long total_items,
                       unsigned long long *__restrict__ counter)
@@ -69,10 +73,12 @@ __global__ void __launch_bounds__(body::NTHREADS, 1)
             ok = body::quad_body<BATCH_M, 4, false, true, true, true>(jd.p, jd.q, g, t0, area, bar0, stage_ctr);
         else if (jd.variant == 2)
             ok = body::quad_body<BATCH_M, 4>(jd.p, jd.q, g, t0, area, bar0, stage_ctr);
-        else if (jd.variant == 6)
+        else if (SP && jd.variant == 6)
             ok = body::quad_sp_body<BATCH_M>(jd.p, jd.q, g, t0, area, bar0, sp_ctr);
-        else
+        else if (jd.variant == 3)
             ok = body::f32_body<BATCH_M>(jd.p, jd.f, g, t0, area, bar0, stage_ctr);
+        else
+            ok = false; // a job this instance has no body for (the host never issues one)
         fence_proxy_async();
         // a tile whose copies timed out ends this CTA (the flag is set); the
         // decision is block-wide so that no thread is left at a barrier
@@ -95,30 +101,36 @@ size_t persistent_job_smem(const BatchJobDev &j)
     return 4 * (body::BAR_WORDS + JD_WORDS + words);
 }
 
-int persistent_blocks_per_sm(size_t smem_bytes)
+int persistent_blocks_per_sm(size_t smem_bytes, bool split_phase)
 {
-    if (cudaFuncSetAttribute(k_ddtr_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem_bytes)) != cudaSuccess)
+    const void *fn = split_phase ? reinterpret_cast<const void *>(k_ddtr_persistent<true>)
+                                 : reinterpret_cast<const void *>(k_ddtr_persistent<false>);
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_bytes)) !=
+        cudaSuccess)
         return 0;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ddtr_persistent, body::NTHREADS, smem_bytes) !=
-        cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, body::NTHREADS, smem_bytes) != cudaSuccess)
         return 0;
     return n;
 }
 
 cudaError_t launch_ddtr_persistent(const BatchJobDev *jobs, int njobs, long long total_items,
-                                   unsigned long long *counter, size_t smem_bytes, int grid, cudaStream_t st)
+                                   unsigned long long *counter, size_t smem_bytes, int grid, bool split_phase,
+                                   cudaStream_t st)
 {
     if (njobs <= 0 || total_items <= 0)
         return cudaSuccess;
     if (grid <= 0 || smem_bytes > 227 * 1024)
         return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(k_ddtr_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem_bytes));
+    const void *fn = split_phase ? reinterpret_cast<const void *>(k_ddtr_persistent<true>)
+                                 : reinterpret_cast<const void *>(k_ddtr_persistent<false>);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_bytes));
     if (e != cudaSuccess)
         return e;
-    k_ddtr_persistent<<<grid, body::NTHREADS, smem_bytes, st>>>(jobs, njobs, total_items, counter);
+    if (split_phase)
+        k_ddtr_persistent<true><<<grid, body::NTHREADS, smem_bytes, st>>>(jobs, njobs, total_items, counter);
+    else
+        k_ddtr_persistent<false><<<grid, body::NTHREADS, smem_bytes, st>>>(jobs, njobs, total_items, counter);
     return cudaGetLastError();
 }
 

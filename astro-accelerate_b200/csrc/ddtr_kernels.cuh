@@ -210,10 +210,13 @@ struct BatchJobDev {
 
 // Dynamic shared memory of one job in the persistent kernel.
 size_t persistent_job_smem(const BatchJobDev &j);
-// CTAs of the persistent kernel that fit one SM at this dynamic shared memory.
-int persistent_blocks_per_sm(size_t smem_bytes);
-// counter: device work counter, zero before the launch.
+// CTAs of the persistent kernel that fit one SM at this dynamic shared memory
+// (split_phase: the instance that runs split-phase jobs too).
+int persistent_blocks_per_sm(size_t smem_bytes, bool split_phase);
+// counter: device work counter, zero before the launch; split_phase must be
+// true when any job is of variant 6.
 cudaError_t launch_ddtr_persistent(const BatchJobDev *jobs, int njobs, long long total_items,
-                                   unsigned long long *counter, size_t smem_bytes, int grid, cudaStream_t st);
+                                   unsigned long long *counter, size_t smem_bytes, int grid, bool split_phase,
+                                   cudaStream_t st);
 
 } // namespace aab200

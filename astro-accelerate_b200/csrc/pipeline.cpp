@@ -245,15 +245,8 @@ bool DdtrPipeline::build_quad_tables(int r)
                 }
             rc.quad_npool_qs[k] = std::max(1, most);
         }
-        auto npool_for = [&](int qs_) { return rc.quad_npool_qs[qs_ == 1 ? 0 : qs_ == 2 ? 1 : qs_ == 4 ? 2 : 3]; };
         const int M = (opt_.tile_words == 2 || opt_.kernel_variant == 7) ? 8 : 16;
-        int qs = 8;
-        QuadGeometry G =
-            quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, nquads, M, qs, npool_for(qs));
-        while (G.smem_bytes > kStagedSmemLimit && qs > 1) {
-            qs /= 2;
-            G = quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, nquads, M, qs, npool_for(qs));
-        }
+        const QuadGeometry G = quad_fit(rc, M);
         if (G.smem_bytes <= kStagedSmemLimit && rc.quad_dmax <= 255) {
             rc.quad = G;
             rc.variant = 2;
@@ -262,6 +255,11 @@ bool DdtrPipeline::build_quad_tables(int r)
             rc.quad_pairs = pairs;
             ok = check_cuda(launch_quad_offsets(d_qtmp, nq_ent, G.W, rc.d_qoff, st_, pairs ? 1 : 0), "quad offsets");
             ++launches_;
+            if (ok && opt_.autotune && !opt_.external_buffers && opt_.kernel_variant == 0 && opt_.tile_words == 0) {
+                // the tile-shape autotuner rebuilds the offsets for other row pitches
+                rc.d_qtmp = d_qtmp;
+                d_qtmp = nullptr;
+            }
         }
     }
     if (ok)
@@ -277,6 +275,21 @@ bool DdtrPipeline::build_quad_tables(int r)
             return fail("the channel-quad kernel does not fit range " + std::to_string(r));
     }
     return ok;
+}
+
+// The deepest stage (1, 2, 4 or 8 quads) whose shared memory fits, for a
+// tile of 32 x M words.
+QuadGeometry DdtrPipeline::quad_fit(const RangeConfig &rc, int M) const
+{
+    int qs = 8;
+    QuadGeometry G = quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, rc.nquads, M, qs,
+                                   rc_npool(rc, qs));
+    while (G.smem_bytes > kStagedSmemLimit && qs > 1) {
+        qs /= 2;
+        G = quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, rc.nquads, M, qs,
+                          rc_npool(rc, qs));
+    }
+    return G;
 }
 
 // Subband tables: skew patterns of every (16-channel subband, DM group),
@@ -670,6 +683,8 @@ bool DdtrPipeline::tune_ranges()
         } else {
             rc.f32.cs = job.f.cs;
         }
+        if (rc.variant == 2 && rc.d_qtmp && !tune_quad_shape(static_cast<int>(r), *op, out, pitch, cache, job))
+            return false;
         if (rc.variant == 2 && opt_.kernel_variant == 0 && quad_sp_depth(rc) > 0) {
             // the split-phase kernel (its own stage depth) against the tuned
             // channel-quad kernel
@@ -715,6 +730,71 @@ bool DdtrPipeline::tune_ranges()
         }
     }
     return check_cuda(cudaStreamSynchronize(st_), "sync");
+}
+
+// Tile shape and flavour of a channel-quad range, after its stage depth:
+// 32 x M words of output per CTA row (M = 16: 16 warps of 4 DM trials, one
+// CTA per SM; M = 8: 8 warps of 8 DM trials, two CTAs per SM, or 16 warps of
+// 4 with the byte-path switch) and the sum-loop flavours that can run the
+// range.  Each candidate is timed on the slice at its own tuned stage depth;
+// the fastest is kept and the offset table rebuilt for its row pitch.  job
+// returns as the chosen candidate's job.
+bool DdtrPipeline::tune_quad_shape(int r, const DdtrOp &op, float *out, long long pitch, StageTuneCache &cache,
+                                   DdtrJob &job)
+{
+    RangeConfig &rc = ranges_[r];
+    struct Cand {
+        int M, flavour;
+    };
+    // flavours 5..7 flag per-byte entries as errors: ranges without them only
+    const std::vector<Cand> cands = rc.quad_ws_ok ? std::vector<Cand>{{16, 7}, {16, 6}, {16, 0}, {8, 0}, {8, 2}}
+                                                  : std::vector<Cand>{{16, 0}, {16, 4}, {16, 1}, {8, 0}, {8, 2}};
+    const size_t nq_ent = static_cast<size_t>(rc.nquads) * strategy_.ndms(r);
+    int built_M = rc.quad.M;
+    float best_ms = 1e30f;
+    QuadGeometry best_G = rc.quad;
+    int best_f = quad_flavour_of(rc);
+    std::string err;
+    for (const Cand &c : cands) {
+        QuadGeometry G = quad_fit(rc, c.M);
+        if (G.smem_bytes > kStagedSmemLimit)
+            continue;
+        if (c.M != built_M) {
+            if (!check_cuda(launch_quad_offsets(rc.d_qtmp, nq_ent, G.W, rc.d_qoff, st_, 0), "quad offsets"))
+                return false;
+            ++launches_;
+            built_M = c.M;
+        }
+        rc.quad = G;
+        rc.quad_flavour = c.flavour;
+        DdtrJob t;
+        if (!make_job(op, d_flat_[op.src_level & 1], flat_elems_, out, pitch, t))
+            return false;
+        if (!tune_stage_depth(t, st_, device_, cache, err))
+            return fail(err);
+        const float ms = time_job_slice(t, st_, device_, err);
+        if (ms < 0.f)
+            return fail(err);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best_G = G;
+            best_G.qs = t.q.qs;
+            best_G.npool = t.q.npool;
+            best_f = c.flavour;
+        }
+    }
+    if (best_G.M != built_M) {
+        if (!check_cuda(launch_quad_offsets(rc.d_qtmp, nq_ent, best_G.W, rc.d_qoff, st_, 0), "quad offsets"))
+            return false;
+        ++launches_;
+    }
+    rc.quad = best_G;
+    rc.quad_flavour = best_f;
+    if (!check_cuda(cudaStreamSynchronize(st_), "sync"))
+        return false;
+    cudaFree(rc.d_qtmp);
+    rc.d_qtmp = nullptr;
+    return make_job(op, d_flat_[op.src_level & 1], flat_elems_, out, pitch, job);
 }
 
 bool DdtrPipeline::rewind()
@@ -803,6 +883,27 @@ bool DdtrPipeline::enumerate_ops()
     return true;
 }
 
+// The autotuner's choice where it made one; else, on a range without
+// per-byte entries, one load per DM trial and no per-byte path in the sum
+// loop (flavour 7), and with per-byte entries the kernel that has that path
+// (flavour 0); kernel_variant 6..12 force the measured alternatives.
+int DdtrPipeline::quad_flavour_of(const RangeConfig &rc) const
+{
+    if (rc.quad_pairs)
+        return 3;
+    if (rc.quad_flavour >= 0)
+        return rc.quad_flavour;
+    const int M = rc.quad.M;
+    const bool plain = opt_.kernel_variant == 0 || opt_.kernel_variant == 2 || opt_.kernel_variant == 12;
+    return (opt_.kernel_variant == 10 && M == 16 && rc.quad_ws_ok)   ? 5
+           : (opt_.kernel_variant == 11 && M == 16 && rc.quad_ws_ok) ? 6
+           : (plain && M == 16 && rc.quad_ws_ok)                     ? 7
+           : (opt_.kernel_variant == 9 && M == 16)                   ? 4
+           : (opt_.kernel_variant == 6 && M == 16)                   ? 1
+           : (opt_.kernel_variant == 7 && M == 8)                    ? 2
+                                                                     : 0;
+}
+
 bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, float *out, long long out_pitch,
                             DdtrJob &job)
 {
@@ -879,15 +980,7 @@ bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, f
         // the default on a range without per-byte entries: one load per DM
         // trial and no per-byte path in the sum loop (flavour 7); with
         // per-byte entries the kernel that has that path (flavour 0)
-        const bool plain = opt_.kernel_variant == 0 || opt_.kernel_variant == 2 || opt_.kernel_variant == 12;
-        q.flavour = rc.quad_pairs                                              ? 3
-                    : (opt_.kernel_variant == 10 && q.M == 16 && rc.quad_ws_ok) ? 5
-                    : (opt_.kernel_variant == 11 && q.M == 16 && rc.quad_ws_ok) ? 6
-                    : (plain && q.M == 16 && rc.quad_ws_ok)                     ? 7
-                    : (opt_.kernel_variant == 9 && q.M == 16)                   ? 4
-                    : (opt_.kernel_variant == 6 && q.M == 16)                   ? 1
-                    : (opt_.kernel_variant == 7 && q.M == 8)                    ? 2
-                                                                                : 0;
+        q.flavour = quad_flavour_of(rc);
     } else if (job.variant == 3) {
         job.f = rc.f32;
     } else if (job.variant == 4) {
@@ -1184,11 +1277,12 @@ bool DdtrPipeline::cleanup()
         cudaFree(rc.d_qpat);
         cudaFree(rc.d_qwin);
         cudaFree(rc.d_qoff);
+        cudaFree(rc.d_qtmp);
         cudaFree(rc.d_sblk);
         cudaFree(rc.d_swin);
         cudaFree(rc.d_soff);
         rc.d_table = rc.d_wmin = rc.d_offtab = nullptr;
-        rc.d_qpat = rc.d_qwin = rc.d_qoff = nullptr;
+        rc.d_qpat = rc.d_qwin = rc.d_qoff = rc.d_qtmp = nullptr;
         rc.d_sblk = rc.d_swin = rc.d_soff = nullptr;
     }
     ranges_.clear();

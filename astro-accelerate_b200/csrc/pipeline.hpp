@@ -26,6 +26,8 @@
 
 namespace aab200 {
 
+struct StageTuneCache;
+
 enum class RunStatus : int { error = -1, finished = 0, has_more = 1, finished_component = 2 };
 
 enum StrideMode : int {
@@ -52,7 +54,7 @@ struct PipelineOptions {
     bool device_output = false; // keep the whole output on the device ([range][dm][t])
     bool time_kernels = false;  // CUDA events around every kernel launch
     bool external_buffers = false; // no filterbank/raw/tile buffers: the caller runs the ops (batch engine)
-    bool autotune = true;          // time the staged kernels' stage depth per range at setup
+    bool autotune = true;          // time stage depth, tile shape and kernel per range at setup
     // the reference runner's optional processing (aa_pipeline::component_option)
     bool zero_dm = false;          // zero_dm
     bool zero_dm_outliers = false; // zero_dm_with_outliers (zero_dm takes precedence)
@@ -145,6 +147,9 @@ struct RangeConfig {
     bool has_sub = false, has_quad = false;
     bool quad_ws_ok = false; // no per-byte entries: the warp-specialised quad kernel may run it
     bool quad_pairs = false; // the offset table is in pair mode (the pair body runs the range)
+    int quad_flavour = -1;   // channel-quad kernel flavour the autotuner chose (-1: the default rule)
+    int32_t *d_qtmp = nullptr; // (stage row, offset) of every (quad, DM trial) before the row pitch, kept
+                               // while the autotuner tries tile shapes (their row pitches differ)
     SubGeometry sub{};
     int nsub = 0;
     int32_t *d_sblk = nullptr;
@@ -210,6 +215,8 @@ public:
         return last_plane_.d != nullptr;
     }
     cudaStream_t stream() const { return st_; }
+    // The channel-quad kernel flavour a range runs (make_job's choice).
+    int quad_flavour_of(const RangeConfig &rc) const;
 
 private:
     bool fail(const std::string &msg);
@@ -220,6 +227,8 @@ private:
     bool quad_ws_fits(const RangeConfig &rc) const;
     int quad_sp_depth(const RangeConfig &rc) const;
     bool build_quad_tables(int r);
+    QuadGeometry quad_fit(const RangeConfig &rc, int M) const;
+    bool tune_quad_shape(int r, const DdtrOp &op, float *out, long long pitch, StageTuneCache &cache, DdtrJob &job);
     bool build_sub_tables(int r);
     bool tune_ranges();
     bool step(bool allow_sync);

@@ -716,6 +716,37 @@ cudaError_t psr_whitening(float2 *d_spectra, size_t nSamples, int nDMs, cudaStre
     return e;
 }
 
+// The medians alone over a caller's boundary table (segments of 1 to
+// PSR_MAX_SEGMENT bins, increasing, the last one at most nSamples): the
+// whitening's first kernel on tables its own lengths never produce.  The
+// table is copied synchronously into a scratch allocation.
+cudaError_t psr_segment_medians(const float2 *d_spectra, size_t nSamples, int nDMs, const int *segments,
+                                int nSegments, float *d_medians, cudaStream_t st)
+{
+    if (nDMs < 1 || nSegments < 2 || nSamples > static_cast<size_t>(INT32_MAX) || segments[0] < 0 ||
+        static_cast<size_t>(segments[nSegments - 1]) > nSamples)
+        return cudaErrorInvalidValue;
+    for (int i = 0; i + 1 < nSegments; ++i)
+        if (segments[i + 1] - segments[i] > PSR_MAX_SEGMENT || segments[i + 1] <= segments[i])
+            return cudaErrorInvalidValue;
+    int *d_seg = nullptr;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&d_seg), nSegments * sizeof(int));
+    if (e != cudaSuccess)
+        return e;
+    e = cudaMemcpy(d_seg, segments, nSegments * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        const dim3 grid((nSegments - 1 + PSR_WARPS_PER_BLOCK - 1) / PSR_WARPS_PER_BLOCK, nDMs);
+        k_segment_medians_warp<<<grid, 32 * PSR_WARPS_PER_BLOCK, 0, st>>>(
+            d_medians, d_spectra, d_seg, static_cast<long long>(nSamples), nSegments);
+        ++g_psr_launches;
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+    }
+    cudaFree(d_seg);
+    return e;
+}
+
 // src/aa_device_harmonic_summing.cu:38-169: which algorithm, the PRESTO
 // count of powers of two; the scalloping-corrected plane is a stream-ordered
 // scratch allocation freed on the same stream

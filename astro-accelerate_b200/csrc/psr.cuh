@@ -56,6 +56,8 @@ std::vector<int> psr_segment_sizes(int min_segment_length, int max_segment_lengt
 // the square root of the medians interpolated between segment middles;
 // bin 0 set to (1, 0).  nSamples complex bins per spectrum (>= 8).
 cudaError_t psr_whitening(float2 *d_spectra, size_t nSamples, int nDMs, cudaStream_t st);
+cudaError_t psr_segment_medians(const float2 *d_spectra, size_t nSamples, int nDMs, const int *segments,
+                                int nSegments, float *d_medians, cudaStream_t st);
 
 long long psr_kernel_launches();
 

@@ -85,9 +85,12 @@ def parse():
     ap.add_argument("--tile-words", type=int, default=0)
     ap.add_argument("--group-dms", type=int, default=0)
     ap.add_argument("--variant", type=int, default=0,
-                    help="0 auto, 1 generic kernels, 2 channel-quad, 3 subband, 4 warp-specialised channel-quad, "
-                         "5 split-phase channel-quad, 6 channel-quad with reuse by offset pattern, 7 channel-quad on "
-                         "256-sample tiles (2-7 run the staged fp32 kernel on two-byte data)")
+                    help="0 auto (autotuned per range), 1 generic kernels, 2 channel-quad, 3 subband, "
+                         "4 warp-specialised channel-quad, 5 split-phase channel-quad, 6 channel-quad with the "
+                         "per-byte warp switch, 7 channel-quad on 256-sample tiles, 8 channel-quad pair rows, "
+                         "9 channel-quad loading every DM trial's word first, 10 as 2 without the per-byte path, "
+                         "11 as 9 without the per-byte path, 12 as 11 with 32-bit shared addresses (2-12 run the "
+                         "staged fp32 kernel on two-byte data)")
     ap.add_argument("--with-analysis", action="store_true",
                     help="add an e2e run through the C ABI with the analysis component after every step")
     ap.add_argument("--spd-nt", type=int, default=0, help="samples per DM trial of the spd config (default 2^19)")
@@ -943,6 +946,91 @@ def spd_snr_plane_bytes(aa, w):
     return first, later, pl
 
 
+def _ref_lib():
+    """oracle/_ref/libaaref.so (the reference built from its sources), or None."""
+    import ctypes
+    path = os.path.join(ROOT, "oracle", "_ref", "libaaref.so")
+    return ctypes.CDLL(path) if os.path.exists(path) else None
+
+
+def reference_gpu_spd(plane, w, reps=3):
+    """The reference's analysis_GPU (aaref_time_spd: its buffers allocated as
+    its runner does, CUDA events around the call, the plane restored from a
+    device copy before each run) on the same device plane.  Returns
+    {"ms": [...], "candidates": n} or {"unavailable": why}."""
+    import ctypes
+    import numpy as np
+    L = _ref_lib()
+    if L is None:
+        return {"unavailable": "oracle/_ref/libaaref.so is not built (the reference sources were absent at build)"}
+    L.aaref_time_spd.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                 ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                 ctypes.c_longlong, ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]
+    L.aaref_time_spd.restype = ctypes.c_int
+    ms = np.zeros(reps, np.float32)
+    nc = ctypes.c_longlong()
+    tsamp = float(np.float32(w["tsamp"] * w["inbin"]))
+    rc = L.aaref_time_spd(plane.data_ptr(), w["ndms"], w["nt"], tsamp, w["inbin"], w["max_width_s"],
+                          w["sigma_constant"], int(w["baseline_noise"]), w["sigma_cutoff"], w["algorithm"], 0, reps,
+                          ms.ctypes.data, ctypes.byref(nc))
+    if rc != 0:
+        return {"unavailable": f"reference analysis returned {rc}"}
+    return {"ms": [float(v) for v in ms], "candidates": int(nc.value)}
+
+
+def reference_gpu_whitening(spec, nbins, ndms, reps=3):
+    """The reference's whitening kernels (aaref_time_psr_whitening: its
+    median and SGP2 kernels as spectrum_whitening_SGP2 launches them, CUDA
+    events, the spectra restored from a device copy before each run) on the
+    same device spectra.  Returns {"ms": [...]} or {"unavailable": why}."""
+    import ctypes
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import psr_oracle as PO
+    seg = PO.segment_sizes(nbins)
+    if seg[-1] - seg[-2] < 3:
+        # its median kernel reads past its shared array for segments of 1 or 2 bins
+        return {"unavailable": "last whitening segment shorter than 3 bins"}
+    L = _ref_lib()
+    if L is None:
+        return {"unavailable": "oracle/_ref/libaaref.so is not built (the reference sources were absent at build)"}
+    L.aaref_time_psr_whitening.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_void_p]
+    L.aaref_time_psr_whitening.restype = ctypes.c_int
+    ms = np.zeros(reps, np.float32)
+    rc = L.aaref_time_psr_whitening(spec.data_ptr(), nbins, ndms, reps, ms.ctypes.data)
+    if rc != 0:
+        return {"unavailable": f"reference whitening returned {rc}"}
+    return {"ms": [float(v) for v in ms]}
+
+
+def reference_gpu_line(args, world, metric, unit, units, config, ref, what):
+    """The reference arm's line for a component the reference runs only on
+    the GPU: its own kernels timed on the same device-resident workload."""
+    if "unavailable" in ref:
+        return {"impl": "reference", "metric": metric, "unavailable": ref["unavailable"]}
+    ms = statistics.median(ref["ms"])
+    value = units / (ms / 1e3)
+    return {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": len(ref["ms"]),
+            "warmup": 0, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "config": config, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": unit, "cores": 0, "kind": "reference", "device": "gpu",
+                             "sample": f"{what}, the whole workload, device-resident, CUDA events, median of "
+                                       f"{len(ref['ms'])} runs (the reference has no CPU path for it)"},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+SPD_METRIC = "DM-trial*samples/s analysed (single-pulse detection, reference rules, bit-exact)"
+
+
+def spd_config(w):
+    n = w["ndms"] * w["nt"]
+    return {"workload": f"single-pulse detection: {w['ndms']} DM trials x {w['nt']} samples f32 "
+                        f"({n * 4 / 1e9:.1f} GB), boxcar widths to {int(w['max_width_s'] / w['tsamp'])} samples, "
+                        f"MSD with outlier rejection, peak finding at {w['sigma_cutoff']:g} sigma",
+            "l2": "inputs larger than L2"}
+
+
 def run_spd(args, rank, world, local):
     """Single-pulse detection (the reference's analysis_GPU rules, bit-exact)
     on one DM-time plane of 1536 DM trials x 2^19 samples float32 (3.2 GB,
@@ -954,13 +1042,19 @@ def run_spd(args, rank, world, local):
     candidate lists."""
     import numpy as np
     import torch
-    import aa_b200 as aa
 
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
     w = dict(SPD_WORKLOAD, nt=args.spd_nt) if args.spd_nt else SPD_WORKLOAD
     n = w["ndms"] * w["nt"]
     pristine = synth_plane_device(w, w["seed"] + rank, device)
+    if args.impl == "reference":
+        if rank == 0:
+            ref = reference_gpu_spd(pristine, w, max(3, args.steps))
+            print(json.dumps(reference_gpu_line(args, world, SPD_METRIC, "DM-trial*samples/s", n, spd_config(w), ref,
+                                                "the reference's analysis_GPU")), flush=True)
+        return 0
+    import aa_b200 as aa
     plane = torch.empty_like(pristine)
     spd = aa.single_pulse_detection(n, 0)
     tsamp = float(np.float32(w["tsamp"] * w["inbin"]))
@@ -1021,15 +1115,16 @@ def run_spd(args, rank, world, local):
     # DRAM bytes of one k_spdt_first launch, from an ncu capture of the
     # 1536 x 65536 plane (1.3527e9 B) scaled by the samples a launch covers
     traffic = 1.3527e9 * (n / (1536 * 65536))
-    line = {"metric": "DM-trial*samples/s analysed (single-pulse detection, reference rules, bit-exact)",
+    ref = reference_gpu_spd(pristine, w) if rank == 0 else None
+    line = {"metric": SPD_METRIC,
             "value": n / (step_ms / 1e3), "unit": "DM-trial*samples/s", "n_gpus": 1, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"single-pulse detection: {w['ndms']} DM trials x {w['nt']} samples f32 "
-                                   f"({n * 4 / 1e9:.1f} GB), widths to {pl['max_width_performed']}, {pl['max_iteration']} "
-                                   "iterations, MSD with outlier rejection, peak finding at 6 sigma",
-                       "l2": "inputs larger than L2"},
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": spd_config(w),
+            "boxcar_plan": {"max_width_performed": pl["max_width_performed"], "iterations": pl["max_iteration"]},
             "candidates": ncand, "gpu_launches": int(launches),
+            "reference_gpu": (dict(ref, ms_per_step=statistics.median(ref["ms"]),
+                                   value=n / (statistics.median(ref["ms"]) / 1e3))
+                              if ref and "ms" in ref else ref),
             "families_ms": {k: v[0] for k, v in fam.items()},
             "families_launches": {k: v[1] for k, v in fam.items()},
             "roofline": {"bound": "hbm", "kernel": "k_spdt_first (first boxcar S/N plane)", "achieved": achieved,
@@ -1047,6 +1142,14 @@ def run_spd(args, rank, world, local):
 
 
 WHITENING_WORKLOAD = dict(ndms=512, nbins=(1 << 20) // 2 + 1, seed=41)
+WHITENING_METRIC = "spectrum bins/s whitened (periodicity spectral whitening, reference rules)"
+
+
+def whitening_config(w):
+    bins = w["ndms"] * w["nbins"]
+    return {"workload": f"spectral whitening: {w['ndms']} spectra x {w['nbins']} complex bins f32 "
+                        f"({bins * 8 / 1e9:.1f} GB), segment medians and SGP2 normalisation",
+            "l2": "inputs larger than L2"}
 
 
 def run_whitening(args, rank, world, local):
@@ -1061,17 +1164,25 @@ def run_whitening(args, rank, world, local):
     through aa_b200_psr_whitening."""
     import numpy as np
     import torch
-    import aa_b200 as aa
 
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
     w = WHITENING_WORKLOAD
     nb, nd = w["nbins"], w["ndms"]
+    bins = nd * nb
     g = torch.Generator(device=device)
     g.manual_seed(w["seed"] + rank)
     k = torch.arange(nb, device=device, dtype=torch.float32)
     amp = torch.sqrt(nb * (1.0 + 300.0 / (1.0 + k / 20.0) ** 2) / 2.0)
     pristine = (torch.randn((nd, nb, 2), device=device, generator=g) * amp[None, :, None]).contiguous()
+    if args.impl == "reference":
+        if rank == 0:
+            ref = reference_gpu_whitening(pristine, nb, nd, max(3, args.steps))
+            print(json.dumps(reference_gpu_line(args, world, WHITENING_METRIC, "bins/s", bins, whitening_config(w),
+                                                ref, "the reference's segmented-median and SGP2 kernels")),
+                  flush=True)
+        return 0
+    import aa_b200 as aa
     spec = torch.empty_like(pristine)
     L = aa.lib()
     stream = torch.cuda.current_stream(device).cuda_stream
@@ -1118,7 +1229,6 @@ def run_whitening(args, rank, world, local):
     except OSError:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
-    bins = nd * nb
     achieved = 24.0 * bins / (step_ms / 1e3) / 1e9
     cpu = None
     if rank == 0:
@@ -1131,17 +1241,21 @@ def run_whitening(args, rank, world, local):
         dt = time.perf_counter() - t0
         cpu = {"value": z.size / dt, "unit": "bins/s", "cores": 1, "kind": "port",
                "sample": f"oracle on 1 spectrum of {z.size} bins, {dt:.1f} s"}
-    line = {"metric": "spectrum bins/s whitened (periodicity spectral whitening, reference rules)",
+    ref = reference_gpu_whitening(pristine, nb, nd) if rank == 0 else None
+    line = {"metric": WHITENING_METRIC,
             "value": bins / (step_ms / 1e3), "unit": "bins/s", "n_gpus": 1, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"spectral whitening: {nd} spectra x {nb} complex bins f32 "
-                                   f"({bins * 8 / 1e9:.1f} GB), segment medians and SGP2 normalisation",
-                       "l2": "inputs larger than L2"},
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": whitening_config(w),
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k_segment_medians + k_whitening_sgp2", "achieved": achieved,
-                         "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-                         "algorithmic_bytes": 24 * bins},
+            "reference_gpu": (dict(ref, ms_per_step=statistics.median(ref["ms"]),
+                                   value=bins / (statistics.median(ref["ms"]) / 1e3))
+                              if ref and "ms" in ref else ref),
+            "roofline": {"bound": "latency", "kernel": "k_segment_medians_warp + k_sgp2_spans",
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                         "algorithmic_bytes": 24 * bins,
+                         "note": "frac is of the measured HBM copy rate, which does not bind: one warp sorts one "
+                                 "segment of at most 79 bins in a 128-slot shuffle network (28 compare-exchange "
+                                 "stages per segment), and one warp scales one interpolation span"},
             "e2e": {"value": bins / (e2e / 1e3), "unit": "bins/s", "h2d_bytes_per_step": bins * 8,
                     "d2h_bytes_per_step": bins * 8},
             "cpu_baseline": cpu, "clocks": clk.summary()}
@@ -1154,13 +1268,14 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference" and args.config not in ("survey", "mid", "small"):
-        # only the plain DDTR configurations have a reference arm; print no
-        # line that would stand for one
+    if args.impl == "reference" and args.config not in ("survey", "mid", "small", "spd", "whitening"):
+        # the plain DDTR configurations and the two GPU-only components have
+        # a reference arm; print no line that would stand for one
         if rank == 0:
             print(json.dumps({"impl": "reference", "config": args.config,
                               "unavailable": f"no reference arm for --config {args.config}: the reference arm times "
-                                             "the plain DDTR path (survey, mid, small)"}), flush=True)
+                                             "the plain DDTR path (survey, mid, small), single-pulse detection "
+                                             "(spd) and spectral whitening"}), flush=True)
         return 0
     if args.config == "batched" and args.impl != "reference":
         return run_batched(args, rank, world, local)
@@ -1168,9 +1283,9 @@ def main():
         return run_refine(args, rank, world, local)
     if args.config == "e2e" and args.impl != "reference":
         return run_e2e(args, rank, world, local)
-    if args.config == "spd" and args.impl != "reference":
+    if args.config == "spd":
         return run_spd(args, rank, world, local)
-    if args.config == "whitening" and args.impl != "reference":
+    if args.config == "whitening":
         return run_whitening(args, rank, world, local)
     cfg = {"survey": SURVEY, "mid": MID, "small": SMALL, "batched": SURVEY, "refine": SURVEY,
            "e2e": SURVEY, "spd": SURVEY, "whitening": SURVEY}[args.config]

@@ -454,6 +454,15 @@ int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms,
  * shared-memory stage of a range, as the autotuner chose it; 0 for the
  * generic kernels */
 int aa_b200_pipeline_stage_depth(void *obj, int range);
+/* The kernel shape a range runs (after set-up, which includes the
+ * autotuner): the channel-quad flavour (-1 for other kernels; 0 with the
+ * per-byte path, 1 with its warp switch, 4 loading every DM trial's word
+ * before the sums, 6 the same without a per-byte path, 7 as 6 with 32-bit
+ * shared addresses, 2 the 16-warp form of the 256-sample tile), the DM trials
+ * and samples of one CTA's output tile and the DM trials one warp sums.
+ * Returns 0, or 1 for an unknown range. */
+int aa_b200_pipeline_range_kernel(void *obj, int range, int *flavour, int *tile_dms, int *tile_samples,
+                                  int *dms_per_warp);
 long long aa_b200_pipeline_kernel_launches(void *obj);
 const char *aa_b200_pipeline_last_error(void *obj);
 int aa_b200_pipeline_num_tchunks(void *obj);
@@ -699,6 +708,15 @@ int aa_b200_psr_whitening(void *d_spectra, size_t nSamples, int nDMs, void *stre
  * (create_dered_segment_sizes_prefix_sum, src/aa_device_spectral_whitening.cu:17-31,
  * lengths 6 .. 250): writes up to cap of them, returns their count. */
 int aa_b200_psr_segment_sizes(size_t nSamples, int *out, int cap);
+/* The whitening's segment medians alone (GPU_kernel_segmented_median,
+ * src/aa_device_spectral_whitening_kernel.cu:338-376) over a caller's
+ * boundary table segments[0..nSegments-1] (host memory; increasing, each
+ * segment 1 to 256 bins, the last boundary at most nSamples): writes
+ * d_medians[dm * nSegments + s] for s < nSegments - 1.  Synchronises the
+ * stream; for checking median selection on segment lengths the whitening's
+ * own table does not produce. */
+int aa_b200_psr_segment_medians(const void *d_spectra, size_t nSamples, int nDMs, const int *segments,
+                                int nSegments, float *d_medians, void *stream);
 long long aa_b200_psr_kernel_launches(void);
 const char *aa_b200_psr_last_error(void);
 

@@ -55,12 +55,16 @@
 #include "aa_device_peak_find.hpp"
 #include "aa_device_threshold.hpp"
 #include "aa_device_spectrum_whitening.hpp"
+#include "aa_device_spectrum_whitening_kernel.hpp"
 
 namespace astroaccelerate {
 /* defined in src/aa_device_analysis.cu without a header declaration */
 void Create_list_of_boxcar_widths(std::vector<int> *boxcar_widths, std::vector<int> *BC_widths, int max_boxcar_width);
 void Create_PD_plan(std::vector<PulseDetection_plan> *PD_plan, std::vector<int> *BC_widths, int nDMs, int nTimesamples);
 int Get_max_iteration(int max_boxcar_width, std::vector<int> *BC_widths, int *max_width_performed);
+/* defined in src/aa_device_spectral_whitening.cu:40-45 without a header declaration */
+void calculate_median_for_segments(float *d_MSD_segments, float2 *d_input, size_t nSamples, int nDMs,
+                                   int *d_segment_sizes, int nSegments, cudaStream_t &stream);
 } // namespace astroaccelerate
 
 using namespace astroaccelerate;
@@ -573,6 +577,58 @@ int aaref_psr_whitening(const float *spectra, long long nSamples, int nDMs, floa
         rc = -5;
     cudaMemcpy(out, d, n * sizeof(float), cudaMemcpyDeviceToHost);
     cudaFree(d);
+    return rc;
+}
+
+/* The reference's whitening kernels as spectrum_whitening_SGP2 launches them
+ * (calculate_median_for_segments, then call_kernel_spectrum_whitening_SGP2 on
+ * nSegments x nDMs blocks of 256 threads, src/aa_device_spectral_whitening.cu:60-118),
+ * timed with CUDA events on a device copy of d_src (a device pointer: nDMs
+ * spectra of nSamples complex bins), reps times; ms[reps] receives the
+ * times.  The boundary table and the median buffer are allocated once,
+ * outside the timed region (the reference allocates, copies and frees them
+ * on every call), each one element longer than the reference's: the last
+ * block of its normalisation kernel reads one boundary and one median past
+ * its tables, and with a zero boundary there that block writes nothing.
+ * Returns 0 or < 0. */
+int aaref_time_psr_whitening(const float *d_src, long long nSamples, int nDMs, int reps, float *ms)
+{
+    const size_t n = 2 * (size_t)nDMs * (size_t)nSamples;
+    std::vector<int> seg;
+    create_dered_segment_sizes_prefix_sum(&seg, 6, 250, (size_t)nSamples);
+    const int nSegments = (int)seg.size();
+    seg.push_back(0);
+    float *d = NULL, *d_med = NULL;
+    int *d_seg = NULL;
+    if (cudaMalloc((void **)&d, n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&d_seg, seg.size() * sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void **)&d_med, ((size_t)nSegments * nDMs + 1) * sizeof(float)) != cudaSuccess)
+        return -3;
+    cudaMemcpy(d_seg, seg.data(), seg.size() * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemset(d_med, 0, ((size_t)nSegments * nDMs + 1) * sizeof(float));
+    cudaStream_t stream = NULL;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int rc = 0;
+    for (int r = 0; r < reps; r++) {
+        cudaMemcpy(d, d_src, n * sizeof(float), cudaMemcpyDeviceToDevice);
+        cudaDeviceSynchronize();
+        cudaEventRecord(e0, stream);
+        calculate_median_for_segments(d_med, (float2 *)d, (size_t)nSamples, nDMs, d_seg, nSegments, stream);
+        call_kernel_spectrum_whitening_SGP2(dim3(256, 1, 1), dim3(nSegments, nDMs, 1), 0, stream, d_med, (float2 *)d,
+                                            d_seg, (size_t)nSamples, nSegments);
+        cudaEventRecord(e1, stream);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms[r], e0, e1);
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess)
+        rc = -5;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d);
+    cudaFree(d_seg);
+    cudaFree(d_med);
     return rc;
 }
 

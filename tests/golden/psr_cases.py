@@ -128,6 +128,18 @@ WHITENING_CASES = {
     "white_1000x5": dict(n=1000, ndms=5, seed=24),
 }
 
+# Whitening cases whose last segment is 1 bin (n = a boundary + 1) and 2 bins
+# (a boundary + 2): median and interpolation branches the cases above never
+# take.  No reference golden run covers them; the oracle pins them.
+WHITENING_EDGE_CASES = {
+    "white_3968x3_last1": dict(n=3968, ndms=3, seed=25),
+    "white_8954x2_last2": dict(n=8954, ndms=2, seed=26),
+}
+
+# Segment lengths for the medians alone, around every register-width switch
+# of the median kernel (32, 64, 128 bins) and at both ends (1 and 256 bins).
+MEDIAN_SEGMENT_LENGTHS = [1, 2, 3, 4, 5, 31, 32, 33, 63, 64, 65, 127, 128, 129, 130, 200, 255, 256, 6, 250, 17, 1, 2]
+
 
 def make_red_spectra(c) -> np.ndarray:
     """[ndms][n] complex64: complex Gaussian bins whose power falls as a red

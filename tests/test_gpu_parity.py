@@ -157,6 +157,25 @@ def test_kernel_choice(aa, oracle_mod, cuda_device, name, variant, kernel):
     assert_matches_oracle(case, s, got, want, kern)
 
 
+@pytest.mark.parametrize("name", [n for n in LIGHT if C.CASES[n]["nbits"] <= 8])
+def test_autotuned_tile_shape_matches_oracle(aa, oracle_mod, cuda_device, name):
+    """With the autotuner on, every channel-quad range runs the tile shape and
+    flavour it timed fastest (a 64 x 512 or 64 x 256 output tile; flavours
+    6 and 7 only where no entry is on the per-byte path); results agree."""
+    case = C.CASES[name]
+    x = C.make_input(case)
+    s, want, kern = oracle_run(oracle_mod, case, x)
+    got, info, _, _ = run_pipeline(aa, case, x, variant=0)
+    for i in info:
+        if i["kernel"] == "quad":
+            assert i["tile"] in ([64, 512], [64, 256]), i
+            assert i["flavour"] in (0, 1, 2, 4, 6, 7), i
+            assert i["dms_per_warp"] == (8 if i["tile"][1] == 256 and i["flavour"] == 0 else 4), i
+        else:
+            assert i["flavour"] == -1, i
+    assert_matches_oracle(case, s, got, want, kern)
+
+
 WS_CASES = [n for n in LIGHT if C.CASES[n]["nbits"] <= 8]
 WS_REFUSED = "warp-specialised channel-quad kernel cannot run"
 

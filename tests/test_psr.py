@@ -266,6 +266,67 @@ def test_whitening_matches_reference_gpu(aa, golden, name):
     assert np.all(ours[:, 0] == 1)
 
 
+@pytest.mark.parametrize("name", list(P.WHITENING_EDGE_CASES))
+def test_edge_whitening_cases_end_in_short_segments(name):
+    n = P.WHITENING_EDGE_CASES[name]["n"]
+    seg = O.segment_sizes(n)
+    assert seg[-1] - seg[-2] == int(name[-1])
+    o = O.whitening(P.make_red_spectra(P.WHITENING_EDGE_CASES[name]))
+    assert np.all(np.isfinite(o)) and np.all(o[:, 0] == 1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(P.WHITENING_EDGE_CASES))
+def test_whitening_short_last_segment_matches_oracle(aa, name):
+    """Every bin against the restatement (exact float sqrt and division
+    against the fast-math forms: 2e-6 relative) where the last segment is
+    1 or 2 bins."""
+    import torch
+    c = P.WHITENING_EDGE_CASES[name]
+    z = P.make_red_spectra(c)
+    d = torch.from_numpy(z.view(np.float32).copy()).cuda()
+    assert aa.lib().aa_b200_psr_whitening(d.data_ptr(), c["n"], c["ndms"], None) == 0
+    torch.cuda.synchronize()
+    ours = d.cpu().numpy().view(np.complex64).reshape(c["ndms"], c["n"])
+    o = O.whitening(z)
+    assert np.all(ours[:, 0] == 1)
+    assert np.allclose(ours.view(np.float32), o.view(np.float32), rtol=2e-6, atol=0)
+
+
+@pytest.mark.gpu
+def test_segment_medians_on_every_segment_length(aa):
+    """The median kernel on a table of 1- to 256-bin segments against the
+    restatement of the reference's zero-padded 256-slot selection (the
+    powers here use one rounding, x^2 + y^2 fused, so 3e-7 relative)."""
+    import torch
+    seg = np.concatenate([[0], np.cumsum(P.MEDIAN_SEGMENT_LENGTHS)]).astype(np.int32)
+    n = int(seg[-1]) + 5
+    c = dict(n=n, ndms=2, seed=27)
+    z = P.make_red_spectra(c)
+    d = torch.from_numpy(z.view(np.float32).copy()).cuda()
+    med = torch.full((c["ndms"] * len(seg),), -1.0, device="cuda")
+    assert aa.lib().aa_b200_psr_segment_medians(d.data_ptr(), n, c["ndms"], seg.ctypes.data, len(seg),
+                                                med.data_ptr(), None) == 0, aa.lib().aa_b200_psr_last_error()
+    got = med.cpu().numpy().reshape(c["ndms"], len(seg))
+    for dm in range(c["ndms"]):
+        p = (z[dm].real.astype(np.float64) ** 2 + z[dm].imag.astype(np.float64) ** 2).astype(np.float32)
+        want = O.segment_medians(p, [int(v) for v in seg])
+        assert np.allclose(got[dm, :-1], want, rtol=3e-7, atol=0), dm
+        assert got[dm, -1] == -1.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("table", [[0, 257], [0, 5, 5], [0, 10, 9000]])
+def test_segment_medians_refuse_bad_tables(aa, table):
+    import torch
+    d = torch.zeros(2 * 4096, device="cuda")
+    med = torch.zeros(8, device="cuda")
+    seg = np.array(table, np.int32)
+    assert aa.lib().aa_b200_psr_segment_medians(d.data_ptr(), 4096, 1, seg.ctypes.data, len(seg), med.data_ptr(),
+                                                None) == 1
+    assert b"segment medians" in aa.lib().aa_b200_psr_last_error()
+
+
 @pytest.mark.gpu
 def test_whitening_refuses_short_spectra(aa):
     import torch
