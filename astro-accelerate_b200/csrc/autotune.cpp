@@ -107,13 +107,18 @@ bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache 
     return true;
 }
 
-float time_job_slice(const DdtrJob &job, cudaStream_t st, int device, std::string &err)
+float time_job_slice(const DdtrJob &job, cudaStream_t st, int device, std::string &err, long long samples,
+                     long long *timed_samples)
 {
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     const long long want_tiles = std::max<long long>(1, (2LL * nsm + job.groups - 1) / std::max(1, job.groups));
     DdtrJob t = job;
-    t.p.tp = static_cast<int>(std::min<long long>(job.p.tp, want_tiles * job.tile_samples));
+    const long long tile = std::max(1, job.tile_samples);
+    const long long want = (samples > 0) ? (samples + tile - 1) / tile * tile : want_tiles * tile;
+    t.p.tp = static_cast<int>(std::min<long long>(job.p.tp, want));
+    if (timed_samples)
+        *timed_samples = t.p.tp;
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         err = "autotune: cudaEventCreate failed";

@@ -34,8 +34,11 @@ struct StageTuneCache {
 
 bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache &cache, std::string &err);
 
-// Device time (ms, best of two after a warm-up launch) of a slice of the job
-// of about two CTAs per SM; negative on a launch error (message in err).
-float time_job_slice(const DdtrJob &job, cudaStream_t st, int device, std::string &err);
+// Device time (ms, best of two after a warm-up launch) of a slice of the job:
+// about two CTAs per SM, or (samples > 0) that many output samples per DM
+// trial rounded up to the job's tile, at most the job's; timed_samples
+// receives the slice's samples.  Negative on a launch error (message in err).
+float time_job_slice(const DdtrJob &job, cudaStream_t st, int device, std::string &err, long long samples = 0,
+                     long long *timed_samples = nullptr);
 
 } // namespace aab200

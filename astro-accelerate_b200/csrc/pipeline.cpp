@@ -750,8 +750,13 @@ bool DdtrPipeline::tune_quad_shape(int r, const DdtrOp &op, float *out, long lon
     const std::vector<Cand> cands = rc.quad_ws_ok ? std::vector<Cand>{{16, 7}, {16, 6}, {16, 0}, {8, 0}, {8, 2}}
                                                   : std::vector<Cand>{{16, 0}, {16, 4}, {16, 1}, {8, 0}, {8, 2}};
     const size_t nq_ent = static_cast<size_t>(rc.nquads) * strategy_.ndms(r);
+    // the same output samples for every shape: four 512-sample tiles per SM
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
+    const int groups = std::max(1, strategy_.ndms(r) / rc.group_dms);
+    const long long samples = 512LL * std::max(1, (4 * nsm + groups - 1) / groups);
     int built_M = rc.quad.M;
-    float best_ms = 1e30f;
+    float best_ms = 1e30f; // per output sample of the slice
     QuadGeometry best_G = rc.quad;
     int best_f = quad_flavour_of(rc);
     std::string err;
@@ -772,9 +777,11 @@ bool DdtrPipeline::tune_quad_shape(int r, const DdtrOp &op, float *out, long lon
             return false;
         if (!tune_stage_depth(t, st_, device_, cache, err))
             return fail(err);
-        const float ms = time_job_slice(t, st_, device_, err);
-        if (ms < 0.f)
+        long long timed = 0;
+        const float t_ms = time_job_slice(t, st_, device_, err, samples, &timed);
+        if (t_ms < 0.f)
             return fail(err);
+        const float ms = t_ms / static_cast<float>(std::max(1LL, timed));
         if (ms < best_ms) {
             best_ms = ms;
             best_G = G;

@@ -514,18 +514,35 @@ __global__ void k_msd_interpolate(const float *__restrict__ dit, float *__restri
 //     better, the pair of pairs likewise), at q = 0 the second pair on a
 //     tie; over q a later group only when strictly better.
 //
-// Design: one warp per window of 128 consecutive positions v of one DM
-// trial, four consecutive positions per lane.  The sum for start u and group
-// q is built by the lane holding v = u + 4q: it starts from P_k(v) and adds
-// S4(v - 4), S4(v - 8), ... one group per step, the S4 of the lane q places
-// below arriving by a shuffle; the group's best S/N then moves down q lanes
-// by a shuffle to the lane that owns u, which folds it into its running
-// best.  No shared memory and no block barrier; a window yields 128 - 4(Q-1)
-// starts (Q = nBoxcars / 4), its last Q-1 lanes only feed the others.
+// Design: one warp per window of 32 x PPL consecutive positions v of one DM
+// trial, PPL consecutive positions per lane (PPL = 4 or 8).  The sum for
+// start u and group q is built where v = u + 4q sits: it starts from P_k(v)
+// and adds S4(v - 4), S4(v - 8), ... one group per step, each S4 taken from
+// a register of the same lane or, 4q positions back, by a shuffle from a
+// lane below; the group's best S/N then moves to the position u the same
+// way, which folds it into its running best.  No shared memory and no block
+// barrier; a window yields 32 PPL - 4(Q-1) starts (Q = nBoxcars / 4), its
+// last 4(Q-1) positions only feed the others, so wider windows waste less.
 // ---------------------------------------------------------------------------
 constexpr int SNR_WARPS = 8;
+#ifndef SPD_BOXCAR_PPL
+#define SPD_BOXCAR_PPL 8
+#endif
 
-template <int NB, bool NTH>
+// Lane offset and register of the position 'a' positions from a lane's
+// register p (a may be negative): floor division by PPL.
+template <int PPL>
+__host__ __device__ constexpr int pos_lane(int a)
+{
+    return (a >= 0) ? a / PPL : -((-a + PPL - 1) / PPL);
+}
+template <int PPL>
+__host__ __device__ constexpr int pos_reg(int a)
+{
+    return a - PPL * pos_lane<PPL>(a);
+}
+
+template <int NB, bool NTH, int PPL>
 __global__ void __launch_bounds__(32 * SNR_WARPS) k_boxcar_snr(const float *__restrict__ in,
                                                                const float *__restrict__ bv_in, float *bv_out,
                                                                float *dec, float *snr_out, uint16_t *taps_out,
@@ -533,7 +550,8 @@ __global__ void __launch_bounds__(32 * SNR_WARPS) k_boxcar_snr(const float *__re
                                                                int dit_value, int dtm)
 {
     constexpr int Q = NB / 4;
-    constexpr int OUT = 128 - 4 * (Q - 1); // starts per window
+    constexpr int OUT = 32 * PPL - 4 * (Q - 1); // starts per window
+    static_assert(OUT > 0 && OUT % 2 == 0, "window too short for the widths");
     const int lane = threadIdx.x & 31;
     const long long window = static_cast<long long>(blockIdx.x) * SNR_WARPS + (threadIdx.x >> 5);
     const long long wbase = window * OUT;
@@ -541,23 +559,23 @@ __global__ void __launch_bounds__(32 * SNR_WARPS) k_boxcar_snr(const float *__re
         return;
     const long long row = static_cast<long long>(blockIdx.y) * nT;
     const float *x = in + row;
-    const long long v0 = wbase + 4 * lane; // this lane's first position
+    const long long v0 = wbase + PPL * lane; // this lane's first position (even)
 
-    // samples v0 .. v0+6 (the last three from the next lane)
-    float xs[7];
+    // samples v0 .. v0+PPL+2 (the last three from the next lane)
+    float xs[PPL + 3];
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < PPL; ++j)
         xs[j] = (v0 + j < nT) ? __ldg(x + v0 + j) : 0.f;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
         const float nx = __shfl_down_sync(0xffffffffu, xs[j], 1);
-        xs[4 + j] = (lane == 31) ? ((v0 + 4 + j < nT) ? __ldg(x + v0 + 4 + j) : 0.f) : nx;
+        xs[PPL + j] = (lane == 31) ? ((v0 + PPL + j < nT) ? __ldg(x + v0 + PPL + j) : 0.f) : nx;
     }
-    // partial sums P_k(v) of the four positions; zeros for pairs without
-    // four samples after their even sample
-    float acc[4][4], s4[4], bv[4], pair[4];
+    // partial sums P_k(v) of the positions; zeros for pairs without four
+    // samples after their even sample
+    float acc[PPL][4], s4[PPL], bv[PPL], pair[PPL];
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
+    for (int p = 0; p < PPL; ++p) {
         const long long v = v0 + p;
         const bool ok = ((v & ~1LL) + 4) < nT;
         const float a1 = xs[p] + xs[p + 1];
@@ -577,28 +595,31 @@ __global__ void __launch_bounds__(32 * SNR_WARPS) k_boxcar_snr(const float *__re
         const float2 st = msd.v[w];
         return NTH ? __fdividef(bvu + (b - st.x), st.y) : __fdividef(b - st.x, st.y);
     };
-    float best[4];
-    int taps[4];
-    float full[4]; // B(u, NB) of this lane's starts (bv_out at even starts)
+    float best[PPL];
+    int taps[PPL];
+    float full[PPL]; // B(u, NB) of this lane's starts (bv_out at even starts)
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-        float bvq[4];
+        float fq[PPL];
+        int tq[PPL];
 #pragma unroll
-        for (int p = 0; p < 4; ++p) {
+        for (int p = 0; p < PPL; ++p) {
+            // the start u = v - 4q: its S4 joins the sum, its running value
+            // enters the S/N
+            const int dl = pos_lane<PPL>(p - 4 * q), pr = pos_reg<PPL>(p - 4 * q);
+            float bvq = 0.f;
             if (q > 0) {
-                const float sv = __shfl_up_sync(0xffffffffu, s4[p], q);
+                const float sv = (dl == 0) ? s4[pr] : __shfl_up_sync(0xffffffffu, s4[pr], -dl);
                 acc[p][0] = acc[p][0] + sv;
                 acc[p][1] = acc[p][1] + sv;
                 acc[p][2] = acc[p][2] + sv;
                 acc[p][3] = acc[p][3] + sv;
             }
-            bvq[p] = NTH ? ((q > 0) ? __shfl_up_sync(0xffffffffu, bv[p], q) : bv[p]) : 0.f;
-        }
-#pragma unroll
-        for (int p = 0; p < 4; ++p) {
+            if (NTH)
+                bvq = (dl == 0) ? bv[pr] : __shfl_up_sync(0xffffffffu, bv[pr], -dl);
             const int d = 4 * q;
-            float f1 = snr(acc[p][0], bvq[p], d);
-            float f2 = snr(acc[p][1], bvq[p], d + 1);
+            float f1 = snr(acc[p][0], bvq, d);
+            float f2 = snr(acc[p][1], bvq, d + 1);
             int t1, t2;
             if (f2 > f1) {
                 f1 = f2;
@@ -606,48 +627,56 @@ __global__ void __launch_bounds__(32 * SNR_WARPS) k_boxcar_snr(const float *__re
             } else {
                 t1 = d + 1;
             }
-            f2 = snr(acc[p][2], bvq[p], d + 2);
-            const float f3 = snr(acc[p][3], bvq[p], d + 3);
+            f2 = snr(acc[p][2], bvq, d + 2);
+            const float f3 = snr(acc[p][3], bvq, d + 3);
             if (f3 > f2) {
                 f2 = f3;
                 t2 = d + 4;
             } else {
                 t2 = d + 3;
             }
-            float c;
-            int ct;
             if (q == 0) {
                 if (f1 > f2) {
-                    c = f1;
-                    ct = t1;
+                    best[p] = f1;
+                    taps[p] = t1;
                 } else {
-                    c = f2;
-                    ct = t2;
+                    best[p] = f2;
+                    taps[p] = t2;
                 }
-                best[p] = c;
-                taps[p] = ct;
             } else {
                 if (f2 > f1) {
                     f1 = f2;
                     t1 = t2;
                 }
-                c = __shfl_down_sync(0xffffffffu, f1, q);
-                ct = __shfl_down_sync(0xffffffffu, t1, q);
+                fq[p] = f1;
+                tq[p] = t1;
+            }
+        }
+        if (q > 0) {
+            // position u takes the group computed 4q positions ahead
+#pragma unroll
+            for (int p = 0; p < PPL; ++p) {
+                const int dl = pos_lane<PPL>(p + 4 * q), pr = pos_reg<PPL>(p + 4 * q);
+                const float c = (dl == 0) ? fq[pr] : __shfl_down_sync(0xffffffffu, fq[pr], dl);
+                const int ct = (dl == 0) ? tq[pr] : __shfl_down_sync(0xffffffffu, tq[pr], dl);
                 if (c > best[p]) {
                     best[p] = c;
                     taps[p] = ct;
                 }
             }
-            if (q == Q - 1)
-                full[p] = (Q > 1) ? __shfl_down_sync(0xffffffffu, acc[p][3], Q - 1) : acc[p][3];
+        }
+        if (q == Q - 1) {
+#pragma unroll
+            for (int p = 0; p < PPL; ++p) {
+                const int dl = pos_lane<PPL>(p + 4 * (Q - 1)), pr = pos_reg<PPL>(p + 4 * (Q - 1));
+                full[p] = (dl == 0) ? acc[pr][3] : __shfl_down_sync(0xffffffffu, acc[pr][3], dl);
+            }
         }
     }
-    if (lane >= 32 - (Q - 1))
-        return;
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
+    for (int p = 0; p < PPL; ++p) {
         const long long u = v0 + p;
-        if (u >= nT)
+        if (PPL * lane + p >= OUT || u >= nT)
             break;
         snr_out[row + u] = best[p];
         taps_out[row + u] = static_cast<uint16_t>(NTH ? startTaps + taps[p] * dit_value : taps[p]);
@@ -1042,21 +1071,23 @@ static cudaError_t launch_boxcar_snr(const float *in, const float *bv_in, float 
 {
     if (nBlocks <= 0 || nT <= 0)
         return cudaSuccess;
-    const int out = 128 - 4 * (nBoxcars / 4 - 1);
+    // positions per lane: 8 where the widths span several lanes' positions
+    const int ppl = (nBoxcars >= 16) ? SPD_BOXCAR_PPL : 4;
+    const int out = 32 * ppl - 4 * (nBoxcars / 4 - 1);
     const long long windows = (static_cast<long long>(nT) + out - 1) / out;
     const dim3 grid(static_cast<unsigned>((windows + SNR_WARPS - 1) / SNR_WARPS), nDMs);
     switch (nBoxcars) {
     case 32:
-        k_boxcar_snr<32, NTH><<<grid, 32 * SNR_WARPS, 0, st>>>(in, bv_in, bv_out, dec, snr, taps, msd, nT, startTaps,
-                                                              dit_value, dtm);
+        k_boxcar_snr<32, NTH, SPD_BOXCAR_PPL><<<grid, 32 * SNR_WARPS, 0, st>>>(in, bv_in, bv_out, dec, snr, taps, msd,
+                                                                              nT, startTaps, dit_value, dtm);
         break;
     case 16:
-        k_boxcar_snr<16, NTH><<<grid, 32 * SNR_WARPS, 0, st>>>(in, bv_in, bv_out, dec, snr, taps, msd, nT, startTaps,
-                                                              dit_value, dtm);
+        k_boxcar_snr<16, NTH, SPD_BOXCAR_PPL><<<grid, 32 * SNR_WARPS, 0, st>>>(in, bv_in, bv_out, dec, snr, taps, msd,
+                                                                              nT, startTaps, dit_value, dtm);
         break;
     case 8:
-        k_boxcar_snr<8, NTH><<<grid, 32 * SNR_WARPS, 0, st>>>(in, bv_in, bv_out, dec, snr, taps, msd, nT, startTaps,
-                                                             dit_value, dtm);
+        k_boxcar_snr<8, NTH, 4><<<grid, 32 * SNR_WARPS, 0, st>>>(in, bv_in, bv_out, dec, snr, taps, msd, nT,
+                                                                startTaps, dit_value, dtm);
         break;
     default:
         return cudaErrorInvalidValue;

@@ -163,8 +163,14 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # the first sample before the timed region starts (nvidia-smi
+            # takes a moment to come up), so short regions are not unsampled
+            t0 = time.perf_counter()
+            while not self.rows and self.proc.poll() is None and time.perf_counter() - t0 < 5.0:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
+        self.n_enter = len(self.rows)
         return self
 
     def _read(self):
@@ -175,6 +181,10 @@ class ClockSampler:
 
     def __exit__(self, *a):
         if self.proc:
+            # one sample at or after the end of a region shorter than the period
+            t0 = time.perf_counter()
+            while len(self.rows) <= self.n_enter and self.proc.poll() is None and time.perf_counter() - t0 < 1.0:
+                time.sleep(0.01)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
