@@ -526,7 +526,7 @@ __global__ void k_msd_interpolate(const float *__restrict__ dit, float *__restri
 // ---------------------------------------------------------------------------
 constexpr int SNR_WARPS = 8;
 #ifndef SPD_BOXCAR_PPL
-#define SPD_BOXCAR_PPL 8
+#define SPD_BOXCAR_PPL 4
 #endif
 
 // Lane offset and register of the position 'a' positions from a lane's
@@ -543,7 +543,7 @@ __host__ __device__ constexpr int pos_reg(int a)
 }
 
 template <int NB, bool NTH, int PPL>
-__global__ void __launch_bounds__(32 * SNR_WARPS) k_boxcar_snr(const float *__restrict__ in,
+__global__ void __launch_bounds__(32 * SNR_WARPS, PPL == 4 ? 4 : 1) k_boxcar_snr(const float *__restrict__ in,
                                                                const float *__restrict__ bv_in, float *bv_out,
                                                                float *dec, float *snr_out, uint16_t *taps_out,
                                                                const SnrMsd msd, int nT, int startTaps,

@@ -1,6 +1,7 @@
-"""The joined search on a reduced multi-beam draw: three beams of 4096
-channels x 2^18 8-bit samples with 4-32 injected pulses each (DM 50-2900),
-the 8-range survey plan to DM 3075.
+"""The joined search on a reduced multi-beam draw: two beams of 4096
+channels x 2^20 8-bit samples with 4-32 injected pulses each (DM 50-2900),
+the 8-range survey plan to DM 3075 (the draw of the end-to-end benchmark,
+16 beams there).
 
   batched DDTR (one persistent launch for every beam's jobs, captured in a
   CUDA graph) -> candidates at 6 sigma of every DM range -> the 64 strongest
@@ -47,7 +48,7 @@ def test_batched_search_and_refinement(aa, cuda_device):
     from aa_b200 import search as SR
     from aa_b200 import workloads as WL
 
-    beams = WL.e2e_beams(seed=11, nbeams=3, nsamp=1 << 18)
+    beams = WL.e2e_beams(seed=11, nbeams=2, nsamp=1 << 20)
     b0 = beams[0]
     kc = R.delay_per_dm(b0["nchans"], b0["fch1"], b0["foff"], b0["tsamp"])
     xs = [WL.synth_e2e_beam(b, torch.device("cuda", 0)) for b in beams]
@@ -112,6 +113,8 @@ def test_batched_search_and_refinement(aa, cuda_device):
         after += af
         injected += len(b["pulses"])
         found += len(fd)
-    assert found >= 0.7 * injected, (found, injected)
+    # events closer than the selection's 4096-sample separation to a
+    # stronger one are merged into it
+    assert found >= 0.75 * injected, (found, injected)
     assert np.median(after) < np.median(before), (np.median(before), np.median(after))
     assert np.median(after) < 0.3, np.median(after)
