@@ -130,7 +130,9 @@ WHITENING_CASES = {
 
 # Whitening cases whose last segment is 1 bin (n = a boundary + 1) and 2 bins
 # (a boundary + 2): median and interpolation branches the cases above never
-# take.  No reference golden run covers them; the oracle pins them.
+# take.  No reference golden run covers them (for a 2-bin segment the
+# reference's median kernel reads one slot past its shared array); the
+# oracle pins them.
 WHITENING_EDGE_CASES = {
     "white_3968x3_last1": dict(n=3968, ndms=3, seed=25),
     "white_8954x2_last2": dict(n=8954, ndms=2, seed=26),
