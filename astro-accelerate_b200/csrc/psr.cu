@@ -716,6 +716,42 @@ cudaError_t psr_whitening(float2 *d_spectra, size_t nSamples, int nDMs, cudaStre
     return e;
 }
 
+// [secondary][primary] -> [primary][secondary] (corner_turn_SM,
+// src/aa_corner_turn.cpp:78-107, which the simple harmonic sum's input
+// goes through): 32 x 32 tiles through a padded shared array.
+__global__ void k_transpose_f32(const float *__restrict__ in, float *__restrict__ out, long long primary,
+                                long long secondary)
+{
+    __shared__ float tile[32][33];
+    const long long x0 = static_cast<long long>(blockIdx.x) * 32, y0 = static_cast<long long>(blockIdx.y) * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5; // 256 threads: 8 rows per pass
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const long long y = y0 + ty + k, x = x0 + tx;
+        if (y < secondary && x < primary)
+            tile[ty + k][tx] = in[y * primary + x];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const long long x = x0 + ty + k, y = y0 + tx;
+        if (x < primary && y < secondary)
+            out[x * secondary + y] = tile[tx][ty + k];
+    }
+}
+
+cudaError_t psr_transpose(const float *d_in, float *d_out, long long primary, long long secondary, cudaStream_t st)
+{
+    if (primary <= 0 || secondary <= 0)
+        return cudaSuccess;
+    const dim3 grid(static_cast<unsigned>((primary + 31) / 32), static_cast<unsigned>((secondary + 31) / 32));
+    if (grid.y > 65535)
+        return cudaErrorInvalidValue;
+    k_transpose_f32<<<grid, 256, 0, st>>>(d_in, d_out, primary, secondary);
+    ++g_psr_launches;
+    return cudaGetLastError();
+}
+
 // The medians alone over a caller's boundary table (segments of 1 to
 // PSR_MAX_SEGMENT bins, increasing, the last one at most nSamples): the
 // whitening's first kernel on tables its own lengths never produce.  The

@@ -59,6 +59,9 @@ cudaError_t psr_whitening(float2 *d_spectra, size_t nSamples, int nDMs, cudaStre
 cudaError_t psr_segment_medians(const float2 *d_spectra, size_t nSamples, int nDMs, const int *segments,
                                 int nSegments, float *d_medians, cudaStream_t st);
 
+// [secondary][primary] -> [primary][secondary]
+cudaError_t psr_transpose(const float *d_in, float *d_out, long long primary, long long secondary, cudaStream_t st);
+
 long long psr_kernel_launches();
 
 } // namespace aab200
