@@ -213,6 +213,12 @@ def lib():
         "aa_py_get_psr_nCandidates": ([vp], P(f)),
         "aa_py_get_psr_interbin_nCandidates": ([vp], P(f)),
         "aa_py_write_to_disk_psr_candidates": ([vp, ctypes.c_char_p], None),
+        "aa_b200_pipeline_bind_periodicity_plan": ([vp, f, i, f, i, i, i, i, i, i], b),
+        "aa_b200_pipeline_set_periodicity_memory": ([vp, ctypes.c_size_t], b),
+        "aa_b200_pipeline_set_device_output": ([vp, i], b),
+        "aa_b200_pipeline_psr_count": ([vp, i], ctypes.c_size_t),
+        "aa_b200_pipeline_write_psr_interbin_candidates": ([vp, ctypes.c_char_p], b),
+        "aa_b200_pipeline_psr_info": ([vp, P(ctypes.c_size_t), P(ctypes.c_size_t), P(i), P(d)], i),
         "aa_py_h_dm": ([vp], P(ctypes.c_uint)),
         "aa_py_h_ts": ([vp], P(ctypes.c_uint)),
         "aa_py_h_snr": ([vp], P(f)),
@@ -408,6 +414,44 @@ class aa_py_analysis_plan:
         return self.m_enable_msd_baseline_noise
 
 
+class aa_py_periodicity_plan:
+    """cmake/py_astro_accelerate.py.in:298-330: the periodicity settings the
+    reference's wrapper passes to aa_py_pipeline_api_bind_periodicity_plan
+    (sigma_constant is the outlier-rejection sigma, enable_msd_baseline_noise
+    switches outlier rejection on; export_powers is kept and unused, as
+    there)."""
+
+    def __init__(self, sigma_cutoff: float, sigma_constant: float, nHarmonics: int, export_powers: int,
+                 candidate_algorithm: int, enable_msd_baseline_noise: bool):
+        self.m_sigma_cutoff = sigma_cutoff
+        self.m_sigma_constant = sigma_constant
+        self.m_nHarmonics = nHarmonics
+        self.m_export_powers = export_powers
+        self.m_candidate_algorithm = candidate_algorithm
+        self.m_enable_msd_baseline_noise = enable_msd_baseline_noise
+
+    def sigma_cutoff(self):
+        return self.m_sigma_cutoff
+
+    def sigma_constant(self):
+        return self.m_sigma_constant
+
+    def nHarmonics(self):
+        return self.m_nHarmonics
+
+    def export_powers(self):
+        return self.m_export_powers
+
+    def candidate_algorithm(self):
+        return self.m_candidate_algorithm
+
+    def candidate_selection_algorithm(self):
+        return int(self.m_candidate_algorithm)
+
+    def enable_msd_baseline_noise(self):
+        return self.m_enable_msd_baseline_noise
+
+
 class aa_py_pipeline:
     """aa_pipeline_api<unsigned short> through the C ABI."""
 
@@ -486,8 +530,64 @@ class aa_py_pipeline:
             raise ValueError(self.last_error())
         return True
 
-    def bind_periodicity_plan(self, plan):
-        return lib().aa_py_pipeline_api_bind_periodicity_plan(self.m_obj, 0.0, False, 0.0, 0, 0)
+    def bind_periodicity_plan(self, plan: "aa_py_periodicity_plan"):
+        """cmake/py_astro_accelerate.py.in:476-479: the plan's sigma cutoff,
+        outlier rejection (its enable_msd_baseline_noise), outlier sigma (its
+        sigma_constant), harmonics and candidate algorithm; the greedy
+        harmonic sum with scalloping-loss mitigation."""
+        return bool(lib().aa_py_pipeline_api_bind_periodicity_plan(
+            self.m_obj, plan.sigma_cutoff(), bool(plan.enable_msd_baseline_noise()), plan.sigma_constant(),
+            int(plan.nHarmonics()), int(plan.candidate_selection_algorithm())))
+
+    def bind_periodicity_plan_full(self, sigma_cutoff=10.0, enable_outlier_rejection=True,
+                                   sigma_outlier_rejection_threshold=3.0, nHarmonics=32, harmonic_sum_algorithm=1,
+                                   candidate_selection_algorithm=0, enable_scalloping_loss_mitigation=True,
+                                   enable_interbinning=True, enable_spectrum_whitening=True):
+        """aa_periodicity_plan's ten-argument constructor
+        (include/aa_periodicity_plan.hpp:62-89): any harmonic sum algorithm
+        (0 simple, 1 greedy, 2 PRESTO plus, 3 PRESTO)."""
+        return bool(lib().aa_b200_pipeline_bind_periodicity_plan(
+            self.m_obj, float(sigma_cutoff), int(bool(enable_outlier_rejection)),
+            float(sigma_outlier_rejection_threshold), int(nHarmonics), int(harmonic_sum_algorithm),
+            int(candidate_selection_algorithm), int(bool(enable_scalloping_loss_mitigation)),
+            int(bool(enable_interbinning)), int(bool(enable_spectrum_whitening))))
+
+    def set_device_output(self, on: bool = True):
+        """Keep every range's output on the device too (before the DDTR plan
+        is bound); the periodicity search then reads the device rows."""
+        if not lib().aa_b200_pipeline_set_device_output(self.m_obj, int(bool(on))):
+            raise ValueError(self.last_error())
+
+    def set_periodicity_memory(self, nbytes: int):
+        """Bytes the periodicity strategy plans for (default: the device's
+        free memory when the plan is bound, as the reference takes it)."""
+        if not lib().aa_b200_pipeline_set_periodicity_memory(self.m_obj, int(nbytes)):
+            raise ValueError(self.last_error())
+
+    def get_psr_candidates(self, interbin: bool = False) -> np.ndarray:
+        """The periodicity candidates [n][4] (DM, frequency, S/N, harmonics)
+        of the power (or interbin) spectra, as aa_py_get_psr_nCandidates /
+        aa_py_get_psr_interbin_nCandidates give them."""
+        n = lib().aa_b200_pipeline_psr_count(self.m_obj, int(bool(interbin)))
+        fn = lib().aa_py_get_psr_interbin_nCandidates if interbin else lib().aa_py_get_psr_nCandidates
+        ptr = fn(self.m_obj)
+        if not ptr:
+            raise RuntimeError(self.last_error())
+        return np.ctypeslib.as_array(ptr, shape=(4 * n + 4,))[:4 * n].reshape(n, 4).copy()
+
+    def write_psr_candidates(self, filename: str, interbin: bool = False):
+        if interbin:
+            if not lib().aa_b200_pipeline_write_psr_interbin_candidates(self.m_obj, filename.encode()):
+                raise RuntimeError(self.last_error())
+        else:
+            lib().aa_py_write_to_disk_psr_candidates(self.m_obj, filename.encode())
+
+    def psr_info(self) -> dict:
+        fl, dpb, nb, ms = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_int(), ctypes.c_double()
+        if lib().aa_b200_pipeline_psr_info(self.m_obj, ctypes.byref(fl), ctypes.byref(dpb), ctypes.byref(nb),
+                                           ctypes.byref(ms)):
+            raise RuntimeError("no periodicity plan bound")
+        return {"fft_length": fl.value, "dms_per_batch": dpb.value, "batches": nb.value, "compute_ms": ms.value}
 
     def bind_fdas_plan(self, plan):
         return lib().aa_py_pipeline_api_bind_fdas_plan(self.m_obj, 0.0, 0.0, False)

@@ -14,6 +14,7 @@
 #include "spd.cuh"
 #include "export.hpp"
 #include "pipeline.hpp"
+#include "psr_search.hpp"
 #include "planner.hpp"
 
 using namespace aab200;
@@ -57,7 +58,21 @@ struct Api {
     SpdCandidates cands;          // the last step's candidates
     bool write_candidates = true; // the reference's peak_analysed/analysed files
     std::string candidate_dir;    // where they go ("" = the working directory)
-    ~Api() { cudaFree(d_spd_plane); }
+    // periodicity search after the last dedispersion step
+    bool psr_bound = false;
+    bool psr_did_run = false;
+    PsrPlanParams psr_plan;
+    PsrStrategy psr_strategy;
+    size_t psr_free_memory = 0; // 0: the device's free memory when the plan is bound
+    std::unique_ptr<PsrSearch> psr;
+    void *psr_power = nullptr, *psr_inter = nullptr; // candidate lists (psr_candidates.cpp)
+    std::vector<float> psr_h_power, psr_h_inter;     // the getters' copies
+    ~Api()
+    {
+        cudaFree(d_spd_plane);
+        aa_b200_psr_candidates_destroy(psr_power);
+        aa_b200_psr_candidates_destroy(psr_inter);
+    }
 };
 
 
@@ -251,10 +266,15 @@ void *aa_py_pipeline_api(pipeline_components_struct pipeline, pipeline_component
     a->input = input_data;
     a->card = card_number;
     a->popt.copy_to_host = options.copy_ddtr_data_to_host;
-    if (pipeline.periodicity || pipeline.fdas || !pipeline.dedispersion) {
+    if (pipeline.fdas || !pipeline.dedispersion) {
         a->supported = false;
-        api_fail(a, "only the dedispersion and analysis components are implemented by this library");
+        api_fail(a, "the dedispersion, analysis and periodicity components are implemented by this library");
     }
+    // the periodicity search reads the host rows, as the reference's runner
+    // does (include/aa_permitted_pipelines_generic.hpp:590), unless they are
+    // kept on the device (aa_b200_pipeline_set_device_output)
+    if (pipeline.periodicity)
+        a->popt.copy_to_host = true;
     a->popt.enable_analysis = pipeline.analysis;
     // include/aa_py_pipeline_api.cpp:24-35 -> the runner's options
     a->popt.zero_dm = options.zero_dm;
@@ -387,21 +407,37 @@ void *aa_py_pipeline_api_analysis_strategy(void *obj)
     return new AnalysisPlan(a->aplan);
 }
 
-// :129-141: periodicity candidates; the periodicity component is refused by
-// this library, so there are none.
-float *aa_py_get_psr_nCandidates(void *obj)
+// :129-141: periodicity candidates (Get_PSR_candidates and
+// Write_to_disk_PSR_candidates of include/aa_permitted_pipelines_generic.hpp:1173-1193):
+// the records (DM, frequency, S/N, harmonics) of every batch in order, in a
+// copy owned by the pipeline object (valid until the next call of the same
+// getter); NULL with an error message when the search has not run.
+namespace {
+float *psr_copy(Api *a, bool interbin)
 {
-    api_fail(as_api(obj), "periodicity search is not implemented by this library");
-    return nullptr;
+    void *list = interbin ? a->psr_inter : a->psr_power;
+    if (!list || !a->psr_did_run) {
+        api_fail(a, "no periodicity candidates: the periodicity search has not run");
+        return nullptr;
+    }
+    std::vector<float> &h = interbin ? a->psr_h_inter : a->psr_h_power;
+    h.assign(4 * aa_b200_psr_candidates_count(list) + 4, 0.f);
+    aa_b200_psr_candidates_copy(list, h.data());
+    return h.data();
 }
-float *aa_py_get_psr_interbin_nCandidates(void *obj)
+} // namespace
+
+float *aa_py_get_psr_nCandidates(void *obj) { return psr_copy(as_api(obj), false); }
+float *aa_py_get_psr_interbin_nCandidates(void *obj) { return psr_copy(as_api(obj), true); }
+void aa_py_write_to_disk_psr_candidates(void *obj, const char *filename)
 {
-    api_fail(as_api(obj), "periodicity search is not implemented by this library");
-    return nullptr;
-}
-void aa_py_write_to_disk_psr_candidates(void *obj, const char *)
-{
-    api_fail(as_api(obj), "periodicity search is not implemented by this library");
+    Api *a = as_api(obj);
+    if (!a->psr_power || !a->psr_did_run) {
+        api_fail(a, "no periodicity candidates: the periodicity search has not run");
+        return;
+    }
+    if (aa_b200_psr_candidates_export(a->psr_power, filename) != 0)
+        api_fail(a, aa_b200_psr_candidates_last_error());
 }
 
 size_t aa_py_spd_nCandidates(void *obj) { return as_api(obj)->cands.dm.size(); }
@@ -425,9 +461,166 @@ unsigned int *aa_py_h_width(void *obj)
     Api *a = as_api(obj);
     return a->cands.bw.empty() ? nullptr : a->cands.bw.data();
 }
-bool aa_py_pipeline_api_bind_periodicity_plan(void *obj, float, bool, float, int, int)
+namespace {
+// aa_pipeline_api::bind(aa_periodicity_plan) (include/aa_pipeline_api.hpp:226-253)
+// with the plan extracted from the DDTR strategy
+// (include/aa_periodicity_plan.hpp:292-321): every range's DM grid, binning
+// and trial count, the processed samples of the whole run and the data's
+// sampling time; the strategy for the device's free memory
+bool bind_psr(Api *a, const PsrPlanParams &p)
 {
-    return api_fail(as_api(obj), "periodicity search is not implemented by this library");
+    if (!a->supported)
+        return false;
+    if (!a->components.periodicity)
+        return api_fail(a, "the pipeline was created without the periodicity component");
+    if (a->psr_bound)
+        return api_fail(a, "a periodicity plan is already bound");
+    if (!a->pipe)
+        return api_fail(a, "bind the DDTR plan before the periodicity plan");
+    const DdtrStrategy &S = a->pipe->strategy();
+    std::vector<PsrDdtrRange> ranges;
+    for (size_t r = 0; r < S.nranges(); ++r) {
+        PsrDdtrRange d;
+        d.dm_low = S.dm(r).low;
+        d.dm_high = S.dm(r).high;
+        d.dm_step = S.dm(r).step;
+        d.inBin = S.dm(r).inBin;
+        d.nTimesamples = S.nProcessedTimesamples();
+        d.nDMs = S.ndms(r);
+        d.sampling_time = a->meta.tsamp;
+        ranges.push_back(d);
+    }
+    size_t free_mem = a->psr_free_memory;
+    if (free_mem == 0) {
+        size_t total = 0;
+        if (cudaSetDevice(a->card) != cudaSuccess || cudaMemGetInfo(&free_mem, &total) != cudaSuccess)
+            return api_fail(a, "cannot read the device's free memory");
+    }
+    std::string err;
+    if (!psr_strategy(p, ranges, free_mem, a->psr_strategy, err))
+        return api_fail(a, err);
+    a->psr_plan = p;
+    a->psr_bound = true;
+    return true;
+}
+
+// GPU_periodicity (src/aa_device_periods.cu:570-682) over the finished run's
+// output rows, host or device
+bool run_psr(Api *a)
+{
+    std::string err;
+    if (!a->psr)
+        a->psr.reset(new PsrSearch());
+    if (!a->psr->setup(a->psr_strategy, err))
+        return api_fail(a, err);
+    aa_b200_psr_candidates_destroy(a->psr_power);
+    aa_b200_psr_candidates_destroy(a->psr_inter);
+    a->psr_power = aa_b200_psr_candidates_create();
+    a->psr_inter = aa_b200_psr_candidates_create();
+    if (!a->psr_power || !a->psr_inter)
+        return api_fail(a, "periodicity search: out of host memory");
+    const DdtrStrategy &S = a->pipe->strategy();
+    std::vector<PsrRows> rows(S.nranges());
+    float ***host = a->pipe->output_buffer();
+    for (size_t r = 0; r < S.nranges(); ++r) {
+        PsrRows &R = rows[r];
+        R.pitch = S.total_samps(r);
+        R.row_len = S.total_samps(r);
+        if (a->pipe->device_output(static_cast<int>(r))) {
+            R.base = a->pipe->device_output(static_cast<int>(r));
+            R.on_device = true;
+        } else if (host && host[r]) {
+            R.base = host[r][0];
+            R.on_device = false;
+        } else {
+            return api_fail(a, "periodicity search: the DM-time rows are neither on the host nor on the device");
+        }
+    }
+    if (!a->psr->run(a->psr_strategy, rows, a->psr_power, a->psr_inter, a->pipe->stream(), err))
+        return api_fail(a, err);
+    a->psr_did_run = true;
+    // the search's device buffers go (GPU_Memory_for_Periodicity_Search's
+    // lifetime, :578-590)
+    a->psr->release();
+    return true;
+}
+} // namespace
+
+bool aa_py_pipeline_api_bind_periodicity_plan(void *obj, float sigma_cutoff, bool enable_outlier_rejection,
+                                              float sigma_outlier_rejection_threshold, int nHarmonics,
+                                              int candidate_selection_algorithm)
+{
+    // src/aa_py_pipeline_api.cpp:82-85 -> aa_periodicity_plan's six-argument
+    // constructor (include/aa_periodicity_plan.hpp:39-60): greedy harmonic
+    // sum, scalloping-loss mitigation, interbinning and whitening on
+    PsrPlanParams p;
+    p.sigma_cutoff = sigma_cutoff;
+    p.enable_outlier_rejection = enable_outlier_rejection;
+    p.sigma_outlier_rejection_threshold = sigma_outlier_rejection_threshold;
+    p.nHarmonics = nHarmonics;
+    p.harmonic_sum_algorithm = 1;
+    p.candidate_selection_algorithm = candidate_selection_algorithm;
+    return bind_psr(as_api(obj), p);
+}
+
+bool aa_b200_pipeline_bind_periodicity_plan(void *obj, float sigma_cutoff, int enable_outlier_rejection,
+                                            float sigma_outlier_rejection_threshold, int nHarmonics,
+                                            int harmonic_sum_algorithm, int candidate_selection_algorithm,
+                                            int enable_scalloping_loss_mitigation, int enable_interbinning,
+                                            int enable_spectrum_whitening)
+{
+    PsrPlanParams p;
+    p.sigma_cutoff = sigma_cutoff;
+    p.enable_outlier_rejection = enable_outlier_rejection != 0;
+    p.sigma_outlier_rejection_threshold = sigma_outlier_rejection_threshold;
+    p.nHarmonics = nHarmonics;
+    p.harmonic_sum_algorithm = harmonic_sum_algorithm;
+    p.candidate_selection_algorithm = candidate_selection_algorithm;
+    p.enable_scalloping_loss_mitigation = enable_scalloping_loss_mitigation != 0;
+    p.enable_interbinning = enable_interbinning != 0;
+    p.enable_spectrum_whitening = enable_spectrum_whitening != 0;
+    return bind_psr(as_api(obj), p);
+}
+
+bool aa_b200_pipeline_set_periodicity_memory(void *obj, size_t bytes)
+{
+    Api *a = as_api(obj);
+    if (a->psr_bound)
+        return api_fail(a, "set the periodicity memory before binding the periodicity plan");
+    a->psr_free_memory = bytes;
+    return true;
+}
+
+size_t aa_b200_pipeline_psr_count(void *obj, int interbin)
+{
+    Api *a = as_api(obj);
+    void *list = interbin ? a->psr_inter : a->psr_power;
+    return list ? aa_b200_psr_candidates_count(list) : 0;
+}
+
+bool aa_b200_pipeline_write_psr_interbin_candidates(void *obj, const char *filename)
+{
+    Api *a = as_api(obj);
+    if (!a->psr_inter || !a->psr_did_run)
+        return api_fail(a, "no periodicity candidates: the periodicity search has not run");
+    if (aa_b200_psr_candidates_export(a->psr_inter, filename) != 0)
+        return api_fail(a, aa_b200_psr_candidates_last_error());
+    return true;
+}
+
+int aa_b200_pipeline_psr_info(void *obj, size_t *fft_length, size_t *dms_per_batch, int *batches, double *compute_ms)
+{
+    Api *a = as_api(obj);
+    if (!a->psr_bound)
+        return 1;
+    int nb = 0;
+    for (const PsrRange &R : a->psr_strategy.ranges)
+        nb += static_cast<int>(R.batches.size());
+    *fft_length = a->psr_strategy.corrected_max_nTimesamples;
+    *dms_per_batch = a->psr_strategy.max_nDMs_in_memory;
+    *batches = nb;
+    *compute_ms = a->psr ? a->psr->last_compute_ms : 0.0;
+    return 0;
 }
 bool aa_py_pipeline_api_bind_fdas_plan(void *obj, float, float, bool)
 {
@@ -464,6 +657,23 @@ bool aa_py_pipeline_api_run(void *obj, int *status_code)
             api_fail(a, a->pipe->last_error());
         *status_code = static_cast<int>(RunStatus::error);
         return false;
+    }
+    // include/aa_permitted_pipelines_generic.hpp:650-655: after the
+    // dedispersion component finished, one more call runs the periodicity
+    // search and reports finished_component
+    if (!more && st == RunStatus::finished && a->components.periodicity && !a->psr_did_run) {
+        if (!a->psr_bound) {
+            *status_code = static_cast<int>(RunStatus::error);
+            return api_fail(a, "the periodicity component needs a periodicity plan bound");
+        }
+        if (!a->pipe->synchronize() || !run_psr(a)) {
+            if (a->error.empty())
+                api_fail(a, a->pipe->last_error());
+            *status_code = static_cast<int>(RunStatus::error);
+            return false;
+        }
+        *status_code = static_cast<int>(RunStatus::finished_component);
+        return true;
     }
     return more;
 }
@@ -774,6 +984,15 @@ bool aa_b200_pipeline_set_packed_input(void *obj, const void *packed)
         return api_fail(a, "the packed input pointer is null");
     a->packed = packed;
     a->popt.packed_input = true;
+    return true;
+}
+
+bool aa_b200_pipeline_set_device_output(void *obj, int on)
+{
+    Api *a = as_api(obj);
+    if (a->pipe)
+        return api_fail(a, "the device output must be chosen before the plan is bound");
+    a->popt.device_output = on != 0;
     return true;
 }
 

@@ -9,8 +9,8 @@
  *     path (AstroAccelerate v1.3.1, src/aa_py_*.cpp, bound by ctypes in
  *     cmake/py_astro_accelerate.py.in).  Same names, argument meaning, return
  *     values and status codes, so the reference's Python wrapper binds this
- *     library by changing the library path.  The dedispersion and analysis
- *     (single-pulse detection) components are implemented; periodicity and
+ *     library by changing the library path.  The dedispersion, analysis
+ *     (single-pulse detection) and periodicity components are implemented;
  *     FDAS plans are refused (return false).
  *
  *  2. aa_b200_* : the seam the reference's runner calls internally
@@ -146,8 +146,13 @@ size_t aa_py_spd_nCandidates(void *obj);
 /* :78-80: the bound analysis settings as a new object (NULL when none is
  * bound); free with aa_analysis_plan_delete. */
 void *aa_py_pipeline_api_analysis_strategy(void *obj);
-/* :129-141: periodicity candidates; periodicity is refused, so these return
- * NULL (write does nothing) and set the pipeline's error message. */
+/* :129-141: periodicity candidates after the search ran (Get_PSR_candidates,
+ * Get_PSR_interbin_candidates, Write_to_disk_PSR_candidates of
+ * include/aa_permitted_pipelines_generic.hpp:1173-1193): records of 4 floats
+ * (DM, frequency, S/N, harmonics), every batch's in order, in a copy the
+ * pipeline object owns (valid until the next call of the same getter; the
+ * count is aa_b200_pipeline_psr_count).  NULL (write: nothing) with an
+ * error message before the search has run. */
 float *aa_py_get_psr_nCandidates(void *obj);
 float *aa_py_get_psr_interbin_nCandidates(void *obj);
 void aa_py_write_to_disk_psr_candidates(void *obj, const char *filename);
@@ -155,13 +160,49 @@ unsigned int *aa_py_h_dm(void *obj);
 unsigned int *aa_py_h_ts(void *obj);
 float *aa_py_h_snr(void *obj);
 unsigned int *aa_py_h_width(void *obj);
-/* :82-85, :87-90: periodicity and FDAS are out of scope for this library
- * and are refused (false). */
+/* :82-85: the periodicity plan (aa_periodicity_plan's six-argument
+ * constructor, include/aa_periodicity_plan.hpp:39-60: greedy harmonic sum,
+ * scalloping-loss mitigation and whitening on) built from the bound DDTR
+ * strategy, and its strategy for the device's free memory
+ * (include/aa_periodicity_strategy.hpp:178-355).  The pipeline must have
+ * been created with the periodicity component and the DDTR plan bound; the
+ * search then runs on the run() call after the dedispersion component
+ * finished (status finished_component), over the host rows or, when they
+ * are kept on the device, the device rows.  :87-90: FDAS is out of scope
+ * and refused (false). */
 bool aa_py_pipeline_api_bind_periodicity_plan(void *obj, float sigma_cutoff, bool enable_outlier_rejection,
                                               float sigma_outlier_rejection_threshold, int nHarmonics,
                                               int candidate_selection_algorithm);
 bool aa_py_pipeline_api_bind_fdas_plan(void *obj, float sigma_cutoff, float sigma_constant,
                                        bool enable_msd_baseline_noise);
+/* aa_periodicity_plan's ten-argument constructor
+ * (include/aa_periodicity_plan.hpp:62-89): harmonic_sum_algorithm 0 simple
+ * (on corner-turned spectra), 1 greedy, 2 PRESTO plus, 3 PRESTO;
+ * candidate_selection_algorithm 0 peak finding, 1 thresholding.  The
+ * interbinning and whitening switches are carried as the reference carries
+ * them (its search computes both either way). */
+bool aa_b200_pipeline_bind_periodicity_plan(void *obj, float sigma_cutoff, int enable_outlier_rejection,
+                                            float sigma_outlier_rejection_threshold, int nHarmonics,
+                                            int harmonic_sum_algorithm, int candidate_selection_algorithm,
+                                            int enable_scalloping_loss_mitigation, int enable_interbinning,
+                                            int enable_spectrum_whitening);
+/* on != 0: keep every range's whole output on the device as well
+ * ([ndms][total samples] per range, aa_b200_pipeline_device_output), also
+ * for pipelines made by aa_py_pipeline_api; before the DDTR plan is bound.
+ * The periodicity search then reads these rows instead of the host rows. */
+bool aa_b200_pipeline_set_device_output(void *obj, int on);
+/* Bytes the periodicity strategy plans its batches for, instead of the
+ * device's free memory at bind time (before binding the plan). */
+bool aa_b200_pipeline_set_periodicity_memory(void *obj, size_t bytes);
+/* Candidates of the power (interbin = 0) or interbin (1) spectra. */
+size_t aa_b200_pipeline_psr_count(void *obj, int interbin);
+/* Write_to_disk_PSR_interbin_candidates (include/aa_pipeline_api.hpp:1142-1144). */
+bool aa_b200_pipeline_write_psr_interbin_candidates(void *obj, const char *filename);
+/* The bound periodicity strategy: FFT length of unbinned ranges, DM trials
+ * per batch, batches over all ranges; compute_ms: device time of the last
+ * search's stages (after each batch's input copy).  Returns 0, or 1 when no
+ * periodicity plan is bound. */
+int aa_b200_pipeline_psr_info(void *obj, size_t *fft_length, size_t *dms_per_batch, int *batches, double *compute_ms);
 /* :92-103: one (time chunk, DM range) step; *status_code receives
  * aa_pipeline_runner::status (-1 error, 0 finished, 1 has_more,
  * 2 finished_component, include/aa_pipeline_runner.hpp:25-30). */

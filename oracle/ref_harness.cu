@@ -372,6 +372,77 @@ int aaref_run_pipeline_spd(const unsigned short *input_tc, int nchans, int nsamp
     return nsteps;
 }
 
+/* The reference runner with dedispersion and periodicity components
+ * (include/aa_permitted_pipelines_generic.hpp:570-660, :916-947): the DDTR
+ * strategy for free_memory, the periodicity plan's ten-argument constructor
+ * (include/aa_periodicity_plan.hpp:62-89) and its strategy for psr_memory
+ * bytes, the run loop to the end, then the power and interbin candidate
+ * lists (4 floats per record) into power/interbin (cap records each) and
+ * their counts into *npower / *ninterbin.  Returns 0, or < 0 (-8: a list
+ * longer than cap; the counts are set). */
+int aaref_run_pipeline_psr(const unsigned short *input_tc, int nchans, int nsamp, double tsamp, double fch1,
+                           double foff, int nbits, const harness_dm *plan, int nranges, size_t free_memory,
+                           size_t psr_memory, float sigma_cutoff, int enable_outlier_rejection,
+                           float sigma_outlier_rejection_threshold, int nHarmonics, int harmonic_sum_algorithm,
+                           int candidate_selection_algorithm, int enable_scalloping_loss_mitigation, float *power,
+                           long long *npower, float *interbin, long long *ninterbin, long long cap)
+{
+    aa_device_info dev(0);
+    aa_ddtr_plan p;
+    for (int i = 0; i < nranges; i++)
+        p.add_dm(plan[i].low, plan[i].high, plan[i].step, plan[i].inBin, plan[i].outBin);
+    aa_filterbank_metadata meta(0.0, tsamp, nbits, nsamp, fch1, foff, nchans);
+    size_t fm = free_memory ? free_memory : dev.free_memory();
+    int rc = 0;
+    {
+        aa_ddtr_strategy s(p, meta, fm, false, &dev);
+        if (!s.ready())
+            return -1;
+        if ((long long)nchans * (long long)(s.t_processed()[0][0] + s.maxshift()) >= (1LL << 31))
+            return -6;
+        aa_periodicity_plan pp(s, sigma_cutoff, enable_outlier_rejection != 0, sigma_outlier_rejection_threshold,
+                               nHarmonics, harmonic_sum_algorithm, candidate_selection_algorithm,
+                               enable_scalloping_loss_mitigation != 0, true, true);
+        aa_periodicity_strategy per(pp, psr_memory ? psr_memory : dev.free_memory());
+        if (!per.ready())
+            return -7;
+        aa_pipeline::pipeline comps;
+        comps.insert(aa_pipeline::component::dedispersion);
+        comps.insert(aa_pipeline::component::periodicity);
+        aa_pipeline::pipeline_option opts;
+        opts.insert(aa_pipeline::component_option::copy_ddtr_data_to_host);
+        aa_analysis_strategy an;
+        aa_fdas_strategy fd;
+        aa_jerk_strategy jk;
+        aa_permitted_pipelines_generic runner(comps, opts, s, an, per, fd, jk, false, false, false, false, false,
+                                              input_tc);
+        if (!runner.setup())
+            return -2;
+        aa_pipeline_runner::status st;
+        bool more = true;
+        while (more) {
+            more = runner.next(st);
+            if (st == aa_pipeline_runner::status::error)
+                return -3;
+        }
+        if (cudaDeviceSynchronize() != cudaSuccess)
+            return -9;
+        *npower = (long long)runner.get_PSR_nCandidates();
+        *ninterbin = (long long)runner.get_PSR_interbin_nCandidates();
+        if (*npower > cap || *ninterbin > cap) {
+            rc = -8;
+        } else {
+            const float *hp = runner.Get_PSR_candidates();
+            if (*npower > 0)
+                memcpy(power, hp, (size_t)*npower * 4 * sizeof(float));
+            const float *hi = runner.Get_PSR_interbin_candidates();
+            if (*ninterbin > 0)
+                memcpy(interbin, hi, (size_t)*ninterbin * 4 * sizeof(float));
+        }
+    }
+    return rc;
+}
+
 /* aaref_time_ddtr with the analysis component: the runner's run(status)
  * loop with dedispersion, D2H (copy_to_host) and analysis_GPU after every
  * step, wall clock after setup.  Candidate files go to the working

@@ -51,18 +51,33 @@ def test_plan_objects_roundtrip(aa):
 
 def test_out_of_scope_components_are_refused(aa):
     md = aa.filterbank_metadata_struct(0.0, 64e-6, 1550.0, -0.39, 8, 1 << 16, 256, 0.0)
-    # periodicity is out of scope (dedispersion and analysis are implemented)
-    comps = aa.aa_py_pipeline_components(True, False, True, False)
+    # FDAS is out of scope (dedispersion, analysis and periodicity are implemented)
+    comps = aa.aa_py_pipeline_components(True, False, False, True)
     opts = aa.aa_py_pipeline_component_options()
     x = np.zeros(256 * (1 << 16), np.uint16)
     p = aa.aa_py_pipeline(comps, opts, md, x, 0)
     plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(0, 100, 1, 1, 1)])
     assert not p.bind_ddtr_plan(plan)
-    assert "dedispersion" in p.last_error()
+    assert "periodicity" in p.last_error()
     assert not p.run() and p.status_code() == aa.STATUS_ERROR
     assert not p.bind_fdas_plan(None)
     p.delete()
     plan.delete()
+
+
+def test_periodicity_plan_needs_its_component_and_a_ddtr_plan(aa):
+    """Host-side refusals (no GPU call): a periodicity plan on a pipeline
+    without the periodicity component, or before the DDTR plan is bound."""
+    md = aa.filterbank_metadata_struct(0.0, 64e-6, 1550.0, -0.39, 8, 1 << 16, 256, 0.0)
+    x = np.zeros(256 * (1 << 16), np.uint16)
+    pp = aa.aa_py_periodicity_plan(6.0, 3.0, 32, 0, 0, True)
+    for comps, needle in ((aa.aa_py_pipeline_components(True, False, False, False), "periodicity component"),
+                          (aa.aa_py_pipeline_components(True, False, True, False), "DDTR plan")):
+        p = aa.aa_py_pipeline(comps, aa.aa_py_pipeline_component_options(), md, x, 0)
+        assert not p.bind_periodicity_plan(pp)
+        assert needle in p.last_error(), p.last_error()
+        assert aa.lib().aa_b200_pipeline_psr_count(p.m_obj, 0) == 0
+        p.delete()
 
 
 def test_strategy_refusal_codes(aa):

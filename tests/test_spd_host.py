@@ -104,18 +104,24 @@ def test_analysis_plan_refusals(aa):
     L.aa_analysis_plan_delete(p)
 
 
-def test_periodicity_and_fdas_still_refused(aa):
+def test_fdas_still_refused(aa):
     md = aa.filterbank_metadata_struct(0.0, 64e-6, 1500.0, -1.0, 8, 1 << 15, 256, 0.0)
     o = aa.aa_py_pipeline_component_options()
+    pipe = aa.aa_py_pipeline(aa.aa_py_pipeline_components(True, True, True, True), o, md,
+                             np.zeros(256 * (1 << 15), np.uint16), 0)
+    assert "the dedispersion, analysis and periodicity components" in pipe.last_error()
+    pipe.delete()
+    # dedispersion, analysis and periodicity together are accepted
     pipe = aa.aa_py_pipeline(aa.aa_py_pipeline_components(True, True, True, False), o, md,
                              np.zeros(256 * (1 << 15), np.uint16), 0)
-    assert "periodicity" in pipe.last_error() or "only the dedispersion and analysis" in pipe.last_error()
+    assert pipe.last_error() == ""
     pipe.delete()
 
 
 def test_analysis_strategy_and_psr_entries(aa):
     """aa_py_pipeline_api_analysis_strategy gives the bound settings (none
-    before bind); the periodicity candidate entries exist and return nothing."""
+    before bind); the periodicity candidate entries exist and return nothing
+    before a periodicity search has run."""
     md = aa.filterbank_metadata_struct(0.0, 64e-6, 1500.0, -1.0, 8, 1 << 15, 256, 0.0)
     o = aa.aa_py_pipeline_component_options()
     pipe = aa.aa_py_pipeline(aa.aa_py_pipeline_components(True, True, False, False), o, md,
