@@ -753,6 +753,79 @@ int aa_b200_strategy(const aa_b200_dm *plan, int nranges, float power, int nchan
     return 0;
 }
 
+int aa_b200_psr_strategy(const aa_b200_dm *plan, int nranges, int nchans, int nsamp, double tsamp, double fch1,
+                         double foff, int nbits, size_t ddtr_memory, size_t memory_available, float sigma_cutoff,
+                         int nHarmonics, int harmonic_sum_algorithm, long long *info, long long *range_info,
+                         int max_ranges, long long *batches, int max_batches)
+{
+    DdtrPlan p;
+    for (int i = 0; i < nranges; ++i)
+        p.add_dm(plan[i].low, plan[i].high, plan[i].step, plan[i].inBin, plan[i].outBin);
+    FilterbankMetadata m;
+    m.tsamp = tsamp;
+    m.fch1 = fch1;
+    m.foff = foff;
+    m.nbits = nbits;
+    m.nsamples = nsamp;
+    m.nchans = nchans;
+    DdtrStrategy s;
+    if (s.compute(p, m, ddtr_memory, false) != STRAT_OK) {
+        set_error("strategy refused the plan");
+        return -1;
+    }
+    std::vector<PsrDdtrRange> ranges;
+    for (size_t r = 0; r < s.nranges(); ++r) {
+        PsrDdtrRange d;
+        d.dm_low = s.dm(r).low;
+        d.dm_high = s.dm(r).high;
+        d.dm_step = s.dm(r).step;
+        d.inBin = s.dm(r).inBin;
+        d.nTimesamples = s.nProcessedTimesamples();
+        d.nDMs = s.ndms(r);
+        d.sampling_time = tsamp;
+        ranges.push_back(d);
+    }
+    PsrPlanParams pp;
+    pp.sigma_cutoff = sigma_cutoff;
+    pp.nHarmonics = nHarmonics;
+    pp.harmonic_sum_algorithm = harmonic_sum_algorithm;
+    PsrStrategy ps;
+    std::string err;
+    info[6] = psr_strategy(pp, ranges, memory_available, ps, err) ? 1 : 0;
+    if (!info[6]) {
+        set_error(err);
+        return 0;
+    }
+    info[0] = static_cast<long long>(ps.corrected_max_nTimesamples);
+    info[1] = static_cast<long long>(ps.nTimesamples_to_copy);
+    info[3] = static_cast<long long>(ps.input_plane_size);
+    info[4] = static_cast<long long>(ps.cufft_workarea_size);
+    info[5] = static_cast<long long>(ps.max_total_MSD_blocks);
+    int nb = 0;
+    for (size_t r = 0; r < ps.ranges.size(); ++r) {
+        const PsrRange &R = ps.ranges[r];
+        if (static_cast<int>(r) < max_ranges) {
+            range_info[2 * r] = static_cast<long long>(R.range.nTimesamples);
+            range_info[2 * r + 1] = static_cast<long long>(R.batches.size());
+        }
+        for (const PsrBatch &b : R.batches) {
+            if (nb < max_batches) {
+                batches[5 * nb + 0] = static_cast<long long>(r);
+                batches[5 * nb + 1] = static_cast<long long>(b.nDMs_per_batch);
+                batches[5 * nb + 2] = static_cast<long long>(b.DM_shift);
+                batches[5 * nb + 3] = static_cast<long long>(b.nTimesamples);
+                batches[5 * nb + 4] = static_cast<long long>(b.nTimesamples_to_copy);
+            }
+            ++nb;
+        }
+    }
+    info[2] = (!ps.ranges.empty() && !ps.ranges[0].batches.empty())
+                  ? static_cast<long long>(ps.ranges[0].batches[0].nDMs_per_batch) /
+                        std::max(1, ps.ranges[0].range.inBin)
+                  : 0;
+    return nb;
+}
+
 int aa_b200_select_kernel(int nbits, float dm_step, float tsamp, float dmshift_last, int failsafe)
 {
     return select_delay_kind(nbits, dm_step, tsamp, dmshift_last, failsafe);

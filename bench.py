@@ -72,7 +72,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="survey", choices=["survey", "mid", "small", "batched", "refine", "e2e", "spd", "whitening"])
+    ap.add_argument("--config", default="survey",
+                    choices=["survey", "mid", "small", "batched", "refine", "e2e", "spd", "whitening", "periodicity"])
     ap.add_argument("--beams", type=int, default=48, help="beams of the multi-beam draw (batched config)")
     ap.add_argument("--snippets", type=int, default=256, help="snippets per step (refine config)")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -1153,6 +1154,103 @@ def run_spd(args, rank, world, local):
     return 0
 
 
+PERIODICITY_METRIC = "DM-trial*FFT-points/s searched (periodicity component, reference rules)"
+
+
+def run_periodicity(args, rank, world, local):
+    """The periodicity component after dedispersion, through the
+    reference-facing C ABI: the 4096-channel x 2^18-sample 8-bit input with
+    the 8-range survey plan (the reference runner's GPU size), every DM
+    trial searched with a 2^17-point FFT (the processed length rounded down
+    to a power of two, halved per binning): whitening, power and interbin
+    spectra, MSD profile, greedy harmonic sums of 32 harmonics with
+    scalloping-loss mitigation, peak finding at 10 sigma.  One step = one
+    whole pipeline run (dedispersion with the rows kept on the device, then
+    the periodicity search); `value` is the search's device time (CUDA
+    events around each batch's stages, after its input copy), `e2e` the
+    wall time of the run() call that performs the search."""
+    import numpy as np
+    import torch
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "metric": PERIODICITY_METRIC,
+                              "unavailable": "the reference's periodicity search is not run here: its whitening "
+                                             "reads one boundary and one median past its tables on every call, "
+                                             "and a run of it in a shared process was followed by an illegal "
+                                             "memory access"}), flush=True)
+        return 0
+    import aa_b200 as aa
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    cfg = MID
+    x, _ = synth_input_device(cfg, cfg["seed"] + rank, device)
+    host = x.cpu().numpy().view(np.uint16).reshape(-1)
+    del x
+    torch.cuda.empty_cache()
+    md = aa.filterbank_metadata_struct(0.0, cfg["tsamp"], cfg["fch1"], cfg["foff"], cfg["nbits"], cfg["nsamp"],
+                                       cfg["nchans"], 0.0)
+
+    def one():
+        comps = aa.aa_py_pipeline_components(True, False, True, False)
+        o = aa.aa_py_pipeline_component_options()
+        o.copy_ddtr_data_to_host = True
+        pipe = aa.aa_py_pipeline(comps, o, md, host, local)
+        pipe.set_device_output(True)
+        plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*q) for q in cfg["plan"]])
+        if not pipe.bind_ddtr_plan(plan) or not pipe.bind_periodicity_plan_full(10.0, True, 3.0, 32, 1, 0, True):
+            raise RuntimeError(pipe.last_error())
+        wall = None
+        while True:
+            comp_done = pipe.status_code() == aa.STATUS_FINISHED_COMPONENT
+            t0 = time.perf_counter()
+            more = pipe.run()
+            dt = time.perf_counter() - t0
+            if pipe.status_code() == aa.STATUS_ERROR:
+                raise RuntimeError(pipe.last_error())
+            if comp_done and pipe.status_code() == aa.STATUS_FINISHED_COMPONENT:
+                wall = dt  # the call after dedispersion's finished_component runs the search
+            if not more:
+                break
+        info = pipe.psr_info()
+        n = (pipe.get_psr_candidates(False).shape[0], pipe.get_psr_candidates(True).shape[0])
+        pipe.cleanUp()
+        pipe.delete()
+        plan.delete()
+        return info, wall, n
+
+    for _ in range(max(1, args.warmup)):
+        one()
+    launches0 = aa.lib().aa_b200_psr_kernel_launches() + aa.spd_kernel_launches()
+    ms, walls = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            info, wall, ncand = one()
+            ms.append(info["compute_ms"])
+            walls.append(wall)
+    # this library's periodicity and MSD kernels (cuFFT's own not counted)
+    launches = (aa.lib().aa_b200_psr_kernel_launches() + aa.spd_kernel_launches() - launches0) // max(1, args.steps)
+    strat = aa.strategy(cfg["plan"], cfg["nchans"], cfg["nsamp"], cfg["fch1"], cfg["foff"], cfg["tsamp"], cfg["nbits"])
+    points = sum(strat["ndms"][r] * (info["fft_length"] // cfg["plan"][r][3]) for r in range(len(cfg["plan"])))
+    step_ms = statistics.median(ms)
+    wall_s = statistics.median(walls)
+    line = {"metric": PERIODICITY_METRIC, "value": points / (step_ms / 1e3), "unit": "DM-trial*FFT-points/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"periodicity search of the {cfg['nchans']} ch x {cfg['nsamp']} samples 8-bit "
+                                   f"run, 8-range survey plan: {sum(strat['ndms'])} DM trials, FFT length "
+                                   f"{info['fft_length']} (halved per binning), greedy harmonic sum of 32, "
+                                   f"peak finding at 10 sigma, {info['batches']} batches",
+                       "l2": "inputs larger than L2"},
+            "candidates": {"power": ncand[0], "interbin": ncand[1]}, "gpu_launches": int(launches),
+            "e2e": {"value": points / wall_s, "unit": "DM-trial*FFT-points/s", "wall_s": wall_s,
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 16 * (ncand[0] + ncand[1]),
+                    "note": "the run() call that performs the search: rows read on the device, candidates copied "
+                            "to the host"},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 WHITENING_WORKLOAD = dict(ndms=512, nbins=(1 << 20) // 2 + 1, seed=41)
 WHITENING_METRIC = "spectrum bins/s whitened (periodicity spectral whitening, reference rules)"
 
@@ -1280,7 +1378,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference" and args.config not in ("survey", "mid", "small", "spd", "whitening"):
+    if args.impl == "reference" and args.config not in ("survey", "mid", "small", "spd", "whitening", "periodicity"):
         # the plain DDTR configurations and the two GPU-only components have
         # a reference arm; print no line that would stand for one
         if rank == 0:
@@ -1299,6 +1397,8 @@ def main():
         return run_spd(args, rank, world, local)
     if args.config == "whitening":
         return run_whitening(args, rank, world, local)
+    if args.config == "periodicity":
+        return run_periodicity(args, rank, world, local)
     cfg = {"survey": SURVEY, "mid": MID, "small": SMALL, "batched": SURVEY, "refine": SURVEY,
            "e2e": SURVEY, "spd": SURVEY, "whitening": SURVEY}[args.config]
     if args.nbits:

@@ -235,6 +235,18 @@ int aa_b200_strategy(const aa_b200_dm *plan, int nranges, float power, int nchan
                      double foff, double tsamp, int nbits, size_t free_memory, int enable_analysis,
                      int max_chunks, float *dmshifts, int *ndms, aa_b200_dm *str_dm, int *maxshift,
                      int *max_ndms, int *num_tchunks, int *t_processed);
+/* The periodicity strategy (include/aa_periodicity_strategy.hpp:178-355)
+ * for the DDTR strategy of a plan (ddtr_memory bytes) and memory_available
+ * bytes, host only: info[0..6] = FFT length of unbinned ranges, samples
+ * copied per row, DM trials of the first batch per unit of binning, input
+ * plane size, cuFFT work area, largest MSD block count, ready flag; per
+ * range (max_ranges) its FFT length and batch count; per batch
+ * (max_batches, ranges in order) range, DM trials, first DM trial, FFT
+ * length, samples copied.  Returns the number of batches, or < 0. */
+int aa_b200_psr_strategy(const aa_b200_dm *plan, int nranges, int nchans, int nsamp, double tsamp, double fch1,
+                         double foff, int nbits, size_t ddtr_memory, size_t memory_available, float sigma_cutoff,
+                         int nHarmonics, int harmonic_sum_algorithm, long long *info, long long *range_info,
+                         int max_ranges, long long *batches, int max_batches);
 
 /* Kernel choice of src/aa_dedisperse.cpp:8-11,20,48-51,62,88-92,101,133:
  * 0 shared 8-bit, 1 shared 16-bit, 2 shared 4-bit, 3 cache ("failsafe"). */

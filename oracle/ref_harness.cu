@@ -372,6 +372,66 @@ int aaref_run_pipeline_spd(const unsigned short *input_tc, int nchans, int nsamp
     return nsteps;
 }
 
+/* aa_periodicity_strategy (include/aa_periodicity_strategy.hpp:178-355) for
+ * the DDTR ranges of a strategy computed as aaref_strategy computes it (no
+ * GPU call): the plan's ten-argument constructor with the given settings and
+ * memory_available bytes.  Outputs: info[0..6] = corrected FFT length,
+ * samples to copy, DM trials per batch in memory, input plane size, cuFFT
+ * work area, largest MSD block count, ready flag; per range (up to
+ * max_ranges) its FFT length and batch count; per batch (up to max_batches,
+ * all ranges in order) range, DM trials, DM shift, samples, samples to copy.
+ * Returns the number of batches, or < 0. */
+int aaref_psr_strategy(const harness_dm *plan, int nranges, int nchans, int nsamp, double tsamp, double fch1,
+                       double foff, int nbits, size_t ddtr_memory, size_t memory_available, float sigma_cutoff,
+                       int nHarmonics, int harmonic_sum_algorithm, long long *info, long long *range_info,
+                       int max_ranges, long long *batches, int max_batches)
+{
+    aa_ddtr_plan p;
+    for (int i = 0; i < nranges; i++)
+        p.add_dm(plan[i].low, plan[i].high, plan[i].step, plan[i].inBin, plan[i].outBin);
+    aa_filterbank_metadata meta(0.0, tsamp, nbits, nsamp, fch1, foff, nchans);
+    aa_device_info dev(0);
+    dev.selected_card_info.available_memory = ddtr_memory;
+    aa_ddtr_strategy s(p, meta, ddtr_memory, false, &dev);
+    if (!s.ready())
+        return -1;
+    aa_periodicity_plan pp(s, sigma_cutoff, true, 3.0f, nHarmonics, harmonic_sum_algorithm, 0, true, true, true);
+    aa_periodicity_strategy per(pp, memory_available);
+    info[6] = per.ready() ? 1 : 0;
+    if (!per.ready())
+        return 0;
+    info[3] = (long long)per.input_plane_size();
+    info[4] = (long long)per.cuFFT_workarea_size();
+    info[5] = (long long)per.max_total_MSD_blocks();
+    int nb = 0;
+    for (int r = 0; r < per.nRanges(); r++) {
+        aa_periodicity_range R = per.get_periodicity_range(r);
+        if (r < max_ranges) {
+            range_info[2 * r] = (long long)R.range.nTimesamples();
+            range_info[2 * r + 1] = (long long)R.batches.size();
+        }
+        for (size_t b = 0; b < R.batches.size(); b++) {
+            if (nb < max_batches) {
+                batches[5 * nb + 0] = r;
+                batches[5 * nb + 1] = (long long)R.batches[b].nDMs_per_batch;
+                batches[5 * nb + 2] = (long long)R.batches[b].DM_shift;
+                batches[5 * nb + 3] = (long long)R.batches[b].nTimesamples;
+                batches[5 * nb + 4] = (long long)R.batches[b].nTimesamples_to_copy;
+                if (r == 0 && b == 0) {
+                    info[0] = (long long)(R.batches[b].nTimesamples * R.range.inBin());
+                    info[1] = (long long)(R.batches[b].nTimesamples_to_copy * R.range.inBin());
+                }
+            }
+            nb++;
+        }
+    }
+    info[2] = per.nRanges() > 0 && !per.get_periodicity_range(0).batches.empty()
+                  ? (long long)per.get_periodicity_range(0).batches[0].nDMs_per_batch /
+                        per.get_periodicity_range(0).range.inBin()
+                  : 0;
+    return nb;
+}
+
 /* The reference runner with dedispersion and periodicity components
  * (include/aa_permitted_pipelines_generic.hpp:570-660, :916-947): the DDTR
  * strategy for free_memory, the periodicity plan's ten-argument constructor

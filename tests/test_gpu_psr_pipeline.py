@@ -38,7 +38,7 @@ def golden():
         return json.load(fh)
 
 
-def run_pipeline(aa, case, x, device_output=False, simple_bind=False, sigma=None):
+def run_pipeline(aa, case, x, device_output=False, simple_bind=False, sigma=None, psr_memory=PC.PSR_MEMORY):
     md = aa.filterbank_metadata_struct(0.0, case["tsamp"], case["fch1"], case["foff"], case["nbits"],
                                        case["nsamp"], case["nchans"], 0.0)
     comps = aa.aa_py_pipeline_components(True, False, True, False)
@@ -48,7 +48,7 @@ def run_pipeline(aa, case, x, device_output=False, simple_bind=False, sigma=None
     pipe.set_options(free_memory=180 * 2**30)
     if device_output:
         pipe.set_device_output(True)
-    pipe.set_periodicity_memory(PC.PSR_MEMORY)
+    pipe.set_periodicity_memory(psr_memory)
     plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in case["plan"]])
     assert pipe.bind_ddtr_plan(plan), pipe.last_error()
     if simple_bind:
@@ -158,3 +158,16 @@ def test_periodicity_from_device_rows_and_reference_binding(aa, cuda_device):
     p2, i2, _, _ = run_pipeline(aa, case, x, simple_bind=True)
     for a, b in ((p0, p1), (i0, i1), (p0, p2), (i0, i2)):
         assert sort_records(a).tobytes() == sort_records(b).tobytes()
+
+
+def test_periodicity_in_batches(aa, cuda_device):
+    """A budget of 300 MB splits each range into batches of 64 DM trials
+    (the strategy the reference computes for it, tests/test_psr_strategy.py):
+    every batch runs (its own MSD), the train is still found and the
+    candidates' DMs come from several batches."""
+    case = PC.PIPELINE_CASES["psr_greedy_peaks"]
+    power, inter, _, info = run_pipeline(aa, case, PC.make_input(case), psr_memory=300 << 20)
+    assert info["batches"] == 6 and info["dms_per_batch"] == 64
+    best = power[np.argmax(power[:, 2])]
+    assert abs(best[0] - case["train"]["dm"]) < 1.0, best
+    assert len(np.unique(np.floor(power[:, 0] / 6.4))) >= 2
