@@ -1287,6 +1287,7 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
 {
     static_assert(NBARS >= SUB_SLOTS, "the barrier area holds one mbarrier per TMA slot");
     constexpr int M2 = 8; // output pairs per lane per DM trial
+    constexpr int NWARPS = NTHREADS / 32;
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int dm0 = g * 64;
@@ -1346,23 +1347,10 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
     };
 
     bool ok = true;
-    // The builds are spread over all 512 threads, one item per (row, group
-    // of words), so that no warp carries a whole row while the others wait at
-    // the stage barrier; item -> (row, column) divides with a float
-    // reciprocal and one correction step.
-    auto split = [](int it, int n, float inv, int &row, int &col) {
-        row = static_cast<int>(static_cast<float>(it) * inv);
-        col = it - row * n;
-        if (col >= n) {
-            ++row;
-            col -= n;
-        } else if (col < 0) {
-            --row;
-            col += n;
-        }
-    };
-
-    // quad-sum rows of stage s into Q buffer qb (waits for the stage's copies)
+    const int NQROW = S.nqrow, NPAT = S.npat, NCH = p.nch_used;
+    // quad-sum rows of stage s into Q buffer qb (waits for the stage's
+    // copies).  One warp per row, everything that depends on the row read
+    // once; the lanes walk the row four samples at a time.
     auto buildA = [&](int s, int qb) {
         const int slot = slot_of(s);
         const unsigned gs = sbase + static_cast<unsigned>(s);
@@ -1373,79 +1361,89 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
         }
         const int *blk = reinterpret_cast<const int *>(&sm[o_blk + slot * SUB_BLK_WORDS]);
         const int q1 = blk[1], q2 = q1 + blk[2], q3 = q2 + blk[3];
-        const int total = min(q3 + blk[4], S.nqrow);
+        const int total = min(q3 + blk[4], NQROW);
         const int n4 = WQ >> 2;
-        const float inv = 1.0f / static_cast<float>(n4);
-        for (int it = tid; it < total * n4; it += NTHREADS) {
-            int r, t4;
-            split(it, n4, inv, r, t4);
+        for (int r = warp; r < total; r += NWARPS) {
             const int i = (r >= q3) ? 3 : (r >= q2) ? 2 : (r >= q1) ? 1 : 0;
             const int base = (i == 3) ? q3 : (i == 2) ? q2 : (i == 1) ? q1 : 0;
             const unsigned pw = static_cast<unsigned>(blk[8 + 8 * i + (r - base)]);
-            const int tau = 4 * t4;
-            uint32_t a[4];
+            int src[4];
+            unsigned shifts = 0u, live = 0u; // byte k: bit shift of channel k; bit k: channel k used
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const int rs = static_cast<int>(sm[o_rsh + slot * 16 + 4 * i + k]);
-                if (rs < 0) {
-                    a[k] = 0u;
-                } else {
-                    const int d = (k == 0) ? 0 : static_cast<int>((pw >> (8 * (k - 1))) & 255u);
-                    const int bb = rs + tau + d;
-                    const int wi = o_raw + (slot * 16 + 4 * i + k) * RAWW + (bb >> 2);
-                    a[k] = __funnelshift_r(sm[wi], sm[wi + 1], 8u * static_cast<unsigned>(bb & 3));
-                }
+                const int d = (k == 0) ? 0 : static_cast<int>((pw >> (8 * (k - 1))) & 255u);
+                live |= (rs >= 0 ? 1u : 0u) << k;
+                const int bb = (rs < 0 ? 0 : rs) + d; // byte offset of sample 0
+                src[k] = o_raw + (slot * 16 + 4 * i + k) * RAWW + (bb >> 2);
+                shifts |= static_cast<unsigned>(8 * (bb & 3)) << (8 * k);
             }
-            // 4x4 byte transpose, then the four channels of each sample summed
-            const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), hi01 = __byte_perm(a[0], a[1], 0x7362);
-            const uint32_t lo23 = __byte_perm(a[2], a[3], 0x5140), hi23 = __byte_perm(a[2], a[3], 0x7362);
-            const uint32_t s0 = __dp4a(__byte_perm(lo01, lo23, 0x5410), 0x01010101u, 0u);
-            const uint32_t s1 = __dp4a(__byte_perm(lo01, lo23, 0x7632), 0x01010101u, 0u);
-            const uint32_t s2 = __dp4a(__byte_perm(hi01, hi23, 0x5410), 0x01010101u, 0u);
-            const uint32_t s3 = __dp4a(__byte_perm(hi01, hi23, 0x7632), 0x01010101u, 0u);
-            uint2 v;
-            v.x = s0 | (s1 << 16);
-            v.y = s2 | (s3 << 16);
-            *reinterpret_cast<uint2 *>(&sm[o_Q + (qb * S.nqrow + r) * HQ + 2 * t4]) = v;
+            uint32_t *qrow = &sm[o_Q + (qb * NQROW + r) * HQ];
+            for (int t4 = lane; t4 < n4; t4 += 32) {
+                uint32_t a[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    a[k] = ((live >> k) & 1u) ? __funnelshift_r(sm[src[k] + t4], sm[src[k] + t4 + 1],
+                                                                (shifts >> (8 * k)) & 31u)
+                                              : 0u;
+                // 4x4 byte transpose, then the four channels of each sample summed
+                const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), hi01 = __byte_perm(a[0], a[1], 0x7362);
+                const uint32_t lo23 = __byte_perm(a[2], a[3], 0x5140), hi23 = __byte_perm(a[2], a[3], 0x7362);
+                const uint32_t s0 = __dp4a(__byte_perm(lo01, lo23, 0x5410), 0x01010101u, 0u);
+                const uint32_t s1 = __dp4a(__byte_perm(lo01, lo23, 0x7632), 0x01010101u, 0u);
+                const uint32_t s2 = __dp4a(__byte_perm(hi01, hi23, 0x5410), 0x01010101u, 0u);
+                const uint32_t s3 = __dp4a(__byte_perm(hi01, hi23, 0x7632), 0x01010101u, 0u);
+                uint2 v;
+                v.x = s0 | (s1 << 16);
+                v.y = s2 | (s3 << 16);
+                *reinterpret_cast<uint2 *>(&qrow[2 * t4]) = v;
+            }
         }
     };
 
-    // partial-sum rows of stage s (from Q buffer qb) into P buffer pb
+    // partial-sum rows of stage s (from Q buffer qb) into P buffer pb.  Work
+    // items are (pattern, part of its row): the parts split each row so that
+    // the patterns fill the warps; the pattern's quad rows, offsets and
+    // their parities are read once per item.
     auto buildB = [&](int s, int qb, int pb) {
         const int slot = slot_of(s);
         const int *blk = reinterpret_cast<const int *>(&sm[o_blk + slot * SUB_BLK_WORDS]);
-        const int npat = min(blk[0], S.npat);
-        const int nq = min(4, (p.nch_used - 16 * s + 3) >> 2);
-        int qbase[4];
-        qbase[0] = 0;
-#pragma unroll
-        for (int i = 1; i < 4; ++i)
-            qbase[i] = qbase[i - 1] + blk[i];
-        const float inv = 1.0f / static_cast<float>(HALF);
-        for (int it = tid; it < npat * HALF; it += NTHREADS) {
-            int pp, k;
-            split(it, HALF, inv, pp, k);
+        const int npat = min(blk[0], NPAT);
+        const int nq = min(4, (NCH - 16 * s + 3) >> 2);
+        const int parts = (npat >= NWARPS) ? 1 : (2 * npat >= NWARPS) ? 2 : (4 * npat >= NWARPS) ? 4 : 8;
+        const int span = (((HALF + parts - 1) / parts) + 31) & ~31; // words per part, whole lane passes
+        for (int item = warp; item < npat * parts; item += NWARPS) {
+            const int pp = item / parts;
+            const int part = item - pp * parts;
             const int key = blk[40 + pp];
-            uint32_t ev = 0u, od = 0u; // (P[2k], P[2k+1]) and (P[2k+1], P[2k+2]) in 16-bit lanes
+            int qrow[4];
+            unsigned odd = 0u; // bit i: quad i's offset is odd
+            int qbase = 0;
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                if (i < nq) {
-                    const int off = (i == 0) ? 0 : blk[56 + 3 * pp + i - 1];
-                    const int u = o_Q + (qb * S.nqrow + qbase[i] + ((key >> (4 * i)) & 15)) * HQ + ((2 * k + off) >> 1);
-                    const uint32_t w0 = sm[u], w1 = sm[u + 1];
-                    const uint32_t mid = __byte_perm(w0, w1, 0x5432); // high half of w0, low half of w1
-                    if (off & 1) {
-                        ev += mid;
-                        od += w1;
-                    } else {
-                        ev += w0;
-                        od += mid;
+                const int off = (i == 0) ? 0 : blk[56 + 3 * pp + i - 1];
+                qrow[i] = o_Q + (qb * NQROW + qbase + ((key >> (4 * i)) & 15)) * HQ + (off >> 1);
+                odd |= static_cast<unsigned>(off & 1) << i;
+                qbase += blk[1 + i];
+            }
+            uint32_t *even = &sm[o_P + pb * PBUF + pp * HALF];
+            uint32_t *oddr = even + NPAT * HALF;
+            const int kend = min(HALF, (part + 1) * span);
+            for (int k = part * span + lane; k < kend; k += 32) {
+                uint32_t ev = 0u, od = 0u; // (P[2k], P[2k+1]) and (P[2k+1], P[2k+2]) in 16-bit lanes
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if (i < nq) {
+                        const uint32_t w0 = sm[qrow[i] + k], w1 = sm[qrow[i] + k + 1];
+                        const uint32_t mid = __byte_perm(w0, w1, 0x5432); // high half of w0, low half of w1
+                        const bool o = (odd >> i) & 1u;
+                        ev += o ? mid : w0;
+                        od += o ? w1 : mid;
                     }
                 }
+                even[k] = ev;
+                oddr[k] = od;
             }
-            const int even = o_P + pb * PBUF + pp * HALF + k;
-            sm[even] = ev;
-            sm[even + S.npat * HALF] = od;
         }
     };
 
