@@ -1379,6 +1379,7 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
                 shifts |= static_cast<unsigned>(8 * (bb & 3)) << (8 * k);
             }
             uint32_t *qrow = &sm[o_Q + (qb * NQROW + r) * HQ];
+#pragma unroll 2
             for (int t4 = lane; t4 < n4; t4 += 32) {
                 uint32_t a[4];
 #pragma unroll
@@ -1429,6 +1430,7 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
             uint32_t *even = &sm[o_P + pb * PBUF + pp * HALF];
             uint32_t *oddr = even + NPAT * HALF;
             const int kend = min(HALF, (part + 1) * span);
+#pragma unroll 2
             for (int k = part * span + lane; k < kend; k += 32) {
                 uint32_t ev = 0u, od = 0u; // (P[2k], P[2k+1]) and (P[2k+1], P[2k+2]) in 16-bit lanes
 #pragma unroll
@@ -1447,26 +1449,45 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
         }
     };
 
-    uint32_t acc[4][2 * M2];
+    // Sums in 16-bit lanes, two outputs per register, flushed every 16
+    // subbands (16 x 16 x 255 < 2^16) into 32-bit totals that live in this
+    // CTA's own output tile (as integers) until the last flush writes the
+    // floats: 32 registers of sums instead of 96, which leaves the builds
+    // room.  The tile is this CTA's alone and stays in L2 between flushes.
     uint32_t a16[4][M2];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-#pragma unroll
-        for (int m = 0; m < 2 * M2; ++m)
-            acc[j][m] = 0u;
+    for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int m = 0; m < M2; ++m)
             a16[j][m] = 0u;
-    }
-    auto flush = [&]() {
+    int nflush = 0;
+    auto flush = [&](bool last) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < 4; ++j) {
+            const int dm = dm0 + 4 * warp + j;
+            float *orow = p.out + static_cast<long long>(dm) * p.out_pitch;
+            int *irow = reinterpret_cast<int *>(orow);
 #pragma unroll
             for (int m = 0; m < M2; ++m) {
-                acc[j][2 * m] += a16[j][m] & 0xFFFFu;
-                acc[j][2 * m + 1] += a16[j][m] >> 16;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const long long t = t0 + 2 * lane + 64 * m + h;
+                    if (dm < p.ndms && t < p.tp) {
+                        int v = static_cast<int>(h ? (a16[j][m] >> 16) : (a16[j][m] & 0xFFFFu));
+                        if (nflush > 0)
+                            v += irow[t];
+                        if (last) {
+                            const float f = static_cast<float>(v);
+                            orow[t] = p.divide_by_bin ? (f / p.nchans_f / p.bin_f) : (f / p.nchans_f);
+                        } else {
+                            irow[t] = v;
+                        }
+                    }
+                }
                 a16[j][m] = 0u;
             }
+        }
+        ++nflush;
     };
 
     // prologue: copies for the first SUB_SLOTS stages, quad rows of 0 and 1, sums of 0
@@ -1513,33 +1534,17 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
                 for (int m = 0; m < M2; ++m)
                     a16[j][m] += w[m];
             }
-            if ((s & 15) == 15)
-                flush();
+            if ((s & 15) == 15 && s + 1 < nstages)
+                flush(false);
         }
         fence_proxy_async();
         __syncthreads();
         issue(s + SUB_SLOTS);
     }
-    flush();
     stage_ctr = sbase + static_cast<unsigned>(nstages);
     if (!ok)
         return false;
-
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int dm = dm0 + 4 * warp + j;
-        if (dm >= p.ndms)
-            continue;
-        float *orow = p.out + static_cast<long long>(dm) * p.out_pitch;
-#pragma unroll
-        for (int m = 0; m < 2 * M2; ++m) {
-            const long long t = t0 + 2 * lane + 64 * (m >> 1) + (m & 1);
-            if (t < p.tp) {
-                const float v = static_cast<float>(static_cast<int>(acc[j][m]));
-                orow[t] = p.divide_by_bin ? (v / p.nchans_f / p.bin_f) : (v / p.nchans_f);
-            }
-        }
-    }
+    flush(true);
     return true;
 }
 
