@@ -706,10 +706,12 @@ int aa_b200_spd_write_candidates(const char *dir, int candidate_algorithm, float
                                  const float *snr, const unsigned *bw, size_t n);
 
 /* ---------------------------------------------------------------------------
- * Periodicity building blocks (the reference's periodicity component,
- * src/aa_device_periods.cu:368-541, is not built yet; these are two of its
- * stages, bit-identical to the reference's kernels).  Device pointers;
- * return 0 or 1 (message in aa_b200_psr_last_error).
+ * Periodicity building blocks: the stages of the reference's periodicity
+ * search (src/aa_device_periods.cu:368-541) one at a time, each
+ * bit-identical to the reference's kernel where the reference is
+ * deterministic; the pipeline's periodicity component
+ * (aa_py_pipeline_api_bind_periodicity_plan) runs them in the reference's
+ * order.  Device pointers; return 0 or 1 (message in aa_b200_psr_last_error).
  *
  * power_interbin (src/aa_device_power.cu:34-52): d_spectra holds nDMs
  * spectra of nTimesamples/2+1 complex float bins (cufftExecR2C output);
