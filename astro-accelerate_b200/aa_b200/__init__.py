@@ -169,12 +169,17 @@ def lib():
         "aa_b200_sigproc_header": ([vp, P(sigproc_header_struct)], b),
         "aa_b200_sigproc_last_error": ([vp], ctypes.c_char_p),
         "aa_b200_pipeline_run_all": ([vp], b),
+        "aa_b200_pipeline_setup": ([vp], b),
         "aa_b200_pipeline_rewind": ([vp], b),
         "aa_b200_pipeline_synchronize": ([vp], b),
         "aa_b200_pipeline_device_output": ([vp, i], vp),
         "aa_b200_pipeline_range_info": ([vp, i, P(i), P(i), P(i), P(i)], i),
         "aa_b200_pipeline_kernel_launches": ([vp], ll),
         "aa_b200_pipeline_stage_depth": ([vp, i], i),
+        "aa_b200_tuned_ranges": ([i], ll),
+        "aa_b200_tuned_ranges_save": ([ctypes.c_char_p], ll),
+        "aa_b200_tuned_ranges_load": ([ctypes.c_char_p], ll),
+        "aa_b200_tuned_ranges_last_error": ([], ctypes.c_char_p),
         "aa_b200_pipeline_range_kernel": ([vp, i, P(i), P(i), P(i), P(i)], i),
         "aa_b200_pipeline_last_error": ([vp], ctypes.c_char_p),
         "aa_b200_pipeline_num_tchunks": ([vp], i),
@@ -190,6 +195,8 @@ def lib():
         "aa_b200_batch_device_output": ([vp, i, i], vp),
         "aa_b200_batch_range_shape": ([vp, i, i, P(i), P(ll), P(i)], i),
         "aa_b200_batch_info": ([vp, P(ll), P(i), P(i), P(i), P(sz), P(sz), P(ll)], i),
+        "aa_b200_batch_set_kernel_choice": ([vp, i], b),
+        "aa_b200_batch_sub_jobs": ([vp], i),
         "aa_b200_batch_last_ms": ([vp, i], d),
         "aa_b200_batch_estimate_bytes": ([filterbank_metadata_struct, vp, sz, P(sz)], i),
         "aa_b200_batch_last_error": ([vp], ctypes.c_char_p),
@@ -657,6 +664,11 @@ class aa_py_pipeline:
     def run_all(self):
         return bool(lib().aa_b200_pipeline_run_all(self.m_obj))
 
+    def setup(self):
+        """Device buffers, tables and the autotuner now rather than at the
+        first run."""
+        return bool(lib().aa_b200_pipeline_setup(self.m_obj))
+
     def rewind(self):
         return bool(lib().aa_b200_pipeline_rewind(self.m_obj))
 
@@ -939,6 +951,15 @@ class batch:
             raise RuntimeError(self.last_error())
         return True
 
+    def set_kernel_choice(self, choice: int):
+        """One-byte ranges both bodies can run (before setup): 0 the faster
+        on a timed slice, 1 channel-quad, 2 subband."""
+        return self._check(lib().aa_b200_batch_set_kernel_choice(self.m_obj, int(choice)))
+
+    def sub_jobs(self) -> int:
+        """Persistent jobs the subband body runs (after setup)."""
+        return int(lib().aa_b200_batch_sub_jobs(self.m_obj))
+
     def setup(self):
         return self._check(lib().aa_b200_batch_setup(self.m_obj))
 
@@ -1113,6 +1134,29 @@ def spd_plan(nt: int, tsamp: float, inBin: int, max_boxcar_width_in_sec: float) 
 
 def spd_kernel_launches() -> int:
     return lib().aa_b200_spd_kernel_launches()
+
+
+def tuned_ranges(clear: bool = False) -> int:
+    """Autotuner choices kept in this process (one per distinct range shape;
+    a later pipeline of the same shape reuses them); clear drops them first."""
+    return int(lib().aa_b200_tuned_ranges(1 if clear else 0))
+
+
+def save_tuned_ranges(path: str) -> int:
+    """Write the kept autotuner choices to a text file; returns the entries."""
+    n = lib().aa_b200_tuned_ranges_save(os.fsencode(path))
+    if n < 0:
+        raise OSError(lib().aa_b200_tuned_ranges_last_error().decode())
+    return int(n)
+
+
+def load_tuned_ranges(path: str) -> int:
+    """Add the choices of a file written by save_tuned_ranges; returns the
+    entries read."""
+    n = lib().aa_b200_tuned_ranges_load(os.fsencode(path))
+    if n < 0:
+        raise OSError(lib().aa_b200_tuned_ranges_last_error().decode())
+    return int(n)
 
 
 def write_candidates(directory: str, candidate_algorithm: int, tstart: float, dm_low: float, dm_high: float,

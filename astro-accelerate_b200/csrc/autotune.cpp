@@ -3,8 +3,128 @@
 #include "autotune.hpp"
 
 #include <algorithm>
+#include <cstdio>
+#include <mutex>
 
 namespace aab200 {
+
+namespace {
+std::mutex g_tuned_mu;
+std::map<std::vector<long long>, TunedRange> g_tuned;
+} // namespace
+
+bool tuned_range_find(const std::vector<long long> &key, TunedRange &out)
+{
+    std::lock_guard<std::mutex> lock(g_tuned_mu);
+    auto it = g_tuned.find(key);
+    if (it == g_tuned.end())
+        return false;
+    out = it->second;
+    return true;
+}
+
+void tuned_range_keep(const std::vector<long long> &key, const TunedRange &t)
+{
+    std::lock_guard<std::mutex> lock(g_tuned_mu);
+    g_tuned[key] = t;
+}
+
+size_t tuned_range_entries(bool clear)
+{
+    std::lock_guard<std::mutex> lock(g_tuned_mu);
+    if (clear)
+        g_tuned.clear();
+    return g_tuned.size();
+}
+
+namespace {
+const char *const kTunedHeader = "aa_b200 tuned ranges 1";
+constexpr int kTunedValues = 10; // variant, M, W, raww, qs, npool, nq_pad, smem_bytes, flavour, f32 cs
+} // namespace
+
+// Line format: <key length> <key...> <the ten values>, decimal.
+long long tuned_ranges_save(const std::string &path, std::string &err)
+{
+    std::lock_guard<std::mutex> lock(g_tuned_mu);
+    FILE *f = std::fopen(path.c_str(), "w");
+    if (!f) {
+        err = "cannot open " + path + " for writing";
+        return -1;
+    }
+    std::fprintf(f, "%s\n", kTunedHeader);
+    for (const auto &kv : g_tuned) {
+        std::fprintf(f, "%zu", kv.first.size());
+        for (long long v : kv.first)
+            std::fprintf(f, " %lld", v);
+        const TunedRange &t = kv.second;
+        std::fprintf(f, " %d %d %d %d %d %d %d %zu %d %d\n", t.variant, t.quad.M, t.quad.W, t.quad.raww, t.quad.qs,
+                     t.quad.npool, t.quad.nq_pad, t.quad.smem_bytes, t.quad_flavour, t.f32_cs);
+    }
+    const bool ok = std::fclose(f) == 0;
+    if (!ok) {
+        err = "cannot write " + path;
+        return -1;
+    }
+    return static_cast<long long>(g_tuned.size());
+}
+
+long long tuned_ranges_load(const std::string &path, std::string &err)
+{
+    FILE *f = std::fopen(path.c_str(), "r");
+    if (!f) {
+        err = "cannot open " + path;
+        return -1;
+    }
+    char head[64] = {0};
+    if (!std::fgets(head, sizeof head, f) || std::string(head) != std::string(kTunedHeader) + "\n") {
+        std::fclose(f);
+        err = path + " is not a tuned-range file";
+        return -1;
+    }
+    std::map<std::vector<long long>, TunedRange> got;
+    long long n = 0;
+    size_t klen = 0;
+    for (;;) {
+        const int r = std::fscanf(f, "%zu", &klen);
+        if (r == EOF)
+            break;
+        if (r != 1 || klen == 0 || klen > (1u << 20)) {
+            std::fclose(f);
+            err = path + ": malformed entry " + std::to_string(n + 1);
+            return -1;
+        }
+        std::vector<long long> key(klen);
+        bool ok = true;
+        for (size_t i = 0; i < klen && ok; ++i)
+            ok = std::fscanf(f, "%lld", &key[i]) == 1;
+        long long v[kTunedValues];
+        for (int i = 0; i < kTunedValues && ok; ++i)
+            ok = std::fscanf(f, "%lld", &v[i]) == 1;
+        if (!ok) {
+            std::fclose(f);
+            err = path + ": malformed entry " + std::to_string(n + 1);
+            return -1;
+        }
+        TunedRange t;
+        t.variant = static_cast<int>(v[0]);
+        t.quad.M = static_cast<int>(v[1]);
+        t.quad.W = static_cast<int>(v[2]);
+        t.quad.raww = static_cast<int>(v[3]);
+        t.quad.qs = static_cast<int>(v[4]);
+        t.quad.npool = static_cast<int>(v[5]);
+        t.quad.nq_pad = static_cast<int>(v[6]);
+        t.quad.smem_bytes = static_cast<size_t>(v[7]);
+        t.quad_flavour = static_cast<int>(v[8]);
+        t.f32_cs = static_cast<int>(v[9]);
+        got[key] = t;
+        ++n;
+    }
+    std::fclose(f);
+    std::lock_guard<std::mutex> lock(g_tuned_mu);
+    for (auto &kv : got)
+        g_tuned[kv.first] = kv.second;
+    return n;
+}
 
 bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache &cache, std::string &err)
 {

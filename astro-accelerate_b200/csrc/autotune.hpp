@@ -21,6 +21,7 @@
 #include <map>
 #include <string>
 #include <tuple>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -40,5 +41,30 @@ bool tune_stage_depth(DdtrJob &job, cudaStream_t st, int device, StageTuneCache 
 // receives the slice's samples.  Negative on a launch error (message in err).
 float time_job_slice(const DdtrJob &job, cudaStream_t st, int device, std::string &err, long long samples = 0,
                      long long *timed_samples = nullptr);
+
+// What the plain pipeline's autotuner chose for a range: the kernel variant,
+// the channel-quad geometry (tile shape, stage depth) and flavour, and the
+// fp32 kernel's stage depth.  The choices are kept for the life of the
+// process under a key of everything the slice timings depend on (device,
+// channel delays, the range, its delay-table summary, chunk length, row
+// pitch and the kernel options), so that a later pipeline of the same shape
+// -- the next beam or file of a survey -- takes them without timing again.
+// No choice changes the output: every kernel gives the same bits.
+struct TunedRange {
+    int variant = 0;
+    QuadGeometry quad{};
+    int quad_flavour = -1;
+    int f32_cs = 0;
+};
+bool tuned_range_find(const std::vector<long long> &key, TunedRange &out);
+void tuned_range_keep(const std::vector<long long> &key, const TunedRange &t);
+// Entries held; clear empties the store first.
+size_t tuned_range_entries(bool clear);
+// The store as a text file (one entry per line), and back: a tuning run's
+// choices reused by later processes (a profiling run, a production run).
+// Loading adds to the entries held.  Return the entries written or read, -1
+// if the file cannot be opened or a line is malformed (err says which).
+long long tuned_ranges_save(const std::string &path, std::string &err);
+long long tuned_ranges_load(const std::string &path, std::string &err);
 
 } // namespace aab200

@@ -129,6 +129,45 @@ bool BatchDdtr::tune_job(DdtrJob &job)
     return true;
 }
 
+// The subband body against the tuned channel-quad body, timed on the same
+// output samples of the job (about four tiles per SM) with the one-launch
+// kernels, which run the same bodies; kept per job shape.  A subband job
+// whose shared memory does not fit beside the job descriptor stays quad.
+bool BatchDdtr::prefer_sub(const DdtrJob &quad, const DdtrJob &sub, bool &use)
+{
+    use = false;
+    BatchJobDev d{};
+    d.p = sub.p;
+    d.s = sub.s;
+    d.variant = 4;
+    if (persistent_job_smem(d) > 227 * 1024)
+        return true;
+    if (kernel_choice_ == 2) {
+        use = true;
+        return true;
+    }
+    const std::vector<long long> key = {quad.p.nch_used, quad.p.ndms, quad.p.kind, quad.p.span, quad.p.stride,
+                                        quad.q.W, quad.q.raww, quad.q.qs, quad.q.npool, quad.q.maxpat,
+                                        quad.q.flavour, sub.s.nsub, sub.s.W, sub.s.wq, sub.s.raww, sub.s.npat,
+                                        sub.s.nqrow, std::min<long long>(quad.p.tp, 1LL << 20)};
+    auto it = sub_choice_.find(key);
+    if (it != sub_choice_.end()) {
+        use = it->second;
+        return true;
+    }
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
+    const long long samples = 512LL * std::max(1, (4 * nsm + quad.groups - 1) / std::max(1, quad.groups));
+    std::string err;
+    const float tq = time_job_slice(quad, st_, device_, err, samples);
+    const float ts = (tq < 0.f) ? -1.f : time_job_slice(sub, st_, device_, err, samples);
+    if (tq < 0.f || ts < 0.f)
+        return fail(err);
+    use = ts < tq;
+    sub_choice_[key] = use;
+    return true;
+}
+
 bool BatchDdtr::build_jobs()
 {
     struct Staged {
@@ -137,7 +176,11 @@ bool BatchDdtr::build_jobs()
         int order;
     };
     std::vector<Staged> staged;
-    std::map<std::pair<int, int>, std::pair<int, int>> tuned; // (beam, range) -> (qs or cs, npool)
+    struct Tuned {
+        int depth, npool; // qs or cs, and the channel-quad row pool
+        bool sub;         // the subband body runs the range
+    };
+    std::map<std::pair<int, int>, Tuned> tuned; // (beam, range)
     for (size_t bi = 0; bi < beams_.size(); ++bi) {
         Beam &b = beams_[bi];
         DdtrPipeline &P = *b.pipe;
@@ -183,52 +226,85 @@ bool BatchDdtr::build_jobs()
                     job.q = d.q;
                     job.f = d.f;
                 }
-                tuned[key] = std::make_pair(quadlike ? job.q.qs : job.f.cs, job.q.npool);
+                bool sub = false;
+                if (job.variant == 2 && P.range_has_sub(op.range) &&
+                    ((opt_.autotune && kernel_choice_ == 0) || kernel_choice_ == 2)) {
+                    DdtrJob js;
+                    if (!P.make_job(op, b.level_ptr[op.chunk][op.src_level], b.level_elems[op.chunk][op.src_level],
+                                    out, P.strategy().total_samps(op.range), js, 4))
+                        return fail("beam " + std::to_string(bi) + ": " + P.last_error());
+                    if (!prefer_sub(job, js, sub))
+                        return false;
+                }
+                it = tuned.emplace(key, Tuned{quadlike ? job.q.qs : job.f.cs, job.q.npool, sub}).first;
             } else {
                 if (quadlike) {
-                    job.q.qs = it->second.first;
-                    job.q.npool = it->second.second;
+                    job.q.qs = it->second.depth;
+                    job.q.npool = it->second.npool;
                 } else {
-                    job.f.cs = it->second.first;
+                    job.f.cs = it->second.depth;
                 }
             }
+            if (it->second.sub &&
+                !P.make_job(op, b.level_ptr[op.chunk][op.src_level], b.level_elems[op.chunk][op.src_level], out,
+                            P.strategy().total_samps(op.range), job, 4))
+                return fail("beam " + std::to_string(bi) + ": " + P.last_error());
             // relative cost of one work item: channels summed, fp32 sums ~3x
             const double cost = static_cast<double>(job.p.nch_used) * (job.variant == 3 ? 3.0 : 1.0);
             staged.push_back({job, cost, static_cast<int>(staged.size())});
         }
     }
     std::stable_sort(staged.begin(), staged.end(), [](const Staged &a, const Staged &b) { return a.cost > b.cost; });
+    // the subband jobs run in a launch of their own, after the others
+    std::stable_partition(staged.begin(), staged.end(), [](const Staged &a) { return a.job.variant != 4; });
     pjobs_.clear();
+    plaunch_.clear();
     total_items_ = 0;
     smem_ = 0;
-    split_phase_ = false;
+    grid_ = 0;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
     for (const Staged &s : staged) {
+        const bool sub = (s.job.variant == 4);
+        if (plaunch_.empty() || (sub && plaunch_.back().set != PSET_SUB)) {
+            PLaunch L;
+            L.first = static_cast<int>(pjobs_.size());
+            L.set = sub ? PSET_SUB : PSET_QUAD;
+            plaunch_.push_back(L);
+        }
+        PLaunch &L = plaunch_.back();
         BatchJobDev d{};
         d.p = s.job.p;
         d.q = s.job.q;
         d.f = s.job.f;
+        d.s = s.job.s;
         d.variant = s.job.variant;
         d.groups = s.job.groups;
-        d.item0 = total_items_;
-        total_items_ += static_cast<long long>(s.job.groups) * s.job.tiles;
-        smem_ = std::max(smem_, persistent_job_smem(d));
-        split_phase_ = split_phase_ || d.variant == 6;
+        d.item0 = L.items;
+        L.items += static_cast<long long>(s.job.groups) * s.job.tiles;
+        L.smem = std::max(L.smem, persistent_job_smem(d));
+        if (d.variant == 6)
+            L.set = PSET_SP;
+        ++L.njobs;
         pjobs_.push_back(d);
     }
-    if (!pjobs_.empty()) {
-        if (smem_ > 227 * 1024)
+    for (PLaunch &L : plaunch_) {
+        if (L.smem > 227 * 1024)
             return fail("persistent kernel shared memory above the per-CTA limit");
-        const int per_sm = persistent_blocks_per_sm(smem_, split_phase_);
+        const int per_sm = persistent_blocks_per_sm(L.smem, L.set);
         if (per_sm < 1)
             return fail("the persistent kernel does not fit an SM");
-        int nsm = 148;
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
-        grid_ = static_cast<int>(std::min<long long>(static_cast<long long>(nsm) * per_sm, total_items_));
+        L.grid = static_cast<int>(std::min<long long>(static_cast<long long>(nsm) * per_sm, L.items));
+        total_items_ += L.items;
+        smem_ = std::max(smem_, L.smem);
+        grid_ = std::max(grid_, L.grid);
+    }
+    if (!pjobs_.empty()) {
         if (!check_cuda(cudaMalloc(&d_jobs_, pjobs_.size() * sizeof(BatchJobDev)), "cudaMalloc(jobs)") ||
             !check_cuda(cudaMemcpyAsync(d_jobs_, pjobs_.data(), pjobs_.size() * sizeof(BatchJobDev),
                                         cudaMemcpyHostToDevice, st_),
                         "H2D jobs") ||
-            !check_cuda(cudaMalloc(&d_counter_, sizeof(unsigned long long)), "cudaMalloc(counter)"))
+            !check_cuda(cudaMalloc(&d_counter_, plaunch_.size() * sizeof(unsigned long long)), "cudaMalloc(counter)"))
             return false;
     }
     return true;
@@ -274,10 +350,13 @@ bool BatchDdtr::issue_work(cudaStream_t st)
             return false;
     if (!check_cuda(cudaEventRecord(ev_dd0_, st), "event"))
         return false;
-    if (!pjobs_.empty()) {
-        if (!check_cuda(cudaMemsetAsync(d_counter_, 0, sizeof(unsigned long long), st), "memset") ||
-            !check_cuda(launch_ddtr_persistent(d_jobs_, static_cast<int>(pjobs_.size()), total_items_, d_counter_, smem_,
-                                               grid_, split_phase_, st),
+    if (!plaunch_.empty() &&
+        !check_cuda(cudaMemsetAsync(d_counter_, 0, plaunch_.size() * sizeof(unsigned long long), st), "memset"))
+        return false;
+    for (size_t i = 0; i < plaunch_.size(); ++i) {
+        const PLaunch &L = plaunch_[i];
+        if (!check_cuda(launch_ddtr_persistent(d_jobs_ + L.first, L.njobs, L.items, d_counter_ + i, L.smem, L.grid,
+                                               L.set, st),
                         "persistent dedispersion"))
             return false;
         ++launches;

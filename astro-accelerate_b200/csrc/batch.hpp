@@ -68,6 +68,21 @@ public:
     size_t level_bytes() const { return level_bytes_; }
     long long work_items() const { return total_items_; }
     int persistent_jobs() const { return static_cast<int>(pjobs_.size()); }
+    int sub_jobs() const
+    {
+        int n = 0;
+        for (const PLaunch &L : plaunch_)
+            n += (L.set == PSET_SUB) ? L.njobs : 0;
+        return n;
+    }
+    // 0 timed, 1 channel-quad, 2 subband (before setup)
+    bool set_kernel_choice(int choice)
+    {
+        if (setup_done_ || choice < 0 || choice > 2)
+            return fail("kernel choice must be 0, 1 or 2, before setup");
+        kernel_choice_ = choice;
+        return true;
+    }
     int other_jobs() const { return static_cast<int>(ojobs_.size()); }
     int grid() const { return grid_; }
     size_t smem_bytes() const { return smem_; }
@@ -100,6 +115,7 @@ private:
     bool build_levels(Beam &b);
     bool build_jobs();
     bool tune_job(DdtrJob &job);
+    bool prefer_sub(const DdtrJob &quad, const DdtrJob &sub, bool &use);
     bool issue_work(cudaStream_t st);
 
     BatchOptions opt_;
@@ -115,12 +131,24 @@ private:
     cudaEvent_t ev_run0_ = nullptr, ev_run1_ = nullptr, ev_dd0_ = nullptr, ev_dd1_ = nullptr;
     std::vector<BatchJobDev> pjobs_;
     std::vector<DdtrJob> ojobs_;
+    // Persistent launches, one per body set: the channel-quad and fp32 jobs
+    // (with the split-phase body when a job needs it), then the subband jobs.
+    // pjobs_ holds the jobs of every launch, launch by launch, each launch's
+    // items numbered from 0 and its jobs heaviest first.
+    struct PLaunch {
+        int first = 0, njobs = 0; // the launch's jobs in pjobs_
+        long long items = 0;
+        size_t smem = 0;
+        int grid = 0;
+        int set = PSET_QUAD;
+    };
+    std::vector<PLaunch> plaunch_;
+    int kernel_choice_ = 0;
     BatchJobDev *d_jobs_ = nullptr;
-    unsigned long long *d_counter_ = nullptr;
+    unsigned long long *d_counter_ = nullptr; // one work counter per launch
     long long total_items_ = 0;
-    size_t smem_ = 0;
-    int grid_ = 0;
-    bool split_phase_ = false; // a split-phase job among the persistent ones
+    size_t smem_ = 0; // the largest of the launches'
+    int grid_ = 0;    // the largest of the launches'
     size_t level_bytes_ = 0;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;
@@ -128,6 +156,7 @@ private:
     long long launches_per_run_ = 0;
     bool ran_ = false;
     StageTuneCache tune_cache_;
+    std::map<std::vector<long long>, bool> sub_choice_; // subband body chosen, by job shape
 };
 
 } // namespace aab200

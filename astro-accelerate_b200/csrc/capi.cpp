@@ -10,6 +10,7 @@
 
 #include <cuda_runtime.h>
 
+#include "autotune.hpp"
 #include "ddtr_kernels.cuh"
 #include "spd.cuh"
 #include "export.hpp"
@@ -1110,6 +1111,14 @@ bool aa_b200_pipeline_run_all(void *obj)
     return true;
 }
 
+bool aa_b200_pipeline_setup(void *obj)
+{
+    Api *a = as_api(obj);
+    if (!a->pipe)
+        return api_fail(a, "no DDTR plan bound");
+    return a->pipe->setup() ? true : api_fail(a, a->pipe->last_error());
+}
+
 bool aa_b200_pipeline_rewind(void *obj)
 {
     Api *a = as_api(obj);
@@ -1216,6 +1225,34 @@ int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms,
     }
     return 0;
 }
+
+long long aa_b200_tuned_ranges(int clear) { return static_cast<long long>(aab200::tuned_range_entries(clear != 0)); }
+
+namespace {
+thread_local std::string g_tuned_error;
+} // namespace
+
+long long aa_b200_tuned_ranges_save(const char *path)
+{
+    g_tuned_error.clear();
+    if (!path) {
+        g_tuned_error = "null path";
+        return -1;
+    }
+    return aab200::tuned_ranges_save(path, g_tuned_error);
+}
+
+long long aa_b200_tuned_ranges_load(const char *path)
+{
+    g_tuned_error.clear();
+    if (!path) {
+        g_tuned_error = "null path";
+        return -1;
+    }
+    return aab200::tuned_ranges_load(path, g_tuned_error);
+}
+
+const char *aa_b200_tuned_ranges_last_error(void) { return g_tuned_error.c_str(); }
 
 int aa_b200_pipeline_stage_depth(void *obj, int range)
 {

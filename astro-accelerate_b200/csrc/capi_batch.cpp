@@ -101,6 +101,18 @@ int aa_b200_batch_range_shape(void *batch, int beam, int range, int *ndms, long 
     return 0;
 }
 
+bool aa_b200_batch_set_kernel_choice(void *batch, int choice)
+{
+    BatchDdtr *b = as_batch(batch);
+    return b && b->set_kernel_choice(choice);
+}
+
+int aa_b200_batch_sub_jobs(void *batch)
+{
+    BatchDdtr *b = as_batch(batch);
+    return b ? b->sub_jobs() : 0;
+}
+
 int aa_b200_batch_info(void *batch, long long *work_items, int *persistent_jobs, int *other_jobs, int *grid,
                        size_t *smem_bytes, size_t *level_bytes, long long *launches_per_run)
 {

@@ -32,13 +32,16 @@ constexpr int QDMW = 4;    // DM trials per warp
 constexpr int NTHREADS = 512;
 
 // The caller-owned barrier area: RING_BARS one-arrival mbarriers for the TMA
-// rings of the quad, fp32 and subband bodies (phases carried by stage_ctr),
-// then the split-phase quad body's own barriers (phases carried by its own
-// counter): SP_QN TMA barriers, SP_NB "rows built" and SP_NB "rows consumed"
-// barriers with one arrival per warp.  Rounded up to 16 bytes: the body area
-// behind it holds TMA destinations and 16-byte vector accesses.
-constexpr int RING_BARS = 8;
-static_assert(RING_BARS >= QNSTAGE && RING_BARS >= SUB_SLOTS, "one ring barrier per TMA slot");
+// rings -- QNSTAGE for the quad and fp32 bodies (phases carried by one
+// counter), then SUB_SLOTS for the subband body (phases carried by its own
+// counter: the two rings have different depths, so a persistent CTA that
+// runs both keeps their phases apart) -- then the split-phase quad body's
+// own barriers (phases carried by a third counter): SP_QN TMA barriers,
+// SP_NB "rows built" and SP_NB "rows consumed" barriers with one arrival per
+// warp.  Rounded up to 16 bytes: the body area behind it holds TMA
+// destinations and 16-byte vector accesses.
+constexpr int SUB_BAR0 = QNSTAGE; // first ring barrier of the subband body
+constexpr int RING_BARS = QNSTAGE + SUB_SLOTS;
 constexpr int SP_QN = 4;      // TMA ring depth of the split-phase quad body
 constexpr int SP_NB = 3;      // pattern-row buffers of the split-phase quad body
 constexpr int SP_WARPS = 16;  // warps of the split-phase quad body (arrivals per phase)
@@ -1285,7 +1288,7 @@ __host__ __device__ inline size_t sub_body_words(int raww, int nsub_pad, int nqr
 __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S, int g, long long t0, uint32_t *sm,
                                          unsigned bar0, unsigned &stage_ctr)
 {
-    static_assert(NBARS >= SUB_SLOTS, "the barrier area holds one mbarrier per TMA slot");
+    static_assert(RING_BARS >= SUB_BAR0 + SUB_SLOTS, "the barrier area holds one mbarrier per TMA slot");
     constexpr int M2 = 8; // output pairs per lane per DM trial
     constexpr int NWARPS = NTHREADS / 32;
     const int tid = threadIdx.x;
@@ -1320,7 +1323,7 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
         const int slot = slot_of(s);
         const int c0 = 16 * s;
         const int nrows = max(0, min(16, p.nch_used - c0));
-        const unsigned bar = bar0 + 8 * slot;
+        const unsigned bar = bar0 + 8 * (SUB_BAR0 + slot);
         fence_proxy_async();
         if (lane == 0)
             mbar_expect_tx(bar, static_cast<unsigned>(nrows * RAWW * 4 + 64 * 4 + SUB_BLK_WORDS * 4));
@@ -1349,12 +1352,13 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
     bool ok = true;
     const int NQROW = S.nqrow, NPAT = S.npat, NCH = p.nch_used;
     // quad-sum rows of stage s into Q buffer qb (waits for the stage's
-    // copies).  One warp per row, everything that depends on the row read
-    // once; the lanes walk the row four samples at a time.
-    auto buildA = [&](int s, int qb) {
+    // copies).  Work items are (row, part of the row): one warp per item,
+    // everything that depends on the row read once; the lanes walk the part
+    // four samples at a time.  Returns the number of items.
+    auto buildA = [&](int s, int qb) -> int {
         const int slot = slot_of(s);
         const unsigned gs = sbase + static_cast<unsigned>(s);
-        if (!mbar_wait_bounded(bar0 + 8 * slot, (gs / SUB_SLOTS) & 1u)) {
+        if (!mbar_wait_bounded(bar0 + 8 * (SUB_BAR0 + slot), (gs / SUB_SLOTS) & 1u)) {
             if (ok)
                 atomicOr(p.err, DERR_TIMEOUT);
             ok = false;
@@ -1363,7 +1367,11 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
         const int q1 = blk[1], q2 = q1 + blk[2], q3 = q2 + blk[3];
         const int total = min(q3 + blk[4], NQROW);
         const int n4 = WQ >> 2;
-        for (int r = warp; r < total; r += NWARPS) {
+        const int parts = (total >= NWARPS) ? 1 : (2 * total >= NWARPS) ? 2 : 4;
+        const int span4 = (((n4 + parts - 1) / parts) + 31) & ~31; // words per part, whole lane passes
+        for (int item = warp; item < total * parts; item += NWARPS) {
+            const int r = item / parts;
+            const int part = item - r * parts;
             const int i = (r >= q3) ? 3 : (r >= q2) ? 2 : (r >= q1) ? 1 : 0;
             const int base = (i == 3) ? q3 : (i == 2) ? q2 : (i == 1) ? q1 : 0;
             const unsigned pw = static_cast<unsigned>(blk[8 + 8 * i + (r - base)]);
@@ -1379,8 +1387,9 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
                 shifts |= static_cast<unsigned>(8 * (bb & 3)) << (8 * k);
             }
             uint32_t *qrow = &sm[o_Q + (qb * NQROW + r) * HQ];
+            const int t4end = min(n4, (part + 1) * span4);
 #pragma unroll 2
-            for (int t4 = lane; t4 < n4; t4 += 32) {
+            for (int t4 = part * span4 + lane; t4 < t4end; t4 += 32) {
                 uint32_t a[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k)
@@ -1400,20 +1409,23 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
                 *reinterpret_cast<uint2 *>(&qrow[2 * t4]) = v;
             }
         }
+        return total * parts;
     };
 
     // partial-sum rows of stage s (from Q buffer qb) into P buffer pb.  Work
     // items are (pattern, part of its row): the parts split each row so that
     // the patterns fill the warps; the pattern's quad rows, offsets and
-    // their parities are read once per item.
-    auto buildB = [&](int s, int qb, int pb) {
+    // their parities are read once per item.  The items continue the warp
+    // rotation of the nA quad-row items built in the same iteration, so the
+    // warps those left short start here.
+    auto buildB = [&](int s, int qb, int pb, int nA) {
         const int slot = slot_of(s);
         const int *blk = reinterpret_cast<const int *>(&sm[o_blk + slot * SUB_BLK_WORDS]);
         const int npat = min(blk[0], NPAT);
         const int nq = min(4, (NCH - 16 * s + 3) >> 2);
         const int parts = (npat >= NWARPS) ? 1 : (2 * npat >= NWARPS) ? 2 : (4 * npat >= NWARPS) ? 4 : 8;
         const int span = (((HALF + parts - 1) / parts) + 31) & ~31; // words per part, whole lane passes
-        for (int item = warp; item < npat * parts; item += NWARPS) {
+        for (int item = (warp - nA % NWARPS + NWARPS) % NWARPS; item < npat * parts; item += NWARPS) {
             const int pp = item / parts;
             const int part = item - pp * parts;
             const int key = blk[40 + pp];
@@ -1454,6 +1466,9 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
     // CTA's own output tile (as integers) until the last flush writes the
     // floats: 32 registers of sums instead of 96, which leaves the builds
     // room.  The tile is this CTA's alone and stays in L2 between flushes.
+    // The first flush stores, the middle ones add in L2 without a return
+    // value (nothing waits for them; a thread's accesses to one address keep
+    // their program order), and only the last reads the totals back.
     uint32_t a16[4][M2];
 #pragma unroll
     for (int j = 0; j < 4; ++j)
@@ -1474,11 +1489,13 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
                     const long long t = t0 + 2 * lane + 64 * m + h;
                     if (dm < p.ndms && t < p.tp) {
                         int v = static_cast<int>(h ? (a16[j][m] >> 16) : (a16[j][m] & 0xFFFFu));
-                        if (nflush > 0)
-                            v += irow[t];
                         if (last) {
+                            if (nflush > 0)
+                                v += irow[t];
                             const float f = static_cast<float>(v);
                             orow[t] = p.divide_by_bin ? (f / p.nchans_f / p.bin_f) : (f / p.nchans_f);
+                        } else if (nflush > 0) {
+                            atomicAdd(&irow[t], v);
                         } else {
                             irow[t] = v;
                         }
@@ -1499,18 +1516,18 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
         buildA(0, 0);
     fence_proxy_async();
     __syncthreads();
-    if (nstages > 1)
-        buildA(1, 1);
-    if (nstages > 0)
-        buildB(0, 0, 0);
+    {
+        const int nA = (nstages > 1) ? buildA(1, 1) : 0;
+        if (nstages > 0)
+            buildB(0, 0, 0, nA);
+    }
     fence_proxy_async();
     __syncthreads();
 
     for (int s = 0; s < nstages; ++s) {
-        if (s + 2 < nstages)
-            buildA(s + 2, s & 1);
+        const int nA = (s + 2 < nstages) ? buildA(s + 2, s & 1) : 0;
         if (s + 1 < nstages)
-            buildB(s + 1, (s + 1) & 1, (s + 1) & 1);
+            buildB(s + 1, (s + 1) & 1, (s + 1) & 1, nA);
         if (ok) {
             const int slot = slot_of(s);
             const int4 e4 = *reinterpret_cast<const int4 *>(&sm[o_ent + slot * 64 + 4 * warp]);

@@ -203,20 +203,25 @@ struct BatchJobDev {
     DdtrLaunch p;
     QuadLaunch q;
     F32Launch f;
-    int variant; // 2 channel-quad, 3 staged fp32, 6 split-phase channel-quad
+    SubLaunch s;
+    int variant; // 2 channel-quad, 3 staged fp32, 4 subband, 6 split-phase channel-quad
     int groups;
     long long item0;
 };
 
+// Body sets of the persistent kernel's instances: the channel-quad and fp32
+// bodies (jobs of variants 2 and 3), those and the split-phase quad body
+// (variant 6 too), the subband body alone (variant 4).
+enum PersistentSet : int { PSET_QUAD = 0, PSET_SP = 1, PSET_SUB = 2 };
+
 // Dynamic shared memory of one job in the persistent kernel.
 size_t persistent_job_smem(const BatchJobDev &j);
-// CTAs of the persistent kernel that fit one SM at this dynamic shared memory
-// (split_phase: the instance that runs split-phase jobs too).
-int persistent_blocks_per_sm(size_t smem_bytes, bool split_phase);
-// counter: device work counter, zero before the launch; split_phase must be
-// true when any job is of variant 6.
+// CTAs of the persistent kernel instance that fit one SM at this dynamic
+// shared memory.
+int persistent_blocks_per_sm(size_t smem_bytes, int set);
+// counter: device work counter, zero before the launch; every job must have
+// a body in the instance's set.
 cudaError_t launch_ddtr_persistent(const BatchJobDev *jobs, int njobs, long long total_items,
-                                   unsigned long long *counter, size_t smem_bytes, int grid, bool split_phase,
-                                   cudaStream_t st);
+                                   unsigned long long *counter, size_t smem_bytes, int grid, int set, cudaStream_t st);
 
 } // namespace aab200

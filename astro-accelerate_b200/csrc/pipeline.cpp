@@ -651,9 +651,46 @@ bool DdtrPipeline::setup()
     return true;
 }
 
+// Key of a range's tuned choices: every input of the slice timings -- the
+// device, the channel delays, the range and its DM trials, the summary of its
+// delay and pattern tables, the geometry before tuning, chunk 0's length, the
+// row pitch and the kernel options.
+std::vector<long long> DdtrPipeline::tune_key(int r, const DdtrOp &op, long long pitch) const
+{
+    const RangeConfig &rc = ranges_[r];
+    const DmRange &d = strategy_.dm(r);
+    auto fb = [](float v) {
+        uint32_t u;
+        std::memcpy(&u, &v, sizeof u);
+        return static_cast<long long>(u);
+    };
+    auto db = [](double v) {
+        long long u;
+        std::memcpy(&u, &v, sizeof u);
+        return u;
+    };
+    std::vector<long long> k = {device_, meta_.nchans, meta_.nbits, db(meta_.tsamp), db(meta_.fch1),
+                                db(meta_.foff), fb(d.low), fb(d.high), fb(d.step), d.inBin, strategy_.ndms(r),
+                                op.tp, op.i_nsamp, pitch, opt_.kernel_variant, opt_.tile_words, opt_.fma_mode,
+                                opt_.device_output ? 1 : 0, rc.kind, rc.elem_bytes, rc.group_dms, rc.tile_words,
+                                rc.span, rc.delay_max, rc.nch_used, fb(rc.mstartdm), fb(rc.mdmstep), fb(rc.tsamp),
+                                rc.variant, rc.quad.M, rc.quad.W, rc.quad.raww, rc.quad.qs, rc.quad.npool,
+                                rc.quad.nq_pad, rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.nquads,
+                                rc.has_sub ? 1 : 0, rc.has_quad ? 1 : 0, rc.quad_ws_ok ? 1 : 0,
+                                rc.quad_pairs ? 1 : 0, rc.quad_flavour, rc.d_qtmp ? 1 : 0, rc.f32.cs, rc.f32.W,
+                                rc.f32.rawh, rc.sub.W, rc.sub.wq, rc.sub.raww, rc.sub.npat, rc.sub.nqrow,
+                                rc.nsub};
+    for (int j = 0; j < 4; ++j)
+        k.push_back(rc.quad_npool_qs[j]);
+    for (float v : strategy_.dmshifts())
+        k.push_back(fb(v));
+    return k;
+}
+
 // Stage depth of every range that runs a staged kernel, timed on chunk 0's
 // job (the buffers hold zeros at this point; the kernels' work does not
-// depend on the sample values).
+// depend on the sample values).  A range whose key was tuned before in this
+// process takes the kept choices instead.
 bool DdtrPipeline::tune_ranges()
 {
     StageTuneCache cache;
@@ -671,6 +708,28 @@ bool DdtrPipeline::tune_ranges()
             continue;
         float *out = opt_.device_output ? d_out_full_[r] + op->out_off : d_tile_[0];
         const long long pitch = opt_.device_output ? strategy_.total_samps(static_cast<int>(r)) : op->tp;
+        const std::vector<long long> key = tune_key(static_cast<int>(r), *op, pitch);
+        TunedRange kept;
+        if (tuned_range_find(key, kept)) {
+            if (rc.d_qtmp) {
+                // the offset table for the kept tile's row pitch
+                if (kept.quad.W != rc.quad.W) {
+                    const size_t nq_ent = static_cast<size_t>(rc.nquads) * strategy_.ndms(r);
+                    if (!check_cuda(launch_quad_offsets(rc.d_qtmp, nq_ent, kept.quad.W, rc.d_qoff, st_, 0),
+                                    "quad offsets") ||
+                        !check_cuda(cudaStreamSynchronize(st_), "sync"))
+                        return false;
+                    ++launches_;
+                }
+                cudaFree(rc.d_qtmp);
+                rc.d_qtmp = nullptr;
+            }
+            rc.variant = kept.variant;
+            rc.quad = kept.quad;
+            rc.quad_flavour = kept.quad_flavour;
+            rc.f32.cs = kept.f32_cs;
+            continue;
+        }
         DdtrJob job;
         if (!make_job(*op, d_flat_[op->src_level & 1], flat_elems_, out, pitch, job))
             return false;
@@ -728,6 +787,12 @@ bool DdtrPipeline::tune_ranges()
             if (t_sub < t_quad)
                 rc.variant = 4;
         }
+        TunedRange t;
+        t.variant = rc.variant;
+        t.quad = rc.quad;
+        t.quad_flavour = rc.quad_flavour;
+        t.f32_cs = rc.f32.cs;
+        tuned_range_keep(key, t);
     }
     return check_cuda(cudaStreamSynchronize(st_), "sync");
 }
@@ -912,20 +977,26 @@ int DdtrPipeline::quad_flavour_of(const RangeConfig &rc) const
 }
 
 bool DdtrPipeline::make_job(const DdtrOp &op, const void *in, size_t in_elems, float *out, long long out_pitch,
-                            DdtrJob &job)
+                            DdtrJob &job, int as_variant)
 {
     const int r = op.range;
     const RangeConfig &rc = ranges_[r];
     const DmRange &d = strategy_.dm(r);
     const int tp = op.tp;
     const long long i_nsamp = op.i_nsamp;
+    int v = rc.variant;
+    if (as_variant != 0) {
+        if (!((as_variant == 4 && rc.has_sub) || (as_variant == 2 && rc.has_quad)))
+            return fail("range " + std::to_string(r) + " has no tables for kernel variant " + std::to_string(as_variant));
+        v = as_variant;
+    }
     job = DdtrJob();
-    job.variant = (elem_bytes_ == 1 && rc.variant == 2)   ? 2
-                  : (elem_bytes_ == 2 && rc.variant == 3) ? 3
-                  : (elem_bytes_ == 1 && rc.variant == 4) ? 4
-                  : (elem_bytes_ == 1 && rc.variant == 5) ? 5
-                  : (elem_bytes_ == 1 && rc.variant == 6) ? 6
-                                                          : 1;
+    job.variant = (elem_bytes_ == 1 && v == 2)   ? 2
+                  : (elem_bytes_ == 2 && v == 3) ? 3
+                  : (elem_bytes_ == 1 && v == 4) ? 4
+                  : (elem_bytes_ == 1 && v == 5) ? 5
+                  : (elem_bytes_ == 1 && v == 6) ? 6
+                                                 : 1;
     job.elem_bytes = elem_bytes_;
     job.tile_words = rc.tile_words;
     job.offtab = rc.d_offtab;

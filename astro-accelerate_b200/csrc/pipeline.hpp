@@ -193,7 +193,11 @@ public:
     int *device_flags() const { return d_err_; }
     // The launch of a DDTR op reading level buffer `in` (in_elems elements)
     // and writing rows of `out` with pitch out_pitch.
-    bool make_job(const DdtrOp &op, const void *in, size_t in_elems, float *out, long long out_pitch, DdtrJob &job);
+    // as_variant 2 or 4: the job with the channel-quad or subband kernel
+    // instead of the range's own (the range must have that kernel's tables)
+    bool make_job(const DdtrOp &op, const void *in, size_t in_elems, float *out, long long out_pitch, DdtrJob &job,
+                  int as_variant = 0);
+    bool range_has_sub(int r) const { return ranges_[r].has_sub; }
     bool check_flags() { return check_device_flags(); }
     long long kernel_launches() const { return launches_; }
     // Device time (ms) and launch count of one kernel family since the last
@@ -231,6 +235,7 @@ private:
     bool tune_quad_shape(int r, const DdtrOp &op, float *out, long long pitch, StageTuneCache &cache, DdtrJob &job);
     bool build_sub_tables(int r);
     bool tune_ranges();
+    std::vector<long long> tune_key(int r, const DdtrOp &op, long long pitch) const;
     bool step(bool allow_sync);
     bool enumerate_ops();
     bool exec_corner_turn(const DdtrOp &op);

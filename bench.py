@@ -80,6 +80,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the timed output")
     ap.add_argument("--no-autotune", action="store_true", help="no per-range kernel timing at set-up")
+    ap.add_argument("--tune-file", default="",
+                    help="autotuner choices: read from this file if it exists (those ranges are not timed again) "
+                         "and written to it after the warm-up (a profiling run reuses a plain run's choices)")
     ap.add_argument("--multibeam-beams", type=int, default=8,
                     help="beams of the reduced multi-beam draw timed batched vs plain in the default line (0: off)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -681,7 +684,9 @@ def run_e2e(args, rank, world, local):
     boxcar candidates, the 64 strongest events per beam cut to 1024-sample
     per-channel snippets, 50 Adam steps on DM through the adjoint kernels.
     The same search runs after the plain per-beam pipeline; wall times
-    exclude data generation; every DDTR output is compared bit for bit."""
+    exclude data generation; set-up (buffers, tables, autotuner: the batch's
+    setup(), the plain pipeline's explicit setup()) is reported apart in
+    *_with_setup_s; every DDTR output is compared bit for bit."""
     import numpy as np
     import torch
     import aa_b200 as aa
@@ -709,6 +714,7 @@ def run_e2e(args, rank, world, local):
     T = dict(b_ddtr=0.0, b_setup=0.0, b_search=0.0, b_refine=0.0, p_ddtr=0.0, p_setup=0.0, p_search=0.0,
              p_refine=0.0)
     errs_b, errs_p, bit_exact, n_found, n_injected, n_cand = [], [], True, 0, 0, 0
+    warmed = False
 
     def sync_time(t0):
         torch.cuda.synchronize(device)
@@ -728,6 +734,17 @@ def run_e2e(args, rank, world, local):
         B.run()
         B.synchronize()
         T["b_ddtr"] += sync_time(t0)
+        if not warmed:
+            # one untimed pass of the search and refinement (first-use set-up
+            # of their kernels and of torch's allocator), so that neither arm
+            # carries it
+            i0 = w[0]
+            outs = [(B.output(0, r), B.range_shape(0, r)[1]) for r in range(len(beams[i0]["plan"]))]
+            top, snip, base = _search_and_refine(aa, SR, R, xs[i0], kc, outs, strats[i0])
+            if snip is not None:
+                R.refine_dm(snip, top["dm"], kc, steps=2, lr=0.05, base=base)
+            torch.cuda.synchronize(device)
+            warmed = True
         t0 = time.perf_counter()
         per_beam = []
         for j, i in enumerate(w):
@@ -759,7 +776,7 @@ def run_e2e(args, rank, world, local):
             pipe = aa.create_pipeline(mds[i], xs[i].data_ptr(), device_input=True, device_output=True,
                                       copy_to_host=False)
             pipe.set_options(free_memory=MULTIBEAM_FREE_MEMORY)
-            if not pipe.bind_ddtr_plan(plans[i]):
+            if not (pipe.bind_ddtr_plan(plans[i]) and pipe.setup()):
                 raise RuntimeError(pipe.last_error())
             T["p_setup"] += sync_time(t0)
             t0 = time.perf_counter()
@@ -1432,6 +1449,8 @@ def main():
     smem = aa.smem_load_rate(8192, stream.cuda_stream)
 
     # ---------------- device-resident value ----------------
+    if args.tune_file and os.path.exists(args.tune_file):
+        aa.load_tuned_ranges(args.tune_file)
     pipe = aa.create_pipeline(md, x.data_ptr(), device_input=True, device_output=True, copy_to_host=False,
                               stream=stream.cuda_stream, card_number=local)
     pipe.set_options(tile_words=args.tile_words, group_dms=args.group_dms)
@@ -1447,6 +1466,8 @@ def main():
     for _ in range(args.warmup):
         if not (pipe.run_all() and pipe.synchronize() and pipe.rewind()):
             raise RuntimeError(pipe.last_error())
+    if args.tune_file and rank == 0:
+        aa.save_tuned_ranges(args.tune_file)
     pipe.time_kernels(True)
     pipe.reset_kernel_times()
     launches0 = aa.lib().aa_b200_pipeline_kernel_launches(pipe.m_obj)

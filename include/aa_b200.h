@@ -495,6 +495,10 @@ void *aa_b200_pipeline_create(aa_py_filterbank_metadata_struct metadata, const u
                               int device_input, int device_output, int copy_to_host, void *stream,
                               int card_number);
 bool aa_b200_pipeline_run_all(void *obj);
+/* The pipeline's set-up (device buffers, delay and pattern tables, the
+ * autotuner) now instead of at the first run, so that it can happen before
+ * the data arrives.  Idempotent; needs a bound DDTR plan. */
+bool aa_b200_pipeline_setup(void *obj);
 bool aa_b200_pipeline_rewind(void *obj);
 bool aa_b200_pipeline_synchronize(void *obj);
 float *aa_b200_pipeline_device_output(void *obj, int range);
@@ -507,6 +511,20 @@ int aa_b200_pipeline_range_info(void *obj, int range, int *kind, int *group_dms,
  * shared-memory stage of a range, as the autotuner chose it; 0 for the
  * generic kernels */
 int aa_b200_pipeline_stage_depth(void *obj, int range);
+/* The autotuner's choices (kernel, tile shape, stage depth, flavour) are
+ * kept for the life of the process, one entry per distinct range shape (the
+ * device, channel delays, DM range, chunk length, row pitch and kernel
+ * options): a later pipeline of the same shape takes them without timing
+ * again.  No choice changes the output.  clear != 0 drops every entry first.
+ * Returns the entries held; host only. */
+long long aa_b200_tuned_ranges(int clear);
+/* The kept choices written to a text file, and read back into this process
+ * (added to the entries held): a tuning run's choices reused by later
+ * processes on the same device.  Return the entries written or read, or -1
+ * (message in aa_b200_tuned_ranges_last_error).  Host only. */
+long long aa_b200_tuned_ranges_save(const char *path);
+long long aa_b200_tuned_ranges_load(const char *path);
+const char *aa_b200_tuned_ranges_last_error(void);
 /* The kernel shape a range runs (after set-up, which includes the
  * autotuner): the channel-quad flavour (-1 for other kernels; 0 with the
  * per-byte path, 1 with its warp switch, 4 loading every DM trial's word
@@ -540,7 +558,10 @@ bool aa_b200_pipeline_reset_kernel_times(void *obj);
  * turns and binning of all beams on parallel streams, then one persistent
  * dedispersion kernel over all (beam, chunk, range, DM group, time tile) work
  * items (persistent = 0: one launch per (beam, chunk, range) instead).
- * autotune != 0 times the shared-memory stage depth per range shape at setup.
+ * autotune != 0 times the shared-memory stage depth per range shape at setup,
+ * and, for one-byte ranges that both kernels can run, the subband body
+ * against the channel-quad body; the subband jobs run in a second
+ * persistent launch right after the first.
  * Each beam's output [range][dm][t] is bit-identical to a plain pipeline's
  * (aa_b200_pipeline_create with device_output) for the same free_memory.
  * run is asynchronous on `stream` (a cudaStream_t as void*, 0 = a stream of
@@ -551,6 +572,13 @@ void *aa_b200_batch_create(int stride_mode, int fma_mode, size_t free_memory, in
 /* returns the beam index, or -1 (message in aa_b200_batch_last_error) */
 int aa_b200_batch_add_beam(void *batch, aa_py_filterbank_metadata_struct metadata, void *ddtr_plan,
                            const unsigned short *d_input);
+/* Before setup: which body runs the one-byte ranges that both can run:
+ * 0 the faster on a timed slice (with autotune; else channel-quad), 1 the
+ * channel-quad body, 2 the subband body.  Returns false for another value
+ * or after setup. */
+bool aa_b200_batch_set_kernel_choice(void *batch, int choice);
+/* After setup: persistent jobs run by the subband body. */
+int aa_b200_batch_sub_jobs(void *batch);
 bool aa_b200_batch_setup(void *batch);
 bool aa_b200_batch_run(void *batch);
 bool aa_b200_batch_synchronize(void *batch);

@@ -88,6 +88,49 @@ def test_strategy_refusal_codes(aa):
         aa.strategy([], 4096, 1 << 20, 1670.0, -0.0732421875, 64e-6, 8)
 
 
+def test_tuned_range_store_is_host_only(aa):
+    """The autotuner's kept choices can be counted and dropped without a GPU."""
+    assert aa.tuned_ranges(clear=True) == 0
+    assert aa.tuned_ranges() == 0
+
+
+def test_tuned_range_file_roundtrip(aa, tmp_path):
+    """The autotuner's kept choices go to a text file and back (host only):
+    an entry read from a file is written out unchanged; a file that is not
+    one, or a malformed entry, is refused."""
+    aa.tuned_ranges(clear=True)
+    line = "3 0 4096 8 2 16 1072 1096 4 37 1028 120304 7 0"
+    src = tmp_path / "in.txt"
+    src.write_text("aa_b200 tuned ranges 1\n" + line + "\n")
+    assert aa.load_tuned_ranges(str(src)) == 1
+    assert aa.tuned_ranges() == 1
+    out = tmp_path / "out.txt"
+    assert aa.save_tuned_ranges(str(out)) == 1
+    assert out.read_text().splitlines() == ["aa_b200 tuned ranges 1", line]
+    bad = tmp_path / "bad.txt"
+    bad.write_text("something else\n")
+    with pytest.raises(OSError, match="not a tuned-range file"):
+        aa.load_tuned_ranges(str(bad))
+    bad.write_text("aa_b200 tuned ranges 1\n3 0 1\n")
+    with pytest.raises(OSError, match="malformed"):
+        aa.load_tuned_ranges(str(bad))
+    with pytest.raises(OSError, match="cannot open"):
+        aa.load_tuned_ranges(str(tmp_path / "missing.txt"))
+    assert aa.tuned_ranges(clear=True) == 0
+
+
+def test_batch_kernel_choice_is_checked(aa):
+    """The batch's kernel choice takes 0, 1 or 2 before setup (host only)."""
+    b = aa.batch()
+    try:
+        with pytest.raises(RuntimeError, match="kernel choice"):
+            b.set_kernel_choice(3)
+        assert b.set_kernel_choice(2) and b.set_kernel_choice(0)
+        assert b.sub_jobs() == 0
+    finally:
+        b.delete()
+
+
 def test_failure_injection_counter(aa):
     """aa_b200_debug_fail_after arms a host-side countdown (no GPU needed to set it)."""
     L = aa.lib()

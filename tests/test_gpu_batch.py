@@ -60,7 +60,7 @@ def beams(aa, cuda_device):
     return data
 
 
-def run_batch(aa, beams, **opts):
+def run_batch(aa, beams, kernel_choice=None, **opts):
     b = aa.batch(free_memory=FREE_MEMORY, **opts)
     plans = []
     try:
@@ -68,6 +68,8 @@ def run_batch(aa, beams, **opts):
             plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in case["plan"]])
             plans.append(plan)
             b.add_beam(md_of(aa, case), plan, d_x)
+        if kernel_choice is not None:
+            b.set_kernel_choice(kernel_choice)
         b.setup()
         results = []
         for _ in range(2):
@@ -75,19 +77,14 @@ def run_batch(aa, beams, **opts):
             b.synchronize()
             results.append([[b.output(i, r).cpu().numpy() for r in range(len(case["plan"]))]
                             for i, (_, case, _, _, _) in enumerate(beams)])
-        return results, b.info()
+        return results, {**b.info(), "sub_jobs": b.sub_jobs()}
     finally:
         b.delete()
         for p in plans:
             p.delete()
 
 
-@pytest.mark.parametrize("persistent,use_graph,autotune", [(True, True, True), (True, False, False),
-                                                           (False, True, True), (False, False, False)])
-def test_batch_matches_plain_pipeline(aa, beams, persistent, use_graph, autotune):
-    results, info = run_batch(aa, beams, persistent=persistent, use_graph=use_graph, autotune=autotune)
-    if persistent:
-        assert info["persistent_jobs"] > 0 and info["work_items"] > 0
+def assert_matches_plain(beams, results):
     for rep, res in enumerate(results):
         for bi, (name, case, _, want, _) in enumerate(beams):
             for r, w in enumerate(want):
@@ -96,6 +93,29 @@ def test_batch_matches_plain_pipeline(aa, beams, persistent, use_graph, autotune
                 bad = np.flatnonzero(g.view(np.uint32) != w.view(np.uint32))
                 assert bad.size == 0, (f"run {rep}, beam {name}, range {r}: {bad.size} outputs differ from the "
                                        f"plain pipeline, first at {np.unravel_index(bad[0], g.shape)}")
+
+
+@pytest.mark.parametrize("persistent,use_graph,autotune", [(True, True, True), (True, False, False),
+                                                           (False, True, True), (False, False, False)])
+def test_batch_matches_plain_pipeline(aa, beams, persistent, use_graph, autotune):
+    results, info = run_batch(aa, beams, persistent=persistent, use_graph=use_graph, autotune=autotune)
+    if persistent:
+        assert info["persistent_jobs"] > 0 and info["work_items"] > 0
+    assert_matches_plain(beams, results)
+
+
+@pytest.mark.parametrize("choice", [1, 2])
+def test_batch_kernel_choice_matches_plain_pipeline(aa, beams, choice):
+    """The channel-quad (1) or the subband (2) body forced on the one-byte
+    ranges both can run: the subband jobs run in a persistent launch of their
+    own after the others, and every beam stays bit-identical to its plain
+    run, on the first run and on the graph's replay."""
+    results, info = run_batch(aa, beams, persistent=True, use_graph=True, autotune=True, kernel_choice=choice)
+    if choice == 2:
+        assert 0 < info["sub_jobs"] < info["persistent_jobs"]
+    else:
+        assert info["sub_jobs"] == 0
+    assert_matches_plain(beams, results)
 
 
 def test_batch_one_persistent_launch(aa, beams):

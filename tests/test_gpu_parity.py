@@ -26,7 +26,7 @@ pytestmark = pytest.mark.gpu
 LIGHT = [n for n, c in C.CASES.items() if not c.get("heavy")]
 
 
-def run_pipeline(aa, case, x, stride_mode=0, variant=0, **opts):
+def run_pipeline(aa, case, x, stride_mode=0, variant=0, explicit_setup=False, **opts):
     md = aa.filterbank_metadata_struct(0.0, case["tsamp"], case["fch1"], case["foff"], case["nbits"],
                                        case["nsamp"], case["nchans"], 0.0)
     comps = aa.aa_py_pipeline_components(True, False, False, False)
@@ -37,6 +37,8 @@ def run_pipeline(aa, case, x, stride_mode=0, variant=0, **opts):
     pipe.set_kernel_variant(variant)
     plan = aa.aa_py_ddtr_plan([aa.aa_py_dm(*p) for p in case["plan"]])
     assert pipe.bind_ddtr_plan(plan), pipe.last_error()
+    if explicit_setup:
+        assert pipe.setup() and pipe.setup(), pipe.last_error()
     steps = 0
     while pipe.run():
         steps += 1
@@ -174,6 +176,32 @@ def test_autotuned_tile_shape_matches_oracle(aa, oracle_mod, cuda_device, name):
         else:
             assert i["flavour"] == -1, i
     assert_matches_oracle(case, s, got, want, kern)
+
+
+@pytest.mark.parametrize("name", ["shared8_binned", "shared16"])
+def test_tuned_choices_kept_for_the_next_pipeline(aa, oracle_mod, cuda_device, tmp_path, name):
+    """The autotuner's choices are kept per range shape: after a round trip
+    through a file, a second pipeline of the same shape (set up explicitly,
+    twice: set-up is idempotent) adds no entry, runs the same kernel shapes
+    and gives the same bits as the first and as the oracle."""
+    case = C.CASES[name]
+    x = C.make_input(case)
+    aa.tuned_ranges(clear=True)
+    first, info1, _, _ = run_pipeline(aa, case, x, variant=0)
+    kept = aa.tuned_ranges()
+    assert kept >= 1
+    # through a file, as another process would take them
+    path = str(tmp_path / "tuned.txt")
+    assert aa.save_tuned_ranges(path) == kept
+    aa.tuned_ranges(clear=True)
+    assert aa.load_tuned_ranges(path) == kept
+    second, info2, _, _ = run_pipeline(aa, case, x, variant=0, explicit_setup=True)
+    assert aa.tuned_ranges() == kept
+    assert info2 == info1
+    for a, b in zip(first, second):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    s, want, kern = oracle_run(oracle_mod, case, x)
+    assert_matches_oracle(case, s, second, want, kern)
 
 
 WS_CASES = [n for n in LIGHT if C.CASES[n]["nbits"] <= 8]
