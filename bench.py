@@ -56,13 +56,16 @@ SMALL = dict(nchans=1024, nbits=8, fch1=1550.0, foff=-0.390625, tsamp=64e-6, nsa
              plan=[(0, 500, 0.5, 1, 1)], npulses=1, seed=1)
 METRIC = "DM-trial*samples/s (plain DDTR, 1 beam per GPU, bit-exact)"
 METRIC_UNCHECKED = "DM-trial*samples/s (plain DDTR, 1 beam per GPU)"
-# DRAM bytes per algorithmic byte of the dedispersion kernel, from one ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum of one launch); the
-# roofline's traffic is this ratio times a launch's algorithmic bytes
-TRAFFIC_PER_ALG_BYTE = 2.31 / 2.46
-TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_ddtr_quad launch (range 0, 4096 ch x "
-                  "2^18 samples: 0.96 + 1.35 GB against 2.46 GB algorithmic), scaled by the algorithmic bytes of "
-                  "an average launch of this workload; profiles/k_ddtr_quad_mid_8bit_4096ch_2e18_range0.md")
+# DRAM bytes per algorithmic byte of each one-byte dedispersion kernel, from
+# one ncu capture each (dram__bytes_read.sum + dram__bytes_write.sum of the
+# range-0 launch of the 4096 ch x 2^18 plan, 2.46 GB algorithmic); the
+# roofline's traffic is each range's ratio times its algorithmic bytes,
+# averaged per launch
+TRAFFIC_PER_ALG_BYTE = {"k_ddtr_quad": (0.96 + 1.35) / 2.46, "k_ddtr_sub": (0.958 + 1.512) / 2.46}
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one range-0 launch of 4096 ch x 2^18 samples "
+                  "per kernel (k_ddtr_quad 0.96 + 1.35 GB, k_ddtr_sub 0.96 + 1.51 GB, against 2.46 GB algorithmic), "
+                  "scaled by the algorithmic bytes of each range of this workload; "
+                  "profiles/k_ddtr_quad_mid_8bit_4096ch_2e18_range0.md, profiles/k_ddtr_sub_mid_8bit_4096ch_2e18_range0.md")
 PUBLISHED_REALTIME = 6.28  # reference wiki, 8-range "b2" plan, unnamed GPU
 
 
@@ -1572,12 +1575,19 @@ def main():
     # ---------------- roofline of the dominant kernel ----------------
     dd_ms, dd_n = kern["dedisperse"]
     nch = cfg["nchans"]
-    alg_bytes = alg_adds = 0
+    kernel_names = {"quad": "k_ddtr_quad", "phase": "k_ddtr_u8", "f32": "k_ddtr_f32", "gather": "k_ddtr_u16",
+                    "sub": "k_ddtr_sub", "quadws": "k_ddtr_quadws", "quadsp": "k_ddtr_quadsp"}
+    alg_bytes = alg_adds = traffic = 0
+    traffic_known = True
     for r in range(len(cfg["plan"])):
+        ratio = TRAFFIC_PER_ALG_BYTE.get(kernel_names[ranges[r]["kernel"]])
+        traffic_known = traffic_known and ratio is not None
         for k in range(strat["num_tchunks"]):
             tp = strat["t_processed"][r][k]
             ms_r = strat["maxshift"] // cfg["plan"][r][3]
-            alg_bytes += nch * (tp + ms_r) * (1 if cfg["nbits"] <= 8 else 2) + strat["ndms"][r] * tp * 4
+            b = nch * (tp + ms_r) * (1 if cfg["nbits"] <= 8 else 2) + strat["ndms"][r] * tp * 4
+            alg_bytes += b
+            traffic += (ratio or 0.0) * b
             alg_adds += strat["ndms"][r] * tp * nch
     launches_per_step = len(cfg["plan"]) * strat["num_tchunks"]
     dd_s_per_step = dd_ms / 1e3 / (dd_n / launches_per_step)
@@ -1589,20 +1599,19 @@ def main():
     except OSError:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
-    kernel_names = {"quad": "k_ddtr_quad", "phase": "k_ddtr_u8", "f32": "k_ddtr_f32", "gather": "k_ddtr_u16",
-                    "sub": "k_ddtr_sub", "quadws": "k_ddtr_quadws", "quadsp": "k_ddtr_quadsp"}
     used = sorted({kernel_names[ri["kernel"]] for ri in ranges})
     hbm_achieved = alg_bytes / dd_s_per_step / 1e9
     roofline = {
         "bound": "shared-memory", "kernel": "+".join(used), "unit": "adds/s",
         "achieved": adds_rate, "peak": smem["adds_per_s"], "frac": adds_rate / smem["adds_per_s"],
-        "traffic": TRAFFIC_PER_ALG_BYTE * alg_bytes / launches_per_step,
+        "traffic": traffic / launches_per_step if traffic_known else None,
         "algorithmic": {"adds_per_launch": alg_adds / launches_per_step,
                         "bytes_per_launch": alg_bytes / launches_per_step,
                         "per_unit": f"{nch} channel adds and, per step, the packed input once per (chunk, range) "
                                     f"plus 4 B per output"},
         "peak_source": f"measured on this GPU by aa_b200_smem_load_rate: {smem['loads_per_s']:.4g} 32-bit shared "
-                       f"loads/s x 4 adds per load (the channel-quad kernel's bound)",
+                       f"loads/s x 4 adds per load (the bound of the direct channel-quad sum; the subband kernel "
+                       f"loads less per add and is issue-bound)",
         "traffic_source": TRAFFIC_SOURCE,
         "hbm": {"achieved": hbm_achieved, "peak": hbm, "unit": "GB/s", "frac": hbm_achieved / hbm,
                 "peak_source": "MEASURED_PEAKS.json (measured)" if "hbm_gbs" in peaks else "fallback"},
