@@ -1351,112 +1351,130 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
 
     bool ok = true;
     const int NQROW = S.nqrow, NPAT = S.npat, NCH = p.nch_used;
-    // quad-sum rows of stage s into Q buffer qb (waits for the stage's
-    // copies).  Work items are (row, part of the row): one warp per item,
-    // everything that depends on the row read once; the lanes walk the part
-    // four samples at a time.  Returns the number of items.
-    auto buildA = [&](int s, int qb) -> int {
-        const int slot = slot_of(s);
-        const unsigned gs = sbase + static_cast<unsigned>(s);
-        if (!mbar_wait_bounded(bar0 + 8 * (SUB_BAR0 + slot), (gs / SUB_SLOTS) & 1u)) {
-            if (ok)
-                atomicOr(p.err, DERR_TIMEOUT);
-            ok = false;
-        }
-        const int *blk = reinterpret_cast<const int *>(&sm[o_blk + slot * SUB_BLK_WORDS]);
-        const int q1 = blk[1], q2 = q1 + blk[2], q3 = q2 + blk[3];
-        const int total = min(q3 + blk[4], NQROW);
+    // The row builds of one iteration as one list of work units split evenly
+    // over the warps.  A unit is one pass of a warp's 32 lanes along a row:
+    // 128 samples of a quad-sum row of stage sa (into Q buffer qa: the four
+    // channels of each sample summed with IDP4A, as 16-bit pairs), or 64
+    // samples of a pattern row of stage sb (from Q buffer qb into P buffer
+    // pb: four quad-sum pairs added in 16-bit lanes, in an even- and an
+    // odd-phase copy).  Each warp takes a contiguous range of units, so it
+    // reads a row's tables (skews and byte shifts, or quad rows, offsets and
+    // their parities) only when its range enters that row: one to three
+    // times per iteration.  sa or sb < 0: no such stage.  Waits for stage
+    // sa's copies.
+    auto build = [&](int sa, int qa, int sb, int qb, int pb) {
         const int n4 = WQ >> 2;
-        const int parts = (total >= NWARPS) ? 1 : (2 * total >= NWARPS) ? 2 : 4;
-        const int span4 = (((n4 + parts - 1) / parts) + 31) & ~31; // words per part, whole lane passes
-        for (int item = warp; item < total * parts; item += NWARPS) {
-            const int r = item / parts;
-            const int part = item - r * parts;
-            const int i = (r >= q3) ? 3 : (r >= q2) ? 2 : (r >= q1) ? 1 : 0;
-            const int base = (i == 3) ? q3 : (i == 2) ? q2 : (i == 1) ? q1 : 0;
-            const unsigned pw = static_cast<unsigned>(blk[8 + 8 * i + (r - base)]);
-            int src[4];
-            unsigned shifts = 0u, live = 0u; // byte k: bit shift of channel k; bit k: channel k used
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int rs = static_cast<int>(sm[o_rsh + slot * 16 + 4 * i + k]);
-                const int d = (k == 0) ? 0 : static_cast<int>((pw >> (8 * (k - 1))) & 255u);
-                live |= (rs >= 0 ? 1u : 0u) << k;
-                const int bb = (rs < 0 ? 0 : rs) + d; // byte offset of sample 0
-                src[k] = o_raw + (slot * 16 + 4 * i + k) * RAWW + (bb >> 2);
-                shifts |= static_cast<unsigned>(8 * (bb & 3)) << (8 * k);
+        const int ua = (n4 + 31) >> 5;   // units per quad-sum row
+        const int ub = (HALF + 31) >> 5; // units per pattern row
+        int slotA = 0, q1 = 0, q2 = 0, q3 = 0, totalA = 0;
+        const int *blkA = nullptr;
+        if (sa >= 0) {
+            slotA = slot_of(sa);
+            const unsigned gs = sbase + static_cast<unsigned>(sa);
+            if (!mbar_wait_bounded(bar0 + 8 * (SUB_BAR0 + slotA), (gs / SUB_SLOTS) & 1u)) {
+                if (ok)
+                    atomicOr(p.err, DERR_TIMEOUT);
+                ok = false;
             }
-            uint32_t *qrow = &sm[o_Q + (qb * NQROW + r) * HQ];
-            const int t4end = min(n4, (part + 1) * span4);
-#pragma unroll 2
-            for (int t4 = part * span4 + lane; t4 < t4end; t4 += 32) {
-                uint32_t a[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    a[k] = ((live >> k) & 1u) ? __funnelshift_r(sm[src[k] + t4], sm[src[k] + t4 + 1],
-                                                                (shifts >> (8 * k)) & 31u)
-                                              : 0u;
-                // 4x4 byte transpose, then the four channels of each sample summed
-                const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), hi01 = __byte_perm(a[0], a[1], 0x7362);
-                const uint32_t lo23 = __byte_perm(a[2], a[3], 0x5140), hi23 = __byte_perm(a[2], a[3], 0x7362);
-                const uint32_t s0 = __dp4a(__byte_perm(lo01, lo23, 0x5410), 0x01010101u, 0u);
-                const uint32_t s1 = __dp4a(__byte_perm(lo01, lo23, 0x7632), 0x01010101u, 0u);
-                const uint32_t s2 = __dp4a(__byte_perm(hi01, hi23, 0x5410), 0x01010101u, 0u);
-                const uint32_t s3 = __dp4a(__byte_perm(hi01, hi23, 0x7632), 0x01010101u, 0u);
-                uint2 v;
-                v.x = s0 | (s1 << 16);
-                v.y = s2 | (s3 << 16);
-                *reinterpret_cast<uint2 *>(&qrow[2 * t4]) = v;
-            }
+            blkA = reinterpret_cast<const int *>(&sm[o_blk + slotA * SUB_BLK_WORDS]);
+            q1 = blkA[1];
+            q2 = q1 + blkA[2];
+            q3 = q2 + blkA[3];
+            totalA = min(q3 + blkA[4], NQROW);
         }
-        return total * parts;
-    };
-
-    // partial-sum rows of stage s (from Q buffer qb) into P buffer pb.  Work
-    // items are (pattern, part of its row): the parts split each row so that
-    // the patterns fill the warps; the pattern's quad rows, offsets and
-    // their parities are read once per item.  The items continue the warp
-    // rotation of the nA quad-row items built in the same iteration, so the
-    // warps those left short start here.
-    auto buildB = [&](int s, int qb, int pb, int nA) {
-        const int slot = slot_of(s);
-        const int *blk = reinterpret_cast<const int *>(&sm[o_blk + slot * SUB_BLK_WORDS]);
-        const int npat = min(blk[0], NPAT);
-        const int nq = min(4, (NCH - 16 * s + 3) >> 2);
-        const int parts = (npat >= NWARPS) ? 1 : (2 * npat >= NWARPS) ? 2 : (4 * npat >= NWARPS) ? 4 : 8;
-        const int span = (((HALF + parts - 1) / parts) + 31) & ~31; // words per part, whole lane passes
-        for (int item = (warp - nA % NWARPS + NWARPS) % NWARPS; item < npat * parts; item += NWARPS) {
-            const int pp = item / parts;
-            const int part = item - pp * parts;
-            const int key = blk[40 + pp];
-            int qrow[4];
-            unsigned odd = 0u; // bit i: quad i's offset is odd
-            int qbase = 0;
+        const int *blkB = nullptr;
+        int npat = 0, nq = 0;
+        if (sb >= 0) {
+            blkB = reinterpret_cast<const int *>(&sm[o_blk + slot_of(sb) * SUB_BLK_WORDS]);
+            npat = min(blkB[0], NPAT);
+            nq = min(4, (NCH - 16 * sb + 3) >> 2);
+        }
+        const int UA = totalA * ua;
+        const int U = UA + npat * ub;
+        const int uend = ((warp + 1) * U) / NWARPS;
+        int u = (warp * U) / NWARPS;
+        while (u < uend) {
+            if (u < UA) {
+                const int r = u / ua;
+                const int j0 = u - r * ua;
+                const int j1 = min(ua, j0 + (uend - u));
+                u += j1 - j0;
+                const int i = (r >= q3) ? 3 : (r >= q2) ? 2 : (r >= q1) ? 1 : 0;
+                const int base = (i == 3) ? q3 : (i == 2) ? q2 : (i == 1) ? q1 : 0;
+                const unsigned pw = static_cast<unsigned>(blkA[8 + 8 * i + (r - base)]);
+                int src[4];
+                unsigned shifts = 0u, live = 0u; // byte k: bit shift of channel k; bit k: channel k used
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int off = (i == 0) ? 0 : blk[56 + 3 * pp + i - 1];
-                qrow[i] = o_Q + (qb * NQROW + qbase + ((key >> (4 * i)) & 15)) * HQ + (off >> 1);
-                odd |= static_cast<unsigned>(off & 1) << i;
-                qbase += blk[1 + i];
-            }
-            uint32_t *even = &sm[o_P + pb * PBUF + pp * HALF];
-            uint32_t *oddr = even + NPAT * HALF;
-            const int kend = min(HALF, (part + 1) * span);
+                for (int k = 0; k < 4; ++k) {
+                    const int rs = static_cast<int>(sm[o_rsh + slotA * 16 + 4 * i + k]);
+                    const int d = (k == 0) ? 0 : static_cast<int>((pw >> (8 * (k - 1))) & 255u);
+                    live |= (rs >= 0 ? 1u : 0u) << k;
+                    const int bb = (rs < 0 ? 0 : rs) + d; // byte offset of sample 0
+                    src[k] = o_raw + (slotA * 16 + 4 * i + k) * RAWW + (bb >> 2);
+                    shifts |= static_cast<unsigned>(8 * (bb & 3)) << (8 * k);
+                }
+                uint32_t *qrow = &sm[o_Q + (qa * NQROW + r) * HQ];
 #pragma unroll 2
-            for (int k = part * span + lane; k < kend; k += 32) {
-                uint32_t ev = 0u, od = 0u; // (P[2k], P[2k+1]) and (P[2k+1], P[2k+2]) in 16-bit lanes
+                for (int j = j0; j < j1; ++j) {
+                    const int t4 = 32 * j + lane;
+                    if (t4 >= n4)
+                        continue;
+                    uint32_t a[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        a[k] = ((live >> k) & 1u) ? __funnelshift_r(sm[src[k] + t4], sm[src[k] + t4 + 1],
+                                                                    (shifts >> (8 * k)) & 31u)
+                                                  : 0u;
+                    // 4x4 byte transpose, then the four channels of each sample summed
+                    const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), hi01 = __byte_perm(a[0], a[1], 0x7362);
+                    const uint32_t lo23 = __byte_perm(a[2], a[3], 0x5140), hi23 = __byte_perm(a[2], a[3], 0x7362);
+                    const uint32_t s0 = __dp4a(__byte_perm(lo01, lo23, 0x5410), 0x01010101u, 0u);
+                    const uint32_t s1 = __dp4a(__byte_perm(lo01, lo23, 0x7632), 0x01010101u, 0u);
+                    const uint32_t s2 = __dp4a(__byte_perm(hi01, hi23, 0x5410), 0x01010101u, 0u);
+                    const uint32_t s3 = __dp4a(__byte_perm(hi01, hi23, 0x7632), 0x01010101u, 0u);
+                    uint2 v;
+                    v.x = s0 | (s1 << 16);
+                    v.y = s2 | (s3 << 16);
+                    *reinterpret_cast<uint2 *>(&qrow[2 * t4]) = v;
+                }
+            } else {
+                const int v = u - UA;
+                const int pp = v / ub;
+                const int j0 = v - pp * ub;
+                const int j1 = min(ub, j0 + (uend - u));
+                u += j1 - j0;
+                const int key = blkB[40 + pp];
+                int qrow[4];
+                unsigned odd = 0u; // bit i: quad i's offset is odd
+                int qbase = 0;
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
-                    if (i < nq) {
-                        const uint32_t w0 = sm[qrow[i] + k], w1 = sm[qrow[i] + k + 1];
-                        const uint32_t mid = __byte_perm(w0, w1, 0x5432); // high half of w0, low half of w1
-                        const bool o = (odd >> i) & 1u;
-                        ev += o ? mid : w0;
-                        od += o ? w1 : mid;
-                    }
+                    const int off = (i == 0) ? 0 : blkB[56 + 3 * pp + i - 1];
+                    qrow[i] = o_Q + (qb * NQROW + qbase + ((key >> (4 * i)) & 15)) * HQ + (off >> 1);
+                    odd |= static_cast<unsigned>(off & 1) << i;
+                    qbase += blkB[1 + i];
                 }
-                even[k] = ev;
-                oddr[k] = od;
+                uint32_t *even = &sm[o_P + pb * PBUF + pp * HALF];
+                uint32_t *oddr = even + NPAT * HALF;
+#pragma unroll 2
+                for (int j = j0; j < j1; ++j) {
+                    const int k = 32 * j + lane;
+                    if (k >= HALF)
+                        continue;
+                    uint32_t ev = 0u, od = 0u; // (P[2k], P[2k+1]) and (P[2k+1], P[2k+2]) in 16-bit lanes
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        if (i < nq) {
+                            const uint32_t w0 = sm[qrow[i] + k], w1 = sm[qrow[i] + k + 1];
+                            const uint32_t mid = __byte_perm(w0, w1, 0x5432); // high half of w0, low half of w1
+                            const bool o = (odd >> i) & 1u;
+                            ev += o ? mid : w0;
+                            od += o ? w1 : mid;
+                        }
+                    }
+                    even[k] = ev;
+                    oddr[k] = od;
+                }
             }
         }
     };
@@ -1513,21 +1531,16 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
         issue(s);
     __syncthreads();
     if (nstages > 0)
-        buildA(0, 0);
+        build(0, 0, -1, 0, 0);
     fence_proxy_async();
     __syncthreads();
-    {
-        const int nA = (nstages > 1) ? buildA(1, 1) : 0;
-        if (nstages > 0)
-            buildB(0, 0, 0, nA);
-    }
+    if (nstages > 0)
+        build(nstages > 1 ? 1 : -1, 1, 0, 0, 0);
     fence_proxy_async();
     __syncthreads();
 
     for (int s = 0; s < nstages; ++s) {
-        const int nA = (s + 2 < nstages) ? buildA(s + 2, s & 1) : 0;
-        if (s + 1 < nstages)
-            buildB(s + 1, (s + 1) & 1, (s + 1) & 1, nA);
+        build(s + 2 < nstages ? s + 2 : -1, s & 1, s + 1 < nstages ? s + 1 : -1, (s + 1) & 1, (s + 1) & 1);
         if (ok) {
             const int slot = slot_of(s);
             const int4 e4 = *reinterpret_cast<const int4 *>(&sm[o_ent + slot * 64 + 4 * warp]);
