@@ -18,6 +18,8 @@
 // g*64 + DW*w .. DW*w + DW-1, lane l owns outputs t0 + l + 32m (m < M).  The
 // fp32 body uses DW = 4.
 #pragma once
+#include <type_traits>
+
 #include "ddtr_kernels.cuh"
 #include "device_util.cuh"
 
@@ -1414,29 +1416,39 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
                     shifts |= static_cast<unsigned>(8 * (bb & 3)) << (8 * k);
                 }
                 uint32_t *qrow = &sm[o_Q + (qa * NQROW + r) * HQ];
+                // ALL: every channel of the quad is used (all but a band's
+                // last quad), so the loop needs no per-channel select
+                auto pass = [&](auto all) {
+                    constexpr bool ALL = decltype(all)::value;
 #pragma unroll 2
-                for (int j = j0; j < j1; ++j) {
-                    const int t4 = 32 * j + lane;
-                    if (t4 >= n4)
-                        continue;
-                    uint32_t a[4];
+                    for (int j = j0; j < j1; ++j) {
+                        const int t4 = 32 * j + lane;
+                        if (t4 >= n4)
+                            continue;
+                        uint32_t a[4];
 #pragma unroll
-                    for (int k = 0; k < 4; ++k)
-                        a[k] = ((live >> k) & 1u) ? __funnelshift_r(sm[src[k] + t4], sm[src[k] + t4 + 1],
-                                                                    (shifts >> (8 * k)) & 31u)
-                                                  : 0u;
-                    // 4x4 byte transpose, then the four channels of each sample summed
-                    const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), hi01 = __byte_perm(a[0], a[1], 0x7362);
-                    const uint32_t lo23 = __byte_perm(a[2], a[3], 0x5140), hi23 = __byte_perm(a[2], a[3], 0x7362);
-                    const uint32_t s0 = __dp4a(__byte_perm(lo01, lo23, 0x5410), 0x01010101u, 0u);
-                    const uint32_t s1 = __dp4a(__byte_perm(lo01, lo23, 0x7632), 0x01010101u, 0u);
-                    const uint32_t s2 = __dp4a(__byte_perm(hi01, hi23, 0x5410), 0x01010101u, 0u);
-                    const uint32_t s3 = __dp4a(__byte_perm(hi01, hi23, 0x7632), 0x01010101u, 0u);
-                    uint2 v;
-                    v.x = s0 | (s1 << 16);
-                    v.y = s2 | (s3 << 16);
-                    *reinterpret_cast<uint2 *>(&qrow[2 * t4]) = v;
-                }
+                        for (int k = 0; k < 4; ++k) {
+                            const uint32_t f = __funnelshift_r(sm[src[k] + t4], sm[src[k] + t4 + 1],
+                                                               (shifts >> (8 * k)) & 31u);
+                            a[k] = (ALL || ((live >> k) & 1u)) ? f : 0u;
+                        }
+                        // 4x4 byte transpose, then the four channels of each sample summed
+                        const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), hi01 = __byte_perm(a[0], a[1], 0x7362);
+                        const uint32_t lo23 = __byte_perm(a[2], a[3], 0x5140), hi23 = __byte_perm(a[2], a[3], 0x7362);
+                        const uint32_t s0 = __dp4a(__byte_perm(lo01, lo23, 0x5410), 0x01010101u, 0u);
+                        const uint32_t s1 = __dp4a(__byte_perm(lo01, lo23, 0x7632), 0x01010101u, 0u);
+                        const uint32_t s2 = __dp4a(__byte_perm(hi01, hi23, 0x5410), 0x01010101u, 0u);
+                        const uint32_t s3 = __dp4a(__byte_perm(hi01, hi23, 0x7632), 0x01010101u, 0u);
+                        uint2 v;
+                        v.x = s0 | (s1 << 16);
+                        v.y = s2 | (s3 << 16);
+                        *reinterpret_cast<uint2 *>(&qrow[2 * t4]) = v;
+                    }
+                };
+                if (live == 0xFu)
+                    pass(std::true_type{});
+                else
+                    pass(std::false_type{});
             } else {
                 const int v = u - UA;
                 const int pp = v / ub;
@@ -1444,14 +1456,20 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
                 const int j1 = min(ub, j0 + (uend - u));
                 u += j1 - j0;
                 const int key = blkB[40 + pp];
+                // per quad, the byte-permute selectors that take from the
+                // words (w0, w1) = (Q[k + off/2], Q[k + off/2 + 1]) the pair
+                // each phase adds: even offset -> w0 and the middle pair
+                // (high half of w0, low half of w1); odd offset -> the middle
+                // pair and w1
                 int qrow[4];
-                unsigned odd = 0u; // bit i: quad i's offset is odd
+                unsigned selE[4], selO[4];
                 int qbase = 0;
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     const int off = (i == 0) ? 0 : blkB[56 + 3 * pp + i - 1];
                     qrow[i] = o_Q + (qb * NQROW + qbase + ((key >> (4 * i)) & 15)) * HQ + (off >> 1);
-                    odd |= static_cast<unsigned>(off & 1) << i;
+                    selE[i] = (off & 1) ? 0x5432u : 0x3210u;
+                    selO[i] = (off & 1) ? 0x7654u : 0x5432u;
                     qbase += blkB[1 + i];
                 }
                 uint32_t *even = &sm[o_P + pb * PBUF + pp * HALF];
@@ -1466,10 +1484,8 @@ __device__ __forceinline__ bool sub_body(const DdtrLaunch &p, const SubLaunch &S
                     for (int i = 0; i < 4; ++i) {
                         if (i < nq) {
                             const uint32_t w0 = sm[qrow[i] + k], w1 = sm[qrow[i] + k + 1];
-                            const uint32_t mid = __byte_perm(w0, w1, 0x5432); // high half of w0, low half of w1
-                            const bool o = (odd >> i) & 1u;
-                            ev += o ? mid : w0;
-                            od += o ? w1 : mid;
+                            ev += __byte_perm(w0, w1, selE[i]);
+                            od += __byte_perm(w0, w1, selO[i]);
                         }
                     }
                     even[k] = ev;

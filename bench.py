@@ -61,9 +61,9 @@ METRIC_UNCHECKED = "DM-trial*samples/s (plain DDTR, 1 beam per GPU)"
 # range-0 launch of the 4096 ch x 2^18 plan, 2.46 GB algorithmic); the
 # roofline's traffic is each range's ratio times its algorithmic bytes,
 # averaged per launch
-TRAFFIC_PER_ALG_BYTE = {"k_ddtr_quad": (0.96 + 1.35) / 2.46, "k_ddtr_sub": (0.958 + 1.512) / 2.46}
+TRAFFIC_PER_ALG_BYTE = {"k_ddtr_quad": (0.96 + 1.35) / 2.46, "k_ddtr_sub": (0.954 + 1.504) / 2.46}
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one range-0 launch of 4096 ch x 2^18 samples "
-                  "per kernel (k_ddtr_quad 0.96 + 1.35 GB, k_ddtr_sub 0.96 + 1.51 GB, against 2.46 GB algorithmic), "
+                  "per kernel (k_ddtr_quad 0.96 + 1.35 GB, k_ddtr_sub 0.95 + 1.50 GB, against 2.46 GB algorithmic), "
                   "scaled by the algorithmic bytes of each range of this workload; "
                   "profiles/k_ddtr_quad_mid_8bit_4096ch_2e18_range0.md, profiles/k_ddtr_sub_mid_8bit_4096ch_2e18_range0.md")
 PUBLISHED_REALTIME = 6.28  # reference wiki, 8-range "b2" plan, unnamed GPU
