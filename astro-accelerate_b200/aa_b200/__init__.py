@@ -180,6 +180,7 @@ def lib():
         "aa_b200_tuned_ranges_save": ([ctypes.c_char_p], ll),
         "aa_b200_tuned_ranges_load": ([ctypes.c_char_p], ll),
         "aa_b200_tuned_ranges_last_error": ([], ctypes.c_char_p),
+        "aa_b200_tuned_ranges_used": ([], ll),
         "aa_b200_pipeline_range_kernel": ([vp, i, P(i), P(i), P(i), P(i)], i),
         "aa_b200_pipeline_last_error": ([vp], ctypes.c_char_p),
         "aa_b200_pipeline_num_tchunks": ([vp], i),
@@ -1140,6 +1141,11 @@ def tuned_ranges(clear: bool = False) -> int:
     """Autotuner choices kept in this process (one per distinct range shape;
     a later pipeline of the same shape reuses them); clear drops them first."""
     return int(lib().aa_b200_tuned_ranges(1 if clear else 0))
+
+
+def tuned_ranges_used() -> int:
+    """Ranges set up from a kept autotuner choice in this process (not timed)."""
+    return int(lib().aa_b200_tuned_ranges_used())
 
 
 def save_tuned_ranges(path: str) -> int:

@@ -3,6 +3,7 @@
 #include "autotune.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <mutex>
 
@@ -11,7 +12,12 @@ namespace aab200 {
 namespace {
 std::mutex g_tuned_mu;
 std::map<std::vector<long long>, TunedRange> g_tuned;
+std::atomic<long long> g_tuned_uses{0};
 } // namespace
+
+void tuned_range_note_use() { g_tuned_uses.fetch_add(1); }
+
+long long tuned_range_uses() { return g_tuned_uses.load(); }
 
 bool tuned_range_find(const std::vector<long long> &key, TunedRange &out)
 {

@@ -60,6 +60,9 @@ bool tuned_range_find(const std::vector<long long> &key, TunedRange &out);
 void tuned_range_keep(const std::vector<long long> &key, const TunedRange &t);
 // Entries held; clear empties the store first.
 size_t tuned_range_entries(bool clear);
+// Ranges set up from a kept choice (counted by the pipeline that took it).
+void tuned_range_note_use();
+long long tuned_range_uses();
 // The store as a text file (one entry per line), and back: a tuning run's
 // choices reused by later processes (a profiling run, a production run).
 // Loading adds to the entries held.  Return the entries written or read, -1

@@ -1254,6 +1254,8 @@ long long aa_b200_tuned_ranges_load(const char *path)
 
 const char *aa_b200_tuned_ranges_last_error(void) { return g_tuned_error.c_str(); }
 
+long long aa_b200_tuned_ranges_used(void) { return aab200::tuned_range_uses(); }
+
 int aa_b200_pipeline_stage_depth(void *obj, int range)
 {
     Api *a = as_api(obj);

@@ -687,6 +687,46 @@ std::vector<long long> DdtrPipeline::tune_key(int r, const DdtrOp &op, long long
     return k;
 }
 
+// A kept choice is taken only if it is one this range could have been given
+// here: a kernel whose tables the range has, and a channel-quad geometry
+// equal to the one set-up derives for its tile shape and stage depth (row
+// pitch, raw row, row pool sized by the range's own pattern counts) that
+// fits shared memory.  A choice read from a file that fails this (another
+// build, an edited file) is timed again instead.
+bool DdtrPipeline::tuned_valid(const RangeConfig &rc, const TunedRange &t) const
+{
+    if (t.variant == 4)
+        return rc.has_sub && elem_bytes_ == 1;
+    if (t.variant == 3)
+        return elem_bytes_ == 2 && (t.f32_cs == 4 || t.f32_cs == 8 || t.f32_cs == 16 || t.f32_cs == 32);
+    if (t.variant != 2 && t.variant != 5 && t.variant != 6)
+        return false;
+    const QuadGeometry &q = t.quad;
+    if (!rc.has_quad || elem_bytes_ != 1 || (q.M != 8 && q.M != 16) ||
+        (q.qs != 1 && q.qs != 2 && q.qs != 4 && q.qs != 8) || q.npool != rc_npool(rc, q.qs))
+        return false;
+    const QuadGeometry G = quad_geometry(rc.quad_span, rc.quad_dmax, rc.quad_maxcnt, rc.group_dms, rc.nquads, q.M,
+                                         q.qs, q.npool);
+    if (q.W != G.W || q.raww != G.raww || q.nq_pad != G.nq_pad)
+        return false;
+    QuadLaunch ql{};
+    ql.raww = q.raww;
+    ql.nq_pad = q.nq_pad;
+    ql.W = q.W;
+    ql.qs = q.qs;
+    ql.npool = q.npool;
+    // the stage-depth tuner's own bound (the per-CTA opt-in limit)
+    const size_t limit = 227 * 1024;
+    if (t.variant == 6)
+        return q.M == 16 && rc.quad_ws_ok && quadsp_smem_bytes(ql) <= limit;
+    if (t.variant == 5)
+        return q.M == 16 && rc.quad_ws_ok && quadws_smem_bytes(ql) <= limit;
+    const int f = t.quad_flavour;
+    const bool flavour_ok = (f == -1) || (f == 0) || (f == 2 && q.M == 8) || ((f == 1 || f == 4) && q.M == 16) ||
+                            ((f == 5 || f == 6 || f == 7) && q.M == 16 && rc.quad_ws_ok);
+    return flavour_ok && G.smem_bytes <= limit;
+}
+
 // Stage depth of every range that runs a staged kernel, timed on chunk 0's
 // job (the buffers hold zeros at this point; the kernels' work does not
 // depend on the sample values).  A range whose key was tuned before in this
@@ -710,7 +750,7 @@ bool DdtrPipeline::tune_ranges()
         const long long pitch = opt_.device_output ? strategy_.total_samps(static_cast<int>(r)) : op->tp;
         const std::vector<long long> key = tune_key(static_cast<int>(r), *op, pitch);
         TunedRange kept;
-        if (tuned_range_find(key, kept)) {
+        if (tuned_range_find(key, kept) && tuned_valid(rc, kept)) {
             if (rc.d_qtmp) {
                 // the offset table for the kept tile's row pitch
                 if (kept.quad.W != rc.quad.W) {
@@ -728,6 +768,7 @@ bool DdtrPipeline::tune_ranges()
             rc.quad = kept.quad;
             rc.quad_flavour = kept.quad_flavour;
             rc.f32.cs = kept.f32_cs;
+            tuned_range_note_use();
             continue;
         }
         DdtrJob job;

@@ -27,6 +27,7 @@
 namespace aab200 {
 
 struct StageTuneCache;
+struct TunedRange;
 
 enum class RunStatus : int { error = -1, finished = 0, has_more = 1, finished_component = 2 };
 
@@ -236,6 +237,7 @@ private:
     bool build_sub_tables(int r);
     bool tune_ranges();
     std::vector<long long> tune_key(int r, const DdtrOp &op, long long pitch) const;
+    bool tuned_valid(const RangeConfig &rc, const TunedRange &t) const;
     bool step(bool allow_sync);
     bool enumerate_ops();
     bool exec_corner_turn(const DdtrOp &op);

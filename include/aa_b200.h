@@ -525,6 +525,10 @@ long long aa_b200_tuned_ranges(int clear);
 long long aa_b200_tuned_ranges_save(const char *path);
 long long aa_b200_tuned_ranges_load(const char *path);
 const char *aa_b200_tuned_ranges_last_error(void);
+/* Ranges set up from a kept choice in this process, without timing.  A kept
+ * choice that does not fit the range (a file from another build, an edited
+ * file) is not taken: the range is timed again.  Host only. */
+long long aa_b200_tuned_ranges_used(void);
 /* The kernel shape a range runs (after set-up, which includes the
  * autotuner): the channel-quad flavour (-1 for other kernels; 0 with the
  * per-byte path, 1 with its warp switch, 4 loading every DM trial's word

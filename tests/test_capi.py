@@ -117,6 +117,7 @@ def test_tuned_range_file_roundtrip(aa, tmp_path):
     with pytest.raises(OSError, match="cannot open"):
         aa.load_tuned_ranges(str(tmp_path / "missing.txt"))
     assert aa.tuned_ranges(clear=True) == 0
+    assert aa.tuned_ranges_used() == 0  # no pipeline has been set up here
 
 
 def test_batch_kernel_choice_is_checked(aa):

@@ -182,8 +182,9 @@ def test_autotuned_tile_shape_matches_oracle(aa, oracle_mod, cuda_device, name):
 def test_tuned_choices_kept_for_the_next_pipeline(aa, oracle_mod, cuda_device, tmp_path, name):
     """The autotuner's choices are kept per range shape: after a round trip
     through a file, a second pipeline of the same shape (set up explicitly,
-    twice: set-up is idempotent) adds no entry, runs the same kernel shapes
-    and gives the same bits as the first and as the oracle."""
+    twice: set-up is idempotent) takes them without timing, adds no entry,
+    runs the same kernel shapes and gives the same bits as the first and as
+    the oracle; choices that do not fit the range are not taken."""
     case = C.CASES[name]
     x = C.make_input(case)
     aa.tuned_ranges(clear=True)
@@ -195,13 +196,28 @@ def test_tuned_choices_kept_for_the_next_pipeline(aa, oracle_mod, cuda_device, t
     assert aa.save_tuned_ranges(path) == kept
     aa.tuned_ranges(clear=True)
     assert aa.load_tuned_ranges(path) == kept
+    used = aa.tuned_ranges_used()
     second, info2, _, _ = run_pipeline(aa, case, x, variant=0, explicit_setup=True)
     assert aa.tuned_ranges() == kept
+    assert aa.tuned_ranges_used() - used >= kept
     assert info2 == info1
     for a, b in zip(first, second):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     s, want, kern = oracle_run(oracle_mod, case, x)
     assert_matches_oracle(case, s, second, want, kern)
+    # an edited file (an unknown kernel in every entry): its choices are not
+    # taken, the ranges are timed again, the output is the same
+    lines = open(path).read().splitlines()
+    fields = [ln.split() for ln in lines[1:]]
+    with open(path, "w") as f:
+        f.write("\n".join([lines[0]] + [" ".join(v[:-10] + ["9"] + v[-9:]) for v in fields]) + "\n")
+    aa.tuned_ranges(clear=True)
+    assert aa.load_tuned_ranges(path) == kept
+    used = aa.tuned_ranges_used()
+    third, _, _, _ = run_pipeline(aa, case, x, variant=0)
+    assert aa.tuned_ranges_used() == used
+    for a, b in zip(first, third):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
 WS_CASES = [n for n in LIGHT if C.CASES[n]["nbits"] <= 8]
