@@ -80,6 +80,17 @@ def test_periodicity_plan_needs_its_component_and_a_ddtr_plan(aa):
         p.delete()
 
 
+def test_setup_needs_a_bound_plan(aa):
+    """Explicit set-up before a DDTR plan is bound is refused with a message
+    (host only: no device call is made)."""
+    md = aa.filterbank_metadata_struct(0.0, 64e-6, 1550.0, -0.39, 8, 1 << 16, 256, 0.0)
+    p = aa.aa_py_pipeline(aa.aa_py_pipeline_components(True, False, False, False),
+                          aa.aa_py_pipeline_component_options(), md, np.zeros(256 * (1 << 16), np.uint16), 0)
+    assert not p.setup()
+    assert "no DDTR plan bound" in p.last_error()
+    p.delete()
+
+
 def test_strategy_refusal_codes(aa):
     import pytest
     with pytest.raises(ValueError):
